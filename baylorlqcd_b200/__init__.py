@@ -1,0 +1,359 @@
+"""B200-native solver hot path of the BaylorLQCD ``qqcd`` code.
+
+Python mirror of the reference's Fortran interface for the path (modules diracops,
+inverters, quark and disconloops) over the C ABI of ``libqqcd_gpu.so``
+(``include/qqcd_gpu.h``).  Arrays use the reference's own layouts:
+
+* Dirac half-vector ``g(6, ntotal, 4, 2, 8)`` -> numpy shape ``(8, 2, 4, ntotal, 6)``
+  (C order equals the Fortran column-major order);
+* gauge field ``u(18, ntotal, 4, 2, 16)`` -> numpy shape ``(16, 2, 4, ntotal, 18)``.
+
+Arrays may be numpy arrays (host) or torch CUDA tensors (device, zero copy).  There is
+no CPU fallback: constructing a :class:`Lattice` without a CUDA device raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "libqqcd_gpu.so"
+
+QQ_OK, QQ_NOT_CONVERGED, QQ_NAN, QQ_BAD_ARG, QQ_CUDA_ERR, QQ_ABORTED, QQ_NO_DEVICE, QQ_SINGULAR = range(8)
+STATUS_NAMES = {0: "OK", 1: "NOT_CONVERGED", 2: "NAN", 3: "BAD_ARG", 4: "CUDA_ERR", 5: "ABORTED",
+                6: "NO_DEVICE", 7: "SINGULAR"}
+
+# Every symbol of include/qqcd_gpu.h
+EXPORTED = [
+    "qq_ctx_create", "qq_ctx_destroy", "qq_ctx_dims", "qq_last_error", "qq_set_coact",
+    "qq_gauge_upload", "qq_hsingle", "qq_hdouble", "qq_hdbletm", "qq_twmshift", "qq_vecdot",
+    "qq_defl_create", "qq_defl_destroy", "qq_defl_size", "qq_gmresdr", "qq_gmresproj", "qq_psc",
+    "qq_bicgstab", "qq_fermprop", "qq_pointsource", "qq_fermprop_batch", "qq_initlagfib",
+    "qq_rnds", "qq_z2source", "qq_z4source", "qq_twaverage_level0", "qq_bench_hsingle",
+]
+
+
+class QQError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+class qq_geom(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("nt", C.c_int),
+                ("bc", C.c_int * 4), ("c1", C.c_double * 4), ("c2", C.c_double * 4)]
+
+
+class qq_solve_info(C.Structure):
+    _fields_ = [("status", C.c_int), ("itercount", C.c_int), ("mvp", C.c_int), ("ncycles", C.c_int),
+                ("true_rel", C.c_double), ("seconds", C.c_double), ("nhist", C.c_int),
+                ("hist", C.c_double * 1024), ("hist_mvp", C.c_int * 1024), ("nritz", C.c_int),
+                ("ritz", C.c_double * 1024)]
+
+
+class qq_method(C.Structure):
+    _fields_ = [("m", C.c_int), ("k", C.c_int), ("precision", C.c_int), ("rhs_block", C.c_int),
+                ("tol", C.c_double), ("max_outer", C.c_int)]
+
+
+@dataclass
+class SolveInfo:
+    status: int
+    itercount: int
+    mvp: int
+    ncycles: int
+    true_rel: float
+    seconds: float
+    hist: np.ndarray
+    hist_mvp: np.ndarray
+    ritz: np.ndarray
+
+    @classmethod
+    def from_c(cls, s: qq_solve_info) -> "SolveInfo":
+        n = s.nhist
+        nr = s.nritz
+        r = np.array(s.ritz[: 2 * nr]).reshape(nr, 2)
+        return cls(s.status, s.itercount, s.mvp, s.ncycles, s.true_rel, s.seconds,
+                   np.array(s.hist[:n]), np.array(s.hist_mvp[:n]), r[:, 0] + 1j * r[:, 1])
+
+
+_lib = None
+
+
+def load_library() -> C.CDLL:
+    """Load libqqcd_gpu.so, building it with nvcc first if it is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        from . import build as _b
+        _b.build()
+    lib = C.CDLL(str(LIB_PATH))
+    P = C.c_void_p
+    I = C.c_int
+    D = C.c_double
+    IP = C.POINTER(C.c_int)
+    DP = C.POINTER(C.c_double)
+    sig = {
+        "qq_ctx_create": ([C.POINTER(qq_geom), I, C.POINTER(P)], I),
+        "qq_ctx_destroy": ([P], I),
+        "qq_ctx_dims": ([P, IP, IP], I),
+        "qq_last_error": ([], C.c_char_p),
+        "qq_set_coact": ([P, DP, DP], I),
+        "qq_gauge_upload": ([P, P, I], I),
+        "qq_hsingle": ([P, P, P, I, I], I),
+        "qq_hdouble": ([P, P, P, I, D], I),
+        "qq_hdbletm": ([P, P, P, I, DP, I], I),
+        "qq_twmshift": ([P, P, P, I, DP, I], I),
+        "qq_vecdot": ([P, P, P, DP], I),
+        "qq_defl_create": ([P, I, I, C.POINTER(P)], I),
+        "qq_defl_destroy": ([P], I),
+        "qq_defl_size": ([P], I),
+        "qq_gmresdr": ([P, P, P, IP, D, I, DP, I, P, C.POINTER(qq_solve_info)], I),
+        "qq_gmresproj": ([P, P, P, IP, D, I, DP, I, P, C.POINTER(qq_solve_info)], I),
+        "qq_psc": ([P, P, P, IP, D, I, DP, I, I, P, C.POINTER(qq_solve_info)], I),
+        "qq_bicgstab": ([P, P, P, D, I, DP, I, I, C.POINTER(qq_solve_info)], I),
+        "qq_fermprop": ([P, P, P, DP, I, D, I, IP, P, P, I, I, P, C.POINTER(qq_solve_info)], I),
+        "qq_pointsource": ([P, P, P, IP, I, I], I),
+        "qq_fermprop_batch": ([P, I, P, P, DP, C.POINTER(qq_method), P, P, C.POINTER(qq_solve_info)], I),
+        "qq_initlagfib": ([I, I], I),
+        "qq_rnds": ([I, DP], I),
+        "qq_z2source": ([P, P, P], I),
+        "qq_z4source": ([P, P, P], I),
+        "qq_twaverage_level0": ([P, P, P, P, P, D, P], I),
+        "qq_bench_hsingle": ([P, I, I, I, I, DP, DP], I),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = res
+    _lib = lib
+    return lib
+
+
+def _check(status: int, allow_not_converged: bool = False) -> int:
+    if status == QQ_OK or (allow_not_converged and status == QQ_NOT_CONVERGED):
+        return status
+    msg = load_library().qq_last_error().decode(errors="replace")
+    raise QQError(status, msg)
+
+
+def _ptr(a) -> int:
+    if isinstance(a, np.ndarray):
+        if not (a.flags["C_CONTIGUOUS"] and a.dtype == np.float64):
+            raise ValueError("reference arrays must be C-contiguous float64")
+        return a.ctypes.data
+    if hasattr(a, "data_ptr"):
+        return int(a.data_ptr())
+    raise TypeError(f"unsupported array type {type(a)}")
+
+
+def _d2(v) -> C.Array:
+    arr = (C.c_double * 2)()
+    arr[0], arr[1] = float(v[0]), float(v[1])
+    return arr
+
+
+def _i2(v) -> C.Array:
+    arr = (C.c_int * 2)()
+    arr[0], arr[1] = int(v[0]), int(v[1])
+    return arr
+
+
+class Deflation:
+    """Deflation space of GMRES-DR (replaces module ``shift`` of Q/shift.f90)."""
+
+    def __init__(self, lat: "Lattice", nmax: int, kmax: int):
+        self.lat = lat
+        self._h = C.c_void_p()
+        _check(lat.lib.qq_defl_create(lat._ctx, nmax, kmax, C.byref(self._h)))
+
+    @property
+    def k(self) -> int:
+        return self.lat.lib.qq_defl_size(self._h)
+
+    def close(self):
+        if self._h:
+            self.lat.lib.qq_defl_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Lattice:
+    """One lattice (geometry, action coefficients and gauge field) on one GPU.
+
+    bc: boundary factors (1 periodic, -1 antiperiodic, 0 fixed), the reference's
+    bc(mu).  c1, c2: coact(3,1,mu) and coact(3,2,mu) (1.0 for the isotropic,
+    tadpole-free actions of every configuration)."""
+
+    def __init__(self, nx, ny, nz, nt, bc=(1, 1, 1, -1), c1=(1.0,) * 4, c2=(1.0,) * 4, device=0):
+        self.lib = load_library()
+        g = qq_geom(nx, ny, nz, nt, (C.c_int * 4)(*bc), (C.c_double * 4)(*c1), (C.c_double * 4)(*c2))
+        self._ctx = C.c_void_p()
+        _check(self.lib.qq_ctx_create(C.byref(g), device, C.byref(self._ctx)))
+        nv, nt_ = C.c_int(), C.c_int()
+        _check(self.lib.qq_ctx_dims(self._ctx, C.byref(nv), C.byref(nt_)))
+        self.dims = (nx, ny, nz, nt)
+        self.bc = tuple(bc)
+        self.nvhalf, self.ntotal = nv.value, nt_.value
+
+    # ---- shapes ----
+    @property
+    def half_shape(self):
+        return (8, 2, 4, self.ntotal, 6)
+
+    @property
+    def gauge_shape(self):
+        return (16, 2, 4, self.ntotal, 18)
+
+    def new_half(self) -> np.ndarray:
+        return np.zeros(self.half_shape)
+
+    def close(self):
+        if self._ctx:
+            self.lib.qq_ctx_destroy(self._ctx)
+            self._ctx = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- gauge ----
+    def gauge_upload(self, u, recon: int = 0):
+        _check(self.lib.qq_gauge_upload(self._ctx, _ptr(u), recon))
+
+    def set_coact(self, c1, c2):
+        _check(self.lib.qq_set_coact(self._ctx, (C.c_double * 4)(*c1), (C.c_double * 4)(*c2)))
+
+    # ---- operator (Q/diracops.f90) ----
+    def hsingle(self, gin, idag: int, gblclr: int, out=None):
+        out = self.new_half() if out is None else out
+        _check(self.lib.qq_hsingle(self._ctx, _ptr(out), _ptr(gin), idag, gblclr))
+        return out
+
+    def hdouble(self, ge, idag: int, kappa: float, out=None):
+        out = self.new_half() if out is None else out
+        _check(self.lib.qq_hdouble(self._ctx, _ptr(out), _ptr(ge), idag, float(kappa)))
+        return out
+
+    def hdbletm(self, ge, idag: int, kappa, iflag: int = -1, out=None):
+        out = self.new_half() if out is None else out
+        _check(self.lib.qq_hdbletm(self._ctx, _ptr(out), _ptr(ge), idag, _d2(kappa), iflag))
+        return out
+
+    def twmshift(self, gwhole, idag: int, kappa, iflag: int = -1, out=None):
+        out = np.zeros((2,) + self.half_shape) if out is None else out
+        _check(self.lib.qq_twmshift(self._ctx, _ptr(out), _ptr(gwhole), idag, _d2(kappa), iflag))
+        return out
+
+    def vecdot(self, a, b) -> complex:
+        r = (C.c_double * 2)()
+        _check(self.lib.qq_vecdot(self._ctx, _ptr(a), _ptr(b), r))
+        return complex(r[0], r[1])
+
+    # ---- inverters (Q/inverters.f90) ----
+    def deflation(self, nmax: int, kmax: int) -> Deflation:
+        return Deflation(self, nmax, kmax)
+
+    def gmresdr(self, phi, x, GMRES, resmax, itermin=0, kappa=(0.15, 0.0), iflag=-1, defl=None):
+        info = qq_solve_info()
+        st = self.lib.qq_gmresdr(self._ctx, _ptr(phi), _ptr(x), _i2(GMRES), float(resmax), itermin,
+                                 _d2(kappa), iflag, defl._h if defl else None, C.byref(info))
+        _check(st, allow_not_converged=True)
+        return x, SolveInfo.from_c(info)
+
+    def gmresproj(self, b, x, GMRES, resmax, itermin=0, kappa=(0.15, 0.0), iflag=-1, defl=None):
+        info = qq_solve_info()
+        st = self.lib.qq_gmresproj(self._ctx, _ptr(b), _ptr(x), _i2(GMRES), float(resmax), itermin,
+                                   _d2(kappa), iflag, defl._h, C.byref(info))
+        _check(st, allow_not_converged=True)
+        return x, SolveInfo.from_c(info)
+
+    def psc(self, b, x, GMRES, resmax, itermin=0, kappa=(0.15, 0.0), iflag=-1, isignal=1, defl=None):
+        info = qq_solve_info()
+        st = self.lib.qq_psc(self._ctx, _ptr(b), _ptr(x), _i2(GMRES), float(resmax), itermin,
+                             _d2(kappa), iflag, isignal, defl._h, C.byref(info))
+        _check(st, allow_not_converged=True)
+        return x, SolveInfo.from_c(info)
+
+    def bicgstab(self, phi, x, resmax, itermin=0, kappa=(0.15, 0.0), iflag=-1, maxiter=0):
+        info = qq_solve_info()
+        st = self.lib.qq_bicgstab(self._ctx, _ptr(phi), _ptr(x), float(resmax), itermin, _d2(kappa),
+                                  iflag, maxiter, C.byref(info))
+        _check(st, allow_not_converged=True)
+        return x, SolveInfo.from_c(info)
+
+    # ---- propagators (Q/quark.f90) ----
+    def fermprop(self, be, bo, kappa, inverter=5, resmax=1e-10, itermin=0, nGMRES=(30, 10),
+                 ntmqcd=0, isignal=1, defl=None, xe=None, xo=None):
+        xe = self.new_half() if xe is None else xe
+        xo = self.new_half() if xo is None else xo
+        info = qq_solve_info()
+        st = self.lib.qq_fermprop(self._ctx, _ptr(be), _ptr(bo), _d2(kappa), inverter, float(resmax),
+                                  itermin, _i2(nGMRES), _ptr(xe), _ptr(xo), ntmqcd, isignal,
+                                  defl._h if defl else None, C.byref(info))
+        _check(st, allow_not_converged=True)
+        return xe, xo, SolveInfo.from_c(info)
+
+    def pointsource(self, src, icsrc: int, idsrc: int):
+        be, bo = self.new_half(), self.new_half()
+        _check(self.lib.qq_pointsource(self._ctx, _ptr(be), _ptr(bo), (C.c_int * 4)(*src), icsrc, idsrc))
+        return be, bo
+
+    def fermprop_batch(self, be, bo, kappa, m=60, k=20, precision=32, rhs_block=4, tol=1e-10,
+                       max_outer=50, xe=None, xo=None):
+        """Batched accelerated solve: be, bo of shape (nrhs,) + half_shape."""
+        nrhs = be.shape[0]
+        xe = np.zeros_like(be) if xe is None else xe
+        xo = np.zeros_like(bo) if xo is None else xo
+        infos = (qq_solve_info * nrhs)()
+        meth = qq_method(m, k, precision, rhs_block, tol, max_outer)
+        st = self.lib.qq_fermprop_batch(self._ctx, nrhs, _ptr(be), _ptr(bo), _d2(kappa), C.byref(meth),
+                                        _ptr(xe), _ptr(xo), infos)
+        _check(st, allow_not_converged=True)
+        return xe, xo, [SolveInfo.from_c(i) for i in infos]
+
+    # ---- noise sources and traces (Q/disconloops.f90) ----
+    def z2source(self):
+        be, bo = self.new_half(), self.new_half()
+        _check(self.lib.qq_z2source(self._ctx, _ptr(be), _ptr(bo)))
+        return be, bo
+
+    def z4source(self):
+        be, bo = self.new_half(), self.new_half()
+        _check(self.lib.qq_z4source(self._ctx, _ptr(be), _ptr(bo)))
+        return be, bo
+
+    def twaverage_level0(self, be, bo, xe, xo, kappa: float):
+        J = np.zeros((6, self.dims[3], 2))
+        _check(self.lib.qq_twaverage_level0(self._ctx, _ptr(be), _ptr(bo), _ptr(xe), _ptr(xo),
+                                            float(kappa), _ptr(J)))
+        return J
+
+
+    def bench_hsingle(self, precision=64, nrhs=1, niter=20, flush_l2=True):
+        """Mean kernel time (ms) and algorithmic bytes of one hopping-term launch."""
+        ms, by = C.c_double(), C.c_double()
+        _check(self.lib.qq_bench_hsingle(self._ctx, precision, nrhs, niter, int(flush_l2),
+                                         C.byref(ms), C.byref(by)))
+        return ms.value, by.value
+
+
+def initlagfib(myid: int, iseed: int):
+    _check(load_library().qq_initlagfib(myid, iseed))
+
+
+def rnds(m: int) -> np.ndarray:
+    out = np.zeros(m)
+    _check(load_library().qq_rnds(m, out.ctypes.data_as(C.POINTER(C.c_double))))
+    return out

@@ -1,0 +1,165 @@
+// Internal context of the B200 qqcd library (host side).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <complex>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/qqcd_gpu.h"
+#include "qq_blas.cuh"
+#include "qq_dense.h"
+#include "qq_dslash.cuh"
+#include "qq_launch.h"
+#include "qq_layout.cuh"
+
+namespace qq {
+
+int set_error(int code, const std::string& msg);
+
+#define QQ_CK(x)                                                                    \
+  do {                                                                              \
+    cudaError_t e_ = (x);                                                           \
+    if (e_ != cudaSuccess)                                                          \
+      return ::qq::set_error(QQ_CUDA_ERR, std::string(#x) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+#define QQ_TRY(x)             \
+  do {                        \
+    int s_ = (x);             \
+    if (s_ != QQ_OK) return s_; \
+  } while (0)
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() {
+    if (p) cudaFree(p);
+  }
+  cudaError_t alloc(size_t b) {
+    if (b <= bytes && p) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+    cudaError_t e = cudaMalloc(&p, b);
+    if (e == cudaSuccess) bytes = b;
+    return e;
+  }
+  template <class T>
+  T* as() const {
+    return static_cast<T*>(p);
+  }
+};
+
+// A Dirac half-vector in GPU layout.
+struct Field {
+  DevBuf data, norm;
+  int prec = P64;
+  Spinor sp() const { return Spinor{data.p, norm.as<float>(), prec}; }
+};
+
+inline size_t field_bytes(int prec, int vh) {
+  return prec == P64 ? (size_t)192 * vh : prec == P32 ? (size_t)96 * vh : (size_t)48 * vh;
+}
+
+// Deflation space: k+1 basis vectors (GPU layout, precision pb) and the projected
+// (k+1) x k matrix of A V_k = V_{k+1} Hk.
+struct DeflSpace {
+  int k = 0;
+  int pb = P64;
+  size_t nel = 0;
+  DevBuf V;
+  dense::Mat Hk;
+};
+
+}  // namespace qq
+
+struct qq_defl {
+  qq_ctx* ctx;
+  int nmax, kmax;
+  qq::DeflSpace space;
+};
+
+struct qq_ctx {
+  int device = 0;
+  cudaStream_t st = nullptr;
+  qq::Geom g{};
+  qq::RefDims rd{};
+  double c1[4], c2[4];
+  qq::DevBuf gauge64, gauge32;
+  int recon64 = 0;
+  bool have_gauge = false;
+  qq::DevBuf stage[4];      // reference-layout staging buffers
+  qq::DevBuf partial;       // reduction partials
+  qq::DevBuf scal;          // device scalar slots
+  double* hpin = nullptr;   // pinned host mirror of scalar results
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::vector<std::unique_ptr<qq::Field>> pool[3];  // temporaries per precision
+  std::vector<bool> pool_busy[3];
+
+  size_t ref_doubles() const { return (size_t)6 * rd.ntotal * 64; }
+};
+
+namespace qq {
+
+// Temporary field from the context pool (returned on scope exit).
+struct Tmp {
+  qq_ctx* c;
+  int prec;
+  int idx;
+  Field* f;
+  Tmp(qq_ctx* c_, int prec_);
+  ~Tmp();
+  Spinor sp() const { return f->sp(); }
+  Tmp(const Tmp&) = delete;
+  Tmp& operator=(const Tmp&) = delete;
+};
+
+// ---- operator and level-1 helpers (qq_ops.cu) ----
+int op_hsingle(qq_ctx* c, Spinor out, Spinor in, int idag, int pout);
+int op_hsingle_multi(qq_ctx* c, const Spinor* out, const Spinor* in, int n, int idag, int pout);
+// he = Hdbletm(ge), tmp is an odd-parity temporary of the same precision.
+int op_dbletm(qq_ctx* c, Spinor out, Spinor in, Spinor tmp, int idag, const double kappa[2]);
+int op_dbletm_multi(qq_ctx* c, const Spinor* out, const Spinor* in, const Spinor* tmp, int n,
+                    int idag, const double kappa[2]);
+int lin(qq_ctx* c, Spinor out, Coef a, Spinor x, Coef b = cimm(0), Spinor y = Spinor{nullptr, nullptr, P64},
+        Coef cc = cimm(0), Spinor z = Spinor{nullptr, nullptr, P64}, double* nrm2_dev = nullptr);
+int dot_dev(qq_ctx* c, Spinor x, Spinor y, double* out3);  // out3 = {re, im, |y|^2}
+int dot_host(qq_ctx* c, Spinor x, Spinor y, std::complex<double>* d, double* ynrm2);
+int norm2_host(qq_ctx* c, Spinor x, double* n2);
+int copy_field(qq_ctx* c, Spinor out, Spinor in);
+int zero_field(qq_ctx* c, Spinor f);
+int read_scalars(qq_ctx* c, const double* dev, int n, double* host);
+
+// reference layout <-> GPU layout
+int ref_to_field(qq_ctx* c, const double* ref_dev, int parity, Spinor out);
+int field_to_ref(qq_ctx* c, Spinor in, int parity, double* ref_dev);
+// Stage a caller pointer (host or device) into device memory; returns device ptr.
+int stage_in(qq_ctx* c, int slot, const double* p, size_t ndoubles, const double** dev);
+int stage_out_begin(qq_ctx* c, int slot, double* p, size_t ndoubles, double** dev);
+int stage_out_end(qq_ctx* c, int slot, double* p, size_t ndoubles, double* dev);
+bool is_device_ptr(const void* p);
+
+// ---- Krylov solvers (qq_solvers.cu) ----
+struct SolveStats {
+  int itercount = 0, mvp = 0, ncycles = 0;
+  double true_rel = 0.0;
+  std::vector<double> hist;
+  std::vector<int> hist_mvp;
+  std::vector<std::complex<double>> ritz;
+};
+
+// Reference-faithful FP64 GMRES-DR (Q/inverters.f90:2871-3572 semantics).
+int gmresdr_fp64(qq_ctx* c, Spinor phi, Spinor x, int m, int k, double resmax, int itermin,
+                 const double kappa[2], DeflSpace* defl, SolveStats* st);
+int gmresproj_fp64(qq_ctx* c, Spinor b, Spinor x, int m, int k, double resmax, int itermin,
+                   const double kappa[2], const DeflSpace& defl, SolveStats* st);
+int bicgstab_fp64(qq_ctx* c, Spinor phi, Spinor x, double resmax, int itermin, int maxiter,
+                  const double kappa[2], SolveStats* st);
+
+void fill_info(qq_solve_info* info, int status, const SolveStats& s, double seconds);
+
+}  // namespace qq

@@ -1,0 +1,313 @@
+// Instantiations and launchers of the library's CUDA kernels (sm_100a).
+#include "qq_blas.cuh"
+#include "qq_dslash.cuh"
+#include "qq_launch.h"
+#include "qq_layout.cuh"
+
+namespace qq {
+
+// ---------------------------------------------------------------------------
+// Dslash
+// ---------------------------------------------------------------------------
+template <int SP, int LP, int RECON, int NRHS>
+static cudaError_t hop_epi(const HopArgs& a, int epi, cudaStream_t st) {
+  dim3 blk(128), grd((a.g.vh + 127) / 128);
+  switch (epi) {
+    case EPI_STORE: hop_kernel<SP, LP, RECON, NRHS, EPI_STORE><<<grd, blk, 0, st>>>(a); break;
+    case EPI_TWIST: hop_kernel<SP, LP, RECON, NRHS, EPI_TWIST><<<grd, blk, 0, st>>>(a); break;
+    case EPI_DBLE: hop_kernel<SP, LP, RECON, NRHS, EPI_DBLE><<<grd, blk, 0, st>>>(a); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+template <int SP>
+static cudaError_t hop_low(const HopArgs& a, int epi, cudaStream_t st) {
+  switch (a.nrhs) {
+    case 1: return hop_epi<SP, P32, 12, 1>(a, epi, st);
+    case 2: return hop_epi<SP, P32, 12, 2>(a, epi, st);
+    case 3: return hop_epi<SP, P32, 12, 3>(a, epi, st);
+    case 4: return hop_epi<SP, P32, 12, 4>(a, epi, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t launch_hop(const HopArgs& a, int sp, int recon, int epi, cudaStream_t st) {
+  if (sp == P64) {
+    if (a.nrhs != 1) return cudaErrorInvalidValue;
+    if (recon == 18) return hop_epi<P64, P64, 18, 1>(a, epi, st);
+    if (recon == 12) return hop_epi<P64, P64, 12, 1>(a, epi, st);
+    return cudaErrorInvalidValue;
+  }
+  if (sp == P32) return hop_low<P32>(a, epi, st);
+  if (sp == P16) return hop_low<P16>(a, epi, st);
+  return cudaErrorInvalidValue;
+}
+
+// ---------------------------------------------------------------------------
+// Level 1
+// ---------------------------------------------------------------------------
+template <int PX, int PY, int PZ, int PO>
+static cudaError_t lin4(const LinArgs& L, cudaStream_t st) {
+  lincomb_kernel<PX, PY, PZ, PO><<<kRedBlocks, kRedThreads, 0, st>>>(L);
+  return cudaGetLastError();
+}
+
+// Supported combinations: all operands of one precision, or FP64 output with any
+// single lower-precision operand in x (promotion), or lower output from FP64 x
+// (demotion).
+cudaError_t launch_lincomb(const LinArgs& L, int px, int py, int pz, int po, cudaStream_t st) {
+  if (!L.y.data) py = po;
+  if (!L.z.data) pz = po;
+  if (!L.x.data) px = po;
+  if (px == po && py == po && pz == po) {
+    if (po == P64) return lin4<P64, P64, P64, P64>(L, st);
+    if (po == P32) return lin4<P32, P32, P32, P32>(L, st);
+    if (po == P16) return lin4<P16, P16, P16, P16>(L, st);
+  }
+  if (po == P64 && py == P64 && pz == P64) {
+    if (px == P32) return lin4<P32, P64, P64, P64>(L, st);
+    if (px == P16) return lin4<P16, P64, P64, P64>(L, st);
+  }
+  if (px == P64 && py == po && pz == po) {
+    if (po == P32) return lin4<P64, P32, P32, P32>(L, st);
+    if (po == P16) return lin4<P64, P16, P16, P16>(L, st);
+  }
+  if (po == P16 && px == P32 && py == P16 && pz == P16) return lin4<P32, P16, P16, P16>(L, st);
+  if (po == P32 && px == P16 && py == P32 && pz == P32) return lin4<P16, P32, P32, P32>(L, st);
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_dot(int vh, Spinor x, Spinor y, double* partial, cudaStream_t st) {
+  if (x.prec == P64 && y.prec == P64)
+    dot_kernel<P64, P64><<<kRedBlocks, kRedThreads, 0, st>>>(vh, x, y, partial);
+  else if (x.prec == P32 && y.prec == P32)
+    dot_kernel<P32, P32><<<kRedBlocks, kRedThreads, 0, st>>>(vh, x, y, partial);
+  else if (x.prec == P16 && y.prec == P16)
+    dot_kernel<P16, P16><<<kRedBlocks, kRedThreads, 0, st>>>(vh, x, y, partial);
+  else if (x.prec == P64 && y.prec == P32)
+    dot_kernel<P64, P32><<<kRedBlocks, kRedThreads, 0, st>>>(vh, x, y, partial);
+  else if (x.prec == P32 && y.prec == P64)
+    dot_kernel<P32, P64><<<kRedBlocks, kRedThreads, 0, st>>>(vh, x, y, partial);
+  else
+    return cudaErrorInvalidValue;
+  return cudaGetLastError();
+}
+
+__global__ void finalize_sum_kernel(const double* partial, int nblocks, int nvstride, int nout,
+                                    double* out, int add) {
+  const int v = blockIdx.x;
+  if (v >= nout) return;
+  __shared__ double red[256];
+  double s = 0.0;
+  for (int b = threadIdx.x; b < nblocks; b += blockDim.x) s += partial[(size_t)b * nvstride + v];
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[v] = add ? out[v] + red[0] : red[0];
+}
+
+cudaError_t launch_finalize(const double* partial, int nblocks, int nvstride, int nout,
+                            double* out, int add, cudaStream_t st) {
+  finalize_sum_kernel<<<nout, 256, 0, st>>>(partial, nblocks, nvstride, nout, out, add);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Krylov basis
+// ---------------------------------------------------------------------------
+cudaError_t launch_multidot(int pb, const BasisArgs& V, int nv, const void* w, double* partial,
+                            int* ngroups_out, cudaStream_t st) {
+  const int ng = (nv + 7) / 8;
+  *ngroups_out = ng;
+  dim3 grd(kRedBlocks, ng);
+  if (pb == P64)
+    multidot_kernel<P64><<<grd, kRedThreads, 0, st>>>(V, nv, w, partial);
+  else if (pb == P32)
+    multidot_kernel<P32><<<grd, kRedThreads, 0, st>>>(V, nv, w, partial);
+  else
+    return cudaErrorInvalidValue;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_multiaxpy(int pb, const BasisArgs& V, int nv, const double* h, double hsign,
+                             const void* w, void* wout, double* partial, cudaStream_t st) {
+  if (nv > 128) return cudaErrorInvalidValue;
+  if (pb == P64)
+    multiaxpy_kernel<P64><<<kRedBlocks, kRedThreads, 0, st>>>(V, nv, h, hsign, w, wout, partial);
+  else if (pb == P32)
+    multiaxpy_kernel<P32><<<kRedBlocks, kRedThreads, 0, st>>>(V, nv, h, hsign, w, wout, partial);
+  else
+    return cudaErrorInvalidValue;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_normalize(int pb, size_t nel, const void* in, void* out, const double* nrm2,
+                             cudaStream_t st) {
+  if (pb == P64)
+    normalize_kernel<P64><<<kRedBlocks, kRedThreads, 0, st>>>(nel, in, out, nrm2);
+  else if (pb == P32)
+    normalize_kernel<P32><<<kRedBlocks, kRedThreads, 0, st>>>(nel, in, out, nrm2);
+  else
+    return cudaErrorInvalidValue;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rotate(int pb, const BasisArgs& V, int nin, int nout, const double* Z, int ldz,
+                          cudaStream_t st) {
+  const size_t smem = sizeof(double) * 2 * (size_t)nin * nout;
+  if (smem > 200 * 1024 || nout > 64) return cudaErrorInvalidValue;
+  const int grid = 148 * 4;
+#define QQ_ROT(PB, MO)                                                                       \
+  do {                                                                                       \
+    auto k = rotate_kernel<PB, MO>;                                                          \
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);         \
+    k<<<grid, 128, smem, st>>>(V, nin, nout, Z, ldz);                                        \
+  } while (0)
+  if (pb == P64) {
+    if (nout <= 16) QQ_ROT(P64, 16);
+    else if (nout <= 32) QQ_ROT(P64, 32);
+    else QQ_ROT(P64, 64);
+  } else if (pb == P32) {
+    if (nout <= 16) QQ_ROT(P32, 16);
+    else if (nout <= 32) QQ_ROT(P32, 32);
+    else QQ_ROT(P32, 64);
+  } else {
+    return cudaErrorInvalidValue;
+  }
+#undef QQ_ROT
+  return cudaGetLastError();
+}
+
+cudaError_t launch_basis_accum(int pb, const BasisArgs& V, int nv, const double* y, int vh,
+                               Spinor x, cudaStream_t st) {
+  if (nv > 128) return cudaErrorInvalidValue;
+  if (pb == P64 && x.prec == P64)
+    basis_accum_kernel<P64, P64><<<kRedBlocks, kRedThreads, 0, st>>>(V, nv, y, vh, x);
+  else if (pb == P32 && x.prec == P64)
+    basis_accum_kernel<P32, P64><<<kRedBlocks, kRedThreads, 0, st>>>(V, nv, y, vh, x);
+  else if (pb == P32 && x.prec == P32)
+    basis_accum_kernel<P32, P32><<<kRedBlocks, kRedThreads, 0, st>>>(V, nv, y, vh, x);
+  else
+    return cudaErrorInvalidValue;
+  return cudaGetLastError();
+}
+
+__global__ void hcol_update_kernel(double* H, int ldh, int j, const double* h2, int nh,
+                                   const double* nrm2) {
+  const int t = threadIdx.x;
+  double* col = H + 2 * (size_t)ldh * j;
+  for (int i = t; i < nh; i += blockDim.x) {
+    col[2 * i] += h2[2 * i];
+    col[2 * i + 1] += h2[2 * i + 1];
+  }
+  if (t == 0) {
+    col[2 * (j + 1)] = sqrt(nrm2[0]);
+    col[2 * (j + 1) + 1] = 0.0;
+  }
+}
+
+cudaError_t launch_hcol_update(double* H, int ldh, int j, const double* h2, int nh,
+                               const double* nrm2, cudaStream_t st) {
+  hcol_update_kernel<<<1, 128, 0, st>>>(H, ldh, j, h2, nh, nrm2);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Layout
+// ---------------------------------------------------------------------------
+cudaError_t launch_spinor_from_ref(const Geom& g, const RefDims& d, int p, const double* ref,
+                                   Spinor out, cudaStream_t st) {
+  dim3 blk(128), grd((g.vh + 127) / 128);
+  if (out.prec == P64)
+    spinor_from_ref_kernel<P64><<<grd, blk, 0, st>>>(g, d, p, ref, out);
+  else if (out.prec == P32)
+    spinor_from_ref_kernel<P32><<<grd, blk, 0, st>>>(g, d, p, ref, out);
+  else
+    spinor_from_ref_kernel<P16><<<grd, blk, 0, st>>>(g, d, p, ref, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_spinor_to_ref(const Geom& g, const RefDims& d, int p, Spinor in, double* ref,
+                                 cudaStream_t st) {
+  dim3 blk(128), grd((g.vh + 127) / 128);
+  if (in.prec == P64)
+    spinor_to_ref_kernel<P64><<<grd, blk, 0, st>>>(g, d, p, in, ref);
+  else if (in.prec == P32)
+    spinor_to_ref_kernel<P32><<<grd, blk, 0, st>>>(g, d, p, in, ref);
+  else
+    spinor_to_ref_kernel<P16><<<grd, blk, 0, st>>>(g, d, p, in, ref);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ref_zero_halo(const RefDims& d, double* ref, cudaStream_t st) {
+  if (d.ntotal == d.nvhalf) return cudaSuccess;
+  ref_zero_halo_kernel<<<148, 256, 0, st>>>(d, ref);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gauge_from_ref(const Geom& g, const RefDims& d, const double* ref, void* out,
+                                  int prec, int recon, cudaStream_t st) {
+  dim3 blk(128), grd((2 * g.vh + 127) / 128);
+  if (prec == P64 && recon == 18)
+    gauge_from_ref_kernel<P64, 18><<<grd, blk, 0, st>>>(g, d, ref, out);
+  else if (prec == P64 && recon == 12)
+    gauge_from_ref_kernel<P64, 12><<<grd, blk, 0, st>>>(g, d, ref, out);
+  else if (prec == P32 && recon == 12)
+    gauge_from_ref_kernel<P32, 12><<<grd, blk, 0, st>>>(g, d, ref, out);
+  else
+    return cudaErrorInvalidValue;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_su3_defect(const Geom& g, const RefDims& d, const double* ref, double* partial,
+                              cudaStream_t st) {
+  su3_defect_kernel<<<kRedBlocks, 256, 0, st>>>(g, d, ref, partial);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Spin mixing: out = a x + ta J(x) + b y + tb J(y)
+// ---------------------------------------------------------------------------
+template <int P>
+__global__ void spinmix_kernel(int vh, Spinor x, Spinor y, Spinor out, double a, double ta,
+                               double b, double tb) {
+  using R = typename SpinorIO<P>::R;
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < vh; s += gridDim.x * blockDim.x) {
+    cplx<R> xv[12], yv[12], o[12];
+    SpinorIO<P>::load(x.data, x.norm, vh, s, xv);
+    if (y.data)
+      SpinorIO<P>::load(y.data, y.norm, vh, s, yv);
+    else
+      for (int c = 0; c < 12; ++c) yv[c] = {(R)0, (R)0};
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      // J(v) = (v2, v3, -v0, -v1)
+      o[0 + c] = cadd(cadd(cscale((R)a, xv[0 + c]), cscale((R)ta, xv[6 + c])),
+                      cadd(cscale((R)b, yv[0 + c]), cscale((R)tb, yv[6 + c])));
+      o[3 + c] = cadd(cadd(cscale((R)a, xv[3 + c]), cscale((R)ta, xv[9 + c])),
+                      cadd(cscale((R)b, yv[3 + c]), cscale((R)tb, yv[9 + c])));
+      o[6 + c] = cadd(csub(cscale((R)a, xv[6 + c]), cscale((R)ta, xv[0 + c])),
+                      csub(cscale((R)b, yv[6 + c]), cscale((R)tb, yv[0 + c])));
+      o[9 + c] = cadd(csub(cscale((R)a, xv[9 + c]), cscale((R)ta, xv[3 + c])),
+                      csub(cscale((R)b, yv[9 + c]), cscale((R)tb, yv[3 + c])));
+    }
+    SpinorIO<P>::store(out.data, out.norm, vh, s, o);
+  }
+}
+
+cudaError_t launch_spinmix(int vh, Spinor x, Spinor y, Spinor out, double a, double ta, double b,
+                           double tb, int prec, cudaStream_t st) {
+  if (prec == P64)
+    spinmix_kernel<P64><<<kRedBlocks, kRedThreads, 0, st>>>(vh, x, y, out, a, ta, b, tb);
+  else if (prec == P32)
+    spinmix_kernel<P32><<<kRedBlocks, kRedThreads, 0, st>>>(vh, x, y, out, a, ta, b, tb);
+  else
+    spinmix_kernel<P16><<<kRedBlocks, kRedThreads, 0, st>>>(vh, x, y, out, a, ta, b, tb);
+  return cudaGetLastError();
+}
+
+}  // namespace qq

@@ -1,0 +1,256 @@
+// Operator application, level-1 helpers and reference-layout staging for the C ABI.
+#include <cstring>
+#include <string>
+
+#include "qq_ctx.h"
+
+namespace qq {
+
+static thread_local std::string g_last_error;
+
+int set_error(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+const char* last_error() { return g_last_error.c_str(); }
+
+Tmp::Tmp(qq_ctx* c_, int prec_) : c(c_), prec(prec_), idx(-1), f(nullptr) {
+  auto& pool = c->pool[prec];
+  auto& busy = c->pool_busy[prec];
+  for (size_t i = 0; i < pool.size(); ++i)
+    if (!busy[i]) {
+      idx = (int)i;
+      break;
+    }
+  if (idx < 0) {
+    pool.emplace_back(new Field());
+    busy.push_back(false);
+    idx = (int)pool.size() - 1;
+    Field* nf = pool.back().get();
+    nf->prec = prec;
+    if (nf->data.alloc(field_bytes(prec, c->g.vh)) != cudaSuccess) {
+      f = nullptr;
+      return;
+    }
+    if (prec == P16) nf->norm.alloc(sizeof(float) * c->g.vh);
+  }
+  busy[idx] = true;
+  f = pool[idx].get();
+}
+
+Tmp::~Tmp() {
+  if (idx >= 0) c->pool_busy[prec][idx] = false;
+}
+
+bool is_device_ptr(const void* p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+int stage_in(qq_ctx* c, int slot, const double* p, size_t n, const double** dev) {
+  if (!p) return set_error(QQ_BAD_ARG, "null array");
+  if (is_device_ptr(p)) {
+    *dev = p;
+    return QQ_OK;
+  }
+  QQ_CK(c->stage[slot].alloc(n * sizeof(double)));
+  QQ_CK(cudaMemcpyAsync(c->stage[slot].p, p, n * sizeof(double), cudaMemcpyHostToDevice, c->st));
+  *dev = c->stage[slot].as<double>();
+  return QQ_OK;
+}
+
+int stage_out_begin(qq_ctx* c, int slot, double* p, size_t n, double** dev) {
+  if (!p) return set_error(QQ_BAD_ARG, "null array");
+  if (is_device_ptr(p)) {
+    *dev = p;
+    return QQ_OK;
+  }
+  QQ_CK(c->stage[slot].alloc(n * sizeof(double)));
+  *dev = c->stage[slot].as<double>();
+  return QQ_OK;
+}
+
+int stage_out_end(qq_ctx* c, int slot, double* p, size_t n, double* dev) {
+  if (dev != p) QQ_CK(cudaMemcpyAsync(p, dev, n * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  (void)slot;
+  return QQ_OK;
+}
+
+int ref_to_field(qq_ctx* c, const double* ref_dev, int parity, Spinor out) {
+  QQ_CK(launch_spinor_from_ref(c->g, c->rd, parity, ref_dev, out, c->st));
+  return QQ_OK;
+}
+
+int field_to_ref(qq_ctx* c, Spinor in, int parity, double* ref_dev) {
+  QQ_CK(launch_ref_zero_halo(c->rd, ref_dev, c->st));
+  QQ_CK(launch_spinor_to_ref(c->g, c->rd, parity, in, ref_dev, c->st));
+  return QQ_OK;
+}
+
+static HopArgs hop_base(qq_ctx* c, int idag, int pout, int prec) {
+  HopArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.g = c->g;
+  a.c = make_hopcoef(c->c1, c->c2, idag);
+  a.pout = pout;
+  a.gauge = prec == P64 ? c->gauge64.p : c->gauge32.p;
+  return a;
+}
+
+static int recon_of(qq_ctx* c, int prec) { return prec == P64 ? c->recon64 : 12; }
+
+int op_hsingle_multi(qq_ctx* c, const Spinor* out, const Spinor* in, int n, int idag, int pout) {
+  if (!c->have_gauge) return set_error(QQ_BAD_ARG, "no gauge field uploaded");
+  const int prec = in[0].prec;
+  for (int r0 = 0; r0 < n; r0 += 4) {
+    const int nb = std::min(4, n - r0);
+    HopArgs a = hop_base(c, idag, pout, prec);
+    a.nrhs = prec == P64 ? 1 : nb;
+    const int step = a.nrhs;
+    for (int r = 0; r < step; ++r) {
+      a.in[r] = in[r0 + r].data;
+      a.in_norm[r] = in[r0 + r].norm;
+      a.out[r] = out[r0 + r].data;
+      a.out_norm[r] = out[r0 + r].norm;
+    }
+    QQ_CK(launch_hop(a, prec, recon_of(c, prec), EPI_STORE, c->st));
+    if (prec == P64 && nb > 1) {  // FP64 runs one right-hand side per launch
+      for (int r = 1; r < nb; ++r) {
+        a.in[0] = in[r0 + r].data;
+        a.out[0] = out[r0 + r].data;
+        QQ_CK(launch_hop(a, prec, recon_of(c, prec), EPI_STORE, c->st));
+      }
+    }
+  }
+  return QQ_OK;
+}
+
+int op_hsingle(qq_ctx* c, Spinor out, Spinor in, int idag, int pout) {
+  return op_hsingle_multi(c, &out, &in, 1, idag, pout);
+}
+
+int op_dbletm_multi(qq_ctx* c, const Spinor* out, const Spinor* in, const Spinor* tmp, int n,
+                    int idag, const double kappa[2]) {
+  if (!c->have_gauge) return set_error(QQ_BAD_ARG, "no gauge field uploaded");
+  const int prec = in[0].prec;
+  const bool wilson = kappa[1] < 0.00000001;  // Q/diracops.f90:467
+  const int maxb = prec == P64 ? 1 : 4;
+  for (int r0 = 0; r0 < n; r0 += maxb) {
+    const int nb = std::min(maxb, n - r0);
+    HopArgs a = hop_base(c, idag, 1, prec);
+    a.nrhs = nb;
+    for (int r = 0; r < nb; ++r) {
+      a.in[r] = in[r0 + r].data;
+      a.in_norm[r] = in[r0 + r].norm;
+      a.out[r] = tmp[r0 + r].data;
+      a.out_norm[r] = tmp[r0 + r].norm;
+    }
+    a.a = 2.0 * kappa[0] * kappa[1];
+    QQ_CK(launch_hop(a, prec, recon_of(c, prec), wilson ? EPI_STORE : EPI_TWIST, c->st));
+    HopArgs b = hop_base(c, idag, 0, prec);
+    b.nrhs = nb;
+    for (int r = 0; r < nb; ++r) {
+      b.in[r] = tmp[r0 + r].data;
+      b.in_norm[r] = tmp[r0 + r].norm;
+      b.out[r] = out[r0 + r].data;
+      b.out_norm[r] = out[r0 + r].norm;
+      b.aux[r] = in[r0 + r].data;
+      b.aux_norm[r] = in[r0 + r].norm;
+    }
+    b.f1 = 1.0 / (kappa[0] * kappa[0]);
+    if (wilson) {
+      b.f2 = 0.0;
+      b.f3 = 1.0;
+    } else {
+      const double t = 2.0 * kappa[0] * kappa[1];
+      b.f2 = 2.0 * kappa[1] / kappa[0];
+      b.f3 = 1.0 / (1.0 + t * t);
+    }
+    QQ_CK(launch_hop(b, prec, recon_of(c, prec), EPI_DBLE, c->st));
+  }
+  return QQ_OK;
+}
+
+int op_dbletm(qq_ctx* c, Spinor out, Spinor in, Spinor tmp, int idag, const double kappa[2]) {
+  return op_dbletm_multi(c, &out, &in, &tmp, 1, idag, kappa);
+}
+
+int lin(qq_ctx* c, Spinor out, Coef a, Spinor x, Coef b, Spinor y, Coef cc, Spinor z,
+        double* nrm2_dev) {
+  LinArgs L;
+  std::memset(&L, 0, sizeof(L));
+  L.vh = c->g.vh;
+  L.x = x;
+  L.y = y;
+  L.z = z;
+  L.out = out;
+  L.a = a;
+  L.b = b;
+  L.c = cc;
+  L.red = nrm2_dev ? 1 : 0;
+  L.partial = c->partial.as<double>();
+  QQ_CK(launch_lincomb(L, x.prec, y.prec, z.prec, out.prec, c->st));
+  if (nrm2_dev) QQ_CK(launch_finalize(L.partial, kRedBlocks, 3, 1, nrm2_dev, 0, c->st));
+  return QQ_OK;
+}
+
+int dot_dev(qq_ctx* c, Spinor x, Spinor y, double* out3) {
+  QQ_CK(launch_dot(c->g.vh, x, y, c->partial.as<double>(), c->st));
+  QQ_CK(launch_finalize(c->partial.as<double>(), kRedBlocks, 3, 3, out3, 0, c->st));
+  return QQ_OK;
+}
+
+int read_scalars(qq_ctx* c, const double* dev, int n, double* host) {
+  QQ_CK(cudaMemcpyAsync(c->hpin, dev, sizeof(double) * n, cudaMemcpyDeviceToHost, c->st));
+  QQ_CK(cudaStreamSynchronize(c->st));
+  std::memcpy(host, c->hpin, sizeof(double) * n);
+  return QQ_OK;
+}
+
+int dot_host(qq_ctx* c, Spinor x, Spinor y, std::complex<double>* d, double* ynrm2) {
+  double* s = c->scal.as<double>();
+  QQ_TRY(dot_dev(c, x, y, s));
+  double h[3];
+  QQ_TRY(read_scalars(c, s, 3, h));
+  if (d) *d = {h[0], h[1]};
+  if (ynrm2) *ynrm2 = h[2];
+  return QQ_OK;
+}
+
+int norm2_host(qq_ctx* c, Spinor x, double* n2) { return dot_host(c, x, x, nullptr, n2); }
+
+int copy_field(qq_ctx* c, Spinor out, Spinor in) { return lin(c, out, cimm(1.0), in); }
+
+int zero_field(qq_ctx* c, Spinor f) {
+  QQ_CK(cudaMemsetAsync(f.data, 0, field_bytes(f.prec, c->g.vh), c->st));
+  if (f.prec == P16 && f.norm) QQ_CK(cudaMemsetAsync(f.norm, 0, sizeof(float) * c->g.vh, c->st));
+  return QQ_OK;
+}
+
+void fill_info(qq_solve_info* info, int status, const SolveStats& s, double seconds) {
+  if (!info) return;
+  std::memset(info, 0, sizeof(*info));
+  info->status = status;
+  info->itercount = s.itercount;
+  info->mvp = s.mvp;
+  info->ncycles = s.ncycles;
+  info->true_rel = s.true_rel;
+  info->seconds = seconds;
+  info->nhist = (int)std::min<size_t>(s.hist.size(), 1024);
+  for (int i = 0; i < info->nhist; ++i) {
+    info->hist[i] = s.hist[i];
+    info->hist_mvp[i] = s.hist_mvp[i];
+  }
+  info->nritz = (int)std::min<size_t>(s.ritz.size(), 512);
+  for (int i = 0; i < info->nritz; ++i) {
+    info->ritz[2 * i] = s.ritz[i].real();
+    info->ritz[2 * i + 1] = s.ritz[i].imag();
+  }
+}
+
+}  // namespace qq

@@ -1,0 +1,185 @@
+/* qqcd_gpu.h -- C ABI of the B200 solver library for the qqcd hot path.
+ *
+ * Every entry point takes plain pointers and sizes, returns an int status (never
+ * aborts) and mirrors one routine of the reference Fortran modules diracops,
+ * inverters, quark and disconloops.  Array arguments use the reference's own
+ * Fortran layouts (column-major, 1-based in the comments below):
+ *
+ *   Dirac half-vector  g(6, ntotal, 4, 2, 8)   real(8)   Q/diracops.f90:41-59
+ *   Gauge field        u(18, ntotal, 4, 2, 16) real(8)   Q/diracops.f90:312-313
+ *
+ * with nvhalf = nx*ny*nz*nt/32 and ntotal = nvhalf + nbmax (one process, nps = 1,
+ * basics.f90:20-31).  Pointers may be host or device memory (detected with
+ * cudaPointerGetAttributes); host arrays are staged through the library's own device
+ * buffers.  Calls on one context are stream ordered and return after the result is
+ * complete.  One context per host thread.
+ */
+#ifndef QQCD_GPU_H
+#define QQCD_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define QQ_OK 0
+#define QQ_NOT_CONVERGED 1
+#define QQ_NAN 2
+#define QQ_BAD_ARG 3
+#define QQ_CUDA_ERR 4
+#define QQ_ABORTED 5
+#define QQ_NO_DEVICE 6
+#define QQ_SINGULAR 7
+
+typedef struct qq_ctx qq_ctx;
+typedef struct qq_defl qq_defl;
+
+/* Lattice geometry and action coefficients.  Replaces the compile-time latdims
+ * (U/latdims.f90:61-70), bc (U/cfgspropsmain.f90:334-337) and the fermion part of
+ * coact (G/lattice.f90:426-429): c1[mu] = coact(3,1,mu), c2[mu] = coact(3,2,mu). */
+typedef struct qq_geom {
+  int nx, ny, nz, nt; /* each a multiple of 4 (latdims.f90:11-13) */
+  int bc[4];          /* 1 periodic, -1 antiperiodic, 0 fixed */
+  double c1[4];
+  double c2[4];
+} qq_geom;
+
+/* Per-solve report (replaces the CFGSPROPS.LOG lines of the reference). */
+typedef struct qq_solve_info {
+  int status;
+  int itercount;      /* Krylov iterations, as the reference counts them */
+  int mvp;            /* applications of the even-odd operator */
+  int ncycles;
+  double true_rel;    /* ||phi - A x|| / ||phi|| on the even system, FP64 */
+  double seconds;     /* device time of the solve */
+  int nhist;          /* per-cycle true relative residuals (gmresdr-norm lines) */
+  double hist[1024];
+  int hist_mvp[1024];
+  int nritz;          /* harmonic Ritz values of the last restart (re, im) */
+  double ritz[2 * 512];
+} qq_solve_info;
+
+/* ---- context ---- */
+int qq_ctx_create(const qq_geom* geom, int device, qq_ctx** out);
+int qq_ctx_destroy(qq_ctx* ctx);
+/* Reference array sizes: nvhalf and ntotal of basics.f90:23-31. */
+int qq_ctx_dims(const qq_ctx* ctx, int* nvhalf, int* ntotal);
+/* Text of the last error on this thread. */
+const char* qq_last_error(void);
+/* Replace coact(3,1,:), coact(3,2,:) (fermpropR's r = -1 flip, Q/quark.f90:921-926). */
+int qq_set_coact(qq_ctx* ctx, const double c1[4], const double c2[4]);
+
+/* ---- gauge field ----
+ * u_ref: reference u(18,ntotal,4,2,16).  recon: 18, 12, or 0 = choose 12 when every
+ * link's third row equals conj(row1 x row2) to 1e-12, else 18.  Also builds the
+ * FP32 recon-12 copy used by the mixed-precision solvers. */
+int qq_gauge_upload(qq_ctx* ctx, const double* u_ref, int recon);
+
+/* ---- Dirac operator (Q/diracops.f90) ---- */
+/* Hsingle :554-599.  gout = H_eo gin (gblclr = 1) or H_oe gin (gblclr = 2).
+ * idag = 1 flips the sign of gamma_mu (H^dagger).  gout's halo slots are zeroed;
+ * gin's halo slots are neither read nor written. */
+int qq_hsingle(qq_ctx* ctx, double* gout, const double* gin, int idag, int gblclr);
+/* Hdouble :264-346.  he = (1/kappa^2 - H_eo H_oe) ge. */
+int qq_hdouble(qq_ctx* ctx, double* he, const double* ge, int idag, double kappa);
+/* Hdbletm :435-550, iflag = -1 (Wilson / twisted mass; the clover branch iflag = -2
+ * is out of scope and returns QQ_BAD_ARG).  kappa[0] = kappa, kappa[1] = mu. */
+int qq_hdbletm(qq_ctx* ctx, double* he, const double* ge, int idag, const double kappa[2],
+               int iflag);
+/* twMshift :1863-1995, iflag = -1.  gwhole/hwhole hold the gblclr = 1 half followed
+ * by the gblclr = 2 half (each 6*ntotal*64 doubles). */
+int qq_twmshift(qq_ctx* ctx, double* hwhole, const double* gwhole, int idag,
+                const double kappa[2], int iflag);
+/* vecdot Q/inverters.f90:13485-13530: adb = sum a^dagger b (FP64). */
+int qq_vecdot(qq_ctx* ctx, const double* a, const double* b, double adb[2]);
+
+/* ---- inverters (Q/inverters.f90) ----
+ * The deflation handle replaces the module variables of Q/shift.f90 (vtemp, hcnew,
+ * beg) and Q/gmresrhs.f90 (isignal) that carry the GMRES-DR eigenvectors to
+ * GMRES-Proj. */
+int qq_defl_create(qq_ctx* ctx, int nmax, int kmax, qq_defl** out);
+int qq_defl_destroy(qq_defl* d);
+/* Number k of deflation vectors held (0 before a GMRES-DR solve). */
+int qq_defl_size(const qq_defl* d);
+
+/* gmresdr :2871-3572.  Solves Hdbletm x = phi.  GMRES[0] = n, GMRES[1] = k.
+ * x: initial guess on entry, solution on exit.  defl (optional) receives the k+1
+ * deflation vectors and the (k+1) x k projected matrix. */
+int qq_gmresdr(qq_ctx* ctx, const double* phi, double* x, const int GMRES[2], double resmax,
+               int itermin, const double kappa[2], int iflag, qq_defl* defl,
+               qq_solve_info* info);
+/* gmresproject :7183-8304 with sigma = 0: GMRES(GMRES[0]) cycles, each preceded by
+ * a minimum-residual projection over the k = GMRES[1] deflation vectors of defl.
+ * The initial guess is zero, as in the reference. */
+int qq_gmresproj(qq_ctx* ctx, const double* b, double* x, const int GMRES[2], double resmax,
+                 int itermin, const double kappa[2], int iflag, const qq_defl* defl,
+                 qq_solve_info* info);
+/* psc :4310-4465.  isignal = 1: gmresdr, keeping the deflation space in defl;
+ * isignal = 2: gmresproj(n - k, k) to the reference's fixed 1e-8 (resmax unused). */
+int qq_psc(qq_ctx* ctx, const double* b, double* x, const int GMRES[2], double resmax,
+           int itermin, const double kappa[2], int iflag, int isignal, qq_defl* defl,
+           qq_solve_info* info);
+/* bicgstab :302-487.  maxiter <= 0 means no limit beyond the reference's. */
+int qq_bicgstab(qq_ctx* ctx, const double* phi, double* x, double resmax, int itermin,
+                const double kappa[2], int iflag, int maxiter, qq_solve_info* info);
+
+/* ---- propagators (Q/quark.f90) ---- */
+/* fermprop :458-842 for nkappa = -1 (Wilson / twisted-mass Wilson, cSW = 0):
+ * source preparation, inverter (0 bicgstab, 5 gmresdr, 6 psc), odd-half
+ * reconstruction and, if ntmqcd != 0 and |mu| > 1e-4, the twisted-basis rotation
+ * (gamma5vector :3484-3548).  bo is read only.  isignal and defl as for qq_psc. */
+int qq_fermprop(qq_ctx* ctx, const double* be, const double* bo, const double kappa[2],
+                int inverter, double resmax, int itermin, const int nGMRES[2], double* xe,
+                double* xo, int ntmqcd, int isignal, qq_defl* defl, qq_solve_info* info);
+/* pointsource :46-108 (src is 1-based global coordinates). */
+int qq_pointsource(qq_ctx* ctx, double* be, double* bo, const int src[4], int icsrc, int idsrc);
+
+/* ---- batched mixed-precision propagators (the accelerated method) ----
+ * Solves nrhs systems M x = b on the full lattice to the FP64 true residual
+ * ||b - M x|| / ||b|| <= tol.  The first right-hand side builds the deflation space
+ * with mixed-precision GMRES-DR(m, k) (FP32 Krylov basis and FP32 operator inside
+ * FP64 iterative refinement); the others are projected onto it and solved together
+ * in blocks with a multi-right-hand-side FP32 (precision = 32) or FP16 (precision =
+ * 16) BiCGStab inside FP64 reliable updates.  be/bo/xe/xo: nrhs reference-layout
+ * halves each, packed one after the other. */
+typedef struct qq_method {
+  int m, k;          /* GMRES-DR(m, k) for the first right-hand side */
+  int precision;     /* 64 (plain FP64 GMRES-DR per RHS), 32 or 16 */
+  int rhs_block;     /* right-hand sides per multi-RHS block (1..8) */
+  double tol;        /* FP64 true relative residual target */
+  int max_outer;     /* refinement steps limit */
+} qq_method;
+int qq_fermprop_batch(qq_ctx* ctx, int nrhs, const double* be, const double* bo,
+                      const double kappa[2], const qq_method* method, double* xe, double* xo,
+                      qq_solve_info* infos);
+
+/* ---- noise sources and loop traces (Q/disconloops.f90, G/lagfib.f90) ---- */
+/* initlagfib G/lagfib.f90:80-92 (process-global generator state, as the reference). */
+int qq_initlagfib(int myid, int iseed);
+/* rnds G/lagfib.f90:219-259. */
+int qq_rnds(int m, double* rn);
+/* z2source :4583-4649 and z4source (active branch) :4518-4570. */
+int qq_z2source(qq_ctx* ctx, double* be, double* bo);
+int qq_z4source(qq_ctx* ctx, double* be, double* bo);
+/* Unsubtracted time-slice traces of one noise solution, the level-0 operators of
+ * twAverage (Q/vevbleft.f90:2541-4704): J(2, nt, 6), op 1 = J4 point-split time
+ * current, 2 = psibar psi, 3..5 = J1..J3 point-split spatial currents,
+ * 6 = psibar gamma5 psi; kappa scaling of Q/disconloops.f90:4045-4049 applied. */
+int qq_twaverage_level0(qq_ctx* ctx, const double* be, const double* bo, const double* xe,
+                        const double* xo, double kappa, double* J);
+
+/* ---- measurement (library-specific; no counterpart in the reference) ----
+ * Times `niter` launches of the hopping kernel alone (H_oe of random fields, output
+ * parity gblclr = 2) with CUDA events on the library's stream.  precision: 64
+ * (links at the uploaded recon), 32 or 16 (FP32 recon-12 links); nrhs right-hand
+ * sides per launch (1 for FP64).  flush_l2 != 0 overwrites a 512 MiB buffer between
+ * launches so every launch reads its operands from HBM.  ms_per_call: mean kernel
+ * time; bytes_per_call: algorithmic bytes of one launch,
+ * V/2 * (8 * link bytes + nrhs * 2 * spinor bytes). */
+int qq_bench_hsingle(qq_ctx* ctx, int precision, int nrhs, int niter, int flush_l2,
+                     double* ms_per_call, double* bytes_per_call);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* QQCD_GPU_H */

@@ -1,0 +1,338 @@
+"""CPU oracle for the qqcd solver hot path -- TEST INFRASTRUCTURE ONLY.
+
+ctypes wrapper of oracle/_build/liboracle.so, the line-by-line C++ restatement of the
+reference Fortran routines (see oracle/oracle.h for the file:line of each).  Parity is
+UNPINNED against the Fortran itself (no Fortran compiler here, and the reference ships
+no golden vectors); it is pinned against analytic known answers and scipy LAPACK in
+tests/.  Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "_build" / "liboracle.so"
+
+_lib = None
+
+
+def build() -> Path:
+    srcs = list(HERE.glob("*.cpp")) + list(HERE.glob("*.h"))
+    if not LIB.exists() or LIB.stat().st_mtime < max(p.stat().st_mtime for p in srcs):
+        subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+    return LIB
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        build()
+        L = C.CDLL(str(LIB))
+        P, I, D = C.c_void_p, C.c_int, C.c_double
+        IP, DP = C.POINTER(C.c_int), C.POINTER(C.c_double)
+        sig = {
+            "oq_geom_create": ([I, I, I, I, IP, DP, DP], P),
+            "oq_geom_destroy": ([P], None),
+            "oq_nvhalf": ([P], I), "oq_ntotal": ([P], I), "oq_nbmax": ([P], I),
+            "oq_tables": ([P, IP, IP, IP, IP, IP, IP, IP, IP], None),
+            "oq_set_coact": ([P, DP, DP], None),
+            "oq_site_of_coords": ([P, IP, IP, IP, IP, IP, IP], None),
+            "oq_initlagfib": ([I, I], None),
+            "oq_rnds": ([I, DP], None),
+            "oq_lagfib_state": ([IP, IP, IP], None),
+            "oq_lagfib_set_state": ([IP, I, I], None),
+            "oq_pointsource": ([P, DP, DP, IP, I, I], None),
+            "oq_z2source": ([P, DP, DP], None),
+            "oq_z4source": ([P, DP, DP], None),
+            "oq_hsingle": ([P, DP, DP, DP, I, I], None),
+            "oq_hdouble": ([P, DP, DP, DP, I, D], None),
+            "oq_hdbletm": ([P, DP, DP, DP, I, DP], None),
+            "oq_twmshift": ([P, DP, DP, DP, I, DP], None),
+            "oq_gam5x": ([P, DP], None),
+            "oq_gamma5vector": ([P, DP, I], None),
+            "oq_vecdot": ([P, DP, DP, DP], None),
+            "oq_defl_create": ([P, I, I], P),
+            "oq_defl_destroy": ([P], None),
+            "oq_defl_get": ([P, I, DP, DP], None),
+            "oq_gmresdr": ([P, DP, DP, IP, D, I, DP, DP, P, P], I),
+            "oq_gmresproject": ([P, DP, DP, IP, D, I, DP, DP, I, P, P], I),
+            "oq_psc": ([P, DP, DP, IP, D, I, DP, DP, I, P, P], I),
+            "oq_bicgstab": ([P, DP, DP, D, I, DP, DP, P, I], I),
+            "oq_fermprop": ([P, DP, DP, DP, I, D, I, IP, DP, DP, DP, I, I, P, P], I),
+            "oq_linearsolver": ([I, I, DP, I, IP, DP, I], None),
+            "oq_hessenberg": ([DP, I, I, I, I, DP], None),
+            "oq_qgenerator": ([I, I, I, DP, I, DP], None),
+            "oq_evalues": ([I, I, I, I, DP, I, DP, DP, I], None),
+            "oq_orgschur": ([IP, I, DP, I, DP, I, DP, IP], None),
+            "oq_twaverage_level0": ([P, DP, DP, DP, DP, DP, D, DP], None),
+            "oq_coldstart": ([P, DP], None),
+            "oq_aveplaq": ([P, DP], D),
+        }
+        for name, (args, res) in sig.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = res
+        _lib = L
+    return _lib
+
+
+def _dp(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _ip(a):
+    a = np.ascontiguousarray(a, dtype=np.int32)
+    return a, a.ctypes.data_as(C.POINTER(C.c_int))
+
+
+class SolveLog(C.Structure):
+    _fields_ = [("itercount", C.c_int), ("mvp", C.c_int), ("ncycles", C.c_int), ("nhist", C.c_int),
+                ("hist", C.c_double * 4096), ("hist_mvp", C.c_int * 4096), ("nritz", C.c_int),
+                ("ritz", C.c_double * 1024), ("final_rel", C.c_double)]
+
+    def history(self):
+        n = self.nhist
+        return np.array(self.hist[:n]), np.array(self.hist_mvp[:n])
+
+    def ritz_values(self):
+        r = np.array(self.ritz[: 2 * self.nritz]).reshape(-1, 2)
+        return r[:, 0] + 1j * r[:, 1]
+
+
+class OracleLattice:
+    """The reference's single-process lattice (nps = 1) with index tables and gauge field."""
+
+    def __init__(self, nx, ny, nz, nt, bc=(1, 1, 1, -1), c1=(1.0,) * 4, c2=(1.0,) * 4):
+        L = lib()
+        self._bc = np.array(bc, np.int32)
+        self._c1 = np.array(c1, np.float64)
+        self._c2 = np.array(c2, np.float64)
+        self._g = L.oq_geom_create(nx, ny, nz, nt, self._bc.ctypes.data_as(C.POINTER(C.c_int)),
+                                   _dp(self._c1), _dp(self._c2))
+        if not self._g:
+            raise ValueError("lattice extents must be multiples of 4")
+        self.dims = (nx, ny, nz, nt)
+        self.nvhalf = L.oq_nvhalf(self._g)
+        self.ntotal = L.oq_ntotal(self._g)
+        self.u = None
+
+    def __del__(self):
+        try:
+            if self._g:
+                lib().oq_geom_destroy(self._g)
+        except Exception:
+            pass
+
+    @property
+    def half_shape(self):
+        return (8, 2, 4, self.ntotal, 6)
+
+    @property
+    def gauge_shape(self):
+        return (16, 2, 4, self.ntotal, 18)
+
+    def new_half(self):
+        return np.zeros(self.half_shape)
+
+    def set_gauge(self, u: np.ndarray):
+        assert u.shape == self.gauge_shape
+        self.u = np.ascontiguousarray(u, dtype=np.float64)
+
+    def set_coact(self, c1, c2):
+        self._c1 = np.array(c1, np.float64)
+        self._c2 = np.array(c2, np.float64)
+        lib().oq_set_coact(self._g, _dp(self._c1), _dp(self._c2))
+
+    def site_of_coords(self, x):
+        x, xp = _ip(x)
+        out = [C.c_int() for _ in range(5)]
+        lib().oq_site_of_coords(self._g, xp, *[C.byref(o) for o in out])
+        return tuple(o.value for o in out)  # isite, ieo, ibl, gblclr, ibleo
+
+    # ---- Dirac operator ----
+    def hsingle(self, gin, idag, gblclr):
+        out = self.new_half()
+        gi = np.array(gin, dtype=np.float64, copy=True)
+        lib().oq_hsingle(self._g, _dp(out), _dp(self.u), _dp(gi), idag, gblclr)
+        return out
+
+    def hdouble(self, ge, idag, kappa):
+        out = self.new_half()
+        gi = np.array(ge, dtype=np.float64, copy=True)
+        lib().oq_hdouble(self._g, _dp(out), _dp(self.u), _dp(gi), idag, float(kappa))
+        return out
+
+    def hdbletm(self, ge, idag, kappa):
+        out = self.new_half()
+        gi = np.array(ge, dtype=np.float64, copy=True)
+        k = np.array(kappa, np.float64)
+        lib().oq_hdbletm(self._g, _dp(out), _dp(self.u), _dp(gi), idag, _dp(k))
+        return out
+
+    def twmshift(self, gwhole, idag, kappa):
+        out = np.zeros((2,) + self.half_shape)
+        gi = np.array(gwhole, dtype=np.float64, copy=True)
+        k = np.array(kappa, np.float64)
+        lib().oq_twmshift(self._g, _dp(out), _dp(self.u), _dp(gi), idag, _dp(k))
+        return out
+
+    def vecdot(self, a, b):
+        r = np.zeros(2)
+        lib().oq_vecdot(self._g, _dp(np.ascontiguousarray(a)), _dp(np.ascontiguousarray(b)), _dp(r))
+        return complex(r[0], r[1])
+
+    def gam5x(self, a):
+        a = np.array(a, dtype=np.float64, copy=True)
+        lib().oq_gam5x(self._g, _dp(a))
+        return a
+
+    # ---- inverters ----
+    def deflation(self, nmax, kmax):
+        return lib().oq_defl_create(self._g, nmax, kmax)
+
+    def defl_get(self, d, k, nmax):
+        vt = np.zeros((k + 1,) + self.half_shape)
+        hc = np.zeros((k, k + 1, 2))
+        lib().oq_defl_get(d, k, _dp(vt), _dp(hc))
+        return vt, hc[..., 0] .T + 1j * hc[..., 1].T
+
+    def gmresdr(self, phi, x, GMRES, resmax, itermin=0, kappa=(0.15, 0.0), defl=None):
+        x = np.array(x, dtype=np.float64, copy=True)
+        log = SolveLog()
+        G, Gp = _ip(GMRES)
+        k = np.array(kappa, np.float64)
+        st = lib().oq_gmresdr(self._g, _dp(np.ascontiguousarray(phi)), _dp(x), Gp, float(resmax), itermin,
+                              _dp(self.u), _dp(k), defl, C.byref(log))
+        return x, st, log
+
+    def gmresproject(self, b, GMRES, resmax, itermin=0, kappa=(0.15, 0.0), isignal=2, defl=None):
+        x = self.new_half()
+        log = SolveLog()
+        G, Gp = _ip(GMRES)
+        k = np.array(kappa, np.float64)
+        st = lib().oq_gmresproject(self._g, _dp(np.ascontiguousarray(b)), _dp(x), Gp, float(resmax), itermin,
+                                   _dp(self.u), _dp(k), isignal, defl, C.byref(log))
+        return x, st, log
+
+    def psc(self, b, x, GMRES, resmax, itermin=0, kappa=(0.15, 0.0), isignal=1, defl=None):
+        x = np.array(x, dtype=np.float64, copy=True)
+        log = SolveLog()
+        G, Gp = _ip(GMRES)
+        k = np.array(kappa, np.float64)
+        st = lib().oq_psc(self._g, _dp(np.ascontiguousarray(b)), _dp(x), Gp, float(resmax), itermin,
+                          _dp(self.u), _dp(k), isignal, defl, C.byref(log))
+        return x, st, log
+
+    def bicgstab(self, phi, x, resmax, itermin=0, kappa=(0.15, 0.0), maxiter=0):
+        x = np.array(x, dtype=np.float64, copy=True)
+        log = SolveLog()
+        k = np.array(kappa, np.float64)
+        st = lib().oq_bicgstab(self._g, _dp(np.ascontiguousarray(phi)), _dp(x), float(resmax), itermin,
+                               _dp(self.u), _dp(k), C.byref(log), maxiter)
+        return x, st, log
+
+    def fermprop(self, be, bo, kappa, inverter=5, resmax=1e-10, itermin=0, nGMRES=(30, 10), ntmqcd=0,
+                 isignal=1, defl=None, xe=None):
+        xe = self.new_half() if xe is None else np.array(xe, dtype=np.float64, copy=True)
+        xo = self.new_half()
+        bo = np.array(bo, dtype=np.float64, copy=True)
+        log = SolveLog()
+        G, Gp = _ip(nGMRES)
+        k = np.array(kappa, np.float64)
+        st = lib().oq_fermprop(self._g, _dp(np.ascontiguousarray(be)), _dp(bo), _dp(k), inverter, float(resmax),
+                               itermin, Gp, _dp(self.u), _dp(xe), _dp(xo), ntmqcd, isignal, defl,
+                               C.byref(log))
+        return xe, xo, st, log
+
+    # ---- sources ----
+    def pointsource(self, src, icsrc, idsrc):
+        be, bo = self.new_half(), self.new_half()
+        s, sp = _ip(src)
+        lib().oq_pointsource(self._g, _dp(be), _dp(bo), sp, icsrc, idsrc)
+        return be, bo
+
+    def z2source(self):
+        be, bo = self.new_half(), self.new_half()
+        lib().oq_z2source(self._g, _dp(be), _dp(bo))
+        return be, bo
+
+    def z4source(self):
+        be, bo = self.new_half(), self.new_half()
+        lib().oq_z4source(self._g, _dp(be), _dp(bo))
+        return be, bo
+
+    def twaverage_level0(self, be, bo, xe, xo, kappa):
+        J = np.zeros((6, self.dims[3], 2))
+        lib().oq_twaverage_level0(self._g, _dp(np.ascontiguousarray(be)), _dp(np.ascontiguousarray(bo)),
+                                  _dp(np.ascontiguousarray(xe)), _dp(np.ascontiguousarray(xo)),
+                                  _dp(self.u), float(kappa), _dp(J))
+        return J
+
+    # ---- gauge helpers ----
+    def coldstart(self):
+        u = np.zeros(self.gauge_shape)
+        lib().oq_coldstart(self._g, _dp(u))
+        return u
+
+    def aveplaq(self, u=None):
+        u = self.u if u is None else u
+        return lib().oq_aveplaq(self._g, _dp(np.ascontiguousarray(u)))
+
+
+def initlagfib(myid: int, iseed: int):
+    lib().oq_initlagfib(myid, iseed)
+
+
+def rnds(m: int) -> np.ndarray:
+    out = np.zeros(m)
+    lib().oq_rnds(m, _dp(out))
+    return out
+
+
+# ---- restated pseudolapack, on complex numpy matrices ----
+def _to_f(a: np.ndarray, ld: int | None = None) -> np.ndarray:
+    m, n = a.shape
+    ld = ld or m
+    buf = np.zeros((n, ld, 2))
+    buf[:, :m, 0] = a.real.T
+    buf[:, :m, 1] = a.imag.T
+    return buf
+
+
+def _from_f(buf: np.ndarray, m: int) -> np.ndarray:
+    return (buf[:, :m, 0] + 1j * buf[:, :m, 1]).T
+
+
+def linearsolver(a: np.ndarray, b: np.ndarray) -> np.ndarray:
+    n = a.shape[0]
+    A = _to_f(a)
+    B = _to_f(b.reshape(n, -1))
+    piv = np.zeros(n, np.int32)
+    lib().oq_linearsolver(n, B.shape[0], _dp(A), n, piv.ctypes.data_as(C.POINTER(C.c_int)), _dp(B), n)
+    return _from_f(B, n)
+
+
+def schur_selected(h: np.ndarray, k: int):
+    """gmresdr's harmonic-Ritz Schur step: hessenberg -> qgenerator -> evalues ->
+    select the k smallest |theta| -> orgschur.  Returns (T, Z, w)."""
+    n = h.shape[0]
+    A = _to_f(h)
+    tau = np.zeros((n, 2))
+    lib().oq_hessenberg(_dp(A), n, n, 1, n, _dp(tau))
+    Z = np.zeros_like(A)
+    for j in range(n):
+        Z[j, j:n] = A[j, j:n]
+    lib().oq_qgenerator(n, 1, n, _dp(Z), n, _dp(tau))
+    w = np.zeros((n, 2))
+    lib().oq_evalues(1, n, 1, n, _dp(A), n, _dp(w), _dp(Z), n)
+    wc = w[:, 0] + 1j * w[:, 1]
+    mag = np.sort(np.abs(wc))
+    sel = (np.abs(wc) <= mag[k - 1]).astype(np.int32)
+    m = C.c_int()
+    lib().oq_orgschur(sel.ctypes.data_as(C.POINTER(C.c_int)), n, _dp(A), n, _dp(Z), n, _dp(w), C.byref(m))
+    return _from_f(A, n), _from_f(Z, n), w[:, 0] + 1j * w[:, 1], wc

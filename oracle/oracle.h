@@ -1,0 +1,139 @@
+// CPU oracle for the qqcd solver hot path -- TEST INFRASTRUCTURE ONLY.
+//
+// This is a line-by-line C++ restatement of the BaylorLQCD `qqcd` Fortran-90 routines
+// on the solver hot path (Wilson / twisted-mass Dirac operator, GMRES-DR, GMRES-Proj,
+// BiCGStab, propagator source preparation / reconstruction, noise sources, lagged
+// Fibonacci RNG, loop traces).  Each function cites the reference file:line it follows.
+//
+// Parity status: UNPINNED against the Fortran itself.  No Fortran compiler exists in
+// this environment and the reference ships no golden vectors, known-answer files or
+// tests, so the restatement cannot be checked against reference outputs.  It is
+// pinned instead against analytic known answers (free-field plane waves, gamma5
+// hermiticity, gauge covariance, dense-matrix solves) and against scipy's LAPACK for
+// the restated pseudolapack steps.
+//
+// Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may use this
+// library, and only as the checker / timed CPU reference -- never as a product path.
+//
+// Array layouts are the reference's Fortran column-major layouts, 1-based in the
+// comments:
+//   Dirac half-vector  g(6, ntotal, 4, 2, 8)   (re/im x colour, site, spin, ieo, ibleo)
+//   Gauge field        u(18, ntotal, 4, 2, 16) (3x3 row-major re/im, site, mu, ieo, ibl)
+// with nvhalf = V/32 and ntotal = nvhalf + nbmax (one process: nps = 1).
+#pragma once
+#include <cstdint>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct oq_geom oq_geom;
+
+// Build the geometry / index tables of lattice.f90:initlat for one process.
+// bc[mu] in {1,-1,0}; c1[mu] = coact(3,1,mu); c2[mu] = coact(3,2,mu).
+oq_geom* oq_geom_create(int nx, int ny, int nz, int nt, const int bc[4],
+                        const double c1[4], const double c2[4]);
+void oq_geom_destroy(oq_geom* g);
+int oq_nvhalf(const oq_geom* g);
+int oq_ntotal(const oq_geom* g);
+int oq_nbmax(const oq_geom* g);
+// Copies of the index tables (1-based values, Fortran order):
+// lv/lvbc(nvhalf,4,2), ib(nbmax,4,2,2), nms(4), lbd(16,4) as int, iblv(16,4),
+// vecbl(2,8), vecblinv(2,16).
+void oq_tables(const oq_geom* g, int* lv, int* lvbc, int* ib, int* nms, int* lbd,
+               int* iblv, int* vecbl, int* vecblinv);
+void oq_set_coact(oq_geom* g, const double c1[4], const double c2[4]);
+
+// ---- map between global 0-based coordinates and the blocked layout ----
+// (G/lattice.f90 siteindex/setblk/gblchker; Q/quark.f90:70-105 pointsource)
+void oq_site_of_coords(const oq_geom* g, const int x[4], int* isite, int* ieo,
+                       int* ibl, int* gblclr, int* ibleo);
+
+// ---- lagged Fibonacci RNG (G/lagfib.f90) ----
+void oq_initlagfib(int myid, int iseed);
+void oq_rnds(int m, double* rn);
+void oq_lagfib_state(int* iw /*521*/, int* jr, int* kr);
+void oq_lagfib_set_state(const int* iw, int jr, int kr);
+
+// ---- sources ----
+void oq_pointsource(const oq_geom* g, double* be, double* bo, const int src[4],
+                    int icsrc, int idsrc);
+void oq_z2source(const oq_geom* g, double* be, double* bo);
+void oq_z4source(const oq_geom* g, double* be, double* bo);
+
+// ---- Dirac operator (Q/diracops.f90) ----
+void oq_hsingle(const oq_geom* g, double* gout, const double* u, double* gin,
+                int idag, int gblclr);
+void oq_hdouble(const oq_geom* g, double* he, const double* u, double* ge, int idag,
+                double kappa);
+void oq_hdbletm(const oq_geom* g, double* he, const double* u, double* ge, int idag,
+                const double kappa[2]);
+void oq_twmshift(const oq_geom* g, double* hwhole, const double* u, double* gwhole,
+                 int idag, const double kappa[2]);
+void oq_gam5x(const oq_geom* g, double* a);
+void oq_gamma5vector(const oq_geom* g, double* a, int ntmqcd);
+void oq_vecdot(const oq_geom* g, const double* a, const double* b, double* adb);
+
+// ---- inverters (Q/inverters.f90) ----
+typedef struct oq_defl oq_defl;  // replaces module `shift` (vtemp, hcnew, beg)
+oq_defl* oq_defl_create(const oq_geom* g, int nmax, int kmax);
+void oq_defl_destroy(oq_defl* d);
+// k+1 deflation vectors (reference layout) and hcnew((k+1) x k, complex, col-major).
+void oq_defl_get(const oq_defl* d, int k, double* vtemp, double* hcnew);
+
+typedef struct oq_solve_log {
+  int itercount;
+  int mvp;
+  int ncycles;
+  int nhist;          // entries written into hist (true residual per cycle)
+  double hist[4096];
+  int hist_mvp[4096];
+  int nritz;          // harmonic Ritz values of the last restart (re,im)
+  double ritz[2 * 512];
+  double final_rel;   // ||phi - A x|| / ||phi|| at exit (even system)
+} oq_solve_log;
+
+int oq_gmresdr(const oq_geom* g, const double* phi, double* x, const int GMRES[2],
+               double resmax, int itermin, const double* u, const double kappa[2],
+               oq_defl* defl, oq_solve_log* log);
+int oq_gmresproject(const oq_geom* g, const double* b, double* x, const int GMRES[2],
+                    double resmax, int itermin, const double* u, const double kappa[2],
+                    int isignal, oq_defl* defl, oq_solve_log* log);
+int oq_psc(const oq_geom* g, const double* b, double* x, const int GMRES[2],
+           double resmax, int itermin, const double* u, const double kappa[2],
+           int isignal, oq_defl* defl, oq_solve_log* log);
+int oq_bicgstab(const oq_geom* g, const double* phi, double* x, double resmax,
+                int itermin, const double* u, const double kappa[2], oq_solve_log* log,
+                int maxiter);
+
+// ---- propagator driver (Q/quark.f90 fermprop, nkappa = -1 Wilson/twisted mass) ----
+int oq_fermprop(const oq_geom* g, const double* be, double* bo, const double kappa[2],
+                int inverter, double resmax, int itermin, const int nGMRES[2],
+                const double* u, double* xe, double* xo, int ntmqcd, int isignal,
+                oq_defl* defl, oq_solve_log* log);
+
+// ---- restated small dense algebra (Q/pseudolapack.f90), exposed for checks ----
+// Complex matrices are (2, ld, ncol) Fortran order: re/im interleaved, column-major.
+void oq_linearsolver(int n, int nrhs, double* a, int lda, int* ipiv, double* b, int ldb);
+void oq_hessenberg(double* a, int lda, int n, int ilo, int ihi, double* tau);
+void oq_qgenerator(int n, int ilo, int ihi, double* a, int lda, const double* tau);
+void oq_evalues(int ischur, int n, int ilo, int ihi, double* h, int ldh, double* w,
+                double* z, int ldz);
+void oq_orgschur(const int* select, int n, double* t, int ldt, double* q, int ldq,
+                 double* w, int* m);
+
+// ---- loop traces (Q/disconloops.f90 loopops/vv/spacesum; Q/vevbleft.f90 twAverage) ----
+// Per-time-slice local bilinears of one noise solution (unsubtracted level).
+// J is (2, nt, 6) : op 1 = J4 point-split time current, 2 = psibar psi,
+// 3..5 = J1..J3 point-split spatial currents, 6 = psibar gamma5 psi.
+void oq_twaverage_level0(const oq_geom* g, const double* be, const double* bo,
+                         const double* xe, const double* xo, const double* u,
+                         double kappa, double* J);
+
+// ---- gauge field helpers ----
+void oq_coldstart(const oq_geom* g, double* u);
+double oq_aveplaq(const oq_geom* g, const double* u);
+
+#ifdef __cplusplus
+}
+#endif

@@ -1,0 +1,95 @@
+// Internal helpers of the CPU oracle (test infrastructure only; see oracle.h).
+#pragma once
+#include <cstddef>
+#include <vector>
+
+#include "oracle.h"
+
+struct oq_geom {
+  int n[4];
+  int bc[4];
+  double c1[4], c2[4];  // coact(3,1,mu), coact(3,2,mu)
+  int nvhalf, nbmax, ntotal;
+  int nms[4];
+  std::vector<int> lv, lvbc;  // (nvhalf, 4, 2), 1-based values
+  std::vector<int> ib;        // (nbmax, 4, 2, 2)
+  bool lbd[16][4];
+  int iblv[16][4];
+  int vecbl[2][8];
+  int vecblinv[2][16];
+
+  // Index of g(a, site, id, ieo, ibleo) (all 1-based) in a (6,ntotal,4,2,8) array.
+  size_t gi(int a, int site, int id, int ieo, int ibleo) const {
+    return (size_t)(a - 1) +
+           6 * ((size_t)(site - 1) +
+                (size_t)ntotal * ((size_t)(id - 1) + 4 * ((size_t)(ieo - 1) + 2 * (size_t)(ibleo - 1))));
+  }
+  // Index of u(a, site, mu, ieo, ibl) in a (18,ntotal,4,2,16) array.
+  size_t ui(int a, int site, int mu, int ieo, int ibl) const {
+    return (size_t)(a - 1) +
+           18 * ((size_t)(site - 1) +
+                 (size_t)ntotal * ((size_t)(mu - 1) + 4 * ((size_t)(ieo - 1) + 2 * (size_t)(ibl - 1))));
+  }
+  size_t vsize() const { return (size_t)6 * ntotal * 4 * 2 * 8; }
+  size_t usize() const { return (size_t)18 * ntotal * 4 * 2 * 16; }
+  int& LV(int i, int mu, int ieo) { return lv[(size_t)(i - 1) + (size_t)nvhalf * ((mu - 1) + 4 * (ieo - 1))]; }
+  int& LVBC(int i, int mu, int ieo) { return lvbc[(size_t)(i - 1) + (size_t)nvhalf * ((mu - 1) + 4 * (ieo - 1))]; }
+  const int& LVBC(int i, int mu, int ieo) const {
+    return lvbc[(size_t)(i - 1) + (size_t)nvhalf * ((mu - 1) + 4 * (ieo - 1))];
+  }
+  int& IB(int i, int mu, int side, int ieo) {
+    return ib[(size_t)(i - 1) + (size_t)nbmax * ((mu - 1) + 4 * ((side - 1) + 2 * (ieo - 1)))];
+  }
+  int IB(int i, int mu, int side, int ieo) const {
+    return ib[(size_t)(i - 1) + (size_t)nbmax * ((mu - 1) + 4 * ((side - 1) + 2 * (ieo - 1)))];
+  }
+
+  // f(k) for every real entry with isite <= nvhalf.
+  template <class F>
+  void for_interior(F f) const {
+    for (int ibleo = 1; ibleo <= 8; ++ibleo)
+      for (int ieo = 1; ieo <= 2; ++ieo)
+        for (int id = 1; id <= 4; ++id)
+          for (int s = 1; s <= nvhalf; ++s)
+            for (int a = 1; a <= 6; ++a) f(gi(a, s, id, ieo, ibleo));
+  }
+  // f(s1,s2,s3,s4): offsets of the same (a, site, ieo, ibleo) entry for spins 1..4.
+  // complex_stride: visit a = 1,3,5 only (f handles re and im).
+  template <class F>
+  void for_spin_range(F f, int smax, bool complex_stride) const {
+    for (int ibleo = 1; ibleo <= 8; ++ibleo)
+      for (int ieo = 1; ieo <= 2; ++ieo)
+        for (int s = 1; s <= smax; ++s)
+          for (int a = 1; a <= 6; a += complex_stride ? 2 : 1)
+            f(gi(a, s, 1, ieo, ibleo), gi(a, s, 2, ieo, ibleo), gi(a, s, 3, ieo, ibleo),
+              gi(a, s, 4, ieo, ibleo));
+  }
+  template <class F>
+  void for_spin_interior(F f, bool complex_stride = false) const {
+    for_spin_range(f, nvhalf, complex_stride);
+  }
+  template <class F>
+  void for_spin_all(F f) const {
+    for_spin_range(f, ntotal, false);
+  }
+};
+
+struct oq_defl {
+  int nmax, kmax;
+  int k;                       // deflation vectors held: k+1 in vtemp
+  std::vector<double> vtemp;   // (kmax+1) vectors of g->vsize()
+  std::vector<double> hcnew;   // (2, nmax+1, nmax) Fortran order
+  std::vector<double> beg;     // one vector
+  size_t vsize;
+};
+
+namespace oq {
+void hsingle(const oq_geom* g, double* gout, const double* u, double* gin, int idag,
+             int gblclr);
+void hdouble(const oq_geom* g, double* he, const double* u, double* ge, int idag,
+             double kappa);
+void hdbletm(const oq_geom* g, double* he, const double* u, double* ge, int idag,
+             const double kappa[2]);
+double vecdot_re(const oq_geom* g, const double* a, const double* b, double* im);
+double twonorm_c(const double* x, int n);
+}  // namespace oq

@@ -33,6 +33,7 @@ EXPORTED = [
     "qq_defl_create", "qq_defl_destroy", "qq_defl_size", "qq_gmresdr", "qq_gmresproj", "qq_psc",
     "qq_bicgstab", "qq_fermprop", "qq_pointsource", "qq_fermprop_batch", "qq_initlagfib",
     "qq_rnds", "qq_z2source", "qq_z4source", "qq_twaverage_level0", "qq_bench_hsingle",
+    "qq_heatbath", "qq_ctx_stream", "qq_launch_count", "qq_profile_hop", "qq_profile_hop_read",
 ]
 
 
@@ -56,7 +57,8 @@ class qq_solve_info(C.Structure):
 
 class qq_method(C.Structure):
     _fields_ = [("m", C.c_int), ("k", C.c_int), ("precision", C.c_int), ("rhs_block", C.c_int),
-                ("tol", C.c_double), ("max_outer", C.c_int)]
+                ("tol", C.c_double), ("max_outer", C.c_int), ("solver", C.c_int), ("deflate", C.c_int),
+                ("defl_tol", C.c_double)]
 
 
 @dataclass
@@ -124,7 +126,12 @@ def load_library() -> C.CDLL:
         "qq_z2source": ([P, P, P], I),
         "qq_z4source": ([P, P, P], I),
         "qq_twaverage_level0": ([P, P, P, P, P, D, P], I),
-        "qq_bench_hsingle": ([P, I, I, I, I, DP, DP], I),
+        "qq_bench_hsingle": ([P, I, I, I, I, I, DP, DP], I),
+        "qq_heatbath": ([P, D, I, C.c_ulonglong, P, DP], I),
+        "qq_ctx_stream": ([P, C.POINTER(P)], I),
+        "qq_launch_count": ([], C.c_longlong),
+        "qq_profile_hop": ([P, I], I),
+        "qq_profile_hop_read": ([P, C.POINTER(C.c_longlong), DP, DP], I),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -232,6 +239,29 @@ class Lattice:
     def gauge_upload(self, u, recon: int = 0):
         _check(self.lib.qq_gauge_upload(self._ctx, _ptr(u), recon))
 
+    def heatbath(self, beta=6.0, nsweeps=200, seed=13, u_out=None):
+        """Generate (cold start + nsweeps heatbath sweeps) and upload a quenched SU(3)
+        configuration; returns (u in reference layout or u_out, plaquette)."""
+        u = np.zeros(self.gauge_shape) if u_out is None else u_out
+        pl = C.c_double()
+        _check(self.lib.qq_heatbath(self._ctx, float(beta), int(nsweeps), int(seed), _ptr(u), C.byref(pl)))
+        return u, pl.value
+
+    def stream_handle(self) -> int:
+        """The cudaStream_t (as an int) all calls of this lattice run on."""
+        h = C.c_void_p()
+        _check(self.lib.qq_ctx_stream(self._ctx, C.byref(h)))
+        return h.value or 0
+
+    def profile_hop(self, enable: bool):
+        _check(self.lib.qq_profile_hop(self._ctx, int(enable)))
+
+    def profile_hop_read(self):
+        """(launches, total ms, total algorithmic bytes) of hopping kernels since enable."""
+        n, ms, by = C.c_longlong(), C.c_double(), C.c_double()
+        _check(self.lib.qq_profile_hop_read(self._ctx, C.byref(n), C.byref(ms), C.byref(by)))
+        return n.value, ms.value, by.value
+
     def set_coact(self, c1, c2):
         _check(self.lib.qq_set_coact(self._ctx, (C.c_double * 4)(*c1), (C.c_double * 4)(*c2)))
 
@@ -310,14 +340,18 @@ class Lattice:
         _check(self.lib.qq_pointsource(self._ctx, _ptr(be), _ptr(bo), (C.c_int * 4)(*src), icsrc, idsrc))
         return be, bo
 
-    def fermprop_batch(self, be, bo, kappa, m=60, k=20, precision=32, rhs_block=4, tol=1e-10,
-                       max_outer=50, xe=None, xo=None):
-        """Batched accelerated solve: be, bo of shape (nrhs,) + half_shape."""
+    def fermprop_batch(self, be, bo, kappa, m=60, k=20, precision=32, rhs_block=12, tol=1e-10,
+                       max_outer=0, solver=1, deflate=1, defl_tol=1e-5, xe=None, xo=None):
+        """Batched propagators (qq_fermprop_batch): be, bo of shape (nrhs,) + half_shape,
+        numpy (host) or torch CUDA tensors.  solver=0 is the reference's plain FP64
+        GMRES-DR(m,k) per right-hand side; solver=1 the deflated batched BiCGStab."""
         nrhs = be.shape[0]
-        xe = np.zeros_like(be) if xe is None else xe
-        xo = np.zeros_like(bo) if xo is None else xo
+        if xe is None:
+            xe = np.zeros(be.shape) if isinstance(be, np.ndarray) else be.new_zeros(be.shape)
+        if xo is None:
+            xo = np.zeros(bo.shape) if isinstance(bo, np.ndarray) else bo.new_zeros(bo.shape)
         infos = (qq_solve_info * nrhs)()
-        meth = qq_method(m, k, precision, rhs_block, tol, max_outer)
+        meth = qq_method(m, k, precision, rhs_block, tol, max_outer, solver, deflate, defl_tol)
         st = self.lib.qq_fermprop_batch(self._ctx, nrhs, _ptr(be), _ptr(bo), _d2(kappa), C.byref(meth),
                                         _ptr(xe), _ptr(xo), infos)
         _check(st, allow_not_converged=True)
@@ -341,12 +375,17 @@ class Lattice:
         return J
 
 
-    def bench_hsingle(self, precision=64, nrhs=1, niter=20, flush_l2=True):
+    def bench_hsingle(self, precision=64, nrhs=1, niter=20, flush_l2=True, tps=0):
         """Mean kernel time (ms) and algorithmic bytes of one hopping-term launch."""
         ms, by = C.c_double(), C.c_double()
-        _check(self.lib.qq_bench_hsingle(self._ctx, precision, nrhs, niter, int(flush_l2),
+        _check(self.lib.qq_bench_hsingle(self._ctx, precision, nrhs, tps, niter, int(flush_l2),
                                          C.byref(ms), C.byref(by)))
         return ms.value, by.value
+
+
+def launch_count() -> int:
+    """Kernels launched by the library in this process so far."""
+    return int(load_library().qq_launch_count())
 
 
 def initlagfib(myid: int, iseed: int):

@@ -1,6 +1,7 @@
 // extern "C" entry points of libqqcd_gpu.so (declared in include/qqcd_gpu.h).
 #include <chrono>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 
 #include "qq_ctx.h"
@@ -86,6 +87,8 @@ int qq_ctx_create(const qq_geom* geom, int device, qq_ctx** out) {
   if (device < 0 || device >= ndev) return set_error(QQ_BAD_ARG, "bad device index");
   auto* c = new qq_ctx();
   c->device = device;
+  if (const char* f = std::getenv("QQ_FORCE_TPS")) c->forced_tps = std::atoi(f);  // testing
+  if (c->forced_tps < 0 || c->forced_tps > 128) c->forced_tps = 0;
   for (int mu = 0; mu < 4; ++mu) {
     c->g.n[mu] = n[mu];
     c->g.bc[mu] = geom->bc[mu];
@@ -104,6 +107,8 @@ int qq_ctx_create(const qq_geom* geom, int device, qq_ctx** out) {
   if (st == QQ_OK && cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess) st = QQ_CUDA_ERR;
   if (st == QQ_OK && cudaEventCreate(&c->ev0) != cudaSuccess) st = QQ_CUDA_ERR;
   if (st == QQ_OK && cudaEventCreate(&c->ev1) != cudaSuccess) st = QQ_CUDA_ERR;
+  if (st == QQ_OK && cudaEventCreate(&c->tev0) != cudaSuccess) st = QQ_CUDA_ERR;
+  if (st == QQ_OK && cudaEventCreate(&c->tev1) != cudaSuccess) st = QQ_CUDA_ERR;
   if (st == QQ_OK && c->partial.alloc(sizeof(double) * kRedBlocks * 16 * 16) != cudaSuccess) st = QQ_CUDA_ERR;
   if (st == QQ_OK && c->scal.alloc(sizeof(double) * 1024) != cudaSuccess) st = QQ_CUDA_ERR;
   if (st == QQ_OK && cudaMallocHost(&c->hpin, sizeof(double) * 1024) != cudaSuccess) st = QQ_CUDA_ERR;
@@ -123,6 +128,8 @@ int qq_ctx_destroy(qq_ctx* c) {
   if (c->hpin) cudaFreeHost(c->hpin);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
+  if (c->tev0) cudaEventDestroy(c->tev0);
+  if (c->tev1) cudaEventDestroy(c->tev1);
   if (c->st) cudaStreamDestroy(c->st);
   delete c;
   return QQ_OK;
@@ -438,13 +445,13 @@ __global__ void fill_kernel(double2* p, size_t n, unsigned seed) {
 }
 }  // namespace
 
-extern "C" int qq_bench_hsingle(qq_ctx* c, int precision, int nrhs, int niter, int flush_l2,
-                                double* ms_per_call, double* bytes_per_call) {
+extern "C" int qq_bench_hsingle(qq_ctx* c, int precision, int nrhs, int tps, int niter,
+                                int flush_l2, double* ms_per_call, double* bytes_per_call) {
   QQ_TRY(check_ctx(c));
   QQ_TRY(set_device(c));
   if (!c->have_gauge) return set_error(QQ_BAD_ARG, "no gauge field uploaded");
   const int prec = precision == 64 ? P64 : precision == 32 ? P32 : precision == 16 ? P16 : -1;
-  if (prec < 0 || nrhs < 1 || nrhs > 4 || (prec == P64 && nrhs != 1) || niter < 1)
+  if (prec < 0 || nrhs < 1 || nrhs > kMaxRhs || niter < 1 || tps < 0 || tps > 128)
     return set_error(QQ_BAD_ARG, "bad benchmark arguments");
   const int vh = c->g.vh;
   std::vector<std::unique_ptr<Field>> in(nrhs), out(nrhs);
@@ -481,12 +488,16 @@ extern "C" int qq_bench_hsingle(qq_ctx* c, int precision, int nrhs, int niter, i
     a.out_norm[r] = out[r]->norm.as<float>();
   }
   const int recon = prec == P64 ? c->recon64 : 12;
-  for (int w = 0; w < 3; ++w) QQ_CK(launch_hop(a, prec, recon, EPI_STORE, c->st));
+  if (tps == 0) {  // the autotuned choice the solvers use
+    QQ_TRY(launch_hop_tuned(c, a, prec, EPI_STORE));
+    tps = c->hop_tune[((prec * 64 + recon) * 16 + nrhs) * 4 + EPI_STORE];
+  }
+  for (int w = 0; w < 3; ++w) QQ_CK(launch_hop(a, prec, recon, EPI_STORE, tps, c->st));
   double total = 0.0;
   for (int it = 0; it < niter; ++it) {
     if (flush_l2) QQ_CK(cudaMemsetAsync(flush.p, it & 0xff, flush_bytes, c->st));
     QQ_CK(cudaEventRecord(c->ev0, c->st));
-    QQ_CK(launch_hop(a, prec, recon, EPI_STORE, c->st));
+    QQ_CK(launch_hop(a, prec, recon, EPI_STORE, tps, c->st));
     QQ_CK(cudaEventRecord(c->ev1, c->st));
     QQ_CK(cudaEventSynchronize(c->ev1));
     float ms = 0.f;
@@ -497,5 +508,60 @@ extern "C" int qq_bench_hsingle(qq_ctx* c, int precision, int nrhs, int niter, i
   const double spinor_bytes = prec == P64 ? 192.0 : prec == P32 ? 96.0 : 52.0;
   if (ms_per_call) *ms_per_call = total / niter;
   if (bytes_per_call) *bytes_per_call = (double)vh * (8.0 * link_bytes + nrhs * 2.0 * spinor_bytes);
+  return QQ_OK;
+}
+
+namespace qq {
+int heatbath_generate(qq_ctx* c, double beta, int nsweeps, unsigned long long seed, double* u_ref,
+                      double* plaq);
+}
+
+extern "C" int qq_heatbath(qq_ctx* c, double beta, int nsweeps, unsigned long long seed,
+                           double* u_ref, double* plaq) {
+  QQ_TRY(check_ctx(c));
+  QQ_TRY(set_device(c));
+  if (!(beta > 0.0) || nsweeps < 0) return set_error(QQ_BAD_ARG, "beta must be > 0, nsweeps >= 0");
+  const size_t nu = (size_t)18 * c->rd.ntotal * 4 * 2 * 16;
+  DevBuf own;
+  double* dst = u_ref;
+  if (!dst) {
+    QQ_CK(own.alloc(nu * sizeof(double)));
+    dst = own.as<double>();
+  }
+  QQ_TRY(heatbath_generate(c, beta, nsweeps, seed, dst, plaq));
+  return qq_gauge_upload(c, dst, 12);
+}
+
+extern "C" int qq_ctx_stream(const qq_ctx* c, void** stream) {
+  QQ_TRY(check_ctx(c));
+  if (!stream) return set_error(QQ_BAD_ARG, "null argument");
+  *stream = (void*)c->st;
+  return QQ_OK;
+}
+
+extern "C" long long qq_launch_count(void) { return qq::launch_count(); }
+
+extern "C" int qq_profile_hop(qq_ctx* c, int enable) {
+  QQ_TRY(check_ctx(c));
+  QQ_CK(cudaStreamSynchronize(c->st));
+  c->prof_hop = enable != 0;
+  if (c->prof_hop) c->prof_used = 0;
+  return QQ_OK;
+}
+
+extern "C" int qq_profile_hop_read(qq_ctx* c, long long* launches, double* ms_total,
+                                   double* bytes_total) {
+  QQ_TRY(check_ctx(c));
+  QQ_CK(cudaStreamSynchronize(c->st));
+  double ms = 0.0, by = 0.0;
+  for (size_t i = 0; i < c->prof_used; ++i) {
+    float t = 0.f;
+    QQ_CK(cudaEventElapsedTime(&t, c->prof_events[i].first, c->prof_events[i].second));
+    ms += t;
+    by += c->prof_bytes[i];
+  }
+  if (launches) *launches = (long long)c->prof_used;
+  if (ms_total) *ms_total = ms;
+  if (bytes_total) *bytes_total = by;
   return QQ_OK;
 }

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <complex>
+#include <map>
 #include <memory>
 #include <string>
 #include <vector>
@@ -97,6 +98,13 @@ struct qq_ctx {
   qq::DevBuf scal;          // device scalar slots
   double* hpin = nullptr;   // pinned host mirror of scalar results
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaEvent_t tev0 = nullptr, tev1 = nullptr;       // autotuner timing
+  std::map<int, int> hop_tune;                       // shape -> threads per site
+  int forced_tps = 0;                                // 0: autotune
+  bool prof_hop = false;                             // per-launch hop timing
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_events;
+  std::vector<double> prof_bytes;
+  size_t prof_used = 0;
   std::vector<std::unique_ptr<qq::Field>> pool[3];  // temporaries per precision
   std::vector<bool> pool_busy[3];
 
@@ -119,6 +127,7 @@ struct Tmp {
 };
 
 // ---- operator and level-1 helpers (qq_ops.cu) ----
+int launch_hop_tuned(qq_ctx* c, const HopArgs& a, int prec, int epi);
 int op_hsingle(qq_ctx* c, Spinor out, Spinor in, int idag, int pout);
 int op_hsingle_multi(qq_ctx* c, const Spinor* out, const Spinor* in, int n, int idag, int pout);
 // he = Hdbletm(ge), tmp is an odd-parity temporary of the same precision.
@@ -159,6 +168,11 @@ int gmresproj_fp64(qq_ctx* c, Spinor b, Spinor x, int m, int k, double resmax, i
                    const double kappa[2], const DeflSpace& defl, SolveStats* st);
 int bicgstab_fp64(qq_ctx* c, Spinor phi, Spinor x, double resmax, int itermin, int maxiter,
                   const double kappa[2], SolveStats* st);
+// Mixed precision (FP32 Arnoldi, FP64 residual/solution); returns an FP32 deflation space.
+int gmresdr_mixed(qq_ctx* c, Spinor b, Spinor x, int m, int k, double tol, int max_cycles,
+                  const double kappa[2], DeflSpace* defl, SolveStats* st);
+int defl_project(qq_ctx* c, const DeflSpace& d, Spinor b, Spinor x, Spinor r, const double kappa[2],
+                 double* rn);
 
 void fill_info(qq_solve_info* info, int status, const SolveStats& s, double seconds);
 

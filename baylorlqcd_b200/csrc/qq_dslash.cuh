@@ -1,14 +1,17 @@
 // Wilson hopping term H_eo / H_oe (the reference's Hsingle, Q/diracops.f90:554-599,
 // with mulbac :950-1159 and mulfor :1163-1391) for the B200.
 //
-// One thread per output site.  For every direction the thread gathers the two
-// neighbour spinors with the periodic / antiperiodic / fixed boundary factor folded
-// into the hop coefficient (the MPI halo exchange of setvector/slidevector becomes
-// in-kernel neighbour indexing), spin-projects them with (1 -/+ gamma_mu) in the
-// reference gamma basis (so only two colour vectors are multiplied by the link),
-// multiplies by U or U^dagger and accumulates in registers.  Links are read once per
-// site and applied to NRHS right-hand sides.  The epilogue fuses the twisted-mass /
-// Schur-complement axpys of Hdouble (:264-346) and Hdbletm (:435-550).
+// A thread owns one (output site, right-hand side, direction group).  For each of its
+// directions it gathers the two neighbour spinors with the periodic / antiperiodic /
+// fixed boundary factor folded into the hop coefficient (the MPI halo exchange of
+// setvector/slidevector becomes in-kernel neighbour indexing), spin-projects them
+// with (1 -/+ gamma_mu) in the reference gamma basis (so only two colour vectors are
+// multiplied by the link), multiplies by U or U^dagger and accumulates in registers.
+// The right-hand sides of a site occupy adjacent lanes, so each link load is one
+// broadcast transaction for the whole RHS block; splitting the 8 hops over 2 or 4
+// direction groups multiplies the resident warps on small lattices.  The epilogue
+// fuses the twisted-mass / Schur-complement axpys of Hdouble (:264-346) and Hdbletm
+// (:435-550).
 #pragma once
 #include "qq_fields.cuh"
 
@@ -20,7 +23,7 @@ enum Epilogue : int {
   EPI_DBLE = 2,   // out = f1*g + f2*J(g) - f3 * H in      (Hdbletm :496-514, Hdouble :340-343)
 };
 
-constexpr int kMaxRhs = 8;
+constexpr int kMaxRhs = 8;  // right-hand sides per launch
 
 struct HopArgs {
   Geom g;
@@ -121,8 +124,9 @@ __device__ inline void reconstruct_acc(cplx<R>* acc, const cplx<R>* w) {
   }
 }
 
-template <int SP, int LP, int RECON, int NRHS, int MU, bool FWD, class R>
-__device__ inline void hop(const HopArgs& a, int s, const int* x, cplx<R> (*acc)[12]) {
+// One hop (forward or backward in direction MU) of right-hand side r at output site s.
+template <int SP, int LP, int RECON, int MU, bool FWD, class R>
+__device__ inline void hop(const HopArgs& a, int s, int r, const int* x, cplx<R>* acc) {
   using SIO = SpinorIO<SP>;
   using LIO = LinkIO<LP, RECON>;
   int y[4] = {x[0], x[1], x[2], x[3]};
@@ -144,94 +148,381 @@ __device__ inline void hop(const HopArgs& a, int s, const int* x, cplx<R> (*acc)
   const int sy = site_index(a.g, y);
   const R cm = sgn * (R)(FWD ? a.c.fm[MU] : a.c.bm[MU]);
   const R cp = sgn * (R)(FWD ? a.c.fp[MU] : a.c.bp[MU]);
+  // All right-hand sides of a site sit in adjacent lanes: this load is one
+  // broadcast transaction for them, so the link crosses HBM once per RHS block.
   Su3<R> u;
   if (FWD)
     LIO::load(a.gauge, a.g.vh, a.pout, MU, s, u);
   else
     LIO::load(a.gauge, a.g.vh, 1 - a.pout, MU, sy, u);
-#pragma unroll
-  for (int r = 0; r < NRHS; ++r) {
-    cplx<R> psi[12];
-    SIO::load(a.in[r], a.in_norm[r], a.g.vh, sy, psi);
-    cplx<R> h[6], w[6];
-    if (cm != (R)0) {
-      project<MU, -1>(psi, cm, h);
-      if (FWD) {
-        matvec(u, h, w);
-        matvec(u, h + 3, w + 3);
-      } else {
-        matvec_dag(u, h, w);
-        matvec_dag(u, h + 3, w + 3);
-      }
-      reconstruct_acc<MU, -1>(acc[r], w);
+  cplx<R> psi[12];
+  SIO::load(a.in[r], a.in_norm[r], a.g.vh, sy, psi);
+  cplx<R> h[6], w[6];
+  if (cm != (R)0) {
+    project<MU, -1>(psi, cm, h);
+    if (FWD) {
+      matvec(u, h, w);
+      matvec(u, h + 3, w + 3);
+    } else {
+      matvec_dag(u, h, w);
+      matvec_dag(u, h + 3, w + 3);
     }
-    if (cp != (R)0) {
-      project<MU, +1>(psi, cp, h);
-      if (FWD) {
-        matvec(u, h, w);
-        matvec(u, h + 3, w + 3);
-      } else {
-        matvec_dag(u, h, w);
-        matvec_dag(u, h + 3, w + 3);
-      }
-      reconstruct_acc<MU, +1>(acc[r], w);
+    reconstruct_acc<MU, -1>(acc, w);
+  }
+  if (cp != (R)0) {
+    project<MU, +1>(psi, cp, h);
+    if (FWD) {
+      matvec(u, h, w);
+      matvec(u, h + 3, w + 3);
+    } else {
+      matvec_dag(u, h, w);
+      matvec_dag(u, h + 3, w + 3);
     }
+    reconstruct_acc<MU, +1>(acc, w);
   }
 }
 
-template <int SP, int LP, int RECON, int NRHS, int EPI>
+// Thread layout: threadIdx.x = (site-in-block) * nrhs + rhs, threadIdx.y = direction
+// group (TPS groups; group t applies the directions mu with mu % TPS == t).  With
+// TPS > 1 the partial sums meet in shared memory and group 0 runs the epilogue.
+template <int SP, int LP, int RECON, int TPS, int EPI>
 __global__ void __launch_bounds__(128) hop_kernel(HopArgs a) {
   using SIO = SpinorIO<SP>;
   using R = typename SIO::R;
   static_assert(sizeof(typename LinkIO<LP, RECON>::R) == sizeof(R), "link/spinor precision");
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= a.g.vh) return;
-  int x[4];
-  site_coords(a.g, a.pout, s, x);
-  cplx<R> acc[NRHS][12];
+  const int nrhs = a.nrhs;
+  const int per_block = blockDim.x / nrhs;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int r = tx % nrhs;
+  const int s = blockIdx.x * per_block + tx / nrhs;
+  const bool active = s < a.g.vh && tx < per_block * nrhs;
+  cplx<R> acc[12];
 #pragma unroll
-  for (int r = 0; r < NRHS; ++r)
+  for (int c = 0; c < 12; ++c) acc[c] = {(R)0, (R)0};
+  int x[4] = {0, 0, 0, 0};
+  if (active) {
+    site_coords(a.g, a.pout, s, x);
+    if (TPS == 1 || ty == 0) {
+      hop<SP, LP, RECON, 0, true>(a, s, r, x, acc);
+      hop<SP, LP, RECON, 0, false>(a, s, r, x, acc);
+    }
+    if (TPS == 1 || ty == (1 % TPS)) {
+      hop<SP, LP, RECON, 1, true>(a, s, r, x, acc);
+      hop<SP, LP, RECON, 1, false>(a, s, r, x, acc);
+    }
+    if (TPS == 1 || ty == (2 % TPS)) {
+      hop<SP, LP, RECON, 2, true>(a, s, r, x, acc);
+      hop<SP, LP, RECON, 2, false>(a, s, r, x, acc);
+    }
+    if (TPS == 1 || ty == (3 % TPS)) {
+      hop<SP, LP, RECON, 3, true>(a, s, r, x, acc);
+      hop<SP, LP, RECON, 3, false>(a, s, r, x, acc);
+    }
+  }
+  if (TPS > 1) {
+    __shared__ cplx<R> red[TPS > 1 ? 128 : 1][12];
+    const int slot = ty * blockDim.x + tx;
+    if (ty > 0) {
 #pragma unroll
-    for (int c = 0; c < 12; ++c) acc[r][c] = {(R)0, (R)0};
+      for (int c = 0; c < 12; ++c) red[slot][c] = acc[c];
+    }
+    __syncthreads();
+    if (ty > 0) return;
+#pragma unroll
+    for (int g = 1; g < TPS; ++g)
+#pragma unroll
+      for (int c = 0; c < 12; ++c) acc[c] = cadd(acc[c], red[g * blockDim.x + tx][c]);
+  }
+  if (!active) return;
+  cplx<R> o[12];
+  if (EPI == EPI_STORE) {
+#pragma unroll
+    for (int c = 0; c < 12; ++c) o[c] = acc[c];
+  } else if (EPI == EPI_TWIST) {
+    const R t = (R)a.a;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      o[0 + c] = csub(acc[0 + c], cscale(t, acc[6 + c]));
+      o[3 + c] = csub(acc[3 + c], cscale(t, acc[9 + c]));
+      o[6 + c] = cadd(acc[6 + c], cscale(t, acc[0 + c]));
+      o[9 + c] = cadd(acc[9 + c], cscale(t, acc[3 + c]));
+    }
+  } else {
+    cplx<R> gg[12];
+    SIO::load(a.aux[r], a.aux_norm[r], a.g.vh, s, gg);
+    const R f1 = (R)a.f1, f2 = (R)a.f2, f3 = (R)a.f3;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      o[0 + c] = csub(cadd(cscale(f1, gg[0 + c]), cscale(f2, gg[6 + c])), cscale(f3, acc[0 + c]));
+      o[3 + c] = csub(cadd(cscale(f1, gg[3 + c]), cscale(f2, gg[9 + c])), cscale(f3, acc[3 + c]));
+      o[6 + c] = csub(csub(cscale(f1, gg[6 + c]), cscale(f2, gg[0 + c])), cscale(f3, acc[6 + c]));
+      o[9 + c] = csub(csub(cscale(f1, gg[9 + c]), cscale(f2, gg[3 + c])), cscale(f3, acc[9 + c]));
+    }
+  }
+  SIO::store(a.out[r], a.out_norm[r], a.g.vh, s, o);
+}
 
-  hop<SP, LP, RECON, NRHS, 0, true>(a, s, x, acc);
-  hop<SP, LP, RECON, NRHS, 0, false>(a, s, x, acc);
-  hop<SP, LP, RECON, NRHS, 1, true>(a, s, x, acc);
-  hop<SP, LP, RECON, NRHS, 1, false>(a, s, x, acc);
-  hop<SP, LP, RECON, NRHS, 2, true>(a, s, x, acc);
-  hop<SP, LP, RECON, NRHS, 2, false>(a, s, x, acc);
-  hop<SP, LP, RECON, NRHS, 3, true>(a, s, x, acc);
-  hop<SP, LP, RECON, NRHS, 3, false>(a, s, x, acc);
+// ---------------------------------------------------------------------------
+// Staged variant.  A thread first issues asynchronous global->shared copies
+// (cp.async, 16 bytes each) of everything its 8 hops read -- the neighbour spinors
+// and the links -- into its own shared-memory slots, in two commit groups (hops 0-3
+// and 4-7).  It then waits for the first group (a hardware wait on its own copies,
+// no spin loop, no block barrier since no thread reads another's slots), computes
+// those hops from shared memory while the second group lands, and so on.  All the
+// loads of a site are in flight at once, independent of register pressure, which is
+// what keeps HBM busy when the lattice is too small for many resident warps.
+// Slot layout: [hop][16-byte element][thread], so every warp access is conflict free.
+// ---------------------------------------------------------------------------
+__device__ inline void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
+}
+__device__ inline void cp_async4(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem));
+}
+__device__ inline void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ inline void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
 
+template <int SP>
+struct SlotSpinor;
+template <>
+struct SlotSpinor<P64> {
+  __device__ static inline void load(const uint4* slot, int T, cplx<double>* v) {
 #pragma unroll
-  for (int r = 0; r < NRHS; ++r) {
-    cplx<R> o[12];
-    if (EPI == EPI_STORE) {
+    for (int c = 0; c < 12; ++c) {
+      const double2 t = *reinterpret_cast<const double2*>(slot + c * T);
+      v[c] = {t.x, t.y};
+    }
+  }
+};
+template <>
+struct SlotSpinor<P32> {
+  __device__ static inline void load(const uint4* slot, int T, cplx<float>* v) {
 #pragma unroll
-      for (int c = 0; c < 12; ++c) o[c] = acc[r][c];
-    } else if (EPI == EPI_TWIST) {
-      const R t = (R)a.a;
+    for (int q = 0; q < 6; ++q) {
+      const float4 t = *reinterpret_cast<const float4*>(slot + q * T);
+      v[2 * q] = {t.x, t.y};
+      v[2 * q + 1] = {t.z, t.w};
+    }
+  }
+};
+template <>
+struct SlotSpinor<P16> {
+  // slots 0..2: the halves; slot 3: the site norm in its first 4 bytes
+  __device__ static inline void load(const uint4* slot, int T, cplx<float>* v) {
+    const float nrm = *reinterpret_cast<const float*>(slot + 3 * T);
 #pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        o[0 + c] = csub(acc[r][0 + c], cscale(t, acc[r][6 + c]));
-        o[3 + c] = csub(acc[r][3 + c], cscale(t, acc[r][9 + c]));
-        o[6 + c] = cadd(acc[r][6 + c], cscale(t, acc[r][0 + c]));
-        o[9 + c] = cadd(acc[r][9 + c], cscale(t, acc[r][3 + c]));
-      }
-    } else {
-      cplx<R> gg[12];
-      SIO::load(a.aux[r], a.aux_norm[r], a.g.vh, s, gg);
-      const R f1 = (R)a.f1, f2 = (R)a.f2, f3 = (R)a.f3;
+    for (int q = 0; q < 3; ++q) {
+      const uint4 t = slot[q * T];
+      const __half2* h = reinterpret_cast<const __half2*>(&t);
 #pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        o[0 + c] = csub(cadd(cscale(f1, gg[0 + c]), cscale(f2, gg[6 + c])), cscale(f3, acc[r][0 + c]));
-        o[3 + c] = csub(cadd(cscale(f1, gg[3 + c]), cscale(f2, gg[9 + c])), cscale(f3, acc[r][3 + c]));
-        o[6 + c] = csub(csub(cscale(f1, gg[6 + c]), cscale(f2, gg[0 + c])), cscale(f3, acc[r][6 + c]));
-        o[9 + c] = csub(csub(cscale(f1, gg[9 + c]), cscale(f2, gg[3 + c])), cscale(f3, acc[r][9 + c]));
+      for (int k = 0; k < 4; ++k) {
+        const float2 f = __half22float2(h[k]);
+        v[4 * q + k] = {f.x * nrm, f.y * nrm};
       }
     }
-    SIO::store(a.out[r], a.out_norm[r], a.g.vh, s, o);
   }
+};
+
+template <int LP, int RECON>
+__device__ inline void slot_link(const uint4* slot, int T, Su3<typename LinkIO<LP, RECON>::R>& u) {
+  if (LP == P64) {
+    constexpr int n = RECON == 18 ? 9 : 6;
+#pragma unroll
+    for (int q = 0; q < n; ++q) {
+      const double2 t = *reinterpret_cast<const double2*>(slot + q * T);
+      reinterpret_cast<Su3<double>&>(u).e[q / 3][q % 3] = {t.x, t.y};
+    }
+    if (RECON == 12) reconstruct_row3(reinterpret_cast<Su3<double>&>(u));
+  } else {
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      const float4 t = *reinterpret_cast<const float4*>(slot + q * T);
+      const int c0 = 2 * q, c1 = 2 * q + 1;
+      reinterpret_cast<Su3<float>&>(u).e[c0 / 3][c0 % 3] = {t.x, t.y};
+      reinterpret_cast<Su3<float>&>(u).e[c1 / 3][c1 % 3] = {t.z, t.w};
+    }
+    reconstruct_row3(reinterpret_cast<Su3<float>&>(u));
+  }
+}
+
+// Neighbour of x in direction MU (forward or backward) and its boundary factor.
+template <int MU, bool FWD>
+__device__ inline int neighbour(const Geom& g, const int* x, int* sgn) {
+  int y[4] = {x[0], x[1], x[2], x[3]};
+  *sgn = 1;
+  if (FWD) {
+    y[MU] += 1;
+    if (y[MU] == g.n[MU]) {
+      y[MU] = 0;
+      *sgn = g.bc[MU];
+    }
+  } else {
+    y[MU] -= 1;
+    if (y[MU] < 0) {
+      y[MU] = g.n[MU] - 1;
+      *sgn = g.bc[MU];
+    }
+  }
+  return site_index(g, y);
+}
+
+template <int SP, int LP, int RECON>
+struct StageShape {
+  static constexpr int SQ = SpinorIO<SP>::planes + (SP == P16 ? 1 : 0);  // + norm slot
+  static constexpr int LQ = LinkIO<LP, RECON>::planes;
+  static constexpr int NQ = SQ + LQ;
+};
+
+template <int SP, int LP, int RECON, int MU, bool FWD>
+__device__ inline void stage_hop(const HopArgs& a, uint4* slots, int T, int s, int r,
+                                 const int* x) {
+  using Sh = StageShape<SP, LP, RECON>;
+  constexpr int H = 2 * MU + (FWD ? 0 : 1);
+  int sgn;
+  const int sy = neighbour<MU, FWD>(a.g, x, &sgn);
+  if (sgn == 0) return;
+  uint4* dst = slots + (size_t)H * Sh::NQ * T;
+  const uint4* sp = static_cast<const uint4*>(a.in[r]);
+#pragma unroll
+  for (int q = 0; q < SpinorIO<SP>::planes; ++q) cp_async16(dst + q * T, sp + (size_t)q * a.g.vh + sy);
+  if (SP == P16) cp_async4(dst + SpinorIO<SP>::planes * T, a.in_norm[r] + sy);
+  const int lp = FWD ? a.pout : 1 - a.pout;
+  const int ls = FWD ? s : sy;
+  const uint4* lk = static_cast<const uint4*>(a.gauge) + (size_t)(lp * 4 + MU) * Sh::LQ * a.g.vh;
+#pragma unroll
+  for (int q = 0; q < Sh::LQ; ++q) cp_async16(dst + (Sh::SQ + q) * T, lk + (size_t)q * a.g.vh + ls);
+}
+
+template <int SP, int LP, int RECON, int MU, bool FWD, class R>
+__device__ inline void apply_hop(const HopArgs& a, const uint4* slots, int T, const int* x,
+                                 cplx<R>* acc) {
+  using Sh = StageShape<SP, LP, RECON>;
+  constexpr int H = 2 * MU + (FWD ? 0 : 1);
+  int isgn;
+  (void)neighbour<MU, FWD>(a.g, x, &isgn);
+  if (isgn == 0) return;
+  const R sgn = (R)isgn;
+  const R cm = sgn * (R)(FWD ? a.c.fm[MU] : a.c.bm[MU]);
+  const R cp = sgn * (R)(FWD ? a.c.fp[MU] : a.c.bp[MU]);
+  const uint4* src = slots + (size_t)H * Sh::NQ * T;
+  cplx<R> psi[12];
+  SlotSpinor<SP>::load(src, T, psi);
+  Su3<R> u;
+  slot_link<LP, RECON>(src + Sh::SQ * T, T, u);
+  cplx<R> h[6], w[6];
+  if (cm != (R)0) {
+    project<MU, -1>(psi, cm, h);
+    if (FWD) {
+      matvec(u, h, w);
+      matvec(u, h + 3, w + 3);
+    } else {
+      matvec_dag(u, h, w);
+      matvec_dag(u, h + 3, w + 3);
+    }
+    reconstruct_acc<MU, -1>(acc, w);
+  }
+  if (cp != (R)0) {
+    project<MU, +1>(psi, cp, h);
+    if (FWD) {
+      matvec(u, h, w);
+      matvec(u, h + 3, w + 3);
+    } else {
+      matvec_dag(u, h, w);
+      matvec_dag(u, h + 3, w + 3);
+    }
+    reconstruct_acc<MU, +1>(acc, w);
+  }
+}
+
+template <int SP, class R>
+__device__ inline void hop_epilogue(const HopArgs& a, int EPI, int s, int r, const cplx<R>* acc) {
+  using SIO = SpinorIO<SP>;
+  cplx<R> o[12];
+  if (EPI == EPI_STORE) {
+#pragma unroll
+    for (int c = 0; c < 12; ++c) o[c] = acc[c];
+  } else if (EPI == EPI_TWIST) {
+    const R t = (R)a.a;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      o[0 + c] = csub(acc[0 + c], cscale(t, acc[6 + c]));
+      o[3 + c] = csub(acc[3 + c], cscale(t, acc[9 + c]));
+      o[6 + c] = cadd(acc[6 + c], cscale(t, acc[0 + c]));
+      o[9 + c] = cadd(acc[9 + c], cscale(t, acc[3 + c]));
+    }
+  } else {
+    cplx<R> gg[12];
+    SIO::load(a.aux[r], a.aux_norm[r], a.g.vh, s, gg);
+    const R f1 = (R)a.f1, f2 = (R)a.f2, f3 = (R)a.f3;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      o[0 + c] = csub(cadd(cscale(f1, gg[0 + c]), cscale(f2, gg[6 + c])), cscale(f3, acc[0 + c]));
+      o[3 + c] = csub(cadd(cscale(f1, gg[3 + c]), cscale(f2, gg[9 + c])), cscale(f3, acc[3 + c]));
+      o[6 + c] = csub(csub(cscale(f1, gg[6 + c]), cscale(f2, gg[0 + c])), cscale(f3, acc[6 + c]));
+      o[9 + c] = csub(csub(cscale(f1, gg[9 + c]), cscale(f2, gg[3 + c])), cscale(f3, acc[9 + c]));
+    }
+  }
+  SIO::store(a.out[r], a.out_norm[r], a.g.vh, s, o);
+}
+
+// blockDim.x = T threads = (T / nrhs) sites x nrhs right-hand sides; dynamic shared
+// memory = 8 * NQ * T * 16 bytes.
+template <int SP, int LP, int RECON, int EPI>
+__global__ void __launch_bounds__(128) hop_staged_kernel(HopArgs a) {
+  using R = typename SpinorIO<SP>::R;
+  extern __shared__ uint4 slots[];
+  const int T = blockDim.x;
+  const int nrhs = a.nrhs;
+  const int per_block = T / nrhs;
+  const int tid = threadIdx.x;
+  const int r = tid % nrhs;
+  const int s = blockIdx.x * per_block + tid / nrhs;
+  if (s >= a.g.vh || tid >= per_block * nrhs) return;
+  uint4* my = slots + tid;
+  int x[4];
+  site_coords(a.g, a.pout, s, x);
+  stage_hop<SP, LP, RECON, 0, true>(a, my, T, s, r, x);
+  stage_hop<SP, LP, RECON, 0, false>(a, my, T, s, r, x);
+  stage_hop<SP, LP, RECON, 1, true>(a, my, T, s, r, x);
+  stage_hop<SP, LP, RECON, 1, false>(a, my, T, s, r, x);
+  cp_async_commit();
+  stage_hop<SP, LP, RECON, 2, true>(a, my, T, s, r, x);
+  stage_hop<SP, LP, RECON, 2, false>(a, my, T, s, r, x);
+  stage_hop<SP, LP, RECON, 3, true>(a, my, T, s, r, x);
+  stage_hop<SP, LP, RECON, 3, false>(a, my, T, s, r, x);
+  cp_async_commit();
+  cplx<R> acc[12];
+#pragma unroll
+  for (int c = 0; c < 12; ++c) acc[c] = {(R)0, (R)0};
+  cp_async_wait<1>();
+  apply_hop<SP, LP, RECON, 0, true>(a, my, T, x, acc);
+  apply_hop<SP, LP, RECON, 0, false>(a, my, T, x, acc);
+  apply_hop<SP, LP, RECON, 1, true>(a, my, T, x, acc);
+  apply_hop<SP, LP, RECON, 1, false>(a, my, T, x, acc);
+  cp_async_wait<0>();
+  apply_hop<SP, LP, RECON, 2, true>(a, my, T, x, acc);
+  apply_hop<SP, LP, RECON, 2, false>(a, my, T, x, acc);
+  apply_hop<SP, LP, RECON, 3, true>(a, my, T, x, acc);
+  apply_hop<SP, LP, RECON, 3, false>(a, my, T, x, acc);
+  hop_epilogue<SP, R>(a, EPI, s, r, acc);
+}
+
+template <int SP, int LP, int RECON>
+inline size_t staged_smem_bytes(int T) {
+  return (size_t)8 * StageShape<SP, LP, RECON>::NQ * T * 16;
+}
+
+// Block shape of hop_kernel for TPS direction groups and nrhs right-hand sides.
+inline void hop_block_shape(int tps, int nrhs, int vh, dim3* blk, dim3* grd) {
+  const int bx_max = 128 / tps;
+  const int per_block = bx_max / nrhs;
+  *blk = dim3(per_block * nrhs, tps);
+  *grd = dim3((vh + per_block - 1) / per_block);
 }
 
 // Host-side helper: the hop coefficients of Hsingle for action coefficients

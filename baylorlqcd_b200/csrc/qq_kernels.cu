@@ -1,4 +1,6 @@
 // Instantiations and launchers of the library's CUDA kernels (sm_100a).
+#include <atomic>
+
 #include "qq_blas.cuh"
 #include "qq_dslash.cuh"
 #include "qq_launch.h"
@@ -6,41 +8,76 @@
 
 namespace qq {
 
+static std::atomic<long long> g_launches{0};
+void count_launch(long long n) { g_launches += n; }
+long long launch_count() { return g_launches.load(); }
+
 // ---------------------------------------------------------------------------
 // Dslash
 // ---------------------------------------------------------------------------
-template <int SP, int LP, int RECON, int NRHS>
+template <int SP, int LP, int RECON, int TPS>
 static cudaError_t hop_epi(const HopArgs& a, int epi, cudaStream_t st) {
-  dim3 blk(128), grd((a.g.vh + 127) / 128);
+  dim3 blk, grd;
+  hop_block_shape(TPS, a.nrhs, a.g.vh, &blk, &grd);
   switch (epi) {
-    case EPI_STORE: hop_kernel<SP, LP, RECON, NRHS, EPI_STORE><<<grd, blk, 0, st>>>(a); break;
-    case EPI_TWIST: hop_kernel<SP, LP, RECON, NRHS, EPI_TWIST><<<grd, blk, 0, st>>>(a); break;
-    case EPI_DBLE: hop_kernel<SP, LP, RECON, NRHS, EPI_DBLE><<<grd, blk, 0, st>>>(a); break;
+    case EPI_STORE: hop_kernel<SP, LP, RECON, TPS, EPI_STORE><<<grd, blk, 0, st>>>(a); break;
+    case EPI_TWIST: hop_kernel<SP, LP, RECON, TPS, EPI_TWIST><<<grd, blk, 0, st>>>(a); break;
+    case EPI_DBLE: hop_kernel<SP, LP, RECON, TPS, EPI_DBLE><<<grd, blk, 0, st>>>(a); break;
     default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();
 }
 
-template <int SP>
-static cudaError_t hop_low(const HopArgs& a, int epi, cudaStream_t st) {
-  switch (a.nrhs) {
-    case 1: return hop_epi<SP, P32, 12, 1>(a, epi, st);
-    case 2: return hop_epi<SP, P32, 12, 2>(a, epi, st);
-    case 3: return hop_epi<SP, P32, 12, 3>(a, epi, st);
-    case 4: return hop_epi<SP, P32, 12, 4>(a, epi, st);
+template <int SP, int LP, int RECON, int EPI>
+static cudaError_t hop_staged_launch(const HopArgs& a, int T, cudaStream_t st) {
+  const size_t smem = staged_smem_bytes<SP, LP, RECON>(T);
+  if (smem > 227 * 1024) return cudaErrorInvalidValue;
+  static bool attr_set = false;  // one attribute call per instantiation
+  if (!attr_set) {
+    cudaError_t e = cudaFuncSetAttribute(hop_staged_kernel<SP, LP, RECON, EPI>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    if (e != cudaSuccess) return e;
+    attr_set = true;
+  }
+  const int per_block = T / a.nrhs;
+  dim3 grd((a.g.vh + per_block - 1) / per_block);
+  hop_staged_kernel<SP, LP, RECON, EPI><<<grd, T, smem, st>>>(a);
+  return cudaGetLastError();
+}
+
+template <int SP, int LP, int RECON>
+static cudaError_t hop_tps(const HopArgs& a, int epi, int tps, cudaStream_t st) {
+  switch (tps) {
+    case 1: return hop_epi<SP, LP, RECON, 1>(a, epi, st);
+    case 2: return hop_epi<SP, LP, RECON, 2>(a, epi, st);
+    case 4: return hop_epi<SP, LP, RECON, 4>(a, epi, st);
+    case 32:
+    case 64:
+    case 96:
+    case 128:
+      switch (epi) {
+        case EPI_STORE: return hop_staged_launch<SP, LP, RECON, EPI_STORE>(a, tps, st);
+        case EPI_TWIST: return hop_staged_launch<SP, LP, RECON, EPI_TWIST>(a, tps, st);
+        case EPI_DBLE: return hop_staged_launch<SP, LP, RECON, EPI_DBLE>(a, tps, st);
+        default: return cudaErrorInvalidValue;
+      }
     default: return cudaErrorInvalidValue;
   }
 }
 
-cudaError_t launch_hop(const HopArgs& a, int sp, int recon, int epi, cudaStream_t st) {
+// tps: 1, 2, 4 = register kernel with that many direction groups per site;
+// 32, 64, 96, 128 = staged kernel with that many threads per block.
+cudaError_t launch_hop(const HopArgs& a, int sp, int recon, int epi, int tps, cudaStream_t st) {
+  count_launch();
+  const int per = tps <= 4 ? 128 / tps : tps;
+  if (a.nrhs < 1 || a.nrhs > kMaxRhs || a.nrhs > per) return cudaErrorInvalidValue;
   if (sp == P64) {
-    if (a.nrhs != 1) return cudaErrorInvalidValue;
-    if (recon == 18) return hop_epi<P64, P64, 18, 1>(a, epi, st);
-    if (recon == 12) return hop_epi<P64, P64, 12, 1>(a, epi, st);
+    if (recon == 18) return hop_tps<P64, P64, 18>(a, epi, tps, st);
+    if (recon == 12) return hop_tps<P64, P64, 12>(a, epi, tps, st);
     return cudaErrorInvalidValue;
   }
-  if (sp == P32) return hop_low<P32>(a, epi, st);
-  if (sp == P16) return hop_low<P16>(a, epi, st);
+  if (sp == P32) return hop_tps<P32, P32, 12>(a, epi, tps, st);
+  if (sp == P16) return hop_tps<P16, P32, 12>(a, epi, tps, st);
   return cudaErrorInvalidValue;
 }
 
@@ -57,6 +94,7 @@ static cudaError_t lin4(const LinArgs& L, cudaStream_t st) {
 // single lower-precision operand in x (promotion), or lower output from FP64 x
 // (demotion).
 cudaError_t launch_lincomb(const LinArgs& L, int px, int py, int pz, int po, cudaStream_t st) {
+  count_launch();
   if (!L.y.data) py = po;
   if (!L.z.data) pz = po;
   if (!L.x.data) px = po;
@@ -79,6 +117,7 @@ cudaError_t launch_lincomb(const LinArgs& L, int px, int py, int pz, int po, cud
 }
 
 cudaError_t launch_dot(int vh, Spinor x, Spinor y, double* partial, cudaStream_t st) {
+  count_launch();
   if (x.prec == P64 && y.prec == P64)
     dot_kernel<P64, P64><<<kRedBlocks, kRedThreads, 0, st>>>(vh, x, y, partial);
   else if (x.prec == P32 && y.prec == P32)
@@ -112,6 +151,7 @@ __global__ void finalize_sum_kernel(const double* partial, int nblocks, int nvst
 
 cudaError_t launch_finalize(const double* partial, int nblocks, int nvstride, int nout,
                             double* out, int add, cudaStream_t st) {
+  count_launch();
   finalize_sum_kernel<<<nout, 256, 0, st>>>(partial, nblocks, nvstride, nout, out, add);
   return cudaGetLastError();
 }
@@ -121,6 +161,7 @@ cudaError_t launch_finalize(const double* partial, int nblocks, int nvstride, in
 // ---------------------------------------------------------------------------
 cudaError_t launch_multidot(int pb, const BasisArgs& V, int nv, const void* w, double* partial,
                             int* ngroups_out, cudaStream_t st) {
+  count_launch();
   const int ng = (nv + 7) / 8;
   *ngroups_out = ng;
   dim3 grd(kRedBlocks, ng);
@@ -135,6 +176,7 @@ cudaError_t launch_multidot(int pb, const BasisArgs& V, int nv, const void* w, d
 
 cudaError_t launch_multiaxpy(int pb, const BasisArgs& V, int nv, const double* h, double hsign,
                              const void* w, void* wout, double* partial, cudaStream_t st) {
+  count_launch();
   if (nv > 128) return cudaErrorInvalidValue;
   if (pb == P64)
     multiaxpy_kernel<P64><<<kRedBlocks, kRedThreads, 0, st>>>(V, nv, h, hsign, w, wout, partial);
@@ -147,6 +189,7 @@ cudaError_t launch_multiaxpy(int pb, const BasisArgs& V, int nv, const double* h
 
 cudaError_t launch_normalize(int pb, size_t nel, const void* in, void* out, const double* nrm2,
                              cudaStream_t st) {
+  count_launch();
   if (pb == P64)
     normalize_kernel<P64><<<kRedBlocks, kRedThreads, 0, st>>>(nel, in, out, nrm2);
   else if (pb == P32)
@@ -158,6 +201,7 @@ cudaError_t launch_normalize(int pb, size_t nel, const void* in, void* out, cons
 
 cudaError_t launch_rotate(int pb, const BasisArgs& V, int nin, int nout, const double* Z, int ldz,
                           cudaStream_t st) {
+  count_launch();
   const size_t smem = sizeof(double) * 2 * (size_t)nin * nout;
   if (smem > 200 * 1024 || nout > 64) return cudaErrorInvalidValue;
   const int grid = 148 * 4;
@@ -184,6 +228,7 @@ cudaError_t launch_rotate(int pb, const BasisArgs& V, int nin, int nout, const d
 
 cudaError_t launch_basis_accum(int pb, const BasisArgs& V, int nv, const double* y, int vh,
                                Spinor x, cudaStream_t st) {
+  count_launch();
   if (nv > 128) return cudaErrorInvalidValue;
   if (pb == P64 && x.prec == P64)
     basis_accum_kernel<P64, P64><<<kRedBlocks, kRedThreads, 0, st>>>(V, nv, y, vh, x);
@@ -212,6 +257,7 @@ __global__ void hcol_update_kernel(double* H, int ldh, int j, const double* h2, 
 
 cudaError_t launch_hcol_update(double* H, int ldh, int j, const double* h2, int nh,
                                const double* nrm2, cudaStream_t st) {
+  count_launch();
   hcol_update_kernel<<<1, 128, 0, st>>>(H, ldh, j, h2, nh, nrm2);
   return cudaGetLastError();
 }
@@ -221,6 +267,7 @@ cudaError_t launch_hcol_update(double* H, int ldh, int j, const double* h2, int 
 // ---------------------------------------------------------------------------
 cudaError_t launch_spinor_from_ref(const Geom& g, const RefDims& d, int p, const double* ref,
                                    Spinor out, cudaStream_t st) {
+  count_launch();
   dim3 blk(128), grd((g.vh + 127) / 128);
   if (out.prec == P64)
     spinor_from_ref_kernel<P64><<<grd, blk, 0, st>>>(g, d, p, ref, out);
@@ -233,6 +280,7 @@ cudaError_t launch_spinor_from_ref(const Geom& g, const RefDims& d, int p, const
 
 cudaError_t launch_spinor_to_ref(const Geom& g, const RefDims& d, int p, Spinor in, double* ref,
                                  cudaStream_t st) {
+  count_launch();
   dim3 blk(128), grd((g.vh + 127) / 128);
   if (in.prec == P64)
     spinor_to_ref_kernel<P64><<<grd, blk, 0, st>>>(g, d, p, in, ref);
@@ -244,6 +292,7 @@ cudaError_t launch_spinor_to_ref(const Geom& g, const RefDims& d, int p, Spinor 
 }
 
 cudaError_t launch_ref_zero_halo(const RefDims& d, double* ref, cudaStream_t st) {
+  count_launch();
   if (d.ntotal == d.nvhalf) return cudaSuccess;
   ref_zero_halo_kernel<<<148, 256, 0, st>>>(d, ref);
   return cudaGetLastError();
@@ -251,6 +300,7 @@ cudaError_t launch_ref_zero_halo(const RefDims& d, double* ref, cudaStream_t st)
 
 cudaError_t launch_gauge_from_ref(const Geom& g, const RefDims& d, const double* ref, void* out,
                                   int prec, int recon, cudaStream_t st) {
+  count_launch();
   dim3 blk(128), grd((2 * g.vh + 127) / 128);
   if (prec == P64 && recon == 18)
     gauge_from_ref_kernel<P64, 18><<<grd, blk, 0, st>>>(g, d, ref, out);
@@ -265,6 +315,7 @@ cudaError_t launch_gauge_from_ref(const Geom& g, const RefDims& d, const double*
 
 cudaError_t launch_su3_defect(const Geom& g, const RefDims& d, const double* ref, double* partial,
                               cudaStream_t st) {
+  count_launch();
   su3_defect_kernel<<<kRedBlocks, 256, 0, st>>>(g, d, ref, partial);
   return cudaGetLastError();
 }
@@ -301,6 +352,7 @@ __global__ void spinmix_kernel(int vh, Spinor x, Spinor y, Spinor out, double a,
 
 cudaError_t launch_spinmix(int vh, Spinor x, Spinor y, Spinor out, double a, double ta, double b,
                            double tb, int prec, cudaStream_t st) {
+  count_launch();
   if (prec == P64)
     spinmix_kernel<P64><<<kRedBlocks, kRedThreads, 0, st>>>(vh, x, y, out, a, ta, b, tb);
   else if (prec == P32)

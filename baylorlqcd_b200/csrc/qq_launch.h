@@ -6,14 +6,19 @@
 
 namespace qq {
 
+// Kernel-launch counter (every launcher below adds its launches).
+void count_launch(long long n = 1);
+long long launch_count();
+
 struct HopArgs;
 struct LinArgs;
 struct BasisArgs;
 struct Coef;
 
 // Dirac hopping term.  sp: spinor precision (P64/P32/P16); recon: 18 or 12 (P64
-// links) -- P32/P16 spinors always use the FP32 recon-12 links; epi: Epilogue.
-cudaError_t launch_hop(const HopArgs& a, int sp, int recon, int epi, cudaStream_t st);
+// links) -- P32/P16 spinors always use the FP32 recon-12 links; epi: Epilogue;
+// tps: threads per site (direction groups: 1, 2 or 4).
+cudaError_t launch_hop(const HopArgs& a, int sp, int recon, int epi, int tps, cudaStream_t st);
 
 // out = a x + b y + c z (+ reductions into partial).  Precisions per operand.
 cudaError_t launch_lincomb(const LinArgs& L, int px, int py, int pz, int po, cudaStream_t st);

@@ -104,28 +104,88 @@ static HopArgs hop_base(qq_ctx* c, int idag, int pout, int prec) {
 
 static int recon_of(qq_ctx* c, int prec) { return prec == P64 ? c->recon64 : 12; }
 
+// Launch the hopping kernel with the number of direction groups (threads per site)
+// that ran fastest for this (precision, links, RHS count, epilogue) on this lattice.
+// The first launch of a shape times each candidate on the real operands (the kernel
+// is idempotent: inputs are never outputs) and caches the winner in the context.
+// Algorithmic bytes of one hop launch: every link once, every input and output spinor
+// once, and the epilogue's extra input for EPI_DBLE.
+static double hop_bytes(qq_ctx* c, int prec, int nrhs, int epi) {
+  const int recon = recon_of(c, prec);
+  const double link = prec == P64 ? (recon == 18 ? 144.0 : 96.0) : 48.0;
+  const double spin = prec == P64 ? 192.0 : prec == P32 ? 96.0 : 52.0;
+  return (double)c->g.vh * (8.0 * link + nrhs * (epi == EPI_DBLE ? 3.0 : 2.0) * spin);
+}
+
+static int launch_hop_profiled(qq_ctx* c, const HopArgs& a, int prec, int recon, int epi, int tps) {
+  if (!c->prof_hop) {
+    QQ_CK(launch_hop(a, prec, recon, epi, tps, c->st));
+    return QQ_OK;
+  }
+  if (c->prof_used == c->prof_events.size()) {
+    cudaEvent_t e0, e1;
+    QQ_CK(cudaEventCreate(&e0));
+    QQ_CK(cudaEventCreate(&e1));
+    c->prof_events.emplace_back(e0, e1);
+    c->prof_bytes.push_back(0.0);
+  }
+  auto& ev = c->prof_events[c->prof_used];
+  c->prof_bytes[c->prof_used] = hop_bytes(c, prec, a.nrhs, epi);
+  ++c->prof_used;
+  QQ_CK(cudaEventRecord(ev.first, c->st));
+  QQ_CK(launch_hop(a, prec, recon, epi, tps, c->st));
+  QQ_CK(cudaEventRecord(ev.second, c->st));
+  return QQ_OK;
+}
+
+int launch_hop_tuned(qq_ctx* c, const HopArgs& a, int prec, int epi) {
+  const int recon = recon_of(c, prec);
+  const int key = ((prec * 64 + recon) * 16 + a.nrhs) * 4 + epi;
+  auto it = c->hop_tune.find(key);
+  if (it != c->hop_tune.end()) return launch_hop_profiled(c, a, prec, recon, epi, it->second);
+  if (c->forced_tps > 0) {
+    c->hop_tune[key] = c->forced_tps;
+    QQ_CK(launch_hop(a, prec, recon, epi, c->forced_tps, c->st));
+    return QQ_OK;
+  }
+  int best = 1;
+  float best_ms = 1e30f;
+  for (int tps : {1, 2, 32, 64, 96, 128}) {
+    const int per = tps <= 4 ? 128 / tps : tps;
+    if (a.nrhs > per) continue;
+    if (launch_hop(a, prec, recon, epi, tps, c->st) != cudaSuccess) {  // warm-up
+      cudaGetLastError();  // shape not launchable (shared memory): skip it
+      continue;
+    }
+    QQ_CK(cudaEventRecord(c->tev0, c->st));
+    for (int i = 0; i < 3; ++i) QQ_CK(launch_hop(a, prec, recon, epi, tps, c->st));
+    QQ_CK(cudaEventRecord(c->tev1, c->st));
+    QQ_CK(cudaEventSynchronize(c->tev1));
+    float ms = 0.f;
+    QQ_CK(cudaEventElapsedTime(&ms, c->tev0, c->tev1));
+    if (ms < best_ms) {
+      best_ms = ms;
+      best = tps;
+    }
+  }
+  c->hop_tune[key] = best;
+  return launch_hop_profiled(c, a, prec, recon, epi, best);
+}
+
 int op_hsingle_multi(qq_ctx* c, const Spinor* out, const Spinor* in, int n, int idag, int pout) {
   if (!c->have_gauge) return set_error(QQ_BAD_ARG, "no gauge field uploaded");
   const int prec = in[0].prec;
-  for (int r0 = 0; r0 < n; r0 += 4) {
-    const int nb = std::min(4, n - r0);
+  for (int r0 = 0; r0 < n; r0 += kMaxRhs) {
+    const int nb = std::min(kMaxRhs, n - r0);
     HopArgs a = hop_base(c, idag, pout, prec);
-    a.nrhs = prec == P64 ? 1 : nb;
-    const int step = a.nrhs;
-    for (int r = 0; r < step; ++r) {
+    a.nrhs = nb;
+    for (int r = 0; r < nb; ++r) {
       a.in[r] = in[r0 + r].data;
       a.in_norm[r] = in[r0 + r].norm;
       a.out[r] = out[r0 + r].data;
       a.out_norm[r] = out[r0 + r].norm;
     }
-    QQ_CK(launch_hop(a, prec, recon_of(c, prec), EPI_STORE, c->st));
-    if (prec == P64 && nb > 1) {  // FP64 runs one right-hand side per launch
-      for (int r = 1; r < nb; ++r) {
-        a.in[0] = in[r0 + r].data;
-        a.out[0] = out[r0 + r].data;
-        QQ_CK(launch_hop(a, prec, recon_of(c, prec), EPI_STORE, c->st));
-      }
-    }
+    QQ_TRY(launch_hop_tuned(c, a, prec, EPI_STORE));
   }
   return QQ_OK;
 }
@@ -139,9 +199,8 @@ int op_dbletm_multi(qq_ctx* c, const Spinor* out, const Spinor* in, const Spinor
   if (!c->have_gauge) return set_error(QQ_BAD_ARG, "no gauge field uploaded");
   const int prec = in[0].prec;
   const bool wilson = kappa[1] < 0.00000001;  // Q/diracops.f90:467
-  const int maxb = prec == P64 ? 1 : 4;
-  for (int r0 = 0; r0 < n; r0 += maxb) {
-    const int nb = std::min(maxb, n - r0);
+  for (int r0 = 0; r0 < n; r0 += kMaxRhs) {
+    const int nb = std::min(kMaxRhs, n - r0);
     HopArgs a = hop_base(c, idag, 1, prec);
     a.nrhs = nb;
     for (int r = 0; r < nb; ++r) {
@@ -151,7 +210,7 @@ int op_dbletm_multi(qq_ctx* c, const Spinor* out, const Spinor* in, const Spinor
       a.out_norm[r] = tmp[r0 + r].norm;
     }
     a.a = 2.0 * kappa[0] * kappa[1];
-    QQ_CK(launch_hop(a, prec, recon_of(c, prec), wilson ? EPI_STORE : EPI_TWIST, c->st));
+    QQ_TRY(launch_hop_tuned(c, a, prec, wilson ? EPI_STORE : EPI_TWIST));
     HopArgs b = hop_base(c, idag, 0, prec);
     b.nrhs = nb;
     for (int r = 0; r < nb; ++r) {
@@ -171,7 +230,7 @@ int op_dbletm_multi(qq_ctx* c, const Spinor* out, const Spinor* in, const Spinor
       b.f2 = 2.0 * kappa[1] / kappa[0];
       b.f3 = 1.0 / (1.0 + t * t);
     }
-    QQ_CK(launch_hop(b, prec, recon_of(c, prec), EPI_DBLE, c->st));
+    QQ_TRY(launch_hop_tuned(c, b, prec, EPI_DBLE));
   }
   return QQ_OK;
 }

@@ -308,6 +308,138 @@ int gmresproj_fp64(qq_ctx* c, Spinor b, Spinor x, int m, int k, double resmax, i
 }
 
 // ---------------------------------------------------------------------------
+// Mixed-precision GMRES-DR(m, k): the Arnoldi process (operator, Krylov basis, Gram-
+// Schmidt) runs in FP32 with FP64 reductions; the solution accumulates in FP64 and
+// every cycle ends with the FP64 true residual r = b - A x.  The next cycle starts
+// from the harmonic-Ritz basis V_{k+1} of the restart with the least-squares
+// right-hand side c = V_{k+1}^H r (the projection of the FP64 residual), so rounding
+// of the FP32 cycle never accumulates into the answer.  Returns the FP32 deflation
+// space (V_{k+1}, Hk) of the last restart for the other right-hand sides.
+// ---------------------------------------------------------------------------
+int gmresdr_mixed(qq_ctx* c, Spinor b, Spinor x, int m, int k, double tol, int max_cycles,
+                  const double kappa[2], DeflSpace* defl, SolveStats* st) {
+  if (m < 2 || k < 1 || k >= m || m > 127) return set_error(QQ_BAD_ARG, "GMRES(n,k) out of range");
+  Arnoldi A;
+  QQ_TRY(A.init(c, P32, m));
+  Tmp tmp32(c, P32), tmp64(c, P64), r(c, P64), r32(c, P32);
+  double* nrm2 = c->scal.as<double>() + 8;
+  double bn = 0.0;
+  QQ_TRY(norm2_host(c, b, &bn));
+  bn = std::sqrt(bn);
+  double rn = 0.0;
+  QQ_TRY(true_residual(c, b, x, r.sp(), tmp64.sp(), kappa, &rn));
+  st->mvp += 1;
+  if (!(bn > 0.0)) return QQ_OK;
+  if (!std::isfinite(rn)) return set_error(QQ_NAN, "NaN in initial residual");
+  st->true_rel = rn / bn;
+  if (rn / bn <= tol) return QQ_OK;
+  QQ_TRY(lin(c, A.sp(0), cimm(1.0 / rn), r.sp()));
+  std::vector<dense::cd> cvec(m + 1, 0.0);
+  cvec[0] = rn;
+  QQ_TRY(A.zeroH());
+  DevBuf cd, Pd;
+  QQ_CK(cd.alloc(sizeof(double) * 2 * 256));
+  QQ_CK(Pd.alloc(sizeof(double) * 2 * (size_t)(m + 1) * (k + 1)));
+  int j0 = 0, icycle = 1, status = QQ_NOT_CONVERGED;
+  dense::Mat Hk_last;
+  bool restarted = false;
+  for (;;) {
+    for (int j = j0; j < m; ++j) {
+      QQ_TRY(arnoldi_step(A, j, tmp32.sp(), kappa, nrm2));
+      st->itercount += 1;
+      st->mvp += 1;
+    }
+    dense::Mat Hb;
+    QQ_TRY(read_H(A, m, Hb));
+    std::vector<dense::cd> y, srv;
+    dense::hess_lsq(Hb, cvec, m, y, srv);
+    QQ_TRY(upload_cvec(c, y, A.y.as<double>()));
+    QQ_CK(launch_basis_accum(P32, A.basis(), m, A.y.as<double>(), c->g.vh, x, c->st));
+    QQ_TRY(true_residual(c, b, x, r.sp(), tmp64.sp(), kappa, &rn));
+    st->mvp += 1;
+    st->true_rel = rn / bn;
+    st->hist.push_back(rn / bn);
+    st->hist_mvp.push_back(st->mvp);
+    st->ncycles = icycle;
+    if (!std::isfinite(rn)) {
+      status = set_error(QQ_NAN, "NaN residual in mixed gmresdr");
+      break;
+    }
+    if (rn / bn <= tol) {
+      status = QQ_OK;
+      break;
+    }
+    if (icycle >= max_cycles) break;
+    dense::Mat P, Hk;
+    std::vector<dense::cd> cnew, ritz;
+    if (!dense::gmresdr_restart(Hb, srv, m, k, P, Hk, cnew, ritz)) {
+      status = set_error(QQ_SINGULAR, "harmonic Ritz step failed");
+      break;
+    }
+    st->ritz = ritz;
+    QQ_TRY(upload_mat(c, P, Pd.as<double>(), m + 1));
+    QQ_CK(launch_rotate(P32, A.basis(), m + 1, k + 1, Pd.as<double>(), m + 1, c->st));
+    QQ_TRY(reorth(A, k, nrm2));
+    QQ_TRY(A.zeroH());
+    QQ_TRY(upload_mat(c, Hk, A.H.as<double>(), m + 1));
+    // c = V_{k+1}^H r with the FP64 residual rounded to the basis precision
+    QQ_TRY(lin(c, r32.sp(), cimm(1.0), r.sp()));
+    int ng = 0;
+    double* part = c->partial.as<double>();
+    QQ_CK(launch_multidot(P32, A.basis(), k + 1, r32.sp().data, part, &ng, c->st));
+    QQ_CK(launch_finalize(part, kRedBlocks, ng * 16, 2 * (k + 1), cd.as<double>(), 0, c->st));
+    std::vector<double> ch(2 * (k + 1));
+    QQ_TRY(read_scalars(c, cd.as<double>(), 2 * (k + 1), ch.data()));
+    std::fill(cvec.begin(), cvec.end(), 0.0);
+    for (int i = 0; i <= k; ++i) cvec[i] = {ch[2 * i], ch[2 * i + 1]};
+    Hk_last = Hk;
+    restarted = true;
+    j0 = k;
+    icycle += 1;
+  }
+  if (defl && restarted) {
+    defl->k = k;
+    defl->pb = P32;
+    defl->nel = A.nel;
+    QQ_CK(defl->V.alloc((size_t)(k + 1) * A.nel * 16));
+    QQ_CK(cudaMemcpyAsync(defl->V.p, A.V.p, (size_t)(k + 1) * A.nel * 16, cudaMemcpyDeviceToDevice, c->st));
+    defl->Hk = Hk_last;
+  }
+  QQ_CK(cudaStreamSynchronize(c->st));
+  return status;
+}
+
+// x += V_k y with y = argmin || V_{k+1}^H r - Hk y ||, then r = b - A x (FP64).
+// The minimum-residual projection of GMRES-Proj (inverters.f90:7515-7601) onto a
+// deflation space of either basis precision.
+int defl_project(qq_ctx* c, const DeflSpace& d, Spinor b, Spinor x, Spinor r, const double kappa[2],
+                 double* rn) {
+  if (d.k <= 0) return QQ_OK;
+  Tmp rl(c, d.pb), tmp64(c, P64);
+  DevBuf cd, yd;
+  QQ_CK(cd.alloc(sizeof(double) * 2 * 256));
+  QQ_CK(yd.alloc(sizeof(double) * 2 * 256));
+  const void* rv = r.data;
+  if (d.pb != P64) {
+    QQ_TRY(lin(c, rl.sp(), cimm(1.0), r));
+    rv = rl.sp().data;
+  }
+  BasisArgs D{d.V.p, d.nel, d.nel};
+  int ng = 0;
+  double* part = c->partial.as<double>();
+  QQ_CK(launch_multidot(d.pb, D, d.k + 1, rv, part, &ng, c->st));
+  QQ_CK(launch_finalize(part, kRedBlocks, ng * 16, 2 * (d.k + 1), cd.as<double>(), 0, c->st));
+  std::vector<double> ch(2 * (d.k + 1));
+  QQ_TRY(read_scalars(c, cd.as<double>(), 2 * (d.k + 1), ch.data()));
+  std::vector<dense::cd> cv(d.k + 1), y, srv;
+  for (int i = 0; i <= d.k; ++i) cv[i] = {ch[2 * i], ch[2 * i + 1]};
+  dense::hess_lsq(d.Hk, cv, d.k, y, srv);
+  QQ_TRY(upload_cvec(c, y, yd.as<double>()));
+  QQ_CK(launch_basis_accum(d.pb, D, d.k, yd.as<double>(), c->g.vh, x, c->st));
+  return true_residual(c, b, x, r, tmp64.sp(), kappa, rn);
+}
+
+// ---------------------------------------------------------------------------
 // BiCGStab (inverters.f90:302-487), FP64.  Stops when ||r|| / ||r0|| < resmax with
 // the recursively updated residual, as the reference.
 // ---------------------------------------------------------------------------

@@ -75,6 +75,18 @@ int qq_set_coact(qq_ctx* ctx, const double c1[4], const double c2[4]);
  * FP32 recon-12 copy used by the mixed-precision solvers. */
 int qq_gauge_upload(qq_ctx* ctx, const double* u_ref, int recon);
 
+/* Quenched SU(3) configuration on the GPU: Wilson plaquette action at `beta`,
+ * cold start, `nsweeps` Cabibbo-Marinari / Kennedy-Pendleton heatbath sweeps with a
+ * counter-based generator seeded by `seed`.  Replaces the configuration-producing
+ * part of the reference's generator (G/heatbath.f90 phbup :33-76 driven from
+ * C/cfgsprops.f90 sweep :1973-2001); the reference's sequential random stream cannot
+ * be reproduced in parallel, so the ensemble is equivalent, not the configuration.
+ * Writes u_ref (reference u(18,ntotal,4,2,16), host or device; may be NULL), the
+ * average plaquette (1/3) Re Tr U_p into *plaq (may be NULL), and uploads the
+ * configuration as the context's gauge field (recon 12). */
+int qq_heatbath(qq_ctx* ctx, double beta, int nsweeps, unsigned long long seed, double* u_ref,
+                double* plaq);
+
 /* ---- Dirac operator (Q/diracops.f90) ---- */
 /* Hsingle :554-599.  gout = H_eo gin (gblclr = 1) or H_oe gin (gblclr = 2).
  * idag = 1 flips the sign of gamma_mu (H^dagger).  gout's halo slots are zeroed;
@@ -143,11 +155,17 @@ int qq_pointsource(qq_ctx* ctx, double* be, double* bo, const int src[4], int ic
  * 16) BiCGStab inside FP64 reliable updates.  be/bo/xe/xo: nrhs reference-layout
  * halves each, packed one after the other. */
 typedef struct qq_method {
-  int m, k;          /* GMRES-DR(m, k) for the first right-hand side */
-  int precision;     /* 64 (plain FP64 GMRES-DR per RHS), 32 or 16 */
-  int rhs_block;     /* right-hand sides per multi-RHS block (1..8) */
-  double tol;        /* FP64 true relative residual target */
-  int max_outer;     /* refinement steps limit */
+  int m, k;          /* GMRES-DR(m, k) */
+  int precision;     /* BiCGStab arithmetic: 64, 32 or 16 (FP64 reliable updates) */
+  int rhs_block;     /* right-hand sides solved together (1..32) */
+  double tol;        /* FP64 true full-lattice relative residual target */
+  int max_outer;     /* iteration limit in thousands (0: none) */
+  int solver;        /* 0: plain FP64 GMRES-DR(m,k) per right-hand side (the reference
+                        method); 1: batched BiCGStab */
+  int deflate;       /* solver 1: build k deflation vectors with mixed-precision
+                        GMRES-DR(m,k) on the first right-hand side and project every
+                        residual onto them at each reliable update */
+  double defl_tol;   /* relative residual the deflation-building solve stops at */
 } qq_method;
 int qq_fermprop_batch(qq_ctx* ctx, int nrhs, const double* be, const double* bo,
                       const double kappa[2], const qq_method* method, double* xe, double* xo,
@@ -172,11 +190,23 @@ int qq_twaverage_level0(qq_ctx* ctx, const double* be, const double* bo, const d
  * Times `niter` launches of the hopping kernel alone (H_oe of random fields, output
  * parity gblclr = 2) with CUDA events on the library's stream.  precision: 64
  * (links at the uploaded recon), 32 or 16 (FP32 recon-12 links); nrhs right-hand
- * sides per launch (1 for FP64).  flush_l2 != 0 overwrites a 512 MiB buffer between
+ * sides per launch (1..8); tps threads per site (1, 2, 4; 0 = the autotuned
+ * choice the solvers use).  flush_l2 != 0 overwrites a 512 MiB buffer between
  * launches so every launch reads its operands from HBM.  ms_per_call: mean kernel
  * time; bytes_per_call: algorithmic bytes of one launch,
  * V/2 * (8 * link bytes + nrhs * 2 * spinor bytes). */
-int qq_bench_hsingle(qq_ctx* ctx, int precision, int nrhs, int niter, int flush_l2,
+/* The cudaStream_t every call of this context runs on (for event timing). */
+int qq_ctx_stream(const qq_ctx* ctx, void** stream);
+/* Number of kernels this library has launched in this process so far. */
+long long qq_launch_count(void);
+/* enable != 0: time every hopping-kernel launch with CUDA events until disabled.
+ * qq_profile_hop_read returns the launches, their summed time and their summed
+ * algorithmic bytes V/2 * (8 * link bytes + nrhs * (2 or 3) * spinor bytes) since the
+ * last enable. */
+int qq_profile_hop(qq_ctx* ctx, int enable);
+int qq_profile_hop_read(qq_ctx* ctx, long long* launches, double* ms_total, double* bytes_total);
+
+int qq_bench_hsingle(qq_ctx* ctx, int precision, int nrhs, int tps, int niter, int flush_l2,
                      double* ms_per_call, double* bytes_per_call);
 
 #ifdef __cplusplus

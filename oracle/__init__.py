@@ -69,6 +69,7 @@ def lib() -> C.CDLL:
             "oq_evalues": ([I, I, I, I, DP, I, DP, DP, I], None),
             "oq_orgschur": ([IP, I, DP, I, DP, I, DP, IP], None),
             "oq_twaverage_level0": ([P, DP, DP, DP, DP, DP, D, DP], None),
+            "oq_set_kcyclim": ([I], None),
             "oq_coldstart": ([P, DP], None),
             "oq_aveplaq": ([P, DP], D),
         }
@@ -282,6 +283,11 @@ class OracleLattice:
     def aveplaq(self, u=None):
         u = self.u if u is None else u
         return lib().oq_aveplaq(self._g, _dp(np.ascontiguousarray(u)))
+
+
+def set_kcyclim(n: int):
+    """Cap GMRES-DR / GMRES-Proj cycles (0 restores the reference's 5000)."""
+    lib().oq_set_kcyclim(int(n))
 
 
 def initlagfib(myid: int, iseed: int):

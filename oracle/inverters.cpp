@@ -14,7 +14,7 @@
 #include "oracle_impl.h"
 
 namespace {
-constexpr int kcyclim = 5000;  // U/latdims.f90:70
+int kcyclim = 5000;  // U/latdims.f90:70 (lowered only to time a bounded sample)
 
 struct CMat {  // (2, ld, ncol) Fortran-order complex matrix, 1-based access
   std::vector<double> a;
@@ -179,6 +179,8 @@ void log_hist(oq_solve_log* log, int mvp, double rel) {
   }
 }
 }  // namespace
+
+extern "C" void oq_set_kcyclim(int n) { kcyclim = n > 0 ? n : 5000; }
 
 extern "C" oq_defl* oq_defl_create(const oq_geom* g, int nmax, int kmax) {
   auto* d = new oq_defl();

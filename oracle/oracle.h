@@ -75,6 +75,9 @@ void oq_gamma5vector(const oq_geom* g, double* a, int ntmqcd);
 void oq_vecdot(const oq_geom* g, const double* a, const double* b, double* adb);
 
 // ---- inverters (Q/inverters.f90) ----
+// Cycle cap of GMRES-DR / GMRES-Proj (kcyclim, U/latdims.f90:70; default 5000).  A
+// small cap times a bounded sample of the reference algorithm.
+void oq_set_kcyclim(int n);
 typedef struct oq_defl oq_defl;  // replaces module `shift` (vtemp, hcnew, beg)
 oq_defl* oq_defl_create(const oq_geom* g, int nmax, int kmax);
 void oq_defl_destroy(oq_defl* d);

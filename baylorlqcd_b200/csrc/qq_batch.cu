@@ -1,17 +1,17 @@
 // Batched mixed-precision propagators (qq_fermprop_batch).
 //
-// Method for nrhs sources on one configuration:
+// Method for nrhs sources on one configuration (solver = 1):
 //   1. source preparation and odd-half reconstruction exactly as fermprop
 //      (Q/quark.f90:595-618, :787-824), in FP64;
-//   2. the first right-hand side is solved with mixed-precision GMRES-DR(m, k), which
-//      also yields an FP32 deflation space (k harmonic-Ritz vectors);
-//   3. the other right-hand sides are first projected onto that space (the minimum-
-//      residual step of GMRES-Proj) and then solved together, in blocks, by BiCGStab
-//      in FP32 or FP16 with FP64 reliable updates: whenever the iterated residual has
-//      dropped by `delta` since the last update, the FP64 solution is updated and the
-//      FP64 true residual replaces the low-precision one (and is re-projected);
-//   4. every answer is judged by its FP64 true residual.
-// precision = 64 runs the plain FP64 GMRES-DR(m, k) of the reference on every RHS.
+//   2. optionally (deflate = 1) mixed-precision GMRES-DR(m, k) on the first source
+//      to tolerance defl_tol builds an FP32 deflation space (k harmonic-Ritz vectors);
+//   3. the right-hand sides are solved together, in blocks of rhs_block, by BiCGStab
+//      on RHS-interleaved block fields in FP64, FP32 or FP16 with FP64 reliable
+//      updates: whenever the iterated residual has dropped by `delta` since the last
+//      update, the FP64 solution is updated and the FP64 true residual replaces the
+//      low-precision one (projected onto the deflation space when there is one);
+//   4. every answer is judged by its FP64 true full-lattice residual.
+// solver = 0 runs the plain FP64 GMRES-DR(m, k) of the reference on every RHS.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -26,54 +26,61 @@ namespace {
 struct PerRhs {
   Field b, x;                  // FP64 even-system source and solution
   Field r64;                   // FP64 residual
-  Field r, rhat, p, v, t, xl;  // low precision BiCGStab vectors
-  Field tmp;                   // odd-parity temporary (low precision)
   double bn = 0.0, rmax = 0.0, rn = 0.0;
   bool done = false;
-  int slot = 0;
 };
 
-int alloc_field(qq_ctx* c, Field& f, int prec) {
+int alloc_field(qq_ctx* c, Field& f, int prec, int nsites_mult = 1) {
   f.prec = prec;
-  QQ_CK(f.data.alloc(field_bytes(prec, c->g.vh)));
-  if (prec == P16) QQ_CK(f.norm.alloc(sizeof(float) * c->g.vh));
+  QQ_CK(f.data.alloc(field_bytes(prec, c->g.vh) * nsites_mult));
+  if (prec == P16) QQ_CK(f.norm.alloc(sizeof(float) * c->g.vh * nsites_mult));
   return QQ_OK;
 }
 
 template <int P>
-int launch_bicg_op(qq_ctx* c, const BatchArgs& A, int op) {
-  dim3 grd(kRedBlocks, A.n);
+int launch_block_op(qq_ctx* c, const BlockBiArgs& A, int op) {
+  const int tb = A.nb * (kRedThreads / A.nb);
   switch (op) {
-    case OP_DOT_RHAT_R: bicg_kernel<P, OP_DOT_RHAT_R><<<grd, kRedThreads, 0, c->st>>>(A); break;
-    case OP_P_UPDATE: bicg_kernel<P, OP_P_UPDATE><<<grd, kRedThreads, 0, c->st>>>(A); break;
-    case OP_DOT_RHAT_V: bicg_kernel<P, OP_DOT_RHAT_V><<<grd, kRedThreads, 0, c->st>>>(A); break;
-    case OP_S_UPDATE: bicg_kernel<P, OP_S_UPDATE><<<grd, kRedThreads, 0, c->st>>>(A); break;
-    case OP_DOTS_T: bicg_kernel<P, OP_DOTS_T><<<grd, kRedThreads, 0, c->st>>>(A); break;
-    case OP_XR_UPDATE: bicg_kernel<P, OP_XR_UPDATE><<<grd, kRedThreads, 0, c->st>>>(A); break;
+    case OP_DOT_RHAT_R: bicg_block_kernel<P, OP_DOT_RHAT_R><<<kRedBlocks, tb, 0, c->st>>>(A); break;
+    case OP_P_UPDATE: bicg_block_kernel<P, OP_P_UPDATE><<<kRedBlocks, tb, 0, c->st>>>(A); break;
+    case OP_DOT_RHAT_V: bicg_block_kernel<P, OP_DOT_RHAT_V><<<kRedBlocks, tb, 0, c->st>>>(A); break;
+    case OP_S_UPDATE: bicg_block_kernel<P, OP_S_UPDATE><<<kRedBlocks, tb, 0, c->st>>>(A); break;
+    case OP_DOTS_T: bicg_block_kernel<P, OP_DOTS_T><<<kRedBlocks, tb, 0, c->st>>>(A); break;
+    case OP_XR_UPDATE: bicg_block_kernel<P, OP_XR_UPDATE><<<kRedBlocks, tb, 0, c->st>>>(A); break;
     default: return set_error(QQ_BAD_ARG, "bad batched op");
   }
   QQ_CK(cudaGetLastError());
   return QQ_OK;
 }
 
-int bicg_op(qq_ctx* c, int prec, const BatchArgs& A, int op, const int* dslots, int step) {
+int block_op(qq_ctx* c, int prec, const BlockBiArgs& A, int op, const int* dslots, int step) {
   count_launch(step >= 0 ? 2 : 1);
   if (prec == P32)
-    QQ_TRY(launch_bicg_op<P32>(c, A, op));
+    QQ_TRY(launch_block_op<P32>(c, A, op));
   else if (prec == P16)
-    QQ_TRY(launch_bicg_op<P16>(c, A, op));
+    QQ_TRY(launch_block_op<P16>(c, A, op));
   else
-    QQ_TRY(launch_bicg_op<P64>(c, A, op));
+    QQ_TRY(launch_block_op<P64>(c, A, op));
   if (step >= 0) {
-    bicg_scalar_kernel<<<A.n, 256, 0, c->st>>>(A.S, dslots, A.partial, kRedBlocks, step);
+    bicg_scalar_kernel<<<A.nb, 256, 0, c->st>>>(A.S, dslots, A.partial, kRedBlocks, step, A.active);
     QQ_CK(cudaGetLastError());
   }
   return QQ_OK;
 }
 
-// Full-lattice FP64 residual ||b - M x|| / ||b|| of the unpreconditioned operator
-// M = (1 + 2 i kappa mu gamma5) - kappa H on both parities (the system fermprop
-// solves, Q/diracops.f90:10-40).
+// mode 0: block[k] = x ; 1: x += block[k] ; 2: block[k] = 0
+int block_slot(qq_ctx* c, int prec, int nb, int k, Spinor blockf, Spinor x, int mode) {
+  count_launch();
+  if (prec == P32)
+    block_slot_kernel<P32><<<kRedBlocks, kRedThreads, 0, c->st>>>(c->g.vh, nb, k, blockf, x, mode);
+  else if (prec == P16)
+    block_slot_kernel<P16><<<kRedBlocks, kRedThreads, 0, c->st>>>(c->g.vh, nb, k, blockf, x, mode);
+  else
+    block_slot_kernel<P64><<<kRedBlocks, kRedThreads, 0, c->st>>>(c->g.vh, nb, k, blockf, x, mode);
+  QQ_CK(cudaGetLastError());
+  return QQ_OK;
+}
+
 int full_residual(qq_ctx* c, Spinor be, Spinor bo, Spinor xe, Spinor xo, const double kappa[2],
                   double* rel) {
   Tmp h(c, P64), m(c, P64);
@@ -98,138 +105,117 @@ int full_residual(qq_ctx* c, Spinor be, Spinor bo, Spinor xe, Spinor xo, const d
 
 }  // namespace
 
-// Deflated mixed-precision BiCGStab on a set of right-hand sides (all active at once).
-int bicgstab_mixed_batch(qq_ctx* c, std::vector<PerRhs*>& rhs, int prec, double tol, double delta,
-                         int maxiter, const double kappa[2], const DeflSpace* defl,
-                         std::vector<SolveStats>& stats) {
-  const int n = (int)rhs.size();
-  if (n == 0) return QQ_OK;
-  if (n > kMaxBatch) return set_error(QQ_BAD_ARG, "too many right-hand sides in one block");
+// BiCGStab on a block of right-hand sides in precision `prec` (block fields), FP64
+// reliable updates (Sleijpen & van der Vorst): when ||r|| has dropped by `delta` since
+// the last update, x64 += x_low, the FP64 true residual replaces the iterated one
+// (projected onto the deflation space first, if any) and the iteration continues with
+// the same search direction.
+int bicgstab_block(qq_ctx* c, std::vector<PerRhs*>& rhs, int prec, double tol, double delta,
+                   int maxiter, const double kappa[2], const DeflSpace* defl,
+                   std::vector<SolveStats>& stats) {
+  const int nb = (int)rhs.size();
+  if (nb == 0) return QQ_OK;
+  if (nb > kMaxBatch) return set_error(QQ_BAD_ARG, "too many right-hand sides in one block");
+  Field r, rhat, p, v, t, xl, tmp;
+  for (Field* f : {&r, &rhat, &p, &v, &t, &xl, &tmp}) {
+    QQ_TRY(alloc_field(c, *f, prec, nb));
+    QQ_CK(cudaMemsetAsync(f->data.p, 0, f->data.bytes, c->st));
+    if (prec == P16) QQ_CK(cudaMemsetAsync(f->norm.p, 0, f->norm.bytes, c->st));
+  }
   DevBuf S, part, dslots;
   QQ_CK(S.alloc(sizeof(double) * kScal * kMaxBatch));
   QQ_CK(part.alloc(sizeof(double) * 3 * kRedBlocks * kMaxBatch));
   QQ_CK(dslots.alloc(sizeof(int) * kMaxBatch));
-  Tmp tmp64(c, P64);
+  Tmp tmp64(c, P64), h(c, P64);
+  double* s1 = c->scal.as<double>();
+  // FP64 residual of x (and of the deflated x) -> slot k of r and rhat
+  auto true_res = [&](PerRhs& R, SolveStats& st) -> int {
+    QQ_TRY(op_dbletm(c, h.sp(), R.x.sp(), tmp64.sp(), 0, kappa));
+    QQ_TRY(lin(c, R.r64.sp(), cimm(1.0), R.b.sp(), cimm(-1.0), h.sp(), cimm(0), Spinor{nullptr, nullptr, P64}, s1));
+    double n2;
+    QQ_TRY(read_scalars(c, s1, 1, &n2));
+    R.rn = std::sqrt(n2);
+    st.mvp += 1;
+    if (defl && defl->k > 0 && R.rn / R.bn > tol) {
+      QQ_TRY(defl_project(c, *defl, R.b.sp(), R.x.sp(), R.r64.sp(), kappa, &R.rn));
+      st.mvp += 1;
+    }
+    return QQ_OK;
+  };
   std::vector<double> hS(kScal * kMaxBatch, 0.0);
-  for (int i = 0; i < n; ++i) {
-    PerRhs& R = *rhs[i];
-    R.slot = i;
+  std::vector<int> slots(nb);
+  unsigned active = 0;
+  for (int k = 0; k < nb; ++k) {
+    PerRhs& R = *rhs[k];
+    slots[k] = k;
     QQ_TRY(norm2_host(c, R.b.sp(), &R.bn));
     R.bn = std::sqrt(R.bn);
-    // r = b - A x, then project onto the deflation space
-    {
-      Tmp h(c, P64);
-      QQ_TRY(op_dbletm(c, h.sp(), R.x.sp(), tmp64.sp(), 0, kappa));
-      double* s = c->scal.as<double>();
-      QQ_TRY(lin(c, R.r64.sp(), cimm(1.0), R.b.sp(), cimm(-1.0), h.sp(), cimm(0), Spinor{nullptr, nullptr, P64}, s));
-      double n2;
-      QQ_TRY(read_scalars(c, s, 1, &n2));
-      R.rn = std::sqrt(n2);
-      stats[i].mvp += 1;
-    }
-    if (defl && defl->k > 0) {
-      QQ_TRY(defl_project(c, *defl, R.b.sp(), R.x.sp(), R.r64.sp(), kappa, &R.rn));
-      stats[i].mvp += 1;
-    }
+    QQ_TRY(true_res(R, stats[k]));
     R.rmax = R.rn;
     R.done = !(R.bn > 0.0) || R.rn / R.bn <= tol;
-    QQ_TRY(lin(c, R.r.sp(), cimm(1.0), R.r64.sp()));
-    QQ_TRY(copy_field(c, R.rhat.sp(), R.r.sp()));
-    QQ_TRY(zero_field(c, R.p.sp()));
-    QQ_TRY(zero_field(c, R.v.sp()));
-    QQ_TRY(zero_field(c, R.xl.sp()));
-    double* s = &hS[(size_t)i * kScal];
-    s[SC_RHO] = s[SC_ALPHA] = s[SC_OMEGA] = 1.0;
-    s[SC_RHO + 1] = s[SC_ALPHA + 1] = s[SC_OMEGA + 1] = 0.0;
-    stats[i].true_rel = R.bn > 0.0 ? R.rn / R.bn : 0.0;
+    stats[k].true_rel = R.bn > 0.0 ? R.rn / R.bn : 0.0;
+    if (!R.done) active |= 1u << k;
+    QQ_TRY(block_slot(c, prec, nb, k, r.sp(), R.r64.sp(), 0));
+    QQ_TRY(block_slot(c, prec, nb, k, rhat.sp(), R.r64.sp(), 0));
+    double* sc = &hS[(size_t)k * kScal];
+    sc[SC_RHO] = sc[SC_ALPHA] = sc[SC_OMEGA] = 1.0;
   }
   QQ_CK(cudaMemcpyAsync(S.p, hS.data(), sizeof(double) * hS.size(), cudaMemcpyHostToDevice, c->st));
+  QQ_CK(cudaMemcpyAsync(dslots.p, slots.data(), sizeof(int) * nb, cudaMemcpyHostToDevice, c->st));
   QQ_CK(cudaStreamSynchronize(c->st));
-  std::vector<double> r2(kMaxBatch);
-  for (int it = 0; it < maxiter; ++it) {
-    std::vector<PerRhs*> act;
-    for (auto* R : rhs)
-      if (!R->done) act.push_back(R);
-    if (act.empty()) break;
-    BatchArgs A;
-    std::memset(&A, 0, sizeof(A));
-    A.vh = c->g.vh;
-    A.n = (int)act.size();
-    A.S = S.as<double>();
-    A.partial = part.as<double>();
-    std::vector<int> slots(A.n);
-    std::vector<Spinor> pin(A.n), vout(A.n), rin(A.n), tout(A.n), tmpo(A.n);
-    for (int k = 0; k < A.n; ++k) {
-      PerRhs& R = *act[k];
-      A.r[k] = R.r.sp();
-      A.rhat[k] = R.rhat.sp();
-      A.p[k] = R.p.sp();
-      A.v[k] = R.v.sp();
-      A.t[k] = R.t.sp();
-      A.x[k] = R.xl.sp();
-      A.slot[k] = R.slot;
-      slots[k] = R.slot;
-      pin[k] = R.p.sp();
-      vout[k] = R.v.sp();
-      rin[k] = R.r.sp();
-      tout[k] = R.t.sp();
-      tmpo[k] = R.tmp.sp();
-    }
-    QQ_CK(cudaMemcpyAsync(dslots.p, slots.data(), sizeof(int) * A.n, cudaMemcpyHostToDevice, c->st));
-    const int* ds = dslots.as<int>();
-    QQ_TRY(bicg_op(c, prec, A, OP_DOT_RHAT_R, ds, ST_BETA));
-    QQ_TRY(bicg_op(c, prec, A, OP_P_UPDATE, ds, -1));
-    QQ_TRY(op_dbletm_multi(c, vout.data(), pin.data(), tmpo.data(), A.n, 0, kappa));
-    QQ_TRY(bicg_op(c, prec, A, OP_DOT_RHAT_V, ds, ST_ALPHA));
-    QQ_TRY(bicg_op(c, prec, A, OP_S_UPDATE, ds, -1));
-    QQ_TRY(op_dbletm_multi(c, tout.data(), rin.data(), tmpo.data(), A.n, 0, kappa));
-    QQ_TRY(bicg_op(c, prec, A, OP_DOTS_T, ds, ST_OMEGA));
-    QQ_TRY(bicg_op(c, prec, A, OP_XR_UPDATE, ds, ST_R2));
-    // read ||r||^2 of the active right-hand sides
-    QQ_CK(cudaMemcpyAsync(hS.data(), S.p, sizeof(double) * kScal * kMaxBatch, cudaMemcpyDeviceToHost, c->st));
+  BlockBiArgs A;
+  std::memset(&A, 0, sizeof(A));
+  A.vh = c->g.vh;
+  A.nb = nb;
+  A.r = r.sp();
+  A.rhat = rhat.sp();
+  A.p = p.sp();
+  A.v = v.sp();
+  A.t = t.sp();
+  A.x = xl.sp();
+  for (int k = 0; k < nb; ++k) A.slot[k] = k;
+  A.S = S.as<double>();
+  A.partial = part.as<double>();
+  const int* ds = dslots.as<int>();
+  for (int it = 0; it < maxiter && active; ++it) {
+    A.active = active;
+    QQ_TRY(block_op(c, prec, A, OP_DOT_RHAT_R, ds, ST_BETA));
+    QQ_TRY(block_op(c, prec, A, OP_P_UPDATE, ds, -1));
+    QQ_TRY(op_dbletm_block(c, v.sp(), p.sp(), tmp.sp(), nb, 0, kappa));
+    QQ_TRY(block_op(c, prec, A, OP_DOT_RHAT_V, ds, ST_ALPHA));
+    QQ_TRY(block_op(c, prec, A, OP_S_UPDATE, ds, -1));
+    QQ_TRY(op_dbletm_block(c, t.sp(), r.sp(), tmp.sp(), nb, 0, kappa));
+    QQ_TRY(block_op(c, prec, A, OP_DOTS_T, ds, ST_OMEGA));
+    QQ_TRY(block_op(c, prec, A, OP_XR_UPDATE, ds, ST_R2));
+    QQ_CK(cudaMemcpyAsync(hS.data(), S.p, sizeof(double) * kScal * nb, cudaMemcpyDeviceToHost, c->st));
     QQ_CK(cudaStreamSynchronize(c->st));
-    std::vector<PerRhs*> upd;
-    for (auto* R : act) {
-      SolveStats& stt = stats[std::find(rhs.begin(), rhs.end(), R) - rhs.begin()];
-      stt.itercount += 1;
-      stt.mvp += 2;
-      const double rn = std::sqrt(hS[(size_t)R->slot * kScal + SC_R2]);
+    for (int k = 0; k < nb; ++k) {
+      if (!((active >> k) & 1u)) continue;
+      PerRhs& R = *rhs[k];
+      SolveStats& st = stats[k];
+      st.itercount += 1;
+      st.mvp += 2;
+      const double rn = std::sqrt(hS[(size_t)k * kScal + SC_R2]);
       if (!std::isfinite(rn)) return set_error(QQ_NAN, "NaN residual in batched BiCGStab");
-      if (rn < delta * R->rmax || rn / R->bn < 0.5 * tol) upd.push_back(R);
-    }
-    // reliable updates: x64 += xl ; r64 = b - A x64 (FP64) ; r = r64
-    for (auto* R : upd) {
-      SolveStats& stt = stats[std::find(rhs.begin(), rhs.end(), R) - rhs.begin()];
-      QQ_TRY(lin(c, R->x.sp(), cimm(1.0), R->xl.sp(), cimm(1.0), R->x.sp()));
-      QQ_TRY(zero_field(c, R->xl.sp()));
-      Tmp h(c, P64);
-      QQ_TRY(op_dbletm(c, h.sp(), R->x.sp(), tmp64.sp(), 0, kappa));
-      double* s = c->scal.as<double>();
-      QQ_TRY(lin(c, R->r64.sp(), cimm(1.0), R->b.sp(), cimm(-1.0), h.sp(), cimm(0), Spinor{nullptr, nullptr, P64}, s));
-      double n2;
-      QQ_TRY(read_scalars(c, s, 1, &n2));
-      R->rn = std::sqrt(n2);
-      stt.mvp += 1;
-      if (defl && defl->k > 0 && R->rn / R->bn > tol) {
-        // re-deflate: the low modes the iteration has re-excited are removed exactly
-        QQ_TRY(defl_project(c, *defl, R->b.sp(), R->x.sp(), R->r64.sp(), kappa, &R->rn));
-        stt.mvp += 1;
-      }
-      stt.true_rel = R->rn / R->bn;
-      stt.hist.push_back(stt.true_rel);
-      stt.hist_mvp.push_back(stt.mvp);
-      if (R->rn / R->bn <= tol) {
-        R->done = true;
+      if (!(rn < delta * R.rmax || rn / R.bn < 0.5 * tol)) continue;
+      // reliable update
+      QQ_TRY(block_slot(c, prec, nb, k, xl.sp(), R.x.sp(), 1));
+      QQ_TRY(block_slot(c, prec, nb, k, xl.sp(), R.x.sp(), 2));
+      QQ_TRY(true_res(R, st));
+      st.true_rel = R.rn / R.bn;
+      st.hist.push_back(st.true_rel);
+      st.hist_mvp.push_back(st.mvp);
+      if (R.rn / R.bn <= tol) {
+        R.done = true;
+        active &= ~(1u << k);
         continue;
       }
-      QQ_TRY(lin(c, R->r.sp(), cimm(1.0), R->r64.sp()));
-      R->rmax = R->rn;
+      QQ_TRY(block_slot(c, prec, nb, k, r.sp(), R.r64.sp(), 0));
+      R.rmax = R.rn;
     }
   }
-  int status = QQ_OK;
-  for (auto* R : rhs)
-    if (!R->done) status = QQ_NOT_CONVERGED;
-  return status;
+  QQ_CK(cudaStreamSynchronize(c->st));
+  return active ? QQ_NOT_CONVERGED : QQ_OK;
 }
 
 int batch_solve(qq_ctx* c, int nrhs, const double* be, const double* bo, const double kappa[2],
@@ -308,19 +294,9 @@ int batch_solve(qq_ctx* c, int nrhs, const double* be, const double* bo, const d
       const int nb = std::min(block, nrhs - i0);
       std::vector<PerRhs*> blk;
       std::vector<SolveStats> bst(nb);
-      for (int k = 0; k < nb; ++k) {
-        PerRhs& r = *R[i0 + k];
-        QQ_TRY(alloc_field(c, r.r, prec));
-        QQ_TRY(alloc_field(c, r.rhat, prec));
-        QQ_TRY(alloc_field(c, r.p, prec));
-        QQ_TRY(alloc_field(c, r.v, prec));
-        QQ_TRY(alloc_field(c, r.t, prec));
-        QQ_TRY(alloc_field(c, r.xl, prec));
-        QQ_TRY(alloc_field(c, r.tmp, prec));
-        blk.push_back(&r);
-      }
+      for (int k = 0; k < nb; ++k) blk.push_back(R[i0 + k].get());
       tic();
-      const int st = bicgstab_mixed_batch(c, blk, prec, tol_even, 0.1, maxiter, kappa,
+      const int st = bicgstab_block(c, blk, prec, tol_even, 0.1, maxiter, kappa,
                                           defl.k > 0 ? &defl : nullptr, bst);
       const double sec = toc();
       for (int k = 0; k < nb; ++k) {

@@ -134,6 +134,10 @@ int op_hsingle_multi(qq_ctx* c, const Spinor* out, const Spinor* in, int n, int 
 int op_dbletm(qq_ctx* c, Spinor out, Spinor in, Spinor tmp, int idag, const double kappa[2]);
 int op_dbletm_multi(qq_ctx* c, const Spinor* out, const Spinor* in, const Spinor* tmp, int n,
                     int idag, const double kappa[2]);
+// RHS-interleaved block fields of nb right-hand sides (element (q, s, r) at
+// q * (vh * nb) + s * nb + r); one launch pair for the whole block.
+int op_dbletm_block(qq_ctx* c, Spinor out, Spinor in, Spinor tmp, int nb, int idag,
+                    const double kappa[2]);
 int lin(qq_ctx* c, Spinor out, Coef a, Spinor x, Coef b = cimm(0), Spinor y = Spinor{nullptr, nullptr, P64},
         Coef cc = cimm(0), Spinor z = Spinor{nullptr, nullptr, P64}, double* nrm2_dev = nullptr);
 int dot_dev(qq_ctx* c, Spinor x, Spinor y, double* out3);  // out3 = {re, im, |y|^2}

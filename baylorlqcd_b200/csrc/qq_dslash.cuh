@@ -30,6 +30,13 @@ struct HopArgs {
   HopCoef c;
   int pout;                    // output parity (0 = gblclr 1, 1 = gblclr 2)
   int nrhs;
+  int blk;                     // 1: in/out/aux[0] are RHS-interleaved block fields of nrhs
+                               //    right-hand sides: element (plane q, site s, rhs r) at
+                               //    q * (vh * nrhs) + s * nrhs + r
+  __device__ const void* in_base(int r) const { return blk ? in[0] : in[r]; }
+  __device__ const float* in_nrm(int r) const { return blk ? in_norm[0] : in_norm[r]; }
+  __device__ int vh_of() const { return blk ? g.vh * nrhs : g.vh; }
+  __device__ int idx_of(int s, int r) const { return blk ? s * nrhs + r : s; }
   const void* gauge;
   const void* in[kMaxRhs];
   const float* in_norm[kMaxRhs];
@@ -156,7 +163,7 @@ __device__ inline void hop(const HopArgs& a, int s, int r, const int* x, cplx<R>
   else
     LIO::load(a.gauge, a.g.vh, 1 - a.pout, MU, sy, u);
   cplx<R> psi[12];
-  SIO::load(a.in[r], a.in_norm[r], a.g.vh, sy, psi);
+  SIO::load(a.in_base(r), a.in_nrm(r), a.vh_of(), a.idx_of(sy, r), psi);
   cplx<R> h[6], w[6];
   if (cm != (R)0) {
     project<MU, -1>(psi, cm, h);
@@ -249,7 +256,8 @@ __global__ void __launch_bounds__(128) hop_kernel(HopArgs a) {
     }
   } else {
     cplx<R> gg[12];
-    SIO::load(a.aux[r], a.aux_norm[r], a.g.vh, s, gg);
+    SIO::load(a.blk ? a.aux[0] : a.aux[r], a.blk ? a.aux_norm[0] : a.aux_norm[r], a.vh_of(),
+              a.idx_of(s, r), gg);
     const R f1 = (R)a.f1, f2 = (R)a.f2, f3 = (R)a.f3;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
@@ -259,7 +267,8 @@ __global__ void __launch_bounds__(128) hop_kernel(HopArgs a) {
       o[9 + c] = csub(csub(cscale(f1, gg[9 + c]), cscale(f2, gg[3 + c])), cscale(f3, acc[9 + c]));
     }
   }
-  SIO::store(a.out[r], a.out_norm[r], a.g.vh, s, o);
+  SIO::store(a.blk ? a.out[0] : a.out[r], a.blk ? a.out_norm[0] : a.out_norm[r], a.vh_of(),
+             a.idx_of(s, r), o);
 }
 
 // ---------------------------------------------------------------------------
@@ -387,10 +396,11 @@ __device__ inline void stage_hop(const HopArgs& a, uint4* slots, int T, int s, i
   const int sy = neighbour<MU, FWD>(a.g, x, &sgn);
   if (sgn == 0) return;
   uint4* dst = slots + (size_t)H * Sh::NQ * T;
-  const uint4* sp = static_cast<const uint4*>(a.in[r]);
+  const uint4* sp = static_cast<const uint4*>(a.in_base(r));
+  const int vhe = a.vh_of(), iy = a.idx_of(sy, r);
 #pragma unroll
-  for (int q = 0; q < SpinorIO<SP>::planes; ++q) cp_async16(dst + q * T, sp + (size_t)q * a.g.vh + sy);
-  if (SP == P16) cp_async4(dst + SpinorIO<SP>::planes * T, a.in_norm[r] + sy);
+  for (int q = 0; q < SpinorIO<SP>::planes; ++q) cp_async16(dst + q * T, sp + (size_t)q * vhe + iy);
+  if (SP == P16) cp_async4(dst + SpinorIO<SP>::planes * T, a.in_nrm(r) + iy);
   const int lp = FWD ? a.pout : 1 - a.pout;
   const int ls = FWD ? s : sy;
   const uint4* lk = static_cast<const uint4*>(a.gauge) + (size_t)(lp * 4 + MU) * Sh::LQ * a.g.vh;
@@ -457,7 +467,8 @@ __device__ inline void hop_epilogue(const HopArgs& a, int EPI, int s, int r, con
     }
   } else {
     cplx<R> gg[12];
-    SIO::load(a.aux[r], a.aux_norm[r], a.g.vh, s, gg);
+    SIO::load(a.blk ? a.aux[0] : a.aux[r], a.blk ? a.aux_norm[0] : a.aux_norm[r], a.vh_of(),
+              a.idx_of(s, r), gg);
     const R f1 = (R)a.f1, f2 = (R)a.f2, f3 = (R)a.f3;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
@@ -467,7 +478,8 @@ __device__ inline void hop_epilogue(const HopArgs& a, int EPI, int s, int r, con
       o[9 + c] = csub(csub(cscale(f1, gg[9 + c]), cscale(f2, gg[3 + c])), cscale(f3, acc[9 + c]));
     }
   }
-  SIO::store(a.out[r], a.out_norm[r], a.g.vh, s, o);
+  SIO::store(a.blk ? a.out[0] : a.out[r], a.blk ? a.out_norm[0] : a.out_norm[r], a.vh_of(),
+             a.idx_of(s, r), o);
 }
 
 // blockDim.x = T threads = (T / nrhs) sites x nrhs right-hand sides; dynamic shared

@@ -1,8 +1,11 @@
-// Batched (multi right-hand side) BiCGStab building blocks.
+// Batched (multi right-hand side) BiCGStab building blocks on RHS-interleaved block
+// fields: a block of nb right-hand sides is one spinor field of vh * nb "sites",
+// element (plane q, site s, rhs r) at q * (vh * nb) + s * nb + r, so a warp reads
+// contiguous 16-byte runs across right-hand sides and sites.
 //
-// One launch updates every active right-hand side (blockIdx.y = RHS slot); each RHS
-// keeps its own complex scalars in device memory, so an iteration needs no host round
-// trip.  Reductions are deterministic: per-block partials, then one block per RHS sums
+// One launch updates every right-hand side of the block; each keeps its own complex
+// scalars in device memory, so an iteration needs no host round trip.  Reductions are
+// deterministic: per-block partials per right-hand side, then one block per RHS sums
 // them in a fixed order inside the scalar kernel that consumes them.
 #pragma once
 #include "qq_blas.cuh"
@@ -31,13 +34,14 @@ enum BiOp : int {
   OP_XR_UPDATE = 5,   // x += alpha p + omega r ; r -= omega t ; red: ||r||^2
 };
 
-struct BatchArgs {
-  int vh;
-  int n;                       // active right-hand sides
-  Spinor r[kMaxBatch], rhat[kMaxBatch], p[kMaxBatch], v[kMaxBatch], t[kMaxBatch], x[kMaxBatch];
-  int slot[kMaxBatch];         // scalar slot of each active RHS
+struct BlockBiArgs {
+  int vh;                      // sites per parity
+  int nb;                      // right-hand sides in the block
+  unsigned active;             // bit r set: right-hand side r still iterates
+  Spinor r, rhat, p, v, t, x;  // block fields
+  int slot[kMaxBatch];         // scalar slot of each right-hand side
   double* S;                   // scalar array
-  double* partial;             // [rhs][kRedBlocks][3]
+  double* partial;             // [rhs][gridDim.x][3]
 };
 
 template <class R>
@@ -45,50 +49,51 @@ __device__ inline cplx<R> cmuld(cplx<double> a, cplx<R> b) {
   return {(R)(a.re * b.re - a.im * b.im), (R)(a.re * b.im + a.im * b.re)};
 }
 
-// x, r, p, ... of one precision P (P32 or P16; P64 for testing)
+// blockDim.x is a multiple of nb and so is the grid stride, hence every thread keeps
+// one right-hand side k = threadIdx.x % nb for its whole loop.
 template <int P, int OP>
-__global__ void __launch_bounds__(kRedThreads) bicg_kernel(BatchArgs A) {
+__global__ void __launch_bounds__(kRedThreads) bicg_block_kernel(BlockBiArgs A) {
   using IO = SpinorIO<P>;
   using R = typename IO::R;
-  const int k = blockIdx.y;
+  const int k = threadIdx.x % A.nb;
+  const bool act = (A.active >> k) & 1u;
   const double* S = A.S + (size_t)A.slot[k] * kScal;
   double acc[3] = {0.0, 0.0, 0.0};
-  cplx<double> alpha{S[SC_ALPHA], S[SC_ALPHA + 1]}, omega{S[SC_OMEGA], S[SC_OMEGA + 1]},
+  const cplx<double> alpha{S[SC_ALPHA], S[SC_ALPHA + 1]}, omega{S[SC_OMEGA], S[SC_OMEGA + 1]},
       beta{S[SC_BETA], S[SC_BETA + 1]};
   const cplx<double> bo = {beta.re * omega.re - beta.im * omega.im, beta.re * omega.im + beta.im * omega.re};
-  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < A.vh; s += gridDim.x * blockDim.x) {
+  const int n = A.vh * A.nb;
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
     cplx<R> a[12], b[12], c[12];
     if (OP == OP_DOT_RHAT_R || OP == OP_DOT_RHAT_V) {
-      IO::load(A.rhat[k].data, A.rhat[k].norm, A.vh, s, a);
+      IO::load(A.rhat.data, A.rhat.norm, n, s, a);
       if (OP == OP_DOT_RHAT_R)
-        IO::load(A.r[k].data, A.r[k].norm, A.vh, s, b);
+        IO::load(A.r.data, A.r.norm, n, s, b);
       else
-        IO::load(A.v[k].data, A.v[k].norm, A.vh, s, b);
+        IO::load(A.v.data, A.v.norm, n, s, b);
 #pragma unroll
       for (int q = 0; q < 12; ++q) {
         acc[0] += (double)a[q].re * b[q].re + (double)a[q].im * b[q].im;
         acc[1] += (double)a[q].re * b[q].im - (double)a[q].im * b[q].re;
       }
     } else if (OP == OP_P_UPDATE) {
-      IO::load(A.r[k].data, A.r[k].norm, A.vh, s, a);
-      IO::load(A.p[k].data, A.p[k].norm, A.vh, s, b);
-      IO::load(A.v[k].data, A.v[k].norm, A.vh, s, c);
+      if (!act) continue;
+      IO::load(A.r.data, A.r.norm, n, s, a);
+      IO::load(A.p.data, A.p.norm, n, s, b);
+      IO::load(A.v.data, A.v.norm, n, s, c);
 #pragma unroll
-      for (int q = 0; q < 12; ++q) {
-        const cplx<R> t1 = cmuld(beta, b[q]);
-        const cplx<R> t2 = cmuld(bo, c[q]);
-        a[q] = csub(cadd(a[q], t1), t2);
-      }
-      IO::store(A.p[k].data, A.p[k].norm, A.vh, s, a);
+      for (int q = 0; q < 12; ++q) a[q] = csub(cadd(a[q], cmuld(beta, b[q])), cmuld(bo, c[q]));
+      IO::store(A.p.data, A.p.norm, n, s, a);
     } else if (OP == OP_S_UPDATE) {
-      IO::load(A.r[k].data, A.r[k].norm, A.vh, s, a);
-      IO::load(A.v[k].data, A.v[k].norm, A.vh, s, b);
+      if (!act) continue;
+      IO::load(A.r.data, A.r.norm, n, s, a);
+      IO::load(A.v.data, A.v.norm, n, s, b);
 #pragma unroll
       for (int q = 0; q < 12; ++q) a[q] = csub(a[q], cmuld(alpha, b[q]));
-      IO::store(A.r[k].data, A.r[k].norm, A.vh, s, a);
+      IO::store(A.r.data, A.r.norm, n, s, a);
     } else if (OP == OP_DOTS_T) {
-      IO::load(A.t[k].data, A.t[k].norm, A.vh, s, a);
-      IO::load(A.r[k].data, A.r[k].norm, A.vh, s, b);
+      IO::load(A.t.data, A.t.norm, n, s, a);
+      IO::load(A.r.data, A.r.norm, n, s, b);
 #pragma unroll
       for (int q = 0; q < 12; ++q) {
         acc[0] += (double)a[q].re * b[q].re + (double)a[q].im * b[q].im;
@@ -96,36 +101,39 @@ __global__ void __launch_bounds__(kRedThreads) bicg_kernel(BatchArgs A) {
         acc[2] += (double)a[q].re * a[q].re + (double)a[q].im * a[q].im;
       }
     } else {  // OP_XR_UPDATE
-      IO::load(A.x[k].data, A.x[k].norm, A.vh, s, a);
-      IO::load(A.p[k].data, A.p[k].norm, A.vh, s, b);
-      IO::load(A.r[k].data, A.r[k].norm, A.vh, s, c);
+      IO::load(A.r.data, A.r.norm, n, s, c);
+      if (act) {
+        IO::load(A.x.data, A.x.norm, n, s, a);
+        IO::load(A.p.data, A.p.norm, n, s, b);
 #pragma unroll
-      for (int q = 0; q < 12; ++q) a[q] = cadd(a[q], cadd(cmuld(alpha, b[q]), cmuld(omega, c[q])));
-      IO::store(A.x[k].data, A.x[k].norm, A.vh, s, a);
-      IO::load(A.t[k].data, A.t[k].norm, A.vh, s, b);
+        for (int q = 0; q < 12; ++q) a[q] = cadd(a[q], cadd(cmuld(alpha, b[q]), cmuld(omega, c[q])));
+        IO::store(A.x.data, A.x.norm, n, s, a);
+        IO::load(A.t.data, A.t.norm, n, s, b);
 #pragma unroll
-      for (int q = 0; q < 12; ++q) c[q] = csub(c[q], cmuld(omega, b[q]));
-      IO::store(A.r[k].data, A.r[k].norm, A.vh, s, c);
-      if (P == P16) IO::load(A.r[k].data, A.r[k].norm, A.vh, s, c);  // reduce what was stored
+        for (int q = 0; q < 12; ++q) c[q] = csub(c[q], cmuld(omega, b[q]));
+        IO::store(A.r.data, A.r.norm, n, s, c);
+        if (P == P16) IO::load(A.r.data, A.r.norm, n, s, c);  // reduce what was stored
+      }
 #pragma unroll
       for (int q = 0; q < 12; ++q) acc[0] += (double)c[q].re * c[q].re + (double)c[q].im * c[q].im;
     }
   }
   if (OP == OP_DOT_RHAT_R || OP == OP_DOT_RHAT_V || OP == OP_DOTS_T || OP == OP_XR_UPDATE) {
-    __shared__ double red[3][kRedThreads / 32];
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    __shared__ double red[3][kRedThreads];
 #pragma unroll
-    for (int q = 0; q < 3; ++q) {
-      double v = acc[q];
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-      if (lane == 0) red[q][wid] = v;
-    }
+    for (int q = 0; q < 3; ++q) red[q][threadIdx.x] = acc[q];
     __syncthreads();
-    if (threadIdx.x < 3) {
-      double sum = 0.0;
-      for (int w = 0; w < kRedThreads / 32; ++w) sum += red[threadIdx.x][w];
-      A.partial[((size_t)k * gridDim.x + blockIdx.x) * 3 + threadIdx.x] = sum;
+    if (threadIdx.x < A.nb) {
+      double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+      for (int j = threadIdx.x; j < blockDim.x; j += A.nb) {
+        s0 += red[0][j];
+        s1 += red[1][j];
+        s2 += red[2][j];
+      }
+      double* dst = A.partial + ((size_t)threadIdx.x * gridDim.x + blockIdx.x) * 3;
+      dst[0] = s0;
+      dst[1] = s1;
+      dst[2] = s2;
     }
   }
 }
@@ -137,9 +145,9 @@ enum ScalStep : int {
   ST_R2 = 3,     // ||r||^2
 };
 
-// one block per RHS: sum the partials (fixed order) and update the scalars
-static __global__ void bicg_scalar_kernel(double* S, const int* slots, const double* partial, int nblocks,
-                                   int step) {
+// one block per right-hand side: sum the partials (fixed order), update the scalars
+static __global__ void bicg_scalar_kernel(double* S, const int* slots, const double* partial,
+                                          int nblocks, int step, unsigned active) {
   const int k = blockIdx.x;
   __shared__ double red[3][256];
   double a[3] = {0.0, 0.0, 0.0};
@@ -152,7 +160,7 @@ static __global__ void bicg_scalar_kernel(double* S, const int* slots, const dou
       for (int q = 0; q < 3; ++q) red[q][threadIdx.x] += red[q][threadIdx.x + o];
     __syncthreads();
   }
-  if (threadIdx.x != 0) return;
+  if (threadIdx.x != 0 || !((active >> k) & 1u)) return;
   double* s = S + (size_t)slots[k] * kScal;
   const double d0 = red[0][0], d1 = red[1][0], d2 = red[2][0];
   auto cdiv = [](double ar, double ai, double br, double bi, double* cr, double* ci) {
@@ -162,7 +170,7 @@ static __global__ void bicg_scalar_kernel(double* S, const int* slots, const dou
   };
   if (step == ST_BETA) {
     double qr, qi, pr, pi;
-    cdiv(d0, d1, s[SC_RHO], s[SC_RHO + 1], &qr, &qi);               // rho'/rho
+    cdiv(d0, d1, s[SC_RHO], s[SC_RHO + 1], &qr, &qi);                           // rho'/rho
     cdiv(s[SC_ALPHA], s[SC_ALPHA + 1], s[SC_OMEGA], s[SC_OMEGA + 1], &pr, &pi);  // alpha/omega
     s[SC_BETA] = qr * pr - qi * pi;
     s[SC_BETA + 1] = qr * pi + qi * pr;
@@ -176,6 +184,36 @@ static __global__ void bicg_scalar_kernel(double* S, const int* slots, const dou
     s[SC_TT] = d2;
   } else {
     s[SC_R2] = d0;
+  }
+}
+
+// Slot k of a block field <-> a separate FP64 field.
+//   mode 0: block[k] = x (rounded to the block precision)   mode 1: x += block[k]
+//   mode 2: block[k] = 0
+template <int P>
+__global__ void block_slot_kernel(int vh, int nb, int k, Spinor blockf, Spinor x, int mode) {
+  using RB = typename SpinorIO<P>::R;
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < vh; s += gridDim.x * blockDim.x) {
+    const int e = s * nb + k, n = vh * nb;
+    cplx<RB> b[12];
+    if (mode == 2) {
+#pragma unroll
+      for (int q = 0; q < 12; ++q) b[q] = {(RB)0, (RB)0};
+      SpinorIO<P>::store(blockf.data, blockf.norm, n, e, b);
+    } else if (mode == 0) {
+      cplx<double> v[12];
+      SpinorIO<P64>::load(x.data, x.norm, vh, s, v);
+#pragma unroll
+      for (int q = 0; q < 12; ++q) b[q] = {(RB)v[q].re, (RB)v[q].im};
+      SpinorIO<P>::store(blockf.data, blockf.norm, n, e, b);
+    } else {
+      cplx<double> v[12];
+      SpinorIO<P64>::load(x.data, x.norm, vh, s, v);
+      SpinorIO<P>::load(blockf.data, blockf.norm, n, e, b);
+#pragma unroll
+      for (int q = 0; q < 12; ++q) v[q] = {v[q].re + (double)b[q].re, v[q].im + (double)b[q].im};
+      SpinorIO<P64>::store(x.data, x.norm, vh, s, v);
+    }
   }
 }
 

@@ -140,7 +140,7 @@ static int launch_hop_profiled(qq_ctx* c, const HopArgs& a, int prec, int recon,
 
 int launch_hop_tuned(qq_ctx* c, const HopArgs& a, int prec, int epi) {
   const int recon = recon_of(c, prec);
-  const int key = ((prec * 64 + recon) * 16 + a.nrhs) * 4 + epi;
+  const int key = (((prec * 64 + recon) * 64 + a.nrhs) * 4 + epi) * 2 + a.blk;
   auto it = c->hop_tune.find(key);
   if (it != c->hop_tune.end()) return launch_hop_profiled(c, a, prec, recon, epi, it->second);
   if (c->forced_tps > 0) {
@@ -233,6 +233,43 @@ int op_dbletm_multi(qq_ctx* c, const Spinor* out, const Spinor* in, const Spinor
     QQ_TRY(launch_hop_tuned(c, b, prec, EPI_DBLE));
   }
   return QQ_OK;
+}
+
+// Hdbletm on RHS-interleaved block fields of nb right-hand sides (one launch pair).
+int op_dbletm_block(qq_ctx* c, Spinor out, Spinor in, Spinor tmp, int nb, int idag,
+                    const double kappa[2]) {
+  if (!c->have_gauge) return set_error(QQ_BAD_ARG, "no gauge field uploaded");
+  if (nb < 1 || nb > 32) return set_error(QQ_BAD_ARG, "block of 1..32 right-hand sides");
+  const int prec = in.prec;
+  const bool wilson = kappa[1] < 0.00000001;  // Q/diracops.f90:467
+  HopArgs a = hop_base(c, idag, 1, prec);
+  a.nrhs = nb;
+  a.blk = 1;
+  a.in[0] = in.data;
+  a.in_norm[0] = in.norm;
+  a.out[0] = tmp.data;
+  a.out_norm[0] = tmp.norm;
+  a.a = 2.0 * kappa[0] * kappa[1];
+  QQ_TRY(launch_hop_tuned(c, a, prec, wilson ? EPI_STORE : EPI_TWIST));
+  HopArgs b = hop_base(c, idag, 0, prec);
+  b.nrhs = nb;
+  b.blk = 1;
+  b.in[0] = tmp.data;
+  b.in_norm[0] = tmp.norm;
+  b.out[0] = out.data;
+  b.out_norm[0] = out.norm;
+  b.aux[0] = in.data;
+  b.aux_norm[0] = in.norm;
+  b.f1 = 1.0 / (kappa[0] * kappa[0]);
+  if (wilson) {
+    b.f2 = 0.0;
+    b.f3 = 1.0;
+  } else {
+    const double t = 2.0 * kappa[0] * kappa[1];
+    b.f2 = 2.0 * kappa[1] / kappa[0];
+    b.f3 = 1.0 / (1.0 + t * t);
+  }
+  return launch_hop_tuned(c, b, prec, EPI_DBLE);
 }
 
 int op_dbletm(qq_ctx* c, Spinor out, Spinor in, Spinor tmp, int idag, const double kappa[2]) {

@@ -451,25 +451,35 @@ extern "C" int qq_bench_hsingle(qq_ctx* c, int precision, int nrhs, int tps, int
   QQ_TRY(set_device(c));
   if (!c->have_gauge) return set_error(QQ_BAD_ARG, "no gauge field uploaded");
   const int prec = precision == 64 ? P64 : precision == 32 ? P32 : precision == 16 ? P16 : -1;
-  if (prec < 0 || nrhs < 1 || nrhs > kMaxRhs || niter < 1 || tps < 0 || tps > 128)
+  if (prec < 0 || nrhs < 1 || nrhs > kMaxBatch || niter < 1 || tps < 0 || tps > 128)
     return set_error(QQ_BAD_ARG, "bad benchmark arguments");
   const int vh = c->g.vh;
-  std::vector<std::unique_ptr<Field>> in(nrhs), out(nrhs);
-  for (int r = 0; r < nrhs; ++r) {
-    in[r].reset(new Field());
-    out[r].reset(new Field());
-    in[r]->prec = out[r]->prec = prec;
-    QQ_CK(in[r]->data.alloc(field_bytes(prec, vh)));
-    QQ_CK(out[r]->data.alloc(field_bytes(prec, vh)));
-    if (prec == P16) {
-      QQ_CK(in[r]->norm.alloc(sizeof(float) * vh));
-      QQ_CK(out[r]->norm.alloc(sizeof(float) * vh));
-    }
-    // random FP64 content converted to the target precision
-    Tmp t(c, P64);
-    fill_kernel<<<592, 256, 0, c->st>>>(static_cast<double2*>(t.f->data.p), (size_t)12 * vh, 17u + r);
+  // nrhs > 1: one RHS-interleaved block field of nrhs right-hand sides (the layout of
+  // the batched solver), random FP64 content converted to the target precision
+  Field in, out;
+  in.prec = out.prec = prec;
+  QQ_CK(in.data.alloc(field_bytes(prec, vh) * nrhs));
+  QQ_CK(out.data.alloc(field_bytes(prec, vh) * nrhs));
+  if (prec == P16) {
+    QQ_CK(in.norm.alloc(sizeof(float) * vh * nrhs));
+    QQ_CK(out.norm.alloc(sizeof(float) * vh * nrhs));
+  }
+  {
+    Field t;
+    t.prec = P64;
+    QQ_CK(t.data.alloc(field_bytes(P64, vh) * nrhs));
+    fill_kernel<<<592, 256, 0, c->st>>>(static_cast<double2*>(t.data.p), (size_t)12 * vh * nrhs, 17u);
     QQ_CK(cudaGetLastError());
-    QQ_TRY(copy_field(c, in[r]->sp(), t.sp()));
+    LinArgs L;
+    std::memset(&L, 0, sizeof(L));
+    L.vh = vh * nrhs;  // a block field is a field of vh * nrhs sites
+    L.x = t.sp();
+    L.y = L.z = Spinor{nullptr, nullptr, P64};
+    L.out = in.sp();
+    L.a = cimm(1.0);
+    L.b = L.c = cimm(0.0);
+    QQ_CK(launch_lincomb(L, P64, P64, P64, prec, c->st));
+    QQ_CK(cudaStreamSynchronize(c->st));
   }
   DevBuf flush;
   const size_t flush_bytes = (size_t)512 << 20;
@@ -481,16 +491,15 @@ extern "C" int qq_bench_hsingle(qq_ctx* c, int precision, int nrhs, int tps, int
   a.pout = 1;
   a.gauge = prec == P64 ? c->gauge64.p : c->gauge32.p;
   a.nrhs = nrhs;
-  for (int r = 0; r < nrhs; ++r) {
-    a.in[r] = in[r]->data.p;
-    a.in_norm[r] = in[r]->norm.as<float>();
-    a.out[r] = out[r]->data.p;
-    a.out_norm[r] = out[r]->norm.as<float>();
-  }
+  a.blk = nrhs > 1 ? 1 : 0;
+  a.in[0] = in.data.p;
+  a.in_norm[0] = in.norm.as<float>();
+  a.out[0] = out.data.p;
+  a.out_norm[0] = out.norm.as<float>();
   const int recon = prec == P64 ? c->recon64 : 12;
   if (tps == 0) {  // the autotuned choice the solvers use
     QQ_TRY(launch_hop_tuned(c, a, prec, EPI_STORE));
-    tps = c->hop_tune[((prec * 64 + recon) * 16 + nrhs) * 4 + EPI_STORE];
+    tps = c->hop_tune.at(hop_tune_key(c, a, prec, EPI_STORE));
   }
   for (int w = 0; w < 3; ++w) QQ_CK(launch_hop(a, prec, recon, EPI_STORE, tps, c->st));
   double total = 0.0;

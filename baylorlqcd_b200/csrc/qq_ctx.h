@@ -128,6 +128,8 @@ struct Tmp {
 
 // ---- operator and level-1 helpers (qq_ops.cu) ----
 int launch_hop_tuned(qq_ctx* c, const HopArgs& a, int prec, int epi);
+// Key of the autotuner's table (c->hop_tune) for this launch shape.
+int hop_tune_key(qq_ctx* c, const HopArgs& a, int prec, int epi);
 int op_hsingle(qq_ctx* c, Spinor out, Spinor in, int idag, int pout);
 int op_hsingle_multi(qq_ctx* c, const Spinor* out, const Spinor* in, int n, int idag, int pout);
 // he = Hdbletm(ge), tmp is an odd-parity temporary of the same precision.

@@ -23,7 +23,8 @@ enum Epilogue : int {
   EPI_DBLE = 2,   // out = f1*g + f2*J(g) - f3 * H in      (Hdbletm :496-514, Hdouble :340-343)
 };
 
-constexpr int kMaxRhs = 8;  // right-hand sides per launch
+constexpr int kMaxRhs = 8;     // right-hand sides per launch, separate fields
+constexpr int kMaxBatch = 32;  // right-hand sides per launch, one block field
 
 struct HopArgs {
   Geom g;

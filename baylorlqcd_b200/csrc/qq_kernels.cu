@@ -70,7 +70,7 @@ static cudaError_t hop_tps(const HopArgs& a, int epi, int tps, cudaStream_t st) 
 cudaError_t launch_hop(const HopArgs& a, int sp, int recon, int epi, int tps, cudaStream_t st) {
   count_launch();
   const int per = tps <= 4 ? 128 / tps : tps;
-  const int maxr = a.blk ? 32 : kMaxRhs;
+  const int maxr = a.blk ? kMaxBatch : kMaxRhs;
   if (a.nrhs < 1 || a.nrhs > maxr || a.nrhs > per) return cudaErrorInvalidValue;
   if (sp == P64) {
     if (recon == 18) return hop_tps<P64, P64, 18>(a, epi, tps, st);

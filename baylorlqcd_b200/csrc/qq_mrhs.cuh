@@ -12,8 +12,6 @@
 
 namespace qq {
 
-constexpr int kMaxBatch = 32;
-
 // per-RHS scalar slots (doubles) in S[rhs * kScal + slot]
 enum ScalSlot : int {
   SC_RHO = 0,      // complex rho

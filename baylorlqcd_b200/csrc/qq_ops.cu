@@ -138,9 +138,13 @@ static int launch_hop_profiled(qq_ctx* c, const HopArgs& a, int prec, int recon,
   return QQ_OK;
 }
 
+int hop_tune_key(qq_ctx* c, const HopArgs& a, int prec, int epi) {
+  return (((prec * 64 + recon_of(c, prec)) * 64 + a.nrhs) * 4 + epi) * 2 + a.blk;
+}
+
 int launch_hop_tuned(qq_ctx* c, const HopArgs& a, int prec, int epi) {
   const int recon = recon_of(c, prec);
-  const int key = (((prec * 64 + recon) * 64 + a.nrhs) * 4 + epi) * 2 + a.blk;
+  const int key = hop_tune_key(c, a, prec, epi);
   auto it = c->hop_tune.find(key);
   if (it != c->hop_tune.end()) return launch_hop_profiled(c, a, prec, recon, epi, it->second);
   if (c->forced_tps > 0) {

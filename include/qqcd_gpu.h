@@ -186,15 +186,7 @@ int qq_z4source(qq_ctx* ctx, double* be, double* bo);
 int qq_twaverage_level0(qq_ctx* ctx, const double* be, const double* bo, const double* xe,
                         const double* xo, double kappa, double* J);
 
-/* ---- measurement (library-specific; no counterpart in the reference) ----
- * Times `niter` launches of the hopping kernel alone (H_oe of random fields, output
- * parity gblclr = 2) with CUDA events on the library's stream.  precision: 64
- * (links at the uploaded recon), 32 or 16 (FP32 recon-12 links); nrhs right-hand
- * sides per launch (1..8); tps threads per site (1, 2, 4; 0 = the autotuned
- * choice the solvers use).  flush_l2 != 0 overwrites a 512 MiB buffer between
- * launches so every launch reads its operands from HBM.  ms_per_call: mean kernel
- * time; bytes_per_call: algorithmic bytes of one launch,
- * V/2 * (8 * link bytes + nrhs * 2 * spinor bytes). */
+/* ---- measurement (library-specific; no counterpart in the reference) ---- */
 /* The cudaStream_t every call of this context runs on (for event timing). */
 int qq_ctx_stream(const qq_ctx* ctx, void** stream);
 /* Number of kernels this library has launched in this process so far. */
@@ -206,6 +198,14 @@ long long qq_launch_count(void);
 int qq_profile_hop(qq_ctx* ctx, int enable);
 int qq_profile_hop_read(qq_ctx* ctx, long long* launches, double* ms_total, double* bytes_total);
 
+/* Times `niter` launches of the hopping kernel alone (H_oe of random fields, output
+ * parity gblclr = 2) with CUDA events on the library's stream.  precision: 64
+ * (links at the uploaded recon), 32 or 16 (FP32 recon-12 links); nrhs right-hand
+ * sides per launch (1..32; for nrhs > 1 one RHS-interleaved block field, the layout
+ * of the batched solver); tps: kernel shape (0 = the autotuned choice the solvers
+ * use).  flush_l2 != 0 overwrites a 512 MiB buffer between launches so every launch
+ * reads its operands from HBM.  ms_per_call: mean kernel time; bytes_per_call:
+ * algorithmic bytes of one launch, V/2 * (8 * link bytes + nrhs * 2 * spinor bytes). */
 int qq_bench_hsingle(qq_ctx* ctx, int precision, int nrhs, int tps, int niter, int flush_l2,
                      double* ms_per_call, double* bytes_per_call);
 

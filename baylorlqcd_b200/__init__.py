@@ -30,6 +30,7 @@ STATUS_NAMES = {0: "OK", 1: "NOT_CONVERGED", 2: "NAN", 3: "BAD_ARG", 4: "CUDA_ER
 EXPORTED = [
     "qq_ctx_create", "qq_ctx_destroy", "qq_ctx_dims", "qq_last_error", "qq_set_coact",
     "qq_gauge_upload", "qq_hsingle", "qq_hdouble", "qq_hdbletm", "qq_twmshift", "qq_vecdot",
+    "qq_vecdot_noalloc",
     "qq_defl_create", "qq_defl_destroy", "qq_defl_size", "qq_gmresdr", "qq_gmresproj", "qq_psc",
     "qq_bicgstab", "qq_fermprop", "qq_pointsource", "qq_fermprop_batch", "qq_initlagfib",
     "qq_rnds", "qq_z2source", "qq_z4source", "qq_twaverage_level0", "qq_bench_hsingle",
@@ -111,6 +112,7 @@ def load_library() -> C.CDLL:
         "qq_hdbletm": ([P, P, P, I, DP, I], I),
         "qq_twmshift": ([P, P, P, I, DP, I], I),
         "qq_vecdot": ([P, P, P, DP], I),
+        "qq_vecdot_noalloc": ([P, P, P, DP], I),
         "qq_defl_create": ([P, I, I, C.POINTER(P)], I),
         "qq_defl_destroy": ([P], I),
         "qq_defl_size": ([P], I),
@@ -289,6 +291,13 @@ class Lattice:
     def vecdot(self, a, b) -> complex:
         r = (C.c_double * 2)()
         _check(self.lib.qq_vecdot(self._ctx, _ptr(a), _ptr(b), r))
+        return complex(r[0], r[1])
+
+    def vecdot_noalloc(self, a, b) -> complex:
+        """vecdot of two torch CUDA tensors in the reference layout, allocating no
+        device memory (qq_vecdot_noalloc)."""
+        r = (C.c_double * 2)()
+        _check(self.lib.qq_vecdot_noalloc(self._ctx, _ptr(a), _ptr(b), r))
         return complex(r[0], r[1])
 
     # ---- inverters (Q/inverters.f90) ----

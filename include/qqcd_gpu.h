@@ -104,6 +104,16 @@ int qq_twmshift(qq_ctx* ctx, double* hwhole, const double* gwhole, int idag,
                 const double kappa[2], int iflag);
 /* vecdot Q/inverters.f90:13485-13530: adb = sum a^dagger b (FP64). */
 int qq_vecdot(qq_ctx* ctx, const double* a, const double* b, double adb[2]);
+/* No counterpart in the reference: vecdot for callers that must not allocate device
+ * memory (a host code that has committed the device to its own preallocated field
+ * arrays, or a solver loop where cudaMalloc/cudaFree would synchronise the device).
+ * a and b: reference-layout half-vectors in device memory of this context's device
+ * (16-byte aligned; host arrays are rejected, since staging them needs a buffer);
+ * adb: host or device memory.  Reduction partials live in a fixed 128 KiB static
+ * device array, which bounds the lattice at 4,194,304 sites (QQ_BAD_ARG above that).
+ * The first call on a device looks that array up (cudaGetSymbolAddress) and should
+ * precede any stream capture.  Calls that overlap on one device race on the array. */
+int qq_vecdot_noalloc(qq_ctx* ctx, const double* a, const double* b, double adb[2]);
 
 /* ---- inverters (Q/inverters.f90) ----
  * The deflation handle replaces the module variables of Q/shift.f90 (vtemp, hcnew,

@@ -142,7 +142,12 @@ int write_out(qq_ctx* c, double* dst, const std::vector<double>& src) {
 }  // namespace
 
 int lagfib_init(int myid, int iseed) {
-  g_rng.seed(myid + iseed);
+  // The delay indexes the skip polynomial, so it must be >= 0 ("ndelay must be a
+  // positive integer", lagfib.f90:89); the reference does not check and overruns.
+  const long long ndelay = (long long)myid + iseed;
+  if (ndelay < 0 || ndelay > 0x7fffffffLL)
+    return set_error(QQ_BAD_ARG, "qq_initlagfib: myid + iseed must be in [0, 2^31)");
+  g_rng.seed((int)ndelay);
   return QQ_OK;
 }
 

@@ -291,6 +291,9 @@ def set_kcyclim(n: int):
 
 
 def initlagfib(myid: int, iseed: int):
+    # bigdelay indexes c(ndelay) (G/lagfib.f90:185): a negative delay overruns it
+    if not 0 <= myid + iseed < 2**31:
+        raise ValueError("myid + iseed must be in [0, 2^31)")
     lib().oq_initlagfib(myid, iseed)
 
 

@@ -144,3 +144,47 @@ def hop_lex(links, psi, bc, c1=(1, 1, 1, 1), c2=(1, 1, 1, 1), idag=0):
         P = c1[mu] * np.eye(4) + s * c2[mu] * GAMMA[mu]
         out += np.einsum("st,...ta->...sa", P, Um)
     return out
+
+
+def su3_gram_schmidt(n, rng, eps=None):
+    """n SU(3) matrices from Gram-Schmidt on Gaussian complex matrices (near 1 when eps
+    is given).  Elementwise arithmetic only -- no LAPACK -- so the fields are
+    bit-reproducible on any machine, as the golden fixtures need."""
+    a = rng.standard_normal((n, 3, 3)) + 1j * rng.standard_normal((n, 3, 3))
+    if eps is not None:
+        a = np.eye(3)[None] + eps * a
+    r1 = a[:, 0] / np.sqrt(np.sum((a[:, 0] * np.conj(a[:, 0])).real, axis=1))[:, None]
+    r2 = a[:, 1] - np.sum(np.conj(r1) * a[:, 1], axis=1)[:, None] * r1
+    r2 = r2 / np.sqrt(np.sum((r2 * np.conj(r2)).real, axis=1))[:, None]
+    r3 = np.conj(np.cross(r1, r2))
+    return np.stack([r1, r2, r3], axis=1)
+
+
+def golden_gauge(dims, ntotal, seed, eps=0.5):
+    """Seeded, machine-independent gauge field: (links (4,nt,nz,ny,nx,3,3), u_ref)."""
+    rng = np.random.default_rng(seed)
+    nx, ny, nz, nt = dims
+    links = su3_gram_schmidt(4 * nx * ny * nz * nt, rng, eps).reshape(4, nt, nz, ny, nx, 3, 3)
+    return links, gauge_to_ref(links, dims, ntotal)
+
+
+def interior_basis(nvhalf):
+    """Index tuples (ibleo, ieo, id, isite, icri) of the real slot of every complex
+    interior component of a half-vector, in C order."""
+    ib, ie, idd, isite, ic = np.meshgrid(np.arange(8), np.arange(2), np.arange(4), np.arange(nvhalf),
+                                         np.arange(3), indexing="ij")
+    return ib.ravel(), ie.ravel(), idd.ravel(), isite.ravel(), 2 * ic.ravel()
+
+
+def half_to_vec(g, nvhalf):
+    """Interior entries of a half-vector as one complex vector (interior_basis order)."""
+    v = g[:, :, :, :nvhalf, :]
+    return (v[..., 0::2] + 1j * v[..., 1::2]).ravel()
+
+
+def vec_to_half(v, ntotal, nvhalf):
+    g = np.zeros((8, 2, 4, ntotal, 6))
+    c = v.reshape(8, 2, 4, nvhalf, 3)
+    g[:, :, :, :nvhalf, 0::2] = c.real
+    g[:, :, :, :nvhalf, 1::2] = c.imag
+    return g

@@ -1,0 +1,95 @@
+#!/usr/bin/env python
+"""Writes tests/golden/golden.json: reference outputs of the oracle (the CPU
+restatement of the qqcd hot path in oracle/) on small, seeded, machine-independent
+inputs.  The reference ships no golden vectors and its Fortran cannot be built here,
+so these pin the oracle against itself over time and give the GPU parity tests
+fixed numbers to meet.  Inputs:
+
+* lagged-Fibonacci draws (G/lagfib.f90) for three (myid, iseed) pairs;
+* Z(4) / Z(2) noise sources (Q/disconloops.f90:4518-4649) on 4x4x4x8, as code strings;
+* GMRES-DR(30,10) (Wilson) and GMRES-DR(20,6) (twisted mass), BiCGStab and
+  GMRES-Proj after a deflating first solve (psc), and fermprop with odd
+  reconstruction, all on 4x4x4x8 with the Gram-Schmidt gauge field of
+  qqtest.golden_gauge(seed 2026, eps 0.25; plaquette 0.52) and point sources.
+
+Usage: python tests/golden/make_golden.py   (rewrites golden.json)
+"""
+import json
+import sys
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+sys.path.insert(0, str(HERE.parent))
+sys.path.insert(0, str(HERE.parent.parent))
+
+import oracle  # noqa: E402
+from qqtest import golden_gauge  # noqa: E402
+
+DIMS = (4, 4, 4, 8)
+BC = (1, 1, 1, -1)
+GAUGE_SEED, GAUGE_EPS = 2026, 0.25
+Z4_CODES = {1: "a", -1: "b", 1j: "c", -1j: "d"}  # +1, -1, +i, -i
+
+
+def noise_codes(half, nvhalf):
+    c = (half[:, :, :, :nvhalf, 0::2] + 1j * half[:, :, :, :nvhalf, 1::2]).ravel()
+    return "".join(Z4_CODES[complex(v)] for v in c)
+
+
+def solve_record(x, st, log, b, ol):
+    hist, hmvp = log.history()
+    return {"status": int(st), "itercount": int(log.itercount), "ncycles": int(log.ncycles),
+            "mvp": int(log.mvp), "hist": [float(h) for h in hist], "hist_mvp": [int(m) for m in hmvp],
+            "ritz": [[float(r.real), float(r.imag)] for r in log.ritz_values()],
+            "x_norm2": float(ol.vecdot(x, x).real),
+            "b_dot_x": [float(ol.vecdot(b, x).real), float(ol.vecdot(b, x).imag)]}
+
+
+def main():
+    out = {"dims": DIMS, "bc": BC, "gauge_seed": GAUGE_SEED, "gauge_eps": GAUGE_EPS}
+    out["lagfib"] = {}
+    for myid, iseed in [(0, 13), (1, 13), (0, 1)]:
+        oracle.initlagfib(myid, iseed)
+        out["lagfib"][f"{myid},{iseed}"] = [float(v) for v in oracle.rnds(32)]
+
+    ol = oracle.OracleLattice(*DIMS, bc=BC)
+    out["noise"] = {}
+    for name, fn in (("z4", ol.z4source), ("z2", ol.z2source)):
+        oracle.initlagfib(0, 13)
+        be, bo = fn()
+        out["noise"][name] = {"be": noise_codes(be, ol.nvhalf), "bo": noise_codes(bo, ol.nvhalf)}
+
+    _, u = golden_gauge(DIMS, ol.ntotal, GAUGE_SEED, GAUGE_EPS)
+    ol.set_gauge(u)
+    out["plaquette"] = float(ol.aveplaq())
+    be, bo = ol.pointsource((1, 1, 1, 1), 1, 1)
+    be2, bo2 = ol.pointsource((2, 3, 1, 4), 2, 3)
+    solves = {}
+    x, st, log = ol.gmresdr(be, ol.new_half(), (30, 10), 1e-10, kappa=(0.15, 0.0))
+    solves["gmresdr_wilson"] = dict(kappa=[0.15, 0.0], GMRES=[30, 10], resmax=1e-10, src="be",
+                                    **solve_record(x, st, log, be, ol))
+    x, st, log = ol.gmresdr(be2, ol.new_half(), (20, 6), 1e-10, kappa=(0.155, 0.01))
+    solves["gmresdr_tm"] = dict(kappa=[0.155, 0.01], GMRES=[20, 6], resmax=1e-10, src="be2",
+                                **solve_record(x, st, log, be2, ol))
+    x, st, log = ol.bicgstab(be, ol.new_half(), 1e-10, kappa=(0.15, 0.0))
+    solves["bicgstab_wilson"] = dict(kappa=[0.15, 0.0], resmax=1e-10, src="be",
+                                     **solve_record(x, st, log, be, ol))
+    d = ol.deflation(20, 6)
+    ol.psc(be, ol.new_half(), (20, 6), 1e-10, kappa=(0.15, 0.0), isignal=1, defl=d)
+    x, st, log = ol.psc(be2, ol.new_half(), (20, 6), 1e-10, kappa=(0.15, 0.0), isignal=2, defl=d)
+    solves["psc_second_rhs"] = dict(kappa=[0.15, 0.0], GMRES=[20, 6], src="be2",
+                                    **solve_record(x, st, log, be2, ol))
+    xe, xo, st, log = ol.fermprop(be, bo, (0.15, 0.0), inverter=5, resmax=1e-10, nGMRES=(30, 10))
+    solves["fermprop_wilson"] = dict(kappa=[0.15, 0.0], nGMRES=[30, 10], inverter=5, src="point 1,1,1,1 c1 s1",
+                                     xe_norm2=float(ol.vecdot(xe, xe).real),
+                                     xo_norm2=float(ol.vecdot(xo, xo).real),
+                                     itercount=int(log.itercount))
+    out["solves"] = solves
+    (HERE / "golden.json").write_text(json.dumps(out, indent=1) + "\n")
+    print("wrote", HERE / "golden.json")
+
+
+if __name__ == "__main__":
+    main()

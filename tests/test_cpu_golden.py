@@ -1,0 +1,102 @@
+"""The oracle against the committed golden fixtures (tests/golden/golden.json,
+written by tests/golden/make_golden.py).  Random streams and noise codes must match
+bit for bit; solver histories, Ritz values and checksums to 1e-10 relative (the oracle
+is compiled for baseline x86-64 without FMA contraction, so it reproduces across x86
+hosts up to the last bits of libm)."""
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import oracle
+from qqtest import golden_gauge
+
+GOLDEN = json.loads((Path(__file__).resolve().parent / "golden" / "golden.json").read_text())
+DIMS = tuple(GOLDEN["dims"])
+BC = tuple(GOLDEN["bc"])
+RTOL = 1e-10
+
+
+@pytest.fixture(scope="module")
+def ol():
+    o = oracle.OracleLattice(*DIMS, bc=BC)
+    _, u = golden_gauge(DIMS, o.ntotal, GOLDEN["gauge_seed"], GOLDEN["gauge_eps"])
+    o.set_gauge(u)
+    return o
+
+
+def sources(ol):
+    return {"be": ol.pointsource((1, 1, 1, 1), 1, 1), "be2": ol.pointsource((2, 3, 1, 4), 2, 3)}
+
+
+def codes(half, nvhalf):
+    m = {1: "a", -1: "b", 1j: "c", -1j: "d"}
+    c = (half[:, :, :, :nvhalf, 0::2] + 1j * half[:, :, :, :nvhalf, 1::2]).ravel()
+    return "".join(m[complex(v)] for v in c)
+
+
+@pytest.mark.parametrize("key", sorted(GOLDEN["lagfib"]))
+def test_lagfib_stream(key):
+    myid, iseed = (int(v) for v in key.split(","))
+    oracle.initlagfib(myid, iseed)
+    assert oracle.rnds(32).tolist() == GOLDEN["lagfib"][key]
+
+
+@pytest.mark.parametrize("kind", ["z4", "z2"])
+def test_noise_codes(ol, kind):
+    oracle.initlagfib(0, 13)
+    be, bo = ol.z4source() if kind == "z4" else ol.z2source()
+    assert codes(be, ol.nvhalf) == GOLDEN["noise"][kind]["be"]
+    assert codes(bo, ol.nvhalf) == GOLDEN["noise"][kind]["bo"]
+
+
+def test_plaquette(ol):
+    assert abs(ol.aveplaq() - GOLDEN["plaquette"]) < 1e-14
+
+
+def check_record(rec, x, st, log, b, ol):
+    assert st == rec["status"]
+    assert log.itercount == rec["itercount"] and log.ncycles == rec["ncycles"]
+    hist, _ = log.history()
+    np.testing.assert_allclose(hist, rec["hist"], rtol=RTOL, atol=1e-22)
+    r = np.array(rec["ritz"]).reshape(-1, 2)
+    np.testing.assert_allclose(log.ritz_values(), r[:, 0] + 1j * r[:, 1], rtol=RTOL)
+    np.testing.assert_allclose(ol.vecdot(x, x).real, rec["x_norm2"], rtol=RTOL)
+    bx = ol.vecdot(b, x)
+    np.testing.assert_allclose([bx.real, bx.imag], rec["b_dot_x"], rtol=RTOL)
+
+
+@pytest.mark.parametrize("name", ["gmresdr_wilson", "gmresdr_tm"])
+def test_gmresdr(ol, name):
+    rec = GOLDEN["solves"][name]
+    b = sources(ol)[rec["src"]][0]
+    x, st, log = ol.gmresdr(b, ol.new_half(), tuple(rec["GMRES"]), rec["resmax"], kappa=tuple(rec["kappa"]))
+    check_record(rec, x, st, log, b, ol)
+
+
+def test_bicgstab(ol):
+    rec = GOLDEN["solves"]["bicgstab_wilson"]
+    b = sources(ol)["be"][0]
+    x, st, log = ol.bicgstab(b, ol.new_half(), rec["resmax"], kappa=tuple(rec["kappa"]))
+    check_record(rec, x, st, log, b, ol)
+
+
+def test_psc_second_rhs(ol):
+    rec = GOLDEN["solves"]["psc_second_rhs"]
+    src = sources(ol)
+    k = tuple(rec["kappa"])
+    d = ol.deflation(20, 6)
+    ol.psc(src["be"][0], ol.new_half(), (20, 6), 1e-10, kappa=k, isignal=1, defl=d)
+    x, st, log = ol.psc(src["be2"][0], ol.new_half(), (20, 6), 1e-10, kappa=k, isignal=2, defl=d)
+    check_record(rec, x, st, log, src["be2"][0], ol)
+
+
+def test_fermprop(ol):
+    rec = GOLDEN["solves"]["fermprop_wilson"]
+    be, bo = sources(ol)["be"]
+    xe, xo, st, log = ol.fermprop(be, bo, tuple(rec["kappa"]), inverter=5, resmax=1e-10,
+                                  nGMRES=tuple(rec["nGMRES"]))
+    assert log.itercount == rec["itercount"]
+    np.testing.assert_allclose(ol.vecdot(xe, xe).real, rec["xe_norm2"], rtol=RTOL)
+    np.testing.assert_allclose(ol.vecdot(xo, xo).real, rec["xo_norm2"], rtol=RTOL)

@@ -1,0 +1,122 @@
+"""The CUDA path, through the C ABI, against the committed golden fixtures
+(tests/golden/golden.json, generated from the oracle by tests/golden/make_golden.py).
+
+Noise sources must match bit for bit.  The GPU Arnoldi orthogonalises with CGS2 where
+the reference uses modified Gram-Schmidt and sums in a different order, so solver
+results agree to rounding: cycle counts within one, per-cycle residual histories
+within 10%, harmonic Ritz values to 1e-6, solution checksums (|x|^2 and <b, x>) to
+1e-7 relative (1e-6 after GMRES-Proj, which stops at the reference's fixed 1e-8)."""
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from qqtest import golden_gauge
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = json.loads((Path(__file__).resolve().parent / "golden" / "golden.json").read_text())
+DIMS = tuple(GOLDEN["dims"])
+BC = tuple(GOLDEN["bc"])
+
+
+@pytest.fixture(scope="module")
+def lat():
+    import baylorlqcd_b200 as qq
+
+    lat = qq.Lattice(*DIMS, bc=BC)
+    _, u = golden_gauge(DIMS, lat.ntotal, GOLDEN["gauge_seed"], GOLDEN["gauge_eps"])
+    lat.gauge_upload(u)  # exact SU(3): the reconstruct-12 path is chosen
+    yield lat
+    lat.close()
+
+
+def vdot(a, b, nv):
+    ca = a[:, :, :, :nv, 0::2] + 1j * a[:, :, :, :nv, 1::2]
+    cb = b[:, :, :, :nv, 0::2] + 1j * b[:, :, :, :nv, 1::2]
+    return np.vdot(ca.ravel(), cb.ravel())
+
+
+def codes(half, nvhalf):
+    m = {1: "a", -1: "b", 1j: "c", -1j: "d"}
+    c = (half[:, :, :, :nvhalf, 0::2] + 1j * half[:, :, :, :nvhalf, 1::2]).ravel()
+    return "".join(m[complex(v)] for v in c)
+
+
+def check(rec, x, info, b, nv, rtol_x=1e-7, cycles=True):
+    assert info.status == rec["status"]
+    if cycles:
+        assert abs(info.ncycles - rec["ncycles"]) <= 1
+        n = min(len(info.hist), len(rec["hist"])) - 1
+        np.testing.assert_allclose(info.hist[:n], rec["hist"][:n], rtol=0.1)
+    np.testing.assert_allclose(vdot(x, x, nv).real, rec["x_norm2"], rtol=rtol_x)
+    bx = vdot(b, x, nv)
+    np.testing.assert_allclose([bx.real, bx.imag], rec["b_dot_x"], rtol=rtol_x, atol=rtol_x * abs(bx))
+
+
+@pytest.mark.parametrize("kind", ["z4", "z2"])
+def test_noise_codes(lat, kind):
+    import baylorlqcd_b200 as qq
+
+    qq.initlagfib(0, 13)
+    be, bo = lat.z4source() if kind == "z4" else lat.z2source()
+    assert codes(be, lat.nvhalf) == GOLDEN["noise"][kind]["be"]
+    assert codes(bo, lat.nvhalf) == GOLDEN["noise"][kind]["bo"]
+
+
+def test_point_sources(lat):
+    import oracle
+
+    ol = oracle.OracleLattice(*DIMS, bc=BC)
+    for src, c, s in [((1, 1, 1, 1), 1, 1), ((2, 3, 1, 4), 2, 3)]:
+        for a, b in zip(lat.pointsource(src, c, s), ol.pointsource(src, c, s)):
+            assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("name", ["gmresdr_wilson", "gmresdr_tm"])
+def test_gmresdr(lat, name):
+    rec = GOLDEN["solves"][name]
+    src = (1, 1, 1, 1), 1, 1
+    if rec["src"] == "be2":
+        src = (2, 3, 1, 4), 2, 3
+    b = lat.pointsource(*src)[0]
+    x, info = lat.gmresdr(b, lat.new_half(), tuple(rec["GMRES"]), rec["resmax"], 0, tuple(rec["kappa"]))
+    check(rec, x, info, b, lat.nvhalf)
+    assert info.true_rel < rec["resmax"]
+    k = rec["GMRES"][1]
+    r = np.array(rec["ritz"]).reshape(-1, 2)
+    want = np.sort_complex((r[:, 0] + 1j * r[:, 1])[:k])
+    got = np.sort_complex(info.ritz[np.argsort(np.abs(info.ritz))[:k]])
+    np.testing.assert_allclose(got, want, rtol=1e-6)
+
+
+def test_bicgstab(lat):
+    rec = GOLDEN["solves"]["bicgstab_wilson"]
+    b = lat.pointsource((1, 1, 1, 1), 1, 1)[0]
+    x, info = lat.bicgstab(b, lat.new_half(), rec["resmax"], 0, tuple(rec["kappa"]))
+    check(rec, x, info, b, lat.nvhalf, cycles=False)
+    assert abs(info.itercount - rec["itercount"]) <= 0.1 * rec["itercount"]
+
+
+def test_psc_second_rhs(lat):
+    rec = GOLDEN["solves"]["psc_second_rhs"]
+    k = tuple(rec["kappa"])
+    b1 = lat.pointsource((1, 1, 1, 1), 1, 1)[0]
+    b2 = lat.pointsource((2, 3, 1, 4), 2, 3)[0]
+    d = lat.deflation(20, 6)
+    lat.psc(b1, lat.new_half(), (20, 6), 1e-10, 0, k, isignal=1, defl=d)
+    x, info = lat.psc(b2, lat.new_half(), (20, 6), 1e-10, 0, k, isignal=2, defl=d)
+    check(rec, x, info, b2, lat.nvhalf, rtol_x=1e-6)
+    d.close()
+
+
+def test_fermprop(lat):
+    rec = GOLDEN["solves"]["fermprop_wilson"]
+    be, bo = lat.pointsource((1, 1, 1, 1), 1, 1)
+    xe, xo, info = lat.fermprop(be, bo, tuple(rec["kappa"]), inverter=5, resmax=1e-10,
+                                nGMRES=tuple(rec["nGMRES"]))
+    assert info.status == 0
+    nv = lat.nvhalf
+    np.testing.assert_allclose(vdot(xe, xe, nv).real, rec["xe_norm2"], rtol=1e-7)
+    np.testing.assert_allclose(vdot(xo, xo, nv).real, rec["xo_norm2"], rtol=1e-7)

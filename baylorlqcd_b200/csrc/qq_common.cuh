@@ -18,27 +18,69 @@
 
 namespace qq {
 
+// Division of a non-negative 31-bit n by a divisor d fixed at set-up, by one high
+// multiply and a shift (Granlund & Montgomery, "Division by invariant integers using
+// multiplication", PLDI 1994, section 4): with l = ceil(log2 d) and
+// m = floor(2^32 (2^l - d) / d) + 1, n / d = (umulhi(n, m) + n) >> l, exact for
+// 0 <= n < 2^31 (the sum stays below 2^32).  Device integer division by a runtime
+// divisor otherwise costs a conversion-pipe sequence per quotient.
+struct FastDiv {
+  unsigned d = 1, m = 1;
+  int l = 0;
+  FastDiv() = default;
+  explicit FastDiv(unsigned dv) : d(dv) {
+    while ((1ull << l) < dv) ++l;
+    m = (unsigned)((((1ull << l) - dv) << 32) / dv) + 1u;
+  }
+  __host__ __device__ inline int div(int n) const {
+#ifdef __CUDA_ARCH__
+    return (int)((__umulhi((unsigned)n, m) + (unsigned)n) >> l);
+#else
+    return (int)(((unsigned)(((unsigned long long)(unsigned)n * m) >> 32) + (unsigned)n) >> l);
+#endif
+  }
+  __host__ __device__ inline int mod(int n, int q) const { return n - q * (int)d; }
+};
+
 struct Geom {
   int n[4];        // nx, ny, nz, nt
   int vh;          // sites per parity
   int nxh;         // nx / 2
   int bc[4];       // boundary factor per direction: 1, -1, 0
+  float bcf[4];    // bc as float and double (no conversion inside the kernels)
+  double bcd[4];
+  FastDiv div_nxh, div_ny, div_nz;
 };
 
+// Fill the derived members of g from n and bc.
+inline void geom_finish(Geom& g) {
+  g.vh = g.n[0] * g.n[1] * g.n[2] * g.n[3] / 2;
+  g.nxh = g.n[0] / 2;
+  for (int mu = 0; mu < 4; ++mu) {
+    g.bcf[mu] = (float)g.bc[mu];
+    g.bcd[mu] = (double)g.bc[mu];
+  }
+  g.div_nxh = FastDiv((unsigned)g.nxh);
+  g.div_ny = FastDiv((unsigned)g.n[1]);
+  g.div_nz = FastDiv((unsigned)g.n[2]);
+}
+
 // Hopping coefficients of one Hsingle call, after folding idag and the projector
-// decomposition (c1 -/+ c2 gamma) = a (1 - gamma) + b (1 + gamma).
+// decomposition (c1 -/+ c2 gamma) = a (1 - gamma) + b (1 + gamma); float copies for
+// the single-precision kernels.
 struct HopCoef {
   double fm[4], fp[4];  // forward hop (x+mu): coefficient of (1-gamma), (1+gamma)
   double bm[4], bp[4];  // backward hop (x-mu): coefficient of (1-gamma), (1+gamma)
+  float fmf[4], fpf[4], bmf[4], bpf[4];
 };
 
 __host__ __device__ inline void site_coords(const Geom& g, int p, int s, int* x) {
-  const int xh = s % g.nxh;
-  int r = s / g.nxh;
-  x[1] = r % g.n[1];
-  r /= g.n[1];
-  x[2] = r % g.n[2];
-  x[3] = r / g.n[2];
+  int r = g.div_nxh.div(s);
+  const int xh = s - r * g.nxh;
+  int r2 = g.div_ny.div(r);
+  x[1] = r - r2 * g.n[1];
+  x[3] = g.div_nz.div(r2);
+  x[2] = r2 - x[3] * g.n[2];
   x[0] = 2 * xh + ((p + x[1] + x[2] + x[3]) & 1);
 }
 

@@ -25,12 +25,15 @@ enum Epilogue : int {
 
 constexpr int kMaxRhs = 8;     // right-hand sides per launch, separate fields
 constexpr int kMaxBatch = 32;  // right-hand sides per launch, one block field
+constexpr int kShapeMrhs = 200;  // kernel-shape code base of hop_mrhs_kernel (200 + RPT)
 
 struct HopArgs {
   Geom g;
   HopCoef c;
   int pout;                    // output parity (0 = gblclr 1, 1 = gblclr 2)
   int nrhs;
+  int per_block;               // sites per thread block (set by the launcher)
+  FastDiv div_nrhs;            // thread -> (site, rhs) split without integer division
   int blk;                     // 1: in/out/aux[0] are RHS-interleaved block fields of nrhs
                                //    right-hand sides: element (plane q, site s, rhs r) at
                                //    q * (vh * nrhs) + s * nrhs + r
@@ -47,6 +50,7 @@ struct HopArgs {
   const float* aux_norm[kMaxRhs];
   double a;                    // EPI_TWIST: 2 kappa mu
   double f1, f2, f3;           // EPI_DBLE factors
+  float af, f1f, f2f, f3f;     // float copies (set by the launcher)
 };
 
 template <class R>
@@ -138,24 +142,26 @@ __device__ inline void hop(const HopArgs& a, int s, int r, const int* x, cplx<R>
   using SIO = SpinorIO<SP>;
   using LIO = LinkIO<LP, RECON>;
   int y[4] = {x[0], x[1], x[2], x[3]};
+  constexpr bool kF = sizeof(R) == 4;
+  const R bcr = kF ? (R)a.g.bcf[MU] : (R)a.g.bcd[MU];  // same type: no conversion
   R sgn = (R)1;
   if (FWD) {
     y[MU] += 1;
     if (y[MU] == a.g.n[MU]) {
       y[MU] = 0;
-      sgn = (R)a.g.bc[MU];
+      sgn = bcr;
     }
   } else {
     y[MU] -= 1;
     if (y[MU] < 0) {
       y[MU] = a.g.n[MU] - 1;
-      sgn = (R)a.g.bc[MU];
+      sgn = bcr;
     }
   }
   if (sgn == (R)0) return;
   const int sy = site_index(a.g, y);
-  const R cm = sgn * (R)(FWD ? a.c.fm[MU] : a.c.bm[MU]);
-  const R cp = sgn * (R)(FWD ? a.c.fp[MU] : a.c.bp[MU]);
+  const R cm = sgn * (kF ? (R)(FWD ? a.c.fmf[MU] : a.c.bmf[MU]) : (R)(FWD ? a.c.fm[MU] : a.c.bm[MU]));
+  const R cp = sgn * (kF ? (R)(FWD ? a.c.fpf[MU] : a.c.bpf[MU]) : (R)(FWD ? a.c.fp[MU] : a.c.bp[MU]));
   // All right-hand sides of a site sit in adjacent lanes: this load is one
   // broadcast transaction for them, so the link crosses HBM once per RHS block.
   Su3<R> u;
@@ -190,6 +196,145 @@ __device__ inline void hop(const HopArgs& a, int s, int r, const int* x, cplx<R>
   }
 }
 
+// Epilogue of one (site, right-hand side): combine the accumulated hopping term with
+// the twist / Schur-complement factors and store.
+template <int SP, int EPI, class R>
+__device__ inline void hop_finish(const HopArgs& a, int s, int r, const cplx<R>* acc) {
+  using SIO = SpinorIO<SP>;
+  constexpr bool kF = sizeof(R) == 4;
+  cplx<R> o[12];
+  if (EPI == EPI_STORE) {
+#pragma unroll
+    for (int c = 0; c < 12; ++c) o[c] = acc[c];
+  } else if (EPI == EPI_TWIST) {
+    const R t = kF ? (R)a.af : (R)a.a;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      o[0 + c] = csub(acc[0 + c], cscale(t, acc[6 + c]));
+      o[3 + c] = csub(acc[3 + c], cscale(t, acc[9 + c]));
+      o[6 + c] = cadd(acc[6 + c], cscale(t, acc[0 + c]));
+      o[9 + c] = cadd(acc[9 + c], cscale(t, acc[3 + c]));
+    }
+  } else {
+    cplx<R> gg[12];
+    SIO::load(a.blk ? a.aux[0] : a.aux[r], a.blk ? a.aux_norm[0] : a.aux_norm[r], a.vh_of(),
+              a.idx_of(s, r), gg);
+    const R f1 = kF ? (R)a.f1f : (R)a.f1, f2 = kF ? (R)a.f2f : (R)a.f2, f3 = kF ? (R)a.f3f : (R)a.f3;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      o[0 + c] = csub(cadd(cscale(f1, gg[0 + c]), cscale(f2, gg[6 + c])), cscale(f3, acc[0 + c]));
+      o[3 + c] = csub(cadd(cscale(f1, gg[3 + c]), cscale(f2, gg[9 + c])), cscale(f3, acc[3 + c]));
+      o[6 + c] = csub(csub(cscale(f1, gg[6 + c]), cscale(f2, gg[0 + c])), cscale(f3, acc[6 + c]));
+      o[9 + c] = csub(csub(cscale(f1, gg[9 + c]), cscale(f2, gg[3 + c])), cscale(f3, acc[9 + c]));
+    }
+  }
+  SIO::store(a.blk ? a.out[0] : a.out[r], a.blk ? a.out_norm[0] : a.out_norm[r], a.vh_of(),
+             a.idx_of(s, r), o);
+}
+
+// ---------------------------------------------------------------------------
+// Several right-hand sides per thread (block fields only).  A thread owns one site
+// and the RPT right-hand sides r0, r0 + G, ..., r0 + (RPT-1) G of the block
+// (G = nrhs / RPT threads per site, so each plane load of a warp still covers whole
+// 32-byte sectors).  Per direction it computes the neighbour index and boundary
+// factor and loads and rebuilds the link once, then applies them to its RPT spinors:
+// the index arithmetic, link loads and recon-12 reconstruction that dominate the
+// instruction count of the one-RHS-per-thread kernel are shared RPT ways.
+// ---------------------------------------------------------------------------
+template <int SP, int LP, int RECON, int MU, bool FWD, int RPT, class R>
+__device__ inline void hop_multi(const HopArgs& a, int s, int r0, int G, const int* x,
+                                 cplx<R> (*acc)[12]) {
+  using SIO = SpinorIO<SP>;
+  using LIO = LinkIO<LP, RECON>;
+  constexpr bool kF = sizeof(R) == 4;
+  int y[4] = {x[0], x[1], x[2], x[3]};
+  R sgn = (R)1;
+  const R bcr = kF ? (R)a.g.bcf[MU] : (R)a.g.bcd[MU];
+  if (FWD) {
+    y[MU] += 1;
+    if (y[MU] == a.g.n[MU]) {
+      y[MU] = 0;
+      sgn = bcr;
+    }
+  } else {
+    y[MU] -= 1;
+    if (y[MU] < 0) {
+      y[MU] = a.g.n[MU] - 1;
+      sgn = bcr;
+    }
+  }
+  if (sgn == (R)0) return;
+  const int sy = site_index(a.g, y);
+  const R cm = sgn * (kF ? (R)(FWD ? a.c.fmf[MU] : a.c.bmf[MU]) : (R)(FWD ? a.c.fm[MU] : a.c.bm[MU]));
+  const R cp = sgn * (kF ? (R)(FWD ? a.c.fpf[MU] : a.c.bpf[MU]) : (R)(FWD ? a.c.fp[MU] : a.c.bp[MU]));
+  Su3<R> u;
+  if (FWD)
+    LIO::load(a.gauge, a.g.vh, a.pout, MU, s, u);
+  else
+    LIO::load(a.gauge, a.g.vh, 1 - a.pout, MU, sy, u);
+  const int n = a.g.vh * a.nrhs;
+  const int base = sy * a.nrhs + r0;
+#pragma unroll
+  for (int k = 0; k < RPT; ++k) {
+    cplx<R> psi[12];
+    SIO::load(a.in[0], a.in_norm[0], n, base + k * G, psi);
+    cplx<R> h[6], w[6];
+    if (cm != (R)0) {
+      project<MU, -1>(psi, cm, h);
+      if (FWD) {
+        matvec(u, h, w);
+        matvec(u, h + 3, w + 3);
+      } else {
+        matvec_dag(u, h, w);
+        matvec_dag(u, h + 3, w + 3);
+      }
+      reconstruct_acc<MU, -1>(acc[k], w);
+    }
+    if (cp != (R)0) {
+      project<MU, +1>(psi, cp, h);
+      if (FWD) {
+        matvec(u, h, w);
+        matvec(u, h + 3, w + 3);
+      } else {
+        matvec_dag(u, h, w);
+        matvec_dag(u, h + 3, w + 3);
+      }
+      reconstruct_acc<MU, +1>(acc[k], w);
+    }
+  }
+}
+
+// Thread layout: threadIdx.x = (site-in-block) * G + j, G = nrhs / RPT; the thread
+// handles right-hand sides j, j + G, ..., j + (RPT - 1) G of its site.
+template <int SP, int LP, int RECON, int RPT, int EPI>
+__global__ void __launch_bounds__(128) hop_mrhs_kernel(HopArgs a) {
+  using SIO = SpinorIO<SP>;
+  using R = typename SIO::R;
+  const int G = a.nrhs / RPT;
+  const int tx = threadIdx.x;
+  const int sl = a.div_nrhs.div(tx);  // div_nrhs divides by G for this kernel
+  const int j = tx - sl * G;
+  const int s = blockIdx.x * a.per_block + sl;
+  if (s >= a.g.vh || sl >= a.per_block) return;
+  cplx<R> acc[RPT][12];
+#pragma unroll
+  for (int k = 0; k < RPT; ++k)
+#pragma unroll
+    for (int c = 0; c < 12; ++c) acc[k][c] = {(R)0, (R)0};
+  int x[4];
+  site_coords(a.g, a.pout, s, x);
+  hop_multi<SP, LP, RECON, 0, true, RPT>(a, s, j, G, x, acc);
+  hop_multi<SP, LP, RECON, 0, false, RPT>(a, s, j, G, x, acc);
+  hop_multi<SP, LP, RECON, 1, true, RPT>(a, s, j, G, x, acc);
+  hop_multi<SP, LP, RECON, 1, false, RPT>(a, s, j, G, x, acc);
+  hop_multi<SP, LP, RECON, 2, true, RPT>(a, s, j, G, x, acc);
+  hop_multi<SP, LP, RECON, 2, false, RPT>(a, s, j, G, x, acc);
+  hop_multi<SP, LP, RECON, 3, true, RPT>(a, s, j, G, x, acc);
+  hop_multi<SP, LP, RECON, 3, false, RPT>(a, s, j, G, x, acc);
+#pragma unroll
+  for (int k = 0; k < RPT; ++k) hop_finish<SP, EPI>(a, s, j + k * G, acc[k]);
+}
+
 // Thread layout: threadIdx.x = (site-in-block) * nrhs + rhs, threadIdx.y = direction
 // group (TPS groups; group t applies the directions mu with mu % TPS == t).  With
 // TPS > 1 the partial sums meet in shared memory and group 0 runs the epilogue.
@@ -199,11 +344,12 @@ __global__ void __launch_bounds__(128) hop_kernel(HopArgs a) {
   using R = typename SIO::R;
   static_assert(sizeof(typename LinkIO<LP, RECON>::R) == sizeof(R), "link/spinor precision");
   const int nrhs = a.nrhs;
-  const int per_block = blockDim.x / nrhs;
+  const int per_block = a.per_block;
   const int tx = threadIdx.x, ty = threadIdx.y;
-  const int r = tx % nrhs;
-  const int s = blockIdx.x * per_block + tx / nrhs;
-  const bool active = s < a.g.vh && tx < per_block * nrhs;
+  const int sl = a.div_nrhs.div(tx);
+  const int r = tx - sl * nrhs;
+  const int s = blockIdx.x * per_block + sl;
+  const bool active = s < a.g.vh && sl < per_block;
   cplx<R> acc[12];
 #pragma unroll
   for (int c = 0; c < 12; ++c) acc[c] = {(R)0, (R)0};
@@ -242,34 +388,7 @@ __global__ void __launch_bounds__(128) hop_kernel(HopArgs a) {
       for (int c = 0; c < 12; ++c) acc[c] = cadd(acc[c], red[g * blockDim.x + tx][c]);
   }
   if (!active) return;
-  cplx<R> o[12];
-  if (EPI == EPI_STORE) {
-#pragma unroll
-    for (int c = 0; c < 12; ++c) o[c] = acc[c];
-  } else if (EPI == EPI_TWIST) {
-    const R t = (R)a.a;
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      o[0 + c] = csub(acc[0 + c], cscale(t, acc[6 + c]));
-      o[3 + c] = csub(acc[3 + c], cscale(t, acc[9 + c]));
-      o[6 + c] = cadd(acc[6 + c], cscale(t, acc[0 + c]));
-      o[9 + c] = cadd(acc[9 + c], cscale(t, acc[3 + c]));
-    }
-  } else {
-    cplx<R> gg[12];
-    SIO::load(a.blk ? a.aux[0] : a.aux[r], a.blk ? a.aux_norm[0] : a.aux_norm[r], a.vh_of(),
-              a.idx_of(s, r), gg);
-    const R f1 = (R)a.f1, f2 = (R)a.f2, f3 = (R)a.f3;
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      o[0 + c] = csub(cadd(cscale(f1, gg[0 + c]), cscale(f2, gg[6 + c])), cscale(f3, acc[0 + c]));
-      o[3 + c] = csub(cadd(cscale(f1, gg[3 + c]), cscale(f2, gg[9 + c])), cscale(f3, acc[3 + c]));
-      o[6 + c] = csub(csub(cscale(f1, gg[6 + c]), cscale(f2, gg[0 + c])), cscale(f3, acc[6 + c]));
-      o[9 + c] = csub(csub(cscale(f1, gg[9 + c]), cscale(f2, gg[3 + c])), cscale(f3, acc[9 + c]));
-    }
-  }
-  SIO::store(a.blk ? a.out[0] : a.out[r], a.blk ? a.out_norm[0] : a.out_norm[r], a.vh_of(),
-             a.idx_of(s, r), o);
+  hop_finish<SP, EPI>(a, s, r, acc);
 }
 
 // ---------------------------------------------------------------------------
@@ -491,11 +610,12 @@ __global__ void __launch_bounds__(128) hop_staged_kernel(HopArgs a) {
   extern __shared__ uint4 slots[];
   const int T = blockDim.x;
   const int nrhs = a.nrhs;
-  const int per_block = T / nrhs;
+  const int per_block = a.per_block;
   const int tid = threadIdx.x;
-  const int r = tid % nrhs;
-  const int s = blockIdx.x * per_block + tid / nrhs;
-  if (s >= a.g.vh || tid >= per_block * nrhs) return;
+  const int sl = a.div_nrhs.div(tid);
+  const int r = tid - sl * nrhs;
+  const int s = blockIdx.x * per_block + sl;
+  if (s >= a.g.vh || sl >= per_block) return;
   uint4* my = slots + tid;
   int x[4];
   site_coords(a.g, a.pout, s, x);
@@ -531,9 +651,17 @@ inline size_t staged_smem_bytes(int T) {
 }
 
 // Block shape of hop_kernel for TPS direction groups and nrhs right-hand sides.
-inline void hop_block_shape(int tps, int nrhs, int vh, dim3* blk, dim3* grd) {
+// Sites per block: as many as fit in 128 / tps threads, reduced to a whole number of
+// warps when that keeps at least half of them (12 RHS: 8 sites = 96 threads, not 120).
+inline int hop_sites_per_block(int tps, int nrhs) {
   const int bx_max = 128 / tps;
-  const int per_block = bx_max / nrhs;
+  int per_block = bx_max / nrhs;
+  for (int p = per_block; p >= (per_block + 1) / 2; --p)
+    if ((p * nrhs) % 32 == 0) return p;
+  return per_block;
+}
+inline void hop_block_shape(int tps, int nrhs, int vh, dim3* blk, dim3* grd) {
+  const int per_block = hop_sites_per_block(tps, nrhs);
   *blk = dim3(per_block * nrhs, tps);
   *grd = dim3((vh + per_block - 1) / per_block);
 }
@@ -550,6 +678,10 @@ inline HopCoef make_hopcoef(const double* c1, const double* c2, int idag) {
     // backward hop: (c1 + c2 gamma) for idag=0, (c1 - c2 gamma) for idag=1
     h.bm[mu] = idag ? a : b;
     h.bp[mu] = idag ? b : a;
+    h.fmf[mu] = (float)h.fm[mu];
+    h.fpf[mu] = (float)h.fp[mu];
+    h.bmf[mu] = (float)h.bm[mu];
+    h.bpf[mu] = (float)h.bp[mu];
   }
   return h;
 }

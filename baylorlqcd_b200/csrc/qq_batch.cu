@@ -349,10 +349,4 @@ int batch_solve(qq_ctx* c, int nrhs, const double* be, const double* bo, const d
   return QQ_OK;
 }
 
-int traces_level0(qq_ctx* c, const double* be, const double* bo, const double* xe,
-                  const double* xo, double kappa, double* J) {
-  (void)c; (void)be; (void)bo; (void)xe; (void)xo; (void)kappa; (void)J;
-  return set_error(QQ_BAD_ARG, "traces not built yet");
-}
-
 }  // namespace qq

@@ -15,7 +15,7 @@ int lagfib_rnds(int m, double* rn);
 int batch_solve(qq_ctx* c, int nrhs, const double* be, const double* bo, const double kappa[2],
                 const qq_method* method, double* xe, double* xo, qq_solve_info* infos);
 int traces_level0(qq_ctx* c, const double* be, const double* bo, const double* xe,
-                  const double* xo, double kappa, double* J);
+                  const double* xo, double kappa, double delta, int dobndry, double* J);
 }  // namespace qq
 
 using namespace qq;
@@ -420,11 +420,11 @@ int qq_fermprop_batch(qq_ctx* c, int nrhs, const double* be, const double* bo, c
 }
 
 int qq_twaverage_level0(qq_ctx* c, const double* be, const double* bo, const double* xe,
-                        const double* xo, double kappa, double* J) {
+                        const double* xo, double kappa, double delta, int dobndry, double* J) {
   QQ_TRY(check_ctx(c));
   QQ_TRY(set_device(c));
   if (!be || !bo || !xe || !xo || !J) return set_error(QQ_BAD_ARG, "null argument");
-  return traces_level0(c, be, bo, xe, xo, kappa, J);
+  return traces_level0(c, be, bo, xe, xo, kappa, delta, dobndry, J);
 }
 
 }  // extern "C"

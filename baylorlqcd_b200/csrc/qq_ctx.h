@@ -96,6 +96,7 @@ struct qq_ctx {
   qq::DevBuf stage[4];      // reference-layout staging buffers
   qq::DevBuf partial;       // reduction partials
   qq::DevBuf scal;          // device scalar slots
+  qq::DevBuf trace_buf;     // per-site loop-trace values and the time-slice sums
   double* hpin = nullptr;   // pinned host mirror of scalar results
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   cudaEvent_t tev0 = nullptr, tev1 = nullptr;       // autotuner timing

@@ -189,12 +189,18 @@ int qq_rnds(int m, double* rn);
 /* z2source :4583-4649 and z4source (active branch) :4518-4570. */
 int qq_z2source(qq_ctx* ctx, double* be, double* bo);
 int qq_z4source(qq_ctx* ctx, double* be, double* bo);
-/* Unsubtracted time-slice traces of one noise solution, the level-0 operators of
- * twAverage (Q/vevbleft.f90:2541-4704): J(2, nt, 6), op 1 = J4 point-split time
+/* Unsubtracted (level-0) time-slice traces of one noise vector: twAverage
+ * (Q/vevbleft.f90:2541-4704) with nsub = 0 and zero momentum, point-split currents of
+ * currentCalc2P (:10863-11247, r = +1), scalarCalc (:9261-9299), and the caller's
+ * kappa scaling of Q/disconloops.f90:4045-4049.  be/bo: the noise (only its real
+ * part enters, as in twAverage); xe/xo: the solution; delta: twist angle (0 for
+ * Wilson); dobndry = 1: fixed time boundary (no time current across it).  Uses the
+ * context's gauge field.  J(2, nt, 6), host or device: op 1 = J4 point-split time
  * current, 2 = psibar psi, 3..5 = J1..J3 point-split spatial currents,
- * 6 = psibar gamma5 psi; kappa scaling of Q/disconloops.f90:4045-4049 applied. */
+ * 6 = psibar gamma5 psi, ops other than 2 and 6 multiplied by kappa.  Averaging over
+ * noises and the division by nx*ny*nz (:4161-4164) are left to the caller. */
 int qq_twaverage_level0(qq_ctx* ctx, const double* be, const double* bo, const double* xe,
-                        const double* xo, double kappa, double* J);
+                        const double* xo, double kappa, double delta, int dobndry, double* J);
 
 /* ---- measurement (library-specific; no counterpart in the reference) ---- */
 /* The cudaStream_t every call of this context runs on (for event timing). */

@@ -68,7 +68,7 @@ def lib() -> C.CDLL:
             "oq_qgenerator": ([I, I, I, DP, I, DP], None),
             "oq_evalues": ([I, I, I, I, DP, I, DP, DP, I], None),
             "oq_orgschur": ([IP, I, DP, I, DP, I, DP, IP], None),
-            "oq_twaverage_level0": ([P, DP, DP, DP, DP, DP, D, DP], None),
+            "oq_twaverage_level0": ([P, DP, DP, DP, DP, DP, D, D, C.c_int, DP], None),
             "oq_set_kcyclim": ([I], None),
             "oq_coldstart": ([P, DP], None),
             "oq_aveplaq": ([P, DP], D),
@@ -267,11 +267,12 @@ class OracleLattice:
         lib().oq_z4source(self._g, _dp(be), _dp(bo))
         return be, bo
 
-    def twaverage_level0(self, be, bo, xe, xo, kappa):
+    def twaverage_level0(self, be, bo, xe, xo, kappa, delta=0.0, dobndry=0):
+        """Level-0 traces of one noise: J[iop, t, re/im] (twAverage, nsub = 0)."""
         J = np.zeros((6, self.dims[3], 2))
         lib().oq_twaverage_level0(self._g, _dp(np.ascontiguousarray(be)), _dp(np.ascontiguousarray(bo)),
                                   _dp(np.ascontiguousarray(xe)), _dp(np.ascontiguousarray(xo)),
-                                  _dp(self.u), float(kappa), _dp(J))
+                                  _dp(self.u), float(kappa), float(delta), int(dobndry), _dp(J))
         return J
 
     # ---- gauge helpers ----

@@ -125,13 +125,15 @@ void oq_evalues(int ischur, int n, int ilo, int ihi, double* h, int ldh, double*
 void oq_orgschur(const int* select, int n, double* t, int ldt, double* q, int ldq,
                  double* w, int* m);
 
-// ---- loop traces (Q/disconloops.f90 loopops/vv/spacesum; Q/vevbleft.f90 twAverage) ----
-// Per-time-slice local bilinears of one noise solution (unsubtracted level).
+// ---- loop traces (Q/vevbleft.f90 twAverage, nsub = 0; see loops.cpp) ----
+// Per-time-slice traces of one noise solution at the unsubtracted level.
 // J is (2, nt, 6) : op 1 = J4 point-split time current, 2 = psibar psi,
-// 3..5 = J1..J3 point-split spatial currents, 6 = psibar gamma5 psi.
+// 3..5 = J1..J3 point-split spatial currents, 6 = psibar gamma5 psi; ops other than
+// 2 and 6 scaled by kappa.  delta: twist angle (0 for Wilson); dobndry = 1: fixed
+// time boundary.
 void oq_twaverage_level0(const oq_geom* g, const double* be, const double* bo,
                          const double* xe, const double* xo, const double* u,
-                         double kappa, double* J);
+                         double kappa, double delta, int dobndry, double* J);
 
 // ---- gauge field helpers ----
 void oq_coldstart(const oq_geom* g, double* u);

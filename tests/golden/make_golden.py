@@ -10,7 +10,9 @@ fixed numbers to meet.  Inputs:
 * GMRES-DR(30,10) (Wilson) and GMRES-DR(20,6) (twisted mass), BiCGStab and
   GMRES-Proj after a deflating first solve (psc), and fermprop with odd
   reconstruction, all on 4x4x4x8 with the Gram-Schmidt gauge field of
-  qqtest.golden_gauge(seed 2026, eps 0.25; plaquette 0.52) and point sources.
+  qqtest.golden_gauge(seed 2026, eps 0.25; plaquette 0.52) and point sources;
+* level-0 loop traces (Q/vevbleft.f90 twAverage, nsub = 0) of the first Z(4) noise
+  after a fermprop solve.
 
 Usage: python tests/golden/make_golden.py   (rewrites golden.json)
 """
@@ -87,6 +89,14 @@ def main():
                                      xo_norm2=float(ol.vecdot(xo, xo).real),
                                      itercount=int(log.itercount))
     out["solves"] = solves
+
+    # level-0 loop traces of the first Z(4) noise (twAverage, nsub = 0)
+    oracle.initlagfib(0, 13)
+    ze, zo = ol.z4source()
+    xe, xo, st, log = ol.fermprop(ze, zo, (0.15, 0.0), inverter=5, resmax=1e-12, nGMRES=(30, 10))
+    J = ol.twaverage_level0(ze, zo, xe, xo, 0.15, 0.0, 0)
+    out["traces_z4_noise1"] = {"kappa": 0.15, "delta": 0.0, "dobndry": 0, "solve": "fermprop GMRES-DR(30,10) 1e-12",
+                               "itercount": int(log.itercount), "J": J.tolist()}
     (HERE / "golden.json").write_text(json.dumps(out, indent=1) + "\n")
     print("wrote", HERE / "golden.json")
 

@@ -100,3 +100,14 @@ def test_fermprop(ol):
     assert log.itercount == rec["itercount"]
     np.testing.assert_allclose(ol.vecdot(xe, xe).real, rec["xe_norm2"], rtol=RTOL)
     np.testing.assert_allclose(ol.vecdot(xo, xo).real, rec["xo_norm2"], rtol=RTOL)
+
+
+def test_traces_z4_noise1(ol):
+    rec = GOLDEN["traces_z4_noise1"]
+    oracle.initlagfib(0, 13)
+    ze, zo = ol.z4source()
+    xe, xo, st, log = ol.fermprop(ze, zo, (rec["kappa"], 0.0), inverter=5, resmax=1e-12, nGMRES=(30, 10))
+    assert log.itercount == rec["itercount"]
+    J = ol.twaverage_level0(ze, zo, xe, xo, rec["kappa"], rec["delta"], rec["dobndry"])
+    want = np.array(rec["J"])
+    assert np.abs(J - want).max() <= RTOL * np.abs(want).max()

@@ -53,7 +53,14 @@ int launch_block_op(qq_ctx* c, const BlockBiArgs& A, int op) {
   return QQ_OK;
 }
 
-int block_op(qq_ctx* c, int prec, const BlockBiArgs& A, int op, const int* dslots, int step) {
+struct ScalarCtl {
+  unsigned* ctl;     // control words (active, pending)
+  double delta;      // reliable-update threshold
+  double half_tol;   // 0.5 * tolerance
+};
+
+int block_op(qq_ctx* c, int prec, const BlockBiArgs& A, int op, const int* dslots, int step,
+             const ScalarCtl& sc) {
   count_launch(step >= 0 ? 2 : 1);
   if (prec == P32)
     QQ_TRY(launch_block_op<P32>(c, A, op));
@@ -62,7 +69,8 @@ int block_op(qq_ctx* c, int prec, const BlockBiArgs& A, int op, const int* dslot
   else
     QQ_TRY(launch_block_op<P64>(c, A, op));
   if (step >= 0) {
-    bicg_scalar_kernel<<<A.nb, 256, 0, c->st>>>(A.S, dslots, A.partial, kRedBlocks, step, A.active);
+    bicg_scalar_kernel<<<A.nb, 256, 0, c->st>>>(A.S, dslots, A.partial, kRedBlocks, step, sc.ctl,
+                                                sc.delta, sc.half_tol);
     QQ_CK(cudaGetLastError());
   }
   return QQ_OK;
@@ -122,10 +130,13 @@ int bicgstab_block(qq_ctx* c, std::vector<PerRhs*>& rhs, int prec, double tol, d
     QQ_CK(cudaMemsetAsync(f->data.p, 0, f->data.bytes, c->st));
     if (prec == P16) QQ_CK(cudaMemsetAsync(f->norm.p, 0, f->norm.bytes, c->st));
   }
+  // scalars of every right-hand side, then the two control words
+  constexpr size_t kScalDoubles = (size_t)kScal * kMaxBatch;
   DevBuf S, part, dslots;
-  QQ_CK(S.alloc(sizeof(double) * kScal * kMaxBatch));
+  QQ_CK(S.alloc(sizeof(double) * (kScalDoubles + 1)));
   QQ_CK(part.alloc(sizeof(double) * 3 * kRedBlocks * kMaxBatch));
   QQ_CK(dslots.alloc(sizeof(int) * kMaxBatch));
+  unsigned* ctl = reinterpret_cast<unsigned*>(S.as<double>() + kScalDoubles);
   Tmp tmp64(c, P64), h(c, P64);
   double* s1 = c->scal.as<double>();
   // FP64 residual of x (and of the deflated x) -> slot k of r and rhat
@@ -142,7 +153,11 @@ int bicgstab_block(qq_ctx* c, std::vector<PerRhs*>& rhs, int prec, double tol, d
     }
     return QQ_OK;
   };
-  std::vector<double> hS(kScal * kMaxBatch, 0.0);
+  // host mirror in the solver's half of the context's pinned buffer
+  static_assert(kScalDoubles + 1 <= 1024, "scalar mirror exceeds the pinned buffer");
+  double* hS = c->hpin + 1024;
+  std::fill(hS, hS + kScalDoubles + 1, 0.0);
+  unsigned* hctl = reinterpret_cast<unsigned*>(hS + kScalDoubles);
   std::vector<int> slots(nb);
   unsigned active = 0;
   for (int k = 0; k < nb; ++k) {
@@ -159,14 +174,19 @@ int bicgstab_block(qq_ctx* c, std::vector<PerRhs*>& rhs, int prec, double tol, d
     QQ_TRY(block_slot(c, prec, nb, k, rhat.sp(), R.r64.sp(), 0));
     double* sc = &hS[(size_t)k * kScal];
     sc[SC_RHO] = sc[SC_ALPHA] = sc[SC_OMEGA] = 1.0;
+    sc[SC_RMAX] = R.rmax;
+    sc[SC_BN] = R.bn;
   }
-  QQ_CK(cudaMemcpyAsync(S.p, hS.data(), sizeof(double) * hS.size(), cudaMemcpyHostToDevice, c->st));
+  hctl[CTL_ACTIVE] = active;
+  hctl[CTL_PENDING] = 0u;
+  QQ_CK(cudaMemcpyAsync(S.p, hS, sizeof(double) * (kScalDoubles + 1), cudaMemcpyHostToDevice, c->st));
   QQ_CK(cudaMemcpyAsync(dslots.p, slots.data(), sizeof(int) * nb, cudaMemcpyHostToDevice, c->st));
   QQ_CK(cudaStreamSynchronize(c->st));
   BlockBiArgs A;
   std::memset(&A, 0, sizeof(A));
   A.vh = c->g.vh;
   A.nb = nb;
+  A.active = ctl + CTL_ACTIVE;
   A.r = r.sp();
   A.rhat = rhat.sp();
   A.p = p.sp();
@@ -177,27 +197,39 @@ int bicgstab_block(qq_ctx* c, std::vector<PerRhs*>& rhs, int prec, double tol, d
   A.S = S.as<double>();
   A.partial = part.as<double>();
   const int* ds = dslots.as<int>();
-  for (int it = 0; it < maxiter && active; ++it) {
-    A.active = active;
-    QQ_TRY(block_op(c, prec, A, OP_DOT_RHAT_R, ds, ST_BETA));
-    QQ_TRY(block_op(c, prec, A, OP_P_UPDATE, ds, -1));
-    QQ_TRY(op_dbletm_block(c, v.sp(), p.sp(), tmp.sp(), nb, 0, kappa));
-    QQ_TRY(block_op(c, prec, A, OP_DOT_RHAT_V, ds, ST_ALPHA));
-    QQ_TRY(block_op(c, prec, A, OP_S_UPDATE, ds, -1));
-    QQ_TRY(op_dbletm_block(c, t.sp(), r.sp(), tmp.sp(), nb, 0, kappa));
-    QQ_TRY(block_op(c, prec, A, OP_DOTS_T, ds, ST_OMEGA));
-    QQ_TRY(block_op(c, prec, A, OP_XR_UPDATE, ds, ST_R2));
-    QQ_CK(cudaMemcpyAsync(hS.data(), S.p, sizeof(double) * kScal * nb, cudaMemcpyDeviceToHost, c->st));
+  const ScalarCtl sc{ctl, delta, 0.5 * tol};
+  // Iterations run in chunks without host synchronisation: a right-hand side whose
+  // residual calls for a reliable update (or may have converged) takes itself out of
+  // the active mask on the device and waits, pending, for the end of the chunk, where
+  // the host does the FP64 update and puts it back.
+  constexpr int kChunk = 4;
+  int done_its = 0;
+  while (active && done_its < maxiter) {
+    const int nchunk = std::min(kChunk, maxiter - done_its);
+    for (int i = 0; i < nchunk; ++i) {
+      QQ_TRY(block_op(c, prec, A, OP_DOT_RHAT_R, ds, ST_BETA, sc));
+      QQ_TRY(block_op(c, prec, A, OP_P_UPDATE, ds, -1, sc));
+      QQ_TRY(op_dbletm_block(c, v.sp(), p.sp(), tmp.sp(), nb, 0, kappa));
+      QQ_TRY(block_op(c, prec, A, OP_DOT_RHAT_V, ds, ST_ALPHA, sc));
+      QQ_TRY(block_op(c, prec, A, OP_S_UPDATE, ds, -1, sc));
+      QQ_TRY(op_dbletm_block(c, t.sp(), r.sp(), tmp.sp(), nb, 0, kappa));
+      QQ_TRY(block_op(c, prec, A, OP_DOTS_T, ds, ST_OMEGA, sc));
+      QQ_TRY(block_op(c, prec, A, OP_XR_UPDATE, ds, ST_R2, sc));
+    }
+    done_its += nchunk;
+    QQ_CK(cudaMemcpyAsync(hS, S.p, sizeof(double) * (kScalDoubles + 1), cudaMemcpyDeviceToHost, c->st));
     QQ_CK(cudaStreamSynchronize(c->st));
+    const unsigned pending = hctl[CTL_PENDING];
+    unsigned back = 0;  // right-hand sides that iterate again after their update
     for (int k = 0; k < nb; ++k) {
-      if (!((active >> k) & 1u)) continue;
       PerRhs& R = *rhs[k];
       SolveStats& st = stats[k];
-      st.itercount += 1;
-      st.mvp += 2;
+      const int its = (int)hS[(size_t)k * kScal + SC_ITS];
+      st.mvp += 2 * (its - st.itercount);
+      st.itercount = its;
+      if (!((pending >> k) & 1u)) continue;
       const double rn = std::sqrt(hS[(size_t)k * kScal + SC_R2]);
       if (!std::isfinite(rn)) return set_error(QQ_NAN, "NaN residual in batched BiCGStab");
-      if (!(rn < delta * R.rmax || rn / R.bn < 0.5 * tol)) continue;
       // reliable update
       QQ_TRY(block_slot(c, prec, nb, k, xl.sp(), R.x.sp(), 1));
       QQ_TRY(block_slot(c, prec, nb, k, xl.sp(), R.x.sp(), 2));
@@ -212,6 +244,14 @@ int bicgstab_block(qq_ctx* c, std::vector<PerRhs*>& rhs, int prec, double tol, d
       }
       QQ_TRY(block_slot(c, prec, nb, k, r.sp(), R.r64.sp(), 0));
       R.rmax = R.rn;
+      hS[(size_t)k * kScal + SC_RMAX] = R.rmax;
+      back |= 1u << k;
+    }
+    if (pending) {
+      active = (hctl[CTL_ACTIVE] | back) & active;
+      hctl[CTL_ACTIVE] = active;
+      hctl[CTL_PENDING] = 0u;
+      QQ_CK(cudaMemcpyAsync(S.p, hS, sizeof(double) * (kScalDoubles + 1), cudaMemcpyHostToDevice, c->st));
     }
   }
   QQ_CK(cudaStreamSynchronize(c->st));

@@ -97,7 +97,8 @@ struct qq_ctx {
   qq::DevBuf partial;       // reduction partials
   qq::DevBuf scal;          // device scalar slots
   qq::DevBuf trace_buf;     // per-site loop-trace values and the time-slice sums
-  double* hpin = nullptr;   // pinned host mirror of scalar results
+  double* hpin = nullptr;   // pinned host memory: [0, 1024) read_scalars staging,
+                            // [1024, 2048) the batched solver's scalar mirror
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   cudaEvent_t tev0 = nullptr, tev1 = nullptr;       // autotuner timing
   std::map<int, int> hop_tune;                       // shape -> threads per site

@@ -20,8 +20,16 @@ enum ScalSlot : int {
   SC_BETA = 6,     // complex beta
   SC_R2 = 8,       // ||r||^2 (iterated residual)
   SC_TT = 9,       // ||t||^2
+  SC_RMAX = 10,    // ||r|| at the last reliable update
+  SC_BN = 11,      // ||b||
+  SC_ITS = 12,     // iterations done
   kScal = 16,
 };
+
+// Control words after the scalar slots: [0] active mask (bit r: right-hand side r
+// iterates), [1] pending mask (bit r: r stopped and waits for the host's reliable
+// update or convergence test).
+enum CtlWord : int { CTL_ACTIVE = 0, CTL_PENDING = 1 };
 
 enum BiOp : int {
   OP_DOT_RHAT_R = 0,  // red: <rhat, r>
@@ -35,7 +43,7 @@ enum BiOp : int {
 struct BlockBiArgs {
   int vh;                      // sites per parity
   int nb;                      // right-hand sides in the block
-  unsigned active;             // bit r set: right-hand side r still iterates
+  const unsigned* active;      // device word, bit r set: right-hand side r iterates
   Spinor r, rhat, p, v, t, x;  // block fields
   int slot[kMaxBatch];         // scalar slot of each right-hand side
   double* S;                   // scalar array
@@ -54,7 +62,7 @@ __global__ void __launch_bounds__(kRedThreads) bicg_block_kernel(BlockBiArgs A) 
   using IO = SpinorIO<P>;
   using R = typename IO::R;
   const int k = threadIdx.x % A.nb;
-  const bool act = (A.active >> k) & 1u;
+  const bool act = (*A.active >> k) & 1u;
   const double* S = A.S + (size_t)A.slot[k] * kScal;
   double acc[3] = {0.0, 0.0, 0.0};
   const cplx<double> alpha{S[SC_ALPHA], S[SC_ALPHA + 1]}, omega{S[SC_OMEGA], S[SC_OMEGA + 1]},
@@ -143,9 +151,14 @@ enum ScalStep : int {
   ST_R2 = 3,     // ||r||^2
 };
 
-// one block per right-hand side: sum the partials (fixed order), update the scalars
+// One block per right-hand side: sum the partials (fixed order), update the scalars.
+// At ST_R2 it also counts the iteration and, when ||r|| has dropped below delta times
+// its value at the last reliable update or below half_tol ||b|| (or is not finite),
+// takes the right-hand side out of the active mask and marks it pending, so the
+// iteration needs no host round trip until the host next looks.
 static __global__ void bicg_scalar_kernel(double* S, const int* slots, const double* partial,
-                                          int nblocks, int step, unsigned active) {
+                                          int nblocks, int step, unsigned* ctl, double delta,
+                                          double half_tol) {
   const int k = blockIdx.x;
   __shared__ double red[3][256];
   double a[3] = {0.0, 0.0, 0.0};
@@ -158,7 +171,7 @@ static __global__ void bicg_scalar_kernel(double* S, const int* slots, const dou
       for (int q = 0; q < 3; ++q) red[q][threadIdx.x] += red[q][threadIdx.x + o];
     __syncthreads();
   }
-  if (threadIdx.x != 0 || !((active >> k) & 1u)) return;
+  if (threadIdx.x != 0 || !((ctl[CTL_ACTIVE] >> k) & 1u)) return;
   double* s = S + (size_t)slots[k] * kScal;
   const double d0 = red[0][0], d1 = red[1][0], d2 = red[2][0];
   auto cdiv = [](double ar, double ai, double br, double bi, double* cr, double* ci) {
@@ -182,6 +195,12 @@ static __global__ void bicg_scalar_kernel(double* S, const int* slots, const dou
     s[SC_TT] = d2;
   } else {
     s[SC_R2] = d0;
+    s[SC_ITS] += 1.0;
+    const double rn = sqrt(d0);
+    if (!isfinite(rn) || rn < delta * s[SC_RMAX] || rn < half_tol * s[SC_BN]) {
+      atomicAnd(&ctl[CTL_ACTIVE], ~(1u << k));
+      atomicOr(&ctl[CTL_PENDING], 1u << k);
+    }
   }
 }
 

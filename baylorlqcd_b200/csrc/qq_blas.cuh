@@ -161,6 +161,8 @@ template <>
 struct BasisIO<P64> {
   using V = double2;
   static constexpr int ncpx = 1;
+  // spinor component held in slot t of plane q
+  __device__ static constexpr int comp(int q, int t) { return q + t; }
   __device__ static inline void ld(const V* p, size_t e, cplx<double>* c) {
     V t = p[e];
     c[0] = {t.x, t.y};
@@ -170,16 +172,17 @@ struct BasisIO<P64> {
   }
 };
 template <>
-struct BasisIO<P32> {
+struct BasisIO<P32> {  // the spin-paired planes of SpinorIO<P32>
   using V = float4;
   static constexpr int ncpx = 2;
+  __device__ static constexpr int comp(int q, int t) { return p32_first(q) + 3 * t; }
   __device__ static inline void ld(const V* p, size_t e, cplx<double>* c) {
     V t = p[e];
-    c[0] = {t.x, t.y};
-    c[1] = {t.z, t.w};
+    c[0] = {t.x, t.z};
+    c[1] = {t.y, t.w};
   }
   __device__ static inline void st(V* p, size_t e, const cplx<double>* c) {
-    p[e] = make_float4((float)c[0].re, (float)c[0].im, (float)c[1].re, (float)c[1].im);
+    p[e] = make_float4((float)c[0].re, (float)c[1].re, (float)c[0].im, (float)c[1].im);
   }
 };
 
@@ -369,7 +372,7 @@ __global__ void __launch_bounds__(kRedThreads) basis_accum_kernel(BasisArgs V, i
         IO::ld(v, (size_t)q * vh + s, vc);
 #pragma unroll
         for (int t = 0; t < IO::ncpx; ++t) {
-          const int c = q * IO::ncpx + t;
+          const int c = IO::comp(q, t);
           acc[c].re += yr * vc[t].re - yi * vc[t].im;
           acc[c].im += yr * vc[t].im + yi * vc[t].re;
         }

@@ -26,6 +26,7 @@ enum Epilogue : int {
 constexpr int kMaxRhs = 8;     // right-hand sides per launch, separate fields
 constexpr int kMaxBatch = 32;  // right-hand sides per launch, one block field
 constexpr int kShapeMrhs = 200;  // kernel-shape code base of hop_mrhs_kernel (200 + RPT)
+constexpr int kShapeF2 = 300;    // kernel-shape code base of hop_f2_kernel (300 + RPT)
 
 struct HopArgs {
   Geom g;
@@ -429,13 +430,14 @@ struct SlotSpinor<P64> {
   }
 };
 template <>
-struct SlotSpinor<P32> {
+struct SlotSpinor<P32> {  // the spin-paired planes of SpinorIO<P32>
   __device__ static inline void load(const uint4* slot, int T, cplx<float>* v) {
 #pragma unroll
     for (int q = 0; q < 6; ++q) {
       const float4 t = *reinterpret_cast<const float4*>(slot + q * T);
-      v[2 * q] = {t.x, t.y};
-      v[2 * q + 1] = {t.z, t.w};
+      const int a = p32_first(q);
+      v[a] = {t.x, t.z};
+      v[a + 3] = {t.y, t.w};
     }
   }
 };

@@ -1,0 +1,239 @@
+// Wilson hopping term for FP32 spinors with packed FP32x2 arithmetic (sm_100).
+//
+// SpinorIO<P32> stores spin pairs: plane q < 3 is colour q of spins (0, 1), plane
+// q >= 3 colour q - 3 of spins (2, 3), as (a.re, b.re, a.im, b.im).  One 16-byte load
+// therefore gives the pair of real parts and the pair of imaginary parts of a spin
+// pair in adjacent registers.  A hop acts on a half spinor whose two rows (h0, h1) are
+// built from the spin pairs (0, 1) and (2, 3) and are multiplied by the same SU(3)
+// link, so every step of the hop -- projection, the link product and the
+// reconstruction -- runs on (h0, h1) pairs with __ffma2_rn / __fmul2_rn: one packed
+// instruction does the work of two scalar ones, and the link's entries are broadcast
+// into pairs once per direction and shared by the RPT right-hand sides of the thread.
+// The projector decompositions and sign patterns are those of project() /
+// reconstruct_acc() in qq_dslash.cuh, regrouped by spin pair.
+#pragma once
+#include "qq_dslash.cuh"
+
+namespace qq {
+
+__device__ inline float2 f2fma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ inline float2 f2mul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ inline float2 f2swap(float2 a) { return make_float2(a.y, a.x); }
+__device__ inline float2 f2bc(float a) { return make_float2(a, a); }
+
+// Spinor as spin pairs: p[0..2] = spins (0,1) colour c, p[3..5] = spins (2,3); re and im pairs.
+struct Pair12 {
+  float2 re[6], im[6];
+};
+
+__device__ inline void load_pairs(const float4* f, int n, int idx, Pair12& p) {
+#pragma unroll
+  for (int q = 0; q < 6; ++q) {
+    const float4 t = __ldg(f + (size_t)q * n + idx);
+    p.re[q] = make_float2(t.x, t.y);
+    p.im[q] = make_float2(t.z, t.w);
+  }
+}
+__device__ inline void store_pairs(float4* f, int n, int idx, const Pair12& p) {
+#pragma unroll
+  for (int q = 0; q < 6; ++q) f[(size_t)q * n + idx] = make_float4(p.re[q].x, p.re[q].y, p.im[q].x, p.im[q].y);
+}
+
+// Matrix M (= U forward, U^+ backward) as broadcast pairs.
+struct LinkPairs {
+  float2 r[3][3], i[3][3];
+};
+
+template <bool FWD>
+__device__ inline void link_pairs(const Su3<float>& u, LinkPairs& m) {
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int b = 0; b < 3; ++b) {
+      const cplx<float> e = FWD ? u.e[a][b] : u.e[b][a];
+      m.r[a][b] = f2bc(e.re);
+      m.i[a][b] = f2bc(FWD ? e.im : -e.im);
+    }
+}
+
+// (h0, h1) = projection of psi for direction MU and sign S (unscaled; MU = 3 omits its 2)
+template <int MU, int S>
+__device__ inline void project2(const Pair12& p, float2* hre, float2* him) {
+  constexpr float s = (float)S;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    if (MU == 0) {
+      hre[c] = f2fma(f2bc(s), f2swap(p.re[3 + c]), p.re[c]);
+      him[c] = f2fma(f2bc(s), f2swap(p.im[3 + c]), p.im[c]);
+    } else if (MU == 1) {
+      hre[c] = f2fma(make_float2(s, -s), f2swap(p.im[3 + c]), p.re[c]);
+      him[c] = f2fma(make_float2(-s, s), f2swap(p.re[3 + c]), p.im[c]);
+    } else if (MU == 2) {
+      hre[c] = f2fma(make_float2(s, -s), p.re[3 + c], p.re[c]);
+      him[c] = f2fma(make_float2(s, -s), p.im[3 + c], p.im[c]);
+    } else {
+      hre[c] = S < 0 ? p.re[3 + c] : p.re[c];
+      him[c] = S < 0 ? p.im[3 + c] : p.im[c];
+    }
+  }
+}
+
+// w = M h on both rows at once
+__device__ inline void matvec2(const LinkPairs& m, const float2* hre, const float2* him, float2* wre,
+                               float2* wim) {
+  float2 nhim[3];
+#pragma unroll
+  for (int b = 0; b < 3; ++b) nhim[b] = f2mul(f2bc(-1.0f), him[b]);
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    float2 xr = f2mul(m.r[a][0], hre[0]);
+    float2 xi = f2mul(m.r[a][0], him[0]);
+    xr = f2fma(m.i[a][0], nhim[0], xr);
+    xi = f2fma(m.i[a][0], hre[0], xi);
+#pragma unroll
+    for (int b = 1; b < 3; ++b) {
+      xr = f2fma(m.r[a][b], hre[b], xr);
+      xr = f2fma(m.i[a][b], nhim[b], xr);
+      xi = f2fma(m.r[a][b], him[b], xi);
+      xi = f2fma(m.i[a][b], hre[b], xi);
+    }
+    wre[a] = xr;
+    wim[a] = xi;
+  }
+}
+
+// acc += k * reconstruct(w) for direction MU and sign S
+template <int MU, int S>
+__device__ inline void recon2(Pair12& acc, float k, const float2* wre, const float2* wim) {
+  const float ks = k * (float)S;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    if (MU == 3) {
+      const int q = S < 0 ? 3 + c : c;
+      acc.re[q] = f2fma(f2bc(k), wre[c], acc.re[q]);
+      acc.im[q] = f2fma(f2bc(k), wim[c], acc.im[q]);
+      continue;
+    }
+    acc.re[c] = f2fma(f2bc(k), wre[c], acc.re[c]);
+    acc.im[c] = f2fma(f2bc(k), wim[c], acc.im[c]);
+    if (MU == 0) {
+      acc.re[3 + c] = f2fma(f2bc(ks), f2swap(wre[c]), acc.re[3 + c]);
+      acc.im[3 + c] = f2fma(f2bc(ks), f2swap(wim[c]), acc.im[3 + c]);
+    } else if (MU == 1) {
+      acc.re[3 + c] = f2fma(make_float2(ks, -ks), f2swap(wim[c]), acc.re[3 + c]);
+      acc.im[3 + c] = f2fma(make_float2(-ks, ks), f2swap(wre[c]), acc.im[3 + c]);
+    } else {
+      acc.re[3 + c] = f2fma(make_float2(ks, -ks), wre[c], acc.re[3 + c]);
+      acc.im[3 + c] = f2fma(make_float2(ks, -ks), wim[c], acc.im[3 + c]);
+    }
+  }
+}
+
+// One direction's hops (forward or backward) for the thread's RPT right-hand sides.
+template <int MU, bool FWD, int RPT>
+__device__ inline void hop2(const HopArgs& a, int s, int r0, int G, const int* x, Pair12* acc) {
+  int y[4] = {x[0], x[1], x[2], x[3]};
+  float sgn = 1.0f;
+  if (FWD) {
+    y[MU] += 1;
+    if (y[MU] == a.g.n[MU]) {
+      y[MU] = 0;
+      sgn = a.g.bcf[MU];
+    }
+  } else {
+    y[MU] -= 1;
+    if (y[MU] < 0) {
+      y[MU] = a.g.n[MU] - 1;
+      sgn = a.g.bcf[MU];
+    }
+  }
+  if (sgn == 0.0f) return;
+  const int sy = site_index(a.g, y);
+  const float twice = MU == 3 ? 2.0f : 1.0f;
+  const float cm = twice * sgn * (FWD ? a.c.fmf[MU] : a.c.bmf[MU]);
+  const float cp = twice * sgn * (FWD ? a.c.fpf[MU] : a.c.bpf[MU]);
+  Su3<float> u;
+  if (FWD)
+    LinkIO<P32, 12>::load(a.gauge, a.g.vh, a.pout, MU, s, u);
+  else
+    LinkIO<P32, 12>::load(a.gauge, a.g.vh, 1 - a.pout, MU, sy, u);
+  LinkPairs m;
+  link_pairs<FWD>(u, m);
+  const int n = a.vh_of();
+#pragma unroll
+  for (int k = 0; k < RPT; ++k) {
+    const int r = r0 + k * G;
+    Pair12 p;
+    load_pairs(static_cast<const float4*>(a.in_base(r)), n, a.idx_of(sy, r), p);
+    float2 hre[3], him[3], wre[3], wim[3];
+    if (cm != 0.0f) {
+      project2<MU, -1>(p, hre, him);
+      matvec2(m, hre, him, wre, wim);
+      recon2<MU, -1>(acc[k], cm, wre, wim);
+    }
+    if (cp != 0.0f) {
+      project2<MU, +1>(p, hre, him);
+      matvec2(m, hre, him, wre, wim);
+      recon2<MU, +1>(acc[k], cp, wre, wim);
+    }
+  }
+}
+
+template <int EPI>
+__device__ inline void finish2(const HopArgs& a, int s, int r, const Pair12& acc) {
+  Pair12 o;
+  if (EPI == EPI_STORE) {
+    o = acc;
+  } else if (EPI == EPI_TWIST) {
+    const float t = a.af;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      o.re[c] = f2fma(f2bc(-t), acc.re[3 + c], acc.re[c]);
+      o.im[c] = f2fma(f2bc(-t), acc.im[3 + c], acc.im[c]);
+      o.re[3 + c] = f2fma(f2bc(t), acc.re[c], acc.re[3 + c]);
+      o.im[3 + c] = f2fma(f2bc(t), acc.im[c], acc.im[3 + c]);
+    }
+  } else {
+    Pair12 g;
+    load_pairs(static_cast<const float4*>(a.blk ? a.aux[0] : a.aux[r]), a.vh_of(), a.idx_of(s, r), g);
+    const float2 f1 = f2bc(a.f1f), f2 = f2bc(a.f2f), nf2 = f2bc(-a.f2f), nf3 = f2bc(-a.f3f);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      o.re[c] = f2fma(nf3, acc.re[c], f2fma(f2, g.re[3 + c], f2mul(f1, g.re[c])));
+      o.im[c] = f2fma(nf3, acc.im[c], f2fma(f2, g.im[3 + c], f2mul(f1, g.im[c])));
+      o.re[3 + c] = f2fma(nf3, acc.re[3 + c], f2fma(nf2, g.re[c], f2mul(f1, g.re[3 + c])));
+      o.im[3 + c] = f2fma(nf3, acc.im[3 + c], f2fma(nf2, g.im[c], f2mul(f1, g.im[3 + c])));
+    }
+  }
+  store_pairs(static_cast<float4*>(a.blk ? a.out[0] : a.out[r]), a.vh_of(), a.idx_of(s, r), o);
+}
+
+// Thread layout as hop_mrhs_kernel: threadIdx.x = (site-in-block) * G + j, G = nrhs / RPT.
+template <int RPT, int EPI>
+__global__ void __launch_bounds__(128) hop_f2_kernel(HopArgs a) {
+  const int G = a.nrhs / RPT;
+  const int tx = threadIdx.x;
+  const int sl = a.div_nrhs.div(tx);  // divides by G for this kernel
+  const int j = tx - sl * G;
+  const int s = blockIdx.x * a.per_block + sl;
+  if (s >= a.g.vh || sl >= a.per_block) return;
+  Pair12 acc[RPT];
+#pragma unroll
+  for (int k = 0; k < RPT; ++k)
+#pragma unroll
+    for (int q = 0; q < 6; ++q) acc[k].re[q] = acc[k].im[q] = make_float2(0.0f, 0.0f);
+  int x[4];
+  site_coords(a.g, a.pout, s, x);
+  hop2<0, true, RPT>(a, s, j, G, x, acc);
+  hop2<0, false, RPT>(a, s, j, G, x, acc);
+  hop2<1, true, RPT>(a, s, j, G, x, acc);
+  hop2<1, false, RPT>(a, s, j, G, x, acc);
+  hop2<2, true, RPT>(a, s, j, G, x, acc);
+  hop2<2, false, RPT>(a, s, j, G, x, acc);
+  hop2<3, true, RPT>(a, s, j, G, x, acc);
+  hop2<3, false, RPT>(a, s, j, G, x, acc);
+#pragma unroll
+  for (int k = 0; k < RPT; ++k) finish2<EPI>(a, s, j + k * G, acc[k]);
+}
+
+}  // namespace qq

@@ -32,6 +32,14 @@ struct SpinorIO<P64> {
   }
 };
 
+// FP32 planes hold spin pairs: plane q < 3 is colour q of spins (0, 1), plane q >= 3
+// colour q - 3 of spins (2, 3), each float4 = (a.re, b.re, a.im, b.im) for the pair
+// (a, b = a + 3) of component indices (spin * 3 + colour).  The real parts and the
+// imaginary parts of a spin pair are then adjacent registers, so the Dirac operator
+// applies the projections and SU(3) products to both halves of a half spinor with
+// packed FP32x2 instructions.
+__host__ __device__ constexpr int p32_first(int q) { return q < 3 ? q : q + 3; }
+
 template <>
 struct SpinorIO<P32> {
   using R = float;
@@ -43,15 +51,18 @@ struct SpinorIO<P32> {
 #pragma unroll
     for (int q = 0; q < 6; ++q) {
       float4 t = __ldg(f + (size_t)q * vh + s);
-      v[2 * q] = {t.x, t.y};
-      v[2 * q + 1] = {t.z, t.w};
+      const int a = p32_first(q);
+      v[a] = {t.x, t.z};
+      v[a + 3] = {t.y, t.w};
     }
   }
   __device__ static inline void store(void* base, float*, int vh, int s, const cplx<R>* v) {
     float4* f = static_cast<float4*>(base);
 #pragma unroll
-    for (int q = 0; q < 6; ++q)
-      f[(size_t)q * vh + s] = make_float4(v[2 * q].re, v[2 * q].im, v[2 * q + 1].re, v[2 * q + 1].im);
+    for (int q = 0; q < 6; ++q) {
+      const int a = p32_first(q);
+      f[(size_t)q * vh + s] = make_float4(v[a].re, v[a + 3].re, v[a].im, v[a + 3].im);
+    }
   }
 };
 

@@ -3,6 +3,7 @@
 
 #include "qq_blas.cuh"
 #include "qq_dslash.cuh"
+#include "qq_dslash_f2.cuh"
 #include "qq_launch.h"
 #include "qq_layout.cuh"
 
@@ -104,14 +105,42 @@ static cudaError_t hop_mrhs(const HopArgs& a, int epi, int rpt, cudaStream_t st)
   }
 }
 
+// FP32 spinors, packed FP32x2 arithmetic, RPT right-hand sides per thread.
+template <int RPT>
+static cudaError_t hop_f2_rpt(const HopArgs& a, int epi, cudaStream_t st) {
+  const int G = a.nrhs / RPT;  // threads per site
+  const int per_block = hop_sites_per_block(1, G);
+  const HopArgs b = hop_prepare(a, per_block, G);
+  const dim3 blk(per_block * G), grd((a.g.vh + per_block - 1) / per_block);
+  switch (epi) {
+    case EPI_STORE: hop_f2_kernel<RPT, EPI_STORE><<<grd, blk, 0, st>>>(b); break;
+    case EPI_TWIST: hop_f2_kernel<RPT, EPI_TWIST><<<grd, blk, 0, st>>>(b); break;
+    case EPI_DBLE: hop_f2_kernel<RPT, EPI_DBLE><<<grd, blk, 0, st>>>(b); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
 // tps: 1, 2, 4 = register kernel with that many direction groups per site;
 // 32, 64, 96, 128 = staged kernel with that many threads per block;
 // kShapeMrhs + RPT (RPT = 2, 3, 4) = block fields with RPT right-hand sides per thread
-// (FP32 / FP16 spinors, nrhs divisible by RPT).
+// (FP32 / FP16 spinors, nrhs divisible by RPT);
+// kShapeF2 + RPT (RPT = 1, 2, 3) = FP32 spinors with packed FP32x2 arithmetic (RPT > 1
+// on block fields only).
 cudaError_t launch_hop(const HopArgs& a, int sp, int recon, int epi, int tps, cudaStream_t st) {
   count_launch();
   const int maxr = a.blk ? kMaxBatch : kMaxRhs;
   if (a.nrhs < 1 || a.nrhs > maxr) return cudaErrorInvalidValue;
+  if (tps > kShapeF2) {
+    const int rpt = tps - kShapeF2;
+    if (sp != P32 || a.nrhs % rpt != 0 || (rpt > 1 && !a.blk)) return cudaErrorInvalidValue;
+    switch (rpt) {
+      case 1: return hop_f2_rpt<1>(a, epi, st);
+      case 2: return hop_f2_rpt<2>(a, epi, st);
+      case 3: return hop_f2_rpt<3>(a, epi, st);
+      default: return cudaErrorInvalidValue;
+    }
+  }
   if (tps > kShapeMrhs) {
     const int rpt = tps - kShapeMrhs;
     if (!a.blk || rpt < 2 || a.nrhs % rpt != 0) return cudaErrorInvalidValue;

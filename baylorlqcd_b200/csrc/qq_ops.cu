@@ -156,10 +156,16 @@ int launch_hop_tuned(qq_ctx* c, const HopArgs& a, int prec, int epi) {
   }
   int best = 1;
   float best_ms = 1e30f;
-  for (int tps : {1, 2, 32, 64, 96, 128, kShapeMrhs + 2, kShapeMrhs + 3, kShapeMrhs + 4}) {
+  for (int tps : {1, 2, 32, 64, 96, 128, kShapeMrhs + 2, kShapeMrhs + 3, kShapeMrhs + 4, kShapeF2 + 1,
+                  kShapeF2 + 2, kShapeF2 + 3}) {
     const int per = tps <= 4 ? 128 / tps : tps;
     if (a.nrhs > per) continue;
-    if (tps > kShapeMrhs && (!a.blk || prec == P64 || a.nrhs % (tps - kShapeMrhs) != 0)) continue;
+    if (tps > kShapeF2) {
+      const int rpt = tps - kShapeF2;
+      if (prec != P32 || a.nrhs % rpt != 0 || (rpt > 1 && !a.blk)) continue;
+    } else if (tps > kShapeMrhs && (!a.blk || prec == P64 || a.nrhs % (tps - kShapeMrhs) != 0)) {
+      continue;
+    }
     if (launch_hop(a, prec, recon, epi, tps, c->st) != cudaSuccess) {  // warm-up
       cudaGetLastError();  // shape not launchable (shared memory): skip it
       continue;

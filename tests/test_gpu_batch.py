@@ -83,12 +83,15 @@ def test_heatbath_plaquette(setup):
     lat.close()
 
 
-@pytest.mark.parametrize("shape", [1, 202, 203, 204])
-@pytest.mark.parametrize("precision", [32, 16])
-def test_block_kernel_shapes(setup, monkeypatch, shape, precision):
-    """Each hopping-kernel shape on 12-RHS block fields (one RHS per thread; 2, 3 or 4
-    RHS per thread sharing links and neighbour indices), forced for the whole solve:
-    same converged answers as the oracle."""
+@pytest.mark.parametrize("shape,precision,deflate", [(1, 32, 0), (202, 32, 0), (203, 32, 0), (204, 32, 0),
+                                                      (1, 16, 0), (202, 16, 0), (203, 16, 0), (204, 16, 0),
+                                                      (301, 32, 0), (302, 32, 0), (303, 32, 0), (301, 32, 1)])
+def test_block_kernel_shapes(setup, monkeypatch, shape, precision, deflate):
+    """Each hopping-kernel shape, forced for the whole solve where the launch supports
+    it: one RHS per thread; 2, 3 or 4 RHS per thread sharing links and neighbour
+    indices; the packed FP32x2 kernel with 1-3 RHS per thread (with deflate = 1 also on
+    the single-RHS FP32 launches of the mixed-precision GMRES-DR).  Same converged
+    answers as the oracle."""
     import baylorlqcd_b200 as qq
 
     _, ol, u = setup
@@ -98,8 +101,8 @@ def test_block_kernel_shapes(setup, monkeypatch, shape, precision):
         lat.gauge_upload(u)
         be, bo = sources(lat, 12)
         kappa = (0.150, 0.01)
-        xe, xo, infos = lat.fermprop_batch(be, bo, kappa, precision=precision, rhs_block=12, tol=1e-10,
-                                           solver=1, deflate=0)
+        xe, xo, infos = lat.fermprop_batch(be, bo, kappa, m=16, k=6, precision=precision, rhs_block=12,
+                                           tol=1e-10, solver=1, deflate=deflate)
         for i in range(12):
             assert infos[i].status == 0 and infos[i].true_rel <= 1e-10, (i, infos[i])
         for i in (0, 7, 11):

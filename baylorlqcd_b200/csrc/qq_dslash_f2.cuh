@@ -208,6 +208,113 @@ __device__ inline void finish2(const HopArgs& a, int s, int r, const Pair12& acc
   store_pairs(static_cast<float4*>(a.blk ? a.out[0] : a.out[r]), a.vh_of(), a.idx_of(s, r), o);
 }
 
+// ---------------------------------------------------------------------------
+// Software-pipelined variant (one RHS per thread): the loads of the next hop (its
+// link and neighbour spinor, 9 x 16 bytes) are issued before the current hop is
+// computed, so every warp keeps two hops of loads in flight instead of one.
+// ---------------------------------------------------------------------------
+struct HopLoad {
+  float4 u[3];
+  float4 p[6];
+  float sgn;
+};
+
+template <int MU, bool FWD>
+__device__ inline void hop_issue(const HopArgs& a, int s, int r, const int* x, HopLoad& L) {
+  int y[4] = {x[0], x[1], x[2], x[3]};
+  L.sgn = 1.0f;
+  if (FWD) {
+    y[MU] += 1;
+    if (y[MU] == a.g.n[MU]) {
+      y[MU] = 0;
+      L.sgn = a.g.bcf[MU];
+    }
+  } else {
+    y[MU] -= 1;
+    if (y[MU] < 0) {
+      y[MU] = a.g.n[MU] - 1;
+      L.sgn = a.g.bcf[MU];
+    }
+  }
+  const int sy = site_index(a.g, y);
+  const float4* gl = static_cast<const float4*>(a.gauge) +
+                     (size_t)((FWD ? a.pout : 1 - a.pout) * 4 + MU) * 3 * a.g.vh + (FWD ? s : sy);
+#pragma unroll
+  for (int q = 0; q < 3; ++q) L.u[q] = __ldg(gl + (size_t)q * a.g.vh);
+  const float4* f = static_cast<const float4*>(a.in_base(r));
+  const int n = a.vh_of(), idx = a.idx_of(sy, r);
+#pragma unroll
+  for (int q = 0; q < 6; ++q) L.p[q] = __ldg(f + (size_t)q * n + idx);
+}
+
+template <int MU, bool FWD>
+__device__ inline void hop_consume(const HopArgs& a, const HopLoad& L, Pair12& acc) {
+  if (L.sgn == 0.0f) return;
+  const float twice = MU == 3 ? 2.0f : 1.0f;
+  const float cm = twice * L.sgn * (FWD ? a.c.fmf[MU] : a.c.bmf[MU]);
+  const float cp = twice * L.sgn * (FWD ? a.c.fpf[MU] : a.c.bpf[MU]);
+  Su3<float> u;  // the layout of LinkIO<P32, 12>
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    const int c0 = 2 * q, c1 = 2 * q + 1;
+    u.e[c0 / 3][c0 % 3] = {L.u[q].x, L.u[q].y};
+    u.e[c1 / 3][c1 % 3] = {L.u[q].z, L.u[q].w};
+  }
+  reconstruct_row3(u);
+  LinkPairs m;
+  link_pairs<FWD>(u, m);
+  Pair12 p;
+#pragma unroll
+  for (int q = 0; q < 6; ++q) {
+    p.re[q] = make_float2(L.p[q].x, L.p[q].y);
+    p.im[q] = make_float2(L.p[q].z, L.p[q].w);
+  }
+  float2 hre[3], him[3], wre[3], wim[3];
+  if (cm != 0.0f) {
+    project2<MU, -1>(p, hre, him);
+    matvec2(m, hre, him, wre, wim);
+    recon2<MU, -1>(acc, cm, wre, wim);
+  }
+  if (cp != 0.0f) {
+    project2<MU, +1>(p, hre, him);
+    matvec2(m, hre, him, wre, wim);
+    recon2<MU, +1>(acc, cp, wre, wim);
+  }
+}
+
+template <int EPI>
+__global__ void __launch_bounds__(128) hop_f2p_kernel(HopArgs a) {
+  const int G = a.nrhs;
+  const int tx = threadIdx.x;
+  const int sl = a.div_nrhs.div(tx);
+  const int r = tx - sl * G;
+  const int s = blockIdx.x * a.per_block + sl;
+  if (s >= a.g.vh || sl >= a.per_block) return;
+  Pair12 acc;
+#pragma unroll
+  for (int q = 0; q < 6; ++q) acc.re[q] = acc.im[q] = make_float2(0.0f, 0.0f);
+  int x[4];
+  site_coords(a.g, a.pout, s, x);
+  HopLoad A, B;
+  hop_issue<0, true>(a, s, r, x, A);
+  hop_issue<0, false>(a, s, r, x, B);
+  hop_consume<0, true>(a, A, acc);
+  hop_issue<1, true>(a, s, r, x, A);
+  hop_consume<0, false>(a, B, acc);
+  hop_issue<1, false>(a, s, r, x, B);
+  hop_consume<1, true>(a, A, acc);
+  hop_issue<2, true>(a, s, r, x, A);
+  hop_consume<1, false>(a, B, acc);
+  hop_issue<2, false>(a, s, r, x, B);
+  hop_consume<2, true>(a, A, acc);
+  hop_issue<3, true>(a, s, r, x, A);
+  hop_consume<2, false>(a, B, acc);
+  hop_issue<3, false>(a, s, r, x, B);
+  hop_consume<3, true>(a, A, acc);
+  hop_consume<3, false>(a, B, acc);
+  finish2<EPI>(a, s, r, acc);
+}
+
 // Thread layout as hop_mrhs_kernel: threadIdx.x = (site-in-block) * G + j, G = nrhs / RPT.
 template <int RPT, int EPI>
 __global__ void __launch_bounds__(128) hop_f2_kernel(HopArgs a) {

@@ -157,10 +157,12 @@ int launch_hop_tuned(qq_ctx* c, const HopArgs& a, int prec, int epi) {
   int best = 1;
   float best_ms = 1e30f;
   for (int tps : {1, 2, 32, 64, 96, 128, kShapeMrhs + 2, kShapeMrhs + 3, kShapeMrhs + 4, kShapeF2 + 1,
-                  kShapeF2 + 2, kShapeF2 + 3}) {
+                  kShapeF2 + 2, kShapeF2 + 3, kShapeF2 + 4}) {
     const int per = tps <= 4 ? 128 / tps : tps;
     if (a.nrhs > per) continue;
-    if (tps > kShapeF2) {
+    if (tps == kShapeF2 + 4) {  // pipelined packed kernel, one RHS per thread
+      if (prec != P32) continue;
+    } else if (tps > kShapeF2) {
       const int rpt = tps - kShapeF2;
       if (prec != P32 || a.nrhs % rpt != 0 || (rpt > 1 && !a.blk)) continue;
     } else if (tps > kShapeMrhs && (!a.blk || prec == P64 || a.nrhs % (tps - kShapeMrhs) != 0)) {

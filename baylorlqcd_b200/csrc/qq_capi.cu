@@ -88,7 +88,7 @@ int qq_ctx_create(const qq_geom* geom, int device, qq_ctx** out) {
   auto* c = new qq_ctx();
   c->device = device;
   if (const char* f = std::getenv("QQ_FORCE_TPS")) c->forced_tps = std::atoi(f);  // testing
-  if (c->forced_tps < 0 || c->forced_tps > kShapeF2 + 4) c->forced_tps = 0;
+  if (c->forced_tps < 0 || c->forced_tps > kShapeF2 + 5) c->forced_tps = 0;
   for (int mu = 0; mu < 4; ++mu) {
     c->g.n[mu] = n[mu];
     c->g.bc[mu] = geom->bc[mu];
@@ -450,7 +450,7 @@ extern "C" int qq_bench_hsingle(qq_ctx* c, int precision, int nrhs, int tps, int
   QQ_TRY(set_device(c));
   if (!c->have_gauge) return set_error(QQ_BAD_ARG, "no gauge field uploaded");
   const int prec = precision == 64 ? P64 : precision == 32 ? P32 : precision == 16 ? P16 : -1;
-  if (prec < 0 || nrhs < 1 || nrhs > kMaxBatch || niter < 1 || tps < 0 || tps > kShapeF2 + 4)
+  if (prec < 0 || nrhs < 1 || nrhs > kMaxBatch || niter < 1 || tps < 0 || tps > kShapeF2 + 5)
     return set_error(QQ_BAD_ARG, "bad benchmark arguments");
   const int vh = c->g.vh;
   // nrhs > 1: one RHS-interleaved block field of nrhs right-hand sides (the layout of

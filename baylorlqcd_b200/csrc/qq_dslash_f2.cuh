@@ -248,6 +248,31 @@ __device__ inline void hop_issue(const HopArgs& a, int s, int r, const int* x, H
 }
 
 template <int MU, bool FWD>
+__device__ inline void hop_issue_spinor(const HopArgs& a, int s, int r, const int* x, HopLoad& L) {
+  int y[4] = {x[0], x[1], x[2], x[3]};
+  L.sgn = 1.0f;
+  if (FWD) {
+    y[MU] += 1;
+    if (y[MU] == a.g.n[MU]) {
+      y[MU] = 0;
+      L.sgn = a.g.bcf[MU];
+    }
+  } else {
+    y[MU] -= 1;
+    if (y[MU] < 0) {
+      y[MU] = a.g.n[MU] - 1;
+      L.sgn = a.g.bcf[MU];
+    }
+  }
+  const int sy = site_index(a.g, y);
+  const float4* f = static_cast<const float4*>(a.in_base(r));
+  const int n = a.vh_of(), idx = a.idx_of(sy, r);
+#pragma unroll
+  for (int q = 0; q < 6; ++q) L.p[q] = __ldg(f + (size_t)q * n + idx);
+  (void)s;
+}
+
+template <int MU, bool FWD>
 __device__ inline void hop_consume(const HopArgs& a, const HopLoad& L, Pair12& acc) {
   if (L.sgn == 0.0f) return;
   const float twice = MU == 3 ? 2.0f : 1.0f;
@@ -312,6 +337,76 @@ __global__ void __launch_bounds__(128) hop_f2p_kernel(HopArgs a) {
   hop_issue<3, false>(a, s, r, x, B);
   hop_consume<3, true>(a, A, acc);
   hop_consume<3, false>(a, B, acc);
+  finish2<EPI>(a, s, r, acc);
+}
+
+// ---------------------------------------------------------------------------
+// Link-staged variant for block fields (one RHS per thread, loads a hop ahead).  All
+// nrhs threads of a site use the same 8 links; loading them per thread sends nrhs
+// copies of every link through L1 (the largest share of the kernel's L1 traffic at
+// 12 RHS).  Here the block first copies the links of its sites -- 8 hops x 3 vectors
+// per site, 6 KiB at most -- into shared memory, one 16-byte vector per thread, and
+// after one barrier every thread reads them as shared-memory broadcasts.
+// ---------------------------------------------------------------------------
+constexpr int kLinkStageSites = 16;  // sites per block at most (nrhs >= 8)
+
+template <int EPI>
+__global__ void __launch_bounds__(128) hop_f2s_kernel(HopArgs a) {
+  __shared__ float4 slink[kLinkStageSites * 8 * 3];  // [site][hop][vector]
+  const int G = a.nrhs;
+  const int tx = threadIdx.x;
+  const int s0 = blockIdx.x * a.per_block;
+  // stage: entry k = (site, hop, vector); hop = 2 mu + (0 forward, 1 backward)
+  for (int k = tx; k < a.per_block * 24; k += blockDim.x) {
+    const int sl = k / 24, h = (k / 3) % 8, q = k % 3, mu = h >> 1;
+    const int ss = s0 + sl;
+    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (ss < a.g.vh) {
+      int x[4];
+      site_coords(a.g, a.pout, ss, x);
+      int site = ss, par = a.pout;
+      if (h & 1) {  // backward hop: U_mu(x - mu) on the other parity
+        x[mu] = x[mu] == 0 ? a.g.n[mu] - 1 : x[mu] - 1;
+        site = site_index(a.g, x);
+        par = 1 - a.pout;
+      }
+      const float4* gl = static_cast<const float4*>(a.gauge) + (size_t)(par * 4 + mu) * 3 * a.g.vh;
+      v = __ldg(gl + (size_t)q * a.g.vh + site);
+    }
+    slink[k] = v;
+  }
+  __syncthreads();
+  const int sl = a.div_nrhs.div(tx);
+  const int r = tx - sl * G;
+  const int s = s0 + sl;
+  if (s >= a.g.vh || sl >= a.per_block) return;
+  Pair12 acc;
+#pragma unroll
+  for (int q = 0; q < 6; ++q) acc.re[q] = acc.im[q] = make_float2(0.0f, 0.0f);
+  int x[4];
+  site_coords(a.g, a.pout, s, x);
+  const float4* sl_link = slink + sl * 24;
+  HopLoad A, B;
+#define QQ_STAGED_ISSUE(MU, FWD, L)                              \
+  hop_issue_spinor<MU, FWD>(a, s, r, x, L);                      \
+  _Pragma("unroll") for (int q = 0; q < 3; ++q) L.u[q] = sl_link[(2 * MU + (FWD ? 0 : 1)) * 3 + q];
+  QQ_STAGED_ISSUE(0, true, A);
+  QQ_STAGED_ISSUE(0, false, B);
+  hop_consume<0, true>(a, A, acc);
+  QQ_STAGED_ISSUE(1, true, A);
+  hop_consume<0, false>(a, B, acc);
+  QQ_STAGED_ISSUE(1, false, B);
+  hop_consume<1, true>(a, A, acc);
+  QQ_STAGED_ISSUE(2, true, A);
+  hop_consume<1, false>(a, B, acc);
+  QQ_STAGED_ISSUE(2, false, B);
+  hop_consume<2, true>(a, A, acc);
+  QQ_STAGED_ISSUE(3, true, A);
+  hop_consume<2, false>(a, B, acc);
+  QQ_STAGED_ISSUE(3, false, B);
+  hop_consume<3, true>(a, A, acc);
+  hop_consume<3, false>(a, B, acc);
+#undef QQ_STAGED_ISSUE
   finish2<EPI>(a, s, r, acc);
 }
 

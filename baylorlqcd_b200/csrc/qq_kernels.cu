@@ -134,6 +134,20 @@ static cudaError_t hop_f2p(const HopArgs& a, int epi, cudaStream_t st) {
   return cudaGetLastError();
 }
 
+static cudaError_t hop_f2s(const HopArgs& a, int epi, cudaStream_t st) {
+  const int per_block = hop_sites_per_block(1, a.nrhs);
+  if (per_block > kLinkStageSites) return cudaErrorInvalidValue;  // nrhs >= 8 only
+  const HopArgs b = hop_prepare(a, per_block, a.nrhs);
+  const dim3 blk(per_block * a.nrhs), grd((a.g.vh + per_block - 1) / per_block);
+  switch (epi) {
+    case EPI_STORE: hop_f2s_kernel<EPI_STORE><<<grd, blk, 0, st>>>(b); break;
+    case EPI_TWIST: hop_f2s_kernel<EPI_TWIST><<<grd, blk, 0, st>>>(b); break;
+    case EPI_DBLE: hop_f2s_kernel<EPI_DBLE><<<grd, blk, 0, st>>>(b); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
 // tps: 1, 2, 4 = register kernel with that many direction groups per site;
 // 32, 64, 96, 128 = staged kernel with that many threads per block;
 // kShapeMrhs + RPT (RPT = 2, 3, 4) = block fields with RPT right-hand sides per thread
@@ -146,13 +160,14 @@ cudaError_t launch_hop(const HopArgs& a, int sp, int recon, int epi, int tps, cu
   if (a.nrhs < 1 || a.nrhs > maxr) return cudaErrorInvalidValue;
   if (tps > kShapeF2) {
     const int rpt = tps - kShapeF2;
-    if (sp != P32 || (rpt < 4 && a.nrhs % rpt != 0) || (rpt > 1 && rpt < 4 && !a.blk))
+    if (sp != P32 || (rpt < 4 && a.nrhs % rpt != 0) || (rpt > 1 && rpt != 4 && !a.blk))
       return cudaErrorInvalidValue;
     switch (rpt) {
       case 1: return hop_f2_rpt<1>(a, epi, st);
       case 2: return hop_f2_rpt<2>(a, epi, st);
       case 3: return hop_f2_rpt<3>(a, epi, st);
       case 4: return hop_f2p(a, epi, st);  // pipelined, one RHS per thread
+      case 5: return a.blk ? hop_f2s(a, epi, st) : cudaErrorInvalidValue;  // + staged links
       default: return cudaErrorInvalidValue;
     }
   }

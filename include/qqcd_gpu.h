@@ -222,7 +222,8 @@ int qq_profile_hop_read(qq_ctx* ctx, long long* launches, double* ms_total, doub
  * use; 1, 2, 4 direction groups per site; 32-128 threads per block of the staged
  * kernel; 202-204 = block fields with 2-4 right-hand sides per thread, FP32/FP16;
  * 301-303 = FP32 with packed FP32x2 arithmetic, 1-3 right-hand sides per thread;
- * 304 = the same, one right-hand side per thread, loads issued a hop ahead).
+ * 304 = the same, one right-hand side per thread, loads issued a hop ahead;
+ * 305 = 304 with the links staged in shared memory, block fields of >= 8 RHS).
  * flush_l2 != 0 overwrites a 512 MiB buffer between launches so every launch reads
  * its operands from HBM.  ms_per_call: mean kernel time; bytes_per_call:
  * algorithmic bytes of one launch, V/2 * (8 * link bytes + nrhs * 2 * spinor bytes). */

@@ -33,7 +33,7 @@ EXPORTED = [
     "qq_vecdot_noalloc",
     "qq_defl_create", "qq_defl_destroy", "qq_defl_size", "qq_gmresdr", "qq_gmresproj", "qq_psc",
     "qq_bicgstab", "qq_fermprop", "qq_pointsource", "qq_fermprop_batch", "qq_initlagfib",
-    "qq_rnds", "qq_z2source", "qq_z4source", "qq_twaverage_level0", "qq_bench_hsingle",
+    "qq_rnds", "qq_z2source", "qq_z4source", "qq_twaverage_level0", "qq_discon_traces", "qq_bench_hsingle",
     "qq_heatbath", "qq_ctx_stream", "qq_launch_count", "qq_profile_hop", "qq_profile_hop_read",
 ]
 
@@ -128,6 +128,7 @@ def load_library() -> C.CDLL:
         "qq_z2source": ([P, P, P], I),
         "qq_z4source": ([P, P, P], I),
         "qq_twaverage_level0": ([P, P, P, P, P, D, D, I, P], I),
+        "qq_discon_traces": ([P, I, I, DP, C.POINTER(qq_method), D, I, P, C.POINTER(qq_solve_info)], I),
         "qq_bench_hsingle": ([P, I, I, I, I, I, DP, DP], I),
         "qq_heatbath": ([P, D, I, C.c_ulonglong, P, DP], I),
         "qq_ctx_stream": ([P, C.POINTER(P)], I),
@@ -376,6 +377,19 @@ class Lattice:
         be, bo = self.new_half(), self.new_half()
         _check(self.lib.qq_z4source(self._ctx, _ptr(be), _ptr(bo)))
         return be, bo
+
+    def discon_traces(self, noise_kind: int, nnoise: int, kappa, solver: int = 1, m: int = 60, k: int = 20,
+                      precision: int = 32, rhs_block: int = 12, tol: float = 1e-10, max_outer: int = 0,
+                      deflate: int = 0, defl_tol: float = 1e-5, delta: float = 0.0, dobndry: int = 0):
+        """Noise-averaged level-0 loop traces (qq_discon_traces): J[iop, t, re/im] and the
+        per-noise solve reports.  Call initlagfib first, as the reference does."""
+        J = np.zeros((6, self.dims[3], 2))
+        infos = (qq_solve_info * nnoise)()
+        meth = qq_method(m, k, precision, rhs_block, tol, max_outer, solver, deflate, defl_tol)
+        st = self.lib.qq_discon_traces(self._ctx, int(noise_kind), int(nnoise), _d2(kappa), C.byref(meth),
+                                       float(delta), int(dobndry), _ptr(J), infos)
+        _check(st, allow_not_converged=True)
+        return J, [SolveInfo.from_c(i) for i in infos]
 
     def twaverage_level0(self, be, bo, xe, xo, kappa: float, delta: float = 0.0, dobndry: int = 0):
         """Level-0 loop traces of one noise (qq_twaverage_level0): J[iop, t, re/im]."""

@@ -201,6 +201,20 @@ int qq_z4source(qq_ctx* ctx, double* be, double* bo);
  * noises and the division by nx*ny*nz (:4161-4164) are left to the caller. */
 int qq_twaverage_level0(qq_ctx* ctx, const double* be, const double* bo, const double* xe,
                         const double* xo, double kappa, double delta, int dobndry, double* J);
+/* Batched disconnected loops at the unsubtracted level: the noise loop of twistdiscon
+ * (Q/disconloops.f90:3612-4170).  For each of nnoise noises, in the generator's order
+ * (qq_initlagfib first, as the reference): draw Z(noise_kind = 2 or 4) noise, solve,
+ * take the level-0 traces of qq_twaverage_level0 and accumulate; J(2, nt, 6) (host or
+ * device) receives the sum divided by nnoise and by nx*ny*nz (:4161-4164).
+ * method->solver: 0 = plain FP64 GMRES-DR(m, k) per noise to tol; 1 = batched
+ * mixed-precision BiCGStab on blocks of rhs_block noises (as qq_fermprop_batch);
+ * 2 = the reference's psc sequence (GMRES-DR(m, k) on the first noise keeping its
+ * deflation space, GMRES-Proj(m - k, k) to the fixed 1e-8 on the rest).  infos (nnoise
+ * entries, may be NULL) receives each solve's report.  Returns QQ_NOT_CONVERGED (with
+ * J filled) if any solve stopped short of its tolerance. */
+int qq_discon_traces(qq_ctx* ctx, int noise_kind, int nnoise, const double kappa[2],
+                     const qq_method* method, double delta, int dobndry, double* J,
+                     qq_solve_info* infos);
 
 /* ---- measurement (library-specific; no counterpart in the reference) ---- */
 /* The cudaStream_t every call of this context runs on (for event timing). */

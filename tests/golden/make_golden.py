@@ -12,7 +12,8 @@ fixed numbers to meet.  Inputs:
   reconstruction, all on 4x4x4x8 with the Gram-Schmidt gauge field of
   qqtest.golden_gauge(seed 2026, eps 0.25; plaquette 0.52) and point sources;
 * level-0 loop traces (Q/vevbleft.f90 twAverage, nsub = 0) of the first Z(4) noise
-  after a fermprop solve.
+  after a fermprop solve, and the noise average of three Z(4) noises solved with psc
+  as the reference's twistdiscon loop does.
 
 Usage: python tests/golden/make_golden.py   (rewrites golden.json)
 """
@@ -97,6 +98,19 @@ def main():
     J = ol.twaverage_level0(ze, zo, xe, xo, 0.15, 0.0, 0)
     out["traces_z4_noise1"] = {"kappa": 0.15, "delta": 0.0, "dobndry": 0, "solve": "fermprop GMRES-DR(30,10) 1e-12",
                                "itercount": int(log.itercount), "J": J.tolist()}
+    # the reference's disconnected-loop method: 3 Z(4) noises through psc (GMRES-DR on
+    # the first, GMRES-Proj on the rest), level-0 traces averaged as twistdiscon does
+    oracle.initlagfib(0, 21)
+    d = ol.deflation(30, 10)
+    Jsum = np.zeros((6, DIMS[3], 2))
+    for i in range(3):
+        ze, zo = ol.z4source()
+        xe, xo, st, log = ol.fermprop(ze, zo, (0.15, 0.0), inverter=6, resmax=1e-10, nGMRES=(30, 10),
+                                      isignal=1 if i == 0 else 2, defl=d)
+        Jsum += ol.twaverage_level0(ze, zo, xe, xo, 0.15, 0.0, 0)
+    J = Jsum / (3 * DIMS[0] * DIMS[1] * DIMS[2])
+    out["discon_z4_psc3"] = {"kappa": 0.15, "nnoise": 3, "iseed": 21, "GMRES": [30, 10], "resmax": 1e-10,
+                             "J": J.tolist()}
     (HERE / "golden.json").write_text(json.dumps(out, indent=1) + "\n")
     print("wrote", HERE / "golden.json")
 

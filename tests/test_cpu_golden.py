@@ -111,3 +111,19 @@ def test_traces_z4_noise1(ol):
     J = ol.twaverage_level0(ze, zo, xe, xo, rec["kappa"], rec["delta"], rec["dobndry"])
     want = np.array(rec["J"])
     assert np.abs(J - want).max() <= RTOL * np.abs(want).max()
+
+
+def test_discon_psc3(ol):
+    """The reference's noise loop (twistdiscon): 3 Z(4) noises, psc, level-0 traces."""
+    rec = GOLDEN["discon_z4_psc3"]
+    oracle.initlagfib(0, rec["iseed"])
+    d = ol.deflation(*rec["GMRES"])
+    Jsum = np.zeros((6, DIMS[3], 2))
+    for i in range(rec["nnoise"]):
+        ze, zo = ol.z4source()
+        xe, xo, st, log = ol.fermprop(ze, zo, (rec["kappa"], 0.0), inverter=6, resmax=rec["resmax"],
+                                      nGMRES=tuple(rec["GMRES"]), isignal=1 if i == 0 else 2, defl=d)
+        Jsum += ol.twaverage_level0(ze, zo, xe, xo, rec["kappa"], 0.0, 0)
+    J = Jsum / (rec["nnoise"] * DIMS[0] * DIMS[1] * DIMS[2])
+    want = np.array(rec["J"])
+    assert np.abs(J - want).max() <= RTOL * np.abs(want).max()

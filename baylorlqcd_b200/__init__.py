@@ -35,6 +35,7 @@ EXPORTED = [
     "qq_bicgstab", "qq_fermprop", "qq_pointsource", "qq_fermprop_batch", "qq_initlagfib",
     "qq_rnds", "qq_z2source", "qq_z4source", "qq_twaverage_level0", "qq_discon_traces", "qq_bench_hsingle",
     "qq_heatbath", "qq_ctx_stream", "qq_launch_count", "qq_profile_hop", "qq_profile_hop_read",
+    "qq_gfwrite", "qq_gfread", "qq_fpwrite", "qq_fpread",
 ]
 
 
@@ -135,6 +136,10 @@ def load_library() -> C.CDLL:
         "qq_launch_count": ([], C.c_longlong),
         "qq_profile_hop": ([P, I], I),
         "qq_profile_hop_read": ([P, C.POINTER(C.c_longlong), DP, DP], I),
+        "qq_gfwrite": ([C.c_char_p, P, I, I, IP, D, DP, DP, I, I], I),
+        "qq_gfread": ([C.c_char_p, P, I, I, IP, DP, DP, DP, IP, IP], I),
+        "qq_fpwrite": ([C.c_char_p, P, P, I, I, D, D, D, I, I, I, I], I),
+        "qq_fpread": ([C.c_char_p, P, P, I, I, DP, DP, DP, IP, IP, IP, IP], I),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -420,3 +425,43 @@ def rnds(m: int) -> np.ndarray:
     out = np.zeros(m)
     _check(load_library().qq_rnds(m, out.ctypes.data_as(C.POINTER(C.c_double))))
     return out
+
+
+# ---- file formats of the reference (G/gaugetools.f90 GFwrite/GFread, Q/quark.f90 FPwrite/FPread)
+def gfwrite(path, u: np.ndarray, nvhalf: int, gaction=(1, 1, 1, 1), beta=6.0, alat=(1.0,) * 4, tad=(1.0,) * 4,
+            icfgsave=1, myid=0):
+    """Write a gauge configuration (re-unitarises u in place, as GFwrite)."""
+    ntotal = u.shape[3]
+    _check(load_library().qq_gfwrite(str(path).encode(), _ptr(u), nvhalf, ntotal, (C.c_int * 4)(*gaction),
+                                     float(beta), (C.c_double * 4)(*alat), (C.c_double * 4)(*tad),
+                                     int(icfgsave), int(myid)))
+
+
+def gfread(path, nvhalf: int, ntotal: int):
+    """Read a gauge configuration: (u, header dict)."""
+    u = np.zeros((16, 2, 4, ntotal, 18))
+    ga, al, td = (C.c_int * 4)(), (C.c_double * 4)(), (C.c_double * 4)()
+    beta, icfg, myid = C.c_double(), C.c_int(), C.c_int()
+    _check(load_library().qq_gfread(str(path).encode(), _ptr(u), nvhalf, ntotal, ga, C.byref(beta), al, td,
+                                    C.byref(icfg), C.byref(myid)))
+    return u, dict(gaction=tuple(ga), beta=beta.value, alat=tuple(al), tad=tuple(td), icfgsave=icfg.value,
+                   myid=myid.value)
+
+
+def fpwrite(path, xe: np.ndarray, xo: np.ndarray, nvhalf: int, kappa=0.0, tmqcd=0.0, cSW=0.0, icsrc=1, idsrc=1,
+            icfg=1, myid=0):
+    """Write a propagator (xe: gblclr 1 half, xo: gblclr 2 half)."""
+    _check(load_library().qq_fpwrite(str(path).encode(), _ptr(xe), _ptr(xo), nvhalf, xe.shape[3], float(kappa),
+                                     float(tmqcd), float(cSW), int(icsrc), int(idsrc), int(icfg), int(myid)))
+
+
+def fpread(path, nvhalf: int, ntotal: int):
+    """Read a propagator: (xe, xo, header dict)."""
+    xe = np.zeros((8, 2, 4, ntotal, 6))
+    xo = np.zeros((8, 2, 4, ntotal, 6))
+    k, t, c = C.c_double(), C.c_double(), C.c_double()
+    ic, idd, cf, my = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+    _check(load_library().qq_fpread(str(path).encode(), _ptr(xe), _ptr(xo), nvhalf, ntotal, C.byref(k), C.byref(t),
+                                    C.byref(c), C.byref(ic), C.byref(idd), C.byref(cf), C.byref(my)))
+    return xe, xo, dict(kappa=k.value, tmqcd=t.value, cSW=c.value, icsrc=ic.value, idsrc=idd.value,
+                        icfg=cf.value, myid=my.value)

@@ -216,6 +216,25 @@ int qq_discon_traces(qq_ctx* ctx, int noise_kind, int nnoise, const double kappa
                      const qq_method* method, double delta, int dobndry, double* J,
                      qq_solve_info* infos);
 
+/* ---- file formats (host memory; no device needed) ----
+ * Fortran unformatted sequential files, as the reference writes them: every record is
+ * framed by its 4-byte length, reals are 8 bytes, integers 4.  nvhalf and ntotal are
+ * the reference array sizes (qq_ctx_dims). */
+/* GFwrite G/gaugetools.f90:1260-1294: re-unitarises u in place (fixsu3 :1338-1432),
+ * then writes rows 1-2 of every link and the trailer (gaction, beta, alat, tad,
+ * icfgsave, myid).  The file must not exist (status="new"). */
+int qq_gfwrite(const char* path, double* u, int nvhalf, int ntotal, const int gaction[4],
+               double beta, const double alat[4], const double tad[4], int icfgsave, int myid);
+/* GFread :1298-1334: reads rows 1-2 and the trailer, completes row 3 with fixsu3. */
+int qq_gfread(const char* path, double* u, int nvhalf, int ntotal, int gaction[4], double* beta,
+              double alat[4], double tad[4], int* icfgsave, int* myid);
+/* FPwrite Q/quark.f90:3379-3434 (xe: gblclr = 1 half, xo: gblclr = 2 half) and
+ * FPread :3438-3481. */
+int qq_fpwrite(const char* path, const double* xe, const double* xo, int nvhalf, int ntotal,
+               double kappa, double tmqcd, double cSW, int icsrc, int idsrc, int icfg, int myid);
+int qq_fpread(const char* path, double* xe, double* xo, int nvhalf, int ntotal, double* kappa,
+              double* tmqcd, double* cSW, int* icsrc, int* idsrc, int* icfg, int* myid);
+
 /* ---- measurement (library-specific; no counterpart in the reference) ---- */
 /* The cudaStream_t every call of this context runs on (for event timing). */
 int qq_ctx_stream(const qq_ctx* ctx, void** stream);

@@ -76,15 +76,17 @@ int block_op(qq_ctx* c, int prec, const BlockBiArgs& A, int op, const int* dslot
   return QQ_OK;
 }
 
-// mode 0: block[k] = x ; 1: x += block[k] ; 2: block[k] = 0
-int block_slot(qq_ctx* c, int prec, int nb, int k, Spinor blockf, Spinor x, int mode) {
+// mode 0: block[k] = x ; 1: x += block[k] ; 2: block[k] = 0.  With `pred`, only when
+// bit k of the device word *pred is set.
+int block_slot(qq_ctx* c, int prec, int nb, int k, Spinor blockf, Spinor x, int mode,
+               const unsigned* pred = nullptr) {
   count_launch();
   if (prec == P32)
-    block_slot_kernel<P32><<<kRedBlocks, kRedThreads, 0, c->st>>>(c->g.vh, nb, k, blockf, x, mode);
+    block_slot_kernel<P32><<<kRedBlocks, kRedThreads, 0, c->st>>>(c->g.vh, nb, k, blockf, x, mode, pred);
   else if (prec == P16)
-    block_slot_kernel<P16><<<kRedBlocks, kRedThreads, 0, c->st>>>(c->g.vh, nb, k, blockf, x, mode);
+    block_slot_kernel<P16><<<kRedBlocks, kRedThreads, 0, c->st>>>(c->g.vh, nb, k, blockf, x, mode, pred);
   else
-    block_slot_kernel<P64><<<kRedBlocks, kRedThreads, 0, c->st>>>(c->g.vh, nb, k, blockf, x, mode);
+    block_slot_kernel<P64><<<kRedBlocks, kRedThreads, 0, c->st>>>(c->g.vh, nb, k, blockf, x, mode, pred);
   QQ_CK(cudaGetLastError());
   return QQ_OK;
 }
@@ -118,9 +120,9 @@ int full_residual(qq_ctx* c, Spinor be, Spinor bo, Spinor xe, Spinor xo, const d
 // the last update, x64 += x_low, the FP64 true residual replaces the iterated one
 // (projected onto the deflation space first, if any) and the iteration continues with
 // the same search direction.
-int bicgstab_block(qq_ctx* c, std::vector<PerRhs*>& rhs, int prec, double tol, double delta,
-                   int maxiter, const double kappa[2], const DeflSpace* defl,
-                   std::vector<SolveStats>& stats) {
+int bicgstab_block_sync(qq_ctx* c, std::vector<PerRhs*>& rhs, int prec, double tol, double delta,
+                        int maxiter, const double kappa[2], const DeflSpace* defl,
+                        std::vector<SolveStats>& stats) {
   const int nb = (int)rhs.size();
   if (nb == 0) return QQ_OK;
   if (nb > kMaxBatch) return set_error(QQ_BAD_ARG, "too many right-hand sides in one block");
@@ -256,6 +258,196 @@ int bicgstab_block(qq_ctx* c, std::vector<PerRhs*>& rhs, int prec, double tol, d
   }
   QQ_CK(cudaStreamSynchronize(c->st));
   return active ? QQ_NOT_CONVERGED : QQ_OK;
+}
+
+// Device-driven variant (no deflation): the reliable update itself runs on the device
+// -- the FP64 true residual, its norm, the convergence decision, the re-insertion of
+// the residual and the re-activation are stream-ordered kernels, the decision a
+// one-thread kernel -- so the host never waits inside the iteration.  It queues chunk
+// c and a snapshot of the scalars, then reads snapshot c - 1 while chunk c runs and
+// queues the updates of right-hand sides that went pending.  Updates queued at step c
+// are visible from snapshot c + 1 on, so earlier snapshots' pending marks for them
+// are skipped.
+int bicgstab_block(qq_ctx* c, std::vector<PerRhs*>& rhs, int prec, double tol, double delta,
+                   int maxiter, const double kappa[2], const DeflSpace* defl,
+                   std::vector<SolveStats>& stats) {
+  if (defl && defl->k > 0) return bicgstab_block_sync(c, rhs, prec, tol, delta, maxiter, kappa, defl, stats);
+  const int nb = (int)rhs.size();
+  if (nb == 0) return QQ_OK;
+  if (nb > kMaxBatch) return set_error(QQ_BAD_ARG, "too many right-hand sides in one block");
+  Field r, rhat, p, v, t, xl, tmp;
+  for (Field* f : {&r, &rhat, &p, &v, &t, &xl, &tmp}) {
+    QQ_TRY(alloc_field(c, *f, prec, nb));
+    QQ_CK(cudaMemsetAsync(f->data.p, 0, f->data.bytes, c->st));
+    if (prec == P16) QQ_CK(cudaMemsetAsync(f->norm.p, 0, f->norm.bytes, c->st));
+  }
+  constexpr size_t kScalDoubles = (size_t)kScal * kMaxBatch;
+  constexpr size_t kSnap = kScalDoubles + 2;  // scalars + 4 control words
+  const size_t sbytes = sizeof(double) * kSnap;
+  static_assert(1024 + 2 * kSnap <= 3072, "snapshots exceed the pinned buffer");
+  DevBuf S, part, dslots;
+  QQ_CK(S.alloc(sbytes));
+  QQ_CK(part.alloc(sizeof(double) * 3 * kRedBlocks * kMaxBatch));
+  QQ_CK(dslots.alloc(sizeof(int) * kMaxBatch));
+  double* Sd = S.as<double>();
+  unsigned* ctl = reinterpret_cast<unsigned*>(Sd + kScalDoubles);
+  double* snap[2] = {c->hpin + 1024, c->hpin + 1024 + kSnap};
+  Tmp tmp64(c, P64), h(c, P64);
+  double* s1 = c->scal.as<double>();
+  // initial FP64 residuals (synchronous, once)
+  double* hS = snap[0];
+  std::fill(hS, hS + kSnap, 0.0);
+  unsigned* hctl = reinterpret_cast<unsigned*>(hS + kScalDoubles);
+  std::vector<int> slots(nb);
+  unsigned active = 0, done = 0;
+  for (int k = 0; k < nb; ++k) {
+    PerRhs& R = *rhs[k];
+    slots[k] = k;
+    QQ_TRY(norm2_host(c, R.b.sp(), &R.bn));
+    R.bn = std::sqrt(R.bn);
+    QQ_TRY(op_dbletm(c, h.sp(), R.x.sp(), tmp64.sp(), 0, kappa));
+    QQ_TRY(lin(c, R.r64.sp(), cimm(1.0), R.b.sp(), cimm(-1.0), h.sp(), cimm(0), Spinor{nullptr, nullptr, P64}, s1));
+    double n2;
+    QQ_TRY(read_scalars(c, s1, 1, &n2));
+    R.rn = std::sqrt(n2);
+    stats[k].mvp += 1;
+    R.rmax = R.rn;
+    R.done = !(R.bn > 0.0) || R.rn / R.bn <= tol;
+    stats[k].true_rel = R.bn > 0.0 ? R.rn / R.bn : 0.0;
+    if (R.done)
+      done |= 1u << k;
+    else
+      active |= 1u << k;
+    QQ_TRY(block_slot(c, prec, nb, k, r.sp(), R.r64.sp(), 0));
+    QQ_TRY(block_slot(c, prec, nb, k, rhat.sp(), R.r64.sp(), 0));
+    double* sc = &hS[(size_t)k * kScal];
+    sc[SC_RHO] = sc[SC_ALPHA] = sc[SC_OMEGA] = 1.0;
+    sc[SC_RMAX] = R.rmax;
+    sc[SC_BN] = R.bn > 0.0 ? R.bn : 1.0;
+  }
+  hctl[CTL_ACTIVE] = active;
+  hctl[CTL_DONE] = done;
+  QQ_CK(cudaMemcpyAsync(Sd, hS, sbytes, cudaMemcpyHostToDevice, c->st));
+  QQ_CK(cudaMemcpyAsync(dslots.p, slots.data(), sizeof(int) * nb, cudaMemcpyHostToDevice, c->st));
+  QQ_CK(cudaStreamSynchronize(c->st));
+  const unsigned all = nb == 32 ? 0xffffffffu : (1u << nb) - 1u;
+  if ((done & all) == all) return QQ_OK;
+  BlockBiArgs A;
+  std::memset(&A, 0, sizeof(A));
+  A.vh = c->g.vh;
+  A.nb = nb;
+  A.active = ctl + CTL_ACTIVE;
+  A.r = r.sp();
+  A.rhat = rhat.sp();
+  A.p = p.sp();
+  A.v = v.sp();
+  A.t = t.sp();
+  A.x = xl.sp();
+  for (int k = 0; k < nb; ++k) A.slot[k] = k;
+  A.S = Sd;
+  A.partial = part.as<double>();
+  const int* ds = dslots.as<int>();
+  const ScalarCtl sctl{ctl, delta, 0.5 * tol};
+  constexpr int kChunk = 1;  // a pending RHS idles 1-2 iterations before its update runs
+  auto run_chunk = [&]() -> int {
+    for (int i = 0; i < kChunk; ++i) {
+      QQ_TRY(block_op(c, prec, A, OP_DOT_RHAT_R, ds, ST_BETA, sctl));
+      QQ_TRY(block_op(c, prec, A, OP_P_UPDATE, ds, -1, sctl));
+      QQ_TRY(op_dbletm_block(c, v.sp(), p.sp(), tmp.sp(), nb, 0, kappa));
+      QQ_TRY(block_op(c, prec, A, OP_DOT_RHAT_V, ds, ST_ALPHA, sctl));
+      QQ_TRY(block_op(c, prec, A, OP_S_UPDATE, ds, -1, sctl));
+      QQ_TRY(op_dbletm_block(c, t.sp(), r.sp(), tmp.sp(), nb, 0, kappa));
+      QQ_TRY(block_op(c, prec, A, OP_DOTS_T, ds, ST_OMEGA, sctl));
+      QQ_TRY(block_op(c, prec, A, OP_XR_UPDATE, ds, ST_R2, sctl));
+    }
+    return QQ_OK;
+  };
+  // right-hand side k's reliable update, all on the device
+  auto reliable = [&](int k) -> int {
+    PerRhs& R = *rhs[k];
+    QQ_TRY(block_slot(c, prec, nb, k, xl.sp(), R.x.sp(), 1));
+    QQ_TRY(block_slot(c, prec, nb, k, xl.sp(), R.x.sp(), 2));
+    QQ_TRY(op_dbletm(c, h.sp(), R.x.sp(), tmp64.sp(), 0, kappa));
+    QQ_TRY(lin(c, R.r64.sp(), cimm(1.0), R.b.sp(), cimm(-1.0), h.sp(), cimm(0), Spinor{nullptr, nullptr, P64},
+               Sd + (size_t)k * kScal + SC_T2));
+    count_launch(2);
+    reliable_decide_kernel<<<1, 1, 0, c->st>>>(Sd, ds, ctl, k, tol);
+    QQ_CK(cudaGetLastError());
+    QQ_TRY(block_slot(c, prec, nb, k, r.sp(), R.r64.sp(), 0, ctl + CTL_INSERT));
+    reliable_resume_kernel<<<1, 1, 0, c->st>>>(ctl, k);
+    QQ_CK(cudaGetLastError());
+    return QQ_OK;
+  };
+  cudaEvent_t ev[2];
+  QQ_CK(cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming));
+  QQ_CK(cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming));
+  struct EvGuard {
+    cudaEvent_t* e;
+    ~EvGuard() {
+      cudaEventDestroy(e[0]);
+      cudaEventDestroy(e[1]);
+    }
+  } evg{ev};
+  std::vector<int> enq(nb, -1), nupd_seen(nb, 0);
+  int chunks = 0;
+  QQ_TRY(run_chunk());
+  ++chunks;
+  QQ_CK(cudaMemcpyAsync(snap[0], Sd, sbytes, cudaMemcpyDeviceToHost, c->st));
+  QQ_CK(cudaEventRecord(ev[0], c->st));
+  bool expect_active = true;
+  int rc = QQ_OK;
+  for (int step = 1;; ++step) {
+    const bool more = expect_active && (long long)chunks * kChunk < maxiter;
+    if (more) {
+      QQ_TRY(run_chunk());
+      ++chunks;
+    }
+    QQ_CK(cudaMemcpyAsync(snap[step % 2], Sd, sbytes, cudaMemcpyDeviceToHost, c->st));
+    QQ_CK(cudaEventRecord(ev[step % 2], c->st));
+    // snapshot step - 1, taken before everything queued at this step
+    QQ_CK(cudaEventSynchronize(ev[(step - 1) % 2]));
+    const double* sv = snap[(step - 1) % 2];
+    const unsigned* sc = reinterpret_cast<const unsigned*>(sv + kScalDoubles);
+    const int sidx = step - 1;
+    for (int k = 0; k < nb; ++k) {
+      SolveStats& st = stats[k];
+      const double* sk = sv + (size_t)k * kScal;
+      const int its = (int)sk[SC_ITS];
+      st.mvp += 2 * (its - st.itercount);
+      st.itercount = its;
+      const int nupd = (int)sk[SC_NUPD];
+      if (nupd > nupd_seen[k]) {
+        const double rel = sk[SC_TRUE];
+        if (!std::isfinite(rel)) return set_error(QQ_NAN, "NaN true residual in batched BiCGStab");
+        st.mvp += nupd - nupd_seen[k];
+        st.true_rel = rel;
+        st.hist.push_back(rel);
+        st.hist_mvp.push_back(st.mvp);
+        nupd_seen[k] = nupd;
+      }
+    }
+    done = sc[CTL_DONE];
+    if ((done & all) == all) break;
+    const unsigned pend = sc[CTL_PENDING] & ~done;
+    bool queued = false, inflight = false;
+    for (int k = 0; k < nb; ++k) {
+      if (enq[k] >= sidx) inflight = true;
+      if (!((pend >> k) & 1u) || enq[k] >= sidx) continue;
+      if (!std::isfinite(sv[(size_t)k * kScal + SC_R2])) return set_error(QQ_NAN, "NaN residual in batched BiCGStab");
+      QQ_TRY(reliable(k));
+      enq[k] = step;
+      queued = true;
+    }
+    const unsigned act = sc[CTL_ACTIVE] & ~done;
+    expect_active = act != 0 || queued || inflight;
+    if (!queued && !inflight && (!more || act == 0)) {
+      rc = QQ_NOT_CONVERGED;  // iteration limit reached (or nothing left that can move)
+      break;
+    }
+  }
+  QQ_CK(cudaStreamSynchronize(c->st));
+  for (int k = 0; k < nb; ++k) rhs[k]->done = (done >> k) & 1u;
+  return rc == QQ_OK && (done & all) == all ? QQ_OK : QQ_NOT_CONVERGED;
 }
 
 int batch_solve(qq_ctx* c, int nrhs, const double* be, const double* bo, const double kappa[2],

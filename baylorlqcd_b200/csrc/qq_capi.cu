@@ -110,7 +110,7 @@ int qq_ctx_create(const qq_geom* geom, int device, qq_ctx** out) {
   if (st == QQ_OK && cudaEventCreate(&c->tev1) != cudaSuccess) st = QQ_CUDA_ERR;
   if (st == QQ_OK && c->partial.alloc(sizeof(double) * kRedBlocks * 16 * 16) != cudaSuccess) st = QQ_CUDA_ERR;
   if (st == QQ_OK && c->scal.alloc(sizeof(double) * 1024) != cudaSuccess) st = QQ_CUDA_ERR;
-  if (st == QQ_OK && cudaMallocHost(&c->hpin, sizeof(double) * 2048) != cudaSuccess) st = QQ_CUDA_ERR;
+  if (st == QQ_OK && cudaMallocHost(&c->hpin, sizeof(double) * 3072) != cudaSuccess) st = QQ_CUDA_ERR;
   if (st != QQ_OK) {
     qq_ctx_destroy(c);
     return set_error(QQ_CUDA_ERR, "context allocation failed");

@@ -97,8 +97,9 @@ struct qq_ctx {
   qq::DevBuf partial;       // reduction partials
   qq::DevBuf scal;          // device scalar slots
   qq::DevBuf trace_buf;     // per-site loop-trace values and the time-slice sums
+  qq::DevBuf tune_flush;    // L2-sized buffer overwritten between autotuner timings
   double* hpin = nullptr;   // pinned host memory: [0, 1024) read_scalars staging,
-                            // [1024, 2048) the batched solver's scalar mirror
+                            // [1024, 3072) the batched solver's two scalar snapshots
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   cudaEvent_t tev0 = nullptr, tev1 = nullptr;       // autotuner timing
   std::map<int, int> hop_tune;                       // shape -> threads per site

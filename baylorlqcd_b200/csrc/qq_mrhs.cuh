@@ -23,13 +23,17 @@ enum ScalSlot : int {
   SC_RMAX = 10,    // ||r|| at the last reliable update
   SC_BN = 11,      // ||b||
   SC_ITS = 12,     // iterations done
+  SC_T2 = 13,      // ||b - A x||^2 of the last reliable update (FP64)
+  SC_TRUE = 14,    // ||b - A x|| / ||b|| of the last reliable update
+  SC_NUPD = 15,    // reliable updates done
   kScal = 16,
 };
 
 // Control words after the scalar slots: [0] active mask (bit r: right-hand side r
-// iterates), [1] pending mask (bit r: r stopped and waits for the host's reliable
-// update or convergence test).
-enum CtlWord : int { CTL_ACTIVE = 0, CTL_PENDING = 1 };
+// iterates), [1] pending mask (bit r: r stopped and waits for its reliable update or
+// convergence test), [2] done mask (r converged), [3] insert mask (r's new FP64
+// residual is to replace its iterated one).
+enum CtlWord : int { CTL_ACTIVE = 0, CTL_PENDING = 1, CTL_DONE = 2, CTL_INSERT = 3 };
 
 enum BiOp : int {
   OP_DOT_RHAT_R = 0,  // red: <rhat, r>
@@ -204,12 +208,45 @@ static __global__ void bicg_scalar_kernel(double* S, const int* slots, const dou
   }
 }
 
+// End of right-hand side k's reliable update, after ||b - A x||^2 has landed in
+// S[SC_T2]: record the true residual, decide convergence, and either mark k done or
+// arm the re-insertion of the FP64 residual (rmax = ||r||).  One thread.
+static __global__ void reliable_decide_kernel(double* S, const int* slots, unsigned* ctl, int k,
+                                              double tol) {
+  double* s = S + (size_t)slots[k] * kScal;
+  const double rn = sqrt(s[SC_T2]);
+  const double rel = rn / s[SC_BN];
+  s[SC_TRUE] = rel;
+  s[SC_NUPD] += 1.0;
+  const unsigned bit = 1u << k;
+  if (!(rel > tol)) {  // converged (a NaN residual is reported as converged and caught on the host)
+    atomicOr(&ctl[CTL_DONE], bit);
+    atomicAnd(&ctl[CTL_INSERT], ~bit);
+  } else {
+    s[SC_RMAX] = rn;
+    atomicOr(&ctl[CTL_INSERT], bit);
+  }
+  atomicAnd(&ctl[CTL_PENDING], ~bit);
+}
+
+// After the (predicated) re-insertion: k iterates again unless it converged.
+static __global__ void reliable_resume_kernel(unsigned* ctl, int k) {
+  const unsigned bit = 1u << k;
+  if (ctl[CTL_INSERT] & bit) {
+    atomicAnd(&ctl[CTL_INSERT], ~bit);
+    atomicOr(&ctl[CTL_ACTIVE], bit);
+  }
+}
+
 // Slot k of a block field <-> a separate FP64 field.
 //   mode 0: block[k] = x (rounded to the block precision)   mode 1: x += block[k]
 //   mode 2: block[k] = 0
+// When `pred` is given the kernel does nothing unless bit k of *pred is set.
 template <int P>
-__global__ void block_slot_kernel(int vh, int nb, int k, Spinor blockf, Spinor x, int mode) {
+__global__ void block_slot_kernel(int vh, int nb, int k, Spinor blockf, Spinor x, int mode,
+                                  const unsigned* pred) {
   using RB = typename SpinorIO<P>::R;
+  if (pred && !((*pred >> k) & 1u)) return;
   for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < vh; s += gridDim.x * blockDim.x) {
     const int e = s * nb + k, n = vh * nb;
     cplx<RB> b[12];

@@ -35,7 +35,7 @@ EXPORTED = [
     "qq_bicgstab", "qq_fermprop", "qq_pointsource", "qq_fermprop_batch", "qq_initlagfib",
     "qq_rnds", "qq_z2source", "qq_z4source", "qq_twaverage_level0", "qq_discon_traces", "qq_bench_hsingle",
     "qq_heatbath", "qq_ctx_stream", "qq_launch_count", "qq_profile_hop", "qq_profile_hop_read",
-    "qq_gfwrite", "qq_gfread", "qq_fpwrite", "qq_fpread",
+    "qq_gfwrite", "qq_gfread", "qq_fpwrite", "qq_fpread", "qq_hsingle_block",
 ]
 
 
@@ -131,6 +131,7 @@ def load_library() -> C.CDLL:
         "qq_twaverage_level0": ([P, P, P, P, P, D, D, I, P], I),
         "qq_discon_traces": ([P, I, I, DP, C.POINTER(qq_method), D, I, P, C.POINTER(qq_solve_info)], I),
         "qq_bench_hsingle": ([P, I, I, I, I, I, DP, DP], I),
+        "qq_hsingle_block": ([P, I, I, I, P, P, I, I], I),
         "qq_heatbath": ([P, D, I, C.c_ulonglong, P, DP], I),
         "qq_ctx_stream": ([P, C.POINTER(P)], I),
         "qq_launch_count": ([], C.c_longlong),
@@ -277,6 +278,15 @@ class Lattice:
     def hsingle(self, gin, idag: int, gblclr: int, out=None):
         out = self.new_half() if out is None else out
         _check(self.lib.qq_hsingle(self._ctx, _ptr(out), _ptr(gin), idag, gblclr))
+        return out
+
+    def hsingle_block(self, gin, idag: int, gblclr: int, precision: int = 32, shape: int = 0):
+        """H on a stack of half vectors (shape (nrhs,) + half_shape) in reduced precision
+        through one hopping-kernel shape (0 = autotuned); returns FP64 half vectors."""
+        gin = np.ascontiguousarray(gin, dtype=np.float64)
+        out = np.zeros_like(gin)
+        _check(self.lib.qq_hsingle_block(self._ctx, precision, gin.shape[0], shape, _ptr(out), _ptr(gin),
+                                         idag, gblclr))
         return out
 
     def hdouble(self, ge, idag: int, kappa: float, out=None):

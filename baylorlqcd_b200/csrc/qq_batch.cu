@@ -581,4 +581,56 @@ int batch_solve(qq_ctx* c, int nrhs, const double* be, const double* bo, const d
   return QQ_OK;
 }
 
+// H (output parity pout) on nrhs reference-layout fields, computed at precision prec
+// on one RHS-interleaved block field (a plain field for nrhs = 1) by kernel shape
+// `shape` (0: the autotuned choice), returned in FP64 reference layout.
+int hsingle_block(qq_ctx* c, int prec, int nrhs, int shape, double* gout, const double* gin, int idag,
+                  int pout) {
+  const int vh = c->g.vh;
+  const size_t nv = c->ref_doubles();
+  Field in, out;
+  in.prec = out.prec = prec;
+  QQ_CK(in.data.alloc(field_bytes(prec, vh) * nrhs));
+  QQ_CK(out.data.alloc(field_bytes(prec, vh) * nrhs));
+  if (prec == P16) {
+    QQ_CK(in.norm.alloc(sizeof(float) * vh * nrhs));
+    QQ_CK(out.norm.alloc(sizeof(float) * vh * nrhs));
+  }
+  Tmp one(c, P64);
+  for (int k = 0; k < nrhs; ++k) {
+    const double* d = nullptr;
+    QQ_TRY(stage_in(c, 1, gin + (size_t)k * nv, nv, &d));
+    QQ_TRY(ref_to_field(c, d, 1 - pout, one.sp()));
+    QQ_TRY(block_slot(c, prec, nrhs, k, in.sp(), one.sp(), 0));
+  }
+  HopArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.g = c->g;
+  a.c = make_hopcoef(c->c1, c->c2, idag);
+  a.pout = pout;
+  a.gauge = c->gauge32.p;
+  a.nrhs = nrhs;
+  a.blk = nrhs > 1 ? 1 : 0;
+  a.in[0] = in.data.p;
+  a.in_norm[0] = in.norm.as<float>();
+  a.out[0] = out.data.p;
+  a.out_norm[0] = out.norm.as<float>();
+  if (shape == 0) {
+    QQ_TRY(launch_hop_tuned(c, a, prec, EPI_STORE));
+  } else if (launch_hop(a, prec, 12, EPI_STORE, shape, c->st) != cudaSuccess) {
+    cudaGetLastError();
+    return set_error(QQ_BAD_ARG, "kernel shape not available for this precision and RHS count");
+  }
+  for (int k = 0; k < nrhs; ++k) {
+    QQ_TRY(zero_field(c, one.sp()));
+    QQ_TRY(block_slot(c, prec, nrhs, k, out.sp(), one.sp(), 1));
+    double* d = nullptr;
+    QQ_TRY(stage_out_begin(c, 2, gout + (size_t)k * nv, nv, &d));
+    QQ_TRY(field_to_ref(c, one.sp(), pout, d));
+    QQ_TRY(stage_out_end(c, 2, gout + (size_t)k * nv, nv, d));
+    QQ_CK(cudaStreamSynchronize(c->st));
+  }
+  return QQ_OK;
+}
+
 }  // namespace qq

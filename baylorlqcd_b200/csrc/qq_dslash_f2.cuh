@@ -179,8 +179,9 @@ __device__ inline void hop2(const HopArgs& a, int s, int r0, int G, const int* x
   }
 }
 
+// Epilogue and store; g is the EPI_DBLE operand at (s, r), read by the caller.
 template <int EPI>
-__device__ inline void finish2(const HopArgs& a, int s, int r, const Pair12& acc) {
+__device__ inline void finish2_g(const HopArgs& a, int s, int r, const Pair12& acc, const Pair12& g) {
   Pair12 o;
   if (EPI == EPI_STORE) {
     o = acc;
@@ -194,8 +195,6 @@ __device__ inline void finish2(const HopArgs& a, int s, int r, const Pair12& acc
       o.im[3 + c] = f2fma(f2bc(t), acc.im[c], acc.im[3 + c]);
     }
   } else {
-    Pair12 g;
-    load_pairs(static_cast<const float4*>(a.blk ? a.aux[0] : a.aux[r]), a.vh_of(), a.idx_of(s, r), g);
     const float2 f1 = f2bc(a.f1f), f2 = f2bc(a.f2f), nf2 = f2bc(-a.f2f), nf3 = f2bc(-a.f3f);
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
@@ -206,6 +205,14 @@ __device__ inline void finish2(const HopArgs& a, int s, int r, const Pair12& acc
     }
   }
   store_pairs(static_cast<float4*>(a.blk ? a.out[0] : a.out[r]), a.vh_of(), a.idx_of(s, r), o);
+}
+
+template <int EPI>
+__device__ inline void finish2(const HopArgs& a, int s, int r, const Pair12& acc) {
+  Pair12 g;
+  if (EPI == EPI_DBLE)
+    load_pairs(static_cast<const float4*>(a.blk ? a.aux[0] : a.aux[r]), a.vh_of(), a.idx_of(s, r), g);
+  finish2_g<EPI>(a, s, r, acc, g);
 }
 
 // ---------------------------------------------------------------------------
@@ -408,6 +415,225 @@ __global__ void __launch_bounds__(128) hop_f2s_kernel(HopArgs a) {
   hop_consume<3, false>(a, B, acc);
 #undef QQ_STAGED_ISSUE
   finish2<EPI>(a, s, r, acc);
+}
+
+// ---------------------------------------------------------------------------
+// Copy-ring variant for block fields.  The kernels above hold a hop's operands in
+// registers: a thread issues the loads, waits a full L2 round trip, computes and only
+// then issues the next hop, and at 96+ registers too few warps are resident to cover
+// that wait (the hop is bound by bytes in flight per SM, not by bandwidth or
+// arithmetic).  Here every thread keeps the neighbour spinors of its next D hops in
+// flight as cp.async copies into its own slots of a shared-memory ring, which holds no
+// registers.  The EPI_DBLE operand travels through the ring as a ninth stage.  A
+// thread reads only its own ring slots, so the ring needs no barrier: the hardware
+// wait on the thread's own copy groups orders it.
+// Everything the nrhs threads of a site would otherwise repeat is done once per block:
+// the neighbour indices and boundary signs of its sites' 8 hops (a table, before any
+// copy is issued) and their 8 hop matrices (U forward, U^+ backward, third row rebuilt
+// from the recon-12 rows) in shared memory.  That leaves the threads with the spin
+// projection, the matrix product and the reconstruction.
+// Measured alternatives: matrices stored as broadcast pairs (9 shared loads per hop,
+// more registers) and 2-3 right-hand sides per thread (160+ registers, 3 blocks per
+// SM) were both slower.
+// Shared memory: neighbour table [site][hop] (int) and signs [site][hop] (float), raw
+// recon-12 rows [site][hop][3] and matrices [site][hop][5] (18 floats in 5 16-byte
+// entries, one entry of padding per site so that a warp reading three sites'
+// matrices hits distinct banks), then the ring [stage][rhs][6 planes][thread]
+// (conflict free: a warp reads consecutive entries).
+// ---------------------------------------------------------------------------
+constexpr int kF2aMatStride = 8 * 5 + 1;  // 16-byte entries per site
+
+inline size_t f2a_smem_bytes(int per_block, int threads, int depth, int rpt) {
+  return (size_t)per_block * 8 * 8 + (size_t)16 * per_block * (24 + kF2aMatStride) +
+         (size_t)16 * depth * rpt * 6 * threads;
+}
+
+struct F2aShared {
+  int* nbr;       // [site][hop] neighbour site index
+  float* sgn;     // [site][hop] boundary factor of the hop (0 = no hop)
+  float4* raw;    // [site][hop][3] recon-12 rows as stored
+  float4* mat;    // [site][kF2aMatStride] hop matrices, 18 floats per hop
+  float4* ring;   // [stage][rhs][6][thread]
+};
+
+// Stage H (hops 0-7, 8 = the EPI_DBLE operand) into ring slot H % D; always one group.
+// Thread j of a site holds right-hand sides j, j + G, ..., j + (RPT - 1) G.
+template <int H, int D, int EPI, int RPT>
+__device__ inline void f2a_issue(const HopArgs& a, const F2aShared& sh, int s, int sl, int j, int G, int T,
+                                 int tx, bool act) {
+  if constexpr (H < 8 || (H == 8 && EPI == EPI_DBLE)) {
+    if (act) {
+      const int site = H < 8 ? sh.nbr[sl * 8 + H] : s;
+      const int n = a.vh_of();
+#pragma unroll
+      for (int k = 0; k < RPT; ++k) {
+        const int r = j + k * G;
+        const void* base = H < 8 ? a.in_base(r) : (a.blk ? a.aux[0] : a.aux[r]);
+        const float4* f = static_cast<const float4*>(base) + a.idx_of(site, r);
+        float4* dst = sh.ring + ((H % D) * RPT + k) * 6 * T + tx;
+#pragma unroll
+        for (int q = 0; q < 6; ++q) cp_async16(dst + q * T, f + (size_t)q * n);
+      }
+    }
+  }
+  cp_async_commit();
+}
+
+template <int H, int D, int EPI, int RPT>
+__device__ inline void f2a_run(const HopArgs& a, const F2aShared& sh, int s, int sl, int j, int G, int T,
+                               int tx, Pair12* acc) {
+  if constexpr (H < 8) {
+    constexpr int MU = H >> 1;
+    constexpr bool FWD = !(H & 1);
+    cp_async_wait<D - 1>();  // stage H has landed; stages H+1 .. H+D-1 may be in flight
+    const float sgn = sh.sgn[sl * 8 + H];
+    if (sgn != 0.0f) {
+      const float twice = MU == 3 ? 2.0f : 1.0f;
+      const float cm = twice * sgn * (FWD ? a.c.fmf[MU] : a.c.bmf[MU]);
+      const float cp = twice * sgn * (FWD ? a.c.fpf[MU] : a.c.bpf[MU]);
+      const float4* mp = sh.mat + sl * kF2aMatStride + H * 5;
+      float me[20];
+#pragma unroll
+      for (int e = 0; e < 5; ++e) {
+        const float4 t = mp[e];
+        me[4 * e] = t.x;
+        me[4 * e + 1] = t.y;
+        me[4 * e + 2] = t.z;
+        me[4 * e + 3] = t.w;
+      }
+      LinkPairs m;
+#pragma unroll
+      for (int e = 0; e < 9; ++e) {
+        m.r[e / 3][e % 3] = f2bc(me[2 * e]);
+        m.i[e / 3][e % 3] = f2bc(me[2 * e + 1]);
+      }
+#pragma unroll
+      for (int k = 0; k < RPT; ++k) {
+        Pair12 p;
+        const float4* src = sh.ring + ((H % D) * RPT + k) * 6 * T + tx;
+#pragma unroll
+        for (int q = 0; q < 6; ++q) {
+          const float4 t = src[q * T];
+          p.re[q] = make_float2(t.x, t.y);
+          p.im[q] = make_float2(t.z, t.w);
+        }
+        float2 hre[3], him[3], wre[3], wim[3];
+        if (cm != 0.0f) {
+          project2<MU, -1>(p, hre, him);
+          matvec2(m, hre, him, wre, wim);
+          recon2<MU, -1>(acc[k], cm, wre, wim);
+        }
+        if (cp != 0.0f) {
+          project2<MU, +1>(p, hre, him);
+          matvec2(m, hre, him, wre, wim);
+          recon2<MU, +1>(acc[k], cp, wre, wim);
+        }
+      }
+    }
+    f2a_issue<H + D, D, EPI, RPT>(a, sh, s, sl, j, G, T, tx, true);
+    f2a_run<H + 1, D, EPI, RPT>(a, sh, s, sl, j, G, T, tx, acc);
+  }
+}
+
+// Thread layout: threadIdx.x = (site-in-block) * G + j, G = nrhs / RPT threads per site.
+template <int EPI, int D, int RPT>
+__global__ void __launch_bounds__(128) hop_f2a_kernel(HopArgs a) {
+  extern __shared__ float4 f2a_smem[];
+  const int T = blockDim.x, per = a.per_block, tx = threadIdx.x;
+  const int G = a.nrhs / RPT;
+  F2aShared sh;
+  sh.raw = f2a_smem;
+  sh.mat = sh.raw + per * 24;
+  sh.ring = sh.mat + per * kF2aMatStride;
+  sh.nbr = reinterpret_cast<int*>(sh.ring + D * RPT * 6 * T);
+  sh.sgn = reinterpret_cast<float*>(sh.nbr + per * 8);
+  const int s0 = blockIdx.x * per;
+  // 1. per (site, hop): neighbour index and sign; copy of the link's recon-12 rows
+  for (int k = tx; k < per * 8; k += T) {
+    const int sl = k >> 3, h = k & 7, mu = h >> 1;
+    const int ss = min(s0 + sl, a.g.vh - 1);  // sites past the end: any valid site, never read
+    int x[4];
+    site_coords(a.g, a.pout, ss, x);
+    const int back = h & 1;
+    int y[4] = {x[0], x[1], x[2], x[3]};
+    float sg = 1.0f;
+#pragma unroll
+    for (int d = 0; d < 4; ++d) {
+      if (d != mu) continue;
+      y[d] += back ? -1 : 1;
+      if (y[d] < 0 || y[d] == a.g.n[d]) {
+        y[d] = y[d] < 0 ? a.g.n[d] - 1 : 0;
+        sg = a.g.bcf[d];
+      }
+    }
+    const int sy = site_index(a.g, y);
+    sh.nbr[k] = sy;
+    sh.sgn[k] = sg;
+    // forward hop: U_mu(x) on the output parity; backward: U_mu(x - mu) on the other
+    const int lsite = back ? sy : ss, par = back ? 1 - a.pout : a.pout;
+    const float4* gl = static_cast<const float4*>(a.gauge) + (size_t)(par * 4 + mu) * 3 * a.g.vh + lsite;
+#pragma unroll
+    for (int q = 0; q < 3; ++q) cp_async16(sh.raw + k * 3 + q, gl + (size_t)q * a.g.vh);
+  }
+  cp_async_commit();
+  __syncthreads();  // the neighbour table
+  const int sl = a.div_nrhs.div(tx);
+  const int j = tx - sl * G;
+  const int s = s0 + sl;
+  const bool act = s < a.g.vh;
+  f2a_issue<0, D, EPI, RPT>(a, sh, s, sl, j, G, T, tx, act);
+  if constexpr (D > 1) f2a_issue<1, D, EPI, RPT>(a, sh, s, sl, j, G, T, tx, act);
+  if constexpr (D > 2) f2a_issue<2, D, EPI, RPT>(a, sh, s, sl, j, G, T, tx, act);
+  if constexpr (D > 3) f2a_issue<3, D, EPI, RPT>(a, sh, s, sl, j, G, T, tx, act);
+  cp_async_wait<D>();  // the link rows (the oldest group) have landed ...
+  __syncthreads();     // ... for every thread of the block
+  // 2. hop matrices: M = U (forward) or U^+ (backward), 18 floats (re, im) row-major
+  for (int k = tx; k < per * 8; k += T) {
+    Su3<float> u;
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      const float4 t = sh.raw[k * 3 + q];
+      const int c0 = 2 * q, c1 = 2 * q + 1;
+      u.e[c0 / 3][c0 % 3] = {t.x, t.y};
+      u.e[c1 / 3][c1 % 3] = {t.z, t.w};
+    }
+    reconstruct_row3(u);
+    float v[20];
+    const bool back = k & 1;
+#pragma unroll
+    for (int e = 0; e < 9; ++e) {
+      const int i = e / 3, c = e % 3;
+      v[2 * e] = back ? u.e[c][i].re : u.e[i][c].re;
+      v[2 * e + 1] = back ? -u.e[c][i].im : u.e[i][c].im;
+    }
+    v[18] = v[19] = 0.0f;
+    float4* dst = sh.mat + (k >> 3) * kF2aMatStride + (k & 7) * 5;
+#pragma unroll
+    for (int e = 0; e < 5; ++e) dst[e] = make_float4(v[4 * e], v[4 * e + 1], v[4 * e + 2], v[4 * e + 3]);
+  }
+  __syncthreads();
+  if (!act) return;
+  Pair12 acc[RPT];
+#pragma unroll
+  for (int k = 0; k < RPT; ++k)
+#pragma unroll
+    for (int q = 0; q < 6; ++q) acc[k].re[q] = acc[k].im[q] = make_float2(0.0f, 0.0f);
+  f2a_run<0, D, EPI, RPT>(a, sh, s, sl, j, G, T, tx, acc);
+  if constexpr (EPI == EPI_DBLE) cp_async_wait<D - 1>();  // stage 8
+#pragma unroll
+  for (int k = 0; k < RPT; ++k) {
+    Pair12 g;
+    if constexpr (EPI == EPI_DBLE) {
+      const float4* src = sh.ring + ((8 % D) * RPT + k) * 6 * T + tx;
+#pragma unroll
+      for (int q = 0; q < 6; ++q) {
+        const float4 t = src[q * T];
+        g.re[q] = make_float2(t.x, t.y);
+        g.im[q] = make_float2(t.z, t.w);
+      }
+    }
+    finish2_g<EPI>(a, s, j + k * G, acc[k], g);
+  }
 }
 
 // Thread layout as hop_mrhs_kernel: threadIdx.x = (site-in-block) * G + j, G = nrhs / RPT.

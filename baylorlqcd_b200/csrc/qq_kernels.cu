@@ -148,19 +148,52 @@ static cudaError_t hop_f2s(const HopArgs& a, int epi, cudaStream_t st) {
   return cudaGetLastError();
 }
 
+// Copy-ring kernel: D stages in flight per thread, RPT right-hand sides per thread.
+template <int EPI, int D, int RPT>
+static cudaError_t hop_f2a_epi(const HopArgs& b, size_t smem, cudaStream_t st) {
+  static bool attr_set = false;  // one attribute call per instantiation
+  if (!attr_set) {
+    const cudaError_t e = cudaFuncSetAttribute(hop_f2a_kernel<EPI, D, RPT>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    if (e != cudaSuccess) return e;
+    attr_set = true;
+  }
+  const int G = b.nrhs / RPT;
+  const dim3 blk(b.per_block * G), grd((b.g.vh + b.per_block - 1) / b.per_block);
+  hop_f2a_kernel<EPI, D, RPT><<<grd, blk, smem, st>>>(b);
+  return cudaGetLastError();
+}
+
+template <int D, int RPT>
+static cudaError_t hop_f2a(const HopArgs& a, int epi, cudaStream_t st) {
+  if (a.nrhs % RPT != 0 || (RPT > 1 && !a.blk)) return cudaErrorInvalidValue;
+  const int G = a.nrhs / RPT;  // threads per site
+  const int per_block = hop_sites_per_block(1, G);
+  const HopArgs b = hop_prepare(a, per_block, G);
+  const size_t smem = f2a_smem_bytes(per_block, per_block * G, D, RPT);
+  if (smem > 227 * 1024) return cudaErrorInvalidValue;
+  switch (epi) {
+    case EPI_STORE: return hop_f2a_epi<EPI_STORE, D, RPT>(b, smem, st);
+    case EPI_TWIST: return hop_f2a_epi<EPI_TWIST, D, RPT>(b, smem, st);
+    case EPI_DBLE: return hop_f2a_epi<EPI_DBLE, D, RPT>(b, smem, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
 // tps: 1, 2, 4 = register kernel with that many direction groups per site;
 // 32, 64, 96, 128 = staged kernel with that many threads per block;
 // kShapeMrhs + RPT (RPT = 2, 3, 4) = block fields with RPT right-hand sides per thread
 // (FP32 / FP16 spinors, nrhs divisible by RPT);
 // kShapeF2 + RPT (RPT = 1, 2, 3) = FP32 spinors with packed FP32x2 arithmetic (RPT > 1
-// on block fields only).
+// on block fields only); kShapeF2 + 4 = the same, loads a hop ahead; + 5 = links staged
+// in shared memory (block fields); + 6, 7, 8 = copy ring with 2, 3, 4 stages in flight.
 cudaError_t launch_hop(const HopArgs& a, int sp, int recon, int epi, int tps, cudaStream_t st) {
   count_launch();
   const int maxr = a.blk ? kMaxBatch : kMaxRhs;
   if (a.nrhs < 1 || a.nrhs > maxr) return cudaErrorInvalidValue;
   if (tps > kShapeF2) {
     const int rpt = tps - kShapeF2;
-    if (sp != P32 || (rpt < 4 && a.nrhs % rpt != 0) || (rpt > 1 && rpt != 4 && !a.blk))
+    if (sp != P32 || ((rpt == 2 || rpt == 3) && (a.nrhs % rpt != 0 || !a.blk)))
       return cudaErrorInvalidValue;
     switch (rpt) {
       case 1: return hop_f2_rpt<1>(a, epi, st);
@@ -168,6 +201,10 @@ cudaError_t launch_hop(const HopArgs& a, int sp, int recon, int epi, int tps, cu
       case 3: return hop_f2_rpt<3>(a, epi, st);
       case 4: return hop_f2p(a, epi, st);  // pipelined, one RHS per thread
       case 5: return a.blk ? hop_f2s(a, epi, st) : cudaErrorInvalidValue;  // + staged links
+      case 6: return hop_f2a<2, 1>(a, epi, st);  // copy ring, 2 / 3 / 4 stages in flight
+      case 7: return hop_f2a<3, 1>(a, epi, st);
+      case 8: return hop_f2a<4, 1>(a, epi, st);
+
       default: return cudaErrorInvalidValue;
     }
   }

@@ -162,10 +162,13 @@ int launch_hop_tuned(qq_ctx* c, const HopArgs& a, int prec, int epi) {
   int best = 1;
   float best_ms = 1e30f;
   for (int tps : {1, 2, 32, 64, 96, 128, kShapeMrhs + 2, kShapeMrhs + 3, kShapeMrhs + 4, kShapeF2 + 1,
-                  kShapeF2 + 2, kShapeF2 + 3, kShapeF2 + 4, kShapeF2 + 5}) {
+                  kShapeF2 + 2, kShapeF2 + 3, kShapeF2 + 4, kShapeF2 + 5, kShapeF2 + 6, kShapeF2 + 7,
+                  kShapeF2 + 8}) {
     const int per = tps <= 4 ? 128 / tps : tps;
     if (a.nrhs > per) continue;
-    if (tps == kShapeF2 + 5) {  // + links staged in shared memory (block fields, nrhs >= 8)
+    if (tps >= kShapeF2 + 6) {  // copy ring (its shared memory pays off from 4 RHS up)
+      if (prec != P32 || a.nrhs < 4) continue;
+    } else if (tps == kShapeF2 + 5) {  // + links staged in shared memory (block fields, nrhs >= 8)
       if (prec != P32 || !a.blk || a.nrhs < 8) continue;
     } else if (tps == kShapeF2 + 4) {  // pipelined packed kernel, one RHS per thread
       if (prec != P32) continue;

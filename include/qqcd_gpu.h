@@ -256,12 +256,27 @@ int qq_profile_hop_read(qq_ctx* ctx, long long* launches, double* ms_total, doub
  * kernel; 202-204 = block fields with 2-4 right-hand sides per thread, FP32/FP16;
  * 301-303 = FP32 with packed FP32x2 arithmetic, 1-3 right-hand sides per thread;
  * 304 = the same, one right-hand side per thread, loads issued a hop ahead;
- * 305 = 304 with the links staged in shared memory, block fields of >= 8 RHS).
+ * 305 = 304 with the links staged in shared memory, block fields of >= 8 RHS;
+ * 306, 307, 308 = one right-hand side per thread, the neighbour spinors of the next 2,
+ * 3, 4 hops in flight as asynchronous copies into a shared-memory ring, the links of
+ * neighbour indices and hop matrices of the block's sites built once per block in
+ * shared memory, >= 4 RHS recommended).
  * flush_l2 != 0 overwrites a 512 MiB buffer between launches so every launch reads
  * its operands from HBM.  ms_per_call: mean kernel time; bytes_per_call:
  * algorithmic bytes of one launch, V/2 * (8 * link bytes + nrhs * 2 * spinor bytes). */
 int qq_bench_hsingle(qq_ctx* ctx, int precision, int nrhs, int tps, int niter, int flush_l2,
                      double* ms_per_call, double* bytes_per_call);
+
+/* The hopping term of qq_hsingle (Hsingle, Q/diracops.f90:554-599) on nrhs half-lattice fields
+ * at once, computed in reduced precision the way the batched solver applies it: gin
+ * holds nrhs reference-layout input vectors back to back (parity opposite to gblclr),
+ * converted to one RHS-interleaved block field of precision 32 or 16 (a plain field for
+ * nrhs = 1), multiplied by kernel shape `shape` (the codes of qq_bench_hsingle; 0 = the
+ * autotuned choice) with FP32 recon-12 links, and written to gout as nrhs FP64
+ * reference-layout vectors.  QQ_BAD_ARG when the shape does not support this precision
+ * or RHS count. */
+int qq_hsingle_block(qq_ctx* ctx, int precision, int nrhs, int shape, double* gout, const double* gin,
+                     int idag, int gblclr);
 
 #ifdef __cplusplus
 }

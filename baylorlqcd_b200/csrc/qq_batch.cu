@@ -14,6 +14,7 @@
 // solver = 0 runs the plain FP64 GMRES-DR(m, k) of the reference on every RHS.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 
 #include "qq_ctx.h"
@@ -90,6 +91,98 @@ int block_slot(qq_ctx* c, int prec, int nb, int k, Spinor blockf, Spinor x, int 
   QQ_CK(cudaGetLastError());
   return QQ_OK;
 }
+
+bool host_loop_forced() {
+  const char* e = std::getenv("QQ_HOST_LOOP");  // testing: the host-driven loop
+  return e && std::atoi(e) != 0;
+}
+
+// The graph of the graph-driven batched BiCGStab: WHILE(iteration; IF(pending k) update k
+// for every k; loop condition).  Built by stream capture into the conditional nodes'
+// body graphs; per_iter and per_update count the library kernels of one iteration and
+// of one reliable update, for the launch counter.
+struct GraphLoop {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaStream_t aux = nullptr;
+  long long per_iter = 0, per_update = 0;
+  ~GraphLoop() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    if (aux) cudaStreamDestroy(aux);
+  }
+  template <class Chunk, class Update>
+  int build(qq_ctx* c, int nb, unsigned* ctl, unsigned all, int maxiter, Chunk& chunk, Update& update) {
+    QQ_CK(cudaStreamCreateWithFlags(&aux, cudaStreamNonBlocking));
+    QQ_CK(cudaGraphCreate(&graph, 0));
+    cudaGraphConditionalHandle hw;
+    QQ_CK(cudaGraphConditionalHandleCreate(&hw, graph, 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams wp = {};
+    wp.type = cudaGraphNodeTypeConditional;
+    wp.conditional.handle = hw;
+    wp.conditional.type = cudaGraphCondTypeWhile;
+    wp.conditional.size = 1;
+    cudaGraphNode_t wn;
+    QQ_CK(cudaGraphAddNode(&wn, graph, nullptr, 0, &wp));
+    CondHandles hs = {};
+    for (int k = 0; k < nb; ++k) QQ_CK(cudaGraphConditionalHandleCreate(&hs.h[k], wp.conditional.phGraph_out[0], 0, 0));
+    const long long n0 = launch_count();
+    QQ_CK(cudaStreamBeginCaptureToGraph(c->st, wp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                        cudaStreamCaptureModeThreadLocal));
+    int rc = chunk();
+    per_iter = launch_count() - n0 + 2;  // + the two condition kernels
+    if (rc == QQ_OK) {
+      count_launch();
+      reliable_conds_kernel<<<1, 32, 0, c->st>>>(ctl, hs, nb);
+      if (cudaGetLastError() != cudaSuccess) rc = set_error(QQ_CUDA_ERR, "condition kernel launch failed");
+    }
+    for (int k = 0; k < nb && rc == QQ_OK; ++k) {
+      cudaStreamCaptureStatus cs;
+      cudaGraph_t cg = nullptr;
+      const cudaGraphNode_t* deps = nullptr;
+      size_t nd = 0;
+      cudaGraphNodeParams ip = {};
+      ip.type = cudaGraphNodeTypeConditional;
+      ip.conditional.handle = hs.h[k];
+      ip.conditional.type = cudaGraphCondTypeIf;
+      ip.conditional.size = 1;
+      cudaGraphNode_t in;
+      if (cudaStreamGetCaptureInfo(c->st, &cs, nullptr, &cg, &deps, &nd) != cudaSuccess ||
+          cudaGraphAddNode(&in, cg, deps, nd, &ip) != cudaSuccess ||
+          cudaStreamUpdateCaptureDependencies(c->st, &in, 1, cudaStreamSetCaptureDependencies) != cudaSuccess) {
+        rc = set_error(QQ_CUDA_ERR, "conditional node construction failed");
+        break;
+      }
+      // the IF body: right-hand side k's update, captured from the second stream
+      std::swap(c->st, aux);
+      const long long m0 = launch_count();
+      if (cudaStreamBeginCaptureToGraph(c->st, ip.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                        cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        std::swap(c->st, aux);
+        rc = set_error(QQ_CUDA_ERR, "capture of a reliable update failed");
+        break;
+      }
+      rc = update(k);
+      per_update = launch_count() - m0;
+      cudaGraph_t ig = nullptr;
+      const cudaError_t ee = cudaStreamEndCapture(c->st, &ig);
+      std::swap(c->st, aux);
+      if (rc == QQ_OK && ee != cudaSuccess) rc = set_error(QQ_CUDA_ERR, "capture of a reliable update failed");
+    }
+    if (rc == QQ_OK) {
+      count_launch();
+      loop_cond_kernel<<<1, 1, 0, c->st>>>(ctl, all, (unsigned)maxiter, hw);
+      if (cudaGetLastError() != cudaSuccess) rc = set_error(QQ_CUDA_ERR, "condition kernel launch failed");
+    }
+    cudaGraph_t bg = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(c->st, &bg);
+    count_launch(-(launch_count() - n0));  // captured, not launched: counted when the graph runs
+    if (rc != QQ_OK) return rc;
+    QQ_CK(e);
+    QQ_CK(cudaGraphInstantiate(&exec, graph, 0));
+    return QQ_OK;
+  }
+};
 
 int full_residual(qq_ctx* c, Spinor be, Spinor bo, Spinor xe, Spinor xo, const double kappa[2],
                   double* rel) {
@@ -263,11 +356,19 @@ int bicgstab_block_sync(qq_ctx* c, std::vector<PerRhs*>& rhs, int prec, double t
 // Device-driven variant (no deflation): the reliable update itself runs on the device
 // -- the FP64 true residual, its norm, the convergence decision, the re-insertion of
 // the residual and the re-activation are stream-ordered kernels, the decision a
-// one-thread kernel -- so the host never waits inside the iteration.  It queues chunk
-// c and a snapshot of the scalars, then reads snapshot c - 1 while chunk c runs and
-// queues the updates of right-hand sides that went pending.  Updates queued at step c
-// are visible from snapshot c + 1 on, so earlier snapshots' pending marks for them
-// are skipped.
+// one-thread kernel.  Two drivers share those kernels:
+//  - graph loop (default): one CUDA graph holds the whole solve.  A WHILE conditional
+//    node repeats the iteration; after it one IF node per right-hand side runs that
+//    right-hand side's reliable update when it went pending, and a one-thread kernel
+//    sets the WHILE condition (some right-hand side still moving, fewer than maxiter
+//    iterations).  The host launches the graph once and waits, so a descheduled host
+//    thread cannot leave the GPU idle, and a pending right-hand side resumes in the
+//    next iteration.  The true-residual history is recorded on the device.
+//  - host loop (when hop profiling is on, or QQ_HOST_LOOP=1): the host queues an
+//    iteration and a snapshot of the scalars, reads the previous snapshot while it
+//    runs and queues the updates of right-hand sides that went pending.  Updates queued
+//    at step c are visible from snapshot c + 1 on, so earlier snapshots' pending marks
+//    for them are skipped.
 int bicgstab_block(qq_ctx* c, std::vector<PerRhs*>& rhs, int prec, double tol, double delta,
                    int maxiter, const double kappa[2], const DeflSpace* defl,
                    std::vector<SolveStats>& stats) {
@@ -282,11 +383,14 @@ int bicgstab_block(qq_ctx* c, std::vector<PerRhs*>& rhs, int prec, double tol, d
     if (prec == P16) QQ_CK(cudaMemsetAsync(f->norm.p, 0, f->norm.bytes, c->st));
   }
   constexpr size_t kScalDoubles = (size_t)kScal * kMaxBatch;
-  constexpr size_t kSnap = kScalDoubles + 2;  // scalars + 4 control words
+  constexpr size_t kSnap = kScalDoubles + (kCtlWords + 1) / 2;  // scalars + control words
+  constexpr int kHist = 1024;  // true-residual history per right-hand side (qq_solve_info)
   const size_t sbytes = sizeof(double) * kSnap;
   static_assert(1024 + 2 * kSnap <= 3072, "snapshots exceed the pinned buffer");
-  DevBuf S, part, dslots;
+  DevBuf S, part, dslots, dhist, dhits;
   QQ_CK(S.alloc(sbytes));
+  QQ_CK(dhist.alloc(sizeof(double) * kHist * nb));
+  QQ_CK(dhits.alloc(sizeof(int) * kHist * nb));
   QQ_CK(part.alloc(sizeof(double) * 3 * kRedBlocks * kMaxBatch));
   QQ_CK(dslots.alloc(sizeof(int) * kMaxBatch));
   double* Sd = S.as<double>();
@@ -371,13 +475,51 @@ int bicgstab_block(qq_ctx* c, std::vector<PerRhs*>& rhs, int prec, double tol, d
     QQ_TRY(lin(c, R.r64.sp(), cimm(1.0), R.b.sp(), cimm(-1.0), h.sp(), cimm(0), Spinor{nullptr, nullptr, P64},
                Sd + (size_t)k * kScal + SC_T2));
     count_launch(2);
-    reliable_decide_kernel<<<1, 1, 0, c->st>>>(Sd, ds, ctl, k, tol);
+    reliable_decide_kernel<<<1, 1, 0, c->st>>>(Sd, ds, ctl, k, tol, dhist.as<double>(), dhits.as<int>(), kHist);
     QQ_CK(cudaGetLastError());
     QQ_TRY(block_slot(c, prec, nb, k, r.sp(), R.r64.sp(), 0, ctl + CTL_INSERT));
     reliable_resume_kernel<<<1, 1, 0, c->st>>>(ctl, k);
     QQ_CK(cudaGetLastError());
     return QQ_OK;
   };
+  if (!c->prof_hop && !host_loop_forced()) {
+    // every hop shape of the loop is tuned here, outside the capture (the autotuner
+    // times its candidates with synchronising events); v is overwritten before use
+    QQ_TRY(op_dbletm_block(c, v.sp(), p.sp(), tmp.sp(), nb, 0, kappa));
+    QQ_CK(cudaStreamSynchronize(c->st));
+    GraphLoop gl;
+    QQ_TRY(gl.build(c, nb, ctl, all, maxiter, run_chunk, reliable));
+    QQ_CK(cudaGraphLaunch(gl.exec, c->st));
+    QQ_CK(cudaMemcpyAsync(hS, Sd, sbytes, cudaMemcpyDeviceToHost, c->st));
+    std::vector<double> hist((size_t)kHist * nb);
+    std::vector<int> hits((size_t)kHist * nb);
+    QQ_CK(cudaMemcpyAsync(hist.data(), dhist.p, sizeof(double) * hist.size(), cudaMemcpyDeviceToHost, c->st));
+    QQ_CK(cudaMemcpyAsync(hits.data(), dhits.p, sizeof(int) * hits.size(), cudaMemcpyDeviceToHost, c->st));
+    QQ_CK(cudaStreamSynchronize(c->st));
+    const unsigned* hc = reinterpret_cast<const unsigned*>(hS + kScalDoubles);
+    long long nupd_all = 0;
+    bool nan = false;
+    for (int k = 0; k < nb; ++k) {
+      SolveStats& st = stats[k];
+      const double* sk = hS + (size_t)k * kScal;
+      const int its = (int)sk[SC_ITS], nupd = (int)sk[SC_NUPD];
+      st.itercount = its;
+      st.mvp += 2 * its + nupd;
+      for (int j = 0; j < std::min(nupd, kHist); ++j) {
+        const double rel = hist[(size_t)k * kHist + j];
+        nan = nan || !std::isfinite(rel);
+        st.hist.push_back(rel);
+        st.hist_mvp.push_back(1 + 2 * hits[(size_t)k * kHist + j] + j + 1);
+      }
+      if (nupd > 0) st.true_rel = sk[SC_TRUE];
+      nupd_all += nupd;
+    }
+    count_launch(gl.per_iter * (long long)hc[CTL_ITER] + gl.per_update * nupd_all);
+    if (nan) return set_error(QQ_NAN, "NaN true residual in batched BiCGStab");
+    done = hc[CTL_DONE];
+    for (int k = 0; k < nb; ++k) rhs[k]->done = (done >> k) & 1u;
+    return (done & all) == all ? QQ_OK : QQ_NOT_CONVERGED;
+  }
   cudaEvent_t ev[2];
   QQ_CK(cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming));
   QQ_CK(cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming));

@@ -33,7 +33,7 @@ enum ScalSlot : int {
 // iterates), [1] pending mask (bit r: r stopped and waits for its reliable update or
 // convergence test), [2] done mask (r converged), [3] insert mask (r's new FP64
 // residual is to replace its iterated one).
-enum CtlWord : int { CTL_ACTIVE = 0, CTL_PENDING = 1, CTL_DONE = 2, CTL_INSERT = 3 };
+enum CtlWord : int { CTL_ACTIVE = 0, CTL_PENDING = 1, CTL_DONE = 2, CTL_INSERT = 3, CTL_ITER = 4, kCtlWords = 5 };
 
 enum BiOp : int {
   OP_DOT_RHAT_R = 0,  // red: <rhat, r>
@@ -211,12 +211,19 @@ static __global__ void bicg_scalar_kernel(double* S, const int* slots, const dou
 // End of right-hand side k's reliable update, after ||b - A x||^2 has landed in
 // S[SC_T2]: record the true residual, decide convergence, and either mark k done or
 // arm the re-insertion of the FP64 residual (rmax = ||r||).  One thread.
+// Every decision is also appended to right-hand side k's history: hist[k * hmax + j] =
+// the j-th true relative residual, hist_its[k * hmax + j] = the iterations done then.
 static __global__ void reliable_decide_kernel(double* S, const int* slots, unsigned* ctl, int k,
-                                              double tol) {
+                                              double tol, double* hist, int* hist_its, int hmax) {
   double* s = S + (size_t)slots[k] * kScal;
   const double rn = sqrt(s[SC_T2]);
   const double rel = rn / s[SC_BN];
   s[SC_TRUE] = rel;
+  const int j = (int)s[SC_NUPD];
+  if (j < hmax) {
+    hist[(size_t)k * hmax + j] = rel;
+    hist_its[(size_t)k * hmax + j] = (int)s[SC_ITS];
+  }
   s[SC_NUPD] += 1.0;
   const unsigned bit = 1u << k;
   if (!(rel > tol)) {  // converged (a NaN residual is reported as converged and caught on the host)
@@ -236,6 +243,30 @@ static __global__ void reliable_resume_kernel(unsigned* ctl, int k) {
     atomicAnd(&ctl[CTL_INSERT], ~bit);
     atomicOr(&ctl[CTL_ACTIVE], bit);
   }
+}
+
+// Conditions of the graph-driven loop (CUDA graph conditional nodes).
+struct CondHandles {
+  cudaGraphConditionalHandle h[kMaxBatch];
+};
+
+// IF node k (right-hand side k's reliable update) runs when k is pending.
+static __global__ void reliable_conds_kernel(const unsigned* ctl, CondHandles hs, int nb) {
+  const int k = threadIdx.x;
+  if (k < nb) {
+    const unsigned pend = ctl[CTL_PENDING] & ~ctl[CTL_DONE];
+    cudaGraphSetConditional(hs.h[k], (pend >> k) & 1u);
+  }
+}
+
+// WHILE node: another iteration while a right-hand side of `all` can still move and
+// fewer than maxiter iterations have run.
+static __global__ void loop_cond_kernel(unsigned* ctl, unsigned all, unsigned maxiter,
+                                        cudaGraphConditionalHandle h) {
+  const unsigned n = ctl[CTL_ITER] + 1u;
+  ctl[CTL_ITER] = n;
+  const unsigned live = (ctl[CTL_ACTIVE] | ctl[CTL_PENDING]) & ~ctl[CTL_DONE] & all;
+  cudaGraphSetConditional(h, live != 0u && n < maxiter ? 1u : 0u);
 }
 
 // Slot k of a block field <-> a separate FP64 field.

@@ -56,6 +56,30 @@ def test_batch_vs_oracle(setup, solver, precision, deflate, kappa):
         assert interior_rel(xo[i], xo_o, ol.nvhalf) < 1e-7
 
 
+@pytest.mark.parametrize("precision", [32, 16])
+def test_graph_and_host_loops_agree(setup, monkeypatch, precision):
+    """The graph-driven loop (one CUDA graph with conditional nodes) and the host-driven
+    loop run the same per-RHS recurrences with fixed-order reductions: a right-hand side
+    that waits for its reliable update does not change its own sequence.  Same iteration
+    counts, update histories and solutions."""
+    lat, ol, u = setup
+    be, bo = sources(lat, 6)
+    kappa = (0.150, 0.01)
+    res = {}
+    for mode in ("0", "1"):
+        monkeypatch.setenv("QQ_HOST_LOOP", mode)
+        res[mode] = lat.fermprop_batch(be, bo, kappa, m=16, k=6, precision=precision, rhs_block=6,
+                                       tol=1e-10, solver=1)
+    (xg, og, ig), (xh, oh, ih) = res["0"], res["1"]
+    for i in range(6):
+        assert ig[i].status == 0 and ih[i].status == 0
+        assert ig[i].itercount == ih[i].itercount and ig[i].mvp == ih[i].mvp
+        assert len(ig[i].hist) == len(ih[i].hist) > 0
+        assert np.array_equal(ig[i].hist, ih[i].hist)
+    assert interior_rel(xg, xh, ol.nvhalf) < 1e-14
+    assert interior_rel(og, oh, ol.nvhalf) < 1e-14
+
+
 def test_batch_device_arrays(setup):
     """Inputs and outputs already in HBM (torch CUDA tensors): same answers."""
     import torch

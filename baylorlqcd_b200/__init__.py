@@ -36,6 +36,7 @@ EXPORTED = [
     "qq_rnds", "qq_z2source", "qq_z4source", "qq_twaverage_level0", "qq_discon_traces", "qq_bench_hsingle",
     "qq_heatbath", "qq_ctx_stream", "qq_launch_count", "qq_profile_hop", "qq_profile_hop_read",
     "qq_gfwrite", "qq_gfread", "qq_fpwrite", "qq_fpread", "qq_hsingle_block",
+    "qq_hop_tuned_shape",
 ]
 
 
@@ -132,6 +133,7 @@ def load_library() -> C.CDLL:
         "qq_discon_traces": ([P, I, I, DP, C.POINTER(qq_method), D, I, P, C.POINTER(qq_solve_info)], I),
         "qq_bench_hsingle": ([P, I, I, I, I, I, DP, DP], I),
         "qq_hsingle_block": ([P, I, I, I, P, P, I, I], I),
+        "qq_hop_tuned_shape": ([P, I, I, IP], I),
         "qq_heatbath": ([P, D, I, C.c_ulonglong, P, DP], I),
         "qq_ctx_stream": ([P, C.POINTER(P)], I),
         "qq_launch_count": ([], C.c_longlong),
@@ -279,6 +281,12 @@ class Lattice:
         out = self.new_half() if out is None else out
         _check(self.lib.qq_hsingle(self._ctx, _ptr(out), _ptr(gin), idag, gblclr))
         return out
+
+    def hop_tuned_shape(self, precision: int, nrhs: int) -> int:
+        """The hopping-kernel shape the autotuner chose for this precision and RHS count."""
+        v = C.c_int()
+        _check(self.lib.qq_hop_tuned_shape(self._ctx, precision, nrhs, C.byref(v)))
+        return v.value
 
     def hsingle_block(self, gin, idag: int, gblclr: int, precision: int = 32, shape: int = 0):
         """H on a stack of half vectors (shape (nrhs,) + half_shape) in reduced precision

@@ -225,10 +225,11 @@ int bicgstab_block_sync(qq_ctx* c, std::vector<PerRhs*>& rhs, int prec, double t
     QQ_CK(cudaMemsetAsync(f->data.p, 0, f->data.bytes, c->st));
     if (prec == P16) QQ_CK(cudaMemsetAsync(f->norm.p, 0, f->norm.bytes, c->st));
   }
-  // scalars of every right-hand side, then the two control words
+  // scalars of every right-hand side, then the control words
   constexpr size_t kScalDoubles = (size_t)kScal * kMaxBatch;
+  constexpr size_t kSyncDoubles = kScalDoubles + (kCtlWords + 1) / 2;
   DevBuf S, part, dslots;
-  QQ_CK(S.alloc(sizeof(double) * (kScalDoubles + 1)));
+  QQ_CK(S.alloc(sizeof(double) * (kSyncDoubles)));
   QQ_CK(part.alloc(sizeof(double) * 3 * kRedBlocks * kMaxBatch));
   QQ_CK(dslots.alloc(sizeof(int) * kMaxBatch));
   unsigned* ctl = reinterpret_cast<unsigned*>(S.as<double>() + kScalDoubles);
@@ -249,9 +250,9 @@ int bicgstab_block_sync(qq_ctx* c, std::vector<PerRhs*>& rhs, int prec, double t
     return QQ_OK;
   };
   // host mirror in the solver's half of the context's pinned buffer
-  static_assert(kScalDoubles + 1 <= 1024, "scalar mirror exceeds the pinned buffer");
+  static_assert(kSyncDoubles <= 1024, "scalar mirror exceeds the pinned buffer");
   double* hS = c->hpin + 1024;
-  std::fill(hS, hS + kScalDoubles + 1, 0.0);
+  std::fill(hS, hS + kSyncDoubles, 0.0);
   unsigned* hctl = reinterpret_cast<unsigned*>(hS + kScalDoubles);
   std::vector<int> slots(nb);
   unsigned active = 0;
@@ -274,7 +275,7 @@ int bicgstab_block_sync(qq_ctx* c, std::vector<PerRhs*>& rhs, int prec, double t
   }
   hctl[CTL_ACTIVE] = active;
   hctl[CTL_PENDING] = 0u;
-  QQ_CK(cudaMemcpyAsync(S.p, hS, sizeof(double) * (kScalDoubles + 1), cudaMemcpyHostToDevice, c->st));
+  QQ_CK(cudaMemcpyAsync(S.p, hS, sizeof(double) * (kSyncDoubles), cudaMemcpyHostToDevice, c->st));
   QQ_CK(cudaMemcpyAsync(dslots.p, slots.data(), sizeof(int) * nb, cudaMemcpyHostToDevice, c->st));
   QQ_CK(cudaStreamSynchronize(c->st));
   BlockBiArgs A;
@@ -312,8 +313,9 @@ int bicgstab_block_sync(qq_ctx* c, std::vector<PerRhs*>& rhs, int prec, double t
       QQ_TRY(block_op(c, prec, A, OP_XR_UPDATE, ds, ST_R2, sc));
     }
     done_its += nchunk;
-    QQ_CK(cudaMemcpyAsync(hS, S.p, sizeof(double) * (kScalDoubles + 1), cudaMemcpyDeviceToHost, c->st));
+    QQ_CK(cudaMemcpyAsync(hS, S.p, sizeof(double) * (kSyncDoubles), cudaMemcpyDeviceToHost, c->st));
     QQ_CK(cudaStreamSynchronize(c->st));
+    if (hctl[CTL_NAN]) return set_error(QQ_NAN, "NaN residual in batched BiCGStab");
     const unsigned pending = hctl[CTL_PENDING];
     unsigned back = 0;  // right-hand sides that iterate again after their update
     for (int k = 0; k < nb; ++k) {
@@ -346,7 +348,7 @@ int bicgstab_block_sync(qq_ctx* c, std::vector<PerRhs*>& rhs, int prec, double t
       active = (hctl[CTL_ACTIVE] | back) & active;
       hctl[CTL_ACTIVE] = active;
       hctl[CTL_PENDING] = 0u;
-      QQ_CK(cudaMemcpyAsync(S.p, hS, sizeof(double) * (kScalDoubles + 1), cudaMemcpyHostToDevice, c->st));
+      QQ_CK(cudaMemcpyAsync(S.p, hS, sizeof(double) * (kSyncDoubles), cudaMemcpyHostToDevice, c->st));
     }
   }
   QQ_CK(cudaStreamSynchronize(c->st));
@@ -515,7 +517,7 @@ int bicgstab_block(qq_ctx* c, std::vector<PerRhs*>& rhs, int prec, double tol, d
       nupd_all += nupd;
     }
     count_launch(gl.per_iter * (long long)hc[CTL_ITER] + gl.per_update * nupd_all);
-    if (nan) return set_error(QQ_NAN, "NaN true residual in batched BiCGStab");
+    if (nan || (hc[CTL_NAN] & all)) return set_error(QQ_NAN, "NaN residual in batched BiCGStab");
     done = hc[CTL_DONE];
     for (int k = 0; k < nb; ++k) rhs[k]->done = (done >> k) & 1u;
     return (done & all) == all ? QQ_OK : QQ_NOT_CONVERGED;
@@ -568,6 +570,7 @@ int bicgstab_block(qq_ctx* c, std::vector<PerRhs*>& rhs, int prec, double tol, d
         nupd_seen[k] = nupd;
       }
     }
+    if (sc[CTL_NAN] & all) return set_error(QQ_NAN, "NaN residual in batched BiCGStab");
     done = sc[CTL_DONE];
     if ((done & all) == all) break;
     const unsigned pend = sc[CTL_PENDING] & ~done;

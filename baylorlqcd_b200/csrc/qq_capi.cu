@@ -464,6 +464,21 @@ extern "C" int qq_hsingle_block(qq_ctx* c, int precision, int nrhs, int shape, d
   return hsingle_block(c, prec, nrhs, shape, gout, gin, idag, gblclr - 1);
 }
 
+extern "C" int qq_hop_tuned_shape(qq_ctx* c, int precision, int nrhs, int* shape) {
+  QQ_TRY(check_ctx(c));
+  if (!shape) return set_error(QQ_BAD_ARG, "null argument");
+  const int prec = precision == 64 ? P64 : precision == 32 ? P32 : precision == 16 ? P16 : -1;
+  if (prec < 0 || nrhs < 1 || nrhs > kMaxBatch) return set_error(QQ_BAD_ARG, "bad precision or nrhs");
+  HopArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.nrhs = nrhs;
+  a.blk = nrhs > 1 ? 1 : 0;
+  auto it = c->hop_tune.find(hop_tune_key(c, a, prec, EPI_STORE));
+  if (it == c->hop_tune.end()) return set_error(QQ_BAD_ARG, "no hopping launch of that kind has been tuned yet");
+  *shape = it->second;
+  return QQ_OK;
+}
+
 extern "C" int qq_bench_hsingle(qq_ctx* c, int precision, int nrhs, int tps, int niter,
                                 int flush_l2, double* ms_per_call, double* bytes_per_call) {
   QQ_TRY(check_ctx(c));

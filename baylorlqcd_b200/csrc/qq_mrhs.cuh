@@ -33,7 +33,18 @@ enum ScalSlot : int {
 // iterates), [1] pending mask (bit r: r stopped and waits for its reliable update or
 // convergence test), [2] done mask (r converged), [3] insert mask (r's new FP64
 // residual is to replace its iterated one).
-enum CtlWord : int { CTL_ACTIVE = 0, CTL_PENDING = 1, CTL_DONE = 2, CTL_INSERT = 3, CTL_ITER = 4, kCtlWords = 5 };
+// Control words: bit k of ACTIVE / PENDING / DONE / INSERT / NAN = right-hand side k
+// iterates / awaits its reliable update / is finished / is re-inserted / stopped on a
+// non-finite residual; ITER counts the iterations of the graph-driven loop.
+enum CtlWord : int {
+  CTL_ACTIVE = 0,
+  CTL_PENDING = 1,
+  CTL_DONE = 2,
+  CTL_INSERT = 3,
+  CTL_ITER = 4,
+  CTL_NAN = 5,
+  kCtlWords = 6
+};
 
 enum BiOp : int {
   OP_DOT_RHAT_R = 0,  // red: <rhat, r>
@@ -201,7 +212,11 @@ static __global__ void bicg_scalar_kernel(double* S, const int* slots, const dou
     s[SC_R2] = d0;
     s[SC_ITS] += 1.0;
     const double rn = sqrt(d0);
-    if (!isfinite(rn) || rn < delta * s[SC_RMAX] || rn < half_tol * s[SC_BN]) {
+    if (!isfinite(rn)) {  // diverged: k stops, flagged for the host
+      atomicAnd(&ctl[CTL_ACTIVE], ~(1u << k));
+      atomicOr(&ctl[CTL_NAN], 1u << k);
+      atomicOr(&ctl[CTL_DONE], 1u << k);
+    } else if (rn < delta * s[SC_RMAX] || rn < half_tol * s[SC_BN]) {
       atomicAnd(&ctl[CTL_ACTIVE], ~(1u << k));
       atomicOr(&ctl[CTL_PENDING], 1u << k);
     }
@@ -226,7 +241,8 @@ static __global__ void reliable_decide_kernel(double* S, const int* slots, unsig
   }
   s[SC_NUPD] += 1.0;
   const unsigned bit = 1u << k;
-  if (!(rel > tol)) {  // converged (a NaN residual is reported as converged and caught on the host)
+  if (!(rel > tol)) {  // converged, or a NaN true residual (flagged for the host)
+    if (!isfinite(rel)) atomicOr(&ctl[CTL_NAN], bit);
     atomicOr(&ctl[CTL_DONE], bit);
     atomicAnd(&ctl[CTL_INSERT], ~bit);
   } else {

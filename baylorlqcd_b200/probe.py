@@ -1,0 +1,98 @@
+"""Profiling drivers for the hopping kernels and the batched solver.
+
+    python -m baylorlqcd_b200.probe hop   [--dims 16,16,16,32] [--nrhs 12] [--precision 32]
+                                          [--shape 0] [--iters 20] [--no-flush]
+    python -m baylorlqcd_b200.probe solve [--dims 16,16,16,32] [--nrhs 12] [--precision 32]
+                                          [--kappa 0.1565] [--sweeps 500] [--gauge-cache FILE]
+
+``hop`` times one hopping-kernel shape (qq_bench_hsingle: random fields, L2 flushed
+between launches unless --no-flush) and prints its time and algorithmic bandwidth.
+
+``solve`` runs the batched mixed-precision solve of the 12 spin-colour point sources
+twice -- the first run tunes every kernel shape -- and wraps the second in the NVTX
+range ``solve``, so a profiler can select its launches (ncu --nvtx --nvtx-include
+"solve/").  With --gauge-cache the heatbath configuration is written to FILE in the
+reference's GFwrite format on the first run and read back on later runs, which keeps
+the heatbath's launches out of a profiled run.
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import sys
+
+import numpy as np
+
+
+def _dims(s: str):
+    return tuple(int(x) for x in s.split(","))
+
+
+def run_hop(a) -> None:
+    import baylorlqcd_b200 as qq
+
+    lat = qq.Lattice(*_dims(a.dims))
+    lat.heatbath(6.0, 20, seed=13)
+    ms, by = lat.bench_hsingle(a.precision, a.nrhs, a.iters, not a.no_flush, a.shape)
+    print(f"hop precision {a.precision} nrhs {a.nrhs} shape {a.shape}: {ms * 1e3:.1f} us, "
+          f"{by / ms / 1e6:.0f} GB/s algorithmic", flush=True)
+    lat.close()
+
+
+def run_solve(a) -> None:
+    import torch
+
+    import baylorlqcd_b200 as qq
+
+    dims = _dims(a.dims)
+    lat = qq.Lattice(*dims, bc=(1, 1, 1, -1))
+    if a.gauge_cache and os.path.exists(a.gauge_cache):
+        u, _ = qq.gfread(a.gauge_cache, lat.nvhalf, lat.ntotal)
+        lat.gauge_upload(u)
+    else:
+        u, _ = lat.heatbath(6.0, a.sweeps, seed=13)
+        if a.gauge_cache:
+            qq.gfwrite(a.gauge_cache, u, lat.nvhalf, beta=6.0)
+    be = np.zeros((a.nrhs,) + lat.half_shape)
+    bo = np.zeros_like(be)
+    for i in range(a.nrhs):
+        be[i], bo[i] = lat.pointsource((1, 1, 1, 1), i % 3 + 1, (i // 3) % 4 + 1)
+    bed, bod = torch.from_numpy(be).cuda(), torch.from_numpy(bo).cuda()
+    xe, xo = torch.zeros_like(bed), torch.zeros_like(bod)
+    kw = dict(precision=a.precision, rhs_block=a.nrhs, tol=1e-10, solver=1, deflate=0, xe=xe, xo=xo)
+    lat.fermprop_batch(bed, bod, (a.kappa, 0.0), **kw)
+    torch.cuda.synchronize()
+    n0 = qq.launch_count()
+    torch.cuda.nvtx.range_push("solve")
+    _, _, infos = lat.fermprop_batch(bed, bod, (a.kappa, 0.0), **kw)
+    torch.cuda.synchronize()
+    torch.cuda.nvtx.range_pop()
+    print("iterations", [i.itercount for i in infos], "max true_rel", max(i.true_rel for i in infos),
+          "library launches", qq.launch_count() - n0, flush=True)
+    lat.close()
+
+
+def main(argv=None) -> int:
+    p = argparse.ArgumentParser(prog="python -m baylorlqcd_b200.probe")
+    sub = p.add_subparsers(dest="cmd", required=True)
+    h = sub.add_parser("hop")
+    h.add_argument("--dims", default="16,16,16,32")
+    h.add_argument("--nrhs", type=int, default=12)
+    h.add_argument("--precision", type=int, default=32)
+    h.add_argument("--shape", type=int, default=0)
+    h.add_argument("--iters", type=int, default=20)
+    h.add_argument("--no-flush", action="store_true")
+    s = sub.add_parser("solve")
+    s.add_argument("--dims", default="16,16,16,32")
+    s.add_argument("--nrhs", type=int, default=12)
+    s.add_argument("--precision", type=int, default=32)
+    s.add_argument("--kappa", type=float, default=0.1565)
+    s.add_argument("--sweeps", type=int, default=500)
+    s.add_argument("--gauge-cache", default=None)
+    a = p.parse_args(argv)
+    (run_hop if a.cmd == "hop" else run_solve)(a)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

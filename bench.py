@@ -101,6 +101,26 @@ def peaks():
     return FALLBACK_HBM, "fallback"
 
 
+def shape_name(shape: int) -> str:
+    """Kernel behind a hopping-kernel shape code (qq_bench_hsingle)."""
+    if shape in (1, 2, 4):
+        return "hop_kernel"
+    if 32 <= shape <= 128:
+        return "hop_staged_kernel"
+    if 202 <= shape <= 204:
+        return "hop_mrhs_kernel"
+    return {301: "hop_f2_kernel", 302: "hop_f2_kernel", 303: "hop_f2_kernel", 304: "hop_f2p_kernel",
+            305: "hop_f2s_kernel", 306: "hop_f2a_kernel", 307: "hop_f2a_kernel",
+            308: "hop_f2a_kernel"}.get(shape, "hop kernel")
+
+
+# DRAM bytes (read + write) of one EPI_STORE launch from an ncu capture, keyed by
+# (shape, precision, RHS, lattice); the capture's summary is the source.
+NCU_TRAFFIC = {
+    (307, 32, 12, (16, 16, 16, 32)): (151.8e6, "profiles/hop_f2a_kernel_fp32_blk12_16x16x16x32.md"),
+}
+
+
 class Clocks:
     """nvidia-smi sampler (200 ms) running during the timed region."""
 
@@ -232,7 +252,9 @@ def run_ours(a, rank, world, local):
     bo_h = torch.from_numpy(bo).pin_memory().numpy()
     xe_h = torch.zeros(be.shape, dtype=torch.float64).pin_memory().numpy()
     xo_h = torch.zeros(bo.shape, dtype=torch.float64).pin_memory().numpy()
-    e2e_ms = [step(be_h, bo_h, xe_h, xo_h)[0] for _ in range(max(1, min(2, a.steps)))]
+    e2e_ms = [step(be_h, bo_h, xe_h, xo_h)[0] for _ in range(a.steps)]
+    print("step ms: timed %s; e2e %s" % (["%.0f" % t for t in times], ["%.0f" % t for t in e2e_ms]),
+          file=sys.stderr, flush=True)
     e2e = sum(e2e_ms) * 1e-3 / (len(e2e_ms) * a.nrhs)
     half_bytes = int(np.prod(lat.half_shape)) * 8
 
@@ -243,6 +265,8 @@ def run_ours(a, rank, world, local):
     lat.profile_hop(False)
     hbm, hbm_kind = peaks()
     achieved = hop_bytes / (hop_ms * 1e-3) / 1e9 if hop_ms > 0 else 0.0
+    shape = lat.hop_tuned_shape(a.precision, a.rhs_block)
+    traffic = NCU_TRAFFIC.get((shape, a.precision, a.rhs_block, dims))
 
     # plain FP64 GMRES-DR (the reference method) on the same GPU
     npl = max(1, min(a.plain_rhs, a.nrhs))
@@ -280,9 +304,10 @@ def run_ours(a, rank, world, local):
         "speedup_vs_plain_gmresdr": plain / (spr * world) if spr > 0 else None,
         "e2e": {"value": e2e, "unit": "s/RHS", "h2d_bytes_per_step": 2 * a.nrhs * half_bytes,
                 "d2h_bytes_per_step": 2 * a.nrhs * half_bytes},
-        "roofline": {"bound": "hbm", "kernel": "hop_kernel (Dslash, %d-bit)" % a.precision,
+        "roofline": {"bound": "hbm", "kernel": "%s (Dslash, %d-bit, shape %d)" % (shape_name(shape), a.precision, shape),
                      "achieved": achieved, "peak": hbm, "peak_kind": hbm_kind, "unit": "GB/s",
-                     "frac": achieved / hbm, "traffic": None, "launches_measured": nlaunch,
+                     "frac": achieved / hbm, "traffic": traffic[0] if traffic else None,
+                     "traffic_source": traffic[1] if traffic else None, "launches_measured": nlaunch,
                      "avg_launch_us": hop_ms * 1e3 / max(nlaunch, 1)},
         "gpu_launches": int(n1 - n0),
         "clocks": clk,

@@ -267,6 +267,11 @@ int qq_profile_hop_read(qq_ctx* ctx, long long* launches, double* ms_total, doub
 int qq_bench_hsingle(qq_ctx* ctx, int precision, int nrhs, int tps, int niter, int flush_l2,
                      double* ms_per_call, double* bytes_per_call);
 
+/* The kernel shape (the codes of qq_bench_hsingle) the autotuner chose for the
+ * EPI_STORE hopping launch of this precision and RHS count (block fields for nrhs > 1)
+ * in this context; QQ_BAD_ARG if no such launch has run yet. */
+int qq_hop_tuned_shape(qq_ctx* ctx, int precision, int nrhs, int* shape);
+
 /* The hopping term of qq_hsingle (Hsingle, Q/diracops.f90:554-599) on nrhs half-lattice fields
  * at once, computed in reduced precision the way the batched solver applies it: gin
  * holds nrhs reference-layout input vectors back to back (parity opposite to gblclr),

@@ -36,7 +36,8 @@ EXPORTED = [
     "qq_rnds", "qq_z2source", "qq_z4source", "qq_twaverage_level0", "qq_discon_traces", "qq_bench_hsingle",
     "qq_heatbath", "qq_ctx_stream", "qq_launch_count", "qq_profile_hop", "qq_profile_hop_read",
     "qq_gfwrite", "qq_gfread", "qq_fpwrite", "qq_fpread", "qq_hsingle_block",
-    "qq_hop_tuned_shape",
+    "qq_hop_tuned_shape", "qq_net_create", "qq_net_destroy", "qq_net_nweights", "qq_net_get_weights",
+    "qq_net_set_weights", "qq_net_apply", "qq_net_grad", "qq_net_train", "qq_fgmres",
 ]
 
 
@@ -55,7 +56,7 @@ class qq_solve_info(C.Structure):
     _fields_ = [("status", C.c_int), ("itercount", C.c_int), ("mvp", C.c_int), ("ncycles", C.c_int),
                 ("true_rel", C.c_double), ("seconds", C.c_double), ("nhist", C.c_int),
                 ("hist", C.c_double * 1024), ("hist_mvp", C.c_int * 1024), ("nritz", C.c_int),
-                ("ritz", C.c_double * 1024)]
+                ("ritz", C.c_double * 1024), ("fallback", C.c_int)]
 
 
 class qq_method(C.Structure):
@@ -75,6 +76,7 @@ class SolveInfo:
     hist: np.ndarray
     hist_mvp: np.ndarray
     ritz: np.ndarray
+    fallback: int = 0
 
     @classmethod
     def from_c(cls, s: qq_solve_info) -> "SolveInfo":
@@ -82,7 +84,7 @@ class SolveInfo:
         nr = s.nritz
         r = np.array(s.ritz[: 2 * nr]).reshape(nr, 2)
         return cls(s.status, s.itercount, s.mvp, s.ncycles, s.true_rel, s.seconds,
-                   np.array(s.hist[:n]), np.array(s.hist_mvp[:n]), r[:, 0] + 1j * r[:, 1])
+                   np.array(s.hist[:n]), np.array(s.hist_mvp[:n]), r[:, 0] + 1j * r[:, 1], s.fallback)
 
 
 _lib = None
@@ -134,6 +136,15 @@ def load_library() -> C.CDLL:
         "qq_bench_hsingle": ([P, I, I, I, I, I, DP, DP], I),
         "qq_hsingle_block": ([P, I, I, I, P, P, I, I], I),
         "qq_hop_tuned_shape": ([P, I, I, IP], I),
+        "qq_net_create": ([I, IP, C.c_ulonglong, D, C.POINTER(P)], I),
+        "qq_net_destroy": ([P], I),
+        "qq_net_nweights": ([P], I),
+        "qq_net_get_weights": ([P, DP], I),
+        "qq_net_set_weights": ([P, DP], I),
+        "qq_net_apply": ([P, P, P, P], I),
+        "qq_net_grad": ([P, P, I, P, P, DP, DP], I),
+        "qq_net_train": ([P, P, DP, I, I, D, C.c_ulonglong, DP], I),
+        "qq_fgmres": ([P, P, P, P, I, D, I, DP, C.POINTER(qq_solve_info)], I),
         "qq_heatbath": ([P, D, I, C.c_ulonglong, P, DP], I),
         "qq_ctx_stream": ([P, C.POINTER(P)], I),
         "qq_launch_count": ([], C.c_longlong),
@@ -335,6 +346,16 @@ class Lattice:
         _check(st, allow_not_converged=True)
         return x, SolveInfo.from_c(info)
 
+    def fgmres(self, phi, kappa, m=20, resmax=1e-10, max_cycles=200, net=None, x=None):
+        """Flexible GMRES(m) with the network `net` (a Net, or None) as right
+        preconditioner, falling back to plain GMRES-DR if it stalls: (x, SolveInfo)."""
+        x = np.zeros_like(phi) if x is None else x
+        info = qq_solve_info()
+        st = self.lib.qq_fgmres(self._ctx, net._h if net is not None else None, _ptr(phi), _ptr(x), int(m),
+                                float(resmax), int(max_cycles), _d2(kappa), C.byref(info))
+        _check(st, allow_not_converged=True)
+        return x, SolveInfo.from_c(info)
+
     def gmresproj(self, b, x, GMRES, resmax, itermin=0, kappa=(0.15, 0.0), iflag=-1, defl=None):
         info = qq_solve_info()
         st = self.lib.qq_gmresproj(self._ctx, _ptr(b), _ptr(x), _i2(GMRES), float(resmax), itermin,
@@ -428,6 +449,66 @@ class Lattice:
         _check(self.lib.qq_bench_hsingle(self._ctx, precision, nrhs, tps, niter, int(flush_l2),
                                          C.byref(ms), C.byref(by)))
         return ms.value, by.value
+
+
+class Net:
+    """The learned preconditioner's network (qq_net_*): linear gauge-covariant
+    parallel-transport convolution layers from 4 spin channels to 4, trained on the GPU
+    to approximate the inverse of Hdbletm."""
+
+    def __init__(self, channels=(4, 8, 8, 4), seed: int = 1, scale: float = 1.0):
+        self.lib = load_library()
+        self._h = C.c_void_p()
+        arr = (C.c_int * len(channels))(*channels)
+        _check(self.lib.qq_net_create(len(channels) - 1, arr, int(seed), float(scale), C.byref(self._h)))
+        self.channels = tuple(channels)
+
+    @property
+    def nweights(self) -> int:
+        return int(self.lib.qq_net_nweights(self._h))
+
+    def get_weights(self) -> np.ndarray:
+        w = np.zeros(2 * self.nweights)
+        _check(self.lib.qq_net_get_weights(self._h, w.ctypes.data_as(C.POINTER(C.c_double))))
+        return w[0::2] + 1j * w[1::2]
+
+    def set_weights(self, w) -> None:
+        a = np.zeros(2 * self.nweights)
+        a[0::2], a[1::2] = np.real(w), np.imag(w)
+        _check(self.lib.qq_net_set_weights(self._h, a.ctypes.data_as(C.POINTER(C.c_double))))
+
+    def apply(self, lat, gin):
+        out = lat.new_half()
+        _check(self.lib.qq_net_apply(lat._ctx, self._h, _ptr(gin), _ptr(out)))
+        return out
+
+    def loss_grad(self, lat, b, x):
+        """Loss and dl/d conj(W) over pairs b[i], x[i] (stacks of half vectors)."""
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        loss = C.c_double()
+        g = np.zeros(2 * self.nweights)
+        _check(self.lib.qq_net_grad(lat._ctx, self._h, b.shape[0], _ptr(b), _ptr(x), C.byref(loss),
+                                    g.ctypes.data_as(C.POINTER(C.c_double))))
+        return loss.value, g[0::2] + 1j * g[1::2]
+
+    def train(self, lat, kappa, nsamples=4, nsteps=100, lr=1e-3, seed=1):
+        """Adam steps on pairs (Hdbletm x, x) with Gaussian x; the loss before each step."""
+        losses = np.zeros(max(nsteps, 1))
+        _check(self.lib.qq_net_train(lat._ctx, self._h, _d2(kappa), int(nsamples), int(nsteps), float(lr),
+                                     int(seed), losses.ctypes.data_as(C.POINTER(C.c_double))))
+        return losses[:nsteps]
+
+    def close(self) -> None:
+        if self._h:
+            self.lib.qq_net_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def launch_count() -> int:

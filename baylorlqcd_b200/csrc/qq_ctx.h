@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <complex>
+#include <functional>
 #include <map>
 #include <memory>
 #include <string>
@@ -184,5 +185,8 @@ int defl_project(qq_ctx* c, const DeflSpace& d, Spinor b, Spinor x, Spinor r, co
                  double* rn);
 
 void fill_info(qq_solve_info* info, int status, const SolveStats& s, double seconds);
+// Flexible GMRES(m) with right preconditioner M(z, v): z = M v (qq_solvers.cu).
+int fgmres_fp64(qq_ctx* c, Spinor phi, Spinor x, int m, double resmax, int max_cycles, const double kappa[2],
+                const std::function<int(Spinor, Spinor)>& M, SolveStats* st, bool* stalled);
 
 }  // namespace qq

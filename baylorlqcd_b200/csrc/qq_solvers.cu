@@ -12,6 +12,7 @@
 // the least-squares solve and the harmonic-Ritz restart, which is where the reference
 // checks convergence with the true residual anyway.
 #include <cmath>
+#include <functional>
 #include <cstring>
 
 #include "qq_ctx.h"
@@ -49,10 +50,11 @@ struct Arnoldi {
   }
 };
 
-// One Arnoldi step: v_{j+1} = normalised (I - V V^H) A v_j, H(:, j) filled.
-int arnoldi_step(Arnoldi& A, int j, Spinor tmp_odd, const double kappa[2], double* nrm2_slot) {
+// One Arnoldi step: v_{j+1} = normalised (I - V V^H) A src, H(:, j) filled; src = v_j
+// for GMRES, the preconditioned z_j = M v_j for flexible GMRES.
+int arnoldi_step_from(Arnoldi& A, int j, Spinor src, Spinor tmp_odd, const double kappa[2], double* nrm2_slot) {
   qq_ctx* c = A.c;
-  QQ_TRY(op_dbletm(c, A.sp(j + 1), A.sp(j), tmp_odd, 0, kappa));
+  QQ_TRY(op_dbletm(c, A.sp(j + 1), src, tmp_odd, 0, kappa));
   double* part = c->partial.as<double>();
   const int nv = j + 1;
   int ng = 0;
@@ -70,6 +72,10 @@ int arnoldi_step(Arnoldi& A, int j, Spinor tmp_odd, const double kappa[2], doubl
   QQ_CK(launch_hcol_update(A.H.as<double>(), A.m + 1, j, hscr, nv, nrm2_slot, c->st));
   QQ_CK(launch_normalize(A.pb, A.nel, w, w, nrm2_slot, c->st));
   return QQ_OK;
+}
+
+int arnoldi_step(Arnoldi& A, int j, Spinor tmp_odd, const double kappa[2], double* nrm2_slot) {
+  return arnoldi_step_from(A, j, A.sp(j), tmp_odd, kappa, nrm2_slot);
 }
 
 // Re-orthogonalise vector `idx` of the basis against vectors [0, idx) and normalise.
@@ -138,6 +144,71 @@ int true_residual(qq_ctx* c, Spinor b, Spinor x, Spinor r, Spinor tmp_odd, const
 }
 
 }  // namespace
+
+// ---------------------------------------------------------------------------
+// Flexible GMRES(m) with a right preconditioner z = M(v) (Saad 1993): Arnoldi on
+// A z_j with z_j = M(v_j), A Z_m = V_{m+1} H_m, update x += Z_m y with y the
+// least-squares solution of H_m y = ||r|| e_1.  M may change between applications
+// (the network runs in FP32).  FP64 basis; the true residual is checked once per
+// cycle against ||phi - A x0||, as GMRES-DR.  *stalled is set when two consecutive
+// cycles each reduce the true residual by less than a factor 2.
+// ---------------------------------------------------------------------------
+int fgmres_fp64(qq_ctx* c, Spinor phi, Spinor x, int m, double resmax, int max_cycles, const double kappa[2],
+                const std::function<int(Spinor, Spinor)>& M, SolveStats* st, bool* stalled) {
+  if (m < 2 || m > 127) return set_error(QQ_BAD_ARG, "FGMRES(m) out of range");
+  *stalled = false;
+  Arnoldi A;
+  QQ_TRY(A.init(c, P64, m));
+  DevBuf Z;
+  QQ_CK(Z.alloc((size_t)m * A.nel * 16));
+  auto zsp = [&](int j) { return Spinor{static_cast<char*>(Z.p) + (size_t)j * A.nel * 16, nullptr, P64}; };
+  Tmp tmp(c, P64), r(c, P64);
+  double* nrm2 = c->scal.as<double>() + 8;
+  double normnum = 0.0;
+  QQ_TRY(true_residual(c, phi, x, r.sp(), tmp.sp(), kappa, &normnum));
+  st->mvp += 1;
+  if (!std::isfinite(normnum)) return set_error(QQ_NAN, "NaN in initial residual");
+  if (!(normnum > 0.0)) {
+    st->true_rel = 0.0;
+    return QQ_OK;
+  }
+  double rn = normnum, prev = 1.0;
+  int slow = 0;
+  for (int cyc = 1; cyc <= max_cycles; ++cyc) {
+    QQ_TRY(lin(c, A.sp(0), cimm(1.0 / rn), r.sp()));
+    std::vector<dense::cd> cvec(m + 1, 0.0);
+    cvec[0] = rn;
+    QQ_TRY(A.zeroH());
+    for (int j = 0; j < m; ++j) {
+      QQ_TRY(M(zsp(j), A.sp(j)));
+      QQ_TRY(arnoldi_step_from(A, j, zsp(j), tmp.sp(), kappa, nrm2));
+      st->itercount += 1;
+      st->mvp += 1;
+    }
+    dense::Mat Hb;
+    QQ_TRY(read_H(A, m, Hb));
+    std::vector<dense::cd> y, srv;
+    dense::hess_lsq(Hb, cvec, m, y, srv);
+    QQ_TRY(upload_cvec(c, y, A.y.as<double>()));
+    QQ_CK(launch_basis_accum(P64, BasisArgs{Z.p, A.nel, A.nel}, m, A.y.as<double>(), c->g.vh, x, c->st));
+    QQ_TRY(true_residual(c, phi, x, r.sp(), tmp.sp(), kappa, &rn));
+    st->mvp += 1;
+    const double rel = rn / normnum;
+    st->hist.push_back(rel);
+    st->hist_mvp.push_back(st->mvp);
+    st->true_rel = rel;
+    st->ncycles = cyc;
+    if (!std::isfinite(rel)) return set_error(QQ_NAN, "NaN residual in flexible GMRES");
+    if (rel < resmax) return QQ_OK;
+    slow = rel > 0.5 * prev ? slow + 1 : 0;
+    prev = rel;
+    if (slow >= 2) {
+      *stalled = true;
+      break;
+    }
+  }
+  return QQ_NOT_CONVERGED;
+}
 
 // ---------------------------------------------------------------------------
 // GMRES-DR(m, k), FP64, reference semantics: convergence is tested once per cycle with

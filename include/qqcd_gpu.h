@@ -57,6 +57,7 @@ typedef struct qq_solve_info {
   int hist_mvp[1024];
   int nritz;          /* harmonic Ritz values of the last restart (re, im) */
   double ritz[2 * 512];
+  int fallback;       /* qq_fgmres: 1 if plain GMRES-DR took over from a stalled cycle */
 } qq_solve_info;
 
 /* ---- context ---- */
@@ -266,6 +267,43 @@ int qq_profile_hop_read(qq_ctx* ctx, long long* launches, double* ms_total, doub
  * algorithmic bytes of one launch, V/2 * (8 * link bytes + nrhs * 2 * spinor bytes). */
 int qq_bench_hsingle(qq_ctx* ctx, int precision, int nrhs, int tps, int niter, int flush_l2,
                      double* ms_per_call, double* bytes_per_call);
+
+/* ---- learned preconditioner (no counterpart in the reference) ----
+ * A gauge-covariant network of linear parallel-transport convolution layers: a layer
+ * maps Cin channels to Cout channels (a channel is one colour vector per site of the
+ * full lattice) by out_co(x) = sum_p sum_ci W[p][co][ci] (T_p f_ci)(x) over the paths
+ * p = 0 (the site itself), 1 + 2 mu (U_mu(x) f(x + mu)) and 2 + 2 mu
+ * (U_mu(x - mu)^+ f(x - mu)), with the lattice's boundary factors on wrapping hops.
+ * The network maps an even-site (gblclr = 1) Dirac vector, channel = spin, to an
+ * even-site vector and is trained to approximate the inverse of Hdbletm; flexible
+ * GMRES uses it as a right preconditioner.  Weights are complex, stored
+ * [layer][p][co][ci] as (re, im) pairs. */
+typedef struct qq_net qq_net;
+/* channels[0..nlayers]: 4, then 4, 8 or 16 per hidden layer, then 4.  The network
+ * starts near scale * identity (kappa^2 approximates the inverse of Hdbletm's leading
+ * term) with small random weights on every other path (seeded). */
+int qq_net_create(int nlayers, const int* channels, unsigned long long seed, double scale, qq_net** out);
+int qq_net_destroy(qq_net* net);
+int qq_net_nweights(const qq_net* net); /* complex weights */
+int qq_net_get_weights(const qq_net* net, double* w);
+int qq_net_set_weights(qq_net* net, const double* w);
+/* out = N(in); reference-layout gblclr = 1 half vectors, host or device. */
+int qq_net_apply(qq_ctx* ctx, qq_net* net, const double* in, double* out);
+/* Loss l = (1/S) sum_i |N(b_i) - x_i|^2 / |x_i|^2 over nsamples pairs (half vectors
+ * back to back) and its gradient dl/d conj(W), same layout as the weights. */
+int qq_net_grad(qq_ctx* ctx, qq_net* net, int nsamples, const double* b, const double* x, double* loss,
+                double* grad);
+/* nsteps Adam steps (learning rate lr) on nsamples pairs (Hdbletm x, x) with Gaussian
+ * x drawn from `seed`; losses[step] (may be NULL) receives the loss before each step. */
+int qq_net_train(qq_ctx* ctx, qq_net* net, const double kappa[2], int nsamples, int nsteps, double lr,
+                 unsigned long long seed, double* losses);
+/* Flexible GMRES(m) on Hdbletm x = phi with the network as right preconditioner (net
+ * NULL: none), FP64; converged when ||phi - A x|| / ||phi - A x0|| < resmax, checked
+ * once per cycle.  If two consecutive cycles each gain less than a factor 2, plain
+ * GMRES-DR(m, m/3) continues from the current x (info->fallback = 1).  x: initial
+ * guess in, solution out. */
+int qq_fgmres(qq_ctx* ctx, qq_net* net, const double* phi, double* x, int m, double resmax, int max_cycles,
+              const double kappa[2], qq_solve_info* info);
 
 /* The kernel shape (the codes of qq_bench_hsingle) the autotuner chose for the
  * EPI_STORE hopping launch of this precision and RHS count (block fields for nrhs > 1)

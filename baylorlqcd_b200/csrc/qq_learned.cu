@@ -382,7 +382,8 @@ struct qq_net {
   std::vector<std::complex<double>> w;  // [layer][9][co][ci], FP64 master copy
   std::vector<size_t> off;              // first weight of each layer
   DevBuf wf, wa;                        // FP32 weights and adjoint weights on the device
-  int wdev = -1;                        // device of wf / wa
+  DevBuf acts[kNetMaxLayers + 1];       // activations (acts[0]: the embedded input), kept
+  int wdev = -1;                        // device of wf / wa / acts
   bool dirty = true;
   std::vector<double> am, av;           // Adam moments (real, imaginary interleaved)
   int at = 0;
@@ -409,6 +410,13 @@ size_t net_field_bytes(qq_ctx* c, int channels) { return (size_t)channels * 3 * 
 // FP32 weights and adjoint weights of every layer on the context's device.
 int net_upload(qq_ctx* c, qq_net* net) {
   if (!net->dirty && net->wdev == c->device) return QQ_OK;
+  if (net->wdev != c->device)  // buffers of another device: release them
+    for (DevBuf& b : net->acts)
+      if (b.p) {
+        cudaFree(b.p);
+        b.p = nullptr;
+        b.bytes = 0;
+      }
   std::vector<float2> wf(net->nw()), wa(net->nw());
   for (int l = 0; l < net->nl; ++l) {
     const int ci = net->ch[l], co = net->ch[l + 1];
@@ -435,7 +443,7 @@ int net_upload(qq_ctx* c, qq_net* net) {
 }
 
 // acts[l + 1] = layer l applied to (l == 0 ? input : acts[l]); acts[0] is not used.
-int net_forward(qq_ctx* c, qq_net* net, const float2* input, std::vector<DevBuf>& acts) {
+int net_forward(qq_ctx* c, qq_net* net, const float2* input, DevBuf* acts) {
   const NetGeom g = net_geom(c);
   for (int l = 0; l < net->nl; ++l) {
     QQ_CK(acts[l + 1].alloc(net_field_bytes(c, net->ch[l + 1])));
@@ -447,11 +455,13 @@ int net_forward(qq_ctx* c, qq_net* net, const float2* input, std::vector<DevBuf>
 
 }  // namespace
 
-// z = N(v) for even-site FP64 fields (the preconditioner of flexible GMRES).
+// z = N(v) for even-site FP64 fields (the preconditioner of flexible GMRES).  The
+// activation buffers live in the network handle, so repeated applications allocate
+// nothing.
 int net_apply_field(qq_ctx* c, qq_net* net, Spinor out, Spinor in) {
   QQ_TRY(net_upload(c, net));
   const NetGeom g = net_geom(c);
-  std::vector<DevBuf> acts(net->nl + 1);
+  DevBuf* acts = net->acts;
   QQ_CK(acts[0].alloc(net_field_bytes(c, 4)));
   QQ_CK(cudaMemsetAsync(acts[0].p, 0, acts[0].bytes, c->st));
   const int nblk = (c->g.vh + 127) / 128;
@@ -484,7 +494,7 @@ int net_loss_grad(qq_ctx* c, qq_net* net, const std::vector<DevBuf>& B, const st
   QQ_CK(grad.alloc(sizeof(double2) * net->nw()));
   QQ_CK(cudaMemsetAsync(grad.p, 0, grad.bytes, c->st));
   std::vector<double> lp(nblk);
-  std::vector<DevBuf> acts(net->nl + 1);
+  DevBuf* acts = net->acts;
   double total = 0.0;
   for (int i = 0; i < S; ++i) {
     QQ_TRY(net_forward(c, net, B[i].as<float2>(), acts));

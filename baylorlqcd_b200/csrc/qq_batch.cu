@@ -77,6 +77,26 @@ int block_op(qq_ctx* c, int prec, const BlockBiArgs& A, int op, const int* dslot
   return QQ_OK;
 }
 
+// The scalar step alone, on partials already written (by a hop with a fused dot product).
+int scalar_step(qq_ctx* c, const BlockBiArgs& A, const int* dslots, int step, int nblocks, const ScalarCtl& sc) {
+  count_launch();
+  bicg_scalar_kernel<<<A.nb, 256, 0, c->st>>>(A.S, dslots, A.partial, nblocks, step, sc.ctl, sc.delta,
+                                              sc.half_tol);
+  QQ_CK(cudaGetLastError());
+  return QQ_OK;
+}
+
+// v = A p with <rhat, v> (step ST_ALPHA), or t = A s with <t, s>, ||t||^2 (ST_OMEGA):
+// fused into the second hop when its kernel supports it, else a separate reduction.
+int op_and_dot(qq_ctx* c, int prec, const BlockBiArgs& A, Spinor out, Spinor in, Spinor tmp, Spinor dot_op,
+               int mode, const double kappa[2], const int* dslots, const ScalarCtl& sc) {
+  int fb = 0;
+  QQ_TRY(op_dbletm_block_dot(c, out, in, tmp, A.nb, kappa, dot_op, A.partial, mode, &fb));
+  const int step = mode == 1 ? ST_ALPHA : ST_OMEGA;
+  if (fb) return scalar_step(c, A, dslots, step, fb, sc);
+  return block_op(c, prec, A, mode == 1 ? OP_DOT_RHAT_V : OP_DOTS_T, dslots, step, sc);
+}
+
 // mode 0: block[k] = x ; 1: x += block[k] ; 2: block[k] = 0.  With `pred`, only when
 // bit k of the device word *pred is set.
 int block_slot(qq_ctx* c, int prec, int nb, int k, Spinor blockf, Spinor x, int mode,
@@ -230,7 +250,7 @@ int bicgstab_block_sync(qq_ctx* c, std::vector<PerRhs*>& rhs, int prec, double t
   constexpr size_t kSyncDoubles = kScalDoubles + (kCtlWords + 1) / 2;
   DevBuf S, part, dslots;
   QQ_CK(S.alloc(sizeof(double) * (kSyncDoubles)));
-  QQ_CK(part.alloc(sizeof(double) * 3 * kRedBlocks * kMaxBatch));
+  QQ_CK(part.alloc(sizeof(double) * 3 * std::max(kRedBlocks, hop_block_count(c, nb)) * kMaxBatch));
   QQ_CK(dslots.alloc(sizeof(int) * kMaxBatch));
   unsigned* ctl = reinterpret_cast<unsigned*>(S.as<double>() + kScalDoubles);
   Tmp tmp64(c, P64), h(c, P64);
@@ -305,11 +325,9 @@ int bicgstab_block_sync(qq_ctx* c, std::vector<PerRhs*>& rhs, int prec, double t
     for (int i = 0; i < nchunk; ++i) {
       QQ_TRY(block_op(c, prec, A, OP_DOT_RHAT_R, ds, ST_BETA, sc));
       QQ_TRY(block_op(c, prec, A, OP_P_UPDATE, ds, -1, sc));
-      QQ_TRY(op_dbletm_block(c, v.sp(), p.sp(), tmp.sp(), nb, 0, kappa));
-      QQ_TRY(block_op(c, prec, A, OP_DOT_RHAT_V, ds, ST_ALPHA, sc));
+      QQ_TRY(op_and_dot(c, prec, A, v.sp(), p.sp(), tmp.sp(), rhat.sp(), 1, kappa, ds, sc));
       QQ_TRY(block_op(c, prec, A, OP_S_UPDATE, ds, -1, sc));
-      QQ_TRY(op_dbletm_block(c, t.sp(), r.sp(), tmp.sp(), nb, 0, kappa));
-      QQ_TRY(block_op(c, prec, A, OP_DOTS_T, ds, ST_OMEGA, sc));
+      QQ_TRY(op_and_dot(c, prec, A, t.sp(), r.sp(), tmp.sp(), r.sp(), 2, kappa, ds, sc));
       QQ_TRY(block_op(c, prec, A, OP_XR_UPDATE, ds, ST_R2, sc));
     }
     done_its += nchunk;
@@ -393,7 +411,7 @@ int bicgstab_block(qq_ctx* c, std::vector<PerRhs*>& rhs, int prec, double tol, d
   QQ_CK(S.alloc(sbytes));
   QQ_CK(dhist.alloc(sizeof(double) * kHist * nb));
   QQ_CK(dhits.alloc(sizeof(int) * kHist * nb));
-  QQ_CK(part.alloc(sizeof(double) * 3 * kRedBlocks * kMaxBatch));
+  QQ_CK(part.alloc(sizeof(double) * 3 * std::max(kRedBlocks, hop_block_count(c, nb)) * kMaxBatch));
   QQ_CK(dslots.alloc(sizeof(int) * kMaxBatch));
   double* Sd = S.as<double>();
   unsigned* ctl = reinterpret_cast<unsigned*>(Sd + kScalDoubles);
@@ -459,11 +477,9 @@ int bicgstab_block(qq_ctx* c, std::vector<PerRhs*>& rhs, int prec, double tol, d
     for (int i = 0; i < kChunk; ++i) {
       QQ_TRY(block_op(c, prec, A, OP_DOT_RHAT_R, ds, ST_BETA, sctl));
       QQ_TRY(block_op(c, prec, A, OP_P_UPDATE, ds, -1, sctl));
-      QQ_TRY(op_dbletm_block(c, v.sp(), p.sp(), tmp.sp(), nb, 0, kappa));
-      QQ_TRY(block_op(c, prec, A, OP_DOT_RHAT_V, ds, ST_ALPHA, sctl));
+      QQ_TRY(op_and_dot(c, prec, A, v.sp(), p.sp(), tmp.sp(), rhat.sp(), 1, kappa, ds, sctl));
       QQ_TRY(block_op(c, prec, A, OP_S_UPDATE, ds, -1, sctl));
-      QQ_TRY(op_dbletm_block(c, t.sp(), r.sp(), tmp.sp(), nb, 0, kappa));
-      QQ_TRY(block_op(c, prec, A, OP_DOTS_T, ds, ST_OMEGA, sctl));
+      QQ_TRY(op_and_dot(c, prec, A, t.sp(), r.sp(), tmp.sp(), r.sp(), 2, kappa, ds, sctl));
       QQ_TRY(block_op(c, prec, A, OP_XR_UPDATE, ds, ST_R2, sctl));
     }
     return QQ_OK;

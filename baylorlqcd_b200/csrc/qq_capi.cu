@@ -473,10 +473,14 @@ extern "C" int qq_hop_tuned_shape(qq_ctx* c, int precision, int nrhs, int* shape
   std::memset(&a, 0, sizeof(a));
   a.nrhs = nrhs;
   a.blk = nrhs > 1 ? 1 : 0;
-  auto it = c->hop_tune.find(hop_tune_key(c, a, prec, EPI_STORE));
-  if (it == c->hop_tune.end()) return set_error(QQ_BAD_ARG, "no hopping launch of that kind has been tuned yet");
-  *shape = it->second;
-  return QQ_OK;
+  for (int epi : {EPI_STORE, EPI_TWIST, EPI_DBLE}) {  // the first hop of Hdbletm, Wilson or twisted
+    auto it = c->hop_tune.find(hop_tune_key(c, a, prec, epi));
+    if (it != c->hop_tune.end()) {
+      *shape = it->second;
+      return QQ_OK;
+    }
+  }
+  return set_error(QQ_BAD_ARG, "no hopping launch of that kind has been tuned yet");
 }
 
 extern "C" int qq_bench_hsingle(qq_ctx* c, int precision, int nrhs, int tps, int niter,

@@ -142,6 +142,11 @@ int op_dbletm_multi(qq_ctx* c, const Spinor* out, const Spinor* in, const Spinor
                     int idag, const double kappa[2]);
 // RHS-interleaved block fields of nb right-hand sides (element (q, s, r) at
 // q * (vh * nb) + s * nb + r); one launch pair for the whole block.
+int op_dbletm_block_impl(qq_ctx* c, Spinor out, Spinor in, Spinor tmp, int nb, int idag, const double kappa[2],
+                         Spinor dot_op, double* dot_part, int dot_mode, int* fused_blocks);
+int op_dbletm_block_dot(qq_ctx* c, Spinor out, Spinor in, Spinor tmp, int nb, const double kappa[2],
+                        Spinor dot_op, double* dot_part, int dot_mode, int* fused_blocks);
+int hop_block_count(qq_ctx* c, int nb);
 int op_dbletm_block(qq_ctx* c, Spinor out, Spinor in, Spinor tmp, int nb, int idag,
                     const double kappa[2]);
 int lin(qq_ctx* c, Spinor out, Coef a, Spinor x, Coef b = cimm(0), Spinor y = Spinor{nullptr, nullptr, P64},

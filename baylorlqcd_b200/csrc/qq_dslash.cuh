@@ -52,6 +52,13 @@ struct HopArgs {
   double a;                    // EPI_TWIST: 2 kappa mu
   double f1, f2, f3;           // EPI_DBLE factors
   float af, f1f, f2f, f3f;     // float copies (set by the launcher)
+  // Optional dot products of the output with a block field of the same layout, fused
+  // into the copy-ring kernel's epilogue (hop_f2a_kernel only): dot_mode 1 gives
+  // sum conj(dot_op) out, 2 gives sum conj(out) dot_op and sum |out|^2, as per-block
+  // partials dot_part[(rhs * gridDim.x + block) * 3 + q].
+  const void* dot_op;
+  double* dot_part;
+  int dot_mode;
 };
 
 template <class R>

@@ -179,9 +179,10 @@ __device__ inline void hop2(const HopArgs& a, int s, int r0, int G, const int* x
   }
 }
 
-// Epilogue and store; g is the EPI_DBLE operand at (s, r), read by the caller.
+// Epilogue and store; g is the EPI_DBLE operand at (s, r), read by the caller.  Returns
+// what was stored.
 template <int EPI>
-__device__ inline void finish2_g(const HopArgs& a, int s, int r, const Pair12& acc, const Pair12& g) {
+__device__ inline Pair12 finish2_g(const HopArgs& a, int s, int r, const Pair12& acc, const Pair12& g) {
   Pair12 o;
   if (EPI == EPI_STORE) {
     o = acc;
@@ -205,6 +206,7 @@ __device__ inline void finish2_g(const HopArgs& a, int s, int r, const Pair12& a
     }
   }
   store_pairs(static_cast<float4*>(a.blk ? a.out[0] : a.out[r]), a.vh_of(), a.idx_of(s, r), o);
+  return o;
 }
 
 template <int EPI>
@@ -456,19 +458,20 @@ struct F2aShared {
   float4* ring;   // [stage][rhs][6][thread]
 };
 
-// Stage H (hops 0-7, 8 = the EPI_DBLE operand) into ring slot H % D; always one group.
-// Thread j of a site holds right-hand sides j, j + G, ..., j + (RPT - 1) G.
+// Stage H (hops 0-7, 8 = the EPI_DBLE operand, 9 = the fused dot product's operand)
+// into ring slot H % D; always one group.  Thread j of a site holds right-hand sides
+// j, j + G, ..., j + (RPT - 1) G.
 template <int H, int D, int EPI, int RPT>
 __device__ inline void f2a_issue(const HopArgs& a, const F2aShared& sh, int s, int sl, int j, int G, int T,
                                  int tx, bool act) {
-  if constexpr (H < 8 || (H == 8 && EPI == EPI_DBLE)) {
-    if (act) {
+  if constexpr (H < 8 || (H >= 8 && H <= 9 && EPI == EPI_DBLE)) {
+    if (act && (H != 9 || a.dot_mode)) {
       const int site = H < 8 ? sh.nbr[sl * 8 + H] : s;
       const int n = a.vh_of();
 #pragma unroll
       for (int k = 0; k < RPT; ++k) {
         const int r = j + k * G;
-        const void* base = H < 8 ? a.in_base(r) : (a.blk ? a.aux[0] : a.aux[r]);
+        const void* base = H < 8 ? a.in_base(r) : H == 8 ? (a.blk ? a.aux[0] : a.aux[r]) : a.dot_op;
         const float4* f = static_cast<const float4*>(base) + a.idx_of(site, r);
         float4* dst = sh.ring + ((H % D) * RPT + k) * 6 * T + tx;
 #pragma unroll
@@ -612,27 +615,70 @@ __global__ void __launch_bounds__(128) hop_f2a_kernel(HopArgs a) {
     for (int e = 0; e < 5; ++e) dst[e] = make_float4(v[4 * e], v[4 * e + 1], v[4 * e + 2], v[4 * e + 3]);
   }
   __syncthreads();
-  if (!act) return;
-  Pair12 acc[RPT];
+  double dsum[3] = {0.0, 0.0, 0.0};  // this thread's share of the fused dot products
+  if (act) {
+    Pair12 acc[RPT];
 #pragma unroll
-  for (int k = 0; k < RPT; ++k)
+    for (int k = 0; k < RPT; ++k)
 #pragma unroll
-    for (int q = 0; q < 6; ++q) acc[k].re[q] = acc[k].im[q] = make_float2(0.0f, 0.0f);
-  f2a_run<0, D, EPI, RPT>(a, sh, s, sl, j, G, T, tx, acc);
-  if constexpr (EPI == EPI_DBLE) cp_async_wait<D - 1>();  // stage 8
+      for (int q = 0; q < 6; ++q) acc[k].re[q] = acc[k].im[q] = make_float2(0.0f, 0.0f);
+    f2a_run<0, D, EPI, RPT>(a, sh, s, sl, j, G, T, tx, acc);
+    if constexpr (EPI == EPI_DBLE) cp_async_wait<D - 2>();  // stages 8 and 9 (D >= 2)
 #pragma unroll
-  for (int k = 0; k < RPT; ++k) {
-    Pair12 g;
-    if constexpr (EPI == EPI_DBLE) {
-      const float4* src = sh.ring + ((8 % D) * RPT + k) * 6 * T + tx;
+    for (int k = 0; k < RPT; ++k) {
+      Pair12 g;
+      if constexpr (EPI == EPI_DBLE) {
+        const float4* src = sh.ring + ((8 % D) * RPT + k) * 6 * T + tx;
 #pragma unroll
-      for (int q = 0; q < 6; ++q) {
-        const float4 t = src[q * T];
-        g.re[q] = make_float2(t.x, t.y);
-        g.im[q] = make_float2(t.z, t.w);
+        for (int q = 0; q < 6; ++q) {
+          const float4 t = src[q * T];
+          g.re[q] = make_float2(t.x, t.y);
+          g.im[q] = make_float2(t.z, t.w);
+        }
+      }
+      const Pair12 o = finish2_g<EPI>(a, s, j + k * G, acc[k], g);
+      if (a.dot_mode) {
+        Pair12 w;
+        const float4* wsrc = sh.ring + ((9 % D) * RPT + k) * 6 * T + tx;
+#pragma unroll
+        for (int q = 0; q < 6; ++q) {
+          const float4 t = wsrc[q * T];
+          w.re[q] = make_float2(t.x, t.y);
+          w.im[q] = make_float2(t.z, t.w);
+        }
+        // conj(w) o (mode 1), else conj(o) w and |o|^2: the thread's 12 products are
+        // summed in packed FP32, the block and grid sums in FP64
+        const float sg = a.dot_mode == 1 ? 1.0f : -1.0f;  // im part flips with the order
+        float2 dre = make_float2(0.f, 0.f), dim = make_float2(0.f, 0.f), dnn = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int q = 0; q < 6; ++q) {
+          dre = f2fma(w.re[q], o.re[q], f2fma(w.im[q], o.im[q], dre));
+          dim = f2fma(w.re[q], o.im[q], f2fma(f2bc(-1.0f), f2mul(w.im[q], o.re[q]), dim));
+          dnn = f2fma(o.re[q], o.re[q], f2fma(o.im[q], o.im[q], dnn));
+        }
+        dsum[0] += (double)dre.x + (double)dre.y;
+        dsum[1] += sg * ((double)dim.x + (double)dim.y);
+        dsum[2] += (double)dnn.x + (double)dnn.y;
       }
     }
-    finish2_g<EPI>(a, s, j + k * G, acc[k], g);
+  }
+  if (a.dot_mode) {  // per right-hand side over the block's sites, fixed order
+    __shared__ double dred[3][128];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) dred[q][tx] = dsum[q];
+    __syncthreads();
+    if (RPT == 1 && tx < a.nrhs) {
+      double t0 = 0.0, t1 = 0.0, t2 = 0.0;
+      for (int site = 0; site < per; ++site) {
+        t0 += dred[0][site * G + tx];
+        t1 += dred[1][site * G + tx];
+        t2 += dred[2][site * G + tx];
+      }
+      double* dst = a.dot_part + ((size_t)tx * gridDim.x + blockIdx.x) * 3;
+      dst[0] = t0;
+      dst[1] = t1;
+      dst[2] = t2;
+    }
   }
 }
 

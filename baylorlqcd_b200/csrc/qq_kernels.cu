@@ -152,12 +152,17 @@ static cudaError_t hop_f2s(const HopArgs& a, int epi, cudaStream_t st) {
 template <int EPI, int D, int RPT>
 static cudaError_t hop_f2a_epi(const HopArgs& b, size_t smem, cudaStream_t st) {
   static bool attr_set = false;  // one attribute call per instantiation
+  static size_t max_dyn = 0;     // 227 KiB less the kernel's static shared memory
   if (!attr_set) {
-    const cudaError_t e = cudaFuncSetAttribute(hop_f2a_kernel<EPI, D, RPT>,
-                                               cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    cudaFuncAttributes fa;
+    cudaError_t e = cudaFuncGetAttributes(&fa, hop_f2a_kernel<EPI, D, RPT>);
+    if (e != cudaSuccess) return e;
+    max_dyn = (size_t)227 * 1024 - fa.sharedSizeBytes;
+    e = cudaFuncSetAttribute(hop_f2a_kernel<EPI, D, RPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_dyn);
     if (e != cudaSuccess) return e;
     attr_set = true;
   }
+  if (smem > max_dyn) return cudaErrorInvalidValue;
   const int G = b.nrhs / RPT;
   const dim3 blk(b.per_block * G), grd((b.g.vh + b.per_block - 1) / b.per_block);
   hop_f2a_kernel<EPI, D, RPT><<<grd, blk, smem, st>>>(b);

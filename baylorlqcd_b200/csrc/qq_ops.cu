@@ -265,9 +265,32 @@ int op_dbletm_multi(qq_ctx* c, const Spinor* out, const Spinor* in, const Spinor
   return QQ_OK;
 }
 
+// Thread blocks of the copy-ring hop kernel for block fields of nb right-hand sides
+// (the partials a fused dot product writes per right-hand side).
+int hop_block_count(qq_ctx* c, int nb) {
+  const int per = hop_sites_per_block(1, nb);
+  return (c->g.vh + per - 1) / per;
+}
+
+// Hdbletm on block fields with, when the autotuned second launch is the FP32 copy-ring
+// kernel, a dot product of the output fused into its epilogue (HopArgs::dot_mode):
+// *fused_blocks = the number of per-block partials written to dot_part, 0 when the
+// caller must compute the dot product itself.
+int op_dbletm_block_dot(qq_ctx* c, Spinor out, Spinor in, Spinor tmp, int nb, const double kappa[2],
+                        Spinor dot_op, double* dot_part, int dot_mode, int* fused_blocks) {
+  *fused_blocks = 0;
+  return op_dbletm_block_impl(c, out, in, tmp, nb, 0, kappa, dot_op, dot_part, dot_mode, fused_blocks);
+}
+
 // Hdbletm on RHS-interleaved block fields of nb right-hand sides (one launch pair).
 int op_dbletm_block(qq_ctx* c, Spinor out, Spinor in, Spinor tmp, int nb, int idag,
                     const double kappa[2]) {
+  return op_dbletm_block_impl(c, out, in, tmp, nb, idag, kappa, Spinor{nullptr, nullptr, in.prec}, nullptr, 0,
+                              nullptr);
+}
+
+int op_dbletm_block_impl(qq_ctx* c, Spinor out, Spinor in, Spinor tmp, int nb, int idag, const double kappa[2],
+                         Spinor dot_op, double* dot_part, int dot_mode, int* fused_blocks) {
   if (!c->have_gauge) return set_error(QQ_BAD_ARG, "no gauge field uploaded");
   if (nb < 1 || nb > 32) return set_error(QQ_BAD_ARG, "block of 1..32 right-hand sides");
   const int prec = in.prec;
@@ -298,6 +321,19 @@ int op_dbletm_block(qq_ctx* c, Spinor out, Spinor in, Spinor tmp, int nb, int id
     const double t = 2.0 * kappa[0] * kappa[1];
     b.f2 = 2.0 * kappa[1] / kappa[0];
     b.f3 = 1.0 / (1.0 + t * t);
+  }
+  if (dot_mode && prec == P32 && fused_blocks) {
+    // the fusion depends on the tuned shape: tune first (that launch's output is
+    // recomputed below), so the first call of a solve is fused like every later one
+    const int key = hop_tune_key(c, b, prec, EPI_DBLE);
+    if (c->hop_tune.find(key) == c->hop_tune.end()) QQ_TRY(launch_hop_tuned(c, b, prec, EPI_DBLE));
+    auto it = c->hop_tune.find(key);
+    if (it != c->hop_tune.end() && it->second >= kShapeF2 + 6 && it->second <= kShapeF2 + 8) {
+      b.dot_op = dot_op.data;
+      b.dot_part = dot_part;
+      b.dot_mode = dot_mode;
+      *fused_blocks = hop_block_count(c, nb);
+    }
   }
   return launch_hop_tuned(c, b, prec, EPI_DBLE);
 }

@@ -305,9 +305,10 @@ int qq_net_train(qq_ctx* ctx, qq_net* net, const double kappa[2], int nsamples, 
 int qq_fgmres(qq_ctx* ctx, qq_net* net, const double* phi, double* x, int m, double resmax, int max_cycles,
               const double kappa[2], qq_solve_info* info);
 
-/* The kernel shape (the codes of qq_bench_hsingle) the autotuner chose for the
- * EPI_STORE hopping launch of this precision and RHS count (block fields for nrhs > 1)
- * in this context; QQ_BAD_ARG if no such launch has run yet. */
+/* The kernel shape (the codes of qq_bench_hsingle) the autotuner chose for the first
+ * hopping launch of Hdbletm (Wilson, else twisted mass, else the second launch) at this
+ * precision and RHS count (block fields for nrhs > 1) in this context; QQ_BAD_ARG if
+ * no such launch has run yet. */
 int qq_hop_tuned_shape(qq_ctx* ctx, int precision, int nrhs, int* shape);
 
 /* The hopping term of qq_hsingle (Hsingle, Q/diracops.f90:554-599) on nrhs half-lattice fields

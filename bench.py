@@ -50,6 +50,7 @@ def parse(argv=None):
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--dims", default="16,16,16,32")
     p.add_argument("--kappa", type=float, default=0.1565)
+    p.add_argument("--mu", type=float, default=0.0, help="twisted mass (0: Wilson)")
     p.add_argument("--nrhs", type=int, default=12)
     p.add_argument("--precision", type=int, default=32, choices=[16, 32, 64])
     p.add_argument("--rhs-block", type=int, default=12)
@@ -99,6 +100,16 @@ def peaks():
         d = json.loads(f.read_text())
         return float(d["hbm_gbs"]), "measured"
     return FALLBACK_HBM, "fallback"
+
+
+def dims_label(dims) -> str:
+    """16^3x32 style lattice label."""
+    nx, ny, nz, nt = dims
+    return "%d^3x%d" % (nx, nt) if nx == ny == nz else "%dx%dx%dx%d" % tuple(dims)
+
+
+def operator_label(mu: float) -> str:
+    return "twisted mass mu=%g" % mu if mu else "Wilson"
 
 
 def shape_name(shape: int) -> str:
@@ -176,7 +187,7 @@ def point_sources(lat, nrhs):
 # CPU leg: the reference algorithm (its C++ restatement) on the host cores.
 def _cpu_sample(args):
     """One process: GMRES-DR(m,k) on one point source, capped at `cycles` cycles."""
-    u, dims, kappa, m, k, src_idx, cycles = args
+    u, dims, kappa, mu, m, k, src_idx, cycles = args
     import oracle
 
     ol = oracle.OracleLattice(*dims, bc=(1, 1, 1, -1))
@@ -185,16 +196,16 @@ def _cpu_sample(args):
     be, bo = ol.pointsource((1, 1, 1, 1), ic, idd)
     oracle.set_kcyclim(cycles)
     t = time.perf_counter()
-    _, _, st, log = ol.fermprop(be, bo, (kappa, 0.0), inverter=5, resmax=1e-30, nGMRES=(m, k))
+    _, _, st, log = ol.fermprop(be, bo, (kappa, mu), inverter=5, resmax=1e-30, nGMRES=(m, k))
     dt = time.perf_counter() - t
     hist, _ = log.history()
     return dt, log.itercount, list(hist)
 
 
-def cpu_parallel(u, dims, kappa, m, k, nproc, cycles):
+def cpu_parallel(u, dims, kappa, mu, m, k, nproc, cycles):
     ctx = mp.get_context("spawn")
     with ctx.Pool(nproc) as pool:
-        return pool.map(_cpu_sample, [(u, dims, kappa, m, k, i, cycles) for i in range(nproc)])
+        return pool.map(_cpu_sample, [(u, dims, kappa, mu, m, k, i, cycles) for i in range(nproc)])
 
 
 # ---------------------------------------------------------------------------
@@ -208,7 +219,7 @@ def run_ours(a, rank, world, local):
     lat = qq.Lattice(*dims, bc=(1, 1, 1, -1), device=local)
     u, plaq = lat.heatbath(6.0, a.sweeps, seed=13 + rank)
     be, bo = point_sources(lat, a.nrhs)
-    kappa = (a.kappa, 0.0)
+    kappa = (a.kappa, a.mu)
     stream = torch.cuda.ExternalStream(lat.stream_handle())
     flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
     be_d, bo_d = torch.from_numpy(be).cuda(), torch.from_numpy(bo).cuda()
@@ -289,11 +300,11 @@ def run_ours(a, rank, world, local):
         "vs_baseline": None,
         "dtype": {16: "fp16/fp64", 32: "fp32/fp64", 64: "fp64"}[a.precision],
         "data": "synthetic: GPU heatbath configuration (beta=6.0, cold start, %d sweeps), point sources" % a.sweeps,
-        "config": {"workload": "16^3x32 Wilson kappa=%.4f, %d point sources, batched FP%d BiCGStab with FP64 "
+        "config": {"workload": "%s %s kappa=%.4f, %d point sources, batched FP%d BiCGStab with FP64 "
                                "reliable updates%s, tol %.0e full-lattice FP64; plain = FP64 GMRES-DR(%d,%d)"
-                               % (a.kappa, a.nrhs, a.precision, " + GMRES-DR deflation" if a.deflate else "",
-                                  a.tol, a.m, a.k),
-                   "lattice": list(dims), "kappa": a.kappa, "nrhs": a.nrhs, "precision": a.precision,
+                               % (dims_label(dims), operator_label(a.mu), a.kappa, a.nrhs, a.precision,
+                                  " + GMRES-DR deflation" if a.deflate else "", a.tol, a.m, a.k),
+                   "lattice": list(dims), "kappa": a.kappa, "mu": a.mu, "nrhs": a.nrhs, "precision": a.precision,
                    "rhs_block": a.rhs_block, "parallelism": "replicas x%d" % world,
                    "l2": "512 MiB buffer written before every step; working set > L2",
                    "plaquette": plaq},
@@ -316,7 +327,7 @@ def run_ours(a, rank, world, local):
 
     # CPU baseline: the reference algorithm's restatement, one core, bounded sample
     if rank == 0 and world == 1 and not a.no_cpu:
-        dt, its, _ = _cpu_sample((u, dims, a.kappa, a.m, a.k, 0, 1))
+        dt, its, _ = _cpu_sample((u, dims, a.kappa, a.mu, a.m, a.k, 0, 1))
         per_it = dt / max(its, 1)
         out["cpu_baseline"] = {"value": per_it * plain_iters, "unit": "s/RHS", "cores": 1, "kind": "port",
                                "sample": "one GMRES-DR(%d,%d) cycle (%d iterations, %.1f s) of the C++ restatement "
@@ -339,10 +350,10 @@ def run_reference(a, rank, world, local):
     nproc = max(1, min(os.cpu_count() or 1, a.nrhs))
     # warm-up: a one-iteration sample per process (imports, page-in)
     for _ in range(a.warmup):
-        cpu_parallel(u, dims, a.kappa, 2, 1, nproc, 1)
+        cpu_parallel(u, dims, a.kappa, a.mu, 2, 1, nproc, 1)
     per_step, details = [], None
     for _ in range(a.steps):
-        res = cpu_parallel(u, dims, a.kappa, a.m, a.k, nproc, 2)
+        res = cpu_parallel(u, dims, a.kappa, a.mu, a.m, a.k, nproc, 2)
         per_it = statistics.mean(dt / max(its, 1) for dt, its, _ in res)
         rates = [h[1] / h[0] for _, _, h in res if len(h) >= 2 and h[0] > 0]
         rate = min(max(statistics.median(rates), 1e-3), 0.999) if rates else 0.5
@@ -356,8 +367,9 @@ def run_reference(a, rank, world, local):
         "metric": METRIC, "impl": "reference", "value": value, "unit": "s/RHS", "n_gpus": world,
         "steps": a.steps, "warmup": a.warmup, "ms_per_step": value * nproc * 1e3, "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "fp64", "data": "same configuration and sources",
-        "config": {"workload": "16^3x32 Wilson kappa=%.4f point sources, GMRES-DR(%d,%d), tol %.0e"
-                               % (a.kappa, a.m, a.k, a.tol), "lattice": list(dims), "plaquette": plaq},
+        "config": {"workload": "%s %s kappa=%.4f point sources, GMRES-DR(%d,%d), tol %.0e"
+                               % (dims_label(dims), operator_label(a.mu), a.kappa, a.m, a.k, a.tol),
+                   "lattice": list(dims), "kappa": a.kappa, "mu": a.mu, "plaquette": plaq},
         "cpu_baseline": {"value": value, "unit": "s/RHS", "cores": nproc, "kind": "port",
                          "sample": "per core: GMRES-DR(%d,%d) capped at 2 cycles on its own point source; "
                                    "cycle %.1f s, %d cycles to tol from the second-cycle rate %.3f"

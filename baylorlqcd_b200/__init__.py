@@ -37,7 +37,7 @@ EXPORTED = [
     "qq_heatbath", "qq_ctx_stream", "qq_launch_count", "qq_profile_hop", "qq_profile_hop_read",
     "qq_gfwrite", "qq_gfread", "qq_fpwrite", "qq_fpread", "qq_hsingle_block",
     "qq_hop_tuned_shape", "qq_net_create", "qq_net_destroy", "qq_net_nweights", "qq_net_get_weights",
-    "qq_net_set_weights", "qq_net_apply", "qq_net_grad", "qq_net_train", "qq_fgmres",
+    "qq_net_set_weights", "qq_net_apply", "qq_net_grad", "qq_net_train", "qq_fgmres", "qq_pionrho",
 ]
 
 
@@ -145,6 +145,7 @@ def load_library() -> C.CDLL:
         "qq_net_grad": ([P, P, I, P, P, DP, DP], I),
         "qq_net_train": ([P, P, DP, I, I, D, C.c_ulonglong, DP], I),
         "qq_fgmres": ([P, P, P, P, I, D, I, DP, C.POINTER(qq_solve_info)], I),
+        "qq_pionrho": ([P, P, P, I, P, P, P], I),
         "qq_heatbath": ([P, D, I, C.c_ulonglong, P, DP], I),
         "qq_ctx_stream": ([P, C.POINTER(P)], I),
         "qq_launch_count": ([], C.c_longlong),
@@ -345,6 +346,16 @@ class Lattice:
                                  _d2(kappa), iflag, defl._h if defl else None, C.byref(info))
         _check(st, allow_not_converged=True)
         return x, SolveInfo.from_c(info)
+
+    def pionrho(self, xe, xo, idsrc: int, pion=None, rho=None, decay=None):
+        """pionrho: add one propagator column's local pion, rho and decay correlators
+        (length nt each) to the given arrays (new zero arrays if None)."""
+        nt = self.dims[3]
+        pion = np.zeros(nt) if pion is None else pion
+        rho = np.zeros(nt) if rho is None else rho
+        decay = np.zeros(nt) if decay is None else decay
+        _check(self.lib.qq_pionrho(self._ctx, _ptr(xe), _ptr(xo), int(idsrc), _ptr(pion), _ptr(rho), _ptr(decay)))
+        return pion, rho, decay
 
     def fgmres(self, phi, kappa, m=20, resmax=1e-10, max_cycles=200, net=None, x=None):
         """Flexible GMRES(m) with the network `net` (a Net, or None) as right

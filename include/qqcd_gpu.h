@@ -268,6 +268,15 @@ int qq_profile_hop_read(qq_ctx* ctx, long long* launches, double* ms_total, doub
 int qq_bench_hsingle(qq_ctx* ctx, int precision, int nrhs, int tps, int niter, int flush_l2,
                      double* ms_per_call, double* bytes_per_call);
 
+/* ---- local meson correlators ----
+ * pionrho Q/quark.f90:1033-1212: adds the local pion, rho (third vector component,
+ * times rsgn(idsrc) = (1,-1,-1,1)) and pion-decay (fourth axial component) correlators
+ * of one propagator column -- the solution xe (gblclr = 1) / xo (gblclr = 2) for source
+ * spin idsrc -- to pion[nt], rho[nt], decay[nt] (host or device), as the reference
+ * accumulates them over its sources. */
+int qq_pionrho(qq_ctx* ctx, const double* xe, const double* xo, int idsrc, double* pion, double* rho,
+               double* decay);
+
 /* ---- learned preconditioner (no counterpart in the reference) ----
  * A gauge-covariant network of linear parallel-transport convolution layers: a layer
  * maps Cin channels to Cout channels (a channel is one colour vector per site of the

@@ -275,6 +275,35 @@ class OracleLattice:
                                   _dp(self.u), float(kappa), float(delta), int(dobndry), _dp(J))
         return J
 
+    def pionrho(self, xe, xo, idsrc):
+        """pionrho (Q/quark.f90:1033-1212), restated loop by loop for one process
+        (npt = 1): the local pion, rho and decay correlators of one propagator column.
+        Time slice it - 1 (ibleo 1..4) and it (ibleo 5..8) of the isite range of itbit
+        (nsite = 2 nvhalf / nt sites per pair of slices); spins 1..4 with the signs of
+        the reference's rbit and dbit; the gamma_5 spin rotation the reference applies
+        at two slices leaves the sums of squares unchanged.  Returns (pion, rho, decay)."""
+        nt = self.dims[3]
+        nsite = 2 * self.nvhalf // nt
+        pbit, rbit, dbit = np.zeros(nt), np.zeros(nt), np.zeros(nt)
+        rs = np.array([1.0, -1.0, -1.0, 1.0])
+        ds = np.array([1.0, 1.0, -1.0, -1.0])
+        sitemin = 0
+        for itbit in range(2, nt + 1, 2):
+            it = itbit
+            sl = slice(sitemin, sitemin + nsite)
+            for ibleo in range(4):
+                for ieo in range(2):
+                    for half, tslot in ((ibleo, it - 2), (ibleo + 4, it - 1)):
+                        sq = np.zeros(4)
+                        for x in (xe, xo):
+                            sq += np.sum(x[half, ieo, :, sl, :] ** 2, axis=(1, 2))
+                        pbit[tslot] += sq.sum()
+                        rbit[tslot] += np.dot(rs, sq)
+                        dbit[tslot] += np.dot(ds, sq)
+            sitemin += nsite
+        rsgn = [1.0, -1.0, -1.0, 1.0][idsrc - 1]
+        return pbit, rsgn * rbit, dbit
+
     # ---- gauge helpers ----
     def coldstart(self):
         u = np.zeros(self.gauge_shape)

@@ -38,6 +38,7 @@ EXPORTED = [
     "qq_gfwrite", "qq_gfread", "qq_fpwrite", "qq_fpread", "qq_hsingle_block",
     "qq_hop_tuned_shape", "qq_net_create", "qq_net_destroy", "qq_net_nweights", "qq_net_get_weights",
     "qq_net_set_weights", "qq_net_apply", "qq_net_grad", "qq_net_train", "qq_fgmres", "qq_pionrho",
+    "qq_fgmresdr",
 ]
 
 
@@ -145,6 +146,7 @@ def load_library() -> C.CDLL:
         "qq_net_grad": ([P, P, I, P, P, DP, DP], I),
         "qq_net_train": ([P, P, DP, I, I, D, C.c_ulonglong, DP], I),
         "qq_fgmres": ([P, P, P, P, I, D, I, DP, C.POINTER(qq_solve_info)], I),
+        "qq_fgmresdr": ([P, P, P, P, IP, D, I, DP, C.POINTER(qq_solve_info)], I),
         "qq_pionrho": ([P, P, P, I, P, P, P], I),
         "qq_heatbath": ([P, D, I, C.c_ulonglong, P, DP], I),
         "qq_ctx_stream": ([P, C.POINTER(P)], I),
@@ -357,13 +359,19 @@ class Lattice:
         _check(self.lib.qq_pionrho(self._ctx, _ptr(xe), _ptr(xo), int(idsrc), _ptr(pion), _ptr(rho), _ptr(decay)))
         return pion, rho, decay
 
-    def fgmres(self, phi, kappa, m=20, resmax=1e-10, max_cycles=200, net=None, x=None):
-        """Flexible GMRES(m) with the network `net` (a Net, or None) as right
-        preconditioner, falling back to plain GMRES-DR if it stalls: (x, SolveInfo)."""
+    def fgmres(self, phi, kappa, m=20, resmax=1e-10, max_cycles=200, net=None, x=None, k=0):
+        """Flexible GMRES(m) -- with k > 0 flexible GMRES-DR(m, k) -- with the network
+        `net` (a Net, or None) as right preconditioner, falling back to plain GMRES-DR
+        if it stalls: (x, SolveInfo)."""
         x = np.zeros_like(phi) if x is None else x
         info = qq_solve_info()
-        st = self.lib.qq_fgmres(self._ctx, net._h if net is not None else None, _ptr(phi), _ptr(x), int(m),
-                                float(resmax), int(max_cycles), _d2(kappa), C.byref(info))
+        h = net._h if net is not None else None
+        if k:
+            st = self.lib.qq_fgmresdr(self._ctx, h, _ptr(phi), _ptr(x), _i2((m, k)), float(resmax),
+                                      int(max_cycles), _d2(kappa), C.byref(info))
+        else:
+            st = self.lib.qq_fgmres(self._ctx, h, _ptr(phi), _ptr(x), int(m), float(resmax), int(max_cycles),
+                                    _d2(kappa), C.byref(info))
         _check(st, allow_not_converged=True)
         return x, SolveInfo.from_c(info)
 

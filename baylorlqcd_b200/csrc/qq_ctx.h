@@ -193,5 +193,9 @@ void fill_info(qq_solve_info* info, int status, const SolveStats& s, double seco
 // Flexible GMRES(m) with right preconditioner M(z, v): z = M v (qq_solvers.cu).
 int fgmres_fp64(qq_ctx* c, Spinor phi, Spinor x, int m, double resmax, int max_cycles, const double kappa[2],
                 const std::function<int(Spinor, Spinor)>& M, SolveStats* st, bool* stalled);
+// Flexible GMRES-DR(m, k) with right preconditioner M (qq_solvers.cu).
+int fgmresdr_fp64(qq_ctx* c, Spinor phi, Spinor x, int m, int k, double resmax, int max_cycles,
+                  const double kappa[2], const std::function<int(Spinor, Spinor)>& M, SolveStats* st,
+                  bool* stalled);
 
 }  // namespace qq

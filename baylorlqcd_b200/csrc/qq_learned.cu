@@ -718,16 +718,18 @@ extern "C" int qq_net_train(qq_ctx* c, qq_net* net, const double kappa[2], int n
   return QQ_OK;
 }
 
-// Flexible GMRES(m) preconditioned by the network (or unpreconditioned when net is
-// null); when two consecutive cycles each gain less than a factor 2, plain FP64
-// GMRES-DR(m, m/3) takes over from the current x to the same overall tolerance.
-extern "C" int qq_fgmres(qq_ctx* c, qq_net* net, const double* phi, double* x, int m, double resmax, int max_cycles,
-                         const double kappa[2], qq_solve_info* info) {
+// Flexible GMRES(m) (k = 0) or flexible GMRES-DR(m, k) preconditioned by the network
+// (or unpreconditioned when net is null); when two consecutive cycles each gain less
+// than a factor 2, plain FP64 GMRES-DR(m, max(k, m/3)) takes over from the current x
+// to the same overall tolerance.
+static int flexible_solve(qq_ctx* c, qq_net* net, const double* phi, double* x, int m, int k, double resmax,
+                          int max_cycles, const double kappa[2], qq_solve_info* info) {
   if (!c) return set_error(QQ_BAD_ARG, "null context");
   QQ_CK(cudaSetDevice(c->device));
   if (!c->have_gauge) return set_error(QQ_BAD_ARG, "no gauge field uploaded");
   if (!phi || !x || !kappa) return set_error(QQ_BAD_ARG, "null argument");
-  if (m < 2 || m > 127 || max_cycles < 1 || !(resmax > 0.0)) return set_error(QQ_BAD_ARG, "bad FGMRES arguments");
+  if (m < 2 || m > 127 || k < 0 || k >= m || max_cycles < 1 || !(resmax > 0.0))
+    return set_error(QQ_BAD_ARG, "bad FGMRES arguments");
   if (net) QQ_TRY(net_check(c, net));
   Tmp fphi(c, P64), fx(c, P64);
   const size_t nv = c->ref_doubles();
@@ -740,13 +742,15 @@ extern "C" int qq_fgmres(qq_ctx* c, qq_net* net, const double* phi, double* x, i
   auto M = [&](Spinor z, Spinor v) -> int { return net ? net_apply_field(c, net, z, v) : copy_field(c, z, v); };
   SolveStats s;
   bool stalled = false;
-  int status = fgmres_fp64(c, fphi.sp(), fx.sp(), m, resmax, max_cycles, kappa, M, &s, &stalled);
+  int status = k == 0 ? fgmres_fp64(c, fphi.sp(), fx.sp(), m, resmax, max_cycles, kappa, M, &s, &stalled)
+                      : fgmresdr_fp64(c, fphi.sp(), fx.sp(), m, k, resmax, max_cycles, kappa, M, &s, &stalled);
   int fallback = 0;
   if (status == QQ_NOT_CONVERGED && stalled && s.true_rel > 0.0) {
     fallback = 1;
     const double r0 = s.true_rel;  // relative to the original initial residual
     SolveStats s2;
-    status = gmresdr_fp64(c, fphi.sp(), fx.sp(), m, std::max(1, m / 3), resmax / r0, 0, kappa, nullptr, &s2);
+    status = gmresdr_fp64(c, fphi.sp(), fx.sp(), m, std::max(std::max(1, k), m / 3), resmax / r0, 0, kappa,
+                          nullptr, &s2);
     s.itercount += s2.itercount;
     const int mvp0 = s.mvp;
     s.mvp += s2.mvp;
@@ -771,4 +775,16 @@ extern "C" int qq_fgmres(qq_ctx* c, qq_net* net, const double* phi, double* x, i
   fill_info(info, status, s, ms * 1e-3);
   if (info) info->fallback = fallback;
   return status;
+}
+
+extern "C" int qq_fgmres(qq_ctx* c, qq_net* net, const double* phi, double* x, int m, double resmax, int max_cycles,
+                         const double kappa[2], qq_solve_info* info) {
+  return flexible_solve(c, net, phi, x, m, 0, resmax, max_cycles, kappa, info);
+}
+
+extern "C" int qq_fgmresdr(qq_ctx* c, qq_net* net, const double* phi, double* x, const int GMRES[2], double resmax,
+                           int max_cycles, const double kappa[2], qq_solve_info* info) {
+  if (!GMRES) return set_error(QQ_BAD_ARG, "null GMRES");
+  if (GMRES[1] < 1) return set_error(QQ_BAD_ARG, "FGMRES-DR needs k >= 1");
+  return flexible_solve(c, net, phi, x, GMRES[0], GMRES[1], resmax, max_cycles, kappa, info);
 }

@@ -211,6 +211,95 @@ int fgmres_fp64(qq_ctx* c, Spinor phi, Spinor x, int m, double resmax, int max_c
 }
 
 // ---------------------------------------------------------------------------
+// Flexible GMRES-DR(m, k): flexible GMRES with Morgan's deflated restarts.  The
+// Arnoldi relation A Z_m = V_{m+1} Hbar_m holds with the preconditioned directions
+// Z stored in FP64, so x = x0 + Z y is consistent with the FP64 residual however
+// M is computed.  At a restart the harmonic Ritz step of GMRES-DR gives P; the bases
+// rotate together, V_{k+1} <- V_{m+1} P and Z_k <- Z_m P(0:m, 0:k) (P's first k
+// columns vanish in row m + 1), and the next cycle continues from column k, so the
+// k smallest harmonic Ritz directions of A M stay in the space.  *stalled is set after
+// three consecutive cycles that each gain less than 10% (the first cycles of a
+// deflated method near the critical kappa are slow while its eigenvector space forms).
+// ---------------------------------------------------------------------------
+int fgmresdr_fp64(qq_ctx* c, Spinor phi, Spinor x, int m, int k, double resmax, int max_cycles,
+                  const double kappa[2], const std::function<int(Spinor, Spinor)>& M, SolveStats* st,
+                  bool* stalled) {
+  if (m < 2 || k < 1 || k >= m || m > 127) return set_error(QQ_BAD_ARG, "FGMRES-DR(m,k) out of range");
+  *stalled = false;
+  Arnoldi A;
+  QQ_TRY(A.init(c, P64, m));
+  DevBuf Z;
+  QQ_CK(Z.alloc((size_t)m * A.nel * 16));
+  auto zsp = [&](int j) { return Spinor{static_cast<char*>(Z.p) + (size_t)j * A.nel * 16, nullptr, P64}; };
+  Tmp tmp(c, P64), r(c, P64);
+  double* nrm2 = c->scal.as<double>() + 8;
+  double normnum = 0.0;
+  QQ_TRY(true_residual(c, phi, x, r.sp(), tmp.sp(), kappa, &normnum));
+  st->mvp += 1;
+  if (!std::isfinite(normnum)) return set_error(QQ_NAN, "NaN in initial residual");
+  if (!(normnum > 0.0)) {
+    st->true_rel = 0.0;
+    return QQ_OK;
+  }
+  QQ_TRY(lin(c, A.sp(0), cimm(1.0 / normnum), r.sp()));
+  std::vector<dense::cd> cvec(m + 1, 0.0);
+  cvec[0] = normnum;
+  QQ_TRY(A.zeroH());
+  int j0 = 0, slow = 0;
+  double prev = 1.0;
+  for (int cyc = 1; cyc <= max_cycles; ++cyc) {
+    for (int j = j0; j < m; ++j) {
+      QQ_TRY(M(zsp(j), A.sp(j)));
+      QQ_TRY(arnoldi_step_from(A, j, zsp(j), tmp.sp(), kappa, nrm2));
+      st->itercount += 1;
+      st->mvp += 1;
+    }
+    dense::Mat Hb;
+    QQ_TRY(read_H(A, m, Hb));
+    std::vector<dense::cd> y, srv;
+    dense::hess_lsq(Hb, cvec, m, y, srv);
+    QQ_TRY(upload_cvec(c, y, A.y.as<double>()));
+    const BasisArgs ZB{Z.p, A.nel, A.nel};
+    QQ_CK(launch_basis_accum(P64, ZB, m, A.y.as<double>(), c->g.vh, x, c->st));
+    double rn = 0.0;
+    QQ_TRY(true_residual(c, phi, x, r.sp(), tmp.sp(), kappa, &rn));
+    st->mvp += 1;
+    const double rel = rn / normnum;
+    st->hist.push_back(rel);
+    st->hist_mvp.push_back(st->mvp);
+    st->true_rel = rel;
+    st->ncycles = cyc;
+    if (!std::isfinite(rel)) return set_error(QQ_NAN, "NaN residual in flexible GMRES-DR");
+    if (rel < resmax) return QQ_OK;
+    slow = rel > 0.9 * prev ? slow + 1 : 0;  // deflation needs a few slow cycles to build up
+    prev = rel;
+    if (slow >= 3) {
+      *stalled = true;
+      return QQ_NOT_CONVERGED;
+    }
+    dense::Mat P, Hk;
+    std::vector<dense::cd> cnew, ritz;
+    if (!dense::gmresdr_restart(Hb, srv, m, k, P, Hk, cnew, ritz)) {
+      *stalled = true;  // no usable harmonic Ritz step: let plain GMRES-DR continue
+      return QQ_NOT_CONVERGED;
+    }
+    st->ritz = ritz;
+    DevBuf Pd;
+    QQ_CK(Pd.alloc(sizeof(double) * 2 * (size_t)(m + 1) * (k + 1)));
+    QQ_TRY(upload_mat(c, P, Pd.as<double>(), m + 1));
+    QQ_CK(launch_rotate(P64, A.basis(), m + 1, k + 1, Pd.as<double>(), m + 1, c->st));
+    QQ_CK(launch_rotate(P64, ZB, m, k, Pd.as<double>(), m + 1, c->st));
+    QQ_TRY(reorth(A, k, nrm2));
+    QQ_TRY(A.zeroH());
+    QQ_TRY(upload_mat(c, Hk, A.H.as<double>(), m + 1));
+    std::fill(cvec.begin(), cvec.end(), 0.0);
+    for (int i = 0; i <= k; ++i) cvec[i] = cnew[i];
+    j0 = k;
+  }
+  return QQ_NOT_CONVERGED;
+}
+
+// ---------------------------------------------------------------------------
 // GMRES-DR(m, k), FP64, reference semantics: convergence is tested once per cycle with
 // the true residual ||phi - A x|| / ||phi - A x0|| < resmax (inverters.f90:3270-3298).
 // ---------------------------------------------------------------------------

@@ -313,6 +313,13 @@ int qq_net_train(qq_ctx* ctx, qq_net* net, const double kappa[2], int nsamples, 
  * guess in, solution out. */
 int qq_fgmres(qq_ctx* ctx, qq_net* net, const double* phi, double* x, int m, double resmax, int max_cycles,
               const double kappa[2], qq_solve_info* info);
+/* Flexible GMRES-DR(GMRES[0], GMRES[1]): qq_fgmres with Morgan's deflated restarts
+ * (both the Krylov basis and the preconditioned directions are rotated onto the
+ * GMRES[1] smallest harmonic Ritz vectors of Hdbletm N), so the low modes the
+ * network cannot learn stay deflated.  Same convergence test; the fallback follows three
+ * consecutive cycles that each gain less than 10%. */
+int qq_fgmresdr(qq_ctx* ctx, qq_net* net, const double* phi, double* x, const int GMRES[2], double resmax,
+                int max_cycles, const double kappa[2], qq_solve_info* info);
 
 /* The kernel shape (the codes of qq_bench_hsingle) the autotuner chose for the first
  * hopping launch of Hdbletm (Wilson, else twisted mass, else the second launch) at this

@@ -143,3 +143,26 @@ def test_stalled_preconditioner_falls_back(config):
     assert info.fallback == 1
     assert info.status == 0 and info.true_rel < 1e-10
     net.close()
+
+
+def test_flexible_gmresdr_gains(config):
+    """Flexible GMRES-DR(32, 10) with the trained network against the same method
+    without it (which is GMRES-DR(32, 10) in flexible form): same 1e-10 true residual,
+    fewer applications of Hdbletm, no fallback; the unpreconditioned flexible form
+    needs the applications of the reference's GMRES-DR."""
+    import baylorlqcd_b200 as qq
+
+    lat, _ = config
+    net = qq.Net((4, 8, 8, 4), seed=4, scale=KAPPA[0] ** 2)
+    net.train(lat, KAPPA, nsamples=6, nsteps=150, lr=2e-3, seed=6)
+    phi = random_half(lat.ntotal, lat.nvhalf, seed=9)
+    x_net, inet = lat.fgmres(phi, KAPPA, m=32, k=10, resmax=1e-10, net=net)
+    x_pl, ipl = lat.fgmres(phi, KAPPA, m=32, k=10, resmax=1e-10, net=None)
+    x_dr, idr = lat.gmresdr(phi, np.zeros_like(phi), (32, 10), 1e-10, kappa=KAPPA)
+    assert inet.status == 0 and ipl.status == 0 and inet.fallback == 0 and ipl.fallback == 0
+    assert inet.true_rel < 1e-10 and ipl.true_rel < 1e-10
+    assert ipl.mvp == idr.mvp
+    nv = lat.nvhalf
+    assert np.linalg.norm((x_net - x_dr)[:, :, :, :nv]) / np.linalg.norm(x_dr[:, :, :, :nv]) < 1e-8
+    assert inet.mvp < 0.8 * ipl.mvp, (inet.mvp, ipl.mvp)
+    net.close()

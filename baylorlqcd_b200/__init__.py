@@ -37,7 +37,7 @@ EXPORTED = [
     "qq_heatbath", "qq_ctx_stream", "qq_launch_count", "qq_profile_hop", "qq_profile_hop_read",
     "qq_gfwrite", "qq_gfread", "qq_fpwrite", "qq_fpread", "qq_hsingle_block",
     "qq_hop_tuned_shape", "qq_net_create", "qq_net_destroy", "qq_net_nweights", "qq_net_get_weights",
-    "qq_net_set_weights", "qq_net_apply", "qq_net_grad", "qq_net_train", "qq_fgmres", "qq_pionrho",
+    "qq_net_set_weights", "qq_net_apply", "qq_net_grad", "qq_net_train", "qq_fgmres", "qq_pionrho", "qq_twvev",
     "qq_fgmresdr",
 ]
 
@@ -148,6 +148,7 @@ def load_library() -> C.CDLL:
         "qq_fgmres": ([P, P, P, P, I, D, I, DP, C.POINTER(qq_solve_info)], I),
         "qq_fgmresdr": ([P, P, P, P, IP, D, I, DP, C.POINTER(qq_solve_info)], I),
         "qq_pionrho": ([P, P, P, I, P, P, P], I),
+        "qq_twvev": ([P, D, D, IP, I, I, I, I, I, P], I),
         "qq_heatbath": ([P, D, I, C.c_ulonglong, P, DP], I),
         "qq_ctx_stream": ([P, C.POINTER(P)], I),
         "qq_launch_count": ([], C.c_longlong),
@@ -358,6 +359,15 @@ class Lattice:
         decay = np.zeros(nt) if decay is None else decay
         _check(self.lib.qq_pionrho(self._ctx, _ptr(xe), _ptr(xo), int(idsrc), _ptr(pion), _ptr(rho), _ptr(decay)))
         return pion, rho, decay
+
+    def twvev(self, kappa, delta=0.0, io=(1, 1, 1), dobndry=0, ir=1, nsub=6, nmom=5, nop=6):
+        """twvev: the perturbative vacuum expectation values Jvev, as an array of shape
+        (nop, nmom, 6, nt, 2) (the reverse of the Fortran (2, nt, 6, nmom, nop))."""
+        J = np.zeros((nop, nmom, 6, self.dims[3], 2))
+        iov = np.ascontiguousarray(io, dtype=np.int32)
+        _check(self.lib.qq_twvev(self._ctx, float(kappa), float(delta), iov.ctypes.data_as(C.POINTER(C.c_int)),
+                                 int(dobndry), int(ir), int(nsub), int(nmom), int(nop), _ptr(J)))
+        return J
 
     def fgmres(self, phi, kappa, m=20, resmax=1e-10, max_cycles=200, net=None, x=None, k=0):
         """Flexible GMRES(m) -- with k > 0 flexible GMRES-DR(m, k) -- with the network

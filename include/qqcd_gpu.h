@@ -277,6 +277,22 @@ int qq_bench_hsingle(qq_ctx* ctx, int precision, int nrhs, int tps, int niter, i
 int qq_pionrho(qq_ctx* ctx, const double* xe, const double* xo, int idsrc, double* pion, double* rho,
                double* decay);
 
+/* ---- perturbative vacuum expectation values of the loop operators ----
+ * twvev Q/vevbleft.f90:757-2536: the hopping-parameter expansion of the twisted-mass
+ * propagator to order kappa^6 from unit sources at every site, colour and spin, with
+ * the context's gauge field; no noise.  Fills Jvev(2, nt, 6, nmom, nop) (Fortran order,
+ * host or device): level 4 (nsub = 4 or 6) holds orders kappa^3 (currents) and kappa^4
+ * (psibar psi, psibar gamma5 psi), plus kappa^1 / kappa^2 when delta /= 0; level 6
+ * (nsub = 6) orders kappa^5 / kappa^6; every other entry is zero, as in the reference.
+ * Operators iop 1..6: J4 point-split time current, psibar psi, J1..J3 point-split
+ * spatial currents, psibar gamma5 psi (momenta imom 2..5: the reference's ffac / fas
+ * projections about the origin io, 1-based).  kappa: the hopping parameter, delta: the
+ * twist angle; dobndry = 1: fixed time boundary; ir = +-1: the Wilson r.  The caller's
+ * kappa scaling and level combination (Q/disconloops.f90:3793-3805) are left to the
+ * caller, as in the reference.  nmom 1..5, nop >= 6 (operators past 6 stay zero). */
+int qq_twvev(qq_ctx* ctx, double kappa, double delta, const int io[3], int dobndry, int ir,
+             int nsub, int nmom, int nop, double* Jvev);
+
 /* ---- learned preconditioner (no counterpart in the reference) ----
  * A gauge-covariant network of linear parallel-transport convolution layers: a layer
  * maps Cin channels to Cout channels (a channel is one colour vector per site of the

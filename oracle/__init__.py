@@ -69,6 +69,8 @@ def lib() -> C.CDLL:
             "oq_evalues": ([I, I, I, I, DP, I, DP, DP, I], None),
             "oq_orgschur": ([IP, I, DP, I, DP, I, DP, IP], None),
             "oq_twaverage_level0": ([P, DP, DP, DP, DP, DP, D, D, C.c_int, DP], None),
+            "oq_twvev": ([P, DP, D, D, IP, I, I, I, I, I, DP], None),
+            "oq_twvev_sites": ([P, DP, D, D, IP, I, I, I, IP, I, DP], None),
             "oq_set_kcyclim": ([I], None),
             "oq_coldstart": ([P, DP], None),
             "oq_aveplaq": ([P, DP], D),
@@ -274,6 +276,26 @@ class OracleLattice:
                                   _dp(np.ascontiguousarray(xe)), _dp(np.ascontiguousarray(xo)),
                                   _dp(self.u), float(kappa), float(delta), int(dobndry), _dp(J))
         return J
+
+    def twvev(self, kappa, delta=0.0, io=(1, 1, 1), dobndry=0, ir=1, nsub=6, nmom=5, nop=6):
+        """twvev (Q/vevbleft.f90:757-2536) on the stored gauge field: Jvev as a numpy
+        array of shape (nop, nmom, 6, nt, 2), the reverse of the Fortran (2, nt, 6, nmom,
+        nop)."""
+        J = np.zeros((nop, nmom, 6, self.dims[3], 2))
+        _, iop = _ip(io)
+        lib().oq_twvev(self._g, _dp(self.u), float(kappa), float(delta), iop, int(dobndry), int(ir), int(nsub),
+                       int(nmom), int(nop), _dp(J))
+        return J
+
+    def twvev_sites(self, sites, kappa, delta=0.0, io=(1, 1, 1), dobndry=0, ir=1, nsub=6):
+        """opertemp contributions of the listed 1-based lexicographic sites:
+        array (isb 2, momentum 5, nt, op 12)."""
+        O = np.zeros((2, 5, self.dims[3], 12))
+        s, sp = _ip(sites)
+        _, iop = _ip(io)
+        lib().oq_twvev_sites(self._g, _dp(self.u), float(kappa), float(delta), iop, int(dobndry), int(ir),
+                             int(nsub), sp, len(s), _dp(O))
+        return O
 
     def pionrho(self, xe, xo, idsrc):
         """pionrho (Q/quark.f90:1033-1212), restated loop by loop for one process

@@ -135,6 +135,18 @@ void oq_twaverage_level0(const oq_geom* g, const double* be, const double* bo,
                          const double* xe, const double* xo, const double* u,
                          double kappa, double delta, int dobndry, double* J);
 
+// ---- perturbative vacuum expectation values (Q/vevbleft.f90 twvev; see vev.cpp) ----
+// Jvev(2, nt, 6, nmom, nop), Fortran order; levels 4 (orders kappa^3 / kappa^4, and
+// kappa^1 / kappa^2 when delta /= 0) and 6 (orders kappa^5 / kappa^6, nsub = 6) are
+// filled, the other levels are zero.  io: momentum origin (1-based); ir = +-1.
+void oq_twvev(const oq_geom* g, const double* u, double kappa, double delta, const int io[3],
+              int dobndry, int ir, int nsub, int nmom, int nop, double* Jvev);
+// The opertemp contributions of the listed sites (1-based lexicographic):
+// opertemp[((isb * 5 + ix) * nt + t) * 12 + op], ix 0..4, op 0..11, isb 0..1.
+void oq_twvev_sites(const oq_geom* g, const double* u, double kappa, double delta,
+                    const int io[3], int dobndry, int ir, int nsub, const int* sites,
+                    int nsites, double* opertemp);
+
 // ---- gauge field helpers ----
 void oq_coldstart(const oq_geom* g, double* u);
 double oq_aveplaq(const oq_geom* g, const double* u);

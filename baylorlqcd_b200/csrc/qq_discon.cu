@@ -13,6 +13,7 @@
 // host, as in the reference.
 #include <algorithm>
 #include <cstring>
+#include <functional>
 #include <vector>
 
 #include "qq_ctx.h"
@@ -21,17 +22,16 @@ namespace qq {
 int sources_z(qq_ctx* c, double* be, double* bo, bool z4);
 int batch_solve(qq_ctx* c, int nrhs, const double* be, const double* bo, const double kappa[2],
                 const qq_method* method, double* xe, double* xo, qq_solve_info* infos);
-int traces_level0(qq_ctx* c, const double* be, const double* bo, const double* xe,
-                  const double* xo, double kappa, double delta, int dobndry, double* J);
-}  // namespace qq
+int traces_mom(qq_ctx* c, const double* be, const double* bo, const double* xe, const double* xo,
+               double kappa, double delta, const int io[3], int dobndry, int nmom, double* J);
 
-using namespace qq;
+namespace {
 
-extern "C" int qq_discon_traces(qq_ctx* c, int noise_kind, int nnoise, const double kappa[2],
-                                const qq_method* method, double delta, int dobndry, double* J,
-                                qq_solve_info* infos) {
-  if (!c) return set_error(QQ_BAD_ARG, "null context");
-  if (!kappa || !method || !J) return set_error(QQ_BAD_ARG, "null argument");
+// The noise loop: per noise (generator order), draw, solve, take the kappa-scaled traces
+// J(2, nt, nmom, 6) and hand them to add().
+int discon_loop(qq_ctx* c, int noise_kind, int nnoise, const double kappa[2], const qq_method* method,
+                double delta, const int io[3], int dobndry, int nmom,
+                const std::function<void(const double*)>& add, qq_solve_info* infos) {
   if (noise_kind != 2 && noise_kind != 4) return set_error(QQ_BAD_ARG, "noise_kind must be 2 or 4");
   if (nnoise < 1) return set_error(QQ_BAD_ARG, "nnoise must be >= 1");
   if (method->solver < 0 || method->solver > 2) return set_error(QQ_BAD_ARG, "solver must be 0, 1 or 2");
@@ -45,7 +45,7 @@ extern "C" int qq_discon_traces(qq_ctx* c, int noise_kind, int nnoise, const dou
   QQ_CK(dbo.alloc(sizeof(double) * nv * block));
   QQ_CK(dxe.alloc(sizeof(double) * nv * block));
   QQ_CK(dxo.alloc(sizeof(double) * nv * block));
-  std::vector<double> hbe(nv), hbo(nv), Jn((size_t)12 * nt), Jsum((size_t)12 * nt, 0.0);
+  std::vector<double> hbe(nv), hbo(nv), Jn((size_t)12 * nt * nmom);
   qq_defl* defl = nullptr;
   if (method->solver == 2) QQ_TRY(qq_defl_create(c, method->m, method->k, &defl));
   int rc = QQ_OK;
@@ -84,15 +84,127 @@ extern "C" int qq_discon_traces(qq_ctx* c, int noise_kind, int nnoise, const dou
     }
     if (st == QQ_NOT_CONVERGED) rc = QQ_NOT_CONVERGED;
     for (int k = 0; k < nb; ++k) {
-      QQ_TRY(traces_level0(c, dbe.as<double>() + nv * k, dbo.as<double>() + nv * k, dxe.as<double>() + nv * k,
-                           dxo.as<double>() + nv * k, kappa[0], delta, dobndry, Jn.data()));
-      for (size_t e = 0; e < Jn.size(); ++e) Jsum[e] += Jn[e];
+      QQ_TRY(traces_mom(c, dbe.as<double>() + nv * k, dbo.as<double>() + nv * k, dxe.as<double>() + nv * k,
+                        dxo.as<double>() + nv * k, kappa[0], delta, io, dobndry, nmom, Jn.data()));
+      add(Jn.data());
     }
   }
   if (defl) qq_defl_destroy(defl);
+  return rc;
+}
+
+// Levels twAverage fills (:4519-4580): 1 always, 4 for nsub = 4 or 6, 6 for nsub = 6
+// (0-based 0, 3, 5); with its subtraction switched off all carry the unsubtracted traces.
+std::vector<int> filled_levels(int nsub) {
+  std::vector<int> lv{0};
+  if (nsub == 4 || nsub == 6) lv.push_back(3);
+  if (nsub == 6) lv.push_back(5);
+  return lv;
+}
+
+// J(2, nt, nmom, 6) -> add into Jl(2, nt, 6, nmom, nop) at the given levels.
+void add_levels(const double* J, int nt, int nmom, int nop, const std::vector<int>& lv, double* Jl) {
+  for (int iop = 0; iop < 6 && iop < nop; ++iop)
+    for (int im = 0; im < nmom; ++im)
+      for (int l : lv)
+        for (int t = 0; t < nt; ++t)
+          for (int ri = 0; ri < 2; ++ri) {
+            const size_t src = (((size_t)iop * nmom + im) * nt + t) * 2 + ri;
+            const size_t dst = ((((size_t)iop * nmom + im) * 6 + l) * nt + t) * 2 + ri;
+            Jl[dst] = Jl[dst] + J[src];
+          }
+}
+
+}  // namespace
+}  // namespace qq
+
+using namespace qq;
+
+extern "C" int qq_twvev(qq_ctx* c, double kappa, double delta, const int io[3], int dobndry, int ir, int nsub,
+                        int nmom, int nop, double* Jvev);
+
+extern "C" int qq_discon_traces(qq_ctx* c, int noise_kind, int nnoise, const double kappa[2],
+                                const qq_method* method, double delta, int dobndry, double* J,
+                                qq_solve_info* infos) {
+  if (!c) return set_error(QQ_BAD_ARG, "null context");
+  if (!kappa || !method || !J) return set_error(QQ_BAD_ARG, "null argument");
+  const int nt = c->g.n[3];
+  const int io[3] = {1, 1, 1};
+  std::vector<double> Jsum((size_t)12 * nt, 0.0);
+  const int rc = discon_loop(c, noise_kind, nnoise, kappa, method, delta, io, dobndry, 1,
+                             [&](const double* Jn) {
+                               for (size_t e = 0; e < Jsum.size(); ++e) Jsum[e] += Jn[e];
+                             },
+                             infos);
   if (rc != QQ_OK && rc != QQ_NOT_CONVERGED) return rc;
   const double norm = 1.0 / ((double)nnoise * c->g.n[0] * c->g.n[1] * c->g.n[2]);
   for (size_t e = 0; e < Jsum.size(); ++e) Jsum[e] *= norm;
   QQ_CK(cudaMemcpy(J, Jsum.data(), sizeof(double) * Jsum.size(), cudaMemcpyDefault));
+  return rc;
+}
+
+extern "C" int qq_twaverage(qq_ctx* c, const double* be, const double* bo, const double* xe, const double* xo,
+                            double kappa, double delta, const int io[3], int dobndry, int nsub, int nmom, int nop,
+                            double* Jave) {
+  (void)kappa;  // enters only the subtraction levels, which the reference leaves switched off
+  if (!c) return set_error(QQ_BAD_ARG, "null context");
+  if (!be || !bo || !xe || !xo || !io || !Jave) return set_error(QQ_BAD_ARG, "null argument");
+  if (nop < 6) return set_error(QQ_BAD_ARG, "nop must be at least 6");
+  QQ_CK(cudaSetDevice(c->device));
+  const int nt = c->g.n[3];
+  std::vector<double> J((size_t)12 * nt * std::max(nmom, 1));
+  QQ_TRY(traces_mom(c, be, bo, xe, xo, 1.0, delta, io, dobndry, nmom, J.data()));
+  std::vector<double> out((size_t)2 * nt * 6 * nmom * nop, 0.0);
+  if (nsub == 0 || nsub == 4 || nsub == 6) add_levels(J.data(), nt, nmom, nop, filled_levels(nsub), out.data());
+  QQ_CK(cudaMemcpy(Jave, out.data(), sizeof(double) * out.size(), cudaMemcpyDefault));
+  return QQ_OK;
+}
+
+extern "C" int qq_twistdiscon(qq_ctx* c, int noise_kind, int nnoise, const double kappa[2],
+                              const qq_method* method, double delta, const int io[3], int dobndry, int nsub,
+                              int nmom, int nop, double* Jtotal, qq_solve_info* infos) {
+  if (!c) return set_error(QQ_BAD_ARG, "null context");
+  if (!kappa || !method || !io || !Jtotal) return set_error(QQ_BAD_ARG, "null argument");
+  if (nop < 6) return set_error(QQ_BAD_ARG, "nop must be at least 6");
+  if (nmom < 1 || nmom > 5) return set_error(QQ_BAD_ARG, "nmom must be 1..5");
+  const int nt = c->g.n[3];
+  const size_t n = (size_t)2 * nt * 6 * nmom * nop;
+  auto at = [&](int ri, int t, int lv, int im, int iop) {
+    return ((((size_t)iop * nmom + im) * 6 + lv) * nt + t) * 2 + ri;
+  };
+  // Jtotal = numnoises * Jvev (:3779-3839): twvev, kappa on every operator but 2 and 6,
+  // the highest order combined with the first for nsub = 6
+  std::vector<double> jt(n, 0.0);
+  if (nsub == 4 || nsub == 6) {
+    std::vector<double> jv(n);
+    QQ_TRY(qq_twvev(c, kappa[0], delta, io, dobndry, 1, nsub, nmom, nop, jv.data()));
+    for (int iop = 0; iop < nop; ++iop)
+      if (iop != 1 && iop != 5)
+        for (int im = 0; im < nmom; ++im)
+          for (int lv = 0; lv < 6; ++lv)
+            for (int t = 0; t < nt; ++t)
+              for (int ri = 0; ri < 2; ++ri) jv[at(ri, t, lv, im, iop)] = kappa[0] * jv[at(ri, t, lv, im, iop)];
+    if (nsub == 6)
+      for (int iop = 0; iop < nop; ++iop)
+        for (int im = 0; im < nmom; ++im)
+          for (int t = 0; t < nt; ++t)
+            for (int ri = 0; ri < 2; ++ri)
+              jv[at(ri, t, 5, im, iop)] = jv[at(ri, t, 3, im, iop)] + jv[at(ri, t, 5, im, iop)];
+    for (size_t e = 0; e < n; ++e) jt[e] = nnoise * jv[e];
+  }
+  // + the kappa-scaled traces of every noise at the levels twAverage fills (:4040-4045)
+  const std::vector<int> lv = filled_levels(nsub);
+  const bool any = nsub == 0 || nsub == 4 || nsub == 6;
+  const int rc = discon_loop(c, noise_kind, nnoise, kappa, method, delta, io, dobndry, nmom,
+                             [&](const double* Jn) {
+                               if (any) add_levels(Jn, nt, nmom, nop, lv, jt.data());
+                             },
+                             infos);
+  if (rc != QQ_OK && rc != QQ_NOT_CONVERGED) return rc;
+  // :4161-4164
+  for (size_t e = 0; e < n; ++e) jt[e] = jt[e] / (double)nnoise;
+  const double nxyz = (double)c->g.n[0] * c->g.n[1] * c->g.n[2];
+  for (size_t e = 0; e < n; ++e) jt[e] = jt[e] / nxyz;
+  QQ_CK(cudaMemcpy(Jtotal, jt.data(), sizeof(double) * n, cudaMemcpyDefault));
   return rc;
 }

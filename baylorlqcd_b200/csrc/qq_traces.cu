@@ -15,6 +15,10 @@
 // solution and the context's links; a second kernel sums each time slice in a fixed
 // order, so results are deterministic.  The test suite checks these closed forms
 // against a literal CPU restatement of the reference's loops.
+#include <cmath>
+#include <cstring>
+#include <vector>
+
 #include "qq_ctx.h"
 
 namespace qq {
@@ -166,18 +170,32 @@ __global__ void __launch_bounds__(128) trace_sites_kernel(Geom g, RefDims rd, co
   for (int k = 0; k < kTraceVals; ++k) val[(size_t)k * V + L] = out[k];
 }
 
-// One block per time slice: fixed-order sum of its sites -> J[(iop * nt + t) * 2 + ri].
+// Momentum projections imom 2..5 (twAverage :4434-4503): output slot o takes per-site
+// value kMomSrc[o] times factor kMomFac[o] of the site (0 = ffac, 1..3 = fas1..3), i.e.
+// rho, psibar psi, psibar gamma5 psi by ffac and (Im J1 fas3, Im J2 fas1),
+// (Im J3 fas2, Im J1 fas2), (Im J2 fas3, Im J3 fas1) for operators 3, 4, 5.
+__device__ __constant__ int kMomSrc[kTraceVals] = {0, 1, 2, 3, 5, 7, 9, 5, 7, 9, 10, 11};
+__device__ __constant__ int kMomFac[kTraceVals] = {0, 0, 0, 0, 3, 1, 2, 2, 3, 1, 0, 0};
+
+// One block per (time slice, momentum): fixed-order sum of the slice's sites ->
+// J[((iop * nmom + imom) * nt + t) * 2 + ri]; mfac[spatial site][imom - 2][4].
 __global__ void __launch_bounds__(256) trace_slices_kernel(const double* val, int V, int v3, int nt,
-                                                           double* J) {
-  const int t = blockIdx.x;
+                                                           const double* mfac, int nmom, double* J) {
+  const int t = blockIdx.x, km = blockIdx.y;
   __shared__ double red[kTraceVals][256];
   double acc[kTraceVals];
 #pragma unroll
   for (int k = 0; k < kTraceVals; ++k) acc[k] = 0.0;
   for (int i = threadIdx.x; i < v3; i += blockDim.x) {
     const size_t L = (size_t)t * v3 + i;
+    if (km == 0) {
 #pragma unroll
-    for (int k = 0; k < kTraceVals; ++k) acc[k] += val[(size_t)k * V + L];
+      for (int k = 0; k < kTraceVals; ++k) acc[k] += val[(size_t)k * V + L];
+    } else {
+      const double* f = mfac + ((size_t)i * 4 + (km - 1)) * 4;
+#pragma unroll
+      for (int k = 0; k < kTraceVals; ++k) acc[k] += val[(size_t)kMomSrc[k] * V + L] * f[kMomFac[k]];
+    }
   }
 #pragma unroll
   for (int k = 0; k < kTraceVals; ++k) red[k][threadIdx.x] = acc[k];
@@ -190,16 +208,57 @@ __global__ void __launch_bounds__(256) trace_slices_kernel(const double* val, in
   }
   if (threadIdx.x < kTraceVals) {
     const int k = threadIdx.x, iop = k / 2, ri = k % 2;
-    J[((size_t)iop * nt + t) * 2 + ri] = red[k][0];
+    J[(((size_t)iop * nmom + km) * nt + t) * 2 + ri] = red[k][0];
   }
 }
 
 }  // namespace
 
+void momentum_table(const int* n, const int io[3], std::vector<double>& mf) {
+  const int nx = n[0], ny = n[1], nz = n[2];
+  mf.assign((size_t)nx * ny * nz * 16, 0.0);
+  const double p1 = 8.0 * std::atan(1.0) / nx, p2 = 8.0 * std::atan(1.0) / ny, p3 = 8.0 * std::atan(1.0) / nz;
+  for (int z = 0; z < nz; ++z)
+    for (int y = 0; y < ny; ++y)
+      for (int x = 0; x < nx; ++x) {
+        const double dx = (double)(x + 1 - io[0]) * p1, dy = (double)(y + 1 - io[1]) * p2,
+                     dz = (double)(z + 1 - io[2]) * p3;
+        const double cx = std::cos(dx), cy = std::cos(dy), cz = std::cos(dz), sx = std::sin(dx), sy = std::sin(dy),
+                     sz = std::sin(dz);
+        const double v[16] = {(cx + cy + cz) / 3.0,
+                              sx,
+                              sy,
+                              sz,
+                              (cx * cy + cx * cz + cy * cz) / 3.0,
+                              sx * (cy + cz) / 2.0,
+                              sy * (cx + cz) / 2.0,
+                              sz * (cx + cy) / 2.0,
+                              cx * cy * cz,
+                              sx * cy * cz,
+                              sy * cx * cz,
+                              sz * cx * cy,
+                              (std::cos(2.0 * dx) + std::cos(2.0 * dy) + std::cos(2.0 * dz)) / 3.0,
+                              std::sin(2.0 * dx),
+                              std::sin(2.0 * dy),
+                              std::sin(2.0 * dz)};
+        std::memcpy(mf.data() + (size_t)(x + nx * (y + ny * z)) * 16, v, sizeof(v));
+      }
+}
+
+int traces_mom(qq_ctx* c, const double* be, const double* bo, const double* xe, const double* xo,
+               double kappa, double delta, const int io[3], int dobndry, int nmom, double* J);
+
 int traces_level0(qq_ctx* c, const double* be, const double* bo, const double* xe,
                   const double* xo, double kappa, double delta, int dobndry, double* J) {
+  const int io[3] = {1, 1, 1};
+  return traces_mom(c, be, bo, xe, xo, kappa, delta, io, dobndry, 1, J);
+}
+
+int traces_mom(qq_ctx* c, const double* be, const double* bo, const double* xe, const double* xo,
+               double kappa, double delta, const int io[3], int dobndry, int nmom, double* J) {
   if (!c->have_gauge) return set_error(QQ_BAD_ARG, "no gauge field uploaded");
   if (dobndry != 0 && dobndry != 1) return set_error(QQ_BAD_ARG, "dobndry must be 0 or 1");
+  if (nmom < 1 || nmom > 5) return set_error(QQ_BAD_ARG, "nmom must be 1..5");
   const size_t nref = c->ref_doubles();
   const double *dbe, *dbo, *dxe, *dxo;
   QQ_TRY(stage_in(c, 0, be, nref, &dbe));
@@ -207,10 +266,17 @@ int traces_level0(qq_ctx* c, const double* be, const double* bo, const double* x
   QQ_TRY(stage_in(c, 2, xe, nref, &dxe));
   QQ_TRY(stage_in(c, 3, xo, nref, &dxo));
   const int V = 2 * c->g.vh, nt = c->g.n[3], v3 = V / nt;
-  const size_t nval = (size_t)kTraceVals * V, nJ = (size_t)kTraceVals * nt;
-  QQ_CK(c->trace_buf.alloc(sizeof(double) * (nval + nJ)));
+  const size_t nval = (size_t)kTraceVals * V, nJ = (size_t)kTraceVals * nt * nmom,
+               nmf = nmom > 1 ? (size_t)v3 * 16 : 0;
+  QQ_CK(c->trace_buf.alloc(sizeof(double) * (nval + nJ + nmf)));
   double* val = c->trace_buf.as<double>();
   double* dJ = val + nval;
+  double* dmf = dJ + nJ;
+  std::vector<double> mf;
+  if (nmom > 1) {
+    momentum_table(c->g.n, io, mf);
+    QQ_CK(cudaMemcpyAsync(dmf, mf.data(), sizeof(double) * nmf, cudaMemcpyHostToDevice, c->st));
+  }
   const dim3 grd((V + 127) / 128);
   if (c->recon64 == 18)
     trace_sites_kernel<18><<<grd, 128, 0, c->st>>>(c->g, c->rd, dbe, dbo, dxe, dxo, c->gauge64.p, kappa,
@@ -219,11 +285,11 @@ int traces_level0(qq_ctx* c, const double* be, const double* bo, const double* x
     trace_sites_kernel<12><<<grd, 128, 0, c->st>>>(c->g, c->rd, dbe, dbo, dxe, dxo, c->gauge64.p, kappa,
                                                    std::cos(delta), std::sin(delta), dobndry, val);
   QQ_CK(cudaGetLastError());
-  trace_slices_kernel<<<nt, 256, 0, c->st>>>(val, V, v3, nt, dJ);
+  trace_slices_kernel<<<dim3(nt, nmom), 256, 0, c->st>>>(val, V, v3, nt, dmf, nmom, dJ);
   QQ_CK(cudaGetLastError());
   count_launch(2);
   QQ_CK(cudaMemcpyAsync(J, dJ, sizeof(double) * nJ, cudaMemcpyDefault, c->st));
-  QQ_CK(cudaStreamSynchronize(c->st));
+  QQ_CK(cudaStreamSynchronize(c->st));  // also keeps mf alive until its copy is done
   return QQ_OK;
 }
 

@@ -438,6 +438,11 @@ struct VevProgram {
 };
 
 using Off = std::array<int, 4>;
+}  // namespace
+
+void momentum_table(const int* n, const int io[3], std::vector<double>& mf);
+
+namespace {
 
 template <class F>
 void vev_shell(int md, F&& f) {  // the reference's shell order (:1172-1180)
@@ -583,24 +588,8 @@ extern "C" int qq_twvev(qq_ctx* c, double kappa, double delta, const int io[3], 
     QQ_TRY(build_vev_program(c->g.n, P));
     const int nx = c->g.n[0], ny = c->g.n[1], nz = c->g.n[2], nxyz = nx * ny * nz;
     // momentum factors (:955-985), at spatial sites
-    std::vector<double> mf((size_t)nxyz * 16);
-    const double p1 = 8.0 * std::atan(1.0) / nx, p2 = 8.0 * std::atan(1.0) / ny, p3 = 8.0 * std::atan(1.0) / nz;
-    for (int z = 0; z < nz; ++z)
-      for (int y = 0; y < ny; ++y)
-        for (int x = 0; x < nx; ++x) {
-          const double dx = (double)(x + 1 - io[0]) * p1, dy = (double)(y + 1 - io[1]) * p2,
-                       dz = (double)(z + 1 - io[2]) * p3;
-          const double cx = std::cos(dx), cy = std::cos(dy), cz = std::cos(dz), sx = std::sin(dx),
-                       sy = std::sin(dy), sz = std::sin(dz);
-          double* m = mf.data() + ((size_t)(x + nx * (y + ny * z))) * 16;
-          const double v[16] = {(cx + cy + cz) / 3.0, sx, sy, sz,
-                                (cx * cy + cx * cz + cy * cz) / 3.0, sx * (cy + cz) / 2.0, sy * (cx + cz) / 2.0,
-                                sz * (cx + cy) / 2.0,
-                                cx * cy * cz, sx * cy * cz, sy * cx * cz, sz * cx * cy,
-                                (std::cos(2.0 * dx) + std::cos(2.0 * dy) + std::cos(2.0 * dz)) / 3.0,
-                                std::sin(2.0 * dx), std::sin(2.0 * dy), std::sin(2.0 * dz)};
-          std::memcpy(m, v, sizeof(v));
-        }
+    std::vector<double> mf;
+    momentum_table(c->g.n, io, mf);
     // block shape: warps sharing one site's link cache, as many as shared memory holds
     int dev_smem = 0;
     QQ_CK(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device));

@@ -32,9 +32,23 @@ struct Lex {
 
 }  // namespace
 
+extern "C" void oq_twaverage_mom(const oq_geom* g, const double* be, const double* bo, const double* xe,
+                                 const double* xo, const double* u, double kappa, double delta, const int io[3],
+                                 int dobndry, int nmom, double* J);
+
 extern "C" void oq_twaverage_level0(const oq_geom* g, const double* be, const double* bo,
                                     const double* xe, const double* xo, const double* u,
                                     double kappa, double delta, int dobndry, double* J) {
+  const int io[3] = {1, 1, 1};
+  oq_twaverage_mom(g, be, bo, xe, xo, u, kappa, delta, io, dobndry, 1, J);
+}
+
+// The same traces with twAverage's momentum projections (:4434-4503): imom 2..5 weight
+// rho, psibar psi and psibar gamma5 psi by ffac and the imaginary parts of the
+// currents by fas1..3 at the site each value sits on; J(2, nt, nmom, 6).
+extern "C" void oq_twaverage_mom(const oq_geom* g, const double* be, const double* bo, const double* xe,
+                                 const double* xo, const double* u, double kappa, double delta, const int io[3],
+                                 int dobndry, int nmom, double* J) {
   const Lex L{g->n[0], g->n[1], g->n[2], g->n[3]};
   const int V = L.nx * L.ny * L.nz * L.nt;
   // lexicographic gathers: [site][colour][spin] (spin, colour 0-based)
@@ -81,8 +95,12 @@ extern "C" void oq_twaverage_level0(const oq_geom* g, const double* be, const do
   const double cosd = std::cos(delta), sind = std::sin(delta);
   const int cd[4] = {2, 3, 0, 1};
   const double sgn[4] = {1.0, 1.0, -1.0, -1.0};
-  std::vector<double> op((size_t)12 * L.nt, 0.0);
-  auto OP = [&](int k, int t) -> double& { return op[(size_t)k * L.nt + t]; };
+  std::vector<double> op((size_t)12 * L.nt * 5, 0.0);
+  auto OPm = [&](int k, int t, int ix) -> double& { return op[((size_t)ix * 12 + k) * L.nt + t]; };
+  auto OP = [&](int k, int t) -> double& { return OPm(k, t, 0); };
+  std::vector<double> ffac, fas1, fas2, fas3;  // [site][k 0..3]
+  oq_momentum_factors(g->n, io, ffac, fas1, fas2, fas3);
+  auto F = [&](const std::vector<double>& f, int site, int k) { return f[(size_t)site * 4 + k]; };
 
   for (int t = 0; t < L.nt; ++t)
     for (int z = 0; z < L.nz; ++z)
@@ -240,15 +258,34 @@ extern "C" void oq_twaverage_level0(const oq_geom* g, const double* be, const do
                 OP(9, t) = OP(9, t) + j3i_h + j3i_l;
                 OP(10, t) += psur;
                 OP(11, t) += psui;
+                for (int ix = 1; ix < 5; ++ix) {
+                  const int k = ix - 1;
+                  const double ff = F(ffac, h, k);
+                  OPm(0, t, ix) += rhor_h * ff;
+                  OPm(0, tm1, ix) += rhor_l * F(ffac, lt, k);
+                  OPm(1, t, ix) += rhoi_h * ff;
+                  OPm(1, tm1, ix) += rhoi_l * F(ffac, lt, k);
+                  OPm(2, t, ix) += psir * ff;
+                  OPm(3, t, ix) += psii * ff;
+                  OPm(4, t, ix) = OPm(4, t, ix) + j1i_h * F(fas3, h, k) + j1i_l * F(fas3, lx, k);
+                  OPm(5, t, ix) = OPm(5, t, ix) + j2i_h * F(fas1, h, k) + j2i_l * F(fas1, ly, k);
+                  OPm(6, t, ix) = OPm(6, t, ix) + j3i_h * F(fas2, h, k) + j3i_l * F(fas2, lz, k);
+                  OPm(7, t, ix) = OPm(7, t, ix) + j1i_h * F(fas2, h, k) + j1i_l * F(fas2, lx, k);
+                  OPm(8, t, ix) = OPm(8, t, ix) + j2i_h * F(fas3, h, k) + j2i_l * F(fas3, ly, k);
+                  OPm(9, t, ix) = OPm(9, t, ix) + j3i_h * F(fas1, h, k) + j3i_l * F(fas1, lz, k);
+                  OPm(10, t, ix) += psur * ff;
+                  OPm(11, t, ix) += psui * ff;
+                }
               }
             }
         }
   for (int iop = 0; iop < 6; ++iop) {
     const double f = (iop == 1 || iop == 5) ? 1.0 : kappa;  // ops 2 and 6 unscaled
-    for (int t = 0; t < L.nt; ++t)
-      for (int ri = 0; ri < 2; ++ri) {
-        const double v = OP(2 * iop + ri, t);
-        J[((size_t)iop * L.nt + t) * 2 + ri] = f == 1.0 ? v : f * v;
-      }
+    for (int im = 0; im < nmom; ++im)
+      for (int t = 0; t < L.nt; ++t)
+        for (int ri = 0; ri < 2; ++ri) {
+          const double v = OPm(2 * iop + ri, t, im);
+          J[(((size_t)iop * nmom + im) * L.nt + t) * 2 + ri] = f == 1.0 ? v : f * v;
+        }
   }
 }

@@ -1,6 +1,7 @@
 // Internal helpers of the CPU oracle (test infrastructure only; see oracle.h).
 #pragma once
 #include <cstddef>
+#include <cmath>
 #include <vector>
 
 #include "oracle.h"
@@ -93,3 +94,44 @@ void hdbletm(const oq_geom* g, double* he, const double* u, double* ge, int idag
 double vecdot_re(const oq_geom* g, const double* a, const double* b, double* im);
 double twonorm_c(const double* x, int n);
 }  // namespace oq
+
+// Momentum factors of the loop operators (Q/vevbleft.f90:955-985 and twAverage's copy):
+// per lexicographic site (t outermost) and k = 0..3 (imom 2..5), origin io (1-based).
+inline void oq_momentum_factors(const int n[4], const int io[3], std::vector<double>& ffac,
+                                std::vector<double>& fas1, std::vector<double>& fas2,
+                                std::vector<double>& fas3) {
+  const int nx = n[0], ny = n[1], nz = n[2], nt = n[3];
+  const size_t V = (size_t)nx * ny * nz * nt;
+  ffac.assign(V * 4, 0.0);
+  fas1.assign(V * 4, 0.0);
+  fas2.assign(V * 4, 0.0);
+  fas3.assign(V * 4, 0.0);
+  const double p1 = 8.0 * std::atan(1.0) / nx, p2 = 8.0 * std::atan(1.0) / ny, p3 = 8.0 * std::atan(1.0) / nz;
+  for (int t = 0; t < nt; ++t)
+    for (int z = 0; z < nz; ++z) {
+      const double dz = (double)(z + 1 - io[2]) * p3;
+      for (int y = 0; y < ny; ++y) {
+        const double dy = (double)(y + 1 - io[1]) * p2;
+        for (int x = 0; x < nx; ++x) {
+          const double dx = (double)(x + 1 - io[0]) * p1;
+          const size_t s = (size_t)(x + nx * (y + ny * (z + (size_t)nz * t))) * 4;
+          ffac[s + 0] = (std::cos(dx) + std::cos(dy) + std::cos(dz)) / 3.0;
+          fas1[s + 0] = std::sin(dx);
+          fas2[s + 0] = std::sin(dy);
+          fas3[s + 0] = std::sin(dz);
+          ffac[s + 1] = (std::cos(dx) * std::cos(dy) + std::cos(dx) * std::cos(dz) + std::cos(dy) * std::cos(dz)) / 3.0;
+          fas1[s + 1] = std::sin(dx) * (std::cos(dy) + std::cos(dz)) / 2.0;
+          fas2[s + 1] = std::sin(dy) * (std::cos(dx) + std::cos(dz)) / 2.0;
+          fas3[s + 1] = std::sin(dz) * (std::cos(dx) + std::cos(dy)) / 2.0;
+          ffac[s + 2] = std::cos(dx) * std::cos(dy) * std::cos(dz);
+          fas1[s + 2] = std::sin(dx) * std::cos(dy) * std::cos(dz);
+          fas2[s + 2] = std::sin(dy) * std::cos(dx) * std::cos(dz);
+          fas3[s + 2] = std::sin(dz) * std::cos(dx) * std::cos(dy);
+          ffac[s + 3] = (std::cos(2.0 * dx) + std::cos(2.0 * dy) + std::cos(2.0 * dz)) / 3.0;
+          fas1[s + 3] = std::sin(2.0 * dx);
+          fas2[s + 3] = std::sin(2.0 * dy);
+          fas3[s + 3] = std::sin(2.0 * dz);
+        }
+      }
+    }
+}

@@ -80,3 +80,73 @@ def test_level0_uses_only_the_real_part_of_the_noise():
     bo[..., 1::2] = -3.0
     J2 = ol.twaverage_level0(be, bo, xe, xo, 0.15)
     assert np.array_equal(J1, J2)
+
+
+def closed_form_mom(links, eta, x, kappa, delta, dobndry, io, nmom):
+    """The same per-site values with twAverage's momentum projections (:4434-4503):
+    imom 2..5 weight rho, psibar psi and psibar gamma5 psi by ffac(y) and take
+    (Im J1 fas3, Im J2 fas1), (Im J3 fas2, Im J1 fas2), (Im J2 fas3, Im J3 fas1) as the
+    (real, imaginary) slots of operators 3, 4, 5, each factor at the site y the value
+    sits on."""
+    import vevref
+
+    J5 = 1j * GAMMA5
+    sp = lambda M, v: np.einsum("st,...ta->...sa", M, v)  # noqa: E731
+    xp = x - np.cos(delta) * (np.cos(delta) * eta - np.sin(delta) * sp(J5, eta))
+    nt, nz, ny, nx = x.shape[:4]
+    axes = {0: 3, 1: 2, 2: 1, 3: 0}
+    site = {}
+    for mu in range(4):
+        U = links[mu]
+        Udx = np.einsum("...ba,...sb->...sa", np.conj(U), xp)
+        Ux = np.einsum("...ab,...sb->...sa", U, np.roll(xp, -1, axis=axes[mu]))
+        a = np.einsum("...sa,...sa->...", np.roll(eta, -1, axis=axes[mu]), sp(np.eye(4) + GAMMA[mu], Udx))
+        b = np.einsum("...sa,...sa->...", eta, sp(np.eye(4) - GAMMA[mu], Ux))
+        val = kappa * (a - b)
+        if mu == 3 and dobndry == 1:
+            val[-1] = 0.0
+        site[mu] = val
+    psi = np.einsum("...sa,...sa->...", eta, xp)
+    psu = np.einsum("...sa,...sa->...", eta, sp(GAMMA5, xp))
+    mf = vevref.momentum_factors((nx, ny, nz, nt), io)
+    fac = np.zeros((4, 5, nz, ny, nx))  # (ffac, fas1, fas2, fas3), k
+    for z in range(nz):
+        for y in range(ny):
+            for xx in range(nx):
+                f = mf(xx, y, z)
+                for k in range(1, 5):
+                    for a_ in range(4):
+                        fac[a_, k, z, y, xx] = f[a_][k]
+    out = np.zeros((6, nmom, nt), complex)
+    S = lambda v, w=1.0: (v * w).sum(axis=(1, 2, 3))  # noqa: E731
+    out[:, 0] = [S(site[3]), S(psi), S(site[0]), S(site[1]), S(site[2]), S(psu)]
+    for k in range(1, nmom):
+        ff, f1, f2, f3 = fac[0, k], fac[1, k], fac[2, k], fac[3, k]
+        out[0, k] = S(site[3], ff)
+        out[1, k] = S(psi, ff)
+        out[2, k] = S(site[0].imag, f3) + 1j * S(site[1].imag, f1)
+        out[3, k] = S(site[2].imag, f2) + 1j * S(site[0].imag, f2)
+        out[4, k] = S(site[1].imag, f3) + 1j * S(site[2].imag, f1)
+        out[5, k] = S(psu, ff)
+    return out
+
+
+@pytest.mark.parametrize("delta,dobndry,io", [(0.0, 0, (1, 1, 1)), (0.37, 1, (3, 2, 4))])
+def test_momentum_traces_closed_form(delta, dobndry, io):
+    dims = (4, 4, 4, 8)
+    ol = oracle.OracleLattice(*dims, bc=BC)
+    links, u = golden_gauge(dims, ol.ntotal, seed=35, eps=0.6)
+    ol.set_gauge(u)
+    oracle.initlagfib(0, 17)
+    be, bo = ol.z4source()
+    xe = random_half(ol.ntotal, ol.nvhalf, 52)
+    xo = random_half(ol.ntotal, ol.nvhalf, 53)
+    J = ol.twaverage(be, bo, xe, xo, 0.1565, delta, io=io, dobndry=dobndry, nmom=5)
+    noise = half_to_lex(be, dims, 1) + half_to_lex(bo, dims, 2)
+    x = half_to_lex(xe, dims, 1) + half_to_lex(xo, dims, 2)
+    want = closed_form_mom(links, noise.real, x, 0.1565, delta, dobndry, io, 5)
+    got = J[..., 0] + 1j * J[..., 1]
+    assert np.abs(got - want).max() < 1e-12 * np.abs(want).max()
+    assert np.abs(want[:, 1:]).max() > 0
+    J0 = ol.twaverage_level0(be, bo, xe, xo, 0.1565, delta, dobndry)
+    assert np.array_equal(J[:, 0], J0)

@@ -5,6 +5,8 @@
     python -m baylorlqcd_b200.probe solve [--dims 16,16,16,32] [--nrhs 12] [--precision 32]
                                           [--kappa 0.1565] [--sweeps 500] [--gauge-cache FILE]
 
+    python -m baylorlqcd_b200.probe twvev [--dims 16,16,16,16] [--nsub 6] [--reps 3]
+
 ``hop`` times one hopping-kernel shape (qq_bench_hsingle: random fields, L2 flushed
 between launches unless --no-flush) and prints its time and algorithmic bandwidth.
 
@@ -72,6 +74,25 @@ def run_solve(a) -> None:
     lat.close()
 
 
+def run_twvev(a):
+    """twvev on a short heatbath configuration: one untimed call, then --reps timed calls
+    (wall clock around the whole entry point, host program build included)."""
+    import time
+
+    import baylorlqcd_b200 as qq
+
+    dims = _dims(a.dims)
+    lat = qq.Lattice(*dims, bc=(1, 1, 1, -1))
+    lat.heatbath(6.0, 5, seed=3)
+    lat.twvev(0.156, delta=0.2, nsub=a.nsub)
+    for _ in range(a.reps):
+        t0 = time.perf_counter()
+        J = lat.twvev(0.156, delta=0.2, nsub=a.nsub)
+        print("twvev", dims, "nsub", a.nsub, "seconds %.4f" % (time.perf_counter() - t0),
+              "psibar psi level 4, t = 1: %.10e" % J[1, 0, 3, 0, 0], flush=True)
+    lat.close()
+
+
 def main(argv=None) -> int:
     p = argparse.ArgumentParser(prog="python -m baylorlqcd_b200.probe")
     sub = p.add_subparsers(dest="cmd", required=True)
@@ -89,8 +110,12 @@ def main(argv=None) -> int:
     s.add_argument("--kappa", type=float, default=0.1565)
     s.add_argument("--sweeps", type=int, default=500)
     s.add_argument("--gauge-cache", default=None)
+    v = sub.add_parser("twvev")
+    v.add_argument("--dims", default="16,16,16,16")
+    v.add_argument("--nsub", type=int, default=6)
+    v.add_argument("--reps", type=int, default=3)
     a = p.parse_args(argv)
-    (run_hop if a.cmd == "hop" else run_solve)(a)
+    {"hop": run_hop, "solve": run_solve, "twvev": run_twvev}[a.cmd](a)
     return 0
 
 

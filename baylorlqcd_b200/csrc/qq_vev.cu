@@ -55,7 +55,6 @@ struct VevArgs {
   int vh;
   const void* gauge;
   const char4* off;       // slot offsets of all levels
-  const int* row;         // per level 1..6: ns[n] + 1 CSR pointers
   const uint32_t* edge;   // src slot | right << 10 | mu << 11 | multiplicity << 13 | link slot << 21
   const int* lpk;         // link slots: offset x | y << 7 | z << 14 | t << 21 | mu << 28
   const double* mfac;     // [nx ny nz][k 0..3][ffac, fas1, fas2, fas3]
@@ -63,20 +62,28 @@ struct VevArgs {
   const int* meta;        // per-level tables, VevMeta layout
   const double* xk;       // (kappa cos(delta))^n, n = 0..6
   int sacc, tacc, qbase;  // slot bases of S[2][9], T[2] and Q within a warp's region
-  int nlink, wbytes, nwarp;  // link slots; bytes of a warp's region; warps per block
+  const uint32_t* item;   // work items: target slot | first edge << 10 | edge count << 26
+  const int* titem;       // per level: ns[n] + 1 item offsets (targets' item ranges)
+  int nlink, gbytes, ngroup;  // link slots; bytes of a group's region; groups per block
+  int scr;                // slot base of the work-item scratch within a group's region
   int nlev;               // 4 (nsub = 4) or 6
   int twist, fixbc;
   double cosd, sind, r;
   int sps, spc, chunks;   // sites per slice, sites per block, blocks per slice
 };
 constexpr int kLinkStride = 10;  // double2 per cached link (9 used)
-constexpr int kVevMaxWarps = 6;  // warps per block (a divisor of the 12 tasks of a site)
+constexpr int kVevGroupLanes = 128;  // threads running one task
+constexpr int kVevMaxGroups = 3;     // tasks in flight per block (a divisor of the 12 of a site)
 
 // Per-level integer tables in device memory (read with runtime level indices):
 // base[7] | ns[7] | rbase[7] | buf[7] | fr9[3][9] (slots of x, x-x, x+x, x-y, x+y, x-z,
 // x+z, x-t, x+t in levels 1, 3, 5) | fr0[3] (slot of x in levels 2, 4, 6) | flk[8]
-// (link slots of U_mu(x) and U_mu(x - mu), mu = 0..3).
-enum VevMeta { kMBase = 0, kMNs = 7, kMRbase = 14, kMBuf = 21, kMFr9 = 28, kMFr0 = 55, kMFlk = 58, kMSize = 66 };
+// (link slots of U_mu(x) and U_mu(x - mu), mu = 0..3) | ibase[7], nitems[7] (work items
+// of each level) | tbase[7] (offset of each level's item ranges in titem).
+enum VevMeta {
+  kMBase = 0, kMNs = 7, kMRbase = 14, kMBuf = 21, kMFr9 = 28, kMFr0 = 55, kMFlk = 58,
+  kMIbase = 66, kMNitems = 73, kMTbase = 80, kMSize = 87
+};
 
 __device__ inline cplx<double> ld(const double2* p) {
   const double2 v = *p;
@@ -122,16 +129,46 @@ __device__ inline void su3_apply(const Su3<double>& u, bool dag, const cplx<doub
   }
 }
 
+// One hop of a work item: y0 = W h0, y1 = W h1 with W = U (hop to -mu) or U^+ (hop to
+// +mu), the link read element by element from the block's link cache.
+__device__ inline void su3_pair(const double2* lk, bool dag, const cplx<double>* h0, const cplx<double>* h1,
+                                cplx<double>* y0, cplx<double>* y1) {
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    y0[a] = {0.0, 0.0};
+    y1[a] = {0.0, 0.0};
+  }
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int b = 0; b < 3; ++b) {
+      const double2 e = lk[3 * a + b];  // U[a][b]
+      const cplx<double> u{e.x, e.y};
+      if (dag) {  // (U^+)[b][a] = conj(U[a][b]) acts on h[a] into y[b]
+        y0[b] = cadd(y0[b], cmulconj(u, h0[a]));
+        y1[b] = cadd(y1[b], cmulconj(u, h1[a]));
+      } else {
+        y0[a] = cadd(y0[a], cmul(u, h0[b]));
+        y1[a] = cadd(y1[a], cmul(u, h1[b]));
+      }
+    }
+}
+
+__device__ inline void group_sync(int grp) {
+  asm volatile("bar.sync %0, %1;" ::"r"(1 + grp), "r"(kVevGroupLanes) : "memory");
+}
+
 template <int RECON>
-__global__ void __launch_bounds__(kVevMaxWarps * 32) vev_sites_kernel(VevArgs A) {
+__global__ void __launch_bounds__(kVevMaxGroups * kVevGroupLanes) vev_sites_kernel(VevArgs A) {
   extern __shared__ double2 smem[];
   const double2* lk = smem;  // link cache [nlink][kLinkStride]
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  double2* sm = smem + (size_t)A.nlink * kLinkStride + (size_t)warp * (A.wbytes / sizeof(double2));
+  const int grp = threadIdx.x / kVevGroupLanes, lane = threadIdx.x % kVevGroupLanes;
+  double2* sm = smem + (size_t)A.nlink * kLinkStride + (size_t)grp * (A.gbytes / sizeof(double2));
+  double2* scr = sm + (size_t)A.scr * kVevStride;  // work-item partial sums
   const int slice = blockIdx.x / A.chunks, chunk = blockIdx.x % A.chunks;
   const int sp0 = chunk * A.spc, sp1 = min(A.sps, sp0 + A.spc);
   const double r = A.r;
-  double accE[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  double accE[2] = {0.0, 0.0};
   for (int sp = sp0; sp < sp1; ++sp) {
     const int x[4] = {sp % A.n[0], (sp / A.n[0]) % A.n[1], sp / (A.n[0] * A.n[1]), slice};
     __syncthreads();  // the previous site's links are no longer read
@@ -150,7 +187,7 @@ __global__ void __launch_bounds__(kVevMaxWarps * 32) vev_sites_kernel(VevArgs A)
         smem[(size_t)l * kLinkStride + qd] = make_double2(u.e[qd / 3][qd % 3].re, u.e[qd / 3][qd % 3].im);
     }
     __syncthreads();
-    for (int task = warp; task < 12; task += A.nwarp) {
+    for (int task = grp; task < 12; task += A.ngroup) {
       const int id = task / 3, ic = task % 3;
       // level 0: R (cos(delta) e(x, ic, id))
       if (lane < 12) {
@@ -162,70 +199,68 @@ __global__ void __launch_bounds__(kVevMaxWarps * 32) vev_sites_kernel(VevArgs A)
         }
         sm[(size_t)__ldg(A.meta + kMBuf) * kVevStride + lane] = make_double2(v, 0.0);
       }
-      __syncwarp();
+      group_sync(grp);
       for (int n = 1; n <= A.nlev; ++n) {
         const double2* src = sm + (size_t)__ldg(A.meta + kMBuf + n - 1) * kVevStride;
         double2* dst = sm + (size_t)__ldg(A.meta + kMBuf + n) * kVevStride;
-        const int* row = A.row + __ldg(A.meta + kMRbase + n);
-        const int ns = __ldg(A.meta + kMNs + n), bn = __ldg(A.meta + kMBase + n),
-                  bp = __ldg(A.meta + kMBase + n - 1);
-        const double xkn = __ldg(A.xk + n);
-        for (int j = lane; j < ns; j += 32) {
+        const int ns = __ldg(A.meta + kMNs + n), bp = __ldg(A.meta + kMBase + n - 1);
+        const int ni = __ldg(A.meta + kMNitems + n);
+        // work items: up to K hops into one target, partial sum to the scratch slot
+        if (lane < ni) {
+          const uint32_t it = __ldg(A.item + __ldg(A.meta + kMIbase + n) + lane);
+          const int e0 = (it >> 10) & 0xFFFF, e1 = e0 + (int)(it >> 26);
           cplx<double> acc[4][3];
-  #pragma unroll
+#pragma unroll
           for (int d = 0; d < 4; ++d)
-  #pragma unroll
+#pragma unroll
             for (int c = 0; c < 3; ++c) acc[d][c] = {0.0, 0.0};
-          for (int k = row[j]; k < row[j + 1]; ++k) {
-            const uint32_t e = A.edge[k];
+          for (int k = e0; k < e1; ++k) {
+            const uint32_t e = __ldg(A.edge + k);
             const int sj = e & 1023, mu = (e >> 11) & 3;
             const bool right = (e >> 10) & 1;
-            const double mult = (double)((e >> 13) & 255);
             if (mu == 3 && A.fixbc) {
               const int st = x[3] + A.off[bp + sj].w;
               const int sct = st >= A.n[3] ? st - A.n[3] : st;
               if (right ? sct == A.n[3] - 1 : sct == 0) continue;
             }
-            Su3<double> u;
-            cached_link(lk, (int)(e >> 21), u);
+            const double mult = (double)((e >> 13) & 255);
             const double2* sv = src + (size_t)sj * kVevStride;
             const double sg = right ? 1.0 : -1.0, sr = sg * r;
             cplx<double> h0[3], h1[3], y0[3], y1[3];
             if (mu == 0) {  // (gamma_1 v)_d = v_{3-d}
-  #pragma unroll
+#pragma unroll
               for (int c = 0; c < 3; ++c) {
                 h0[c] = cadd(cscale(r, ld(sv + c)), cscale(sg, ld(sv + 9 + c)));
                 h1[c] = cadd(cscale(r, ld(sv + 3 + c)), cscale(sg, ld(sv + 6 + c)));
               }
             } else if (mu == 1) {  // gamma_2 v = (-i v3, i v2, -i v1, i v0)
-  #pragma unroll
+#pragma unroll
               for (int c = 0; c < 3; ++c) {
                 h0[c] = cadd(cscale(r, ld(sv + c)), cmuli(-sg, ld(sv + 9 + c)));
                 h1[c] = cadd(cscale(r, ld(sv + 3 + c)), cmuli(sg, ld(sv + 6 + c)));
               }
             } else if (mu == 2) {  // gamma_3 v = (v2, -v3, v0, -v1)
-  #pragma unroll
+#pragma unroll
               for (int c = 0; c < 3; ++c) {
                 h0[c] = cadd(cscale(r, ld(sv + c)), cscale(sg, ld(sv + 6 + c)));
                 h1[c] = csub(cscale(r, ld(sv + 3 + c)), cscale(sg, ld(sv + 9 + c)));
               }
             } else {  // gamma_4 = diag(1, 1, -1, -1): (r + sg gamma_4) keeps spins 0,1 (r = sg) or 2,3
               const int o = (r == sg) ? 0 : 6;
-  #pragma unroll
+#pragma unroll
               for (int c = 0; c < 3; ++c) {
                 h0[c] = cscale(2.0 * r, ld(sv + o + c));
                 h1[c] = cscale(2.0 * r, ld(sv + o + 3 + c));
               }
             }
-            su3_apply(u, right, h0, y0);
-            su3_apply(u, right, h1, y1);
+            su3_pair(lk + (size_t)(e >> 21) * kLinkStride, right, h0, h1, y0, y1);
             if (mult != 1.0)
-  #pragma unroll
+#pragma unroll
               for (int c = 0; c < 3; ++c) {
                 y0[c] = cscale(mult, y0[c]);
                 y1[c] = cscale(mult, y1[c]);
               }
-  #pragma unroll
+#pragma unroll
             for (int c = 0; c < 3; ++c) {
               if (mu == 3) {
                 if (r == sg) {
@@ -251,9 +286,31 @@ __global__ void __launch_bounds__(kVevMaxWarps * 32) vev_sites_kernel(VevArgs A)
               }
             }
           }
-          // store R acc
-          double2* dv = dst + (size_t)j * kVevStride;
-  #pragma unroll
+          double2* pv = scr + (size_t)lane * kVevStride;
+#pragma unroll
+          for (int d = 0; d < 4; ++d)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) st(pv + 3 * d + c, acc[d][c]);
+        }
+        group_sync(grp);
+        // combine: each target adds its items in order, then R
+        if (lane < ns) {
+          const int* tr = A.titem + __ldg(A.meta + kMTbase + n);
+          const int i0 = __ldg(tr + lane), i1 = __ldg(tr + lane + 1);
+          cplx<double> acc[4][3];
+#pragma unroll
+          for (int d = 0; d < 4; ++d)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) acc[d][c] = {0.0, 0.0};
+          for (int i = i0; i < i1; ++i) {
+            const double2* pv = scr + (size_t)i * kVevStride;
+#pragma unroll
+            for (int d = 0; d < 4; ++d)
+#pragma unroll
+              for (int c = 0; c < 3; ++c) acc[d][c] = cadd(acc[d][c], ld(pv + 3 * d + c));
+          }
+          double2* dv = dst + (size_t)lane * kVevStride;
+#pragma unroll
           for (int c = 0; c < 3; ++c) {
             st(dv + c, csub(cscale(A.cosd, acc[0][c]), cscale(A.sind, acc[2][c])));
             st(dv + 3 + c, csub(cscale(A.cosd, acc[1][c]), cscale(A.sind, acc[3][c])));
@@ -261,20 +318,21 @@ __global__ void __launch_bounds__(kVevMaxWarps * 32) vev_sites_kernel(VevArgs A)
             st(dv + 9 + c, cadd(cscale(A.cosd, acc[3][c]), cscale(A.sind, acc[1][c])));
           }
         }
-        __syncwarp();
+        group_sync(grp);
         // fold the read sites into S (odd orders) and T (even orders)
+        const double xkn = __ldg(A.xk + n);
         if (n & 1) {
           const int which = n >> 1;  // 0, 1, 2 for orders 1, 3, 5
           const bool use = n == 5 || n == 3 || A.twist;
-          if (use)
-            for (int i = lane; i < 9 * 12; i += 32) {
-              const int site = i / 12, comp = i % 12;
-              const int isb = n == 5 ? 1 : 0;
-              double2* s = sm + (size_t)(A.sacc + isb * 9 + site) * kVevStride + comp;
-              const cplx<double> v = cscale(xkn, ld(dst + (size_t)__ldg(A.meta + kMFr9 + which * 9 + site) * kVevStride + comp));
-              const bool first = n == 5 || n == 1 || !A.twist;
-              st(s, first ? v : cadd(ld(s), v));
-            }
+          if (use && lane < 9 * 12) {
+            const int site = lane / 12, comp = lane % 12;
+            const int isb = n == 5 ? 1 : 0;
+            double2* s = sm + (size_t)(A.sacc + isb * 9 + site) * kVevStride + comp;
+            const cplx<double> v =
+                cscale(xkn, ld(dst + (size_t)__ldg(A.meta + kMFr9 + which * 9 + site) * kVevStride + comp));
+            const bool first = n == 5 || n == 1 || !A.twist;
+            st(s, first ? v : cadd(ld(s), v));
+          }
         } else {
           const int which = (n >> 1) - 1;  // 0, 1, 2 for orders 2, 4, 6
           const bool use = n == 6 || n == 4 || A.twist;
@@ -286,7 +344,7 @@ __global__ void __launch_bounds__(kVevMaxWarps * 32) vev_sites_kernel(VevArgs A)
             st(s, first ? v : cadd(ld(s), v));
           }
         }
-        __syncwarp();
+        group_sync(grp);
       }
       // closed-form operators: lane = isb * 10 + (rho(x), rho(x-t), J1(x), J1(x-x), J2(x),
       // J2(x-y), J3(x), J3(x-z), psibar psi, psibar gamma5 psi)
@@ -337,7 +395,7 @@ __global__ void __launch_bounds__(kVevMaxWarps * 32) vev_sites_kernel(VevArgs A)
         }
         st(sm + A.qbase + lane, val);
       }
-      __syncwarp();
+      group_sync(grp);
       // this task's share of the lane's sums
       {
         const double2* Q = sm + A.qbase;
@@ -345,9 +403,9 @@ __global__ void __launch_bounds__(kVevMaxWarps * 32) vev_sites_kernel(VevArgs A)
         const int lx = (x[0] == 0 ? A.n[0] - 1 : x[0] - 1) + A.n[0] * (x[1] + A.n[1] * x[2]);
         const int ly = x[0] + A.n[0] * ((x[1] == 0 ? A.n[1] - 1 : x[1] - 1) + A.n[1] * x[2]);
         const int lz = x[0] + A.n[0] * (x[1] + A.n[1] * (x[2] == 0 ? A.n[2] - 1 : x[2] - 1));
-  #pragma unroll
-        for (int i = 0; i < 5; ++i) {
-          const int e = lane + 32 * i;
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+          const int e = lane + kVevGroupLanes * i;
           if (e >= kVevEntries) break;
           const int isb = e / 70, rem = e % 70, km = rem / 14, j = rem % 14;
           if (isb == 1 && A.nlev != 6) continue;
@@ -394,13 +452,13 @@ __global__ void __launch_bounds__(kVevMaxWarps * 32) vev_sites_kernel(VevArgs A)
           accE[i] += v;
         }
       }
-      __syncwarp();
+      group_sync(grp);
     }
   }
 #pragma unroll
-  for (int i = 0; i < 5; ++i) {
-    const int e = lane + 32 * i;
-    if (e < kVevEntries) A.part[((size_t)blockIdx.x * A.nwarp + warp) * kVevEntries + e] = accE[i];
+  for (int i = 0; i < 2; ++i) {
+    const int e = lane + kVevGroupLanes * i;
+    if (e < kVevEntries) A.part[((size_t)blockIdx.x * A.ngroup + grp) * kVevEntries + e] = accE[i];
   }
 }
 
@@ -432,6 +490,9 @@ struct VevProgram {
   std::vector<int> row;
   std::vector<uint32_t> edge;
   std::vector<int> lpk;  // link slots
+  std::vector<uint32_t> item;  // work items of all levels
+  std::vector<int> titem;      // per level: item offsets of its targets
+  int ibase[7] = {0}, nitems[7] = {0}, tbase[7] = {0}, max_items = 0;
   int base[7], ns[7], rbase[7];
   int fr9[3][9], fr0[3], flk[8];
   int max_odd = 0, max_even = 0;
@@ -554,6 +615,32 @@ int build_vev_program(const int* dims, VevProgram& P) {
       k += (int)in[j].size();
     }
     P.row.push_back(k);
+    // work items: the smallest K whose items (each <= K hops into one target) fit the
+    // lanes of a group
+    if (P.ns[n] > kVevGroupLanes) return set_error(QQ_BAD_ARG, "twvev program: a level has too many slots");
+    int K = 1;
+    for (;; ++K) {
+      int cnt = 0;
+      for (int j = 0; j < P.ns[n]; ++j) cnt += ((int)in[j].size() + K - 1) / K;
+      if (cnt <= kVevGroupLanes) break;
+      if (K > 63) return set_error(QQ_BAD_ARG, "twvev program: work items do not fit");
+    }
+    P.ibase[n] = (int)P.item.size();
+    P.tbase[n] = (int)P.titem.size();
+    int e0 = P.row[P.rbase[n]];
+    for (int j = 0; j < P.ns[n]; ++j) {
+      P.titem.push_back((int)P.item.size() - P.ibase[n]);
+      const int ne = (int)in[j].size();
+      for (int q = 0; q < ne; q += K) {
+        const int c = std::min(K, ne - q);
+        if (e0 + q > 0xFFFF) return set_error(QQ_BAD_ARG, "twvev program: too many edges");
+        P.item.push_back((uint32_t)j | (uint32_t)(e0 + q) << 10 | (uint32_t)c << 26);
+      }
+      e0 += ne;
+    }
+    P.titem.push_back((int)P.item.size() - P.ibase[n]);
+    P.nitems[n] = (int)P.item.size() - P.ibase[n];
+    P.max_items = std::max(P.max_items, P.nitems[n]);
   }
   for (int w = 0; w < 3; ++w) {
     for (int s = 0; s < 9; ++s) P.fr9[w][s] = idx[2 * w + 1].at(wrap(nine[s]));
@@ -590,33 +677,34 @@ extern "C" int qq_twvev(qq_ctx* c, double kappa, double delta, const int io[3], 
     // momentum factors (:955-985), at spatial sites
     std::vector<double> mf;
     momentum_table(c->g.n, io, mf);
-    // block shape: warps sharing one site's link cache, as many as shared memory holds
+    // block shape: groups of 128 threads, one task each, sharing one site's link cache
     int dev_smem = 0;
     QQ_CK(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device));
-    const int wslots = 1 + P.max_odd + P.max_even + 20;
-    const size_t wbytes = ((size_t)wslots * kVevStride + kVevQ) * sizeof(double2);
+    const int gslots = 1 + P.max_odd + P.max_even + 20 + P.max_items;
+    const size_t gbytes = ((size_t)gslots * kVevStride + kVevQ) * sizeof(double2);
     const size_t lbytes = P.lpk.size() * kLinkStride * sizeof(double2);
-    int nwarp = 0;
-    for (int w : {kVevMaxWarps, 4, 3, 2, 1})
-      if (lbytes + w * wbytes <= (size_t)dev_smem) {
-        nwarp = w;
+    int ngroup = 0;
+    for (int w : {kVevMaxGroups, 2, 1})
+      if (lbytes + w * gbytes <= (size_t)dev_smem) {
+        ngroup = w;
         break;
       }
-    if (nwarp == 0) return set_error(QQ_BAD_ARG, "twvev: shared memory plan too large");
-    const size_t smem = lbytes + nwarp * wbytes;
+    if (ngroup == 0) return set_error(QQ_BAD_ARG, "twvev: shared memory plan too large");
+    const size_t smem = lbytes + ngroup * gbytes;
     const int sps = nxyz;
     int chunks = std::max(1, (8 * 148 + nt - 1) / nt);
     chunks = std::min(chunks, sps);
     const int spc = (sps + chunks - 1) / chunks;
     chunks = (sps + spc - 1) / spc;
     const int nblk = nt * chunks;
-    const size_t b_off = P.off.size() * sizeof(char4), b_row = P.row.size() * sizeof(int),
+    const size_t b_off = P.off.size() * sizeof(char4),
                  b_edge = P.edge.size() * sizeof(uint32_t), b_mf = mf.size() * sizeof(double),
-                 b_part = (size_t)nblk * nwarp * kVevEntries * sizeof(double), b_lpk = P.lpk.size() * sizeof(int);
+                 b_part = (size_t)nblk * ngroup * kVevEntries * sizeof(double), b_lpk = P.lpk.size() * sizeof(int),
+                 b_item = P.item.size() * sizeof(uint32_t), b_titem = P.titem.size() * sizeof(int);
     auto al = [](size_t b) { return (b + 255) / 256 * 256; };
     DevBuf tab;
-    QQ_CK(tab.alloc(al(b_off) + al(b_row) + al(b_edge) + al(b_mf) + al(b_part) + al(kMSize * sizeof(int)) +
-                    al(7 * sizeof(double)) + al(b_lpk)));
+    QQ_CK(tab.alloc(al(b_off) + al(b_edge) + al(b_mf) + al(b_part) + al(kMSize * sizeof(int)) +
+                    al(7 * sizeof(double)) + al(b_lpk) + al(b_item) + al(b_titem)));
     char* p = (char*)tab.p;
     VevArgs A{};
     for (int d = 0; d < 4; ++d) A.n[d] = c->g.n[d];
@@ -625,9 +713,6 @@ extern "C" int qq_twvev(qq_ctx* c, double kappa, double delta, const int io[3], 
     A.off = (const char4*)p;
     QQ_CK(cudaMemcpyAsync(p, P.off.data(), b_off, cudaMemcpyHostToDevice, c->st));
     p += al(b_off);
-    A.row = (const int*)p;
-    QQ_CK(cudaMemcpyAsync(p, P.row.data(), b_row, cudaMemcpyHostToDevice, c->st));
-    p += al(b_row);
     A.edge = (const uint32_t*)p;
     QQ_CK(cudaMemcpyAsync(p, P.edge.data(), b_edge, cudaMemcpyHostToDevice, c->st));
     p += al(b_edge);
@@ -643,6 +728,9 @@ extern "C" int qq_twvev(qq_ctx* c, double kappa, double delta, const int io[3], 
       meta[kMNs + n] = P.ns[n];
       meta[kMRbase + n] = n >= 1 ? P.rbase[n] : 0;
       meta[kMBuf + n] = n == 0 ? 0 : (n & 1 ? 1 : 1 + P.max_odd);
+      meta[kMIbase + n] = P.ibase[n];
+      meta[kMNitems + n] = P.nitems[n];
+      meta[kMTbase + n] = P.tbase[n];
     }
     std::memcpy(meta + kMFr9, P.fr9, sizeof(P.fr9));
     std::memcpy(meta + kMFr0, P.fr0, sizeof(P.fr0));
@@ -652,7 +740,8 @@ extern "C" int qq_twvev(qq_ctx* c, double kappa, double delta, const int io[3], 
     p += al(sizeof(meta));
     A.sacc = 1 + P.max_odd + P.max_even;
     A.tacc = A.sacc + 18;
-    A.qbase = (A.tacc + 2) * kVevStride;
+    A.scr = A.tacc + 2;
+    A.qbase = (A.scr + P.max_items) * kVevStride;
     A.nlev = nsub == 6 ? 6 : 4;
     A.twist = std::fabs(delta) > 1.e-12;
     A.fixbc = dobndry == 1;
@@ -668,24 +757,30 @@ extern "C" int qq_twvev(qq_ctx* c, double kappa, double delta, const int io[3], 
     p += al(sizeof(xk));
     A.lpk = (const int*)p;
     QQ_CK(cudaMemcpyAsync(p, P.lpk.data(), b_lpk, cudaMemcpyHostToDevice, c->st));
+    p += al(b_lpk);
+    A.item = (const uint32_t*)p;
+    QQ_CK(cudaMemcpyAsync(p, P.item.data(), b_item, cudaMemcpyHostToDevice, c->st));
+    p += al(b_item);
+    A.titem = (const int*)p;
+    QQ_CK(cudaMemcpyAsync(p, P.titem.data(), b_titem, cudaMemcpyHostToDevice, c->st));
     A.nlink = (int)P.lpk.size();
-    A.wbytes = (int)wbytes;
-    A.nwarp = nwarp;
+    A.gbytes = (int)gbytes;
+    A.ngroup = ngroup;
     A.sps = sps;
     A.spc = spc;
     A.chunks = chunks;
     count_launch();
     if (c->recon64 == 18) {
       QQ_CK(cudaFuncSetAttribute(vev_sites_kernel<18>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      vev_sites_kernel<18><<<nblk, 32 * nwarp, smem, c->st>>>(A);
+      vev_sites_kernel<18><<<nblk, kVevGroupLanes * ngroup, smem, c->st>>>(A);
     } else {
       QQ_CK(cudaFuncSetAttribute(vev_sites_kernel<12>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      vev_sites_kernel<12><<<nblk, 32 * nwarp, smem, c->st>>>(A);
+      vev_sites_kernel<12><<<nblk, kVevGroupLanes * ngroup, smem, c->st>>>(A);
     }
     QQ_CK(cudaGetLastError());
     const int nout = nt * 2 * nmom * 12;
     count_launch();
-    vev_reduce_kernel<<<(nout + 127) / 128, 128, 0, c->st>>>(A.part, chunks * nwarp, nt, A.nlev, nmom,
+    vev_reduce_kernel<<<(nout + 127) / 128, 128, 0, c->st>>>(A.part, chunks * ngroup, nt, A.nlev, nmom,
                                                              dJ.as<double>());
     QQ_CK(cudaGetLastError());
     QQ_CK(cudaMemcpyAsync(Jvev, dJ.p, sizeof(double) * nJ, cudaMemcpyDefault, c->st));

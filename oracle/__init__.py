@@ -74,6 +74,7 @@ def lib() -> C.CDLL:
             "oq_twvev_sites": ([P, DP, D, D, IP, I, I, I, IP, I, DP], None),
             "oq_set_kcyclim": ([I], None),
             "oq_coldstart": ([P, DP], None),
+            "oq_heatbath": ([P, DP, D, I, I, DP], None),
             "oq_aveplaq": ([P, DP], D),
         }
         for name, (args, res) in sig.items():
@@ -343,6 +344,14 @@ class OracleLattice:
         u = np.zeros(self.gauge_shape)
         lib().oq_coldstart(self._g, _dp(u))
         return u
+
+    def heatbath(self, u, beta, nsweeps, nhit=1):
+        """The reference's pseudo-heatbath on u (reference layout, updated in place),
+        drawing from the lagfib stream (call initlagfib first).  Returns the average
+        plaquette after each sweep."""
+        plaq = np.zeros(nsweeps)
+        lib().oq_heatbath(self._g, _dp(u), float(beta), int(nsweeps), int(nhit), _dp(plaq))
+        return plaq
 
     def aveplaq(self, u=None):
         u = self.u if u is None else u

@@ -154,6 +154,11 @@ void oq_twvev_sites(const oq_geom* g, const double* u, double kappa, double delt
 
 // ---- gauge field helpers ----
 void oq_coldstart(const oq_geom* g, double* u);
+// The reference's pseudo-heatbath for the Wilson plaquette action at beta (sweep
+// C/cfgsprops.f90:1973-2001, staple G/gaugetools.f90:39-345, phbup / su2up / sprd1
+// G/heatbath.f90:33-467), drawing from the lagfib stream; u in place.  plaq (nsweeps
+// entries, may be NULL) receives the average plaquette after each sweep.
+void oq_heatbath(const oq_geom* g, double* u, double beta, int nsweeps, int nhit, double* plaq);
 double oq_aveplaq(const oq_geom* g, const double* u);
 
 #ifdef __cplusplus

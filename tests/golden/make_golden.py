@@ -14,6 +14,10 @@ fixed numbers to meet.  Inputs:
 * level-0 loop traces (Q/vevbleft.f90 twAverage, nsub = 0) of the first Z(4) noise
   after a fermprop solve, and the noise average of three Z(4) noises solved with psc
   as the reference's twistdiscon loop does.
+* KAT-5: the oracle's restatement of the reference's pseudo-heatbath (G/heatbath.f90,
+  C/cfgsprops.f90 sweep) on 8x8x8x8 at beta = 6.0 from a cold start with lagfib seed
+  (0, 7): the plaquette after every sweep of 200 (a reproducible oracle number, not
+  a literature value).
 
 Usage: python tests/golden/make_golden.py   (rewrites golden.json)
 """
@@ -111,6 +115,13 @@ def main():
     J = Jsum / (3 * DIMS[0] * DIMS[1] * DIMS[2])
     out["discon_z4_psc3"] = {"kappa": 0.15, "nnoise": 3, "iseed": 21, "GMRES": [30, 10], "resmax": 1e-10,
                              "J": J.tolist()}
+    # KAT-5: the oracle heatbath, 8^4 at beta = 6.0, cold start, 200 sweeps
+    hb = oracle.OracleLattice(8, 8, 8, 8, bc=BC)
+    u = hb.coldstart()
+    oracle.initlagfib(0, 7)
+    plaq = hb.heatbath(u, 6.0, 200)
+    out["kat5_heatbath"] = {"dims": [8, 8, 8, 8], "beta": 6.0, "iseed": 7, "start": "cold",
+                            "plaquette": [float(v) for v in plaq]}
     (HERE / "golden.json").write_text(json.dumps(out, indent=1) + "\n")
     print("wrote", HERE / "golden.json")
 

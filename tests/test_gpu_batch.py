@@ -96,6 +96,27 @@ def test_batch_device_arrays(setup):
     assert interior_rel(xod.cpu().numpy(), xo_h, ol.nvhalf) < 1e-9
 
 
+def test_heatbath_matches_oracle_ensemble():
+    """KAT-5 against the GPU heatbath: the oracle's restatement of the reference's
+    pseudo-heatbath gives, on 8^4 at beta = 6.0 from a cold start, a plaquette that
+    averages 0.5943 over sweeps 101..200 (committed record).  The GPU heatbath draws from
+    another generator, so only the ensembles can agree: the mean final plaquette of 8
+    GPU streams after 200 sweeps must lie within 4 standard errors (GPU spread over the
+    streams and the record's spread over its sweeps) of the record's mean."""
+    import json
+    from pathlib import Path
+
+    import baylorlqcd_b200 as qq
+
+    rec = json.loads((Path(__file__).resolve().parent / "golden" / "golden.json").read_text())["kat5_heatbath"]
+    ref = np.array(rec["plaquette"][100:])
+    lat = qq.Lattice(8, 8, 8, 8)
+    got = np.array([lat.heatbath(6.0, 200, seed=100 + s)[1] for s in range(8)])
+    lat.close()
+    err = np.sqrt(got.var(ddof=1) / len(got) + ref.var(ddof=1) / 10)  # the record's sweeps are correlated
+    assert abs(got.mean() - ref.mean()) < 4 * err, (got.mean(), ref.mean(), err)
+
+
 def test_heatbath_plaquette(setup):
     """The GPU heatbath thermalises to the known beta = 6.0 plaquette (about 0.594)."""
     import baylorlqcd_b200 as qq

@@ -6,6 +6,8 @@
                                           [--kappa 0.1565] [--sweeps 500] [--gauge-cache FILE]
 
     python -m baylorlqcd_b200.probe twvev [--dims 16,16,16,16] [--nsub 6] [--reps 3]
+    python -m baylorlqcd_b200.probe discon [--dims 16,16,16,32] [--nnoise 24] [--kappa 0.1565]
+                                           [--mu 0.0] [--solver 1] [--nsub 6]
 
 ``hop`` times one hopping-kernel shape (qq_bench_hsingle: random fields, L2 flushed
 between launches unless --no-flush) and prints its time and algorithmic bandwidth.
@@ -93,6 +95,31 @@ def run_twvev(a):
     lat.close()
 
 
+def run_discon(a):
+    """twistdiscon (qq_twistdiscon) on a heatbath configuration: nnoise Z(4) noises,
+    subtraction levels, five momenta.  Prints wall seconds per noise (the twvev part
+    included) and the largest true residual of the solves."""
+    import time
+
+    import baylorlqcd_b200 as qq
+
+    dims = _dims(a.dims)
+    lat = qq.Lattice(*dims, bc=(1, 1, 1, -1))
+    lat.heatbath(6.0, a.sweeps, seed=3)
+    kw = dict(nsub=a.nsub, nmom=5, nop=6, delta=0.0, dobndry=0, solver=a.solver, m=60, k=20, precision=32,
+              rhs_block=12, tol=1e-10)
+    qq.initlagfib(0, 5)
+    lat.twistdiscon(4, min(a.nnoise, 12), (a.kappa, a.mu), **kw)  # warm-up (tuning, graph capture)
+    qq.initlagfib(0, 5)
+    t0 = time.perf_counter()
+    J, infos = lat.twistdiscon(4, a.nnoise, (a.kappa, a.mu), **kw)
+    dt = time.perf_counter() - t0
+    print("twistdiscon", dims, "solver", a.solver, "noises", a.nnoise, "seconds %.3f" % dt,
+          "per noise %.4f" % (dt / a.nnoise), "max true_rel %.2e" % max(i.true_rel for i in infos),
+          "psibar psi level 4, t = 1: %.8e" % J[1, 0, 3, 0, 0], flush=True)
+    lat.close()
+
+
 def main(argv=None) -> int:
     p = argparse.ArgumentParser(prog="python -m baylorlqcd_b200.probe")
     sub = p.add_subparsers(dest="cmd", required=True)
@@ -114,8 +141,16 @@ def main(argv=None) -> int:
     v.add_argument("--dims", default="16,16,16,16")
     v.add_argument("--nsub", type=int, default=6)
     v.add_argument("--reps", type=int, default=3)
+    d = sub.add_parser("discon")
+    d.add_argument("--dims", default="16,16,16,32")
+    d.add_argument("--nnoise", type=int, default=24)
+    d.add_argument("--kappa", type=float, default=0.1565)
+    d.add_argument("--mu", type=float, default=0.0)
+    d.add_argument("--solver", type=int, default=1)
+    d.add_argument("--nsub", type=int, default=6)
+    d.add_argument("--sweeps", type=int, default=200)
     a = p.parse_args(argv)
-    {"hop": run_hop, "solve": run_solve, "twvev": run_twvev}[a.cmd](a)
+    {"hop": run_hop, "solve": run_solve, "twvev": run_twvev, "discon": run_discon}[a.cmd](a)
     return 0
 
 

@@ -14,6 +14,7 @@
 #include <algorithm>
 #include <cstring>
 #include <functional>
+#include <thread>
 #include <vector>
 
 #include "qq_ctx.h"
@@ -28,10 +29,12 @@ int traces_mom(qq_ctx* c, const double* be, const double* bo, const double* xe, 
 namespace {
 
 // The noise loop: per noise (generator order), draw, solve, take the kappa-scaled traces
-// J(2, nt, nmom, 6) and hand them to add().
+// J(2, nt, nmom, 6) and hand them to add().  pre (may be empty) runs on the calling
+// thread while the first block of noises is drawn; it must not draw random numbers.
 int discon_loop(qq_ctx* c, int noise_kind, int nnoise, const double kappa[2], const qq_method* method,
                 double delta, const int io[3], int dobndry, int nmom,
-                const std::function<void(const double*)>& add, qq_solve_info* infos) {
+                const std::function<void(const double*)>& add, qq_solve_info* infos,
+                const std::function<int()>& pre = {}) {
   if (noise_kind != 2 && noise_kind != 4) return set_error(QQ_BAD_ARG, "noise_kind must be 2 or 4");
   if (nnoise < 1) return set_error(QQ_BAD_ARG, "nnoise must be >= 1");
   if (method->solver < 0 || method->solver > 2) return set_error(QQ_BAD_ARG, "solver must be 0, 1 or 2");
@@ -45,20 +48,63 @@ int discon_loop(qq_ctx* c, int noise_kind, int nnoise, const double kappa[2], co
   QQ_CK(dbo.alloc(sizeof(double) * nv * block));
   QQ_CK(dxe.alloc(sizeof(double) * nv * block));
   QQ_CK(dxo.alloc(sizeof(double) * nv * block));
-  std::vector<double> hbe(nv), hbo(nv), Jn((size_t)12 * nt * nmom);
-  qq_defl* defl = nullptr;
-  if (method->solver == 2) QQ_TRY(qq_defl_create(c, method->m, method->k, &defl));
+  std::vector<double> Jn((size_t)12 * nt * nmom);
+  // Host noise, double-buffered: a second thread draws the next block while the device
+  // solves this one.  The generator has one user at a time and draws noise by noise,
+  // be then bo, exactly as many noises as requested: the stream is the reference's.
+  std::vector<double> hb[2] = {std::vector<double>(2 * nv * block), std::vector<double>(2 * nv * block)};
+  const bool z4 = noise_kind == 4;
+  auto draw = [c, nv, z4, &hb](int which, int nb) -> int {
+    for (int k = 0; k < nb; ++k) {
+      double* e = hb[which].data() + 2 * nv * k;
+      const int st = sources_z(c, e, e + nv, z4);
+      if (st != QQ_OK) return st;
+    }
+    return QQ_OK;
+  };
+  int gen_rc = QQ_OK;  // declared before the joiner, which joins the thread on every exit
+  struct Joiner {
+    std::thread t;
+    ~Joiner() {
+      if (t.joinable()) t.join();
+    }
+  } gen;
+  struct DeflGuard {
+    qq_defl* d = nullptr;
+    ~DeflGuard() {
+      if (d) qq_defl_destroy(d);
+    }
+  } defl;
+  if (method->solver == 2) QQ_TRY(qq_defl_create(c, method->m, method->k, &defl.d));
+  int cur = 0;
+  if (pre) {
+    gen.t = std::thread([&gen_rc, &draw, nb0 = std::min(block, nnoise), dev = c->device] {
+      cudaSetDevice(dev);
+      gen_rc = draw(0, nb0);
+    });
+    const int pre_rc = pre();
+    gen.t.join();
+    QQ_TRY(pre_rc);
+    QQ_TRY(gen_rc);
+  } else {
+    QQ_TRY(draw(cur, std::min(block, nnoise)));
+  }
   int rc = QQ_OK;
   for (int i0 = 0; i0 < nnoise && rc == QQ_OK; i0 += block) {
     const int nb = std::min(block, nnoise - i0);
-    for (int k = 0; k < nb; ++k) {  // the generator's order: noise by noise, be then bo
-      QQ_TRY(sources_z(c, hbe.data(), hbo.data(), noise_kind == 4));
-      QQ_CK(cudaMemcpyAsync(dbe.as<double>() + nv * k, hbe.data(), sizeof(double) * nv,
-                            cudaMemcpyHostToDevice, c->st));
-      QQ_CK(cudaMemcpyAsync(dbo.as<double>() + nv * k, hbo.data(), sizeof(double) * nv,
-                            cudaMemcpyHostToDevice, c->st));
-      QQ_CK(cudaStreamSynchronize(c->st));  // hbe / hbo are reused for the next noise
+    for (int k = 0; k < nb; ++k) {
+      const double* e = hb[cur].data() + 2 * nv * k;
+      QQ_CK(cudaMemcpyAsync(dbe.as<double>() + nv * k, e, sizeof(double) * nv, cudaMemcpyHostToDevice, c->st));
+      QQ_CK(cudaMemcpyAsync(dbo.as<double>() + nv * k, e + nv, sizeof(double) * nv, cudaMemcpyHostToDevice,
+                            c->st));
     }
+    QQ_CK(cudaStreamSynchronize(c->st));  // hb[cur] may be redrawn from here on
+    const int nb1 = std::min(block, nnoise - (i0 + nb));
+    gen_rc = QQ_OK;
+    if (nb1 > 0) gen.t = std::thread([&gen_rc, &draw, cur, nb1, dev = c->device] {
+      cudaSetDevice(dev);
+      gen_rc = draw(1 - cur, nb1);
+    });
     qq_solve_info* inf = infos ? infos + i0 : nullptr;
     std::vector<qq_solve_info> local;
     if (!inf) {
@@ -71,7 +117,7 @@ int discon_loop(qq_ctx* c, int noise_kind, int nnoise, const double kappa[2], co
       QQ_CK(cudaMemsetAsync(dxe.p, 0, sizeof(double) * nv, c->st));
       QQ_CK(cudaMemsetAsync(dxo.p, 0, sizeof(double) * nv, c->st));
       st = qq_fermprop(c, dbe.as<double>(), dbo.as<double>(), kappa, 6, method->tol, 0, gm, dxe.as<double>(),
-                       dxo.as<double>(), 0, i0 == 0 ? 1 : 2, defl, inf);
+                       dxo.as<double>(), 0, i0 == 0 ? 1 : 2, defl.d, inf);
     } else {
       QQ_CK(cudaMemsetAsync(dxe.p, 0, sizeof(double) * nv * nb, c->st));
       QQ_CK(cudaMemsetAsync(dxo.p, 0, sizeof(double) * nv * nb, c->st));
@@ -88,8 +134,10 @@ int discon_loop(qq_ctx* c, int noise_kind, int nnoise, const double kappa[2], co
                         dxo.as<double>() + nv * k, kappa[0], delta, io, dobndry, nmom, Jn.data()));
       add(Jn.data());
     }
+    if (gen.t.joinable()) gen.t.join();
+    if (gen_rc != QQ_OK) return gen_rc;
+    cur = 1 - cur;
   }
-  if (defl) qq_defl_destroy(defl);
   return rc;
 }
 
@@ -173,9 +221,11 @@ extern "C" int qq_twistdiscon(qq_ctx* c, int noise_kind, int nnoise, const doubl
     return ((((size_t)iop * nmom + im) * 6 + lv) * nt + t) * 2 + ri;
   };
   // Jtotal = numnoises * Jvev (:3779-3839): twvev, kappa on every operator but 2 and 6,
-  // the highest order combined with the first for nsub = 6
+  // the highest order combined with the first for nsub = 6 (run while the first block of
+  // noises is drawn)
   std::vector<double> jt(n, 0.0);
-  if (nsub == 4 || nsub == 6) {
+  auto vev = [&]() -> int {
+    if (nsub != 4 && nsub != 6) return QQ_OK;
     std::vector<double> jv(n);
     QQ_TRY(qq_twvev(c, kappa[0], delta, io, dobndry, 1, nsub, nmom, nop, jv.data()));
     for (int iop = 0; iop < nop; ++iop)
@@ -191,7 +241,8 @@ extern "C" int qq_twistdiscon(qq_ctx* c, int noise_kind, int nnoise, const doubl
             for (int ri = 0; ri < 2; ++ri)
               jv[at(ri, t, 5, im, iop)] = jv[at(ri, t, 3, im, iop)] + jv[at(ri, t, 5, im, iop)];
     for (size_t e = 0; e < n; ++e) jt[e] = nnoise * jv[e];
-  }
+    return QQ_OK;
+  };
   // + the kappa-scaled traces of every noise at the levels twAverage fills (:4040-4045)
   const std::vector<int> lv = filled_levels(nsub);
   const bool any = nsub == 0 || nsub == 4 || nsub == 6;
@@ -199,7 +250,7 @@ extern "C" int qq_twistdiscon(qq_ctx* c, int noise_kind, int nnoise, const doubl
                              [&](const double* Jn) {
                                if (any) add_levels(Jn, nt, nmom, nop, lv, jt.data());
                              },
-                             infos);
+                             infos, vev);
   if (rc != QQ_OK && rc != QQ_NOT_CONVERGED) return rc;
   // :4161-4164
   for (size_t e = 0; e < n; ++e) jt[e] = jt[e] / (double)nnoise;

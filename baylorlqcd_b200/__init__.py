@@ -149,8 +149,8 @@ def load_library() -> C.CDLL:
         "qq_fgmresdr": ([P, P, P, P, IP, D, I, DP, C.POINTER(qq_solve_info)], I),
         "qq_pionrho": ([P, P, P, I, P, P, P], I),
         "qq_twvev": ([P, D, D, IP, I, I, I, I, I, P], I),
-        "qq_twaverage": ([P, P, P, P, P, D, D, IP, I, I, I, I, P], I),
-        "qq_twistdiscon": ([P, I, I, DP, P, D, IP, I, I, I, I, P, P], I),
+        "qq_twaverage": ([P, P, P, P, P, D, D, IP, I, I, I, I, I, P], I),
+        "qq_twistdiscon": ([P, I, I, DP, P, D, IP, I, I, I, I, I, P, P], I),
         "qq_heatbath": ([P, D, I, C.c_ulonglong, P, DP], I),
         "qq_ctx_stream": ([P, C.POINTER(P)], I),
         "qq_launch_count": ([], C.c_longlong),
@@ -467,17 +467,18 @@ class Lattice:
         return J, [SolveInfo.from_c(i) for i in infos]
 
     def twaverage(self, be, bo, xe, xo, kappa: float = 0.0, delta: float = 0.0, io=(1, 1, 1), dobndry: int = 0,
-                  nsub: int = 0, nmom: int = 5, nop: int = 6):
+                  nsub: int = 0, nmom: int = 5, nop: int = 6, ir: int = 1):
         """twAverage of one noise (qq_twaverage): Jave as an array (nop, nmom, 6, nt, 2)."""
         J = np.zeros((nop, nmom, 6, self.dims[3], 2))
         iov = np.ascontiguousarray(io, dtype=np.int32)
         _check(self.lib.qq_twaverage(self._ctx, _ptr(be), _ptr(bo), _ptr(xe), _ptr(xo), float(kappa), float(delta),
-                                     iov.ctypes.data_as(C.POINTER(C.c_int)), int(dobndry), int(nsub), int(nmom),
-                                     int(nop), _ptr(J)))
+                                     iov.ctypes.data_as(C.POINTER(C.c_int)), int(dobndry), int(ir), int(nsub),
+                                     int(nmom), int(nop), _ptr(J)))
         return J
 
     def twistdiscon(self, noise_kind: int, nnoise: int, kappa, nsub: int = 6, nmom: int = 5, nop: int = 6,
-                    io=(1, 1, 1), delta: float = 0.0, dobndry: int = 0, solver: int = 0, m: int = 30, k: int = 10,
+                    io=(1, 1, 1), delta: float = 0.0, dobndry: int = 0, ir: int = 1, solver: int = 0, m: int = 30,
+                    k: int = 10,
                     precision: int = 32, rhs_block: int = 12, tol: float = 1e-10, max_outer: int = 0,
                     deflate: int = 0, defl_tol: float = 1e-5):
         """twistdiscon (qq_twistdiscon): Jtotal as an array (nop, nmom, 6, nt, 2) and the
@@ -487,8 +488,8 @@ class Lattice:
         meth = qq_method(m, k, precision, rhs_block, tol, max_outer, solver, deflate, defl_tol)
         iov = np.ascontiguousarray(io, dtype=np.int32)
         st = self.lib.qq_twistdiscon(self._ctx, int(noise_kind), int(nnoise), _d2(kappa), C.byref(meth),
-                                     float(delta), iov.ctypes.data_as(C.POINTER(C.c_int)), int(dobndry), int(nsub),
-                                     int(nmom), int(nop), _ptr(J), infos)
+                                     float(delta), iov.ctypes.data_as(C.POINTER(C.c_int)), int(dobndry), int(ir),
+                                     int(nsub), int(nmom), int(nop), _ptr(J), infos)
         _check(st, allow_not_converged=True)
         return J, [SolveInfo.from_c(i) for i in infos]
 

@@ -24,7 +24,7 @@ int sources_z(qq_ctx* c, double* be, double* bo, bool z4);
 int batch_solve(qq_ctx* c, int nrhs, const double* be, const double* bo, const double kappa[2],
                 const qq_method* method, double* xe, double* xo, qq_solve_info* infos);
 int traces_mom(qq_ctx* c, const double* be, const double* bo, const double* xe, const double* xo,
-               double kappa, double delta, const int io[3], int dobndry, int nmom, double* J);
+               double kappa, double delta, const int io[3], int dobndry, int nmom, double* J, int ir);
 
 namespace {
 
@@ -32,7 +32,7 @@ namespace {
 // J(2, nt, nmom, 6) and hand them to add().  pre (may be empty) runs on the calling
 // thread while the first block of noises is drawn; it must not draw random numbers.
 int discon_loop(qq_ctx* c, int noise_kind, int nnoise, const double kappa[2], const qq_method* method,
-                double delta, const int io[3], int dobndry, int nmom,
+                double delta, const int io[3], int dobndry, int ir, int nmom,
                 const std::function<void(const double*)>& add, qq_solve_info* infos,
                 const std::function<int()>& pre = {}) {
   if (noise_kind != 2 && noise_kind != 4) return set_error(QQ_BAD_ARG, "noise_kind must be 2 or 4");
@@ -131,7 +131,7 @@ int discon_loop(qq_ctx* c, int noise_kind, int nnoise, const double kappa[2], co
     if (st == QQ_NOT_CONVERGED) rc = QQ_NOT_CONVERGED;
     for (int k = 0; k < nb; ++k) {
       QQ_TRY(traces_mom(c, dbe.as<double>() + nv * k, dbo.as<double>() + nv * k, dxe.as<double>() + nv * k,
-                        dxo.as<double>() + nv * k, kappa[0], delta, io, dobndry, nmom, Jn.data()));
+                        dxo.as<double>() + nv * k, kappa[0], delta, io, dobndry, nmom, Jn.data(), ir));
       add(Jn.data());
     }
     if (gen.t.joinable()) gen.t.join();
@@ -179,7 +179,7 @@ extern "C" int qq_discon_traces(qq_ctx* c, int noise_kind, int nnoise, const dou
   const int nt = c->g.n[3];
   const int io[3] = {1, 1, 1};
   std::vector<double> Jsum((size_t)12 * nt, 0.0);
-  const int rc = discon_loop(c, noise_kind, nnoise, kappa, method, delta, io, dobndry, 1,
+  const int rc = discon_loop(c, noise_kind, nnoise, kappa, method, delta, io, dobndry, 1, 1,
                              [&](const double* Jn) {
                                for (size_t e = 0; e < Jsum.size(); ++e) Jsum[e] += Jn[e];
                              },
@@ -192,8 +192,8 @@ extern "C" int qq_discon_traces(qq_ctx* c, int noise_kind, int nnoise, const dou
 }
 
 extern "C" int qq_twaverage(qq_ctx* c, const double* be, const double* bo, const double* xe, const double* xo,
-                            double kappa, double delta, const int io[3], int dobndry, int nsub, int nmom, int nop,
-                            double* Jave) {
+                            double kappa, double delta, const int io[3], int dobndry, int ir, int nsub, int nmom,
+                            int nop, double* Jave) {
   (void)kappa;  // enters only the subtraction levels, which the reference leaves switched off
   if (!c) return set_error(QQ_BAD_ARG, "null context");
   if (!be || !bo || !xe || !xo || !io || !Jave) return set_error(QQ_BAD_ARG, "null argument");
@@ -201,7 +201,7 @@ extern "C" int qq_twaverage(qq_ctx* c, const double* be, const double* bo, const
   QQ_CK(cudaSetDevice(c->device));
   const int nt = c->g.n[3];
   std::vector<double> J((size_t)12 * nt * std::max(nmom, 1));
-  QQ_TRY(traces_mom(c, be, bo, xe, xo, 1.0, delta, io, dobndry, nmom, J.data()));
+  QQ_TRY(traces_mom(c, be, bo, xe, xo, 1.0, delta, io, dobndry, nmom, J.data(), ir));
   std::vector<double> out((size_t)2 * nt * 6 * nmom * nop, 0.0);
   if (nsub == 0 || nsub == 4 || nsub == 6) add_levels(J.data(), nt, nmom, nop, filled_levels(nsub), out.data());
   QQ_CK(cudaMemcpy(Jave, out.data(), sizeof(double) * out.size(), cudaMemcpyDefault));
@@ -209,8 +209,8 @@ extern "C" int qq_twaverage(qq_ctx* c, const double* be, const double* bo, const
 }
 
 extern "C" int qq_twistdiscon(qq_ctx* c, int noise_kind, int nnoise, const double kappa[2],
-                              const qq_method* method, double delta, const int io[3], int dobndry, int nsub,
-                              int nmom, int nop, double* Jtotal, qq_solve_info* infos) {
+                              const qq_method* method, double delta, const int io[3], int dobndry, int ir,
+                              int nsub, int nmom, int nop, double* Jtotal, qq_solve_info* infos) {
   if (!c) return set_error(QQ_BAD_ARG, "null context");
   if (!kappa || !method || !io || !Jtotal) return set_error(QQ_BAD_ARG, "null argument");
   if (nop < 6) return set_error(QQ_BAD_ARG, "nop must be at least 6");
@@ -227,7 +227,7 @@ extern "C" int qq_twistdiscon(qq_ctx* c, int noise_kind, int nnoise, const doubl
   auto vev = [&]() -> int {
     if (nsub != 4 && nsub != 6) return QQ_OK;
     std::vector<double> jv(n);
-    QQ_TRY(qq_twvev(c, kappa[0], delta, io, dobndry, 1, nsub, nmom, nop, jv.data()));
+    QQ_TRY(qq_twvev(c, kappa[0], delta, io, dobndry, ir, nsub, nmom, nop, jv.data()));
     for (int iop = 0; iop < nop; ++iop)
       if (iop != 1 && iop != 5)
         for (int im = 0; im < nmom; ++im)
@@ -246,7 +246,8 @@ extern "C" int qq_twistdiscon(qq_ctx* c, int noise_kind, int nnoise, const doubl
   // + the kappa-scaled traces of every noise at the levels twAverage fills (:4040-4045)
   const std::vector<int> lv = filled_levels(nsub);
   const bool any = nsub == 0 || nsub == 4 || nsub == 6;
-  const int rc = discon_loop(c, noise_kind, nnoise, kappa, method, delta, io, dobndry, nmom,
+  if (ir != 1 && ir != -1) return set_error(QQ_BAD_ARG, "ir must be 1 or -1");
+  const int rc = discon_loop(c, noise_kind, nnoise, kappa, method, delta, io, dobndry, ir, nmom,
                              [&](const double* Jn) {
                                if (any) add_levels(Jn, nt, nmom, nop, lv, jt.data());
                              },

@@ -67,8 +67,9 @@ __device__ inline void load_site(const Geom& g, const RefDims& rd, const double*
   }
 }
 
-// sum_{d,c} eta_d,c [ (1 + s gamma_mu) w ]_d,c
-__device__ inline cplx<double> proj_dot(const double eta[4][3], int mu, double s, const cplx<double> w[4][3]) {
+// sum_{d,c} eta_d,c [ (r + s gamma_mu) w ]_d,c  (Wilson r = +-1)
+__device__ inline cplx<double> proj_dot(const double eta[4][3], int mu, double r, double s,
+                                        const cplx<double> w[4][3]) {
   cplx<double> acc{0.0, 0.0};
 #pragma unroll
   for (int d = 0; d < 4; ++d) {
@@ -77,8 +78,8 @@ __device__ inline cplx<double> proj_dot(const double eta[4][3], int mu, double s
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       const cplx<double> gw{pr * w[e][c].re - pi * w[e][c].im, pr * w[e][c].im + pi * w[e][c].re};
-      acc.re += eta[d][c] * (w[d][c].re + gw.re);
-      acc.im += eta[d][c] * (w[d][c].im + gw.im);
+      acc.re += eta[d][c] * (r * w[d][c].re + gw.re);
+      acc.im += eta[d][c] * (r * w[d][c].im + gw.im);
     }
   }
   return acc;
@@ -88,7 +89,7 @@ template <int RECON>
 __global__ void __launch_bounds__(128) trace_sites_kernel(Geom g, RefDims rd, const double* be,
                                                           const double* bo, const double* xe,
                                                           const double* xo, const void* gauge,
-                                                          double kappa, double cosd, double sind,
+                                                          double kappa, double r, double cosd, double sind,
                                                           int dobndry, double* val) {
   const int V = 2 * g.vh;
   const int L = blockIdx.x * blockDim.x + threadIdx.x;
@@ -149,7 +150,7 @@ __global__ void __launch_bounds__(128) trace_sites_kernel(Geom g, RefDims rd, co
           for (int b = 0; b < 3; ++b) t = cadd(t, cmulconj(u.e[b][a], xp.v[d][b]));
           w[d][a] = t;
         }
-      const cplx<double> av = proj_dot(etaf, mu, 1.0, w);
+      const cplx<double> av = proj_dot(etaf, mu, r, 1.0, w);
       // b = eta(y)^T (1 - gamma_mu) U x'(y+mu)
 #pragma unroll
       for (int d = 0; d < 4; ++d)
@@ -160,7 +161,7 @@ __global__ void __launch_bounds__(128) trace_sites_kernel(Geom g, RefDims rd, co
           for (int b = 0; b < 3; ++b) t = cadd(t, cmul(u.e[a][b], xpf.v[d][b]));
           w[d][a] = t;
         }
-      const cplx<double> bv = proj_dot(eta, mu, -1.0, w);
+      const cplx<double> bv = proj_dot(eta, mu, r, -1.0, w);
       jm = {kappa * (av.re - bv.re), kappa * (av.im - bv.im)};
     }
     out[slot[mu]] = jm.re;
@@ -246,7 +247,7 @@ void momentum_table(const int* n, const int io[3], std::vector<double>& mf) {
 }
 
 int traces_mom(qq_ctx* c, const double* be, const double* bo, const double* xe, const double* xo,
-               double kappa, double delta, const int io[3], int dobndry, int nmom, double* J);
+               double kappa, double delta, const int io[3], int dobndry, int nmom, double* J, int ir = 1);
 
 int traces_level0(qq_ctx* c, const double* be, const double* bo, const double* xe,
                   const double* xo, double kappa, double delta, int dobndry, double* J) {
@@ -255,7 +256,8 @@ int traces_level0(qq_ctx* c, const double* be, const double* bo, const double* x
 }
 
 int traces_mom(qq_ctx* c, const double* be, const double* bo, const double* xe, const double* xo,
-               double kappa, double delta, const int io[3], int dobndry, int nmom, double* J) {
+               double kappa, double delta, const int io[3], int dobndry, int nmom, double* J, int ir) {
+  if (ir != 1 && ir != -1) return set_error(QQ_BAD_ARG, "ir must be 1 or -1");
   if (!c->have_gauge) return set_error(QQ_BAD_ARG, "no gauge field uploaded");
   if (dobndry != 0 && dobndry != 1) return set_error(QQ_BAD_ARG, "dobndry must be 0 or 1");
   if (nmom < 1 || nmom > 5) return set_error(QQ_BAD_ARG, "nmom must be 1..5");
@@ -279,10 +281,10 @@ int traces_mom(qq_ctx* c, const double* be, const double* bo, const double* xe, 
   }
   const dim3 grd((V + 127) / 128);
   if (c->recon64 == 18)
-    trace_sites_kernel<18><<<grd, 128, 0, c->st>>>(c->g, c->rd, dbe, dbo, dxe, dxo, c->gauge64.p, kappa,
+    trace_sites_kernel<18><<<grd, 128, 0, c->st>>>(c->g, c->rd, dbe, dbo, dxe, dxo, c->gauge64.p, kappa, (double)ir,
                                                    std::cos(delta), std::sin(delta), dobndry, val);
   else
-    trace_sites_kernel<12><<<grd, 128, 0, c->st>>>(c->g, c->rd, dbe, dbo, dxe, dxo, c->gauge64.p, kappa,
+    trace_sites_kernel<12><<<grd, 128, 0, c->st>>>(c->g, c->rd, dbe, dbo, dxe, dxo, c->gauge64.p, kappa, (double)ir,
                                                    std::cos(delta), std::sin(delta), dobndry, val);
   QQ_CK(cudaGetLastError());
   trace_slices_kernel<<<dim3(nt, nmom), 256, 0, c->st>>>(val, V, v3, nt, dmf, nmom, dJ);

@@ -219,15 +219,17 @@ int qq_discon_traces(qq_ctx* ctx, int noise_kind, int nnoise, const double kappa
 
 /* twAverage Q/vevbleft.f90:2541-4704 for one noise: the loop operators of the noise be/bo
  * and its solution xe/xo with the momentum projections imom 2..5 about the origin io
- * (1-based), into Jave(2, nt, 6, nmom, nop) (Fortran order, host or device), unscaled.
+ * (1-based) and Wilson r = ir (+-1: currentCalc2P / currentCalc2M, :10863-11635), into
+ * Jave(2, nt, 6, nmom, nop) (Fortran order, host or device), unscaled.
  * The reference's perturbative subtraction inside twAverage is switched off
  * (if (.false.), :2990-3935), so every level it fills -- 1, and 4 (nsub = 4, 6) and 6
  * (nsub = 6) -- holds the unsubtracted traces; every other entry is zero.  kappa enters
  * only that switched-off subtraction.  nmom 1..5, nop >= 6. */
 int qq_twaverage(qq_ctx* ctx, const double* be, const double* bo, const double* xe,
                  const double* xo, double kappa, double delta, const int io[3], int dobndry,
-                 int nsub, int nmom, int nop, double* Jave);
-/* twistdiscon Q/disconloops.f90:3612-4351 at subtraction levels nsub = 0, 4 or 6 (r = 1):
+                 int ir, int nsub, int nmom, int nop, double* Jave);
+/* twistdiscon Q/disconloops.f90:3612-4351 at subtraction levels nsub = 0, 4 or 6, Wilson
+ * r = ir (+-1, passed to twvev and twAverage as the reference does):
  * Jtotal = numnoises * Jvev' + sum over noises of Jave' , divided by numnoises and by
  * nx*ny*nz (:4161-4164), where Jvev' is qq_twvev's output with every operator but 2 and
  * 6 times kappa and level 6 combined with level 4 (:3793-3805), and Jave' is qq_twaverage
@@ -235,8 +237,8 @@ int qq_twaverage(qq_ctx* ctx, const double* be, const double* bo, const double* 
  * qq_discon_traces (call qq_initlagfib first).  Jtotal(2, nt, 6, nmom, nop), host or
  * device.  Returns QQ_NOT_CONVERGED (with Jtotal filled) if a solve stopped short. */
 int qq_twistdiscon(qq_ctx* ctx, int noise_kind, int nnoise, const double kappa[2],
-                   const qq_method* method, double delta, const int io[3], int dobndry, int nsub,
-                   int nmom, int nop, double* Jtotal, qq_solve_info* infos);
+                   const qq_method* method, double delta, const int io[3], int dobndry, int ir,
+                   int nsub, int nmom, int nop, double* Jtotal, qq_solve_info* infos);
 
 /* ---- file formats (host memory; no device needed) ----
  * Fortran unformatted sequential files, as the reference writes them: every record is

@@ -70,7 +70,7 @@ def lib() -> C.CDLL:
             "oq_orgschur": ([IP, I, DP, I, DP, I, DP, IP], None),
             "oq_twaverage_level0": ([P, DP, DP, DP, DP, DP, D, D, C.c_int, DP], None),
             "oq_twvev": ([P, DP, D, D, IP, I, I, I, I, I, DP], None),
-            "oq_twaverage_mom": ([P, DP, DP, DP, DP, DP, D, D, IP, I, I, DP], None),
+            "oq_twaverage_mom": ([P, DP, DP, DP, DP, DP, D, D, IP, I, I, I, DP], None),
             "oq_twvev_sites": ([P, DP, D, D, IP, I, I, I, IP, I, DP], None),
             "oq_set_kcyclim": ([I], None),
             "oq_coldstart": ([P, DP], None),
@@ -279,7 +279,7 @@ class OracleLattice:
                                   _dp(self.u), float(kappa), float(delta), int(dobndry), _dp(J))
         return J
 
-    def twaverage(self, be, bo, xe, xo, kappa, delta=0.0, io=(1, 1, 1), dobndry=0, nmom=5):
+    def twaverage(self, be, bo, xe, xo, kappa, delta=0.0, io=(1, 1, 1), dobndry=0, nmom=5, ir=1):
         """Level-0 traces of one noise with twAverage's momentum projections:
         J[iop, imom, t, re/im] (the reverse of (2, nt, nmom, 6)), ops other than 2 and
         6 scaled by kappa."""
@@ -287,7 +287,7 @@ class OracleLattice:
         _, iop = _ip(io)
         lib().oq_twaverage_mom(self._g, _dp(np.ascontiguousarray(be)), _dp(np.ascontiguousarray(bo)),
                                _dp(np.ascontiguousarray(xe)), _dp(np.ascontiguousarray(xo)), _dp(self.u),
-                               float(kappa), float(delta), iop, int(dobndry), int(nmom), _dp(J))
+                               float(kappa), float(delta), iop, int(dobndry), int(nmom), int(ir), _dp(J))
         return J
 
     def twvev(self, kappa, delta=0.0, io=(1, 1, 1), dobndry=0, ir=1, nsub=6, nmom=5, nop=6):

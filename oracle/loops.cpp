@@ -34,21 +34,25 @@ struct Lex {
 
 extern "C" void oq_twaverage_mom(const oq_geom* g, const double* be, const double* bo, const double* xe,
                                  const double* xo, const double* u, double kappa, double delta, const int io[3],
-                                 int dobndry, int nmom, double* J);
+                                 int dobndry, int nmom, int ir, double* J);
 
 extern "C" void oq_twaverage_level0(const oq_geom* g, const double* be, const double* bo,
                                     const double* xe, const double* xo, const double* u,
                                     double kappa, double delta, int dobndry, double* J) {
   const int io[3] = {1, 1, 1};
-  oq_twaverage_mom(g, be, bo, xe, xo, u, kappa, delta, io, dobndry, 1, J);
+  oq_twaverage_mom(g, be, bo, xe, xo, u, kappa, delta, io, dobndry, 1, 1, J);
 }
 
-// The same traces with twAverage's momentum projections (:4434-4503): imom 2..5 weight
+// The same traces with twAverage's momentum projections (:4434-4503) and either Wilson r
+// (currentCalc2, :10832-10859): imom 2..5 weight
 // rho, psibar psi and psibar gamma5 psi by ffac and the imaginary parts of the
 // currents by fas1..3 at the site each value sits on; J(2, nt, nmom, 6).
 extern "C" void oq_twaverage_mom(const oq_geom* g, const double* be, const double* bo, const double* xe,
                                  const double* xo, const double* u, double kappa, double delta, const int io[3],
-                                 int dobndry, int nmom, double* J) {
+                                 int dobndry, int nmom, int ir, double* J) {
+  // Wilson r = +-1: currentCalc2P / currentCalc2M (:10863-11635) differ by the sign of
+  // the diagonal (Wilson) terms and by the spins and sign of the time current
+  const double rs = ir, tf = 2.0 * ir;
   const Lex L{g->n[0], g->n[1], g->n[2], g->n[3]};
   const int V = L.nx * L.ny * L.nz * L.nt;
   // lexicographic gathers: [site][colour][spin] (spin, colour 0-based)
@@ -134,47 +138,49 @@ extern "C" void oq_twaverage_mom(const oq_geom* g, const double* be, const doubl
                 const int jd = d + 1;  // 1-based spin index of the reference
                 const int od = 5 - jd - 1, o3 = (jd % 2 == 1 ? 3 / jd : 8 / jd) - 1;
                 for (int jc = 0; jc < 3; ++jc) {
-                  // point-split J4
-                  if ((jd == 1 || jd == 2) && (!fixbc || t != L.nt - 1)) {
+                  // point-split J4: r = 1 takes spins 1,2 at ahere and 3,4 at leftt
+                  // (currentCalc2P); r = -1 the reverse, with the opposite sign (currentCalc2M)
+                  const bool hset = ir == 1 ? (jd == 1 || jd == 2) : (jd == 3 || jd == 4);
+                  if (hset && (!fixbc || t != L.nt - 1)) {
                     if (jri == 1) {
-                      rhor_h = rhor_h + 2.0 * s * Ul(h, 3, 0, c, jc) * E(rt, jc, d);
-                      rhoi_h = rhoi_h - 2.0 * s * Ul(h, 3, 1, c, jc) * E(rt, jc, d);
+                      rhor_h = rhor_h + tf * s * Ul(h, 3, 0, c, jc) * E(rt, jc, d);
+                      rhoi_h = rhoi_h - tf * s * Ul(h, 3, 1, c, jc) * E(rt, jc, d);
                     } else {
-                      rhor_h = rhor_h + 2.0 * s * Ul(h, 3, 1, c, jc) * E(rt, jc, d);
-                      rhoi_h = rhoi_h + 2.0 * s * Ul(h, 3, 0, c, jc) * E(rt, jc, d);
+                      rhor_h = rhor_h + tf * s * Ul(h, 3, 1, c, jc) * E(rt, jc, d);
+                      rhoi_h = rhoi_h + tf * s * Ul(h, 3, 0, c, jc) * E(rt, jc, d);
                     }
-                  } else if ((jd == 3 || jd == 4) && (!fixbc || t != 0)) {
+                  } else if (!hset && (!fixbc || t != 0)) {
                     if (jri == 1) {
-                      rhor_l = rhor_l - 2.0 * s * Ul(lt, 3, 0, jc, c) * E(lt, jc, d);
-                      rhoi_l = rhoi_l - 2.0 * s * Ul(lt, 3, 1, jc, c) * E(lt, jc, d);
+                      rhor_l = rhor_l - tf * s * Ul(lt, 3, 0, jc, c) * E(lt, jc, d);
+                      rhoi_l = rhoi_l - tf * s * Ul(lt, 3, 1, jc, c) * E(lt, jc, d);
                     } else {
-                      rhor_l = rhor_l + 2.0 * s * Ul(lt, 3, 1, jc, c) * E(lt, jc, d);
-                      rhoi_l = rhoi_l - 2.0 * s * Ul(lt, 3, 0, jc, c) * E(lt, jc, d);
+                      rhor_l = rhor_l + tf * s * Ul(lt, 3, 1, jc, c) * E(lt, jc, d);
+                      rhoi_l = rhoi_l - tf * s * Ul(lt, 3, 0, jc, c) * E(lt, jc, d);
                     }
                   }
                   // point-split J1
                   if (jri == 1) {
-                    j1r_l = j1r_l - s * Ul(lx, 0, 0, jc, c) * E(lx, jc, d) + s * Ul(lx, 0, 0, jc, c) * E(lx, jc, od);
-                    j1i_l = j1i_l - s * Ul(lx, 0, 1, jc, c) * E(lx, jc, d) + s * Ul(lx, 0, 1, jc, c) * E(lx, jc, od);
-                    j1r_h = j1r_h + s * Ul(h, 0, 0, c, jc) * E(rx, jc, d) + s * Ul(h, 0, 0, c, jc) * E(rx, jc, od);
-                    j1i_h = j1i_h - s * Ul(h, 0, 1, c, jc) * E(rx, jc, d) - s * Ul(h, 0, 1, c, jc) * E(rx, jc, od);
+                    j1r_l = j1r_l - rs * s * Ul(lx, 0, 0, jc, c) * E(lx, jc, d) + s * Ul(lx, 0, 0, jc, c) * E(lx, jc, od);
+                    j1i_l = j1i_l - rs * s * Ul(lx, 0, 1, jc, c) * E(lx, jc, d) + s * Ul(lx, 0, 1, jc, c) * E(lx, jc, od);
+                    j1r_h = j1r_h + rs * s * Ul(h, 0, 0, c, jc) * E(rx, jc, d) + s * Ul(h, 0, 0, c, jc) * E(rx, jc, od);
+                    j1i_h = j1i_h - rs * s * Ul(h, 0, 1, c, jc) * E(rx, jc, d) - s * Ul(h, 0, 1, c, jc) * E(rx, jc, od);
                   } else {
-                    j1r_l = j1r_l + s * Ul(lx, 0, 1, jc, c) * E(lx, jc, d) - s * Ul(lx, 0, 1, jc, c) * E(lx, jc, od);
-                    j1i_l = j1i_l - s * Ul(lx, 0, 0, jc, c) * E(lx, jc, d) + s * Ul(lx, 0, 0, jc, c) * E(lx, jc, od);
-                    j1r_h = j1r_h + s * Ul(h, 0, 1, c, jc) * E(rx, jc, d) + s * Ul(h, 0, 1, c, jc) * E(rx, jc, od);
-                    j1i_h = j1i_h + s * Ul(h, 0, 0, c, jc) * E(rx, jc, d) + s * Ul(h, 0, 0, c, jc) * E(rx, jc, od);
+                    j1r_l = j1r_l + rs * s * Ul(lx, 0, 1, jc, c) * E(lx, jc, d) - s * Ul(lx, 0, 1, jc, c) * E(lx, jc, od);
+                    j1i_l = j1i_l - rs * s * Ul(lx, 0, 0, jc, c) * E(lx, jc, d) + s * Ul(lx, 0, 0, jc, c) * E(lx, jc, od);
+                    j1r_h = j1r_h + rs * s * Ul(h, 0, 1, c, jc) * E(rx, jc, d) + s * Ul(h, 0, 1, c, jc) * E(rx, jc, od);
+                    j1i_h = j1i_h + rs * s * Ul(h, 0, 0, c, jc) * E(rx, jc, d) + s * Ul(h, 0, 0, c, jc) * E(rx, jc, od);
                   }
                   // point-split J2, diagonal part
                   if (jri == 1) {
-                    j2r_l = j2r_l - s * Ul(ly, 1, 0, jc, c) * E(ly, jc, d);
-                    j2i_l = j2i_l - s * Ul(ly, 1, 1, jc, c) * E(ly, jc, d);
-                    j2r_h = j2r_h + s * Ul(h, 1, 0, c, jc) * E(ry, jc, d);
-                    j2i_h = j2i_h - s * Ul(h, 1, 1, c, jc) * E(ry, jc, d);
+                    j2r_l = j2r_l - rs * s * Ul(ly, 1, 0, jc, c) * E(ly, jc, d);
+                    j2i_l = j2i_l - rs * s * Ul(ly, 1, 1, jc, c) * E(ly, jc, d);
+                    j2r_h = j2r_h + rs * s * Ul(h, 1, 0, c, jc) * E(ry, jc, d);
+                    j2i_h = j2i_h - rs * s * Ul(h, 1, 1, c, jc) * E(ry, jc, d);
                   } else {
-                    j2r_l = j2r_l + s * Ul(ly, 1, 1, jc, c) * E(ly, jc, d);
-                    j2i_l = j2i_l - s * Ul(ly, 1, 0, jc, c) * E(ly, jc, d);
-                    j2r_h = j2r_h + s * Ul(h, 1, 1, c, jc) * E(ry, jc, d);
-                    j2i_h = j2i_h + s * Ul(h, 1, 0, c, jc) * E(ry, jc, d);
+                    j2r_l = j2r_l + rs * s * Ul(ly, 1, 1, jc, c) * E(ly, jc, d);
+                    j2i_l = j2i_l - rs * s * Ul(ly, 1, 0, jc, c) * E(ly, jc, d);
+                    j2r_h = j2r_h + rs * s * Ul(h, 1, 1, c, jc) * E(ry, jc, d);
+                    j2i_h = j2i_h + rs * s * Ul(h, 1, 0, c, jc) * E(ry, jc, d);
                   }
                   // J2, off-diagonal part
                   if (jd % 2 == 1) {
@@ -204,15 +210,15 @@ extern "C" void oq_twaverage_mom(const oq_geom* g, const double* be, const doubl
                   }
                   // point-split J3, diagonal part
                   if (jri == 1) {
-                    j3r_l = j3r_l - s * Ul(lz, 2, 0, jc, c) * E(lz, jc, d);
-                    j3i_l = j3i_l - s * Ul(lz, 2, 1, jc, c) * E(lz, jc, d);
-                    j3r_h = j3r_h + s * Ul(h, 2, 0, c, jc) * E(rz, jc, d);
-                    j3i_h = j3i_h - s * Ul(h, 2, 1, c, jc) * E(rz, jc, d);
+                    j3r_l = j3r_l - rs * s * Ul(lz, 2, 0, jc, c) * E(lz, jc, d);
+                    j3i_l = j3i_l - rs * s * Ul(lz, 2, 1, jc, c) * E(lz, jc, d);
+                    j3r_h = j3r_h + rs * s * Ul(h, 2, 0, c, jc) * E(rz, jc, d);
+                    j3i_h = j3i_h - rs * s * Ul(h, 2, 1, c, jc) * E(rz, jc, d);
                   } else {
-                    j3r_l = j3r_l + s * Ul(lz, 2, 1, jc, c) * E(lz, jc, d);
-                    j3i_l = j3i_l - s * Ul(lz, 2, 0, jc, c) * E(lz, jc, d);
-                    j3r_h = j3r_h + s * Ul(h, 2, 1, c, jc) * E(rz, jc, d);
-                    j3i_h = j3i_h + s * Ul(h, 2, 0, c, jc) * E(rz, jc, d);
+                    j3r_l = j3r_l + rs * s * Ul(lz, 2, 1, jc, c) * E(lz, jc, d);
+                    j3i_l = j3i_l - rs * s * Ul(lz, 2, 0, jc, c) * E(lz, jc, d);
+                    j3r_h = j3r_h + rs * s * Ul(h, 2, 1, c, jc) * E(rz, jc, d);
+                    j3i_h = j3i_h + rs * s * Ul(h, 2, 0, c, jc) * E(rz, jc, d);
                   }
                   // J3, off-diagonal part
                   if (jd % 2 == 1) {

@@ -134,11 +134,11 @@ void oq_orgschur(const int* select, int n, double* t, int ldt, double* q, int ld
 void oq_twaverage_level0(const oq_geom* g, const double* be, const double* bo,
                          const double* xe, const double* xo, const double* u,
                          double kappa, double delta, int dobndry, double* J);
-// The same with the momentum projections imom 2..5 about the origin io (1-based):
-// J(2, nt, nmom, 6), nmom 1..5.
+// The same with the momentum projections imom 2..5 about the origin io (1-based) and
+// Wilson r = ir (+-1): J(2, nt, nmom, 6), nmom 1..5.
 void oq_twaverage_mom(const oq_geom* g, const double* be, const double* bo, const double* xe,
                       const double* xo, const double* u, double kappa, double delta,
-                      const int io[3], int dobndry, int nmom, double* J);
+                      const int io[3], int dobndry, int nmom, int ir, double* J);
 
 // ---- perturbative vacuum expectation values (Q/vevbleft.f90 twvev; see vev.cpp) ----
 // Jvev(2, nt, 6, nmom, nop), Fortran order; levels 4 (orders kappa^3 / kappa^4, and

@@ -82,12 +82,13 @@ def test_level0_uses_only_the_real_part_of_the_noise():
     assert np.array_equal(J1, J2)
 
 
-def closed_form_mom(links, eta, x, kappa, delta, dobndry, io, nmom):
+def closed_form_mom(links, eta, x, kappa, delta, dobndry, io, nmom, r=1):
     """The same per-site values with twAverage's momentum projections (:4434-4503):
     imom 2..5 weight rho, psibar psi and psibar gamma5 psi by ffac(y) and take
     (Im J1 fas3, Im J2 fas1), (Im J3 fas2, Im J1 fas2), (Im J2 fas3, Im J3 fas1) as the
     (real, imaginary) slots of operators 3, 4, 5, each factor at the site y the value
-    sits on."""
+    sits on.  Wilson r enters as (r +- gamma_mu) in place of (1 +- gamma_mu)
+    (currentCalc2M differs from currentCalc2P by the sign of the diagonal terms)."""
     import vevref
 
     J5 = 1j * GAMMA5
@@ -100,8 +101,8 @@ def closed_form_mom(links, eta, x, kappa, delta, dobndry, io, nmom):
         U = links[mu]
         Udx = np.einsum("...ba,...sb->...sa", np.conj(U), xp)
         Ux = np.einsum("...ab,...sb->...sa", U, np.roll(xp, -1, axis=axes[mu]))
-        a = np.einsum("...sa,...sa->...", np.roll(eta, -1, axis=axes[mu]), sp(np.eye(4) + GAMMA[mu], Udx))
-        b = np.einsum("...sa,...sa->...", eta, sp(np.eye(4) - GAMMA[mu], Ux))
+        a = np.einsum("...sa,...sa->...", np.roll(eta, -1, axis=axes[mu]), sp(r * np.eye(4) + GAMMA[mu], Udx))
+        b = np.einsum("...sa,...sa->...", eta, sp(r * np.eye(4) - GAMMA[mu], Ux))
         val = kappa * (a - b)
         if mu == 3 and dobndry == 1:
             val[-1] = 0.0
@@ -131,8 +132,9 @@ def closed_form_mom(links, eta, x, kappa, delta, dobndry, io, nmom):
     return out
 
 
-@pytest.mark.parametrize("delta,dobndry,io", [(0.0, 0, (1, 1, 1)), (0.37, 1, (3, 2, 4))])
-def test_momentum_traces_closed_form(delta, dobndry, io):
+@pytest.mark.parametrize("delta,dobndry,io,r", [(0.0, 0, (1, 1, 1), 1), (0.37, 1, (3, 2, 4), 1),
+                                                (0.0, 0, (2, 1, 1), -1), (-0.21, 1, (1, 3, 2), -1)])
+def test_momentum_traces_closed_form(delta, dobndry, io, r):
     dims = (4, 4, 4, 8)
     ol = oracle.OracleLattice(*dims, bc=BC)
     links, u = golden_gauge(dims, ol.ntotal, seed=35, eps=0.6)
@@ -141,12 +143,13 @@ def test_momentum_traces_closed_form(delta, dobndry, io):
     be, bo = ol.z4source()
     xe = random_half(ol.ntotal, ol.nvhalf, 52)
     xo = random_half(ol.ntotal, ol.nvhalf, 53)
-    J = ol.twaverage(be, bo, xe, xo, 0.1565, delta, io=io, dobndry=dobndry, nmom=5)
+    J = ol.twaverage(be, bo, xe, xo, 0.1565, delta, io=io, dobndry=dobndry, nmom=5, ir=r)
     noise = half_to_lex(be, dims, 1) + half_to_lex(bo, dims, 2)
     x = half_to_lex(xe, dims, 1) + half_to_lex(xo, dims, 2)
-    want = closed_form_mom(links, noise.real, x, 0.1565, delta, dobndry, io, 5)
+    want = closed_form_mom(links, noise.real, x, 0.1565, delta, dobndry, io, 5, r)
     got = J[..., 0] + 1j * J[..., 1]
     assert np.abs(got - want).max() < 1e-12 * np.abs(want).max()
     assert np.abs(want[:, 1:]).max() > 0
-    J0 = ol.twaverage_level0(be, bo, xe, xo, 0.1565, delta, dobndry)
-    assert np.array_equal(J[:, 0], J0)
+    if r == 1:
+        J0 = ol.twaverage_level0(be, bo, xe, xo, 0.1565, delta, dobndry)
+        assert np.array_equal(J[:, 0], J0)

@@ -39,13 +39,13 @@ def pair():
     lat.close()
 
 
-@pytest.mark.parametrize("nsub", [0, 4, 6])
-def test_twaverage_matches_oracle(pair, nsub):
+@pytest.mark.parametrize("nsub,ir", [(0, 1), (4, 1), (6, 1), (6, -1)])
+def test_twaverage_matches_oracle(pair, nsub, ir):
     lat, ol = pair
     oracle.initlagfib(0, 9)
     be, bo = ol.z4source()
     xe, xo = random_half(ol.ntotal, ol.nvhalf, 61), random_half(ol.ntotal, ol.nvhalf, 62)
-    kw = dict(delta=0.3, io=(2, 1, 3), dobndry=1)
+    kw = dict(delta=0.3, io=(2, 1, 3), dobndry=1, ir=ir)
     got = lat.twaverage(be, bo, xe, xo, 0.15, nsub=nsub, nmom=5, nop=7, **kw)
     T = ol.twaverage(be, bo, xe, xo, 1.0, nmom=5, **kw)  # (6, nmom, nt, 2), unscaled
     want = np.zeros_like(got)
@@ -55,8 +55,8 @@ def test_twaverage_matches_oracle(pair, nsub):
     assert np.all(got[6:] == 0)
 
 
-def expected_twistdiscon(ol, kind, nnoise, kappa, nsub, nmom, nop, io, delta, dobndry):
-    jv = ol.twvev(kappa[0], delta=delta, io=io, dobndry=dobndry, ir=1, nsub=nsub, nmom=nmom, nop=nop)
+def expected_twistdiscon(ol, kind, nnoise, kappa, nsub, nmom, nop, io, delta, dobndry, ir=1):
+    jv = ol.twvev(kappa[0], delta=delta, io=io, dobndry=dobndry, ir=ir, nsub=nsub, nmom=nmom, nop=nop)
     for iop in range(nop):
         if iop not in (1, 5):
             jv[iop] = kappa[0] * jv[iop]
@@ -67,23 +67,24 @@ def expected_twistdiscon(ol, kind, nnoise, kappa, nsub, nmom, nop, io, delta, do
         be, bo = ol.z4source() if kind == 4 else ol.z2source()
         xe, xo, st, _ = ol.fermprop(be, bo, kappa, inverter=5, resmax=1e-12, nGMRES=(30, 10))
         assert st == 0
-        T = ol.twaverage(be, bo, xe, xo, kappa[0], delta=delta, io=io, dobndry=dobndry, nmom=nmom)
+        T = ol.twaverage(be, bo, xe, xo, kappa[0], delta=delta, io=io, dobndry=dobndry, nmom=nmom, ir=ir)
         for lv in LEVELS.get(nsub, []):
             jt[:6, :, lv] = jt[:6, :, lv] + T
     jt = jt / nnoise
     return jt / (DIMS[0] * DIMS[1] * DIMS[2])
 
 
-@pytest.mark.parametrize("kappa,delta,dobndry,nsub", [((0.15, 0.0), 0.0, 0, 6), ((0.15, 0.01), 0.2, 1, 4)])
-def test_twistdiscon_matches_oracle(pair, kappa, delta, dobndry, nsub):
+@pytest.mark.parametrize("kappa,delta,dobndry,nsub,ir", [((0.15, 0.0), 0.0, 0, 6, 1), ((0.15, 0.01), 0.2, 1, 4, 1),
+                                                          ((0.15, 0.01), 0.2, 0, 6, -1)])
+def test_twistdiscon_matches_oracle(pair, kappa, delta, dobndry, nsub, ir):
     import baylorlqcd_b200 as qq
 
     lat, ol = pair
     io = (1, 2, 1)
     oracle.initlagfib(0, 5)
-    want = expected_twistdiscon(ol, 4, 2, kappa, nsub, 5, 6, io, delta, dobndry)
+    want = expected_twistdiscon(ol, 4, 2, kappa, nsub, 5, 6, io, delta, dobndry, ir)
     qq.initlagfib(0, 5)
-    got, infos = lat.twistdiscon(4, 2, kappa, nsub=nsub, nmom=5, nop=6, io=io, delta=delta, dobndry=dobndry,
+    got, infos = lat.twistdiscon(4, 2, kappa, nsub=nsub, nmom=5, nop=6, io=io, delta=delta, dobndry=dobndry, ir=ir,
                                  solver=0, m=30, k=10, tol=1e-11)
     assert all(i.status == 0 for i in infos)
     assert np.abs(got - want).max() <= 1e-8 * np.abs(want).max()

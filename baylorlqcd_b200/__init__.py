@@ -150,7 +150,7 @@ def load_library() -> C.CDLL:
         "qq_pionrho": ([P, P, P, I, P, P, P], I),
         "qq_twvev": ([P, D, D, IP, I, I, I, I, I, P], I),
         "qq_twaverage": ([P, P, P, P, P, D, D, IP, I, I, I, I, I, P], I),
-        "qq_twistdiscon": ([P, I, I, DP, P, D, IP, I, I, I, I, I, P, P], I),
+        "qq_twistdiscon": ([P, I, I, DP, P, D, IP, I, I, I, I, I, P, P, P], I),
         "qq_heatbath": ([P, D, I, C.c_ulonglong, P, DP], I),
         "qq_ctx_stream": ([P, C.POINTER(P)], I),
         "qq_launch_count": ([], C.c_longlong),
@@ -480,17 +480,22 @@ class Lattice:
                     io=(1, 1, 1), delta: float = 0.0, dobndry: int = 0, ir: int = 1, solver: int = 0, m: int = 30,
                     k: int = 10,
                     precision: int = 32, rhs_block: int = 12, tol: float = 1e-10, max_outer: int = 0,
-                    deflate: int = 0, defl_tol: float = 1e-5):
+                    deflate: int = 0, defl_tol: float = 1e-5, per_noise: bool = False):
         """twistdiscon (qq_twistdiscon): Jtotal as an array (nop, nmom, 6, nt, 2) and the
-        per-noise solve reports.  Call initlagfib first, as the reference does."""
+        per-noise solve reports; with per_noise also every noise's values as an array
+        (nnoise, nop, nmom, 6, nt, 2).  Call initlagfib first, as the reference does."""
         J = np.zeros((nop, nmom, 6, self.dims[3], 2))
+        Jn = np.zeros((nnoise, nop, nmom, 6, self.dims[3], 2)) if per_noise else None
         infos = (qq_solve_info * nnoise)()
         meth = qq_method(m, k, precision, rhs_block, tol, max_outer, solver, deflate, defl_tol)
         iov = np.ascontiguousarray(io, dtype=np.int32)
         st = self.lib.qq_twistdiscon(self._ctx, int(noise_kind), int(nnoise), _d2(kappa), C.byref(meth),
                                      float(delta), iov.ctypes.data_as(C.POINTER(C.c_int)), int(dobndry), int(ir),
-                                     int(nsub), int(nmom), int(nop), _ptr(J), infos)
+                                     int(nsub), int(nmom), int(nop), _ptr(J), _ptr(Jn) if per_noise else None,
+                                     infos)
         _check(st, allow_not_converged=True)
+        if per_noise:
+            return J, [SolveInfo.from_c(i) for i in infos], Jn
         return J, [SolveInfo.from_c(i) for i in infos]
 
     def twaverage_level0(self, be, bo, xe, xo, kappa: float, delta: float = 0.0, dobndry: int = 0):

@@ -210,7 +210,7 @@ extern "C" int qq_twaverage(qq_ctx* c, const double* be, const double* bo, const
 
 extern "C" int qq_twistdiscon(qq_ctx* c, int noise_kind, int nnoise, const double kappa[2],
                               const qq_method* method, double delta, const int io[3], int dobndry, int ir,
-                              int nsub, int nmom, int nop, double* Jtotal, qq_solve_info* infos) {
+                              int nsub, int nmom, int nop, double* Jtotal, double* Jnoise, qq_solve_info* infos) {
   if (!c) return set_error(QQ_BAD_ARG, "null context");
   if (!kappa || !method || !io || !Jtotal) return set_error(QQ_BAD_ARG, "null argument");
   if (nop < 6) return set_error(QQ_BAD_ARG, "nop must be at least 6");
@@ -223,7 +223,10 @@ extern "C" int qq_twistdiscon(qq_ctx* c, int noise_kind, int nnoise, const doubl
   // Jtotal = numnoises * Jvev (:3779-3839): twvev, kappa on every operator but 2 and 6,
   // the highest order combined with the first for nsub = 6 (run while the first block of
   // noises is drawn)
-  std::vector<double> jt(n, 0.0);
+  std::vector<double> jt(n, 0.0), jvev;
+  // per-noise values Jtemp(..., inoise) = Jave' + Jvev' (:4112-4114), kept when asked for
+  std::vector<double> jn(Jnoise ? n * (size_t)nnoise : 0, 0.0);
+  int inoise = 0;
   auto vev = [&]() -> int {
     if (nsub != 4 && nsub != 6) return QQ_OK;
     std::vector<double> jv(n);
@@ -241,6 +244,7 @@ extern "C" int qq_twistdiscon(qq_ctx* c, int noise_kind, int nnoise, const doubl
             for (int ri = 0; ri < 2; ++ri)
               jv[at(ri, t, 5, im, iop)] = jv[at(ri, t, 3, im, iop)] + jv[at(ri, t, 5, im, iop)];
     for (size_t e = 0; e < n; ++e) jt[e] = nnoise * jv[e];
+    jvev.swap(jv);
     return QQ_OK;
   };
   // + the kappa-scaled traces of every noise at the levels twAverage fills (:4040-4045)
@@ -250,6 +254,8 @@ extern "C" int qq_twistdiscon(qq_ctx* c, int noise_kind, int nnoise, const doubl
   const int rc = discon_loop(c, noise_kind, nnoise, kappa, method, delta, io, dobndry, ir, nmom,
                              [&](const double* Jn) {
                                if (any) add_levels(Jn, nt, nmom, nop, lv, jt.data());
+                               if (Jnoise && any) add_levels(Jn, nt, nmom, nop, lv, jn.data() + n * inoise);
+                               ++inoise;
                              },
                              infos, vev);
   if (rc != QQ_OK && rc != QQ_NOT_CONVERGED) return rc;
@@ -258,5 +264,15 @@ extern "C" int qq_twistdiscon(qq_ctx* c, int noise_kind, int nnoise, const doubl
   const double nxyz = (double)c->g.n[0] * c->g.n[1] * c->g.n[2];
   for (size_t e = 0; e < n; ++e) jt[e] = jt[e] / nxyz;
   QQ_CK(cudaMemcpy(Jtotal, jt.data(), sizeof(double) * n, cudaMemcpyDefault));
+  if (Jnoise) {  // written out as fac * Jtemp, fac = 1/(nx*ny*nz) (:4230-4233)
+    const double fac = 1.0 / nxyz;
+    for (int k = 0; k < nnoise; ++k)
+      for (size_t e = 0; e < n; ++e) {
+        double& v = jn[n * k + e];
+        if (!jvev.empty()) v = v + jvev[e];
+        v = fac * v;
+      }
+    QQ_CK(cudaMemcpy(Jnoise, jn.data(), sizeof(double) * jn.size(), cudaMemcpyDefault));
+  }
   return rc;
 }

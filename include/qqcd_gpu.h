@@ -235,10 +235,14 @@ int qq_twaverage(qq_ctx* ctx, const double* be, const double* bo, const double* 
  * 6 times kappa and level 6 combined with level 4 (:3793-3805), and Jave' is qq_twaverage
  * of each noise with the same kappa factor (:4040-4045).  Noises, solves and method as
  * qq_discon_traces (call qq_initlagfib first).  Jtotal(2, nt, 6, nmom, nop), host or
- * device.  Returns QQ_NOT_CONVERGED (with Jtotal filled) if a solve stopped short. */
+ * device.  Jnoise (may be NULL): every noise's Jtemp = (Jave' + Jvev') / (nx*ny*nz), the
+ * per-noise values the reference writes for its error analysis (:4112-4114, :4230-4260),
+ * as Jnoise(2, nt, 6, nmom, nop, nnoise).  Returns QQ_NOT_CONVERGED (with the outputs
+ * filled) if a solve stopped short. */
 int qq_twistdiscon(qq_ctx* ctx, int noise_kind, int nnoise, const double kappa[2],
                    const qq_method* method, double delta, const int io[3], int dobndry, int ir,
-                   int nsub, int nmom, int nop, double* Jtotal, qq_solve_info* infos);
+                   int nsub, int nmom, int nop, double* Jtotal, double* Jnoise,
+                   qq_solve_info* infos);
 
 /* ---- file formats (host memory; no device needed) ----
  * Fortran unformatted sequential files, as the reference writes them: every record is

@@ -4,7 +4,8 @@ against the oracle.
 
 qq_twaverage: random noise and solution, every level layout (nsub 0, 4, 6), five
 momenta about a moved origin, twist and fixed time boundary: 1e-12 relative.
-qq_twistdiscon: the expected Jtotal is assembled here as the reference does --
+qq_twistdiscon: the expected Jtotal (and each noise's Jtemp) is assembled here as the
+reference does --
 numnoises * Jvev (twvev, kappa on operators other than 2 and 6, level 6 += level 4)
 plus every noise's kappa-scaled twAverage, over numnoises and nx*ny*nz -- from the
 oracle's noise stream, solves (FP64 GMRES-DR to 1e-12), twAverage and twvev.  Both
@@ -63,15 +64,19 @@ def expected_twistdiscon(ol, kind, nnoise, kappa, nsub, nmom, nop, io, delta, do
     if nsub == 6:
         jv[:, :, 5] = jv[:, :, 3] + jv[:, :, 5]
     jt = nnoise * jv
+    per = []
     for _ in range(nnoise):
         be, bo = ol.z4source() if kind == 4 else ol.z2source()
         xe, xo, st, _ = ol.fermprop(be, bo, kappa, inverter=5, resmax=1e-12, nGMRES=(30, 10))
         assert st == 0
         T = ol.twaverage(be, bo, xe, xo, kappa[0], delta=delta, io=io, dobndry=dobndry, nmom=nmom, ir=ir)
+        one = jv.copy()
         for lv in LEVELS.get(nsub, []):
             jt[:6, :, lv] = jt[:6, :, lv] + T
+            one[:6, :, lv] = one[:6, :, lv] + T
+        per.append(one / (DIMS[0] * DIMS[1] * DIMS[2]))  # Jtemp, written out times 1/(nx ny nz)
     jt = jt / nnoise
-    return jt / (DIMS[0] * DIMS[1] * DIMS[2])
+    return jt / (DIMS[0] * DIMS[1] * DIMS[2]), np.array(per)
 
 
 @pytest.mark.parametrize("kappa,delta,dobndry,nsub,ir", [((0.15, 0.0), 0.0, 0, 6, 1), ((0.15, 0.01), 0.2, 1, 4, 1),
@@ -82,11 +87,13 @@ def test_twistdiscon_matches_oracle(pair, kappa, delta, dobndry, nsub, ir):
     lat, ol = pair
     io = (1, 2, 1)
     oracle.initlagfib(0, 5)
-    want = expected_twistdiscon(ol, 4, 2, kappa, nsub, 5, 6, io, delta, dobndry, ir)
+    want, want_per = expected_twistdiscon(ol, 4, 2, kappa, nsub, 5, 6, io, delta, dobndry, ir)
     qq.initlagfib(0, 5)
-    got, infos = lat.twistdiscon(4, 2, kappa, nsub=nsub, nmom=5, nop=6, io=io, delta=delta, dobndry=dobndry, ir=ir,
-                                 solver=0, m=30, k=10, tol=1e-11)
+    got, infos, per = lat.twistdiscon(4, 2, kappa, nsub=nsub, nmom=5, nop=6, io=io, delta=delta, dobndry=dobndry,
+                                      ir=ir, solver=0, m=30, k=10, tol=1e-11, per_noise=True)
     assert all(i.status == 0 for i in infos)
     assert np.abs(got - want).max() <= 1e-8 * np.abs(want).max()
+    assert np.abs(per - want_per).max() <= 1e-8 * np.abs(want_per).max()
+    assert np.abs(per.mean(axis=0) - got).max() <= 1e-13 * np.abs(got).max()
     # the perturbative part is there: level 4 differs from level 1 by Jvev
     assert np.abs(got[:, :, 3] - got[:, :, 0]).max() > 1e-6 * np.abs(got).max()

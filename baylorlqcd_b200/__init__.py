@@ -37,7 +37,7 @@ EXPORTED = [
     "qq_heatbath", "qq_ctx_stream", "qq_launch_count", "qq_profile_hop", "qq_profile_hop_read",
     "qq_gfwrite", "qq_gfread", "qq_fpwrite", "qq_fpread", "qq_hsingle_block",
     "qq_hop_tuned_shape", "qq_net_create", "qq_net_destroy", "qq_net_nweights", "qq_net_get_weights",
-    "qq_net_set_weights", "qq_net_apply", "qq_net_grad", "qq_net_train", "qq_fgmres", "qq_pionrho", "qq_twvev", "qq_twaverage", "qq_twistdiscon",
+    "qq_net_set_weights", "qq_net_apply", "qq_net_grad", "qq_net_train", "qq_fgmres", "qq_pionrho", "qq_twvev", "qq_twaverage", "qq_twistdiscon", "qq_average",
     "qq_fgmresdr",
 ]
 
@@ -149,6 +149,7 @@ def load_library() -> C.CDLL:
         "qq_fgmresdr": ([P, P, P, P, IP, D, I, DP, C.POINTER(qq_solve_info)], I),
         "qq_pionrho": ([P, P, P, I, P, P, P], I),
         "qq_twvev": ([P, D, D, IP, I, I, I, I, I, P], I),
+        "qq_average": ([P, P, P, P, P, D, I, I, I, P, P], I),
         "qq_twaverage": ([P, P, P, P, P, D, D, IP, I, I, I, I, I, P], I),
         "qq_twistdiscon": ([P, I, I, DP, P, D, IP, I, I, I, I, I, P, P, P], I),
         "qq_heatbath": ([P, D, I, C.c_ulonglong, P, DP], I),
@@ -361,6 +362,16 @@ class Lattice:
         decay = np.zeros(nt) if decay is None else decay
         _check(self.lib.qq_pionrho(self._ctx, _ptr(xe), _ptr(xo), int(idsrc), _ptr(pion), _ptr(rho), _ptr(decay)))
         return pion, rho, decay
+
+    def average(self, be, bo, xe, xo, kappa, nsub=6, nmom=5, nop=9, momfac=None):
+        """average (qq_average): the Wilson loop operators of one noise at subtraction
+        levels 1..nsub; momfac in numpy shape (>= 5, nmom-1, 16, 2, nvhalf).  Returns
+        Jtime as an array (nop, nmom, nsub, nt, 2)."""
+        J = np.zeros((nop, nmom, nsub, self.dims[3], 2))
+        mf = None if momfac is None else np.ascontiguousarray(momfac, dtype=np.float64)
+        _check(self.lib.qq_average(self._ctx, _ptr(be), _ptr(bo), _ptr(xe), _ptr(xo), float(kappa), int(nsub),
+                                   int(nmom), int(nop), _ptr(mf) if mf is not None else None, _ptr(J)))
+        return J
 
     def twvev(self, kappa, delta=0.0, io=(1, 1, 1), dobndry=0, ir=1, nsub=6, nmom=5, nop=6):
         """twvev: the perturbative vacuum expectation values Jvev, as an array of shape

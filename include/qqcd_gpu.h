@@ -244,6 +244,18 @@ int qq_twistdiscon(qq_ctx* ctx, int noise_kind, int nnoise, const double kappa[2
                    int nsub, int nmom, int nop, double* Jtotal, double* Jnoise,
                    qq_solve_info* infos);
 
+/* average Q/disconloops.f90:5343-5733 (the Wilson loop driver's operators of one noise):
+ * for levels isub = 1..nsub (<= 6), the solution x (isub = 1) or x minus the hopping
+ * expansion of the propagator applied to the noise, sum_{n=0}^{isub+1} kappa^n H^n b
+ * (isub >= 2), goes through loopops (:7769-7910: point-split currents J1..J4 with the
+ * boundary factors, psibar psi with +12 on subtracted levels, local vector currents
+ * J5+mu; the complex noise kept whole) and spacesum (:9012-9124) into
+ * Jtime(2, nt, nsub, nmom, nop) (Fortran order, host or device, nop >= 9); operators
+ * 1..4 are multiplied by kappa.  momfac(nvhalf, 2, 16, nmom-1, >= 5): the caller's
+ * momentum factors (host or device; may be NULL when nmom = 1). */
+int qq_average(qq_ctx* ctx, const double* be, const double* bo, const double* xe, const double* xo,
+               double kappa, int nsub, int nmom, int nop, const double* momfac, double* Jtime);
+
 /* ---- file formats (host memory; no device needed) ----
  * Fortran unformatted sequential files, as the reference writes them: every record is
  * framed by its 4-byte length, reals are 8 bytes, integers 4.  nvhalf and ntotal are

@@ -70,6 +70,7 @@ def lib() -> C.CDLL:
             "oq_orgschur": ([IP, I, DP, I, DP, I, DP, IP], None),
             "oq_twaverage_level0": ([P, DP, DP, DP, DP, DP, D, D, C.c_int, DP], None),
             "oq_twvev": ([P, DP, D, D, IP, I, I, I, I, I, DP], None),
+            "oq_average": ([P, DP, DP, DP, DP, DP, D, I, I, I, DP, DP], None),
             "oq_twaverage_mom": ([P, DP, DP, DP, DP, DP, D, D, IP, I, I, I, DP], None),
             "oq_twvev_sites": ([P, DP, D, D, IP, I, I, I, IP, I, DP], None),
             "oq_set_kcyclim": ([I], None),
@@ -288,6 +289,18 @@ class OracleLattice:
         lib().oq_twaverage_mom(self._g, _dp(np.ascontiguousarray(be)), _dp(np.ascontiguousarray(bo)),
                                _dp(np.ascontiguousarray(xe)), _dp(np.ascontiguousarray(xo)), _dp(self.u),
                                float(kappa), float(delta), iop, int(dobndry), int(nmom), int(ir), _dp(J))
+        return J
+
+    def average(self, be, bo, xe, xo, kappa, nsub=6, nmom=5, nop=9, momfac=None):
+        """average (Q/disconloops.f90:5343-5733): the Wilson loop operators of one noise at
+        subtraction levels 1..nsub.  momfac has the reference's shape (nvhalf, 2, 16,
+        nmom-1, >= 5) in Fortran order, i.e. numpy shape (>= 5, nmom-1, 16, 2, nvhalf).
+        Returns Jtime as (nop, nmom, nsub, nt, 2)."""
+        J = np.zeros((nop, nmom, nsub, self.dims[3], 2))
+        mf = np.zeros(1) if momfac is None else np.ascontiguousarray(momfac, dtype=np.float64)
+        lib().oq_average(self._g, _dp(self.u), _dp(np.ascontiguousarray(be)), _dp(np.ascontiguousarray(bo)),
+                         _dp(np.ascontiguousarray(xe)), _dp(np.ascontiguousarray(xo)), float(kappa), int(nsub),
+                         int(nmom), int(nop), _dp(mf), _dp(J))
         return J
 
     def twvev(self, kappa, delta=0.0, io=(1, 1, 1), dobndry=0, ir=1, nsub=6, nmom=5, nop=6):

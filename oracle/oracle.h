@@ -140,6 +140,14 @@ void oq_twaverage_mom(const oq_geom* g, const double* be, const double* bo, cons
                       const double* xo, const double* u, double kappa, double delta,
                       const int io[3], int dobndry, int nmom, int ir, double* J);
 
+// ---- Wilson loop operators with subtraction levels (Q/disconloops.f90 average,
+// loopops, spacesum; see average.cpp) ----
+// Jtime(2, nt, nsub, nmom, nop), nop >= 9; momfac(nvhalf, 2, 16, nmom-1, >= 5) as the
+// reference's caller builds it (may be NULL when nmom = 1).
+void oq_average(const oq_geom* g, const double* u, const double* be, const double* bo,
+                const double* xe, const double* xo, double kappa, int nsub, int nmom, int nop,
+                const double* momfac, double* Jtime);
+
 // ---- perturbative vacuum expectation values (Q/vevbleft.f90 twvev; see vev.cpp) ----
 // Jvev(2, nt, 6, nmom, nop), Fortran order; levels 4 (orders kappa^3 / kappa^4, and
 // kappa^1 / kappa^2 when delta /= 0) and 6 (orders kappa^5 / kappa^6, nsub = 6) are

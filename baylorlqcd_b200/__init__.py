@@ -37,7 +37,7 @@ EXPORTED = [
     "qq_heatbath", "qq_ctx_stream", "qq_launch_count", "qq_profile_hop", "qq_profile_hop_read",
     "qq_gfwrite", "qq_gfread", "qq_fpwrite", "qq_fpread", "qq_hsingle_block",
     "qq_hop_tuned_shape", "qq_net_create", "qq_net_destroy", "qq_net_nweights", "qq_net_get_weights",
-    "qq_net_set_weights", "qq_net_apply", "qq_net_grad", "qq_net_train", "qq_fgmres", "qq_pionrho", "qq_twvev", "qq_twaverage", "qq_twistdiscon", "qq_average",
+    "qq_net_set_weights", "qq_net_apply", "qq_net_grad", "qq_net_train", "qq_fgmres", "qq_pionrho", "qq_twvev", "qq_twaverage", "qq_twistdiscon", "qq_average", "qq_momfacs",
     "qq_fgmresdr",
 ]
 
@@ -150,6 +150,7 @@ def load_library() -> C.CDLL:
         "qq_pionrho": ([P, P, P, I, P, P, P], I),
         "qq_twvev": ([P, D, D, IP, I, I, I, I, I, P], I),
         "qq_average": ([P, P, P, P, P, D, I, I, I, P, P], I),
+        "qq_momfacs": ([IP, IP, P], I),
         "qq_twaverage": ([P, P, P, P, P, D, D, IP, I, I, I, I, I, P], I),
         "qq_twistdiscon": ([P, I, I, DP, P, D, IP, I, I, I, I, I, P, P, P], I),
         "qq_heatbath": ([P, D, I, C.c_ulonglong, P, DP], I),
@@ -588,6 +589,18 @@ class Net:
 def launch_count() -> int:
     """Kernels launched by the library in this process so far."""
     return int(load_library().qq_launch_count())
+
+
+def momfacs(dims, io=(1, 1, 1)) -> np.ndarray:
+    """momfacs (qq_momfacs, host only): the Wilson driver's momentum factors as numpy
+    shape (5, 4, 16, 2, nvhalf), the reverse of the Fortran (nvhalf, 2, 16, 4, 5)."""
+    nv = dims[0] * dims[1] * dims[2] * dims[3] // 32
+    mf = np.zeros((5, 4, 16, 2, nv))
+    d = np.ascontiguousarray(dims, dtype=np.int32)
+    o = np.ascontiguousarray(io, dtype=np.int32)
+    _check(load_library().qq_momfacs(d.ctypes.data_as(C.POINTER(C.c_int)), o.ctypes.data_as(C.POINTER(C.c_int)),
+                                     _ptr(mf)))
+    return mf
 
 
 def initlagfib(myid: int, iseed: int):

@@ -327,3 +327,50 @@ extern "C" int qq_average(qq_ctx* c, const double* be, const double* bo, const d
   QQ_CK(cudaMemcpy(Jtime, out.data(), sizeof(double) * out.size(), cudaMemcpyDefault));
   return QQ_OK;
 }
+
+// momfacs, Q/disconloops.f90:8925-8984 (host only): the momentum factors qq_average
+// takes, momfac(nvhalf, 2, 16, 4, 5), nvhalf = nx ny nz nt / 32.  The reference's twoPi
+// is a default-kind literal, so it carries the single-precision value.
+extern "C" int qq_momfacs(const int dims[4], const int io[3], double* momfac) {
+  if (!dims || !io || !momfac) return set_error(QQ_BAD_ARG, "null argument");
+  Geom g{};
+  for (int d = 0; d < 4; ++d) {
+    if (dims[d] < 4 || dims[d] % 4 != 0) return set_error(QQ_BAD_ARG, "lattice extents must be multiples of 4");
+    g.n[d] = dims[d];
+    g.bc[d] = 1;
+  }
+  geom_finish(g);
+  const int nx = dims[0], ny = dims[1], nz = dims[2], nt = dims[3];
+  const size_t nv = (size_t)nx * ny * nz * nt / 32;
+  const double twoPi = (double)6.283185307179586f;
+  auto M = [&](int isite, int ieo, int ibl, int im, int k) -> double& {
+    return momfac[((((size_t)(k - 1) * 4 + (im - 1)) * 16 + (ibl - 1)) * 2 + (ieo - 1)) * nv + (isite - 1)];
+  };
+  for (int it = 1; it <= nt; ++it)
+    for (int iz = 1; iz <= nz; ++iz) {
+      const double dz = twoPi * (double)(iz - io[2]) / (double)nz;
+      for (int iy = 1; iy <= ny; ++iy) {
+        const double dy = twoPi * (double)(iy - io[1]) / (double)ny;
+        for (int ix = 1; ix <= nx; ++ix) {
+          const double dx = twoPi * (double)(ix - io[0]) / (double)nx;
+          const int x[4] = {ix - 1, iy - 1, iz - 1, it - 1};
+          int isite, ieo, ibleo;
+          ref_site(g, x, &isite, &ieo, &ibleo);
+          const int ibl = 1 + (x[0] & 1) + 2 * (x[1] & 1) + 4 * (x[2] & 1) + 8 * (x[3] & 1);
+          const double cx = std::cos(dx), cy = std::cos(dy), cz = std::cos(dz);
+          const double sx = std::sin(dx), sy = std::sin(dy), sz = std::sin(dz);
+          const double v[4][4] = {{sx, sy, sz, (cx + cy + cz) / 3.0},
+                                  {sx * (cy + cz) / 2.0, sy * (cx + cz) / 2.0, sz * (cx + cy) / 2.0,
+                                   (cx * cy + cx * cz + cy * cz) / 3.0},
+                                  {sx * cy * cz, sy * cx * cz, sz * cx * cy, cx * cy * cz},
+                                  {std::sin(2.0 * dx), std::sin(2.0 * dy), std::sin(2.0 * dz),
+                                   (std::cos(2.0 * dx) + std::cos(2.0 * dy) + std::cos(2.0 * dz)) / 3.0}};
+          for (int im = 1; im <= 4; ++im) {
+            for (int k = 1; k <= 4; ++k) M(isite, ieo, ibl, im, k) = v[im - 1][k - 1];
+            M(isite, ieo, ibl, im, 5) = v[im - 1][3];
+          }
+        }
+      }
+    }
+  return QQ_OK;
+}

@@ -255,6 +255,10 @@ int qq_twistdiscon(qq_ctx* ctx, int noise_kind, int nnoise, const double kappa[2
  * momentum factors (host or device; may be NULL when nmom = 1). */
 int qq_average(qq_ctx* ctx, const double* be, const double* bo, const double* xe, const double* xo,
                double kappa, int nsub, int nmom, int nop, const double* momfac, double* Jtime);
+/* momfacs Q/disconloops.f90:8925-8984 (host memory; no device needed): the momentum
+ * factors of the Wilson driver for 4 momenta about the origin io (1-based),
+ * momfac(nvhalf, 2, 16, 4, 5), nvhalf = nx*ny*nz*nt/32. */
+int qq_momfacs(const int dims[4], const int io[3], double* momfac);
 
 /* ---- file formats (host memory; no device needed) ----
  * Fortran unformatted sequential files, as the reference writes them: every record is

@@ -71,6 +71,7 @@ def lib() -> C.CDLL:
             "oq_twaverage_level0": ([P, DP, DP, DP, DP, DP, D, D, C.c_int, DP], None),
             "oq_twvev": ([P, DP, D, D, IP, I, I, I, I, I, DP], None),
             "oq_average": ([P, DP, DP, DP, DP, DP, D, I, I, I, DP, DP], None),
+            "oq_momfacs": ([P, IP, DP], None),
             "oq_twaverage_mom": ([P, DP, DP, DP, DP, DP, D, D, IP, I, I, I, DP], None),
             "oq_twvev_sites": ([P, DP, D, D, IP, I, I, I, IP, I, DP], None),
             "oq_set_kcyclim": ([I], None),
@@ -290,6 +291,13 @@ class OracleLattice:
                                _dp(np.ascontiguousarray(xe)), _dp(np.ascontiguousarray(xo)), _dp(self.u),
                                float(kappa), float(delta), iop, int(dobndry), int(nmom), int(ir), _dp(J))
         return J
+
+    def momfacs(self, io=(1, 1, 1)):
+        """momfacs (Q/disconloops.f90:8925-8984): numpy shape (5, 4, 16, 2, nvhalf)."""
+        mf = np.zeros((5, 4, 16, 2, self.nvhalf))
+        _, iop = _ip(io)
+        lib().oq_momfacs(self._g, iop, _dp(mf))
+        return mf
 
     def average(self, be, bo, xe, xo, kappa, nsub=6, nmom=5, nop=9, momfac=None):
         """average (Q/disconloops.f90:5343-5733): the Wilson loop operators of one noise at

@@ -230,3 +230,45 @@ extern "C" void oq_average(const oq_geom* g, const double* u, const double* be, 
         for (int t = 0; t < nt; ++t)
           for (int ri = 0; ri < 2; ++ri) J(ri, t, isub, im, iop) = kappa * J(ri, t, isub, im, iop);
 }
+
+// momfacs, Q/disconloops.f90:8925-8984: the momentum factors spacesum takes,
+// momfac(nvhalf, 2, 16, 4, 5) for imom - 1 = 1..4, components 1..3 sine-type along
+// x, y, z and 4 cosine-type, component 5 a copy of 4, about the origin io (1-based).
+// twoPi is a default-kind literal in the reference, so its value is single precision.
+extern "C" void oq_momfacs(const oq_geom* g, const int io[3], double* momfac) {
+  const int nx = g->n[0], ny = g->n[1], nz = g->n[2], nt = g->n[3], nv = g->nvhalf;
+  const double twoPi = (double)6.283185307179586f;
+  auto M = [&](int isite, int ieo, int ibl, int im, int k) -> double& {
+    return momfac[((((size_t)(k - 1) * 4 + (im - 1)) * 16 + (ibl - 1)) * 2 + (ieo - 1)) * nv + (isite - 1)];
+  };
+  for (int it = 1; it <= nt; ++it)
+    for (int iz = 1; iz <= nz; ++iz) {
+      const double dz = twoPi * (double)(iz - io[2]) / (double)nz;
+      for (int iy = 1; iy <= ny; ++iy) {
+        const double dy = twoPi * (double)(iy - io[1]) / (double)ny;
+        for (int ix = 1; ix <= nx; ++ix) {
+          const double dx = twoPi * (double)(ix - io[0]) / (double)nx;
+          const int xc[4] = {ix - 1, iy - 1, iz - 1, it - 1};
+          int isite, ieo, ibl, gblclr, ibleo;
+          oq_site_of_coords(g, xc, &isite, &ieo, &ibl, &gblclr, &ibleo);
+          M(isite, ieo, ibl, 1, 1) = std::sin(dx);
+          M(isite, ieo, ibl, 1, 2) = std::sin(dy);
+          M(isite, ieo, ibl, 1, 3) = std::sin(dz);
+          M(isite, ieo, ibl, 1, 4) = (std::cos(dx) + std::cos(dy) + std::cos(dz)) / 3.0;
+          M(isite, ieo, ibl, 2, 1) = std::sin(dx) * (std::cos(dy) + std::cos(dz)) / 2.0;
+          M(isite, ieo, ibl, 2, 2) = std::sin(dy) * (std::cos(dx) + std::cos(dz)) / 2.0;
+          M(isite, ieo, ibl, 2, 3) = std::sin(dz) * (std::cos(dx) + std::cos(dy)) / 2.0;
+          M(isite, ieo, ibl, 2, 4) = (std::cos(dx) * std::cos(dy) + std::cos(dx) * std::cos(dz) + std::cos(dy) * std::cos(dz)) / 3.0;
+          M(isite, ieo, ibl, 3, 1) = std::sin(dx) * std::cos(dy) * std::cos(dz);
+          M(isite, ieo, ibl, 3, 2) = std::sin(dy) * std::cos(dx) * std::cos(dz);
+          M(isite, ieo, ibl, 3, 3) = std::sin(dz) * std::cos(dx) * std::cos(dy);
+          M(isite, ieo, ibl, 3, 4) = std::cos(dx) * std::cos(dy) * std::cos(dz);
+          M(isite, ieo, ibl, 4, 1) = std::sin(2.0 * dx);
+          M(isite, ieo, ibl, 4, 2) = std::sin(2.0 * dy);
+          M(isite, ieo, ibl, 4, 3) = std::sin(2.0 * dz);
+          M(isite, ieo, ibl, 4, 4) = (std::cos(2.0 * dx) + std::cos(2.0 * dy) + std::cos(2.0 * dz)) / 3.0;
+          for (int im = 1; im <= 4; ++im) M(isite, ieo, ibl, im, 5) = M(isite, ieo, ibl, im, 4);
+        }
+      }
+    }
+}

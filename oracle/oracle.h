@@ -148,6 +148,9 @@ void oq_average(const oq_geom* g, const double* u, const double* be, const doubl
                 const double* xe, const double* xo, double kappa, int nsub, int nmom, int nop,
                 const double* momfac, double* Jtime);
 
+// momfacs: momfac(nvhalf, 2, 16, 4, 5) about the origin io (1-based).
+void oq_momfacs(const oq_geom* g, const int io[3], double* momfac);
+
 // ---- perturbative vacuum expectation values (Q/vevbleft.f90 twvev; see vev.cpp) ----
 // Jvev(2, nt, 6, nmom, nop), Fortran order; levels 4 (orders kappa^3 / kappa^4, and
 // kappa^1 / kappa^2 when delta /= 0) and 6 (orders kappa^5 / kappa^6, nsub = 6) are

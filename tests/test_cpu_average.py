@@ -86,3 +86,15 @@ def test_average_closed_form():
     assert np.abs(got - want).max() <= 1e-12 * np.abs(want).max()
     # every level differs (the subtraction is active) and each operator is exercised
     assert np.all(np.abs(np.diff(got[:9, 0], axis=1)).max(axis=(1, 2)) > 0)
+
+
+def test_momfacs_library_matches_oracle():
+    """qq_momfacs (host code of the library) against the oracle's literal restatement
+    of momfacs (Q/disconloops.f90:8925-8984): bit for bit, two origins, two shapes."""
+    import baylorlqcd_b200 as qq
+
+    for dims, io in [((4, 4, 4, 8), (1, 1, 1)), ((8, 4, 4, 8), (3, 2, 4))]:
+        ol = oracle.OracleLattice(*dims, bc=BC)
+        assert np.array_equal(qq.momfacs(dims, io), ol.momfacs(io))
+        mf = ol.momfacs(io)
+        assert np.array_equal(mf[4], mf[3]) and np.abs(mf).max() > 0

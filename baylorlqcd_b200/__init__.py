@@ -29,9 +29,9 @@ STATUS_NAMES = {0: "OK", 1: "NOT_CONVERGED", 2: "NAN", 3: "BAD_ARG", 4: "CUDA_ER
 # Every symbol of include/qqcd_gpu.h
 EXPORTED = [
     "qq_ctx_create", "qq_ctx_destroy", "qq_ctx_dims", "qq_last_error", "qq_set_coact",
-    "qq_gauge_upload", "qq_hsingle", "qq_hdouble", "qq_hdbletm", "qq_twmshift", "qq_vecdot",
+    "qq_gauge_upload", "qq_hsingle", "qq_hdouble", "qq_hdbletm", "qq_twmshift", "qq_gamma5mult", "qq_vecdot",
     "qq_vecdot_noalloc",
-    "qq_defl_create", "qq_defl_destroy", "qq_defl_size", "qq_gmresdr", "qq_gmresproj", "qq_psc",
+    "qq_defl_create", "qq_defl_destroy", "qq_defl_size", "qq_gmresdr", "qq_gmresproj", "qq_gmresdrshift", "qq_psc",
     "qq_bicgstab", "qq_fermprop", "qq_pointsource", "qq_fermprop_batch", "qq_initlagfib",
     "qq_rnds", "qq_z2source", "qq_z4source", "qq_twaverage_level0", "qq_discon_traces", "qq_bench_hsingle",
     "qq_heatbath", "qq_ctx_stream", "qq_launch_count", "qq_profile_hop", "qq_profile_hop_read",
@@ -116,6 +116,7 @@ def load_library() -> C.CDLL:
         "qq_hdouble": ([P, P, P, I, D], I),
         "qq_hdbletm": ([P, P, P, I, DP, I], I),
         "qq_twmshift": ([P, P, P, I, DP, I], I),
+        "qq_gamma5mult": ([P, P, P, I, DP, I], I),
         "qq_vecdot": ([P, P, P, DP], I),
         "qq_vecdot_noalloc": ([P, P, P, DP], I),
         "qq_defl_create": ([P, I, I, C.POINTER(P)], I),
@@ -123,6 +124,7 @@ def load_library() -> C.CDLL:
         "qq_defl_size": ([P], I),
         "qq_gmresdr": ([P, P, P, IP, D, I, DP, I, P, C.POINTER(qq_solve_info)], I),
         "qq_gmresproj": ([P, P, P, IP, D, I, DP, I, P, C.POINTER(qq_solve_info)], I),
+        "qq_gmresdrshift": ([P, P, P, I, P, IP, D, I, DP, I, P, C.POINTER(qq_solve_info)], I),
         "qq_psc": ([P, P, P, IP, D, I, DP, I, I, P, C.POINTER(qq_solve_info)], I),
         "qq_bicgstab": ([P, P, P, D, I, DP, I, I, C.POINTER(qq_solve_info)], I),
         "qq_fermprop": ([P, P, P, DP, I, D, I, IP, P, P, I, I, P, C.POINTER(qq_solve_info)], I),
@@ -331,6 +333,12 @@ class Lattice:
         _check(self.lib.qq_twmshift(self._ctx, _ptr(out), _ptr(gwhole), idag, _d2(kappa), iflag))
         return out
 
+    def gamma5mult(self, ge, idag: int, kappa, iflag: int = -1, out=None):
+        """gamma5mult (Q/diracops.f90:1750-1860): -i gamma5 Hdbletm(ge) / (2 kappa mu)."""
+        out = self.new_half() if out is None else out
+        _check(self.lib.qq_gamma5mult(self._ctx, _ptr(out), _ptr(ge), idag, _d2(kappa), iflag))
+        return out
+
     def vecdot(self, a, b) -> complex:
         r = (C.c_double * 2)()
         _check(self.lib.qq_vecdot(self._ctx, _ptr(a), _ptr(b), r))
@@ -405,6 +413,20 @@ class Lattice:
                                    _d2(kappa), iflag, defl._h, C.byref(info))
         _check(st, allow_not_converged=True)
         return x, SolveInfo.from_c(info)
+
+    def gmresdrshift(self, b, sigma, GMRES, resmax, itermin=0, kappa=(0.15, 0.01), iflag=-1):
+        """gmresdrshift (Q/inverters.f90:6041-7179): solutions of (A - sigma_s) x_s = b for
+        every shift, A = gamma5mult, from one deflated Krylov space.  Returns
+        (x[nshifts, ...], resid[nshifts] (absolute), SolveInfo)."""
+        sig = np.ascontiguousarray(sigma, dtype=np.float64)
+        ns = int(sig.shape[0])
+        x = np.zeros((ns,) + self.half_shape)
+        resid = np.zeros(ns)
+        info = qq_solve_info()
+        st = self.lib.qq_gmresdrshift(self._ctx, _ptr(b), _ptr(x), ns, _ptr(sig), _i2(GMRES), float(resmax),
+                                      itermin, _d2(kappa), iflag, _ptr(resid), C.byref(info))
+        _check(st, allow_not_converged=True)
+        return x, resid, SolveInfo.from_c(info)
 
     def psc(self, b, x, GMRES, resmax, itermin=0, kappa=(0.15, 0.0), iflag=-1, isignal=1, defl=None):
         info = qq_solve_info()

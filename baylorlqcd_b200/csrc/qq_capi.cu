@@ -229,6 +229,56 @@ int qq_twmshift(qq_ctx* c, double* hwhole, const double* gwhole, int idag, const
   return store_half(c, 3, ho.sp(), 1, hwhole + nv);
 }
 
+// gamma5mult (Q/diracops.f90:1750-1860): he = -i gamma5 Hdbletm'(ge) / (2 kappa mu), with
+// Hdbletm' the twisted form for every mu /= 0.  iflag must be -1 (the reference stops on
+// the clover flag).
+int qq_gamma5mult(qq_ctx* c, double* he, const double* ge, int idag, const double kappa[2], int iflag) {
+  QQ_TRY(check_ctx(c));
+  QQ_TRY(set_device(c));
+  if (iflag != -1) return set_error(QQ_BAD_ARG, "gamma5mult: iflag must be -1 (no clover term)");
+  if (!he || !ge || !kappa) return set_error(QQ_BAD_ARG, "null argument");
+  if (idag != 0 && idag != 1) return set_error(QQ_BAD_ARG, "idag must be 0 or 1");
+  Tmp in(c, P64), out(c, P64), tmp(c, P64);
+  QQ_TRY(load_half(c, 1, ge, 0, in.sp()));
+  QQ_TRY(op_g5mult(c, out.sp(), in.sp(), tmp.sp(), idag, kappa, 0.0));
+  return store_half(c, 2, out.sp(), 0, he);
+}
+
+// gmresdrshift (Q/inverters.f90:6041-7179) with the shifts as an argument.
+int qq_gmresdrshift(qq_ctx* c, const double* b, double* xshift, int nshifts, const double* sigma,
+                    const int GMRES[2], double resmax, int itermin, const double kappa[2], int iflag,
+                    double* resid, qq_solve_info* info) {
+  QQ_TRY(check_ctx(c));
+  QQ_TRY(set_device(c));
+  if (iflag != -1) return set_error(QQ_BAD_ARG, "gmresdrshift: iflag must be -1 (no clover term)");
+  if (!b || !xshift || !sigma || !GMRES || !kappa || !resid) return set_error(QQ_BAD_ARG, "null argument");
+  if (nshifts < 1 || nshifts > 512) return set_error(QQ_BAD_ARG, "nshifts must be in 1..512");
+  for (int q = 0; q < nshifts; ++q)
+    if (!std::isfinite(sigma[q])) return set_error(QQ_BAD_ARG, "shift is not finite");
+  const double t = 2.0 * kappa[0] * kappa[1];
+  if (!(t != 0.0) || !std::isfinite(1.0 / t)) return set_error(QQ_BAD_ARG, "gmresdrshift needs kappa*mu /= 0");
+  Tmp fb(c, P64);
+  QQ_TRY(load_half(c, 1, b, 0, fb.sp()));
+  std::vector<std::unique_ptr<Tmp>> fx, fr;
+  std::vector<Spinor> xs, rs;
+  for (int q = 0; q < nshifts; ++q) {
+    fx.emplace_back(new Tmp(c, P64));
+    fr.emplace_back(new Tmp(c, P64));
+    xs.push_back(fx.back()->sp());
+    rs.push_back(fr.back()->sp());
+  }
+  Timer tm(c);
+  SolveStats st;
+  int status = gmresdrshift_fp64(c, fb.sp(), xs, rs, sigma, GMRES[0], GMRES[1], resmax, itermin, kappa,
+                                 resid, &st);
+  const double sec = tm.seconds();
+  fill_info(info, status, st, sec);
+  if (status != QQ_OK && status != QQ_NOT_CONVERGED) return status;
+  const size_t nv = c->ref_doubles();
+  for (int q = 0; q < nshifts; ++q) QQ_TRY(store_half(c, 3, xs[q], 0, xshift + (size_t)q * nv));
+  return status;
+}
+
 int qq_vecdot(qq_ctx* c, const double* a, const double* b, double adb[2]) {
   QQ_TRY(check_ctx(c));
   QQ_TRY(set_device(c));

@@ -138,6 +138,9 @@ int op_hsingle(qq_ctx* c, Spinor out, Spinor in, int idag, int pout);
 int op_hsingle_multi(qq_ctx* c, const Spinor* out, const Spinor* in, int n, int idag, int pout);
 // he = Hdbletm(ge), tmp is an odd-parity temporary of the same precision.
 int op_dbletm(qq_ctx* c, Spinor out, Spinor in, Spinor tmp, int idag, const double kappa[2]);
+// out = gamma5mult(in) - sigma in (Q/diracops.f90:1750-1860), tmp odd-parity.
+int op_g5mult(qq_ctx* c, Spinor out, Spinor in, Spinor tmp, int idag, const double kappa[2],
+              double sigma);
 int op_dbletm_multi(qq_ctx* c, const Spinor* out, const Spinor* in, const Spinor* tmp, int n,
                     int idag, const double kappa[2]);
 // RHS-interleaved block fields of nb right-hand sides (element (q, s, r) at
@@ -179,6 +182,11 @@ struct SolveStats {
 // Reference-faithful FP64 GMRES-DR (Q/inverters.f90:2871-3572 semantics).
 int gmresdr_fp64(qq_ctx* c, Spinor phi, Spinor x, int m, int k, double resmax, int itermin,
                  const double kappa[2], DeflSpace* defl, SolveStats* st);
+// Multi-shift GMRES-DR on gamma5mult (Q/inverters.f90:6041-7179): xs/rs hold one solution
+// and one residual field per shift; resid receives ||r_s||.
+int gmresdrshift_fp64(qq_ctx* c, Spinor b, const std::vector<Spinor>& xs, const std::vector<Spinor>& rs,
+                      const double* sigma, int m, int k, double resmax, int itermin, const double kappa[2],
+                      double* resid, SolveStats* st);
 int gmresproj_fp64(qq_ctx* c, Spinor b, Spinor x, int m, int k, double resmax, int itermin,
                    const double kappa[2], const DeflSpace& defl, SolveStats* st);
 int bicgstab_fp64(qq_ctx* c, Spinor phi, Spinor x, double resmax, int itermin, int maxiter,

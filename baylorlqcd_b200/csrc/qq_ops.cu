@@ -1,5 +1,6 @@
 // Operator application, level-1 helpers and reference-layout staging for the C ABI.
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <string>
 
@@ -336,6 +337,43 @@ int op_dbletm_block_impl(qq_ctx* c, Spinor out, Spinor in, Spinor tmp, int nb, i
     }
   }
   return launch_hop_tuned(c, b, prec, EPI_DBLE);
+}
+
+// gamma5mult (Q/diracops.f90:1750-1860) minus a real shift:
+//   out = -i gamma5 [ (1 + 2 i kappa mu gamma5)/kappa^2
+//                     - H_eo (1 - 2 i kappa mu gamma5) H_oe / (1 + 4 kappa^2 mu^2) ] in / (2 kappa mu)
+//         - sigma in.
+// The bracket is Hdbletm's twisted form for every mu /= 0 (Hdbletm itself switches to
+// Hdouble below mu = 1e-8, gamma5mult does not).  -i gamma5 takes the spins
+// (v0, v1, v2, v3) to (-v2, -v3, v0, v1), which is -J of the spin-mixing kernel.
+int op_g5mult(qq_ctx* c, Spinor out, Spinor in, Spinor tmp, int idag, const double kappa[2],
+              double sigma) {
+  if (!c->have_gauge) return set_error(QQ_BAD_ARG, "no gauge field uploaded");
+  const double t = 2.0 * kappa[0] * kappa[1];
+  if (!(t != 0.0) || !std::isfinite(1.0 / t)) return set_error(QQ_BAD_ARG, "gamma5mult needs kappa*mu /= 0");
+  const int prec = in.prec;
+  HopArgs a = hop_base(c, idag, 1, prec);
+  a.nrhs = 1;
+  a.in[0] = in.data;
+  a.in_norm[0] = in.norm;
+  a.out[0] = tmp.data;
+  a.out_norm[0] = tmp.norm;
+  a.a = t;
+  QQ_TRY(launch_hop_tuned(c, a, prec, EPI_TWIST));
+  HopArgs b = hop_base(c, idag, 0, prec);
+  b.nrhs = 1;
+  b.in[0] = tmp.data;
+  b.in_norm[0] = tmp.norm;
+  b.out[0] = out.data;
+  b.out_norm[0] = out.norm;
+  b.aux[0] = in.data;
+  b.aux_norm[0] = in.norm;
+  b.f1 = 1.0 / (kappa[0] * kappa[0]);
+  b.f2 = 2.0 * kappa[1] / kappa[0];
+  b.f3 = 1.0 / (1.0 + t * t);
+  QQ_TRY(launch_hop_tuned(c, b, prec, EPI_DBLE));
+  QQ_CK(launch_spinmix(c->g.vh, in, out, out, -sigma, 0.0, 0.0, -1.0 / t, prec, c->st));
+  return QQ_OK;
 }
 
 int op_dbletm(qq_ctx* c, Spinor out, Spinor in, Spinor tmp, int idag, const double kappa[2]) {

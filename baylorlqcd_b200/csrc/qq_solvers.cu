@@ -2,6 +2,7 @@
 //
 //   GMRES-DR(m,k)   Q/inverters.f90:2871-3572  (Morgan 2002)
 //   GMRES-Proj      Q/inverters.f90:7183-8304
+//   GMRES-DR-shift  Q/inverters.f90:6041-7179 (multi-shift, on gamma5mult)
 //   BiCGStab        Q/inverters.f90:302-487
 //
 // The Krylov basis lives in HBM in the GPU spinor layout.  Arnoldi orthogonalisation
@@ -22,6 +23,7 @@ namespace qq {
 namespace {
 
 constexpr int kCycleLimit = 5000;  // kcyclim, U/latdims.f90:70
+constexpr int kMaxShifts = 512;   // per-shift norms live in the 1024-double scalar buffer
 
 struct Arnoldi {
   qq_ctx* c;
@@ -29,6 +31,9 @@ struct Arnoldi {
   int m;         // Krylov dimension (m+1 vectors)
   size_t nel;    // 16-byte elements per vector
   DevBuf V, H, hscr, y;
+  // Krylov operator: Hdbletm, or gamma5mult - g5shift (gmresdrshift)
+  bool g5 = false;
+  double g5shift = 0.0;
   int init(qq_ctx* c_, int pb_, int m_) {
     c = c_;
     pb = pb_;
@@ -54,7 +59,10 @@ struct Arnoldi {
 // for GMRES, the preconditioned z_j = M v_j for flexible GMRES.
 int arnoldi_step_from(Arnoldi& A, int j, Spinor src, Spinor tmp_odd, const double kappa[2], double* nrm2_slot) {
   qq_ctx* c = A.c;
-  QQ_TRY(op_dbletm(c, A.sp(j + 1), src, tmp_odd, 0, kappa));
+  if (A.g5)
+    QQ_TRY(op_g5mult(c, A.sp(j + 1), src, tmp_odd, 0, kappa, A.g5shift));
+  else
+    QQ_TRY(op_dbletm(c, A.sp(j + 1), src, tmp_odd, 0, kappa));
   double* part = c->partial.as<double>();
   const int nv = j + 1;
   int ng = 0;
@@ -381,6 +389,123 @@ int gmresdr_fp64(qq_ctx* c, Spinor phi, Spinor x, int m, int k, double resmax, i
     QQ_CK(defl->V.alloc((size_t)(k + 1) * A.nel * 16));
     QQ_CK(cudaMemcpyAsync(defl->V.p, A.V.p, (size_t)(k + 1) * A.nel * 16, cudaMemcpyDeviceToDevice, c->st));
     defl->Hk = Hk_last;
+  }
+  QQ_CK(cudaStreamSynchronize(c->st));
+  return status;
+}
+
+// ---------------------------------------------------------------------------
+// Multi-shift GMRES-DR (gmresdrshift, inverters.f90:6041-7179; Darnell, Morgan and
+// Wilcox 2008): (A - sigma_s) x_s = b for every shift s, A = gamma5mult.  Arnoldi and
+// the deflated restart run on A - sigma_0.  At the end of each cycle the base system
+// takes the least-squares solution y, and each further shift solves
+//   [Hbar + (sigma_0 - sigma_s) I~ | srv] (d_s, alpha_s) = cmult_s c      (:6576-6747)
+// so that its residual stays alpha_s times the base residual; cmult_s <- alpha_s.
+// Each x_s += V d_s and r_s -= (A - sigma_s) V d_s (:6816-6830).  Stops when
+// ||r_0|| < resmax (absolute, :6865).  Zero initial guess for every shift.
+// ---------------------------------------------------------------------------
+int gmresdrshift_fp64(qq_ctx* c, Spinor b, const std::vector<Spinor>& xs, const std::vector<Spinor>& rs,
+                      const double* sigma, int m, int k, double resmax, int itermin, const double kappa[2],
+                      double* resid, SolveStats* st) {
+  const int ns = (int)xs.size();
+  if (m < 2 || k < 1 || k >= m || m > 127) return set_error(QQ_BAD_ARG, "GMRES(n,k) out of range");
+  constexpr int kNormSlot = 32;  // per-shift ||r_s||^2 in c->scal[32 .. 32 + ns)
+  if (ns < 1 || ns > kMaxShifts || (int)rs.size() != ns)
+    return set_error(QQ_BAD_ARG, "nshifts must be in 1..512");
+  Arnoldi A;
+  QQ_TRY(A.init(c, P64, m));
+  A.g5 = true;
+  A.g5shift = sigma[0];
+  Tmp tmp(c, P64), xb(c, P64), h(c, P64);
+  double* nrm2 = c->scal.as<double>() + 8;
+  double* s = c->scal.as<double>();
+  double n2 = 0.0;
+  QQ_TRY(lin(c, A.sp(0), cimm(1.0), b, cimm(0), Spinor{nullptr, nullptr, P64}, cimm(0),
+             Spinor{nullptr, nullptr, P64}, s));
+  QQ_TRY(read_scalars(c, s, 1, &n2));
+  const double normnum = std::sqrt(n2);
+  for (int q = 0; q < ns; ++q) {
+    QQ_TRY(zero_field(c, xs[q]));
+    QQ_TRY(lin(c, rs[q], cimm(1.0), b));
+    resid[q] = normnum;
+  }
+  if (!std::isfinite(normnum)) return set_error(QQ_NAN, "NaN in the right-hand side");
+  if (!(normnum > 0.0)) return QQ_OK;
+  QQ_TRY(lin(c, A.sp(0), cimm(1.0 / normnum), A.sp(0)));
+  std::vector<dense::cd> cvec(m + 1, 0.0), cmult(ns, 1.0);
+  cvec[0] = normnum;
+  QQ_TRY(A.zeroH());
+  int j0 = 0, icycle = 1, status = QQ_NOT_CONVERGED;
+  for (;;) {
+    for (int j = j0; j < m; ++j) {
+      QQ_TRY(arnoldi_step(A, j, tmp.sp(), kappa, nrm2));
+      st->itercount += 1;
+      st->mvp += 1;
+    }
+    dense::Mat Hb;
+    QQ_TRY(read_H(A, m, Hb));
+    std::vector<dense::cd> y, srv;
+    dense::hess_lsq(Hb, cvec, m, y, srv);
+    for (int q = 0; q < ns; ++q) {
+      std::vector<dense::cd> d;
+      if (q == 0) {
+        d = y;
+      } else {
+        dense::Mat M(m + 1, m + 1);
+        for (int jj = 0; jj < m; ++jj)
+          for (int i = 0; i <= m; ++i) M(i, jj) = Hb(i, jj);
+        for (int jj = 0; jj < m; ++jj) M(jj, jj) += sigma[0] - sigma[q];
+        for (int i = 0; i <= m; ++i) M(i, m) = srv[i];
+        std::vector<dense::cd> rhs(m + 1);
+        for (int i = 0; i <= m; ++i) rhs[i] = cmult[q] * cvec[i];
+        if (!dense::lu_solve(M, rhs)) return set_error(QQ_SINGULAR, "shifted collinear system singular");
+        d.assign(rhs.begin(), rhs.begin() + m);
+        cmult[q] = rhs[m];
+      }
+      QQ_TRY(upload_cvec(c, d, A.y.as<double>()));
+      QQ_TRY(zero_field(c, xb.sp()));
+      QQ_CK(launch_basis_accum(P64, A.basis(), m, A.y.as<double>(), c->g.vh, xb.sp(), c->st));
+      QQ_TRY(lin(c, xs[q], cimm(1.0), xs[q], cimm(1.0), xb.sp()));
+      QQ_TRY(op_g5mult(c, h.sp(), xb.sp(), tmp.sp(), 0, kappa, sigma[q]));
+      st->mvp += 1;
+      QQ_TRY(lin(c, rs[q], cimm(1.0), rs[q], cimm(-1.0), h.sp(), cimm(0), Spinor{nullptr, nullptr, P64},
+                 s + kNormSlot + q));
+    }
+    std::vector<double> r2(ns);
+    QQ_TRY(read_scalars(c, s + kNormSlot, ns, r2.data()));
+    for (int q = 0; q < ns; ++q) resid[q] = std::sqrt(r2[q]);
+    const double rel = resid[0] / normnum;
+    st->hist.push_back(rel);
+    st->hist_mvp.push_back(st->mvp);
+    st->true_rel = rel;
+    st->ncycles = icycle;
+    if (!std::isfinite(resid[0])) {
+      status = set_error(QQ_NAN, "NaN residual in gmresdrshift");
+      break;
+    }
+    if (resid[0] < resmax && st->itercount >= itermin) {
+      status = QQ_OK;
+      break;
+    }
+    if (icycle >= kCycleLimit) break;
+    dense::Mat P, Hk;
+    std::vector<dense::cd> cnew, ritz;
+    if (!dense::gmresdr_restart(Hb, srv, m, k, P, Hk, cnew, ritz)) {
+      status = set_error(QQ_SINGULAR, "harmonic Ritz step failed");
+      break;
+    }
+    st->ritz = ritz;
+    DevBuf Pd;
+    QQ_CK(Pd.alloc(sizeof(double) * 2 * (size_t)(m + 1) * (k + 1)));
+    QQ_TRY(upload_mat(c, P, Pd.as<double>(), m + 1));
+    QQ_CK(launch_rotate(P64, A.basis(), m + 1, k + 1, Pd.as<double>(), m + 1, c->st));
+    QQ_TRY(reorth(A, k, nrm2));
+    QQ_TRY(A.zeroH());
+    QQ_TRY(upload_mat(c, Hk, A.H.as<double>(), m + 1));
+    std::fill(cvec.begin(), cvec.end(), 0.0);
+    for (int i = 0; i <= k; ++i) cvec[i] = cnew[i];
+    j0 = k;
+    icycle += 1;
   }
   QQ_CK(cudaStreamSynchronize(c->st));
   return status;

@@ -8,6 +8,8 @@
     python -m baylorlqcd_b200.probe twvev [--dims 16,16,16,16] [--nsub 6] [--reps 3]
     python -m baylorlqcd_b200.probe discon [--dims 16,16,16,32] [--nnoise 24] [--kappa 0.1565]
                                            [--mu 0.0] [--solver 1] [--nsub 6]
+    python -m baylorlqcd_b200.probe shift [--dims 16,16,16,32] [--kappa 0.1566] [--mu 0.005]
+                                          [--shifts 0,-0.099,-0.199,-0.3,-0.5] [--m 40] [--k 12]
 
 ``hop`` times one hopping-kernel shape (qq_bench_hsingle: random fields, L2 flushed
 between launches unless --no-flush) and prints its time and algorithmic bandwidth.
@@ -120,6 +122,40 @@ def run_discon(a):
     lat.close()
 
 
+def run_shift(a):
+    """gmresdrshift (qq_gmresdrshift) on a heatbath configuration: one multi-shift solve
+    of a unit-norm Z(4) noise for every shift (in units of 1/kappa^2), then each shift
+    solved alone, timed with the library's own solve timer.  Prints seconds, operator
+    applications and the largest residual of both."""
+    import baylorlqcd_b200 as qq
+
+    dims = _dims(a.dims)
+    lat = qq.Lattice(*dims, bc=(1, 1, 1, -1))
+    lat.heatbath(6.0, a.sweeps, seed=3)
+    kappa = (a.kappa, a.mu)
+    sig = np.array([float(x) for x in a.shifts.split(",")]) / a.kappa**2
+    qq.initlagfib(0, 5)
+    be, _ = lat.z4source()
+    be /= np.sqrt(lat.vecdot(be, be).real)
+    G = (a.m, a.k)
+    lat.gmresdrshift(be, sig[:2], (8, 2), 1e-3, kappa=kappa)  # warm-up (tuning)
+    x, resid, info = lat.gmresdrshift(be, sig, G, a.tol, kappa=kappa)
+    print("gmresdrshift", dims, "kappa", kappa, "GMRES", G, "shifts", len(sig), "seconds %.3f" % info.seconds,
+          "mvp", info.mvp, "cycles", info.ncycles, "max resid %.2e" % resid.max(),
+          "status", info.status, flush=True)
+    tot, mvp, worst = 0.0, 0, 0.0
+    for s in range(len(sig)):
+        _, r1, i1 = lat.gmresdrshift(be, sig[s:s + 1], G, a.tol, kappa=kappa)
+        tot += i1.seconds
+        mvp += i1.mvp
+        worst = max(worst, r1[0])
+        print("  alone: shift %+.3f/kappa^2 seconds %.3f mvp %d status %d" % (sig[s] * a.kappa**2, i1.seconds,
+                                                                           i1.mvp, i1.status), flush=True)
+    print("separate solves: seconds %.3f mvp %d max resid %.2e; multi-shift speed-up %.2f" %
+          (tot, mvp, worst, tot / info.seconds), flush=True)
+    lat.close()
+
+
 def main(argv=None) -> int:
     p = argparse.ArgumentParser(prog="python -m baylorlqcd_b200.probe")
     sub = p.add_subparsers(dest="cmd", required=True)
@@ -149,8 +185,17 @@ def main(argv=None) -> int:
     d.add_argument("--solver", type=int, default=1)
     d.add_argument("--nsub", type=int, default=6)
     d.add_argument("--sweeps", type=int, default=200)
+    f = sub.add_parser("shift")
+    f.add_argument("--dims", default="16,16,16,32")
+    f.add_argument("--kappa", type=float, default=0.1566)
+    f.add_argument("--mu", type=float, default=0.005)
+    f.add_argument("--shifts", default="0,-0.099,-0.199,-0.3,-0.5")
+    f.add_argument("--m", type=int, default=40)
+    f.add_argument("--k", type=int, default=12)
+    f.add_argument("--tol", type=float, default=1e-10)
+    f.add_argument("--sweeps", type=int, default=200)
     a = p.parse_args(argv)
-    {"hop": run_hop, "solve": run_solve, "twvev": run_twvev, "discon": run_discon}[a.cmd](a)
+    {"hop": run_hop, "solve": run_solve, "twvev": run_twvev, "discon": run_discon, "shift": run_shift}[a.cmd](a)
     return 0
 
 

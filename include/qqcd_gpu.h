@@ -103,6 +103,11 @@ int qq_hdbletm(qq_ctx* ctx, double* he, const double* ge, int idag, const double
  * by the gblclr = 2 half (each 6*ntotal*64 doubles). */
 int qq_twmshift(qq_ctx* ctx, double* hwhole, const double* gwhole, int idag,
                 const double kappa[2], int iflag);
+/* gamma5mult :1750-1860, iflag = -1: he = -i gamma5 [(1 + 2 i kappa mu gamma5)/kappa^2
+ * - H_eo (1 - 2 i kappa mu gamma5) H_oe / (1 + 4 kappa^2 mu^2)] ge / (2 kappa mu),
+ * even half in, even half out; kappa[0]*kappa[1] must not be 0. */
+int qq_gamma5mult(qq_ctx* ctx, double* he, const double* ge, int idag, const double kappa[2],
+                  int iflag);
 /* vecdot Q/inverters.f90:13485-13530: adb = sum a^dagger b (FP64). */
 int qq_vecdot(qq_ctx* ctx, const double* a, const double* b, double adb[2]);
 /* No counterpart in the reference: vecdot for callers that must not allocate device
@@ -142,6 +147,20 @@ int qq_gmresproj(qq_ctx* ctx, const double* b, double* x, const int GMRES[2], do
 int qq_psc(qq_ctx* ctx, const double* b, double* x, const int GMRES[2], double resmax,
            int itermin, const double kappa[2], int iflag, int isignal, qq_defl* defl,
            qq_solve_info* info);
+/* gmresdrshift :6041-7179 (Darnell, Morgan and Wilcox multi-shift GMRES-DR): solves
+ * (A - sigma[s]) x_s = b for s = 0..nshifts-1, A = gamma5mult (qq_gamma5mult), with one
+ * Krylov space: GMRES-DR(GMRES[0], GMRES[1]) on A - sigma[0], every other shift kept with a
+ * residual collinear to the base residual.  xshift: nshifts consecutive even-half arrays
+ * in the reference layout, written on exit (the initial guess is zero for every shift).
+ * resid[s] = ||b - (A - sigma[s]) x_s|| (absolute, recursively updated as in the
+ * reference); the iteration stops when resid[0] < resmax.  The reference leaves its
+ * local sigma unassigned and forms the shifted solutions only when j reaches its
+ * compile-time nmaxGMRES; here the shifts are an argument and the solutions are formed
+ * at the end of every cycle.  iflag must be -1; kappa[0]*kappa[1] must not be 0.
+ * Returns QQ_NOT_CONVERGED after 5000 cycles (kcyclim). */
+int qq_gmresdrshift(qq_ctx* ctx, const double* b, double* xshift, int nshifts, const double* sigma,
+                    const int GMRES[2], double resmax, int itermin, const double kappa[2], int iflag,
+                    double* resid, qq_solve_info* info);
 /* bicgstab :302-487.  maxiter <= 0 means no limit beyond the reference's. */
 int qq_bicgstab(qq_ctx* ctx, const double* phi, double* x, double resmax, int itermin,
                 const double kappa[2], int iflag, int maxiter, qq_solve_info* info);

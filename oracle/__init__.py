@@ -52,6 +52,7 @@ def lib() -> C.CDLL:
             "oq_hdouble": ([P, DP, DP, DP, I, D], None),
             "oq_hdbletm": ([P, DP, DP, DP, I, DP], None),
             "oq_twmshift": ([P, DP, DP, DP, I, DP], None),
+            "oq_gamma5mult": ([P, DP, DP, DP, I, DP], None),
             "oq_gam5x": ([P, DP], None),
             "oq_gamma5vector": ([P, DP, I], None),
             "oq_vecdot": ([P, DP, DP, DP], None),
@@ -59,6 +60,7 @@ def lib() -> C.CDLL:
             "oq_defl_destroy": ([P], None),
             "oq_defl_get": ([P, I, DP, DP], None),
             "oq_gmresdr": ([P, DP, DP, IP, D, I, DP, DP, P, P], I),
+            "oq_gmresdrshift": ([P, DP, DP, I, DP, IP, D, I, DP, DP, DP, P], I),
             "oq_gmresproject": ([P, DP, DP, IP, D, I, DP, DP, I, P, P], I),
             "oq_psc": ([P, DP, DP, IP, D, I, DP, DP, I, P, P], I),
             "oq_bicgstab": ([P, DP, DP, D, I, DP, DP, P, I], I),
@@ -188,6 +190,13 @@ class OracleLattice:
         lib().oq_twmshift(self._g, _dp(out), _dp(self.u), _dp(gi), idag, _dp(k))
         return out
 
+    def gamma5mult(self, ge, idag, kappa):
+        out = self.new_half()
+        gi = np.array(ge, dtype=np.float64, copy=True)
+        k = np.array(kappa, np.float64)
+        lib().oq_gamma5mult(self._g, _dp(out), _dp(self.u), _dp(gi), idag, _dp(k))
+        return out
+
     def vecdot(self, a, b):
         r = np.zeros(2)
         lib().oq_vecdot(self._g, _dp(np.ascontiguousarray(a)), _dp(np.ascontiguousarray(b)), _dp(r))
@@ -216,6 +225,20 @@ class OracleLattice:
         st = lib().oq_gmresdr(self._g, _dp(np.ascontiguousarray(phi)), _dp(x), Gp, float(resmax), itermin,
                               _dp(self.u), _dp(k), defl, C.byref(log))
         return x, st, log
+
+    def gmresdrshift(self, b, sigma, GMRES, resmax, itermin=0, kappa=(0.15, 0.01)):
+        """Solutions of (A - sigma_s) x_s = b, A = gamma5mult; returns (x[ns], status,
+        resid[ns] (absolute, recursively updated), log)."""
+        sig = np.ascontiguousarray(sigma, dtype=np.float64)
+        ns = len(sig)
+        x = np.zeros((ns,) + self.half_shape)
+        resid = np.zeros(ns)
+        log = SolveLog()
+        G, Gp = _ip(GMRES)
+        k = np.array(kappa, np.float64)
+        st = lib().oq_gmresdrshift(self._g, _dp(np.ascontiguousarray(b)), _dp(x), ns, _dp(sig), Gp,
+                                   float(resmax), itermin, _dp(self.u), _dp(k), _dp(resid), C.byref(log))
+        return x, st, resid, log
 
     def gmresproject(self, b, GMRES, resmax, itermin=0, kappa=(0.15, 0.0), isignal=2, defl=None):
         x = self.new_half()

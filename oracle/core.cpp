@@ -658,6 +658,44 @@ extern "C" void oq_twmshift(const oq_geom* g, double* hwhole, const double* u,
   }
 }
 
+// gamma5mult Q/diracops.f90:1750-1860 (iflag = -1): the even-odd twisted operator
+// multiplied by -i gamma5 / (2 kappa mu),
+//   he = ge/kappa^2 + fac4 J'[ ge/kappa^2 - fac3 H_eo (1 - 2 i kappa mu gamma5) H_oe ge ],
+// with J'(v) = (-v3, -v4, v1, v2), fac3 = 1/(1 + 4 kappa^2 mu^2), fac4 = 1/(2 kappa mu),
+// in the reference's expression order.
+namespace oq {
+void gamma5mult(const oq_geom* g, double* he, const double* u, double* ge, int idag,
+                const double kappa[2]) {
+  const size_t nv = g->vsize();
+  std::vector<double> hx(nv, 0.0), htmp(nv, 0.0);
+  const double basekappa = kappa[0], basemu = kappa[1];
+  oq::hsingle(g, hx.data(), u, ge, idag, 2);
+  const double f = 2.0 * basekappa * basemu;
+  g->for_spin_interior([&](size_t s1, size_t s2, size_t s3, size_t s4) {
+    htmp[s1] = hx[s1] - f * hx[s3];
+    htmp[s2] = hx[s2] - f * hx[s4];
+    htmp[s3] = hx[s3] + f * hx[s1];
+    htmp[s4] = hx[s4] + f * hx[s2];
+  });
+  oq::hsingle(g, hx.data(), u, htmp.data(), idag, 1);
+  const double fac1 = 1.0 / (basekappa * basekappa);
+  const double fac3 = 1.0 / (1.0 + (2.0 * basekappa * basemu) * (2.0 * basekappa * basemu));
+  const double fac4 = 1.0 / (2.0 * basekappa * basemu);
+  g->for_spin_interior([&](size_t s1, size_t s2, size_t s3, size_t s4) {
+    const double h1 = hx[s1], h2 = hx[s2], h3 = hx[s3], h4 = hx[s4];
+    he[s1] = -fac4 * fac1 * ge[s3] + fac1 * ge[s1] + fac4 * fac3 * h3;
+    he[s2] = -fac4 * fac1 * ge[s4] + fac1 * ge[s2] + fac4 * fac3 * h4;
+    he[s3] = fac4 * fac1 * ge[s1] + fac1 * ge[s3] - fac4 * fac3 * h1;
+    he[s4] = fac4 * fac1 * ge[s2] + fac1 * ge[s4] - fac4 * fac3 * h2;
+  });
+}
+}  // namespace oq
+
+extern "C" void oq_gamma5mult(const oq_geom* g, double* he, const double* u, double* ge,
+                              int idag, const double kappa[2]) {
+  oq::gamma5mult(g, he, u, ge, idag, kappa);
+}
+
 // gam5x C/basics.f90:408-454
 extern "C" void oq_gam5x(const oq_geom* g, double* a) {
   std::vector<double> b(a, a + g->vsize());

@@ -207,56 +207,38 @@ extern "C" void oq_defl_get(const oq_defl* d, int k, double* vtemp, double* hcne
 }
 
 // ------------------------------------------------------------------------------------
-// GMRES-DR(n,k): Q/inverters.f90:2871-3572
+// GMRES-DR(n,k) cycle shared by gmresdr (Q/inverters.f90:2871-3572) and gmresdrshift
+// (:6041-7179), which run the same Arnoldi, Givens and harmonic-Ritz restart code.
 // ------------------------------------------------------------------------------------
-extern "C" int oq_gmresdr(const oq_geom* g, const double* phi, double* x, const int GMRES[2],
-                          double resmax, int itermin, const double* u, const double kappa[2],
-                          oq_defl* defl, oq_solve_log* log) {
-  const int nDR = GMRES[0], kDR = GMRES[1];
-  const int nmax = nDR, ld = nmax + 1;
-  const size_t nv = g->vsize();
-  if (log) std::memset(log, 0, sizeof(*log));
-  std::vector<double> v((size_t)(nDR + 1) * nv, 0.0);
-  auto V = [&](int j) { return v.data() + (size_t)(j - 1) * nv; };
-  std::vector<double> r(nv, 0.0), h(nv, 0.0), xt(nv, 0.0), xb(nv, 0.0);
+namespace {
+struct DR {
+  const oq_geom* g;
+  int nDR, kDR, nmax, ld;
+  size_t nv;
+  std::vector<double> v;
   CMat hc, hc2, hc3, hcht, z, ws, gca, gsa;
-  hc.init(ld, nmax); hc2.init(ld, nmax); hc3.init(ld, nmax); hcht.init(nmax, nmax + 1);
-  z.init(ld, nmax + 1); ws.init(ld, kDR); gca.init(kDR + 1, kDR); gsa.init(kDR + 1, kDR);
   CVec c, c2, srv, ss, gc, gs, w, em, tau;
-  c.init(nmax + 1); c2.init(nmax + 1); srv.init(nmax + 1); ss.init(nmax); gc.init(nmax);
-  gs.init(nmax); w.init(nmax); em.init(nmax); tau.init(nmax);
-  std::vector<int> ipiv(nmax), myselect(nmax);
-  std::vector<double> mag(nmax);
-  int icycle = 1, mvp = 0, didmaindo = 0;
-  (void)didmaindo;
-  double beta[2];
+  std::vector<int> ipiv, myselect;
+  std::vector<double> mag;
+  DR(const oq_geom* g_, int n, int k) : g(g_), nDR(n), kDR(k), nmax(n), ld(n + 1), nv(g_->vsize()) {
+    v.assign((size_t)(nDR + 1) * nv, 0.0);
+    hc.init(ld, nmax); hc2.init(ld, nmax); hc3.init(ld, nmax); hcht.init(nmax, nmax + 1);
+    z.init(ld, nmax + 1); ws.init(ld, kDR); gca.init(kDR + 1, kDR); gsa.init(kDR + 1, kDR);
+    c.init(nmax + 1); c2.init(nmax + 1); srv.init(nmax + 1); ss.init(nmax); gc.init(nmax);
+    gs.init(nmax); w.init(nmax); em.init(nmax); tau.init(nmax);
+    ipiv.assign(nmax, 0);
+    myselect.assign(nmax, 0);
+    mag.assign(nmax, 0.0);
+  }
+  double* V(int j) { return v.data() + (size_t)(j - 1) * nv; }
 
-  // MORGAN'S STEP 1.
-  std::vector<double> xin(x, x + nv);
-  oq::hdbletm(g, h.data(), u, x, 0, kappa);
-  mvp += 1;
-  g->for_interior([&](size_t k) {
-    r[k] = phi[k] - h[k];
-    V(1)[k] = r[k];
-    xt[k] = x[k];
-  });
-  oq_vecdot(g, V(1), V(1), beta);
-  beta[0] = std::sqrt(beta[0]);
-  const double normnum = beta[0];
-  scale_all(g, V(1), 1.0 / beta[0]);
-  c.r(1) = beta[0];
-  c.c(1) = 0.0;
-  c2.r(1) = c.r(1);
-  c2.c(1) = c.c(1);
-
-  int itercount = 0, j = 0, status = 1;
-  for (;;) {
-    if (icycle > kcyclim) break;
-    j += 1;
+  // Arnoldi step j on V(j+1) = A V(j) (modified Gram-Schmidt, :3099-3155), the diagonal
+  // shift hc(j,j) - sigma of gmresdrshift (:6407-6412; gmresdr has sigma = 0), the
+  // Givens rotations of the new column (:3157-3218) and the least-squares solution ss
+  // (:3221-3245).
+  void step(int j, int icycle, double sigma) {
     const int jp1 = j + 1;
-    itercount += 1;
-    oq::hdbletm(g, V(jp1), u, V(j), 0, kappa);
-    mvp += 1;
+    double beta[2];
     for (int i = 1; i <= j; ++i) {
       oq_vecdot(g, V(i), V(jp1), beta);
       hc.r(i, j) = beta[0]; hc.c(i, j) = beta[1];
@@ -265,6 +247,13 @@ extern "C" int oq_gmresdr(const oq_geom* g, const double* phi, double* x, const 
       hcht.r(j, i) = hc.r(i, j);
       hcht.c(j, i) = -hc.c(i, j);
       caxpy_minus(g, V(jp1), V(i), beta);
+    }
+    if (sigma != 0.0) {
+      hc.r(j, j) = hc.r(j, j) - sigma;
+      hc2.r(j, j) = hc.r(j, j); hc2.c(j, j) = hc.c(j, j);
+      hc3.r(j, j) = hc.r(j, j); hc3.c(j, j) = hc.c(j, j);
+      hcht.r(j, j) = hc.r(j, j);
+      hcht.c(j, j) = -hc.c(j, j);
     }
     oq_vecdot(g, V(jp1), V(jp1), beta);
     hc.r(jp1, j) = std::sqrt(beta[0]); hc.c(jp1, j) = 0.0;
@@ -296,11 +285,10 @@ extern "C" int oq_gmresdr(const oq_geom* g, const double* phi, double* x, const 
     }
     new_rotation(hc, c, gc, gs, j);
     backsub(hc, c, ss, j);
+  }
 
-    std::fill(xb.begin(), xb.end(), 0.0);
-    for (int jj = 1; jj <= j; ++jj) caxpy_plus(g, xb.data(), V(jj), ss.r(jj), ss.c(jj));
-    g->for_interior([&](size_t k) { x[k] = xt[k] + xb[k]; });
-
+  // srv = c2 - hc3 ss, the residual in the basis V_{n+1} (:3257-3268)
+  void residual_coords() {
     for (int i = 1; i <= nDR + 1; ++i) {
       srv.r(i) = c2.r(i);
       srv.c(i) = c2.c(i);
@@ -311,6 +299,213 @@ extern "C" int oq_gmresdr(const oq_geom* g, const double* phi, double* x, const 
         srv.c(i) = srv.c(i) - ss.r(jj) * hc3.c(i, jj) - ss.c(jj) * hc3.r(i, jj);
         srv.r(i) = a;
       }
+  }
+
+  // Harmonic-Ritz restart (:3300-3556): the k smallest harmonic Ritz vectors of
+  // H + h_{n+1,n}^2 H^-H e_n e_n^T and the residual give V_{k+1}, hcnew, c; the new
+  // (k+1) x k block is triangularised with gca/gsa.
+  void restart(oq_defl* defl, oq_solve_log* log) {
+    double beta[2];
+    for (int i = 1; i <= nDR; ++i) em.r(i) = em.c(i) = 0.0;
+    em.r(nDR) = 1.0;
+    oq_linearsolver(nDR, 1, hcht.data(), hcht.ld, ipiv.data(), em.a.data(), nDR);
+    const double hr = hc2.r(nDR + 1, nDR), hi = hc2.c(nDR + 1, nDR);
+    for (int i = 1; i <= nDR; ++i) {
+      double a = hc2.r(i, nDR) + em.r(i) * hr * hr - em.r(i) * hi * hi - 2.0 * em.c(i) * hr * hi;
+      double b = hc2.c(i, nDR) + em.c(i) * hr * hr + 2.0 * em.r(i) * hi * hr - em.c(i) * hi * hi;
+      hc2.r(i, nDR) = a;
+      hc2.c(i, nDR) = b;
+    }
+    oq_hessenberg(hc2.data(), hc2.ld, nDR, 1, nDR, tau.a.data());
+    for (int jj = 1; jj <= nDR; ++jj)
+      for (int i = jj; i <= nDR; ++i) {
+        z.r(i, jj) = hc2.r(i, jj);
+        z.c(i, jj) = hc2.c(i, jj);
+      }
+    oq_qgenerator(nDR, 1, nDR, z.data(), z.ld, tau.a.data());
+    oq_evalues(1, nDR, 1, nDR, hc2.data(), hc2.ld, w.a.data(), z.data(), z.ld);
+    mag[0] = std::sqrt(w.r(1) * w.r(1) + w.c(1) * w.c(1));
+    for (int i = 2; i <= nDR; ++i) {
+      mag[i - 1] = std::sqrt(w.r(i) * w.r(i) + w.c(i) * w.c(i));
+      int is = 0;
+      for (;;) {
+        is += 1;
+        if (is > i - 1) break;
+        if (mag[i - 1] < mag[is - 1]) {
+          double tval = mag[i - 1];
+          for (int ivb = i - 1; ivb >= is; --ivb) mag[ivb] = mag[ivb - 1];
+          mag[is - 1] = tval;
+          break;
+        }
+      }
+    }
+    for (int i = 1; i <= nDR; ++i)
+      myselect[i - 1] = std::sqrt(w.r(i) * w.r(i) + w.c(i) * w.c(i)) <= mag[kDR - 1] ? 1 : 0;
+    int idis = 0;
+    oq_orgschur(myselect.data(), nDR, hc2.data(), hc2.ld, z.data(), z.ld, w.a.data(), &idis);
+    if (log) {
+      log->nritz = nDR < 512 ? nDR : 512;
+      for (int i = 0; i < log->nritz; ++i) {
+        log->ritz[2 * i] = w.r(i + 1);
+        log->ritz[2 * i + 1] = w.c(i + 1);
+      }
+    }
+    for (int i = 1; i <= kDR; ++i) z.r(nDR + 1, i) = z.c(nDR + 1, i) = 0.0;
+    for (int i = 1; i <= nDR + 1; ++i) {
+      z.r(i, kDR + 1) = srv.r(i);
+      z.c(i, kDR + 1) = srv.c(i);
+    }
+    for (int jj = 1; jj <= kDR; ++jj) {
+      double tv0 = 0.0, tv1 = 0.0;
+      for (int i = 1; i <= nDR + 1; ++i) {
+        tv0 = tv0 + z.r(i, jj) * z.r(i, kDR + 1) + z.c(i, jj) * z.c(i, kDR + 1);
+        tv1 = tv1 + z.r(i, jj) * z.c(i, kDR + 1) - z.c(i, jj) * z.r(i, kDR + 1);
+      }
+      for (int i = 1; i <= nDR + 1; ++i) {
+        double a = z.r(i, kDR + 1) - tv0 * z.r(i, jj) + tv1 * z.c(i, jj);
+        double b = z.c(i, kDR + 1) - tv0 * z.c(i, jj) - tv1 * z.r(i, jj);
+        z.r(i, kDR + 1) = a;
+        z.c(i, kDR + 1) = b;
+      }
+    }
+    double rv = 1.0 / oq::twonorm_c(&z.r(1, kDR + 1), nDR + 1);
+    for (int i = 1; i <= nDR + 1; ++i) {
+      z.r(i, kDR + 1) *= rv;
+      z.c(i, kDR + 1) *= rv;
+    }
+    for (int jj = 1; jj <= kDR; ++jj) {
+      for (int ii = 1; ii <= nDR + 1; ++ii) ws.r(ii, jj) = ws.c(ii, jj) = 0.0;
+      for (int ii = 1; ii <= nDR; ++ii)
+        for (int i = 1; i <= nDR + 1; ++i) {
+          double a = ws.r(i, jj) + z.r(ii, jj) * hc3.r(i, ii) - z.c(ii, jj) * hc3.c(i, ii);
+          double b = ws.c(i, jj) + z.r(ii, jj) * hc3.c(i, ii) + z.c(ii, jj) * hc3.r(i, ii);
+          ws.r(i, jj) = a;
+          ws.c(i, jj) = b;
+        }
+    }
+    CMat hcnew;
+    hcnew.init(ld, nmax);
+    for (int jj = 1; jj <= kDR; ++jj)
+      for (int ii = 1; ii <= kDR + 1; ++ii) {
+        double a = 0.0, b = 0.0;
+        for (int i = 1; i <= nDR + 1; ++i) {
+          a = a + z.r(i, ii) * ws.r(i, jj) + z.c(i, ii) * ws.c(i, jj);
+          b = b + z.r(i, ii) * ws.c(i, jj) - z.c(i, ii) * ws.r(i, jj);
+        }
+        hcnew.r(ii, jj) = a;
+        hcnew.c(ii, jj) = b;
+      }
+    for (int jj = 1; jj <= nDR; ++jj)
+      for (int ii = 1; ii <= nDR; ++ii) {
+        hcht.r(ii, jj) = hcht.c(ii, jj) = 0.0;
+        hc2.r(ii, jj) = hc2.c(ii, jj) = 0.0;
+      }
+    for (int jj = 1; jj <= kDR; ++jj) {
+      for (int ii = 1; ii <= kDR + 1; ++ii) {
+        hc.r(ii, jj) = hc2.r(ii, jj) = hc3.r(ii, jj) = hcnew.r(ii, jj);
+        hc.c(ii, jj) = hc2.c(ii, jj) = hc3.c(ii, jj) = hcnew.c(ii, jj);
+      }
+      for (int ii = 1; ii <= kDR + 1; ++ii) {
+        hcht.r(jj, ii) = hcnew.r(ii, jj);
+        hcht.c(jj, ii) = -hcnew.c(ii, jj);
+      }
+    }
+    for (int ii = 1; ii <= kDR + 1; ++ii) {
+      double a = 0.0, b = 0.0;
+      for (int i = 1; i <= nDR + 1; ++i) {
+        a = a + z.r(i, ii) * srv.r(i) + z.c(i, ii) * srv.c(i);
+        b = b + z.r(i, ii) * srv.c(i) - z.c(i, ii) * srv.r(i);
+      }
+      c.r(ii) = a; c.c(ii) = b;
+      c2.r(ii) = a; c2.c(ii) = b;
+    }
+    // V_{k+1} <- V_{m+1} Z, site by site (inverters.f90:3461-3485).
+    std::vector<double> vt(6 * (size_t)(kDR + 1));
+    for (int ibleo = 1; ibleo <= 8; ++ibleo)
+      for (int ieo = 1; ieo <= 2; ++ieo)
+        for (int id = 1; id <= 4; ++id)
+          for (int i = 1; i <= g->nvhalf; ++i) {
+            const size_t off = g->gi(1, i, id, ieo, ibleo);
+            for (int jj = 1; jj <= kDR + 1; ++jj) {
+              double* VT = vt.data() + 6 * (jj - 1);
+              for (int q = 0; q < 6; ++q) VT[q] = 0.0;
+              for (int k = 1; k <= nDR + 1; ++k) {
+                const double* Vk = V(k) + off;
+                for (int icri = 0; icri < 6; icri += 2) {
+                  double a = VT[icri] + z.r(k, jj) * Vk[icri] - z.c(k, jj) * Vk[icri + 1];
+                  double b = VT[icri + 1] + z.c(k, jj) * Vk[icri] + z.r(k, jj) * Vk[icri + 1];
+                  VT[icri] = a;
+                  VT[icri + 1] = b;
+                }
+              }
+            }
+            for (int jj = 1; jj <= kDR + 1; ++jj)
+              for (int q = 0; q < 6; ++q) V(jj)[off + q] = vt[6 * (jj - 1) + q];
+          }
+    for (int jj = 1; jj <= kDR; ++jj) {
+      oq_vecdot(g, V(jj), V(kDR + 1), beta);
+      caxpy_minus(g, V(kDR + 1), V(jj), beta);
+    }
+    oq_vecdot(g, V(kDR + 1), V(kDR + 1), beta);
+    scale_interior(g, V(kDR + 1), 1.0 / std::sqrt(beta[0]));
+    if (defl) {  // module shift: vtemp(:, 1..k+1), hcnew
+      defl->k = kDR;
+      if ((int)defl->vtemp.size() < (int)((kDR + 1) * nv)) defl->vtemp.resize((kDR + 1) * nv);
+      std::fill(defl->vtemp.begin(), defl->vtemp.end(), 0.0);
+      for (int jj = 1; jj <= kDR + 1; ++jj)
+        g->for_interior([&](size_t k) { defl->vtemp[(size_t)(jj - 1) * nv + k] = V(jj)[k]; });
+      defl->nmax = nmax;
+      defl->hcnew.assign(hcnew.a.begin(), hcnew.a.end());
+    }
+    block_triangularise(hc, c, gca, gsa, kDR);
+  }
+};
+}  // namespace
+
+// ------------------------------------------------------------------------------------
+// GMRES-DR(n,k): Q/inverters.f90:2871-3572
+// ------------------------------------------------------------------------------------
+extern "C" int oq_gmresdr(const oq_geom* g, const double* phi, double* x, const int GMRES[2],
+                          double resmax, int itermin, const double* u, const double kappa[2],
+                          oq_defl* defl, oq_solve_log* log) {
+  const int nDR = GMRES[0], kDR = GMRES[1];
+  const size_t nv = g->vsize();
+  if (log) std::memset(log, 0, sizeof(*log));
+  DR D(g, nDR, kDR);
+  std::vector<double> r(nv, 0.0), h(nv, 0.0), xt(nv, 0.0), xb(nv, 0.0);
+  int icycle = 1, mvp = 0;
+  double beta[2];
+
+  // MORGAN'S STEP 1.
+  oq::hdbletm(g, h.data(), u, x, 0, kappa);
+  mvp += 1;
+  g->for_interior([&](size_t k) {
+    r[k] = phi[k] - h[k];
+    D.V(1)[k] = r[k];
+    xt[k] = x[k];
+  });
+  oq_vecdot(g, D.V(1), D.V(1), beta);
+  beta[0] = std::sqrt(beta[0]);
+  const double normnum = beta[0];
+  scale_all(g, D.V(1), 1.0 / beta[0]);
+  D.c.r(1) = beta[0];
+  D.c.c(1) = 0.0;
+  D.c2.r(1) = D.c.r(1);
+  D.c2.c(1) = D.c.c(1);
+
+  int itercount = 0, j = 0, status = 1;
+  for (;;) {
+    if (icycle > kcyclim) break;
+    j += 1;
+    itercount += 1;
+    oq::hdbletm(g, D.V(j + 1), u, D.V(j), 0, kappa);
+    mvp += 1;
+    D.step(j, icycle, 0.0);
+
+    std::fill(xb.begin(), xb.end(), 0.0);
+    for (int jj = 1; jj <= j; ++jj) caxpy_plus(g, xb.data(), D.V(jj), D.ss.r(jj), D.ss.c(jj));
+    g->for_interior([&](size_t k) { x[k] = xt[k] + xb[k]; });
+    D.residual_coords();
 
     if (j >= nDR) {
       oq::hdbletm(g, h.data(), u, x, 0, kappa);
@@ -323,160 +518,8 @@ extern "C" int oq_gmresdr(const oq_geom* g, const double* phi, double* x, const 
         status = 0;
         break;
       }
-      didmaindo = 1;
       g->for_interior([&](size_t k) { xt[k] = x[k]; });
-      for (int i = 1; i <= nDR; ++i) em.r(i) = em.c(i) = 0.0;
-      em.r(nDR) = 1.0;
-      oq_linearsolver(nDR, 1, hcht.data(), hcht.ld, ipiv.data(), em.a.data(), nDR);
-      const double hr = hc2.r(nDR + 1, nDR), hi = hc2.c(nDR + 1, nDR);
-      for (int i = 1; i <= nDR; ++i) {
-        double a = hc2.r(i, nDR) + em.r(i) * hr * hr - em.r(i) * hi * hi - 2.0 * em.c(i) * hr * hi;
-        double b = hc2.c(i, nDR) + em.c(i) * hr * hr + 2.0 * em.r(i) * hi * hr - em.c(i) * hi * hi;
-        hc2.r(i, nDR) = a;
-        hc2.c(i, nDR) = b;
-      }
-      oq_hessenberg(hc2.data(), hc2.ld, nDR, 1, nDR, tau.a.data());
-      for (int jj = 1; jj <= nDR; ++jj)
-        for (int i = jj; i <= nDR; ++i) {
-          z.r(i, jj) = hc2.r(i, jj);
-          z.c(i, jj) = hc2.c(i, jj);
-        }
-      oq_qgenerator(nDR, 1, nDR, z.data(), z.ld, tau.a.data());
-      oq_evalues(1, nDR, 1, nDR, hc2.data(), hc2.ld, w.a.data(), z.data(), z.ld);
-      mag[0] = std::sqrt(w.r(1) * w.r(1) + w.c(1) * w.c(1));
-      for (int i = 2; i <= nDR; ++i) {
-        mag[i - 1] = std::sqrt(w.r(i) * w.r(i) + w.c(i) * w.c(i));
-        int is = 0;
-        for (;;) {
-          is += 1;
-          if (is > i - 1) break;
-          if (mag[i - 1] < mag[is - 1]) {
-            double tval = mag[i - 1];
-            for (int ivb = i - 1; ivb >= is; --ivb) mag[ivb] = mag[ivb - 1];
-            mag[is - 1] = tval;
-            break;
-          }
-        }
-      }
-      for (int i = 1; i <= nDR; ++i)
-        myselect[i - 1] = std::sqrt(w.r(i) * w.r(i) + w.c(i) * w.c(i)) <= mag[kDR - 1] ? 1 : 0;
-      int idis = 0;
-      oq_orgschur(myselect.data(), nDR, hc2.data(), hc2.ld, z.data(), z.ld, w.a.data(), &idis);
-      if (log) {
-        log->nritz = nDR < 512 ? nDR : 512;
-        for (int i = 0; i < log->nritz; ++i) {
-          log->ritz[2 * i] = w.r(i + 1);
-          log->ritz[2 * i + 1] = w.c(i + 1);
-        }
-      }
-      for (int i = 1; i <= kDR; ++i) z.r(nDR + 1, i) = z.c(nDR + 1, i) = 0.0;
-      for (int i = 1; i <= nDR + 1; ++i) {
-        z.r(i, kDR + 1) = srv.r(i);
-        z.c(i, kDR + 1) = srv.c(i);
-      }
-      for (int jj = 1; jj <= kDR; ++jj) {
-        double tv0 = 0.0, tv1 = 0.0;
-        for (int i = 1; i <= nDR + 1; ++i) {
-          tv0 = tv0 + z.r(i, jj) * z.r(i, kDR + 1) + z.c(i, jj) * z.c(i, kDR + 1);
-          tv1 = tv1 + z.r(i, jj) * z.c(i, kDR + 1) - z.c(i, jj) * z.r(i, kDR + 1);
-        }
-        for (int i = 1; i <= nDR + 1; ++i) {
-          double a = z.r(i, kDR + 1) - tv0 * z.r(i, jj) + tv1 * z.c(i, jj);
-          double b = z.c(i, kDR + 1) - tv0 * z.c(i, jj) - tv1 * z.r(i, jj);
-          z.r(i, kDR + 1) = a;
-          z.c(i, kDR + 1) = b;
-        }
-      }
-      double rv = 1.0 / oq::twonorm_c(&z.r(1, kDR + 1), nDR + 1);
-      for (int i = 1; i <= nDR + 1; ++i) {
-        z.r(i, kDR + 1) *= rv;
-        z.c(i, kDR + 1) *= rv;
-      }
-      for (int jj = 1; jj <= kDR; ++jj) {
-        for (int ii = 1; ii <= nDR + 1; ++ii) ws.r(ii, jj) = ws.c(ii, jj) = 0.0;
-        for (int ii = 1; ii <= nDR; ++ii)
-          for (int i = 1; i <= nDR + 1; ++i) {
-            double a = ws.r(i, jj) + z.r(ii, jj) * hc3.r(i, ii) - z.c(ii, jj) * hc3.c(i, ii);
-            double b = ws.c(i, jj) + z.r(ii, jj) * hc3.c(i, ii) + z.c(ii, jj) * hc3.r(i, ii);
-            ws.r(i, jj) = a;
-            ws.c(i, jj) = b;
-          }
-      }
-      CMat hcnew;
-      hcnew.init(ld, nmax);
-      for (int jj = 1; jj <= kDR; ++jj)
-        for (int ii = 1; ii <= kDR + 1; ++ii) {
-          double a = 0.0, b = 0.0;
-          for (int i = 1; i <= nDR + 1; ++i) {
-            a = a + z.r(i, ii) * ws.r(i, jj) + z.c(i, ii) * ws.c(i, jj);
-            b = b + z.r(i, ii) * ws.c(i, jj) - z.c(i, ii) * ws.r(i, jj);
-          }
-          hcnew.r(ii, jj) = a;
-          hcnew.c(ii, jj) = b;
-        }
-      for (int jj = 1; jj <= nDR; ++jj)
-        for (int ii = 1; ii <= nDR; ++ii) {
-          hcht.r(ii, jj) = hcht.c(ii, jj) = 0.0;
-          hc2.r(ii, jj) = hc2.c(ii, jj) = 0.0;
-        }
-      for (int jj = 1; jj <= kDR; ++jj) {
-        for (int ii = 1; ii <= kDR + 1; ++ii) {
-          hc.r(ii, jj) = hc2.r(ii, jj) = hc3.r(ii, jj) = hcnew.r(ii, jj);
-          hc.c(ii, jj) = hc2.c(ii, jj) = hc3.c(ii, jj) = hcnew.c(ii, jj);
-        }
-        for (int ii = 1; ii <= kDR + 1; ++ii) {
-          hcht.r(jj, ii) = hcnew.r(ii, jj);
-          hcht.c(jj, ii) = -hcnew.c(ii, jj);
-        }
-      }
-      for (int ii = 1; ii <= kDR + 1; ++ii) {
-        double a = 0.0, b = 0.0;
-        for (int i = 1; i <= nDR + 1; ++i) {
-          a = a + z.r(i, ii) * srv.r(i) + z.c(i, ii) * srv.c(i);
-          b = b + z.r(i, ii) * srv.c(i) - z.c(i, ii) * srv.r(i);
-        }
-        c.r(ii) = a; c.c(ii) = b;
-        c2.r(ii) = a; c2.c(ii) = b;
-      }
-      // V_{k+1} <- V_{m+1} Z, site by site (inverters.f90:3461-3485).
-      std::vector<double> vt(6 * (size_t)(kDR + 1));
-      for (int ibleo = 1; ibleo <= 8; ++ibleo)
-        for (int ieo = 1; ieo <= 2; ++ieo)
-          for (int id = 1; id <= 4; ++id)
-            for (int i = 1; i <= g->nvhalf; ++i) {
-              const size_t off = g->gi(1, i, id, ieo, ibleo);
-              for (int jj = 1; jj <= kDR + 1; ++jj) {
-                double* VT = vt.data() + 6 * (jj - 1);
-                for (int q = 0; q < 6; ++q) VT[q] = 0.0;
-                for (int k = 1; k <= nDR + 1; ++k) {
-                  const double* Vk = V(k) + off;
-                  for (int icri = 0; icri < 6; icri += 2) {
-                    double a = VT[icri] + z.r(k, jj) * Vk[icri] - z.c(k, jj) * Vk[icri + 1];
-                    double b = VT[icri + 1] + z.c(k, jj) * Vk[icri] + z.r(k, jj) * Vk[icri + 1];
-                    VT[icri] = a;
-                    VT[icri + 1] = b;
-                  }
-                }
-              }
-              for (int jj = 1; jj <= kDR + 1; ++jj)
-                for (int q = 0; q < 6; ++q) V(jj)[off + q] = vt[6 * (jj - 1) + q];
-            }
-      for (int jj = 1; jj <= kDR; ++jj) {
-        oq_vecdot(g, V(jj), V(kDR + 1), beta);
-        caxpy_minus(g, V(kDR + 1), V(jj), beta);
-      }
-      oq_vecdot(g, V(kDR + 1), V(kDR + 1), beta);
-      scale_interior(g, V(kDR + 1), 1.0 / std::sqrt(beta[0]));
-      if (defl) {  // module shift: vtemp(:, 1..k+1), hcnew
-        defl->k = kDR;
-        if ((int)defl->vtemp.size() < (int)((kDR + 1) * nv)) defl->vtemp.resize((kDR + 1) * nv);
-        std::fill(defl->vtemp.begin(), defl->vtemp.end(), 0.0);
-        for (int jj = 1; jj <= kDR + 1; ++jj)
-          g->for_interior([&](size_t k) { defl->vtemp[(size_t)(jj - 1) * nv + k] = V(jj)[k]; });
-        defl->nmax = nmax;
-        defl->hcnew.assign(hcnew.a.begin(), hcnew.a.end());
-      }
-      block_triangularise(hc, c, gca, gsa, kDR);
+      D.restart(defl, log);
       j = kDR;
       icycle += 1;
     }
@@ -489,7 +532,127 @@ extern "C" int oq_gmresdr(const oq_geom* g, const double* phi, double* x, const 
     log->ncycles = icycle;
     log->final_rel = std::sqrt(norm2(g, r.data())) / std::sqrt(norm2(g, phi));
   }
-  (void)xin;
+  return status;
+}
+
+// ------------------------------------------------------------------------------------
+// gmresdrshift: Q/inverters.f90:6041-7179.  GMRES-DR(n,k) on A - sigma_1, A the
+// operator of gamma5mult (Q/diracops.f90:1750-1860), and for every further shift s the
+// solution of (A - sigma_s) x_s = b whose residual stays collinear with the base
+// residual (Frommer-Glaessner; Darnell, Morgan and Wilcox 2008):
+//   [Hbar + (sigma_1 - sigma_s) I~ | srv] (d_s, alpha_s) = cmult_s c2      (:6576-6747)
+// solved here with linearsolver on the square (j+1) system instead of zgeqrf/zungqr
+// (the same unique solution).  Where the reference cannot run as written, the
+// evident intent is kept and stated:
+//   * sigma is an argument (the reference's local sigma is never assigned);
+//   * the shifted solutions are formed at the end of every cycle (the reference tests
+//     j >= nmaxGMRES at :6754, which GMRES-DR(n < nmaxGMRES) never reaches before restarting);
+//   * the initial guess is zero for every shift, so the initial residuals are b and
+//     collinear (the reference copies b - A x_1 to every shift, :6297-6315).
+// Each shift's residual is updated recursively, r_s -= (A - sigma_s) xb_s (:6816-6830),
+// and the iteration stops when ||r_1|| < resmax (absolute, as :6865).
+// ------------------------------------------------------------------------------------
+extern "C" int oq_gmresdrshift(const oq_geom* g, const double* b, double* xshift, int nshifts,
+                               const double* sigma, const int GMRES[2], double resmax,
+                               int itermin, const double* u, const double kappa[2],
+                               double* resid, oq_solve_log* log) {
+  const int nDR = GMRES[0], kDR = GMRES[1];
+  const size_t nv = g->vsize();
+  if (log) std::memset(log, 0, sizeof(*log));
+  DR D(g, nDR, kDR);
+  std::vector<double> h(nv, 0.0), xb(nv, 0.0), rshift((size_t)nshifts * nv, 0.0);
+  auto X = [&](int s) { return xshift + (size_t)(s - 1) * nv; };
+  auto R = [&](int s) { return rshift.data() + (size_t)(s - 1) * nv; };
+  std::vector<double> cmr(nshifts + 1, 1.0), cmi(nshifts + 1, 0.0);  // cmult
+  std::vector<double> dr((size_t)(nDR + 1) * (nshifts + 1)), di(dr.size());
+  int icycle = 1, mvp = 0;
+  double beta[2];
+
+  std::fill(xshift, xshift + (size_t)nshifts * nv, 0.0);
+  g->for_interior([&](size_t k) {
+    D.V(1)[k] = b[k];
+    for (int s = 1; s <= nshifts; ++s) R(s)[k] = b[k];
+  });
+  oq_vecdot(g, D.V(1), D.V(1), beta);
+  beta[0] = std::sqrt(beta[0]);
+  const double normnum = beta[0];
+  for (int s = 1; s <= nshifts; ++s) resid[s - 1] = normnum;
+  if (!(normnum > 0.0)) return 0;
+  scale_all(g, D.V(1), 1.0 / beta[0]);
+  D.c.r(1) = beta[0];
+  D.c.c(1) = 0.0;
+  D.c2.r(1) = D.c.r(1);
+  D.c2.c(1) = D.c.c(1);
+
+  int itercount = 0, j = 0, status = 1;
+  for (;;) {
+    if (icycle > kcyclim) break;
+    j += 1;
+    itercount += 1;
+    oq::gamma5mult(g, D.V(j + 1), u, D.V(j), 0, kappa);
+    mvp += 1;
+    D.step(j, icycle, sigma[0]);
+    D.residual_coords();
+    if (j < nDR) continue;
+
+    // base shift: d = ss; further shifts: the collinear solve with the base srv
+    for (int i = 1; i <= j; ++i) {
+      dr[i] = D.ss.r(i);
+      di[i] = D.ss.c(i);
+    }
+    for (int s = 2; s <= nshifts; ++s) {
+      const int n1 = j + 1;
+      std::vector<double> a(2 * (size_t)n1 * n1, 0.0), rhs(2 * (size_t)n1, 0.0);
+      std::vector<int> piv(n1);
+      for (int jj = 1; jj <= j; ++jj)
+        for (int ii = 1; ii <= n1; ++ii) {
+          a[2 * ((ii - 1) + (size_t)n1 * (jj - 1))] = D.hc2.r(ii, jj);
+          a[2 * ((ii - 1) + (size_t)n1 * (jj - 1)) + 1] = D.hc2.c(ii, jj);
+        }
+      for (int jj = 1; jj <= j; ++jj)
+        a[2 * ((jj - 1) + (size_t)n1 * (jj - 1))] += sigma[0] - sigma[s - 1];
+      for (int ii = 1; ii <= n1; ++ii) {
+        a[2 * ((ii - 1) + (size_t)n1 * j)] = D.srv.r(ii);
+        a[2 * ((ii - 1) + (size_t)n1 * j) + 1] = D.srv.c(ii);
+        rhs[2 * (ii - 1)] = cmr[s] * D.c2.r(ii) - cmi[s] * D.c2.c(ii);
+        rhs[2 * (ii - 1) + 1] = cmr[s] * D.c2.c(ii) + cmi[s] * D.c2.r(ii);
+      }
+      oq_linearsolver(n1, 1, a.data(), n1, piv.data(), rhs.data(), n1);
+      for (int i = 1; i <= j; ++i) {
+        dr[(size_t)(s - 1) * (nDR + 1) + i] = rhs[2 * (i - 1)];
+        di[(size_t)(s - 1) * (nDR + 1) + i] = rhs[2 * (i - 1) + 1];
+      }
+      cmr[s] = rhs[2 * j];
+      cmi[s] = rhs[2 * j + 1];
+    }
+    for (int s = 1; s <= nshifts; ++s) {
+      std::fill(xb.begin(), xb.end(), 0.0);
+      for (int jj = 1; jj <= j; ++jj)
+        caxpy_plus(g, xb.data(), D.V(jj), dr[(size_t)(s - 1) * (nDR + 1) + jj],
+                   di[(size_t)(s - 1) * (nDR + 1) + jj]);
+      g->for_interior([&](size_t k) { X(s)[k] = X(s)[k] + xb[k]; });
+      oq::gamma5mult(g, h.data(), u, xb.data(), 0, kappa);
+      mvp += 1;
+      const double sg = sigma[s - 1];
+      g->for_interior([&](size_t k) { R(s)[k] = R(s)[k] - h[k] + sg * xb[k]; });
+      oq_vecdot(g, R(s), R(s), beta);
+      resid[s - 1] = std::sqrt(beta[0]);
+    }
+    log_hist(log, mvp, resid[0] / normnum);
+    if (resid[0] < resmax && itercount >= itermin) {
+      status = 0;
+      break;
+    }
+    D.restart(nullptr, log);
+    j = kDR;
+    icycle += 1;
+  }
+  if (log) {
+    log->itercount = itercount;
+    log->mvp = mvp;
+    log->ncycles = icycle;
+    log->final_rel = resid[0] / normnum;
+  }
   return status;
 }
 

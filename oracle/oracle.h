@@ -70,6 +70,8 @@ void oq_hdbletm(const oq_geom* g, double* he, const double* u, double* ge, int i
                 const double kappa[2]);
 void oq_twmshift(const oq_geom* g, double* hwhole, const double* u, double* gwhole,
                  int idag, const double kappa[2]);
+void oq_gamma5mult(const oq_geom* g, double* he, const double* u, double* ge, int idag,
+                   const double kappa[2]);
 void oq_gam5x(const oq_geom* g, double* a);
 void oq_gamma5vector(const oq_geom* g, double* a, int ntmqcd);
 void oq_vecdot(const oq_geom* g, const double* a, const double* b, double* adb);
@@ -99,6 +101,11 @@ typedef struct oq_solve_log {
 int oq_gmresdr(const oq_geom* g, const double* phi, double* x, const int GMRES[2],
                double resmax, int itermin, const double* u, const double kappa[2],
                oq_defl* defl, oq_solve_log* log);
+// gmresdrshift with explicit shifts sigma[nshifts]: xshift receives nshifts vectors
+// (zero initial guess), resid the final ||r_s|| (absolute).
+int oq_gmresdrshift(const oq_geom* g, const double* b, double* xshift, int nshifts,
+                    const double* sigma, const int GMRES[2], double resmax, int itermin,
+                    const double* u, const double kappa[2], double* resid, oq_solve_log* log);
 int oq_gmresproject(const oq_geom* g, const double* b, double* x, const int GMRES[2],
                     double resmax, int itermin, const double* u, const double kappa[2],
                     int isignal, oq_defl* defl, oq_solve_log* log);

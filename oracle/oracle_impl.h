@@ -91,6 +91,8 @@ void hdouble(const oq_geom* g, double* he, const double* u, double* ge, int idag
              double kappa);
 void hdbletm(const oq_geom* g, double* he, const double* u, double* ge, int idag,
              const double kappa[2]);
+void gamma5mult(const oq_geom* g, double* he, const double* u, double* ge, int idag,
+                const double kappa[2]);
 double vecdot_re(const oq_geom* g, const double* a, const double* b, double* im);
 double twonorm_c(const double* x, int n);
 }  // namespace oq

@@ -98,3 +98,27 @@ def test_momfacs_library_matches_oracle():
         assert np.array_equal(qq.momfacs(dims, io), ol.momfacs(io))
         mf = ol.momfacs(io)
         assert np.array_equal(mf[4], mf[3]) and np.abs(mf).max() > 0
+
+
+def test_generalaverage_styles_1_and_2_are_average_levels():
+    """generalaverage (Q/disconloops.f90:119-333) builds its style 1 from nsaverage (the
+    operators of the unsubtracted solution with zero momentum factors, :3079-3143) and its
+    style 2 as NS - PS, PS = -average of a zero solution.  average is linear in the solution
+    apart from the constant on psibar psi of the subtracted levels, which the zero-solution
+    run carries too, so NS - PS at level k equals average's level k: checked on the oracle,
+    at imom = 1 and zero momentum factors, as generalaverage calls them."""
+    ol = oracle.OracleLattice(*DIMS, bc=BC)
+    _, u = golden_gauge(DIMS, ol.ntotal, seed=41, eps=0.6)
+    ol.set_gauge(u)
+    be, bo = random_half(ol.ntotal, ol.nvhalf, 81), random_half(ol.ntotal, ol.nvhalf, 82)
+    xe, xo = random_half(ol.ntotal, ol.nvhalf, 83), random_half(ol.ntotal, ol.nvhalf, 84)
+    kappa, nsub, nmom, nop = 0.153, 6, 5, 9
+    zero = np.zeros((5, nmom - 1, 16, 2, ol.nvhalf))
+    J = ol.average(be, bo, xe, xo, kappa, nsub, nmom, nop, zero)
+    PS = -ol.average(be, bo, ol.new_half(), ol.new_half(), kappa, nsub, nmom, nop, zero)
+    NS = J[:, 0, 0]  # style 1: level 1, imom = 1
+    assert np.abs(PS[:, 0, 0]).max() == 0.0  # nothing to subtract at level 1
+    for k in range(nsub):
+        style2 = NS - PS[:, 0, k]
+        np.testing.assert_allclose(style2, J[:, 0, k], rtol=0, atol=1e-12 * np.abs(J).max())
+    assert np.abs(J[:, 1:]).max() == 0.0  # zero momentum factors: only imom = 1 survives

@@ -31,6 +31,7 @@ struct Arnoldi {
   int m;         // Krylov dimension (m+1 vectors)
   size_t nel;    // 16-byte elements per vector
   DevBuf V, H, hscr, y;
+  DevBuf Pdev;  // restart rotation ((m+1) x (k+1), k < m), allocated once
   // Krylov operator: Hdbletm, or gamma5mult - g5shift (gmresdrshift)
   bool g5 = false;
   double g5shift = 0.0;
@@ -43,6 +44,7 @@ struct Arnoldi {
     QQ_CK(H.alloc(sizeof(double) * 2 * (size_t)(m + 1) * m));
     QQ_CK(hscr.alloc(sizeof(double) * 2 * 128));
     QQ_CK(y.alloc(sizeof(double) * 2 * 256));
+    QQ_CK(Pdev.alloc(sizeof(double) * 2 * (size_t)(m + 1) * m));
     return QQ_OK;
   }
   void* vec(int i) const { return static_cast<char*>(V.p) + (size_t)i * nel * 16; }
@@ -292,11 +294,9 @@ int fgmresdr_fp64(qq_ctx* c, Spinor phi, Spinor x, int m, int k, double resmax, 
       return QQ_NOT_CONVERGED;
     }
     st->ritz = ritz;
-    DevBuf Pd;
-    QQ_CK(Pd.alloc(sizeof(double) * 2 * (size_t)(m + 1) * (k + 1)));
-    QQ_TRY(upload_mat(c, P, Pd.as<double>(), m + 1));
-    QQ_CK(launch_rotate(P64, A.basis(), m + 1, k + 1, Pd.as<double>(), m + 1, c->st));
-    QQ_CK(launch_rotate(P64, ZB, m, k, Pd.as<double>(), m + 1, c->st));
+    QQ_TRY(upload_mat(c, P, A.Pdev.as<double>(), m + 1));
+    QQ_CK(launch_rotate(P64, A.basis(), m + 1, k + 1, A.Pdev.as<double>(), m + 1, c->st));
+    QQ_CK(launch_rotate(P64, ZB, m, k, A.Pdev.as<double>(), m + 1, c->st));
     QQ_TRY(reorth(A, k, nrm2));
     QQ_TRY(A.zeroH());
     QQ_TRY(upload_mat(c, Hk, A.H.as<double>(), m + 1));
@@ -368,10 +368,8 @@ int gmresdr_fp64(qq_ctx* c, Spinor phi, Spinor x, int m, int k, double resmax, i
       break;
     }
     st->ritz = ritz;
-    DevBuf Pd;
-    QQ_CK(Pd.alloc(sizeof(double) * 2 * (size_t)(m + 1) * (k + 1)));
-    QQ_TRY(upload_mat(c, P, Pd.as<double>(), m + 1));
-    QQ_CK(launch_rotate(P64, A.basis(), m + 1, k + 1, Pd.as<double>(), m + 1, c->st));
+    QQ_TRY(upload_mat(c, P, A.Pdev.as<double>(), m + 1));
+    QQ_CK(launch_rotate(P64, A.basis(), m + 1, k + 1, A.Pdev.as<double>(), m + 1, c->st));
     QQ_TRY(reorth(A, k, nrm2));
     QQ_TRY(A.zeroH());
     QQ_TRY(upload_mat(c, Hk, A.H.as<double>(), m + 1));
@@ -495,10 +493,8 @@ int gmresdrshift_fp64(qq_ctx* c, Spinor b, const std::vector<Spinor>& xs, const 
       break;
     }
     st->ritz = ritz;
-    DevBuf Pd;
-    QQ_CK(Pd.alloc(sizeof(double) * 2 * (size_t)(m + 1) * (k + 1)));
-    QQ_TRY(upload_mat(c, P, Pd.as<double>(), m + 1));
-    QQ_CK(launch_rotate(P64, A.basis(), m + 1, k + 1, Pd.as<double>(), m + 1, c->st));
+    QQ_TRY(upload_mat(c, P, A.Pdev.as<double>(), m + 1));
+    QQ_CK(launch_rotate(P64, A.basis(), m + 1, k + 1, A.Pdev.as<double>(), m + 1, c->st));
     QQ_TRY(reorth(A, k, nrm2));
     QQ_TRY(A.zeroH());
     QQ_TRY(upload_mat(c, Hk, A.H.as<double>(), m + 1));

@@ -94,3 +94,32 @@ def test_gmresdrshift_argument_checks(pair):
         lat.gmresdrshift(b, np.array([0.0]), (4, 4), 1e-10, kappa=(0.18, 0.03))
     with pytest.raises(qq.QQError):
         lat.gamma5mult(b, 0, (0.18, 0.0))
+
+
+def test_gmresdrshift_heatbath_recon12_physical_mass():
+    """8^4 heatbath configuration (recon-12 links on the device), the twisted mass of the
+    noise-trace workload (kappa 0.1566, mu 0.005) and the shifts of the reference's
+    commented variants: every shift's solution equal to the oracle's to 1e-7."""
+    import baylorlqcd_b200 as qq
+
+    dims = (8, 8, 8, 8)
+    nv = dims[0] * dims[1] * dims[2] * dims[3] // 32
+    lat = qq.Lattice(*dims, bc=BC)
+    try:
+        u, _ = lat.heatbath(6.0, 20, seed=11)
+        ol = oracle.OracleLattice(*dims, bc=BC)
+        ol.set_gauge(u)
+        kappa = (0.1566, 0.005)
+        sig = np.array([0.0, -0.099, -0.199, -0.3, -0.5]) / kappa[0] ** 2
+        b = random_half(ol.ntotal, ol.nvhalf, 31)
+        xo, st, ro, log = ol.gmresdrshift(b, sig, (40, 12), 1e-10, kappa=kappa)
+        assert st == 0
+        x, resid, info = lat.gmresdrshift(b, sig, (40, 12), 1e-10, kappa=kappa)
+        assert info.status == 0
+        assert abs(info.ncycles - log.ncycles) <= 1
+        for s in range(len(sig)):
+            d = x[s][:, :, :, :nv, :] - xo[s][:, :, :, :nv, :]
+            assert np.linalg.norm(d) / np.linalg.norm(xo[s][:, :, :, :nv, :]) < 1e-7
+        assert resid[0] < 1e-10 and np.all(resid < 1e-9) and np.all(ro < 1e-9)
+    finally:
+        lat.close()

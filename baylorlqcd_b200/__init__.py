@@ -38,7 +38,7 @@ EXPORTED = [
     "qq_gfwrite", "qq_gfread", "qq_fpwrite", "qq_fpread", "qq_hsingle_block",
     "qq_hop_tuned_shape", "qq_net_create", "qq_net_destroy", "qq_net_nweights", "qq_net_get_weights",
     "qq_net_set_weights", "qq_net_apply", "qq_net_grad", "qq_net_train", "qq_fgmres", "qq_pionrho", "qq_twvev", "qq_twaverage", "qq_twistdiscon", "qq_average", "qq_momfacs",
-    "qq_fgmresdr",
+    "qq_fgmresdr", "qq_fermprop_uneven",
 ]
 
 
@@ -64,6 +64,12 @@ class qq_method(C.Structure):
     _fields_ = [("m", C.c_int), ("k", C.c_int), ("precision", C.c_int), ("rhs_block", C.c_int),
                 ("tol", C.c_double), ("max_outer", C.c_int), ("solver", C.c_int), ("deflate", C.c_int),
                 ("defl_tol", C.c_double)]
+
+
+class qq_uneven_group(C.Structure):
+    _fields_ = [("ctx", C.c_void_p), ("nrhs", C.c_int), ("kappa", C.c_double * 2), ("be", C.c_void_p),
+                ("bo", C.c_void_p), ("xe", C.c_void_p), ("xo", C.c_void_p),
+                ("infos", C.POINTER(qq_solve_info))]
 
 
 @dataclass
@@ -130,6 +136,7 @@ def load_library() -> C.CDLL:
         "qq_fermprop": ([P, P, P, DP, I, D, I, IP, P, P, I, I, P, C.POINTER(qq_solve_info)], I),
         "qq_pointsource": ([P, P, P, IP, I, I], I),
         "qq_fermprop_batch": ([P, I, P, P, DP, C.POINTER(qq_method), P, P, C.POINTER(qq_solve_info)], I),
+        "qq_fermprop_uneven": ([I, C.POINTER(qq_uneven_group), C.POINTER(qq_method), I, DP], I),
         "qq_initlagfib": ([I, I], I),
         "qq_rnds": ([I, DP], I),
         "qq_z2source": ([P, P, P], I),
@@ -623,6 +630,31 @@ def momfacs(dims, io=(1, 1, 1)) -> np.ndarray:
     _check(load_library().qq_momfacs(d.ctypes.data_as(C.POINTER(C.c_int)), o.ctypes.data_as(C.POINTER(C.c_int)),
                                      _ptr(mf)))
     return mf
+
+
+def fermprop_uneven(groups, m=60, k=20, precision=32, rhs_block=12, tol=1e-10, max_outer=0, solver=1,
+                    deflate=0, defl_tol=1e-5, concurrent=True):
+    """Uneven batch (qq_fermprop_uneven): groups is a list of (lattice, be, bo, kappa),
+    be/bo of shape (nrhs,) + that lattice's half_shape, numpy or torch CUDA tensors.
+    Each group is solved as Lattice.fermprop_batch solves it; with concurrent=True the
+    lattices run side by side on their own streams.  Returns ([(xe, xo, infos)] per
+    group, wall seconds of the call)."""
+    n = len(groups)
+    arr = (qq_uneven_group * n)()
+    keep = []
+    for i, (lat, be, bo, kappa) in enumerate(groups):
+        nrhs = be.shape[0]
+        xe = np.zeros(be.shape) if isinstance(be, np.ndarray) else be.new_zeros(be.shape)
+        xo = np.zeros(bo.shape) if isinstance(bo, np.ndarray) else bo.new_zeros(bo.shape)
+        infos = (qq_solve_info * nrhs)()
+        arr[i] = qq_uneven_group(lat._ctx.value, nrhs, (C.c_double * 2)(*kappa), _ptr(be), _ptr(bo), _ptr(xe),
+                                 _ptr(xo), C.cast(infos, C.POINTER(qq_solve_info)))
+        keep.append((xe, xo, infos))
+    meth = qq_method(m, k, precision, rhs_block, tol, max_outer, solver, deflate, defl_tol)
+    secs = C.c_double(0.0)
+    _check(load_library().qq_fermprop_uneven(n, arr, C.byref(meth), int(bool(concurrent)), C.byref(secs)),
+           allow_not_converged=True)
+    return [(xe, xo, [SolveInfo.from_c(i) for i in infos]) for xe, xo, infos in keep], secs.value
 
 
 def initlagfib(myid: int, iseed: int):

@@ -46,13 +46,11 @@ template <int SP, int LP, int RECON, int EPI>
 static cudaError_t hop_staged_launch(const HopArgs& a, int T, cudaStream_t st) {
   const size_t smem = staged_smem_bytes<SP, LP, RECON>(T);
   if (smem > 227 * 1024) return cudaErrorInvalidValue;
-  static bool attr_set = false;  // one attribute call per instantiation
-  if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(hop_staged_kernel<SP, LP, RECON, EPI>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-    if (e != cudaSuccess) return e;
-    attr_set = true;
-  }
+  // one attribute call per instantiation; a function-local static is initialised once
+  // even when several host threads (one per context) launch at the same time
+  static const cudaError_t attr = cudaFuncSetAttribute(hop_staged_kernel<SP, LP, RECON, EPI>,
+                                                       cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+  if (attr != cudaSuccess) return attr;
   const HopArgs b = hop_prepare(a, T / a.nrhs, a.nrhs);
   dim3 grd((a.g.vh + b.per_block - 1) / b.per_block);
   hop_staged_kernel<SP, LP, RECON, EPI><<<grd, T, smem, st>>>(b);
@@ -151,18 +149,23 @@ static cudaError_t hop_f2s(const HopArgs& a, int epi, cudaStream_t st) {
 // Copy-ring kernel: D stages in flight per thread, RPT right-hand sides per thread.
 template <int EPI, int D, int RPT>
 static cudaError_t hop_f2a_epi(const HopArgs& b, size_t smem, cudaStream_t st) {
-  static bool attr_set = false;  // one attribute call per instantiation
-  static size_t max_dyn = 0;     // 227 KiB less the kernel's static shared memory
-  if (!attr_set) {
+  // One attribute call per instantiation: 227 KiB less the kernel's static shared
+  // memory.  A function-local static is initialised once even when several host
+  // threads (one per context) launch at the same time.
+  struct Attr {
+    cudaError_t err;
+    size_t max_dyn;
+  };
+  static const Attr attr = [] {
     cudaFuncAttributes fa;
     cudaError_t e = cudaFuncGetAttributes(&fa, hop_f2a_kernel<EPI, D, RPT>);
-    if (e != cudaSuccess) return e;
-    max_dyn = (size_t)227 * 1024 - fa.sharedSizeBytes;
-    e = cudaFuncSetAttribute(hop_f2a_kernel<EPI, D, RPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_dyn);
-    if (e != cudaSuccess) return e;
-    attr_set = true;
-  }
-  if (smem > max_dyn) return cudaErrorInvalidValue;
+    if (e != cudaSuccess) return Attr{e, 0};
+    const size_t md = (size_t)227 * 1024 - fa.sharedSizeBytes;
+    e = cudaFuncSetAttribute(hop_f2a_kernel<EPI, D, RPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)md);
+    return Attr{e, md};
+  }();
+  if (attr.err != cudaSuccess) return attr.err;
+  if (smem > attr.max_dyn) return cudaErrorInvalidValue;
   const int G = b.nrhs / RPT;
   const dim3 blk(b.per_block * G), grd((b.g.vh + b.per_block - 1) / b.per_block);
   hop_f2a_kernel<EPI, D, RPT><<<grd, blk, smem, st>>>(b);
@@ -356,10 +359,12 @@ cudaError_t launch_rotate(int pb, const BasisArgs& V, int nin, int nout, const d
   const size_t smem = sizeof(double) * 2 * (size_t)nin * nout;
   if (smem > 200 * 1024 || nout > 64) return cudaErrorInvalidValue;
   const int grid = 148 * 4;
+  // The attribute is the bound checked above, the same for every call, so host threads
+  // that launch side by side (one per context) never lower it under another's launch.
 #define QQ_ROT(PB, MO)                                                                       \
   do {                                                                                       \
     auto k = rotate_kernel<PB, MO>;                                                          \
-    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);         \
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);        \
     k<<<grid, 128, smem, st>>>(V, nin, nout, Z, ldz);                                        \
   } while (0)
   if (pb == P64) {

@@ -10,6 +10,7 @@
                                            [--mu 0.0] [--solver 1] [--nsub 6]
     python -m baylorlqcd_b200.probe shift [--dims 16,16,16,32] [--kappa 0.1566] [--mu 0.005]
                                           [--shifts 0,-0.099,-0.199,-0.3,-0.5] [--m 40] [--k 12]
+    python -m baylorlqcd_b200.probe uneven [--sweeps 200] [--precision 32] [--rhs-block 4]
 
 ``hop`` times one hopping-kernel shape (qq_bench_hsingle: random fields, L2 flushed
 between launches unless --no-flush) and prints its time and algorithmic bandwidth.
@@ -156,6 +157,56 @@ def run_shift(a):
     lat.close()
 
 
+UNEVEN_DIMS = ((8, 8, 8, 16), (12, 12, 12, 24), (16, 16, 16, 32), (20, 20, 20, 40))
+UNEVEN_KAPPAS = (0.150, 0.155, 0.1565)
+
+
+def run_uneven(a):
+    """Uneven batch (qq_fermprop_uneven): 48 Wilson solves over four heatbath
+    configurations (8^3x16, 12^3x24, 16^3x32, 20^3x40 at beta = 6.0), three kappa
+    values each, two point and two Z(4) sources per (configuration, kappa), FP32
+    BiCGStab inside FP64 reliable updates to the FP64 full-lattice residual 1e-10.
+    One untimed call tunes the kernel shapes of every lattice; then the same call runs
+    with the lattices side by side (one host thread and stream each) and one after the
+    other.  Prints each schedule's wall seconds, aggregate sec/RHS and worst residual."""
+    import baylorlqcd_b200 as qq
+
+    lats, groups = [], []
+    qq.initlagfib(0, 11)
+    for n, dims in enumerate(UNEVEN_DIMS):
+        lat = qq.Lattice(*dims, bc=(1, 1, 1, -1))
+        _, plaq = lat.heatbath(6.0, a.sweeps, seed=31 + n)
+        lats.append(lat)
+        print("configuration", dims, "plaquette %.6f" % plaq, flush=True)
+        for kappa in UNEVEN_KAPPAS:
+            be = np.zeros((4,) + lat.half_shape)
+            bo = np.zeros((4,) + lat.half_shape)
+            for i in range(2):
+                be[i], bo[i] = lat.pointsource((1 + i, 1, 1, 1), i + 1, 2 * i + 1)
+            for i in range(2, 4):
+                be[i], bo[i] = lat.z4source()
+            groups.append((lat, be, bo, (kappa, 0.0)))
+    nrhs = sum(g[1].shape[0] for g in groups)
+    kw = dict(precision=a.precision, rhs_block=a.rhs_block, tol=1e-10, deflate=0)
+    try:
+        qq.fermprop_uneven(groups, concurrent=False, **kw)  # tuning
+    except qq.QQError as e:
+        print("tuning call:", e, flush=True)
+    for conc in (True, False):
+        try:
+            out, secs = qq.fermprop_uneven(groups, concurrent=conc, **kw)
+        except qq.QQError as e:
+            print("uneven batch, %s: %s" % ("concurrent" if conc else "sequential", e), flush=True)
+            continue
+        infos = [i for _, _, inf in out for i in inf]
+        worst = max(i.true_rel for i in infos)
+        bad = sum(i.status != 0 for i in infos)
+        print("uneven batch, %s: %d solves on %d lattices, %.3f s, %.4f s/RHS, max true rel %.2e, %d not converged"
+              % ("concurrent" if conc else "sequential", nrhs, len(lats), secs, secs / nrhs, worst, bad), flush=True)
+    for lat in lats:
+        lat.close()
+
+
 def main(argv=None) -> int:
     p = argparse.ArgumentParser(prog="python -m baylorlqcd_b200.probe")
     sub = p.add_subparsers(dest="cmd", required=True)
@@ -194,8 +245,13 @@ def main(argv=None) -> int:
     f.add_argument("--k", type=int, default=12)
     f.add_argument("--tol", type=float, default=1e-10)
     f.add_argument("--sweeps", type=int, default=200)
+    w = sub.add_parser("uneven")
+    w.add_argument("--sweeps", type=int, default=200)
+    w.add_argument("--precision", type=int, default=32)
+    w.add_argument("--rhs-block", type=int, default=4)
     a = p.parse_args(argv)
-    {"hop": run_hop, "solve": run_solve, "twvev": run_twvev, "discon": run_discon, "shift": run_shift}[a.cmd](a)
+    {"hop": run_hop, "solve": run_solve, "twvev": run_twvev, "discon": run_discon, "shift": run_shift,
+     "uneven": run_uneven}[a.cmd](a)
     return 0
 
 

@@ -201,6 +201,31 @@ int qq_fermprop_batch(qq_ctx* ctx, int nrhs, const double* be, const double* bo,
                       const double kappa[2], const qq_method* method, double* xe, double* xo,
                       qq_solve_info* infos);
 
+/* Uneven batch: propagator solves over several lattices, gauge fields and kappa values
+ * in one call (the reference runs them as separate cfgsprops jobs, one fermprop per
+ * source: Q/quark.f90:458-842 through C/cfgsprops.f90).  A group is nrhs sources on
+ * the lattice and gauge field of its context at one kappa, solved exactly as
+ * qq_fermprop_batch solves them (be/bo/xe/xo in that entry point's layout for the
+ * group's context; infos: nrhs reports, may be NULL).  concurrent = 1: one host thread
+ * per distinct context, its groups in array order, the contexts side by side on their
+ * own streams; concurrent = 0: every group in array order on the calling thread.
+ * A context must not be used by any other thread during the call.  seconds (may be
+ * NULL): wall time of the whole call, every solve synchronised.  Returns the worst
+ * status (a hard error stops that context's later groups; QQ_NOT_CONVERGED with every
+ * output filled if a solve stopped short). */
+typedef struct qq_uneven_group {
+  qq_ctx* ctx;
+  int nrhs;
+  double kappa[2];   /* kappa, twisted mass mu */
+  const double* be;
+  const double* bo;
+  double* xe;
+  double* xo;
+  qq_solve_info* infos;
+} qq_uneven_group;
+int qq_fermprop_uneven(int ngroups, const qq_uneven_group* groups, const qq_method* method,
+                       int concurrent, double* seconds);
+
 /* ---- noise sources and loop traces (Q/disconloops.f90, G/lagfib.f90) ---- */
 /* initlagfib G/lagfib.f90:80-92 (process-global generator state, as the reference). */
 int qq_initlagfib(int myid, int iseed);

@@ -61,6 +61,20 @@ def test_bad_boundary_rejected():
     assert e.value.status == qq.QQ_BAD_ARG
 
 
+def test_uneven_batch_rejects_bad_arguments_before_device():
+    """qq_fermprop_uneven checks every group before it starts a solve (no device needed)."""
+    lib = qq.load_library()
+    meth = qq.qq_method(16, 6, 32, 4, 1e-10, 0, 1, 0, 1e-5)
+    assert lib.qq_fermprop_uneven(0, None, C.byref(meth), 1, None) == qq.QQ_BAD_ARG
+    buf = np.zeros(8)
+    groups = (qq.qq_uneven_group * 2)()
+    for i in range(2):  # null context in both groups (positional, as fermprop_uneven builds them)
+        groups[i] = qq.qq_uneven_group(None, 1, (C.c_double * 2)(0.15, 0.0), buf.ctypes.data, buf.ctypes.data,
+                                       buf.ctypes.data, buf.ctypes.data, None)
+    assert lib.qq_fermprop_uneven(2, groups, C.byref(meth), 1, None) == qq.QQ_BAD_ARG
+    assert b"group 0" in lib.qq_last_error()
+
+
 def test_missing_gpu_fails_loudly():
     """No CPU fallback: without a device the context cannot be created."""
     if gpu_present():

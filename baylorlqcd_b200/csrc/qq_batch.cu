@@ -689,9 +689,34 @@ int batch_solve(qq_ctx* c, int nrhs, const double* be, const double* bo, const d
       std::vector<SolveStats> bst(nb);
       for (int k = 0; k < nb; ++k) blk.push_back(R[i0 + k].get());
       tic();
-      const int st = bicgstab_block(c, blk, prec, tol_even, 0.1, maxiter, kappa,
-                                          defl.k > 0 ? &defl : nullptr, bst);
+      int st = bicgstab_block(c, blk, prec, tol_even, 0.1, maxiter, kappa,
+                                    defl.k > 0 ? &defl : nullptr, bst);
       const double sec = toc();
+      // A breakdown of the reduced-precision recurrences (a NaN, met near critical kappa
+      // on small heatbath lattices) hands every unfinished right-hand side of the block
+      // to the reference method: plain FP64 GMRES-DR(m, k) from a zero guess, reported
+      // with fallback = 1.  Finished right-hand sides keep their solutions; the
+      // full-lattice residual below judges every one.
+      std::vector<int> fb_status(nb, -1);
+      std::vector<double> fb_sec(nb, 0.0);
+      if (st == QQ_NAN) {
+        for (int k = 0; k < nb && rc == QQ_OK; ++k) {
+          if (blk[k]->done) continue;
+          QQ_TRY(zero_field(c, blk[k]->x.sp()));
+          SolveStats fs;
+          tic();
+          const int sf = gmresdr_fp64(c, blk[k]->b.sp(), blk[k]->x.sp(), meth->m, meth->k, tol_even, 0, kappa,
+                                      nullptr, &fs);
+          fb_sec[k] = toc();
+          if (sf != QQ_OK && sf != QQ_NOT_CONVERGED) rc = sf;
+          fs.itercount += bst[k].itercount;
+          fs.mvp += bst[k].mvp;
+          fs.fallback = 1;
+          bst[k] = fs;
+          fb_status[k] = sf == QQ_OK ? QQ_OK : QQ_NOT_CONVERGED;
+        }
+        st = QQ_OK;
+      }
       for (int k = 0; k < nb; ++k) {
         // the deflation-building solve is charged to the first right-hand side
         if (i0 + k == 0 && meth->deflate) {
@@ -700,8 +725,8 @@ int batch_solve(qq_ctx* c, int nrhs, const double* be, const double* bo, const d
           bst[k].ritz = stats[0].ritz;
         }
         stats[i0 + k] = bst[k];
-        seconds[i0 + k] = sec / nb + (i0 + k == 0 ? defl_sec : 0.0);
-        status[i0 + k] = blk[k]->done ? QQ_OK : QQ_NOT_CONVERGED;
+        seconds[i0 + k] = sec / nb + fb_sec[k] + (i0 + k == 0 ? defl_sec : 0.0);
+        status[i0 + k] = fb_status[k] >= 0 ? fb_status[k] : blk[k]->done ? QQ_OK : QQ_NOT_CONVERGED;
       }
       if (st != QQ_OK && st != QQ_NOT_CONVERGED) rc = st;
     }

@@ -173,6 +173,7 @@ bool is_device_ptr(const void* p);
 // ---- Krylov solvers (qq_solvers.cu) ----
 struct SolveStats {
   int itercount = 0, mvp = 0, ncycles = 0;
+  int fallback = 0;  // 1: the reference method finished this solve (qq_solve_info.fallback)
   double true_rel = 0.0;
   std::vector<double> hist;
   std::vector<int> hist_mvp;

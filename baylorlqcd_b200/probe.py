@@ -201,8 +201,10 @@ def run_uneven(a):
         infos = [i for _, _, inf in out for i in inf]
         worst = max(i.true_rel for i in infos)
         bad = sum(i.status != 0 for i in infos)
-        print("uneven batch, %s: %d solves on %d lattices, %.3f s, %.4f s/RHS, max true rel %.2e, %d not converged"
-              % ("concurrent" if conc else "sequential", nrhs, len(lats), secs, secs / nrhs, worst, bad), flush=True)
+        fb = sum(i.fallback for i in infos)
+        print("uneven batch, %s: %d solves on %d lattices, %.3f s, %.4f s/RHS, max true rel %.2e, %d not converged, "
+              "%d by the GMRES-DR fallback" % ("concurrent" if conc else "sequential", nrhs, len(lats), secs,
+                                               secs / nrhs, worst, bad, fb), flush=True)
     for lat in lats:
         lat.close()
 

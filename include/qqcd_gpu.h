@@ -57,7 +57,9 @@ typedef struct qq_solve_info {
   int hist_mvp[1024];
   int nritz;          /* harmonic Ritz values of the last restart (re, im) */
   double ritz[2 * 512];
-  int fallback;       /* qq_fgmres: 1 if plain GMRES-DR took over from a stalled cycle */
+  int fallback;       /* qq_fgmres: 1 if plain GMRES-DR took over from a stalled cycle;
+                        qq_fermprop_batch: 1 if the batched BiCGStab broke down (NaN) and
+                        plain FP64 GMRES-DR(m, k) solved this right-hand side from zero */
 } qq_solve_info;
 
 /* ---- context ---- */
@@ -182,8 +184,10 @@ int qq_pointsource(qq_ctx* ctx, double* be, double* bo, const int src[4], int ic
  * with mixed-precision GMRES-DR(m, k) (FP32 Krylov basis and FP32 operator inside
  * FP64 iterative refinement); the others are projected onto it and solved together
  * in blocks with a multi-right-hand-side FP32 (precision = 32) or FP16 (precision =
- * 16) BiCGStab inside FP64 reliable updates.  be/bo/xe/xo: nrhs reference-layout
- * halves each, packed one after the other. */
+ * 16) BiCGStab inside FP64 reliable updates.  If that BiCGStab breaks down (a NaN in
+ * its recurrences), every unfinished right-hand side of the block is solved again from
+ * zero by plain FP64 GMRES-DR(m, k) and reported with fallback = 1.  be/bo/xe/xo: nrhs
+ * reference-layout halves each, packed one after the other. */
 typedef struct qq_method {
   int m, k;          /* GMRES-DR(m, k) */
   int precision;     /* BiCGStab arithmetic: 64, 32 or 16 (FP64 reliable updates) */

@@ -87,3 +87,26 @@ def test_uneven_rejects_bad_group(lattices):
     be = np.zeros((0,) + lat.half_shape)
     with pytest.raises(qq.QQError):
         qq.fermprop_uneven([(lat, be, be, (0.150, 0.0))])
+
+
+def test_breakdown_falls_back_to_gmresdr(lattices):
+    """Twisted mass at kappa = 0.1565, mu = 0.005 on the 8^4 configuration, where the
+    FP32 batched BiCGStab has broken down (NaN) on Z(4) sources: every right-hand side
+    must still reach the FP64 residual (through the GMRES-DR fallback where the
+    BiCGStab broke down) and agree with the oracle's FP64 solve."""
+    import baylorlqcd_b200 as qq
+
+    lat, ol = lattices[0]
+    qq.initlagfib(0, 9)
+    be, bo = mixed_sources(qq, lat, 1, 1)
+    kappa = (0.1565, 0.005)
+    xe, xo, infos = lat.fermprop_batch(be, bo, kappa, m=16, k=6, precision=32, rhs_block=4, tol=1e-10,
+                                       solver=1, deflate=0)
+    for i in range(2):
+        assert infos[i].status == 0, (i, infos[i])
+        assert infos[i].true_rel <= 1e-10
+        assert infos[i].fallback in (0, 1)
+        xe_o, xo_o, st, _ = ol.fermprop(be[i], bo[i], kappa, inverter=5, resmax=1e-12, nGMRES=(16, 6))
+        assert st == 0
+        assert interior_rel(xe[i], xe_o, ol.nvhalf) < 1e-7, i
+        assert interior_rel(xo[i], xo_o, ol.nvhalf) < 1e-7, i

@@ -63,7 +63,7 @@ class qq_solve_info(C.Structure):
 class qq_method(C.Structure):
     _fields_ = [("m", C.c_int), ("k", C.c_int), ("precision", C.c_int), ("rhs_block", C.c_int),
                 ("tol", C.c_double), ("max_outer", C.c_int), ("solver", C.c_int), ("deflate", C.c_int),
-                ("defl_tol", C.c_double)]
+                ("defl_tol", C.c_double), ("stall_window", C.c_int)]
 
 
 class qq_uneven_group(C.Structure):
@@ -467,17 +467,19 @@ class Lattice:
         return be, bo
 
     def fermprop_batch(self, be, bo, kappa, m=60, k=20, precision=32, rhs_block=12, tol=1e-10,
-                       max_outer=0, solver=1, deflate=1, defl_tol=1e-5, xe=None, xo=None):
+                       max_outer=0, solver=1, deflate=1, defl_tol=1e-5, xe=None, xo=None, stall_window=0):
         """Batched propagators (qq_fermprop_batch): be, bo of shape (nrhs,) + half_shape,
         numpy (host) or torch CUDA tensors.  solver=0 is the reference's plain FP64
-        GMRES-DR(m,k) per right-hand side; solver=1 the deflated batched BiCGStab."""
+        GMRES-DR(m,k) per right-hand side; solver=1 the deflated batched BiCGStab, whose
+        right-hand sides that break down, stall for stall_window iterations (0: 2000) or
+        run out of iterations are finished by plain FP64 GMRES-DR (info.fallback)."""
         nrhs = be.shape[0]
         if xe is None:
             xe = np.zeros(be.shape) if isinstance(be, np.ndarray) else be.new_zeros(be.shape)
         if xo is None:
             xo = np.zeros(bo.shape) if isinstance(bo, np.ndarray) else bo.new_zeros(bo.shape)
         infos = (qq_solve_info * nrhs)()
-        meth = qq_method(m, k, precision, rhs_block, tol, max_outer, solver, deflate, defl_tol)
+        meth = qq_method(m, k, precision, rhs_block, tol, max_outer, solver, deflate, defl_tol, stall_window)
         st = self.lib.qq_fermprop_batch(self._ctx, nrhs, _ptr(be), _ptr(bo), _d2(kappa), C.byref(meth),
                                         _ptr(xe), _ptr(xo), infos)
         _check(st, allow_not_converged=True)
@@ -633,7 +635,7 @@ def momfacs(dims, io=(1, 1, 1)) -> np.ndarray:
 
 
 def fermprop_uneven(groups, m=60, k=20, precision=32, rhs_block=12, tol=1e-10, max_outer=0, solver=1,
-                    deflate=0, defl_tol=1e-5, concurrent=True):
+                    deflate=0, defl_tol=1e-5, concurrent=True, stall_window=0):
     """Uneven batch (qq_fermprop_uneven): groups is a list of (lattice, be, bo, kappa),
     be/bo of shape (nrhs,) + that lattice's half_shape, numpy or torch CUDA tensors.
     Each group is solved as Lattice.fermprop_batch solves it; with concurrent=True the
@@ -650,7 +652,7 @@ def fermprop_uneven(groups, m=60, k=20, precision=32, rhs_block=12, tol=1e-10, m
         arr[i] = qq_uneven_group(lat._ctx.value, nrhs, (C.c_double * 2)(*kappa), _ptr(be), _ptr(bo), _ptr(xe),
                                  _ptr(xo), C.cast(infos, C.POINTER(qq_solve_info)))
         keep.append((xe, xo, infos))
-    meth = qq_method(m, k, precision, rhs_block, tol, max_outer, solver, deflate, defl_tol)
+    meth = qq_method(m, k, precision, rhs_block, tol, max_outer, solver, deflate, defl_tol, stall_window)
     secs = C.c_double(0.0)
     _check(load_library().qq_fermprop_uneven(n, arr, C.byref(meth), int(bool(concurrent)), C.byref(secs)),
            allow_not_converged=True)

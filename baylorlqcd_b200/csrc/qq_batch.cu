@@ -24,19 +24,55 @@ namespace qq {
 
 namespace {
 
+// Workspace ids of the batched solver in the context (qq_ctx::ws).  Solves of the
+// same size reuse the buffers, so a repeated qq_fermprop_batch allocates nothing.
+enum WsId : int {
+  WS_BLOCK = 0,  // + 2 f: data of block field f (7 fields), + 2 f + 1: its FP16 norms
+  WS_SCAL = 20,  // scalars and control words
+  WS_PART,       // reduction partials
+  WS_DSLOTS,     // scalar slot of each right-hand side
+  WS_HIST,       // true-residual history
+  WS_HITS,       // iterations at each history entry
+  WS_RHS = 64,   // + 3 i + j: right-hand side i's b, x, r64
+};
+
+// A field carved from a context workspace (non-owning).
+struct WsField {
+  Spinor s{nullptr, nullptr, P64};
+  size_t bytes = 0, norm_bytes = 0;
+  Spinor sp() const { return s; }
+};
+
+int ws_field(qq_ctx* c, WsField& f, int id, int prec, int nsites_mult = 1) {
+  void* d = nullptr;
+  void* n = nullptr;
+  f.bytes = field_bytes(prec, c->g.vh) * nsites_mult;
+  QQ_CK(ws_get(c, id, f.bytes, &d));
+  f.norm_bytes = 0;
+  if (prec == P16) {
+    f.norm_bytes = sizeof(float) * c->g.vh * nsites_mult;
+    QQ_CK(ws_get(c, id + 1, f.norm_bytes, &n));
+  }
+  f.s = Spinor{d, static_cast<float*>(n), prec};
+  return QQ_OK;
+}
+
+// The seven block fields of a batched BiCGStab, zeroed.
+int block_fields(qq_ctx* c, int prec, int nb, WsField* const* fs) {
+  for (int i = 0; i < 7; ++i) {
+    QQ_TRY(ws_field(c, *fs[i], WS_BLOCK + 2 * i, prec, nb));
+    QQ_CK(cudaMemsetAsync(fs[i]->s.data, 0, fs[i]->bytes, c->st));
+    if (prec == P16) QQ_CK(cudaMemsetAsync(fs[i]->s.norm, 0, fs[i]->norm_bytes, c->st));
+  }
+  return QQ_OK;
+}
+
 struct PerRhs {
-  Field b, x;                  // FP64 even-system source and solution
-  Field r64;                   // FP64 residual
+  WsField b, x;                // FP64 even-system source and solution
+  WsField r64;                 // FP64 residual
   double bn = 0.0, rmax = 0.0, rn = 0.0;
   bool done = false;
 };
-
-int alloc_field(qq_ctx* c, Field& f, int prec, int nsites_mult = 1) {
-  f.prec = prec;
-  QQ_CK(f.data.alloc(field_bytes(prec, c->g.vh) * nsites_mult));
-  if (prec == P16) QQ_CK(f.norm.alloc(sizeof(float) * c->g.vh * nsites_mult));
-  return QQ_OK;
-}
 
 template <int P>
 int launch_block_op(qq_ctx* c, const BlockBiArgs& A, int op) {
@@ -58,6 +94,7 @@ struct ScalarCtl {
   unsigned* ctl;     // control words (active, pending)
   double delta;      // reliable-update threshold
   double half_tol;   // 0.5 * tolerance
+  int window;        // stall window in iterations (0: none)
 };
 
 int block_op(qq_ctx* c, int prec, const BlockBiArgs& A, int op, const int* dslots, int step,
@@ -71,7 +108,7 @@ int block_op(qq_ctx* c, int prec, const BlockBiArgs& A, int op, const int* dslot
     QQ_TRY(launch_block_op<P64>(c, A, op));
   if (step >= 0) {
     bicg_scalar_kernel<<<A.nb, 256, 0, c->st>>>(A.S, dslots, A.partial, kRedBlocks, step, sc.ctl,
-                                                sc.delta, sc.half_tol);
+                                                sc.delta, sc.half_tol, sc.window);
     QQ_CK(cudaGetLastError());
   }
   return QQ_OK;
@@ -81,7 +118,7 @@ int block_op(qq_ctx* c, int prec, const BlockBiArgs& A, int op, const int* dslot
 int scalar_step(qq_ctx* c, const BlockBiArgs& A, const int* dslots, int step, int nblocks, const ScalarCtl& sc) {
   count_launch();
   bicg_scalar_kernel<<<A.nb, 256, 0, c->st>>>(A.S, dslots, A.partial, nblocks, step, sc.ctl, sc.delta,
-                                              sc.half_tol);
+                                              sc.half_tol, sc.window);
   QQ_CK(cudaGetLastError());
   return QQ_OK;
 }
@@ -112,6 +149,21 @@ int block_slot(qq_ctx* c, int prec, int nb, int k, Spinor blockf, Spinor x, int 
   return QQ_OK;
 }
 
+// Stall window of the batched BiCGStab (iterations without a 10x fall of the FP64 true
+// residual) when the method leaves it at 0.
+constexpr int kStallWindow = 2000;
+
+// Iteration limit of the batched BiCGStab when the method sets none: 40 iterations per
+// lattice extent per decade of tolerance, clamped to [2000, 100000] -- 20,000 for
+// 24^3x48 at 1e-10, 3,600 for 8^4.  Near critical kappa the iteration count grows with
+// the lattice extent (the lowest Dirac mode falls like 1/L), and linearly with the
+// decades to cover.
+int default_maxiter(const Geom& g, double tol) {
+  const int lmax = std::max(std::max(g.n[0], g.n[1]), std::max(g.n[2], g.n[3]));
+  const double decades = std::max(1.0, std::ceil(-std::log10(std::max(tol, 1e-300))));
+  return (int)std::min(100000.0, std::max(2000.0, 40.0 * lmax * decades));
+}
+
 bool host_loop_forced() {
   const char* e = std::getenv("QQ_HOST_LOOP");  // testing: the host-driven loop
   return e && std::atoi(e) != 0;
@@ -124,16 +176,18 @@ bool host_loop_forced() {
 struct GraphLoop {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
-  cudaStream_t aux = nullptr;
+  cudaStream_t aux = nullptr;  // the context's second stream (kept with the context)
   long long per_iter = 0, per_update = 0;
+  // The launches of a finished run: iters iterations and nupd reliable updates.
+  void count(long long iters, long long nupd) const { count_launch(per_iter * iters + per_update * nupd); }
   ~GraphLoop() {
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
-    if (aux) cudaStreamDestroy(aux);
   }
   template <class Chunk, class Update>
   int build(qq_ctx* c, int nb, unsigned* ctl, unsigned all, int maxiter, Chunk& chunk, Update& update) {
-    QQ_CK(cudaStreamCreateWithFlags(&aux, cudaStreamNonBlocking));
+    if (!c->aux_st) QQ_CK(cudaStreamCreateWithFlags(&c->aux_st, cudaStreamNonBlocking));
+    aux = c->aux_st;
     QQ_CK(cudaGraphCreate(&graph, 0));
     cudaGraphConditionalHandle hw;
     QQ_CK(cudaGraphConditionalHandleCreate(&hw, graph, 1, cudaGraphCondAssignDefault));
@@ -146,11 +200,13 @@ struct GraphLoop {
     QQ_CK(cudaGraphAddNode(&wn, graph, nullptr, 0, &wp));
     CondHandles hs = {};
     for (int k = 0; k < nb; ++k) QQ_CK(cudaGraphConditionalHandleCreate(&hs.h[k], wp.conditional.phGraph_out[0], 0, 0));
-    const long long n0 = launch_count();
+    // launches are counted per host thread, so contexts capturing side by side (the
+    // uneven batch) do not pick up each other's launches
+    const long long n0 = thread_launch_count();
     QQ_CK(cudaStreamBeginCaptureToGraph(c->st, wp.conditional.phGraph_out[0], nullptr, nullptr, 0,
                                         cudaStreamCaptureModeThreadLocal));
     int rc = chunk();
-    per_iter = launch_count() - n0 + 2;  // + the two condition kernels
+    per_iter = thread_launch_count() - n0 + 2;  // + the two condition kernels
     if (rc == QQ_OK) {
       count_launch();
       reliable_conds_kernel<<<1, 32, 0, c->st>>>(ctl, hs, nb);
@@ -175,7 +231,7 @@ struct GraphLoop {
       }
       // the IF body: right-hand side k's update, captured from the second stream
       std::swap(c->st, aux);
-      const long long m0 = launch_count();
+      const long long m0 = thread_launch_count();
       if (cudaStreamBeginCaptureToGraph(c->st, ip.conditional.phGraph_out[0], nullptr, nullptr, 0,
                                         cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
         std::swap(c->st, aux);
@@ -183,7 +239,7 @@ struct GraphLoop {
         break;
       }
       rc = update(k);
-      per_update = launch_count() - m0;
+      per_update = thread_launch_count() - m0;
       cudaGraph_t ig = nullptr;
       const cudaError_t ee = cudaStreamEndCapture(c->st, &ig);
       std::swap(c->st, aux);
@@ -196,7 +252,7 @@ struct GraphLoop {
     }
     cudaGraph_t bg = nullptr;
     const cudaError_t e = cudaStreamEndCapture(c->st, &bg);
-    count_launch(-(launch_count() - n0));  // captured, not launched: counted when the graph runs
+    count_launch(-(thread_launch_count() - n0));  // captured, not launched: counted when the graph runs
     if (rc != QQ_OK) return rc;
     QQ_CK(e);
     QQ_CK(cudaGraphInstantiate(&exec, graph, 0));
@@ -226,6 +282,19 @@ int full_residual(qq_ctx* c, Spinor be, Spinor bo, Spinor xe, Spinor xo, const d
   return QQ_OK;
 }
 
+// Scalars of a right-hand side before its first iteration: rhat = r = the FP64
+// residual of the initial guess, whose norm also anchors the stall test.
+void init_scalars(double* sc, const PerRhs& R) {
+  sc[SC_RHO] = sc[SC_ALPHA] = sc[SC_OMEGA] = 1.0;
+  sc[SC_RMAX] = R.rmax;
+  sc[SC_BN] = R.bn > 0.0 ? R.bn : 1.0;
+  sc[SC_R2] = R.rn * R.rn;
+  sc[SC_RHATN] = R.rn;
+  sc[SC_CHK_R] = R.rn;
+  sc[SC_CHK_ITS] = 0.0;
+  sc[SC_FAIL] = 0.0;
+}
+
 }  // namespace
 
 // BiCGStab on a block of right-hand sides in precision `prec` (block fields), FP64
@@ -234,25 +303,26 @@ int full_residual(qq_ctx* c, Spinor be, Spinor bo, Spinor xe, Spinor xo, const d
 // (projected onto the deflation space first, if any) and the iteration continues with
 // the same search direction.
 int bicgstab_block_sync(qq_ctx* c, std::vector<PerRhs*>& rhs, int prec, double tol, double delta,
-                        int maxiter, const double kappa[2], const DeflSpace* defl,
+                        int maxiter, int window, const double kappa[2], const DeflSpace* defl,
                         std::vector<SolveStats>& stats) {
   const int nb = (int)rhs.size();
   if (nb == 0) return QQ_OK;
   if (nb > kMaxBatch) return set_error(QQ_BAD_ARG, "too many right-hand sides in one block");
-  Field r, rhat, p, v, t, xl, tmp;
-  for (Field* f : {&r, &rhat, &p, &v, &t, &xl, &tmp}) {
-    QQ_TRY(alloc_field(c, *f, prec, nb));
-    QQ_CK(cudaMemsetAsync(f->data.p, 0, f->data.bytes, c->st));
-    if (prec == P16) QQ_CK(cudaMemsetAsync(f->norm.p, 0, f->norm.bytes, c->st));
+  WsField r, rhat, p, v, t, xl, tmp;
+  {
+    WsField* const fs[7] = {&r, &rhat, &p, &v, &t, &xl, &tmp};
+    QQ_TRY(block_fields(c, prec, nb, fs));
   }
   // scalars of every right-hand side, then the control words
   constexpr size_t kScalDoubles = (size_t)kScal * kMaxBatch;
   constexpr size_t kSyncDoubles = kScalDoubles + (kCtlWords + 1) / 2;
-  DevBuf S, part, dslots;
-  QQ_CK(S.alloc(sizeof(double) * (kSyncDoubles)));
-  QQ_CK(part.alloc(sizeof(double) * 3 * std::max(kRedBlocks, hop_block_count(c, nb)) * kMaxBatch));
-  QQ_CK(dslots.alloc(sizeof(int) * kMaxBatch));
-  unsigned* ctl = reinterpret_cast<unsigned*>(S.as<double>() + kScalDoubles);
+  double *Sd = nullptr, *partd = nullptr;
+  int* ds = nullptr;
+  QQ_CK(ws_get(c, WS_SCAL, sizeof(double) * (kSyncDoubles), reinterpret_cast<void**>(&Sd)));
+  QQ_CK(ws_get(c, WS_PART, sizeof(double) * 3 * std::max(kRedBlocks, hop_block_count(c, nb)) * kMaxBatch,
+               reinterpret_cast<void**>(&partd)));
+  QQ_CK(ws_get(c, WS_DSLOTS, sizeof(int) * kMaxBatch, reinterpret_cast<void**>(&ds)));
+  unsigned* ctl = reinterpret_cast<unsigned*>(Sd + kScalDoubles);
   Tmp tmp64(c, P64), h(c, P64);
   double* s1 = c->scal.as<double>();
   // FP64 residual of x (and of the deflated x) -> slot k of r and rhat
@@ -288,15 +358,12 @@ int bicgstab_block_sync(qq_ctx* c, std::vector<PerRhs*>& rhs, int prec, double t
     if (!R.done) active |= 1u << k;
     QQ_TRY(block_slot(c, prec, nb, k, r.sp(), R.r64.sp(), 0));
     QQ_TRY(block_slot(c, prec, nb, k, rhat.sp(), R.r64.sp(), 0));
-    double* sc = &hS[(size_t)k * kScal];
-    sc[SC_RHO] = sc[SC_ALPHA] = sc[SC_OMEGA] = 1.0;
-    sc[SC_RMAX] = R.rmax;
-    sc[SC_BN] = R.bn;
+    init_scalars(&hS[(size_t)k * kScal], R);
   }
   hctl[CTL_ACTIVE] = active;
   hctl[CTL_PENDING] = 0u;
-  QQ_CK(cudaMemcpyAsync(S.p, hS, sizeof(double) * (kSyncDoubles), cudaMemcpyHostToDevice, c->st));
-  QQ_CK(cudaMemcpyAsync(dslots.p, slots.data(), sizeof(int) * nb, cudaMemcpyHostToDevice, c->st));
+  QQ_CK(cudaMemcpyAsync(Sd, hS, sizeof(double) * (kSyncDoubles), cudaMemcpyHostToDevice, c->st));
+  QQ_CK(cudaMemcpyAsync(ds, slots.data(), sizeof(int) * nb, cudaMemcpyHostToDevice, c->st));
   QQ_CK(cudaStreamSynchronize(c->st));
   BlockBiArgs A;
   std::memset(&A, 0, sizeof(A));
@@ -310,10 +377,9 @@ int bicgstab_block_sync(qq_ctx* c, std::vector<PerRhs*>& rhs, int prec, double t
   A.t = t.sp();
   A.x = xl.sp();
   for (int k = 0; k < nb; ++k) A.slot[k] = k;
-  A.S = S.as<double>();
-  A.partial = part.as<double>();
-  const int* ds = dslots.as<int>();
-  const ScalarCtl sc{ctl, delta, 0.5 * tol};
+  A.S = Sd;
+  A.partial = partd;
+  const ScalarCtl sc{ctl, delta, 0.5 * tol, window};
   // Iterations run in chunks without host synchronisation: a right-hand side whose
   // residual calls for a reliable update (or may have converged) takes itself out of
   // the active mask on the device and waits, pending, for the end of the chunk, where
@@ -331,10 +397,14 @@ int bicgstab_block_sync(qq_ctx* c, std::vector<PerRhs*>& rhs, int prec, double t
       QQ_TRY(block_op(c, prec, A, OP_XR_UPDATE, ds, ST_R2, sc));
     }
     done_its += nchunk;
-    QQ_CK(cudaMemcpyAsync(hS, S.p, sizeof(double) * (kSyncDoubles), cudaMemcpyDeviceToHost, c->st));
+    QQ_CK(cudaMemcpyAsync(hS, Sd, sizeof(double) * (kSyncDoubles), cudaMemcpyDeviceToHost, c->st));
     QQ_CK(cudaStreamSynchronize(c->st));
-    if (hctl[CTL_NAN]) return set_error(QQ_NAN, "NaN residual in batched BiCGStab");
-    const unsigned pending = hctl[CTL_PENDING];
+    // right-hand sides the device stopped (NaN, breakdown, stagnation) leave the loop
+    const unsigned failed = hctl[CTL_FAIL] & active;
+    for (int k = 0; k < nb; ++k)
+      if ((failed >> k) & 1u) stats[k].fallback = (int)hS[(size_t)k * kScal + SC_FAIL];
+    active &= ~failed;
+    const unsigned pending = hctl[CTL_PENDING] & active;
     unsigned back = 0;  // right-hand sides that iterate again after their update
     for (int k = 0; k < nb; ++k) {
       PerRhs& R = *rhs[k];
@@ -343,8 +413,7 @@ int bicgstab_block_sync(qq_ctx* c, std::vector<PerRhs*>& rhs, int prec, double t
       st.mvp += 2 * (its - st.itercount);
       st.itercount = its;
       if (!((pending >> k) & 1u)) continue;
-      const double rn = std::sqrt(hS[(size_t)k * kScal + SC_R2]);
-      if (!std::isfinite(rn)) return set_error(QQ_NAN, "NaN residual in batched BiCGStab");
+      double* sk = &hS[(size_t)k * kScal];
       // reliable update
       QQ_TRY(block_slot(c, prec, nb, k, xl.sp(), R.x.sp(), 1));
       QQ_TRY(block_slot(c, prec, nb, k, xl.sp(), R.x.sp(), 2));
@@ -352,6 +421,15 @@ int bicgstab_block_sync(qq_ctx* c, std::vector<PerRhs*>& rhs, int prec, double t
       st.true_rel = R.rn / R.bn;
       st.hist.push_back(st.true_rel);
       st.hist_mvp.push_back(st.mvp);
+      if (R.rn < 0.1 * sk[SC_CHK_R]) {  // progress anchor of the stall test
+        sk[SC_CHK_R] = R.rn;
+        sk[SC_CHK_ITS] = its;
+      }
+      if (!std::isfinite(R.rn)) {
+        st.fallback = FAIL_NAN;
+        active &= ~(1u << k);
+        continue;
+      }
       if (R.rn / R.bn <= tol) {
         R.done = true;
         active &= ~(1u << k);
@@ -359,18 +437,23 @@ int bicgstab_block_sync(qq_ctx* c, std::vector<PerRhs*>& rhs, int prec, double t
       }
       QQ_TRY(block_slot(c, prec, nb, k, r.sp(), R.r64.sp(), 0));
       R.rmax = R.rn;
-      hS[(size_t)k * kScal + SC_RMAX] = R.rmax;
+      sk[SC_RMAX] = R.rmax;
+      sk[SC_R2] = R.rn * R.rn;
       back |= 1u << k;
     }
-    if (pending) {
+    if (pending || failed) {
       active = (hctl[CTL_ACTIVE] | back) & active;
       hctl[CTL_ACTIVE] = active;
       hctl[CTL_PENDING] = 0u;
-      QQ_CK(cudaMemcpyAsync(S.p, hS, sizeof(double) * (kSyncDoubles), cudaMemcpyHostToDevice, c->st));
+      QQ_CK(cudaMemcpyAsync(Sd, hS, sizeof(double) * (kSyncDoubles), cudaMemcpyHostToDevice, c->st));
     }
   }
   QQ_CK(cudaStreamSynchronize(c->st));
-  return active ? QQ_NOT_CONVERGED : QQ_OK;
+  for (int k = 0; k < nb; ++k)
+    if (!rhs[k]->done && stats[k].fallback == FAIL_NONE) stats[k].fallback = FAIL_MAXITER;
+  bool all_done = true;
+  for (auto* R : rhs) all_done = all_done && R->done;
+  return all_done ? QQ_OK : QQ_NOT_CONVERGED;
 }
 
 // Device-driven variant (no deflation): the reliable update itself runs on the device
@@ -390,30 +473,31 @@ int bicgstab_block_sync(qq_ctx* c, std::vector<PerRhs*>& rhs, int prec, double t
 //    at step c are visible from snapshot c + 1 on, so earlier snapshots' pending marks
 //    for them are skipped.
 int bicgstab_block(qq_ctx* c, std::vector<PerRhs*>& rhs, int prec, double tol, double delta,
-                   int maxiter, const double kappa[2], const DeflSpace* defl,
+                   int maxiter, int window, const double kappa[2], const DeflSpace* defl,
                    std::vector<SolveStats>& stats) {
-  if (defl && defl->k > 0) return bicgstab_block_sync(c, rhs, prec, tol, delta, maxiter, kappa, defl, stats);
+  if (defl && defl->k > 0)
+    return bicgstab_block_sync(c, rhs, prec, tol, delta, maxiter, window, kappa, defl, stats);
   const int nb = (int)rhs.size();
   if (nb == 0) return QQ_OK;
   if (nb > kMaxBatch) return set_error(QQ_BAD_ARG, "too many right-hand sides in one block");
-  Field r, rhat, p, v, t, xl, tmp;
-  for (Field* f : {&r, &rhat, &p, &v, &t, &xl, &tmp}) {
-    QQ_TRY(alloc_field(c, *f, prec, nb));
-    QQ_CK(cudaMemsetAsync(f->data.p, 0, f->data.bytes, c->st));
-    if (prec == P16) QQ_CK(cudaMemsetAsync(f->norm.p, 0, f->norm.bytes, c->st));
+  WsField r, rhat, p, v, t, xl, tmp;
+  {
+    WsField* const fs[7] = {&r, &rhat, &p, &v, &t, &xl, &tmp};
+    QQ_TRY(block_fields(c, prec, nb, fs));
   }
   constexpr size_t kScalDoubles = (size_t)kScal * kMaxBatch;
   constexpr size_t kSnap = kScalDoubles + (kCtlWords + 1) / 2;  // scalars + control words
   constexpr int kHist = 1024;  // true-residual history per right-hand side (qq_solve_info)
   const size_t sbytes = sizeof(double) * kSnap;
   static_assert(1024 + 2 * kSnap <= 3072, "snapshots exceed the pinned buffer");
-  DevBuf S, part, dslots, dhist, dhits;
-  QQ_CK(S.alloc(sbytes));
-  QQ_CK(dhist.alloc(sizeof(double) * kHist * nb));
-  QQ_CK(dhits.alloc(sizeof(int) * kHist * nb));
-  QQ_CK(part.alloc(sizeof(double) * 3 * std::max(kRedBlocks, hop_block_count(c, nb)) * kMaxBatch));
-  QQ_CK(dslots.alloc(sizeof(int) * kMaxBatch));
-  double* Sd = S.as<double>();
+  double *Sd = nullptr, *partd = nullptr, *dhist = nullptr;
+  int *ds = nullptr, *dhits = nullptr;
+  QQ_CK(ws_get(c, WS_SCAL, sbytes, reinterpret_cast<void**>(&Sd)));
+  QQ_CK(ws_get(c, WS_HIST, sizeof(double) * kHist * nb, reinterpret_cast<void**>(&dhist)));
+  QQ_CK(ws_get(c, WS_HITS, sizeof(int) * kHist * nb, reinterpret_cast<void**>(&dhits)));
+  QQ_CK(ws_get(c, WS_PART, sizeof(double) * 3 * std::max(kRedBlocks, hop_block_count(c, nb)) * kMaxBatch,
+               reinterpret_cast<void**>(&partd)));
+  QQ_CK(ws_get(c, WS_DSLOTS, sizeof(int) * kMaxBatch, reinterpret_cast<void**>(&ds)));
   unsigned* ctl = reinterpret_cast<unsigned*>(Sd + kScalDoubles);
   double* snap[2] = {c->hpin + 1024, c->hpin + 1024 + kSnap};
   Tmp tmp64(c, P64), h(c, P64);
@@ -444,15 +528,12 @@ int bicgstab_block(qq_ctx* c, std::vector<PerRhs*>& rhs, int prec, double tol, d
       active |= 1u << k;
     QQ_TRY(block_slot(c, prec, nb, k, r.sp(), R.r64.sp(), 0));
     QQ_TRY(block_slot(c, prec, nb, k, rhat.sp(), R.r64.sp(), 0));
-    double* sc = &hS[(size_t)k * kScal];
-    sc[SC_RHO] = sc[SC_ALPHA] = sc[SC_OMEGA] = 1.0;
-    sc[SC_RMAX] = R.rmax;
-    sc[SC_BN] = R.bn > 0.0 ? R.bn : 1.0;
+    init_scalars(&hS[(size_t)k * kScal], R);
   }
   hctl[CTL_ACTIVE] = active;
   hctl[CTL_DONE] = done;
   QQ_CK(cudaMemcpyAsync(Sd, hS, sbytes, cudaMemcpyHostToDevice, c->st));
-  QQ_CK(cudaMemcpyAsync(dslots.p, slots.data(), sizeof(int) * nb, cudaMemcpyHostToDevice, c->st));
+  QQ_CK(cudaMemcpyAsync(ds, slots.data(), sizeof(int) * nb, cudaMemcpyHostToDevice, c->st));
   QQ_CK(cudaStreamSynchronize(c->st));
   const unsigned all = nb == 32 ? 0xffffffffu : (1u << nb) - 1u;
   if ((done & all) == all) return QQ_OK;
@@ -469,9 +550,8 @@ int bicgstab_block(qq_ctx* c, std::vector<PerRhs*>& rhs, int prec, double tol, d
   A.x = xl.sp();
   for (int k = 0; k < nb; ++k) A.slot[k] = k;
   A.S = Sd;
-  A.partial = part.as<double>();
-  const int* ds = dslots.as<int>();
-  const ScalarCtl sctl{ctl, delta, 0.5 * tol};
+  A.partial = partd;
+  const ScalarCtl sctl{ctl, delta, 0.5 * tol, window};
   constexpr int kChunk = 1;  // a pending RHS idles 1-2 iterations before its update runs
   auto run_chunk = [&]() -> int {
     for (int i = 0; i < kChunk; ++i) {
@@ -493,7 +573,7 @@ int bicgstab_block(qq_ctx* c, std::vector<PerRhs*>& rhs, int prec, double tol, d
     QQ_TRY(lin(c, R.r64.sp(), cimm(1.0), R.b.sp(), cimm(-1.0), h.sp(), cimm(0), Spinor{nullptr, nullptr, P64},
                Sd + (size_t)k * kScal + SC_T2));
     count_launch(2);
-    reliable_decide_kernel<<<1, 1, 0, c->st>>>(Sd, ds, ctl, k, tol, dhist.as<double>(), dhits.as<int>(), kHist);
+    reliable_decide_kernel<<<1, 1, 0, c->st>>>(Sd, ds, ctl, k, tol, dhist, dhits, kHist);
     QQ_CK(cudaGetLastError());
     QQ_TRY(block_slot(c, prec, nb, k, r.sp(), R.r64.sp(), 0, ctl + CTL_INSERT));
     reliable_resume_kernel<<<1, 1, 0, c->st>>>(ctl, k);
@@ -511,12 +591,12 @@ int bicgstab_block(qq_ctx* c, std::vector<PerRhs*>& rhs, int prec, double tol, d
     QQ_CK(cudaMemcpyAsync(hS, Sd, sbytes, cudaMemcpyDeviceToHost, c->st));
     std::vector<double> hist((size_t)kHist * nb);
     std::vector<int> hits((size_t)kHist * nb);
-    QQ_CK(cudaMemcpyAsync(hist.data(), dhist.p, sizeof(double) * hist.size(), cudaMemcpyDeviceToHost, c->st));
-    QQ_CK(cudaMemcpyAsync(hits.data(), dhits.p, sizeof(int) * hits.size(), cudaMemcpyDeviceToHost, c->st));
+    QQ_CK(cudaMemcpyAsync(hist.data(), dhist, sizeof(double) * hist.size(), cudaMemcpyDeviceToHost, c->st));
+    QQ_CK(cudaMemcpyAsync(hits.data(), dhits, sizeof(int) * hits.size(), cudaMemcpyDeviceToHost, c->st));
     QQ_CK(cudaStreamSynchronize(c->st));
     const unsigned* hc = reinterpret_cast<const unsigned*>(hS + kScalDoubles);
     long long nupd_all = 0;
-    bool nan = false;
+    const unsigned failed = hc[CTL_FAIL] & all;
     for (int k = 0; k < nb; ++k) {
       SolveStats& st = stats[k];
       const double* sk = hS + (size_t)k * kScal;
@@ -524,18 +604,19 @@ int bicgstab_block(qq_ctx* c, std::vector<PerRhs*>& rhs, int prec, double tol, d
       st.itercount = its;
       st.mvp += 2 * its + nupd;
       for (int j = 0; j < std::min(nupd, kHist); ++j) {
-        const double rel = hist[(size_t)k * kHist + j];
-        nan = nan || !std::isfinite(rel);
-        st.hist.push_back(rel);
+        st.hist.push_back(hist[(size_t)k * kHist + j]);
         st.hist_mvp.push_back(1 + 2 * hits[(size_t)k * kHist + j] + j + 1);
       }
       if (nupd > 0) st.true_rel = sk[SC_TRUE];
       nupd_all += nupd;
+      if ((failed >> k) & 1u) st.fallback = (int)sk[SC_FAIL];
     }
-    count_launch(gl.per_iter * (long long)hc[CTL_ITER] + gl.per_update * nupd_all);
-    if (nan || (hc[CTL_NAN] & all)) return set_error(QQ_NAN, "NaN residual in batched BiCGStab");
-    done = hc[CTL_DONE];
-    for (int k = 0; k < nb; ++k) rhs[k]->done = (done >> k) & 1u;
+    gl.count(hc[CTL_ITER], nupd_all);
+    done = hc[CTL_DONE] & ~failed;  // converged
+    for (int k = 0; k < nb; ++k) {
+      rhs[k]->done = (done >> k) & 1u;
+      if (!rhs[k]->done && stats[k].fallback == FAIL_NONE) stats[k].fallback = FAIL_MAXITER;
+    }
     return (done & all) == all ? QQ_OK : QQ_NOT_CONVERGED;
   }
   cudaEvent_t ev[2];
@@ -549,6 +630,7 @@ int bicgstab_block(qq_ctx* c, std::vector<PerRhs*>& rhs, int prec, double tol, d
     }
   } evg{ev};
   std::vector<int> enq(nb, -1), nupd_seen(nb, 0);
+  unsigned failed = 0;
   int chunks = 0;
   QQ_TRY(run_chunk());
   ++chunks;
@@ -578,7 +660,6 @@ int bicgstab_block(qq_ctx* c, std::vector<PerRhs*>& rhs, int prec, double tol, d
       const int nupd = (int)sk[SC_NUPD];
       if (nupd > nupd_seen[k]) {
         const double rel = sk[SC_TRUE];
-        if (!std::isfinite(rel)) return set_error(QQ_NAN, "NaN true residual in batched BiCGStab");
         st.mvp += nupd - nupd_seen[k];
         st.true_rel = rel;
         st.hist.push_back(rel);
@@ -586,15 +667,14 @@ int bicgstab_block(qq_ctx* c, std::vector<PerRhs*>& rhs, int prec, double tol, d
         nupd_seen[k] = nupd;
       }
     }
-    if (sc[CTL_NAN] & all) return set_error(QQ_NAN, "NaN residual in batched BiCGStab");
-    done = sc[CTL_DONE];
+    failed = sc[CTL_FAIL] & all;
+    done = sc[CTL_DONE];  // converged or stopped
     if ((done & all) == all) break;
     const unsigned pend = sc[CTL_PENDING] & ~done;
     bool queued = false, inflight = false;
     for (int k = 0; k < nb; ++k) {
       if (enq[k] >= sidx) inflight = true;
       if (!((pend >> k) & 1u) || enq[k] >= sidx) continue;
-      if (!std::isfinite(sv[(size_t)k * kScal + SC_R2])) return set_error(QQ_NAN, "NaN residual in batched BiCGStab");
       QQ_TRY(reliable(k));
       enq[k] = step;
       queued = true;
@@ -607,7 +687,17 @@ int bicgstab_block(qq_ctx* c, std::vector<PerRhs*>& rhs, int prec, double tol, d
     }
   }
   QQ_CK(cudaStreamSynchronize(c->st));
-  for (int k = 0; k < nb; ++k) rhs[k]->done = (done >> k) & 1u;
+  {  // the final scalars: failure reasons of stopped right-hand sides
+    QQ_CK(cudaMemcpy(hS, Sd, sbytes, cudaMemcpyDeviceToHost));
+    const unsigned* hc = reinterpret_cast<const unsigned*>(hS + kScalDoubles);
+    failed = hc[CTL_FAIL] & all;
+    done = hc[CTL_DONE] & ~failed;
+  }
+  for (int k = 0; k < nb; ++k) {
+    rhs[k]->done = (done >> k) & 1u;
+    if ((failed >> k) & 1u) stats[k].fallback = (int)hS[(size_t)k * kScal + SC_FAIL];
+    else if (!rhs[k]->done) stats[k].fallback = FAIL_MAXITER;
+  }
   return rc == QQ_OK && (done & all) == all ? QQ_OK : QQ_NOT_CONVERGED;
 }
 
@@ -634,9 +724,9 @@ int batch_solve(qq_ctx* c, int nrhs, const double* be, const double* bo, const d
   for (int i = 0; i < nrhs; ++i) {
     R[i].reset(new PerRhs());
     PerRhs& r = *R[i];
-    QQ_TRY(alloc_field(c, r.b, P64));
-    QQ_TRY(alloc_field(c, r.x, P64));
-    QQ_TRY(alloc_field(c, r.r64, P64));
+    QQ_TRY(ws_field(c, r.b, WS_RHS + 3 * i, P64));
+    QQ_TRY(ws_field(c, r.x, WS_RHS + 3 * i + 1, P64));
+    QQ_TRY(ws_field(c, r.r64, WS_RHS + 3 * i + 2, P64));
     QQ_TRY(zero_field(c, r.x.sp()));
     // fermprop source: b_e/kappa^2 + H_eo (1 - 2 i kappa mu gamma5) b_o / (kappa (1 + tk^2))
     const double* de = nullptr;
@@ -661,7 +751,8 @@ int batch_solve(qq_ctx* c, int nrhs, const double* be, const double* bo, const d
     return ms * 1e-3;
   };
   int rc = QQ_OK;
-  const int maxiter = meth->max_outer > 0 ? 1000 * meth->max_outer : 200000;
+  const int maxiter = meth->max_outer > 0 ? 1000 * meth->max_outer : default_maxiter(c->g, meth->tol);
+  const int window = meth->stall_window > 0 ? meth->stall_window : kStallWindow;
   if (meth->solver == 0) {
     for (int i = 0; i < nrhs && rc == QQ_OK; ++i) {
       tic();
@@ -689,29 +780,42 @@ int batch_solve(qq_ctx* c, int nrhs, const double* be, const double* bo, const d
       std::vector<SolveStats> bst(nb);
       for (int k = 0; k < nb; ++k) blk.push_back(R[i0 + k].get());
       tic();
-      int st = bicgstab_block(c, blk, prec, tol_even, 0.1, maxiter, kappa,
-                                    defl.k > 0 ? &defl : nullptr, bst);
+      int st = bicgstab_block(c, blk, prec, tol_even, 0.1, maxiter, window, kappa,
+                              defl.k > 0 ? &defl : nullptr, bst);
       const double sec = toc();
-      // A breakdown of the reduced-precision recurrences (a NaN, met near critical kappa
-      // on small heatbath lattices) hands every unfinished right-hand side of the block
-      // to the reference method: plain FP64 GMRES-DR(m, k) from a zero guess, reported
-      // with fallback = 1.  Finished right-hand sides keep their solutions; the
+      // Every right-hand side the batched BiCGStab did not finish -- a breakdown (NaN,
+      // vanishing rho or omega), a stall, or the iteration limit; bst[k].fallback holds
+      // the reason -- goes to the reference method, plain FP64 GMRES-DR(m, k).  It
+      // starts from the BiCGStab's FP64 solution when that is finite and better than
+      // zero, with its relative tolerance rescaled so that it stops at the same
+      // ||b - A x|| <= tol ||b||.  Finished right-hand sides keep their solutions; the
       // full-lattice residual below judges every one.
       std::vector<int> fb_status(nb, -1);
       std::vector<double> fb_sec(nb, 0.0);
-      if (st == QQ_NAN) {
+      if (st == QQ_OK || st == QQ_NOT_CONVERGED) {
         for (int k = 0; k < nb && rc == QQ_OK; ++k) {
           if (blk[k]->done) continue;
-          QQ_TRY(zero_field(c, blk[k]->x.sp()));
-          SolveStats fs;
+          PerRhs& B = *blk[k];
           tic();
-          const int sf = gmresdr_fp64(c, blk[k]->b.sp(), blk[k]->x.sp(), meth->m, meth->k, tol_even, 0, kappa,
-                                      nullptr, &fs);
+          double r0 = 0.0;
+          QQ_TRY(op_dbletm(c, h.sp(), B.x.sp(), fbo.sp(), 0, kappa));
+          QQ_TRY(lin(c, B.r64.sp(), cimm(1.0), B.b.sp(), cimm(-1.0), h.sp(), cimm(0),
+                     Spinor{nullptr, nullptr, P64}, c->scal.as<double>()));
+          QQ_TRY(read_scalars(c, c->scal.as<double>(), 1, &r0));
+          r0 = std::sqrt(r0);
+          double resmax = tol_even;
+          if (std::isfinite(r0) && r0 > 0.0 && r0 < B.bn) {
+            resmax = std::min(1.0, tol_even * B.bn / r0);
+          } else {
+            QQ_TRY(zero_field(c, B.x.sp()));
+          }
+          SolveStats fs;
+          const int sf = gmresdr_fp64(c, B.b.sp(), B.x.sp(), meth->m, meth->k, resmax, 0, kappa, nullptr, &fs);
           fb_sec[k] = toc();
           if (sf != QQ_OK && sf != QQ_NOT_CONVERGED) rc = sf;
           fs.itercount += bst[k].itercount;
-          fs.mvp += bst[k].mvp;
-          fs.fallback = 1;
+          fs.mvp += bst[k].mvp + 1;
+          fs.fallback = bst[k].fallback != FAIL_NONE ? bst[k].fallback : FAIL_MAXITER;
           bst[k] = fs;
           fb_status[k] = sf == QQ_OK ? QQ_OK : QQ_NOT_CONVERGED;
         }
@@ -764,6 +868,38 @@ int batch_solve(qq_ctx* c, int nrhs, const double* be, const double* bo, const d
   }
   for (int i = 0; i < nrhs; ++i)
     if (status[i] != QQ_OK) return QQ_NOT_CONVERGED;
+  return QQ_OK;
+}
+
+// Launch once every hopping shape a qq_fermprop_batch of nrhs sources with this method
+// uses, so the autotuner makes its choices now and caches them in the context: the
+// block operator (and its fused-dot form) at every block size the solve will form, and
+// the FP64 single-field operators of the setup, the reliable updates and the fallback.
+// The uneven batch runs this for each context on the calling thread before its worker
+// threads start, so no candidate is timed while other contexts' solves share the GPU.
+int tune_batch_shapes(qq_ctx* c, int nrhs, const double kappa[2], const qq_method* meth) {
+  const int prec = meth->precision == 64 ? P64 : meth->precision == 32 ? P32 : meth->precision == 16 ? P16 : -1;
+  if (prec < 0 || nrhs < 1) return set_error(QQ_BAD_ARG, "bad method or nrhs");
+  Tmp a64(c, P64), b64(c, P64), t64(c, P64);
+  QQ_TRY(zero_field(c, a64.sp()));
+  QQ_TRY(op_dbletm(c, b64.sp(), a64.sp(), t64.sp(), 0, kappa));
+  QQ_TRY(op_hsingle(c, b64.sp(), a64.sp(), 0, 0));
+  QQ_TRY(op_hsingle(c, b64.sp(), a64.sp(), 0, 1));
+  if (meth->solver == 1) {
+    const int block = std::max(1, std::min(meth->rhs_block, kMaxBatch));
+    for (int nb : {std::min(block, nrhs), nrhs % block}) {
+      if (nb < 1) continue;
+      WsField in, out, tmp;
+      WsField* const fs[3] = {&in, &out, &tmp};
+      for (int i = 0; i < 3; ++i) {
+        QQ_TRY(ws_field(c, *fs[i], WS_BLOCK + 2 * i, prec, nb));
+        QQ_CK(cudaMemsetAsync(fs[i]->s.data, 0, fs[i]->bytes, c->st));
+        if (prec == P16) QQ_CK(cudaMemsetAsync(fs[i]->s.norm, 0, fs[i]->norm_bytes, c->st));
+      }
+      QQ_TRY(op_dbletm_block(c, out.sp(), in.sp(), tmp.sp(), nb, 0, kappa));
+    }
+  }
+  QQ_CK(cudaStreamSynchronize(c->st));
   return QQ_OK;
 }
 

@@ -124,6 +124,8 @@ int qq_ctx_destroy(qq_ctx* c) {
   cudaSetDevice(c->device);
   if (c->st) cudaStreamSynchronize(c->st);
   for (auto& p : c->pool) p.clear();
+  c->ws.clear();
+  if (c->aux_st) cudaStreamDestroy(c->aux_st);
   if (c->hpin) cudaFreeHost(c->hpin);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);

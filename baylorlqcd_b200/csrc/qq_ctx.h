@@ -98,7 +98,6 @@ struct qq_ctx {
   qq::DevBuf partial;       // reduction partials
   qq::DevBuf scal;          // device scalar slots
   qq::DevBuf trace_buf;     // per-site loop-trace values and the time-slice sums
-  qq::DevBuf tune_flush;    // L2-sized buffer overwritten between autotuner timings
   double* hpin = nullptr;   // pinned host memory: [0, 1024) read_scalars staging,
                             // [1024, 3072) the batched solver's two scalar snapshots
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -111,11 +110,26 @@ struct qq_ctx {
   size_t prof_used = 0;
   std::vector<std::unique_ptr<qq::Field>> pool[3];  // temporaries per precision
   std::vector<bool> pool_busy[3];
+  // Persistent workspaces of the batched solver, by id (qq::ws_get): allocated on first
+  // use, grown when a later call needs more, freed with the context.
+  std::map<int, std::unique_ptr<qq::DevBuf>> ws;
+  cudaStream_t aux_st = nullptr;  // second stream: graph capture of reliable updates
 
   size_t ref_doubles() const { return (size_t)6 * rd.ntotal * 64; }
 };
 
 namespace qq {
+
+// Workspace `id` of the context with at least `bytes` bytes.  Repeated solves of the
+// same size reuse it, so they call neither cudaMalloc nor the device-synchronising
+// cudaFree.  Ids are owned by one routine at a time (see qq_batch.cu).
+inline cudaError_t ws_get(qq_ctx* c, int id, size_t bytes, void** p) {
+  auto& slot = c->ws[id];
+  if (!slot) slot.reset(new DevBuf());
+  const cudaError_t e = slot->alloc(bytes);
+  *p = slot->p;
+  return e;
+}
 
 // Temporary field from the context pool (returned on scope exit).
 struct Tmp {
@@ -199,6 +213,8 @@ int defl_project(qq_ctx* c, const DeflSpace& d, Spinor b, Spinor x, Spinor r, co
                  double* rn);
 
 void fill_info(qq_solve_info* info, int status, const SolveStats& s, double seconds);
+// Tune every hopping shape a qq_fermprop_batch(nrhs, meth) launches (qq_batch.cu).
+int tune_batch_shapes(qq_ctx* c, int nrhs, const double kappa[2], const qq_method* meth);
 // Flexible GMRES(m) with right preconditioner M(z, v): z = M v (qq_solvers.cu).
 int fgmres_fp64(qq_ctx* c, Spinor phi, Spinor x, int m, double resmax, int max_cycles, const double kappa[2],
                 const std::function<int(Spinor, Spinor)>& M, SolveStats* st, bool* stalled);

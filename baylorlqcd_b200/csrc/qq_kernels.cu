@@ -1,5 +1,8 @@
 // Instantiations and launchers of the library's CUDA kernels (sm_100a).
 #include <atomic>
+#include <map>
+#include <mutex>
+#include <utility>
 
 #include "qq_blas.cuh"
 #include "qq_dslash.cuh"
@@ -10,8 +13,31 @@
 namespace qq {
 
 static std::atomic<long long> g_launches{0};
-void count_launch(long long n) { g_launches += n; }
+static thread_local long long t_launches = 0;
+void count_launch(long long n) {
+  g_launches += n;
+  t_launches += n;
+}
 long long launch_count() { return g_launches.load(); }
+long long thread_launch_count() { return t_launches; }
+
+// The dynamic shared-memory limit of a kernel is a per-device attribute: set it once per
+// (kernel, device) -- the current device -- and remember the result.  Host threads that
+// launch side by side (one per context) serialise here only on the first launch.
+static cudaError_t smem_attr_once(const void* kernel, int bytes) {
+  static std::mutex mu;
+  static std::map<std::pair<const void*, int>, cudaError_t> done;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lock(mu);
+  const auto key = std::make_pair(kernel, dev);
+  auto it = done.find(key);
+  if (it != done.end()) return it->second;
+  e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  done[key] = e;
+  return e;
+}
 
 // ---------------------------------------------------------------------------
 // Dslash
@@ -46,10 +72,7 @@ template <int SP, int LP, int RECON, int EPI>
 static cudaError_t hop_staged_launch(const HopArgs& a, int T, cudaStream_t st) {
   const size_t smem = staged_smem_bytes<SP, LP, RECON>(T);
   if (smem > 227 * 1024) return cudaErrorInvalidValue;
-  // one attribute call per instantiation; a function-local static is initialised once
-  // even when several host threads (one per context) launch at the same time
-  static const cudaError_t attr = cudaFuncSetAttribute(hop_staged_kernel<SP, LP, RECON, EPI>,
-                                                       cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+  const cudaError_t attr = smem_attr_once((const void*)hop_staged_kernel<SP, LP, RECON, EPI>, 227 * 1024);
   if (attr != cudaSuccess) return attr;
   const HopArgs b = hop_prepare(a, T / a.nrhs, a.nrhs);
   dim3 grd((a.g.vh + b.per_block - 1) / b.per_block);
@@ -149,9 +172,8 @@ static cudaError_t hop_f2s(const HopArgs& a, int epi, cudaStream_t st) {
 // Copy-ring kernel: D stages in flight per thread, RPT right-hand sides per thread.
 template <int EPI, int D, int RPT>
 static cudaError_t hop_f2a_epi(const HopArgs& b, size_t smem, cudaStream_t st) {
-  // One attribute call per instantiation: 227 KiB less the kernel's static shared
-  // memory.  A function-local static is initialised once even when several host
-  // threads (one per context) launch at the same time.
+  // The limit is 227 KiB less the kernel's static shared memory (the same on every
+  // device; a function-local static is initialised once even under concurrent launches).
   struct Attr {
     cudaError_t err;
     size_t max_dyn;
@@ -160,12 +182,12 @@ static cudaError_t hop_f2a_epi(const HopArgs& b, size_t smem, cudaStream_t st) {
     cudaFuncAttributes fa;
     cudaError_t e = cudaFuncGetAttributes(&fa, hop_f2a_kernel<EPI, D, RPT>);
     if (e != cudaSuccess) return Attr{e, 0};
-    const size_t md = (size_t)227 * 1024 - fa.sharedSizeBytes;
-    e = cudaFuncSetAttribute(hop_f2a_kernel<EPI, D, RPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)md);
-    return Attr{e, md};
+    return Attr{cudaSuccess, (size_t)227 * 1024 - fa.sharedSizeBytes};
   }();
   if (attr.err != cudaSuccess) return attr.err;
   if (smem > attr.max_dyn) return cudaErrorInvalidValue;
+  const cudaError_t e = smem_attr_once((const void*)hop_f2a_kernel<EPI, D, RPT>, (int)attr.max_dyn);
+  if (e != cudaSuccess) return e;
   const int G = b.nrhs / RPT;
   const dim3 blk(b.per_block * G), grd((b.g.vh + b.per_block - 1) / b.per_block);
   hop_f2a_kernel<EPI, D, RPT><<<grd, blk, smem, st>>>(b);
@@ -364,7 +386,8 @@ cudaError_t launch_rotate(int pb, const BasisArgs& V, int nin, int nout, const d
 #define QQ_ROT(PB, MO)                                                                       \
   do {                                                                                       \
     auto k = rotate_kernel<PB, MO>;                                                          \
-    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);        \
+    const cudaError_t ea = smem_attr_once((const void*)k, 200 * 1024);                       \
+    if (ea != cudaSuccess) return ea;                                                        \
     k<<<grid, 128, smem, st>>>(V, nin, nout, Z, ldz);                                        \
   } while (0)
   if (pb == P64) {

@@ -6,9 +6,11 @@
 
 namespace qq {
 
-// Kernel-launch counter (every launcher below adds its launches).
+// Kernel-launch counter (every launcher below adds its launches): the process total,
+// and the launches made by the calling host thread.
 void count_launch(long long n = 1);
 long long launch_count();
+long long thread_launch_count();
 
 struct HopArgs;
 struct LinArgs;

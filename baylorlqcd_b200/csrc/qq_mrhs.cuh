@@ -26,16 +26,18 @@ enum ScalSlot : int {
   SC_T2 = 13,      // ||b - A x||^2 of the last reliable update (FP64)
   SC_TRUE = 14,    // ||b - A x|| / ||b|| of the last reliable update
   SC_NUPD = 15,    // reliable updates done
-  kScal = 16,
+  SC_RHATN = 16,   // ||rhat|| (the shadow residual is fixed for the whole solve)
+  SC_CHK_R = 17,   // progress anchor: the FP64 true ||b - A x|| that last fell 10x
+  SC_CHK_ITS = 18, // iterations done when the anchor was set
+  SC_FAIL = 19,    // why the right-hand side was stopped (FailCode), 0 while it runs
+  kScal = 20,
 };
 
-// Control words after the scalar slots: [0] active mask (bit r: right-hand side r
-// iterates), [1] pending mask (bit r: r stopped and waits for its reliable update or
-// convergence test), [2] done mask (r converged), [3] insert mask (r's new FP64
-// residual is to replace its iterated one).
-// Control words: bit k of ACTIVE / PENDING / DONE / INSERT / NAN = right-hand side k
-// iterates / awaits its reliable update / is finished / is re-inserted / stopped on a
-// non-finite residual; ITER counts the iterations of the graph-driven loop.
+// Control words after the scalar slots: bit k of ACTIVE / PENDING / DONE / INSERT /
+// NAN / FAIL = right-hand side k iterates / awaits its reliable update or convergence
+// test / is finished (converged or stopped) / is re-inserted / stopped on a non-finite
+// value / stopped without converging (reason in its SC_FAIL); ITER counts the
+// iterations of the graph-driven loop.
 enum CtlWord : int {
   CTL_ACTIVE = 0,
   CTL_PENDING = 1,
@@ -43,8 +45,24 @@ enum CtlWord : int {
   CTL_INSERT = 3,
   CTL_ITER = 4,
   CTL_NAN = 5,
-  kCtlWords = 6
+  CTL_FAIL = 6,
+  kCtlWords = 7
 };
+
+// Why the batched BiCGStab stopped a right-hand side short of its tolerance; the
+// caller hands such a right-hand side to plain FP64 GMRES-DR (qq_solve_info.fallback).
+enum FailCode : int {
+  FAIL_NONE = 0,
+  FAIL_NAN = 1,        // a non-finite scalar or residual
+  FAIL_BREAKDOWN = 2,  // rho = <rhat, r>, <rhat, v>, ||t|| or omega = <t, s> / ||t||^2 vanished
+  FAIL_STALL = 3,      // the FP64 true residual did not fall 10x within the stall window
+  FAIL_MAXITER = 4,    // the iteration limit ran out (set by the host)
+};
+
+// Relative size below which a BiCGStab inner product counts as a breakdown:
+// |<rhat, r>| <= kBreakEps ||rhat|| ||r||, and the same for omega.  Only a degenerate
+// (numerically zero) product trips it; slow progress is the stall window's business.
+constexpr double kBreakEps = 1e-12;
 
 enum BiOp : int {
   OP_DOT_RHAT_R = 0,  // red: <rhat, r>
@@ -166,14 +184,31 @@ enum ScalStep : int {
   ST_R2 = 3,     // ||r||^2
 };
 
+// Right-hand side k stops for good, short of its tolerance, for reason `code`: it
+// leaves the active mask and counts as finished for the loop; the host reads CTL_FAIL
+// and SC_FAIL and solves it again with the fallback method.
+__device__ inline void bicg_fail(double* s, unsigned* ctl, int k, int code) {
+  const unsigned bit = 1u << k;
+  s[SC_FAIL] = (double)code;
+  atomicAnd(&ctl[CTL_ACTIVE], ~bit);
+  atomicAnd(&ctl[CTL_PENDING], ~bit);
+  atomicOr(&ctl[CTL_FAIL], bit);
+  atomicOr(&ctl[CTL_DONE], bit);
+  if (code == FAIL_NAN) atomicOr(&ctl[CTL_NAN], bit);
+}
+
 // One block per right-hand side: sum the partials (fixed order), update the scalars.
 // At ST_R2 it also counts the iteration and, when ||r|| has dropped below delta times
-// its value at the last reliable update or below half_tol ||b|| (or is not finite),
-// takes the right-hand side out of the active mask and marks it pending, so the
-// iteration needs no host round trip until the host next looks.
+// its value at the last reliable update or below half_tol ||b||, takes the right-hand
+// side out of the active mask and marks it pending, so the iteration needs no host
+// round trip until the host next looks.
+// A right-hand side stops (bicg_fail) when a scalar is not finite, when BiCGStab breaks
+// down (<rhat, r>, <rhat, v>, ||t|| or <t, s> numerically zero), or when `window` > 0
+// iterations have passed since its FP64 true residual last fell 10x (stagnation; the
+// anchor is moved by reliable_decide_kernel).
 static __global__ void bicg_scalar_kernel(double* S, const int* slots, const double* partial,
                                           int nblocks, int step, unsigned* ctl, double delta,
-                                          double half_tol) {
+                                          double half_tol, int window) {
   const int k = blockIdx.x;
   __shared__ double red[3][256];
   double a[3] = {0.0, 0.0, 0.0};
@@ -194,7 +229,11 @@ static __global__ void bicg_scalar_kernel(double* S, const int* slots, const dou
     *cr = (ar * br + ai * bi) / den;
     *ci = (ai * br - ar * bi) / den;
   };
+  const double rnorm = sqrt(s[SC_R2]);  // ||r|| of the previous iteration (or update)
   if (step == ST_BETA) {
+    const double rho = sqrt(d0 * d0 + d1 * d1);
+    if (!isfinite(rho)) return bicg_fail(s, ctl, k, FAIL_NAN);
+    if (rho <= kBreakEps * s[SC_RHATN] * rnorm) return bicg_fail(s, ctl, k, FAIL_BREAKDOWN);
     double qr, qi, pr, pi;
     cdiv(d0, d1, s[SC_RHO], s[SC_RHO + 1], &qr, &qi);                           // rho'/rho
     cdiv(s[SC_ALPHA], s[SC_ALPHA + 1], s[SC_OMEGA], s[SC_OMEGA + 1], &pr, &pi);  // alpha/omega
@@ -202,9 +241,17 @@ static __global__ void bicg_scalar_kernel(double* S, const int* slots, const dou
     s[SC_BETA + 1] = qr * pi + qi * pr;
     s[SC_RHO] = d0;
     s[SC_RHO + 1] = d1;
+    if (!isfinite(s[SC_BETA]) || !isfinite(s[SC_BETA + 1])) return bicg_fail(s, ctl, k, FAIL_NAN);
   } else if (step == ST_ALPHA) {
+    const double den = sqrt(d0 * d0 + d1 * d1);
+    if (!isfinite(den)) return bicg_fail(s, ctl, k, FAIL_NAN);
+    if (!(den > 0.0)) return bicg_fail(s, ctl, k, FAIL_BREAKDOWN);
     cdiv(s[SC_RHO], s[SC_RHO + 1], d0, d1, &s[SC_ALPHA], &s[SC_ALPHA + 1]);
+    if (!isfinite(s[SC_ALPHA]) || !isfinite(s[SC_ALPHA + 1])) return bicg_fail(s, ctl, k, FAIL_NAN);
   } else if (step == ST_OMEGA) {
+    if (!isfinite(d0) || !isfinite(d1) || !isfinite(d2)) return bicg_fail(s, ctl, k, FAIL_NAN);
+    if (!(d2 > 0.0) || sqrt(d0 * d0 + d1 * d1) <= kBreakEps * sqrt(d2) * rnorm)
+      return bicg_fail(s, ctl, k, FAIL_BREAKDOWN);
     s[SC_OMEGA] = d0 / d2;
     s[SC_OMEGA + 1] = d1 / d2;
     s[SC_TT] = d2;
@@ -212,20 +259,20 @@ static __global__ void bicg_scalar_kernel(double* S, const int* slots, const dou
     s[SC_R2] = d0;
     s[SC_ITS] += 1.0;
     const double rn = sqrt(d0);
-    if (!isfinite(rn)) {  // diverged: k stops, flagged for the host
-      atomicAnd(&ctl[CTL_ACTIVE], ~(1u << k));
-      atomicOr(&ctl[CTL_NAN], 1u << k);
-      atomicOr(&ctl[CTL_DONE], 1u << k);
-    } else if (rn < delta * s[SC_RMAX] || rn < half_tol * s[SC_BN]) {
+    if (!isfinite(rn)) return bicg_fail(s, ctl, k, FAIL_NAN);
+    if (rn < delta * s[SC_RMAX] || rn < half_tol * s[SC_BN]) {
       atomicAnd(&ctl[CTL_ACTIVE], ~(1u << k));
       atomicOr(&ctl[CTL_PENDING], 1u << k);
+    } else if (window > 0 && s[SC_ITS] - s[SC_CHK_ITS] >= (double)window) {
+      bicg_fail(s, ctl, k, FAIL_STALL);
     }
   }
 }
 
 // End of right-hand side k's reliable update, after ||b - A x||^2 has landed in
-// S[SC_T2]: record the true residual, decide convergence, and either mark k done or
-// arm the re-insertion of the FP64 residual (rmax = ||r||).  One thread.
+// S[SC_T2]: record the true residual, move the progress anchor when it has fallen 10x,
+// decide convergence, and either mark k done or arm the re-insertion of the FP64
+// residual (rmax = ||r||).  One thread.
 // Every decision is also appended to right-hand side k's history: hist[k * hmax + j] =
 // the j-th true relative residual, hist_its[k * hmax + j] = the iterations done then.
 static __global__ void reliable_decide_kernel(double* S, const int* slots, unsigned* ctl, int k,
@@ -241,12 +288,21 @@ static __global__ void reliable_decide_kernel(double* S, const int* slots, unsig
   }
   s[SC_NUPD] += 1.0;
   const unsigned bit = 1u << k;
-  if (!(rel > tol)) {  // converged, or a NaN true residual (flagged for the host)
-    if (!isfinite(rel)) atomicOr(&ctl[CTL_NAN], bit);
+  if (rn < 0.1 * s[SC_CHK_R]) {
+    s[SC_CHK_R] = rn;
+    s[SC_CHK_ITS] = s[SC_ITS];
+  }
+  if (!isfinite(rel)) {
+    atomicAnd(&ctl[CTL_INSERT], ~bit);
+    bicg_fail(s, ctl, k, FAIL_NAN);
+    return;
+  }
+  if (!(rel > tol)) {  // converged
     atomicOr(&ctl[CTL_DONE], bit);
     atomicAnd(&ctl[CTL_INSERT], ~bit);
   } else {
     s[SC_RMAX] = rn;
+    s[SC_R2] = s[SC_T2];
     atomicOr(&ctl[CTL_INSERT], bit);
   }
   atomicAnd(&ctl[CTL_PENDING], ~bit);

@@ -1,5 +1,7 @@
 // Operator application, level-1 helpers and reference-layout staging for the C ABI.
 #include <algorithm>
+#include <map>
+#include <mutex>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -140,6 +142,30 @@ static int launch_hop_profiled(qq_ctx* c, const HopArgs& a, int prec, int recon,
   return QQ_OK;
 }
 
+// The autotuner's L2 flush buffer: one per device, shared by every context on it and
+// kept until the process exits, so a context's first tuning allocates nothing (and does
+// not synchronise the device under other contexts' solves) once any context has tuned.
+static cudaError_t tune_flush_buffer(void** p, size_t* bytes) {
+  static std::mutex mu;
+  static std::map<int, void*> bufs;
+  constexpr size_t kBytes = (size_t)256 << 20;  // twice the L2
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lock(mu);
+  void*& b = bufs[dev];
+  if (!b) {
+    e = cudaMalloc(&b, kBytes);
+    if (e != cudaSuccess) {
+      b = nullptr;
+      return e;
+    }
+  }
+  *p = b;
+  *bytes = kBytes;
+  return cudaSuccess;
+}
+
 int hop_tune_key(qq_ctx* c, const HopArgs& a, int prec, int epi) {
   return (((prec * 64 + recon_of(c, prec)) * 64 + a.nrhs) * 4 + epi) * 2 + a.blk;
 }
@@ -159,7 +185,9 @@ int launch_hop_tuned(qq_ctx* c, const HopArgs& a, int prec, int epi) {
   // Candidates are timed as the solvers run them, with operands streamed from HBM: a
   // 256 MiB buffer (twice the L2) is overwritten before every timed launch.  Each
   // candidate is timed three times and its median kept, so the choice is stable.
-  QQ_CK(c->tune_flush.alloc((size_t)256 << 20));
+  void* flush = nullptr;
+  size_t flush_bytes = 0;
+  QQ_CK(tune_flush_buffer(&flush, &flush_bytes));
   int best = 1;
   float best_ms = 1e30f;
   for (int tps : {1, 2, 32, 64, 96, 128, kShapeMrhs + 2, kShapeMrhs + 3, kShapeMrhs + 4, kShapeF2 + 1,
@@ -185,7 +213,7 @@ int launch_hop_tuned(qq_ctx* c, const HopArgs& a, int prec, int epi) {
     }
     float t[3];
     for (int rep = 0; rep < 3; ++rep) {
-      QQ_CK(cudaMemsetAsync(c->tune_flush.p, rep + 1, c->tune_flush.bytes, c->st));
+      QQ_CK(cudaMemsetAsync(flush, rep + 1, flush_bytes, c->st));
       QQ_CK(cudaEventRecord(c->tev0, c->st));
       QQ_CK(launch_hop(a, prec, recon, epi, tps, c->st));
       QQ_CK(cudaEventRecord(c->tev1, c->st));

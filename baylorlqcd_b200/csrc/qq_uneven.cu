@@ -54,6 +54,15 @@ extern "C" int qq_fermprop_uneven(int ngroups, const qq_uneven_group* groups, co
   }
   const auto t0 = std::chrono::steady_clock::now();
   if (concurrent && work.size() > 1) {
+    // every context's hop shapes are tuned here, one context at a time, so no autotuner
+    // timing runs beside another context's solve (and the choice does not depend on the
+    // schedule); the solves below then find every shape in their context's table
+    for (int i = 0; i < ngroups; ++i) {
+      const qq_uneven_group& G = groups[i];
+      int st = cudaSetDevice(G.ctx->device) == cudaSuccess ? QQ_OK : QQ_CUDA_ERR;
+      if (st == QQ_OK) st = qq::tune_batch_shapes(G.ctx, G.nrhs, G.kappa, method);
+      if (st != QQ_OK) return qq::set_error(st, "group " + std::to_string(i) + ": " + qq_last_error());
+    }
     std::vector<std::thread> th;
     th.reserve(work.size());
     for (auto& w : work) th.emplace_back(run_ctx, std::ref(w), groups, method);

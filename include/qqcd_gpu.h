@@ -58,8 +58,13 @@ typedef struct qq_solve_info {
   int nritz;          /* harmonic Ritz values of the last restart (re, im) */
   double ritz[2 * 512];
   int fallback;       /* qq_fgmres: 1 if plain GMRES-DR took over from a stalled cycle;
-                        qq_fermprop_batch: 1 if the batched BiCGStab broke down (NaN) and
-                        plain FP64 GMRES-DR(m, k) solved this right-hand side from zero */
+                        qq_fermprop_batch: nonzero if the batched BiCGStab stopped short of
+                        the tolerance and plain FP64 GMRES-DR(m, k) finished this
+                        right-hand side (from the BiCGStab's solution when it is finite and
+                        better than zero): 1 a non-finite value, 2 a breakdown (rho,
+                        <rhat, v>, ||t|| or omega vanished), 3 a stall (the true residual
+                        did not fall 10x within qq_method.stall_window iterations),
+                        4 the iteration limit */
 } qq_solve_info;
 
 /* ---- context ---- */
@@ -200,6 +205,9 @@ typedef struct qq_method {
                         GMRES-DR(m,k) on the first right-hand side and project every
                         residual onto them at each reliable update */
   double defl_tol;   /* relative residual the deflation-building solve stops at */
+  int stall_window;  /* solver 1: a right-hand side whose FP64 true residual has not fallen
+                        10x within this many BiCGStab iterations stops and is solved by
+                        plain FP64 GMRES-DR(m, k), as after a breakdown (0: 2000) */
 } qq_method;
 int qq_fermprop_batch(qq_ctx* ctx, int nrhs, const double* be, const double* bo,
                       const double kappa[2], const qq_method* method, double* xe, double* xo,

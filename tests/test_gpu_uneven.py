@@ -89,11 +89,37 @@ def test_uneven_rejects_bad_group(lattices):
         qq.fermprop_uneven([(lat, be, be, (0.150, 0.0))])
 
 
-def test_breakdown_falls_back_to_gmresdr(lattices):
-    """Twisted mass at kappa = 0.1565, mu = 0.005 on the 8^4 configuration, where the
-    FP32 batched BiCGStab has broken down (NaN) on Z(4) sources: every right-hand side
-    must still reach the FP64 residual (through the GMRES-DR fallback where the
-    BiCGStab broke down) and agree with the oracle's FP64 solve."""
+def test_stall_forces_gmresdr_fallback(lattices):
+    """The fallback path, triggered on purpose: with a stall window of one iteration no
+    right-hand side can show the required 10x fall of its FP64 true residual, so the
+    batched BiCGStab stops every one of them after its first iteration (fallback = 3,
+    stagnation) and plain FP64 GMRES-DR(m, k) finishes it from the BiCGStab's solution.
+    Every answer must still reach the FP64 full-lattice residual and agree with the
+    oracle's FP64 solve (Q/quark.f90:458-842 with GMRES-DR, Q/inverters.f90:2871-3572)."""
+    import baylorlqcd_b200 as qq
+
+    lat, ol = lattices[0]
+    qq.initlagfib(0, 9)
+    be, bo = mixed_sources(qq, lat, 2, 2)
+    kappa = (0.1565, 0.005)
+    xe, xo, infos = lat.fermprop_batch(be, bo, kappa, m=16, k=6, precision=32, rhs_block=4, tol=1e-10,
+                                       solver=1, deflate=0, stall_window=1)
+    for i in range(be.shape[0]):
+        assert infos[i].status == 0, (i, infos[i])
+        assert infos[i].fallback == 3, (i, infos[i].fallback)
+        assert infos[i].true_rel <= 1e-10
+        xe_o, xo_o, st, _ = ol.fermprop(be[i], bo[i], kappa, inverter=5, resmax=1e-12, nGMRES=(16, 6))
+        assert st == 0
+        assert interior_rel(xe[i], xe_o, ol.nvhalf) < 1e-7, i
+        assert interior_rel(xo[i], xo_o, ol.nvhalf) < 1e-7, i
+
+
+def test_near_critical_default_rules(lattices):
+    """Twisted mass at kappa = 0.1565, mu = 0.005 on the 8^4 heatbath configuration,
+    where the FP32 batched BiCGStab has broken down (NaN) or stalled on Z(4) sources,
+    with the default stall window and iteration limit: whichever way each right-hand
+    side ends (converged, or any fallback reason), it must reach the FP64 residual and
+    agree with the oracle's FP64 solve, and nothing may run to an unbounded count."""
     import baylorlqcd_b200 as qq
 
     lat, ol = lattices[0]
@@ -105,7 +131,7 @@ def test_breakdown_falls_back_to_gmresdr(lattices):
     for i in range(2):
         assert infos[i].status == 0, (i, infos[i])
         assert infos[i].true_rel <= 1e-10
-        assert infos[i].fallback in (0, 1)
+        assert infos[i].fallback in (0, 1, 2, 3, 4)
         xe_o, xo_o, st, _ = ol.fermprop(be[i], bo[i], kappa, inverter=5, resmax=1e-12, nGMRES=(16, 6))
         assert st == 0
         assert interior_rel(xe[i], xe_o, ol.nvhalf) < 1e-7, i

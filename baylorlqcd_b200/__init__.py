@@ -35,6 +35,7 @@ EXPORTED = [
     "qq_bicgstab", "qq_fermprop", "qq_pointsource", "qq_fermprop_batch", "qq_initlagfib",
     "qq_rnds", "qq_z2source", "qq_z4source", "qq_twaverage_level0", "qq_discon_traces", "qq_bench_hsingle",
     "qq_heatbath", "qq_ctx_stream", "qq_launch_count", "qq_profile_hop", "qq_profile_hop_read",
+    "qq_profile_hop_select",
     "qq_gfwrite", "qq_gfread", "qq_fpwrite", "qq_fpread", "qq_hsingle_block",
     "qq_hop_tuned_shape", "qq_net_create", "qq_net_destroy", "qq_net_nweights", "qq_net_get_weights",
     "qq_net_set_weights", "qq_net_apply", "qq_net_grad", "qq_net_train", "qq_fgmres", "qq_pionrho", "qq_twvev", "qq_twaverage", "qq_twistdiscon", "qq_average", "qq_momfacs",
@@ -167,6 +168,7 @@ def load_library() -> C.CDLL:
         "qq_launch_count": ([], C.c_longlong),
         "qq_profile_hop": ([P, I], I),
         "qq_profile_hop_read": ([P, C.POINTER(C.c_longlong), DP, DP], I),
+        "qq_profile_hop_select": ([P, I, I, C.POINTER(C.c_longlong), DP, DP, DP], I),
         "qq_gfwrite": ([C.c_char_p, P, I, I, IP, D, DP, DP, I, I], I),
         "qq_gfread": ([C.c_char_p, P, I, I, IP, DP, DP, DP, IP, IP], I),
         "qq_fpwrite": ([C.c_char_p, P, P, I, I, D, D, D, I, I, I, I], I),
@@ -300,6 +302,14 @@ class Lattice:
         n, ms, by = C.c_longlong(), C.c_double(), C.c_double()
         _check(self.lib.qq_profile_hop_read(self._ctx, C.byref(n), C.byref(ms), C.byref(by)))
         return n.value, ms.value, by.value
+
+    def profile_hop_select(self, precision: int = 0, nrhs: int = 0):
+        """(launches, total ms, algorithmic bytes, flops) of the profiled hopping launches
+        of one spinor precision and RHS count (0: any)."""
+        n, ms, by, fl = C.c_longlong(), C.c_double(), C.c_double(), C.c_double()
+        _check(self.lib.qq_profile_hop_select(self._ctx, int(precision), int(nrhs), C.byref(n), C.byref(ms),
+                                              C.byref(by), C.byref(fl)))
+        return n.value, ms.value, by.value, fl.value
 
     def set_coact(self, c1, c2):
         _check(self.lib.qq_set_coact(self._ctx, (C.c_double * 4)(*c1), (C.c_double * 4)(*c2)))

@@ -664,3 +664,26 @@ extern "C" int qq_profile_hop_read(qq_ctx* c, long long* launches, double* ms_to
   if (bytes_total) *bytes_total = by;
   return QQ_OK;
 }
+
+extern "C" int qq_profile_hop_select(qq_ctx* c, int precision, int nrhs, long long* launches, double* ms_total,
+                                     double* bytes_total, double* flops_total) {
+  QQ_TRY(check_ctx(c));
+  QQ_CK(cudaStreamSynchronize(c->st));
+  long long n = 0;
+  double ms = 0.0, by = 0.0, fl = 0.0;
+  for (size_t i = 0; i < c->prof_used; ++i) {
+    const int p = c->prof_shape[i] / 1000, r = c->prof_shape[i] % 1000;
+    if ((precision && p != precision) || (nrhs && r != nrhs)) continue;
+    float t = 0.f;
+    QQ_CK(cudaEventElapsedTime(&t, c->prof_events[i].first, c->prof_events[i].second));
+    ++n;
+    ms += t;
+    by += c->prof_bytes[i];
+    fl += 1320.0 * (double)c->g.vh * r;  // spin-projected hop: 1320 flops per output site and RHS
+  }
+  if (launches) *launches = n;
+  if (ms_total) *ms_total = ms;
+  if (bytes_total) *bytes_total = by;
+  if (flops_total) *flops_total = fl;
+  return QQ_OK;
+}

@@ -132,9 +132,11 @@ static int launch_hop_profiled(qq_ctx* c, const HopArgs& a, int prec, int recon,
     QQ_CK(cudaEventCreate(&e1));
     c->prof_events.emplace_back(e0, e1);
     c->prof_bytes.push_back(0.0);
+    c->prof_shape.push_back(0);
   }
   auto& ev = c->prof_events[c->prof_used];
   c->prof_bytes[c->prof_used] = hop_bytes(c, prec, a.nrhs, epi);
+  c->prof_shape[c->prof_used] = (prec == P64 ? 64 : prec == P32 ? 32 : 16) * 1000 + a.nrhs;
   ++c->prof_used;
   QQ_CK(cudaEventRecord(ev.first, c->st));
   QQ_CK(launch_hop(a, prec, recon, epi, tps, c->st));

@@ -346,6 +346,11 @@ long long qq_launch_count(void);
  * last enable. */
 int qq_profile_hop(qq_ctx* ctx, int enable);
 int qq_profile_hop_read(qq_ctx* ctx, long long* launches, double* ms_total, double* bytes_total);
+/* The same over the profiled launches of one spinor precision (64, 32, 16; 0: any) and
+ * RHS count (0: any), with their algorithmic flops: 1320 per output site and
+ * right-hand side (the standard spin-projected count of Q/diracops.f90:554-599). */
+int qq_profile_hop_select(qq_ctx* ctx, int precision, int nrhs, long long* launches, double* ms_total,
+                          double* bytes_total, double* flops_total);
 
 /* Times `niter` launches of the hopping kernel alone (H_oe of random fields, output
  * parity gblclr = 2) with CUDA events on the library's stream.  precision: 64

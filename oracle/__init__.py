@@ -16,22 +16,39 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 LIB = HERE / "_build" / "liboracle.so"
+LIB_OMP = HERE / "_build" / "liboracle_omp.so"  # timing build (OpenMP site loops)
 
 _lib = None
+_use = LIB
 
 
 def build() -> Path:
-    srcs = list(HERE.glob("*.cpp")) + list(HERE.glob("*.h"))
-    if not LIB.exists() or LIB.stat().st_mtime < max(p.stat().st_mtime for p in srcs):
+    srcs = list(HERE.glob("*.cpp")) + list(HERE.glob("*.h")) + [HERE / "Makefile"]
+    newest = max(p.stat().st_mtime for p in srcs)
+    if any(not f.exists() or f.stat().st_mtime < newest for f in (LIB, LIB_OMP)):
         subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
     return LIB
+
+
+def use_timing_build(threads: int | None = None) -> int:
+    """Load the OpenMP timing build (CPU-baseline legs of bench.py only; the parity
+    tests use the serial build).  Must come before the first oracle call of the
+    process.  Returns the number of host threads it will use."""
+    global _use
+    if _lib is not None and _use != LIB_OMP:
+        raise RuntimeError("the serial oracle is already loaded in this process")
+    _use = LIB_OMP
+    L = lib()
+    if threads:
+        L.oq_set_threads(int(threads))
+    return int(L.oq_threads())
 
 
 def lib() -> C.CDLL:
     global _lib
     if _lib is None:
         build()
-        L = C.CDLL(str(LIB))
+        L = C.CDLL(str(_use))
         P, I, D = C.c_void_p, C.c_int, C.c_double
         IP, DP = C.POINTER(C.c_int), C.POINTER(C.c_double)
         sig = {
@@ -77,6 +94,8 @@ def lib() -> C.CDLL:
             "oq_twaverage_mom": ([P, DP, DP, DP, DP, DP, D, D, IP, I, I, I, DP], None),
             "oq_twvev_sites": ([P, DP, D, D, IP, I, I, I, IP, I, DP], None),
             "oq_set_kcyclim": ([I], None),
+            "oq_set_threads": ([I], None),
+            "oq_threads": ([], I),
             "oq_coldstart": ([P, DP], None),
             "oq_heatbath": ([P, DP, D, I, I, DP], None),
             "oq_aveplaq": ([P, DP], D),

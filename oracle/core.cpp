@@ -2,6 +2,9 @@
 // the Dirac operator family and vecdot, restated from the qqcd Fortran sources.
 // Parity unpinned against the Fortran (no compiler, no golden vectors): see oracle.h.
 #include "oracle_impl.h"
+#ifdef _OPENMP
+#include <omp.h>
+#endif
 
 #include <algorithm>
 #include <cmath>
@@ -353,6 +356,7 @@ namespace {
 
 // w(i) = y(i) * v(j(i)) ; j == nullptr means j(i) = i  (mv / mvg)
 inline void mvg(int n, const double* y, const double* v, double* w, const int* j) {
+  OQ_PAR_FOR
   for (int i = 0; i < n; ++i) {
     const double* Y = y + 18 * (size_t)i;
     const double* V = v + 6 * (size_t)(j ? j[i] - 1 : i);
@@ -368,6 +372,7 @@ inline void mvg(int n, const double* y, const double* v, double* w, const int* j
 
 // w(i) = y(i)^dagger * v(i)  (mdv)
 inline void mdv(int n, const double* y, const double* v, double* w) {
+  OQ_PAR_FOR
   for (int i = 0; i < n; ++i) {
     const double* Y = y + 18 * (size_t)i;
     const double* V = v + 6 * (size_t)i;
@@ -399,6 +404,7 @@ void accumulate(const oq_geom* g, double* h, const double* wx, int ldw, int mu, 
   const bool minus = sgn < 0;
   switch (mu) {
     case 1:
+      OQ_PAR_FOR
       for (int i = 0; i < nvhalf; ++i)
         for (int ir = 0; ir < 6; ++ir) {
           size_t k = 6 * (size_t)i + ir;
@@ -416,6 +422,7 @@ void accumulate(const oq_geom* g, double* h, const double* wx, int ldw, int mu, 
         }
       break;
     case 2:
+      OQ_PAR_FOR
       for (int i = 0; i < nvhalf; ++i)
         for (int ir = 0; ir < 6; ir += 2) {
           size_t k = 6 * (size_t)i + ir;
@@ -441,6 +448,7 @@ void accumulate(const oq_geom* g, double* h, const double* wx, int ldw, int mu, 
         }
       break;
     case 3:
+      OQ_PAR_FOR
       for (int i = 0; i < nvhalf; ++i)
         for (int ir = 0; ir < 6; ++ir) {
           size_t k = 6 * (size_t)i + ir;
@@ -458,6 +466,7 @@ void accumulate(const oq_geom* g, double* h, const double* wx, int ldw, int mu, 
         }
       break;
     case 4:
+      OQ_PAR_FOR
       for (int i = 0; i < nvhalf; ++i)
         for (int ir = 0; ir < 6; ++ir) {
           size_t k = 6 * (size_t)i + ir;
@@ -533,6 +542,7 @@ void mulfor(const oq_geom* g, double* h, const double* u, const double* gin, int
         if (g->lbd[jbl - 1][mu - 1]) {
           std::memcpy(w, wy.data(), sizeof(double) * 6 * nvhalf);
         } else {
+          OQ_PAR_FOR
           for (int j = 1; j <= nvhalf; ++j) {
             const int t = g->LVBC(j, mu, jeo);
             for (int a6 = 0; a6 < 6; ++a6)
@@ -729,8 +739,26 @@ extern "C" void oq_gamma5vector(const oq_geom* g, double* a, int ntmqcd) {
 }
 
 // vecdot Q/inverters.f90:13485-13530
+// Host threads of the timing build (liboracle_omp.so); the default build is serial and
+// ignores it.
+extern "C" void oq_set_threads(int n) {
+#ifdef _OPENMP
+  if (n > 0) omp_set_num_threads(n);
+#else
+  (void)n;
+#endif
+}
+extern "C" int oq_threads(void) {
+#ifdef _OPENMP
+  return omp_get_max_threads();
+#else
+  return 1;
+#endif
+}
+
 extern "C" void oq_vecdot(const oq_geom* g, const double* a, const double* b, double* adb) {
   double re = 0.0, im = 0.0;
+  OQ_PAR_SUM3
   for (int ibleo = 1; ibleo <= 8; ++ibleo)
     for (int ieo = 1; ieo <= 2; ++ieo)
       for (int id = 1; id <= 4; ++id)

@@ -38,6 +38,7 @@ struct CVec {  // (2, n) complex vector, 1-based
 // v_dst(icri..) = v_dst - beta*v_src over interior sites (complex axpy in the
 // reference's expression order, e.g. inverters.f90:3124-3131).
 void caxpy_minus(const oq_geom* g, double* dst, const double* src, const double* beta) {
+  OQ_PAR_FOR3
   for (int ibleo = 1; ibleo <= 8; ++ibleo)
     for (int ieo = 1; ieo <= 2; ++ieo)
       for (int id = 1; id <= 4; ++id)
@@ -55,6 +56,7 @@ void caxpy_minus(const oq_geom* g, double* dst, const double* src, const double*
 
 // acc += s*v over interior sites, expression order of inverters.f90:3226-3234.
 void caxpy_plus(const oq_geom* g, double* acc, const double* v, double sr, double si) {
+  OQ_PAR_FOR3
   for (int ibleo = 1; ibleo <= 8; ++ibleo)
     for (int ieo = 1; ieo <= 2; ++ieo)
       for (int id = 1; id <= 4; ++id)
@@ -72,6 +74,7 @@ void caxpy_plus(const oq_geom* g, double* acc, const double* v, double sr, doubl
 
 void scale_all(const oq_geom* g, double* v, double s) {
   const size_t n = g->vsize();
+  OQ_PAR_FOR
   for (size_t k = 0; k < n; ++k) v[k] = s * v[k];
 }
 void scale_interior(const oq_geom* g, double* v, double s) {

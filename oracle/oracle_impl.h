@@ -6,6 +6,22 @@
 
 #include "oracle.h"
 
+// The timing build of the oracle (liboracle_omp.so, -fopenmp) splits the site loops over
+// the host threads; the default build ignores these and runs in the reference's serial
+// order.  Only loops whose iterations touch disjoint entries (or reduce into OQ_SUM)
+// are split, so the arithmetic per entry is the reference's.
+#ifdef _OPENMP
+#define OQ_PAR_FOR _Pragma("omp parallel for schedule(static)")
+#define OQ_PAR_FOR2 _Pragma("omp parallel for collapse(2) schedule(static)")
+#define OQ_PAR_FOR3 _Pragma("omp parallel for collapse(3) schedule(static)")
+#define OQ_PAR_SUM3 _Pragma("omp parallel for collapse(3) schedule(static) reduction(+ : re, im)")
+#else
+#define OQ_PAR_FOR
+#define OQ_PAR_FOR2
+#define OQ_PAR_FOR3
+#define OQ_PAR_SUM3
+#endif
+
 struct oq_geom {
   int n[4];
   int bc[4];
@@ -48,6 +64,7 @@ struct oq_geom {
   // f(k) for every real entry with isite <= nvhalf.
   template <class F>
   void for_interior(F f) const {
+    OQ_PAR_FOR3
     for (int ibleo = 1; ibleo <= 8; ++ibleo)
       for (int ieo = 1; ieo <= 2; ++ieo)
         for (int id = 1; id <= 4; ++id)
@@ -58,6 +75,7 @@ struct oq_geom {
   // complex_stride: visit a = 1,3,5 only (f handles re and im).
   template <class F>
   void for_spin_range(F f, int smax, bool complex_stride) const {
+    OQ_PAR_FOR3
     for (int ibleo = 1; ibleo <= 8; ++ibleo)
       for (int ieo = 1; ieo <= 2; ++ieo)
         for (int s = 1; s <= smax; ++s)

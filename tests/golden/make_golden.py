@@ -18,6 +18,10 @@ fixed numbers to meet.  Inputs:
   C/cfgsprops.f90 sweep) on 8x8x8x8 at beta = 6.0 from a cold start with lagfib seed
   (0, 7): the plaquette after every sweep of 200 (a reproducible oracle number, not
   a literature value).
+* KAT-6 at configuration C1: the same heatbath on 8^4 from a cold start with lagfib seed
+  (0, 13), 200 sweeps, then fermprop with GMRES-DR(30,10) to 1e-10 at kappa = 0.150 on
+  the point source at site (1,1,1,1): cycle count, the gmresdr-norm history and the
+  harmonic Ritz values of the last restart.
 
 Usage: python tests/golden/make_golden.py   (rewrites golden.json)
 """
@@ -122,6 +126,24 @@ def main():
     plaq = hb.heatbath(u, 6.0, 200)
     out["kat5_heatbath"] = {"dims": [8, 8, 8, 8], "beta": 6.0, "iseed": 7, "start": "cold",
                             "plaquette": [float(v) for v in plaq]}
+    # KAT-6 at configuration C1: the same heatbath with lagfib seed (0, 13), then the
+    # reference's fermprop (Q/quark.f90:458-842) with GMRES-DR(30,10) to 1e-10 at
+    # kappa = 0.150 on the point source at site (1,1,1,1), colour 1, spin 1
+    c1 = oracle.OracleLattice(8, 8, 8, 8, bc=BC)
+    u = c1.coldstart()
+    oracle.initlagfib(0, 13)
+    plaq = c1.heatbath(u, 6.0, 200)
+    c1.set_gauge(u)
+    be, bo = c1.pointsource((1, 1, 1, 1), 1, 1)
+    xe, xo, st, log = c1.fermprop(be, bo, (0.150, 0.0), inverter=5, resmax=1e-10, nGMRES=(30, 10))
+    hist, hmvp = log.history()
+    out["kat6_c1"] = {"dims": [8, 8, 8, 8], "beta": 6.0, "iseed": 13, "sweeps": 200, "start": "cold",
+                      "plaquette": float(plaq[-1]), "kappa": [0.150, 0.0], "nGMRES": [30, 10], "resmax": 1e-10,
+                      "src": "point 1,1,1,1 c1 s1", "status": int(st), "itercount": int(log.itercount),
+                      "ncycles": int(log.ncycles), "mvp": int(log.mvp), "hist": [float(h) for h in hist],
+                      "hist_mvp": [int(m) for m in hmvp],
+                      "ritz": [[float(r.real), float(r.imag)] for r in log.ritz_values()],
+                      "xe_norm2": float(c1.vecdot(xe, xe).real), "xo_norm2": float(c1.vecdot(xo, xo).real)}
     (HERE / "golden.json").write_text(json.dumps(out, indent=1) + "\n")
     print("wrote", HERE / "golden.json")
 

@@ -127,3 +127,28 @@ def test_discon_psc3(ol):
     J = Jsum / (rec["nnoise"] * DIMS[0] * DIMS[1] * DIMS[2])
     want = np.array(rec["J"])
     assert np.abs(J - want).max() <= RTOL * np.abs(want).max()
+
+
+def test_kat6_c1_reproduces_record():
+    """KAT-6 at configuration C1: the oracle's heatbath (8^4, beta = 6.0, cold start,
+    lagfib seed (0, 13), 200 sweeps) and its fermprop with GMRES-DR(30,10) to 1e-10 at
+    kappa = 0.150 reproduce the committed record: plaquette, cycles, the gmresdr-norm
+    history, the harmonic Ritz values and the solution norms."""
+    rec = GOLDEN["kat6_c1"]
+    c1 = oracle.OracleLattice(*rec["dims"], bc=BC)
+    u = c1.coldstart()
+    oracle.initlagfib(0, rec["iseed"])
+    plaq = c1.heatbath(u, rec["beta"], rec["sweeps"])
+    assert plaq[-1] == rec["plaquette"]
+    c1.set_gauge(u)
+    be, bo = c1.pointsource((1, 1, 1, 1), 1, 1)
+    xe, xo, st, log = c1.fermprop(be, bo, tuple(rec["kappa"]), inverter=5, resmax=rec["resmax"],
+                                  nGMRES=tuple(rec["nGMRES"]))
+    assert st == rec["status"] == 0
+    assert log.itercount == rec["itercount"] and log.ncycles == rec["ncycles"]
+    hist, _ = log.history()
+    np.testing.assert_allclose(hist, rec["hist"], rtol=RTOL, atol=1e-22)
+    r = np.array(rec["ritz"]).reshape(-1, 2)
+    np.testing.assert_allclose(log.ritz_values(), r[:, 0] + 1j * r[:, 1], rtol=RTOL)
+    np.testing.assert_allclose(c1.vecdot(xe, xe).real, rec["xe_norm2"], rtol=RTOL)
+    np.testing.assert_allclose(c1.vecdot(xo, xo).real, rec["xo_norm2"], rtol=RTOL)

@@ -1,0 +1,168 @@
+"""Parity at the benchmark configurations, not only on toy lattices.
+
+C1 (KAT-6): 8^4 heatbath configuration from the oracle's restatement of the reference's
+pseudo-heatbath (lagfib seed (0, 13), cold start, 200 sweeps at beta = 6.0), uploaded to
+the GPU; the GPU fermprop with GMRES-DR(30,10) to 1e-10 at kappa = 0.150
+(Q/quark.f90:458-842, Q/inverters.f90:2871-3572) against the committed record: cycle
+count within one, the per-cycle gmresdr-norm history within 10%, the ten harmonic Ritz
+values of the last restart to 1e-6, and the solution to 1e-7 of the oracle's.
+
+C2 (error against the FP64 solve, per precision): on a heatbath configuration near
+critical kappa, the batched FP32 and FP16 solves are compared with the solution of the
+reference's plain FP64 GMRES-DR: ||x_P - x_64|| / ||x_64|| must stay within 1e-7 at
+C1's kappa and 1e-6 at C2's near-critical kappa (every solve stops at an FP64 true
+residual of 1e-10; the operator's condition number sets how much solution error that
+residual allows).
+
+C3 (the deflated disconnected-loop solver sequence): GMRES-DR(m, 30) on the first Z(4)
+noise, then GMRES-Proj deflated by its 30 eigenvectors (psc with isignal = 2 at the
+reference's fixed 1e-8) for the next noises, GPU against the oracle on the C3 operator
+(twisted mass kappa = 0.1566, mu = 0.005) on a lattice the oracle finishes in seconds.
+"""
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = json.loads((Path(__file__).resolve().parent / "golden" / "golden.json").read_text())
+BC = (1, 1, 1, -1)
+
+
+def vdot(a, b, nv):
+    ca = a[..., :nv, 0::2] + 1j * a[..., :nv, 1::2]
+    cb = b[..., :nv, 0::2] + 1j * b[..., :nv, 1::2]
+    return np.vdot(ca.ravel(), cb.ravel())
+
+
+def rel(a, b, nv):
+    return np.linalg.norm((a - b)[..., :nv, :]) / np.linalg.norm(b[..., :nv, :])
+
+
+@pytest.fixture(scope="module")
+def c1():
+    """The C1 configuration, made by the oracle's heatbath on the host."""
+    import baylorlqcd_b200 as qq
+
+    rec = GOLDEN["kat6_c1"]
+    ol = oracle.OracleLattice(*rec["dims"], bc=BC)
+    u = ol.coldstart()
+    oracle.initlagfib(0, rec["iseed"])
+    plaq = ol.heatbath(u, rec["beta"], rec["sweeps"])
+    assert plaq[-1] == rec["plaquette"]
+    ol.set_gauge(u)
+    lat = qq.Lattice(*rec["dims"], bc=BC)
+    lat.gauge_upload(u)
+    yield rec, lat, ol
+    lat.close()
+
+
+def test_kat6_c1_gmresdr(c1):
+    rec, lat, ol = c1
+    be, bo = lat.pointsource((1, 1, 1, 1), 1, 1)
+    xe, xo, info = lat.fermprop(be, bo, tuple(rec["kappa"]), inverter=5, resmax=rec["resmax"],
+                                nGMRES=tuple(rec["nGMRES"]))
+    assert info.status == 0
+    assert abs(info.ncycles - rec["ncycles"]) <= 1
+    n = min(len(info.hist), len(rec["hist"])) - 1
+    np.testing.assert_allclose(info.hist[:n], rec["hist"][:n], rtol=0.1)
+    k = rec["nGMRES"][1]
+    r = np.array(rec["ritz"]).reshape(-1, 2)
+    want = np.sort_complex((r[:, 0] + 1j * r[:, 1])[np.argsort(np.hypot(r[:, 0], r[:, 1]))[:k]])
+    got = np.sort_complex(info.ritz[np.argsort(np.abs(info.ritz))[:k]])
+    np.testing.assert_allclose(got, want, rtol=1e-6)
+    nv = lat.nvhalf
+    np.testing.assert_allclose(vdot(xe, xe, nv).real, rec["xe_norm2"], rtol=1e-7)
+    np.testing.assert_allclose(vdot(xo, xo, nv).real, rec["xo_norm2"], rtol=1e-7)
+    xe_o, xo_o, st, _ = ol.fermprop(be, bo, tuple(rec["kappa"]), inverter=5, resmax=1e-12,
+                                    nGMRES=tuple(rec["nGMRES"]))
+    assert st == 0
+    assert rel(xe, xe_o, nv) < 1e-7 and rel(xo, xo_o, nv) < 1e-7
+
+
+def test_kat6_c1_batched_methods(c1):
+    """The accelerated methods on the C1 system reach the FP64 residual and the FP64
+    solution (FP32 and FP16 inner solves, graph-driven batched BiCGStab)."""
+    rec, lat, ol = c1
+    srcs = [lat.pointsource((1, 1, 1, 1), c, s) for c, s in ((1, 1), (2, 2), (3, 3), (1, 4))]
+    be = np.stack([e for e, _ in srcs])
+    bo = np.stack([o for _, o in srcs])
+    xe64, xo64, i64 = lat.fermprop_batch(be, bo, tuple(rec["kappa"]), m=30, k=10, precision=64, rhs_block=1,
+                                         tol=1e-11, solver=0)
+    assert all(i.status == 0 for i in i64)
+    nv = lat.nvhalf
+    for prec in (32, 16):
+        xe, xo, infos = lat.fermprop_batch(be, bo, tuple(rec["kappa"]), m=30, k=10, precision=prec, rhs_block=4,
+                                           tol=1e-10, solver=1, deflate=0)
+        for i in range(4):
+            assert infos[i].status == 0 and infos[i].true_rel <= 1e-10, (prec, i)
+            assert rel(xe[i], xe64[i], nv) < 1e-7, (prec, i)
+            assert rel(xo[i], xo64[i], nv) < 1e-7, (prec, i)
+
+
+def test_c2_error_against_fp64_per_precision():
+    """Configuration C2's report, at a size the suite runs in seconds: 8^3x16 heatbath
+    configuration (beta = 6.0), Wilson kappa = 0.1565 near critical, 12 spin-colour point
+    sources; the FP64 solution of plain GMRES-DR(60,20) is the reference solve, and the
+    batched FP32 and FP16 inner solves must agree with it."""
+    import baylorlqcd_b200 as qq
+
+    dims, kappa = (8, 8, 8, 16), (0.1565, 0.0)
+    lat = qq.Lattice(*dims, bc=BC)
+    lat.heatbath(6.0, 100, seed=13)
+    be = np.zeros((12,) + lat.half_shape)
+    bo = np.zeros((12,) + lat.half_shape)
+    for i in range(12):
+        be[i], bo[i] = lat.pointsource((1, 1, 1, 1), i % 3 + 1, i // 3 + 1)
+    xe64, xo64, i64 = lat.fermprop_batch(be, bo, kappa, m=60, k=20, precision=64, rhs_block=1, tol=1e-11,
+                                         solver=0)
+    assert all(i.status == 0 for i in i64)
+    nv = lat.nvhalf
+    errs = {}
+    for prec in (32, 16):
+        xe, xo, infos = lat.fermprop_batch(be, bo, kappa, m=60, k=20, precision=prec, rhs_block=12, tol=1e-10,
+                                           solver=1, deflate=0)
+        assert all(i.status == 0 and i.true_rel <= 1e-10 for i in infos), prec
+        errs[prec] = max(max(rel(xe[i], xe64[i], nv), rel(xo[i], xo64[i], nv)) for i in range(12))
+        assert errs[prec] < 1e-6, (prec, errs[prec])
+    lat.close()
+
+
+def test_c3_gmresdr_then_gmresproj_against_oracle():
+    """C3's solver sequence on the C3 operator: psc (Q/inverters.f90:4310-4465) with
+    GMRES-DR(40,30) on the first Z(4) noise and GMRES-Proj(10,30) deflated by its 30
+    vectors on the next three, GPU against the oracle on a 4^3x8 heatbath configuration:
+    cycle counts within one and solutions to 1e-7 (GMRES-DR) and 1e-5 (GMRES-Proj, which
+    stops at 1e-8)."""
+    import baylorlqcd_b200 as qq
+
+    dims, kappa = (4, 4, 4, 8), (0.1566, 0.005)
+    lat = qq.Lattice(*dims, bc=BC)
+    u, _ = lat.heatbath(6.0, 100, seed=3)
+    ol = oracle.OracleLattice(*dims, bc=BC)
+    ol.set_gauge(u)
+    qq.initlagfib(0, 21)
+    noises = [lat.z4source() for _ in range(4)]
+    oracle.initlagfib(0, 21)
+    onoises = [ol.z4source() for _ in range(4)]
+    for (a, b), (c, d) in zip(noises, onoises):
+        assert np.array_equal(a, c) and np.array_equal(b, d)
+    dg = lat.deflation(40, 30)
+    do = ol.deflation(40, 30)
+    nv = lat.nvhalf
+    for i, (ze, zo) in enumerate(noises):
+        isig = 1 if i == 0 else 2
+        xe, xo, info = lat.fermprop(ze, zo, kappa, inverter=6, resmax=1e-10, nGMRES=(40, 30), isignal=isig,
+                                    defl=dg)
+        xe_o, xo_o, st, log = ol.fermprop(ze, zo, kappa, inverter=6, resmax=1e-10, nGMRES=(40, 30), isignal=isig,
+                                          defl=do)
+        assert info.status == 0 and st == 0, i
+        assert abs(info.ncycles - log.ncycles) <= 1, (i, info.ncycles, log.ncycles)
+        tol = 1e-7 if i == 0 else 1e-5
+        assert rel(xe, xe_o, nv) < tol and rel(xo, xo_o, nv) < tol, i
+    dg.close()
+    lat.close()

@@ -14,6 +14,13 @@ C1's kappa and 1e-6 at C2's near-critical kappa (every solve stops at an FP64 tr
 residual of 1e-10; the operator's condition number sets how much solution error that
 residual allows).
 
+C5 (the benchmark configuration, 24^3x48 twisted mass kappa = 0.1566, mu = 0.0025): the
+GPU's plain FP64 GMRES-DR(60,20) on the GPU heatbath configuration (seed 13, 500 sweeps,
+the same on every B200) against the oracle's complete solve of the same system, recorded
+by tests/golden/make_c5_record.py: the same cycle count within one and the per-cycle
+residual history within 1e-4 relative over the first 50 cycles (10% after, where the
+two summation orders part).
+
 C3 (the deflated disconnected-loop solver sequence): GMRES-DR(m, 30) on the first Z(4)
 noise, then GMRES-Proj deflated by its 30 eigenvectors (psc with isignal = 2 at the
 reference's fixed 1e-8) for the next noises, GPU against the oracle on the C3 operator
@@ -165,4 +172,24 @@ def test_c3_gmresdr_then_gmresproj_against_oracle():
         tol = 1e-7 if i == 0 else 1e-5
         assert rel(xe, xe_o, nv) < tol and rel(xo, xo_o, nv) < tol, i
     dg.close()
+    lat.close()
+
+
+def test_c5_gmresdr_matches_oracle_record():
+    import baylorlqcd_b200 as qq
+
+    rec = json.loads((Path(__file__).resolve().parent / "golden" / "c5_gmresdr_record.json").read_text())
+    lat = qq.Lattice(*rec["dims"], bc=BC)
+    _, plaq = lat.heatbath(rec["beta"], rec["sweeps"], seed=rec["seed"])
+    assert abs(plaq - rec["plaquette"]) < 1e-12
+    be, bo = lat.pointsource((1, 1, 1, 1), 1, 1)
+    xe, xo, info = lat.fermprop(be, bo, tuple(rec["kappa"]), inverter=5, resmax=rec["resmax"],
+                                nGMRES=tuple(rec["nGMRES"]))
+    o = rec["oracle"]
+    assert info.status == 0 and o["status"] == 0
+    assert abs(info.ncycles - o["cycles"]) <= 1
+    assert abs(info.itercount - o["iterations"]) <= rec["nGMRES"][0]
+    n = min(len(info.hist), len(o["hist"]))
+    np.testing.assert_allclose(info.hist[:min(n, 50)], o["hist"][:min(n, 50)], rtol=1e-4)
+    np.testing.assert_allclose(info.hist[:n - 1], o["hist"][:n - 1], rtol=0.1)
     lat.close()

@@ -88,7 +88,7 @@ int qq_ctx_create(const qq_geom* geom, int device, qq_ctx** out) {
   auto* c = new qq_ctx();
   c->device = device;
   if (const char* f = std::getenv("QQ_FORCE_TPS")) c->forced_tps = std::atoi(f);  // testing
-  if (c->forced_tps < 0 || c->forced_tps > kShapeF2 + 8) c->forced_tps = 0;
+  if (c->forced_tps < 0 || c->forced_tps > kShapeMax) c->forced_tps = 0;
   for (int mu = 0; mu < 4; ++mu) {
     c->g.n[mu] = n[mu];
     c->g.bc[mu] = geom->bc[mu];
@@ -509,7 +509,7 @@ extern "C" int qq_hsingle_block(qq_ctx* c, int precision, int nrhs, int shape, d
   const int prec = precision == 32 ? P32 : precision == 16 ? P16 : -1;
   if (prec < 0) return set_error(QQ_BAD_ARG, "precision must be 32 or 16");
   if (nrhs < 1 || nrhs > kMaxBatch) return set_error(QQ_BAD_ARG, "nrhs must be 1..32");
-  if (shape < 0 || shape > kShapeF2 + 8) return set_error(QQ_BAD_ARG, "bad kernel shape");
+  if (shape < 0 || shape > kShapeMax) return set_error(QQ_BAD_ARG, "bad kernel shape");
   if (gblclr != 1 && gblclr != 2) return set_error(QQ_BAD_ARG, "gblclr must be 1 or 2");
   if (idag != 0 && idag != 1) return set_error(QQ_BAD_ARG, "idag must be 0 or 1");
   if (!gout || !gin) return set_error(QQ_BAD_ARG, "null array");
@@ -541,7 +541,7 @@ extern "C" int qq_bench_hsingle(qq_ctx* c, int precision, int nrhs, int tps, int
   QQ_TRY(set_device(c));
   if (!c->have_gauge) return set_error(QQ_BAD_ARG, "no gauge field uploaded");
   const int prec = precision == 64 ? P64 : precision == 32 ? P32 : precision == 16 ? P16 : -1;
-  if (prec < 0 || nrhs < 1 || nrhs > kMaxBatch || niter < 1 || tps < 0 || tps > kShapeF2 + 8)
+  if (prec < 0 || nrhs < 1 || nrhs > kMaxBatch || niter < 1 || tps < 0 || tps > kShapeMax)
     return set_error(QQ_BAD_ARG, "bad benchmark arguments");
   const int vh = c->g.vh;
   // nrhs > 1: one RHS-interleaved block field of nrhs right-hand sides (the layout of

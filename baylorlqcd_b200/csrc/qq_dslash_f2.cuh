@@ -458,6 +458,10 @@ struct F2aShared {
   float4* ring;   // [stage][rhs][6][thread]
 };
 
+// The fused dot product's operand is the EPI_DBLE operand itself (the <t, s> step of
+// BiCGStab): stage 8 serves both, and stage 9 is not loaded.
+__device__ inline bool f2a_dot_is_aux(const HopArgs& a) { return a.blk && a.dot_op == a.aux[0]; }
+
 // Stage H (hops 0-7, 8 = the EPI_DBLE operand, 9 = the fused dot product's operand)
 // into ring slot H % D; always one group.  Thread j of a site holds right-hand sides
 // j, j + G, ..., j + (RPT - 1) G.
@@ -465,7 +469,7 @@ template <int H, int D, int EPI, int RPT>
 __device__ inline void f2a_issue(const HopArgs& a, const F2aShared& sh, int s, int sl, int j, int G, int T,
                                  int tx, bool act) {
   if constexpr (H < 8 || (H >= 8 && H <= 9 && EPI == EPI_DBLE)) {
-    if (act && (H != 9 || a.dot_mode)) {
+    if (act && (H != 9 || (a.dot_mode && !f2a_dot_is_aux(a)))) {
       const int site = H < 8 ? sh.nbr[sl * 8 + H] : s;
       const int n = a.vh_of();
 #pragma unroll
@@ -539,8 +543,10 @@ __device__ inline void f2a_run(const HopArgs& a, const F2aShared& sh, int s, int
 }
 
 // Thread layout: threadIdx.x = (site-in-block) * G + j, G = nrhs / RPT threads per site.
-template <int EPI, int D, int RPT>
-__global__ void __launch_bounds__(128) hop_f2a_kernel(HopArgs a) {
+// MINB: resident blocks per SM the register allocation is capped for (4: none; 5 and 6
+// trade a few spilled registers for 25-50% more resident warps).
+template <int EPI, int D, int RPT, int MINB>
+__global__ void __launch_bounds__(128, MINB) hop_f2a_kernel(HopArgs a) {
   extern __shared__ float4 f2a_smem[];
   const int T = blockDim.x, per = a.per_block, tx = threadIdx.x;
   const int G = a.nrhs / RPT;
@@ -639,7 +645,7 @@ __global__ void __launch_bounds__(128) hop_f2a_kernel(HopArgs a) {
       const Pair12 o = finish2_g<EPI>(a, s, j + k * G, acc[k], g);
       if (a.dot_mode) {
         Pair12 w;
-        const float4* wsrc = sh.ring + ((9 % D) * RPT + k) * 6 * T + tx;
+        const float4* wsrc = sh.ring + (((f2a_dot_is_aux(a) ? 8 : 9) % D) * RPT + k) * 6 * T + tx;
 #pragma unroll
         for (int q = 0; q < 6; ++q) {
           const float4 t = wsrc[q * T];
@@ -663,7 +669,10 @@ __global__ void __launch_bounds__(128) hop_f2a_kernel(HopArgs a) {
     }
   }
   if (a.dot_mode) {  // per right-hand side over the block's sites, fixed order
-    __shared__ double dred[3][128];
+    // the partial sums reuse the start of the ring (3 KB, smaller than one stage), once
+    // every thread is done reading its own ring slots
+    double(*dred)[128] = reinterpret_cast<double(*)[128]>(sh.ring);
+    __syncthreads();
 #pragma unroll
     for (int q = 0; q < 3; ++q) dred[q][tx] = dsum[q];
     __syncthreads();

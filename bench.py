@@ -23,6 +23,16 @@ GMRES-DR(30,10)) complete solves on one core and on all cores.
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 Multi-GPU: one process per GPU (torchrun); every rank solves its own configuration
 (replicas, weak scaling).
+
+Other measurements (one JSON line each, single GPU), the commands behind the design
+notes' figures and the ncu captures under profiles/:
+  --mode dslash   the hopping kernel alone (qq_bench_hsingle): --dims, --precision,
+                  --nrhs, --shape (0: autotuned), --iters; L2 flushed between launches
+  --mode c3       disconnected loops (twistdiscon): --nnoise Z(4) noises, --solver
+                  (1 batched, 2 the reference's psc sequence), subtraction level --nsub
+  --mode c4       the uneven batch: 48 Wilson solves over 8^3x16 .. 20^3x40
+  --mode shift    multi-shift GMRES-DR against each shift alone
+  --mode twvev    perturbative VEVs of the loop operators
 """
 from __future__ import annotations
 
@@ -91,6 +101,12 @@ def parse(argv=None):
     p.add_argument("--e2e-steps", type=int, default=0, help="end-to-end steps (0: min(steps, 5))")
     p.add_argument("--cpu-threads", type=int, default=0, help="host threads of the CPU legs (0: all)")
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--mode", default="solve", choices=["solve", "dslash", "c3", "c4", "shift", "twvev"])
+    p.add_argument("--shape", type=int, default=0, help="--mode dslash: kernel shape (0: autotuned)")
+    p.add_argument("--iters", type=int, default=20, help="--mode dslash: timed launches")
+    p.add_argument("--nnoise", type=int, default=24, help="--mode c3: noises")
+    p.add_argument("--solver", type=int, default=1, help="--mode c3: 1 batched, 2 psc")
+    p.add_argument("--nsub", type=int, default=6, help="--mode c3 / twvev: subtraction level")
     return p.parse_args(argv)
 
 
@@ -150,12 +166,12 @@ def shape_name(shape: int) -> str:
         return "hop_mrhs_kernel"
     return {301: "hop_f2_kernel", 302: "hop_f2_kernel", 303: "hop_f2_kernel", 304: "hop_f2p_kernel",
             305: "hop_f2s_kernel", 306: "hop_f2a_kernel", 307: "hop_f2a_kernel",
-            308: "hop_f2a_kernel"}.get(shape, "hop kernel")
+            308: "hop_f2a_kernel", 309: "hop_f2a_kernel", 310: "hop_f2a_kernel"}.get(shape, "hop kernel")
 
 
 # DRAM bytes (read + write) of one EPI_STORE launch from an ncu capture, keyed by
 # (kernel, precision, RHS, lattice); the capture's summary is the source.  The ring
-# depths of hop_f2a_kernel (shapes 306-308) move the same bytes.
+# depths and register caps of hop_f2a_kernel (shapes 306-310) move the same bytes.
 NCU_TRAFFIC = {
     ("hop_f2a_kernel", 32, 12, (16, 16, 16, 32)): (150.6e6, "profiles/hop_f2a_kernel_fp32_blk12_16x16x16x32.md"),
 }
@@ -490,8 +506,139 @@ def run_reference(a, rank, world, local):
     }
 
 
+# ---------------------------------------------------------------------------
+# Other measurements (--mode)
+def run_dslash(a):
+    """The hopping kernel alone on random fields of a heatbath configuration."""
+    import baylorlqcd_b200 as qq
+
+    dims = tuple(int(x) for x in a.dims.split(","))
+    lat = qq.Lattice(*dims, bc=(1, 1, 1, -1))
+    lat.heatbath(6.0, 20, seed=13)
+    ms, by = lat.bench_hsingle(a.precision, a.nrhs, a.iters, True, a.shape)
+    shape = a.shape
+    if not shape:
+        try:
+            shape = lat.hop_tuned_shape(a.precision, a.nrhs)
+        except qq.QQError:
+            shape = 0
+    hbm, kind = peaks()
+    flops = 1320.0 * lat.nvhalf * 16 * a.nrhs
+    lat.close()
+    return {"mode": "dslash", "kernel": "%s (shape %d)" % (shape_name(shape), shape), "lattice": list(dims),
+            "precision": a.precision, "nrhs": a.nrhs, "us_per_launch": ms * 1e3, "bytes_per_launch": by,
+            "gbs": by / ms / 1e6, "frac": by / ms / 1e6 / hbm, "peak": hbm, "peak_kind": kind,
+            "gflops": flops / ms / 1e6, "l2": "512 MiB written between launches"}
+
+
+def heatbath_lattice(qq, dims, sweeps, seed):
+    lat = qq.Lattice(*dims, bc=(1, 1, 1, -1))
+    _, plaq = lat.heatbath(6.0, sweeps, seed=seed)
+    return lat, plaq
+
+
+def run_c3(a):
+    """twistdiscon with nnoise Z(4) noises (noise drawing, solves, traces and twvev), wall
+    time per noise after one warm-up call."""
+    import baylorlqcd_b200 as qq
+
+    dims = tuple(int(x) for x in a.dims.split(","))
+    lat, plaq = heatbath_lattice(qq, dims, a.sweeps, 3)
+    kw = dict(nsub=a.nsub, nmom=5, nop=6, delta=0.0, dobndry=0, solver=a.solver, m=a.m, k=a.k,
+              precision=a.precision, rhs_block=a.rhs_block, tol=a.tol)
+    kappa = (a.kappa, a.mu)
+    qq.initlagfib(0, 5)
+    lat.twistdiscon(4, min(a.nnoise, a.rhs_block), kappa, **kw)
+    qq.initlagfib(0, 5)
+    t0 = time.perf_counter()
+    _, infos = lat.twistdiscon(4, a.nnoise, kappa, **kw)
+    dt = time.perf_counter() - t0
+    lat.close()
+    return {"mode": "c3", "lattice": list(dims), "kappa": a.kappa, "mu": a.mu, "nnoise": a.nnoise,
+            "solver": a.solver, "nsub": a.nsub, "plaquette": plaq, "seconds": dt, "sec_per_noise": dt / a.nnoise,
+            "max_true_rel": max(i.true_rel for i in infos), "fallback": sum(1 for i in infos if i.fallback)}
+
+
+def run_c4(a):
+    """The uneven batch: 48 Wilson solves over four heatbath configurations, three kappa
+    values each, two point and two Z(4) sources per (configuration, kappa); one tuning
+    call, then the lattices side by side and one after the other."""
+    import baylorlqcd_b200 as qq
+
+    lats, groups = [], []
+    qq.initlagfib(0, 11)
+    for n, dims in enumerate(((8, 8, 8, 16), (12, 12, 12, 24), (16, 16, 16, 32), (20, 20, 20, 40))):
+        lat, _ = heatbath_lattice(qq, dims, a.sweeps, 31 + n)
+        lats.append(lat)
+        for kappa in (0.150, 0.155, 0.1565):
+            be = np.zeros((4,) + lat.half_shape)
+            bo = np.zeros((4,) + lat.half_shape)
+            for i in range(2):
+                be[i], bo[i] = lat.pointsource((1 + i, 1, 1, 1), i + 1, 2 * i + 1)
+            for i in range(2, 4):
+                be[i], bo[i] = lat.z4source()
+            groups.append((lat, be, bo, (kappa, 0.0)))
+    nrhs = sum(g[1].shape[0] for g in groups)
+    kw = dict(precision=a.precision, rhs_block=4, tol=a.tol, deflate=0)
+    qq.fermprop_uneven(groups, concurrent=False, **kw)  # tuning
+    out = {"mode": "c4", "solves": nrhs, "lattices": len(lats)}
+    for conc in (True, False):
+        res, secs = qq.fermprop_uneven(groups, concurrent=conc, **kw)
+        infos = [i for _, _, inf in res for i in inf]
+        out["concurrent" if conc else "sequential"] = {
+            "seconds": secs, "sec_per_rhs": secs / nrhs, "max_true_rel": max(i.true_rel for i in infos),
+            "not_converged": sum(i.status != 0 for i in infos), "fallback": sum(1 for i in infos if i.fallback)}
+    for lat in lats:
+        lat.close()
+    return out
+
+
+def run_shift(a):
+    """Multi-shift GMRES-DR of a unit-norm Z(4) noise for five shifts (in units of
+    1/kappa^2) against each shift solved alone (the library's own solve timer)."""
+    import baylorlqcd_b200 as qq
+
+    dims = tuple(int(x) for x in a.dims.split(","))
+    lat, _ = heatbath_lattice(qq, dims, a.sweeps, 3)
+    kappa = (a.kappa, a.mu)
+    sig = np.array([0.0, -0.099, -0.199, -0.3, -0.5]) / a.kappa**2
+    qq.initlagfib(0, 5)
+    be, _ = lat.z4source()
+    be /= np.sqrt(lat.vecdot(be, be).real)
+    lat.gmresdrshift(be, sig[:2], (8, 2), 1e-3, kappa=kappa)  # tuning
+    _, resid, info = lat.gmresdrshift(be, sig, (a.m, a.k), a.tol, kappa=kappa)
+    alone = [lat.gmresdrshift(be, sig[i:i + 1], (a.m, a.k), a.tol, kappa=kappa) for i in range(len(sig))]
+    lat.close()
+    return {"mode": "shift", "lattice": list(dims), "kappa": kappa, "GMRES": [a.m, a.k], "shifts": len(sig),
+            "multishift": {"seconds": info.seconds, "mvp": info.mvp, "cycles": info.ncycles,
+                           "max_resid": float(resid.max())},
+            "alone": {"seconds": sum(r[2].seconds for r in alone), "mvp": sum(r[2].mvp for r in alone),
+                      "max_resid": float(max(r[1][0] for r in alone))}}
+
+
+def run_twvev(a):
+    """twvev on a short heatbath configuration: one untimed call, then three timed calls
+    (wall clock around the entry point, host program build included)."""
+    import baylorlqcd_b200 as qq
+
+    dims = tuple(int(x) for x in a.dims.split(","))
+    lat, _ = heatbath_lattice(qq, dims, 5, 3)
+    lat.twvev(0.156, delta=0.2, nsub=a.nsub)
+    ts = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        lat.twvev(0.156, delta=0.2, nsub=a.nsub)
+        ts.append(time.perf_counter() - t0)
+    lat.close()
+    return {"mode": "twvev", "lattice": list(dims), "nsub": a.nsub, "seconds": ts}
+
+
 def main(argv=None):
     a = parse(argv)
+    if a.mode != "solve":
+        fn = {"dslash": run_dslash, "c3": run_c3, "c4": run_c4, "shift": run_shift, "twvev": run_twvev}[a.mode]
+        print(json.dumps(fn(a)), flush=True)
+        return 0
     rank, world, local = dist_env()
     if a.impl == "reference":
         # the reference's CPU path runs once, on rank 0; other ranks have no work

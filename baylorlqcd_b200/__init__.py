@@ -31,7 +31,7 @@ EXPORTED = [
     "qq_ctx_create", "qq_ctx_destroy", "qq_ctx_dims", "qq_last_error", "qq_set_coact",
     "qq_gauge_upload", "qq_hsingle", "qq_hdouble", "qq_hdbletm", "qq_twmshift", "qq_gamma5mult", "qq_vecdot",
     "qq_vecdot_noalloc",
-    "qq_defl_create", "qq_defl_destroy", "qq_defl_size", "qq_gmresdr", "qq_gmresproj", "qq_gmresdrshift", "qq_psc",
+    "qq_defl_create", "qq_defl_destroy", "qq_defl_size", "qq_defl_vector", "qq_net_train_pairs", "qq_gmresdr", "qq_gmresproj", "qq_gmresdrshift", "qq_psc",
     "qq_bicgstab", "qq_fermprop", "qq_pointsource", "qq_fermprop_batch", "qq_initlagfib",
     "qq_rnds", "qq_z2source", "qq_z4source", "qq_twaverage_level0", "qq_discon_traces", "qq_bench_hsingle",
     "qq_heatbath", "qq_ctx_stream", "qq_launch_count", "qq_profile_hop", "qq_profile_hop_read",
@@ -129,6 +129,8 @@ def load_library() -> C.CDLL:
         "qq_defl_create": ([P, I, I, C.POINTER(P)], I),
         "qq_defl_destroy": ([P], I),
         "qq_defl_size": ([P], I),
+        "qq_defl_vector": ([P, I, P], I),
+        "qq_net_train_pairs": ([P, P, I, P, P, I, D, DP], I),
         "qq_gmresdr": ([P, P, P, IP, D, I, DP, I, P, C.POINTER(qq_solve_info)], I),
         "qq_gmresproj": ([P, P, P, IP, D, I, DP, I, P, C.POINTER(qq_solve_info)], I),
         "qq_gmresdrshift": ([P, P, P, I, P, IP, D, I, DP, I, P, C.POINTER(qq_solve_info)], I),
@@ -222,6 +224,12 @@ class Deflation:
     @property
     def k(self) -> int:
         return self.lat.lib.qq_defl_size(self._h)
+
+    def vector(self, j: int, out=None):
+        """Deflation vector j (0..k) as a reference-layout even half vector."""
+        out = self.lat.new_half() if out is None else out
+        _check(self.lat.lib.qq_defl_vector(self._h, int(j), _ptr(out)))
+        return out
 
     def close(self):
         if self._h:
@@ -613,6 +621,14 @@ class Net:
         losses = np.zeros(max(nsteps, 1))
         _check(self.lib.qq_net_train(lat._ctx, self._h, _d2(kappa), int(nsamples), int(nsteps), float(lr),
                                      int(seed), losses.ctypes.data_as(C.POINTER(C.c_double))))
+        return losses[:nsteps]
+
+    def train_pairs(self, lat, b, x, nsteps=100, lr=1e-3):
+        """Adam steps on the caller's pairs: sources b and targets x (arrays of shape
+        (n,) + half_shape), the network learning N(b) = x; the loss before each step."""
+        losses = np.zeros(max(nsteps, 1))
+        _check(self.lib.qq_net_train_pairs(lat._ctx, self._h, int(b.shape[0]), _ptr(b), _ptr(x), int(nsteps),
+                                           float(lr), losses.ctypes.data_as(C.POINTER(C.c_double))))
         return losses[:nsteps]
 
     def close(self) -> None:

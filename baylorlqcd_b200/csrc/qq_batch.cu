@@ -164,6 +164,25 @@ int default_maxiter(const Geom& g, double tol) {
   return (int)std::min(100000.0, std::max(2000.0, 40.0 * lmax * decades));
 }
 
+// After right-hand side k's FP64 residual went back into slot k of r: the next
+// iteration's rho' = <rhat, r> and beta for k alone (the fused dot of the iteration saw
+// the old residual).  pred: the insert mask (graph and host-driven loops), or nullptr
+// (the host did the insertion).
+int reinsert_rho(qq_ctx* c, int prec, const BlockBiArgs& A, int k, const int* dslots, unsigned* ctl,
+                 const unsigned* pred) {
+  count_launch(2);
+  if (prec == P32)
+    slot_dot_kernel<P32><<<kRedBlocks, kRedThreads, 0, c->st>>>(A.vh, A.nb, k, A.rhat, A.r, pred, A.partial);
+  else if (prec == P16)
+    slot_dot_kernel<P16><<<kRedBlocks, kRedThreads, 0, c->st>>>(A.vh, A.nb, k, A.rhat, A.r, pred, A.partial);
+  else
+    slot_dot_kernel<P64><<<kRedBlocks, kRedThreads, 0, c->st>>>(A.vh, A.nb, k, A.rhat, A.r, pred, A.partial);
+  QQ_CK(cudaGetLastError());
+  reliable_rho_kernel<<<1, 256, 0, c->st>>>(A.S, dslots, ctl, k, A.partial, kRedBlocks, pred ? 0 : 1);
+  QQ_CK(cudaGetLastError());
+  return QQ_OK;
+}
+
 bool host_loop_forced() {
   const char* e = std::getenv("QQ_HOST_LOOP");  // testing: the host-driven loop
   return e && std::atoi(e) != 0;
@@ -285,7 +304,12 @@ int full_residual(qq_ctx* c, Spinor be, Spinor bo, Spinor xe, Spinor xo, const d
 // Scalars of a right-hand side before its first iteration: rhat = r = the FP64
 // residual of the initial guess, whose norm also anchors the stall test.
 void init_scalars(double* sc, const PerRhs& R) {
-  sc[SC_RHO] = sc[SC_ALPHA] = sc[SC_OMEGA] = 1.0;
+  // rhat = r = the residual, so rho = <rhat, r> = ||r||^2; with p = v = 0 the first
+  // P_UPDATE gives p = r whatever beta is
+  sc[SC_ALPHA] = sc[SC_OMEGA] = 1.0;
+  sc[SC_RHO] = R.rn * R.rn;
+  sc[SC_RHO + 1] = 0.0;
+  sc[SC_BETA] = sc[SC_BETA + 1] = 0.0;
   sc[SC_RMAX] = R.rmax;
   sc[SC_BN] = R.bn > 0.0 ? R.bn : 1.0;
   sc[SC_R2] = R.rn * R.rn;
@@ -389,7 +413,6 @@ int bicgstab_block_sync(qq_ctx* c, std::vector<PerRhs*>& rhs, int prec, double t
   while (active && done_its < maxiter) {
     const int nchunk = std::min(kChunk, maxiter - done_its);
     for (int i = 0; i < nchunk; ++i) {
-      QQ_TRY(block_op(c, prec, A, OP_DOT_RHAT_R, ds, ST_BETA, sc));
       QQ_TRY(block_op(c, prec, A, OP_P_UPDATE, ds, -1, sc));
       QQ_TRY(op_and_dot(c, prec, A, v.sp(), p.sp(), tmp.sp(), rhat.sp(), 1, kappa, ds, sc));
       QQ_TRY(block_op(c, prec, A, OP_S_UPDATE, ds, -1, sc));
@@ -446,6 +469,8 @@ int bicgstab_block_sync(qq_ctx* c, std::vector<PerRhs*>& rhs, int prec, double t
       hctl[CTL_ACTIVE] = active;
       hctl[CTL_PENDING] = 0u;
       QQ_CK(cudaMemcpyAsync(Sd, hS, sizeof(double) * (kSyncDoubles), cudaMemcpyHostToDevice, c->st));
+      for (int k = 0; k < nb; ++k)  // rho and beta of the re-inserted residuals, on the device
+        if ((back >> k) & 1u) QQ_TRY(reinsert_rho(c, prec, A, k, ds, ctl, nullptr));
     }
   }
   QQ_CK(cudaStreamSynchronize(c->st));
@@ -555,7 +580,6 @@ int bicgstab_block(qq_ctx* c, std::vector<PerRhs*>& rhs, int prec, double tol, d
   constexpr int kChunk = 1;  // a pending RHS idles 1-2 iterations before its update runs
   auto run_chunk = [&]() -> int {
     for (int i = 0; i < kChunk; ++i) {
-      QQ_TRY(block_op(c, prec, A, OP_DOT_RHAT_R, ds, ST_BETA, sctl));
       QQ_TRY(block_op(c, prec, A, OP_P_UPDATE, ds, -1, sctl));
       QQ_TRY(op_and_dot(c, prec, A, v.sp(), p.sp(), tmp.sp(), rhat.sp(), 1, kappa, ds, sctl));
       QQ_TRY(block_op(c, prec, A, OP_S_UPDATE, ds, -1, sctl));
@@ -576,6 +600,7 @@ int bicgstab_block(qq_ctx* c, std::vector<PerRhs*>& rhs, int prec, double tol, d
     reliable_decide_kernel<<<1, 1, 0, c->st>>>(Sd, ds, ctl, k, tol, dhist, dhits, kHist);
     QQ_CK(cudaGetLastError());
     QQ_TRY(block_slot(c, prec, nb, k, r.sp(), R.r64.sp(), 0, ctl + CTL_INSERT));
+    QQ_TRY(reinsert_rho(c, prec, A, k, ds, ctl, ctl + CTL_INSERT));
     reliable_resume_kernel<<<1, 1, 0, c->st>>>(ctl, k);
     QQ_CK(cudaGetLastError());
     return QQ_OK;

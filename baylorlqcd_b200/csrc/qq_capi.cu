@@ -313,6 +313,27 @@ int qq_defl_destroy(qq_defl* d) {
 
 int qq_defl_size(const qq_defl* d) { return d ? d->space.k : 0; }
 
+int qq_defl_vector(const qq_defl* d, int j, double* v) {
+  if (!d || !v) return set_error(QQ_BAD_ARG, "null argument");
+  if (j < 0 || j > d->space.k || d->space.k == 0) return set_error(QQ_BAD_ARG, "no such deflation vector");
+  qq_ctx* c = d->ctx;
+  QQ_TRY(set_device(c));
+  const Spinor f{static_cast<char*>(d->space.V.p) + (size_t)j * d->space.nel * 16, nullptr, d->space.pb};
+  double* o = nullptr;
+  const size_t nv = c->ref_doubles();
+  QQ_TRY(stage_out_begin(c, 2, v, nv, &o));
+  if (d->space.pb == P64) {
+    QQ_TRY(field_to_ref(c, f, 0, o));
+  } else {  // a reduced-precision space: through an FP64 temporary
+    Tmp t(c, P64);
+    QQ_TRY(lin(c, t.sp(), cimm(1.0), f));
+    QQ_TRY(field_to_ref(c, t.sp(), 0, o));
+  }
+  QQ_TRY(stage_out_end(c, 2, v, nv, o));
+  QQ_CK(cudaStreamSynchronize(c->st));
+  return QQ_OK;
+}
+
 int qq_gmresdr(qq_ctx* c, const double* phi, double* x, const int GMRES[2], double resmax,
                int itermin, const double kappa[2], int iflag, qq_defl* defl, qq_solve_info* info) {
   QQ_TRY(check_ctx(c));

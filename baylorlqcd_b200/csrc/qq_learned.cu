@@ -664,6 +664,13 @@ extern "C" int qq_net_grad(qq_ctx* c, qq_net* net, int nsamples, const double* b
   return QQ_OK;
 }
 
+namespace qq {
+namespace {
+int adam_steps(qq_ctx* c, qq_net* net, const std::vector<DevBuf>& B, const std::vector<DevBuf>& X,
+               const std::vector<double>& xn2, int nsteps, double lr, double* losses);
+}  // namespace
+}  // namespace qq
+
 extern "C" int qq_net_train(qq_ctx* c, qq_net* net, const double kappa[2], int nsamples, int nsteps, double lr,
                             unsigned long long seed, double* losses) {
   QQ_TRY(net_check(c, net));
@@ -689,6 +696,28 @@ extern "C" int qq_net_train(qq_ctx* c, qq_net* net, const double kappa[2], int n
     net_embed_kernel<<<nblk, 128, 0, c->st>>>(c->g, g, xf.sp(), X[i].as<float2>());
     QQ_CK(cudaGetLastError());
   }
+  return adam_steps(c, net, B, X, xn2, nsteps, lr, losses);
+}
+
+extern "C" int qq_net_train_pairs(qq_ctx* c, qq_net* net, int nsamples, const double* b, const double* x, int nsteps,
+                                  double lr, double* losses) {
+  QQ_TRY(net_check(c, net));
+  if (nsamples < 1 || !b || !x || nsteps < 0 || !(lr > 0.0)) return set_error(QQ_BAD_ARG, "bad arguments");
+  std::vector<DevBuf> B(nsamples), X(nsamples);
+  std::vector<double> xn2;
+  QQ_TRY(net_embed_refs(c, nsamples, b, B, nullptr));
+  QQ_TRY(net_embed_refs(c, nsamples, x, X, &xn2));
+  for (double v : xn2)
+    if (!(v > 0.0)) return set_error(QQ_BAD_ARG, "a target vector is zero");
+  return adam_steps(c, net, B, X, xn2, nsteps, lr, losses);
+}
+
+namespace qq {
+namespace {
+// nsteps Adam steps (learning rate lr) on the loss of net_loss_grad over the embedded
+// pairs (B[i], X[i]); losses[step] (may be null) = the loss before each step.
+int adam_steps(qq_ctx* c, qq_net* net, const std::vector<DevBuf>& B, const std::vector<DevBuf>& X,
+               const std::vector<double>& xn2, int nsteps, double lr, double* losses) {
   const size_t n = net->nw();
   std::vector<double2> gh(n);
   constexpr double b1 = 0.9, b2 = 0.999, eps = 1e-12;
@@ -717,6 +746,8 @@ extern "C" int qq_net_train(qq_ctx* c, qq_net* net, const double kappa[2], int n
   }
   return QQ_OK;
 }
+}  // namespace
+}  // namespace qq
 
 // Flexible GMRES(m) (k = 0) or flexible GMRES-DR(m, k) preconditioned by the network
 // (or unpreconditioned when net is null); when two consecutive cycles each gain less

@@ -70,7 +70,7 @@ enum BiOp : int {
   OP_DOT_RHAT_V = 2,  // red: <rhat, v>
   OP_S_UPDATE = 3,    // r = r - alpha v
   OP_DOTS_T = 4,      // red: <t, r>, ||t||^2
-  OP_XR_UPDATE = 5,   // x += alpha p + omega r ; r -= omega t ; red: ||r||^2
+  OP_XR_UPDATE = 5,   // x += alpha p + omega r ; r -= omega t ; red: ||r||^2, <rhat, r>
 };
 
 struct BlockBiArgs {
@@ -153,8 +153,14 @@ __global__ void __launch_bounds__(kRedThreads) bicg_block_kernel(BlockBiArgs A) 
         IO::store(A.r.data, A.r.norm, n, s, c);
         if (P == P16) IO::load(A.r.data, A.r.norm, n, s, c);  // reduce what was stored
       }
+      // ||r||^2 and, fused, the next iteration's rho' = <rhat, r>
+      IO::load(A.rhat.data, A.rhat.norm, n, s, b);
 #pragma unroll
-      for (int q = 0; q < 12; ++q) acc[0] += (double)c[q].re * c[q].re + (double)c[q].im * c[q].im;
+      for (int q = 0; q < 12; ++q) {
+        acc[0] += (double)c[q].re * c[q].re + (double)c[q].im * c[q].im;
+        acc[1] += (double)b[q].re * c[q].re + (double)b[q].im * c[q].im;
+        acc[2] += (double)b[q].re * c[q].im - (double)b[q].im * c[q].re;
+      }
     }
   }
   if (OP == OP_DOT_RHAT_R || OP == OP_DOT_RHAT_V || OP == OP_DOTS_T || OP == OP_XR_UPDATE) {
@@ -181,7 +187,7 @@ enum ScalStep : int {
   ST_BETA = 0,   // rho' = <rhat,r>; beta = (rho'/rho)(alpha/omega); rho = rho'
   ST_ALPHA = 1,  // alpha = rho / <rhat, v>
   ST_OMEGA = 2,  // omega = <t, r> / ||t||^2
-  ST_R2 = 3,     // ||r||^2
+  ST_R2 = 3,     // ||r||^2, then (still iterating) ST_BETA on the fused <rhat, r>
 };
 
 // Right-hand side k stops for good, short of its tolerance, for reason `code`: it
@@ -192,9 +198,31 @@ __device__ inline void bicg_fail(double* s, unsigned* ctl, int k, int code) {
   s[SC_FAIL] = (double)code;
   atomicAnd(&ctl[CTL_ACTIVE], ~bit);
   atomicAnd(&ctl[CTL_PENDING], ~bit);
+  atomicAnd(&ctl[CTL_INSERT], ~bit);
   atomicOr(&ctl[CTL_FAIL], bit);
   atomicOr(&ctl[CTL_DONE], bit);
   if (code == FAIL_NAN) atomicOr(&ctl[CTL_NAN], bit);
+}
+
+// rho' = <rhat, r> arrived: beta = (rho'/rho)(alpha/omega), rho = rho' -- or a stop on a
+// non-finite or vanishing rho' (rnorm = ||r||).
+__device__ inline void bicg_beta(double* s, unsigned* ctl, int k, double d0, double d1, double rnorm) {
+  const double rho = sqrt(d0 * d0 + d1 * d1);
+  if (!isfinite(rho)) return bicg_fail(s, ctl, k, FAIL_NAN);
+  if (rho <= kBreakEps * s[SC_RHATN] * rnorm) return bicg_fail(s, ctl, k, FAIL_BREAKDOWN);
+  auto cdiv = [](double ar, double ai, double br, double bi, double* cr, double* ci) {
+    const double den = br * br + bi * bi;
+    *cr = (ar * br + ai * bi) / den;
+    *ci = (ai * br - ar * bi) / den;
+  };
+  double qr, qi, pr, pi;
+  cdiv(d0, d1, s[SC_RHO], s[SC_RHO + 1], &qr, &qi);                           // rho'/rho
+  cdiv(s[SC_ALPHA], s[SC_ALPHA + 1], s[SC_OMEGA], s[SC_OMEGA + 1], &pr, &pi);  // alpha/omega
+  s[SC_BETA] = qr * pr - qi * pi;
+  s[SC_BETA + 1] = qr * pi + qi * pr;
+  s[SC_RHO] = d0;
+  s[SC_RHO + 1] = d1;
+  if (!isfinite(s[SC_BETA]) || !isfinite(s[SC_BETA + 1])) bicg_fail(s, ctl, k, FAIL_NAN);
 }
 
 // One block per right-hand side: sum the partials (fixed order), update the scalars.
@@ -231,17 +259,7 @@ static __global__ void bicg_scalar_kernel(double* S, const int* slots, const dou
   };
   const double rnorm = sqrt(s[SC_R2]);  // ||r|| of the previous iteration (or update)
   if (step == ST_BETA) {
-    const double rho = sqrt(d0 * d0 + d1 * d1);
-    if (!isfinite(rho)) return bicg_fail(s, ctl, k, FAIL_NAN);
-    if (rho <= kBreakEps * s[SC_RHATN] * rnorm) return bicg_fail(s, ctl, k, FAIL_BREAKDOWN);
-    double qr, qi, pr, pi;
-    cdiv(d0, d1, s[SC_RHO], s[SC_RHO + 1], &qr, &qi);                           // rho'/rho
-    cdiv(s[SC_ALPHA], s[SC_ALPHA + 1], s[SC_OMEGA], s[SC_OMEGA + 1], &pr, &pi);  // alpha/omega
-    s[SC_BETA] = qr * pr - qi * pi;
-    s[SC_BETA + 1] = qr * pi + qi * pr;
-    s[SC_RHO] = d0;
-    s[SC_RHO + 1] = d1;
-    if (!isfinite(s[SC_BETA]) || !isfinite(s[SC_BETA + 1])) return bicg_fail(s, ctl, k, FAIL_NAN);
+    bicg_beta(s, ctl, k, d0, d1, rnorm);
   } else if (step == ST_ALPHA) {
     const double den = sqrt(d0 * d0 + d1 * d1);
     if (!isfinite(den)) return bicg_fail(s, ctl, k, FAIL_NAN);
@@ -265,8 +283,74 @@ static __global__ void bicg_scalar_kernel(double* S, const int* slots, const dou
       atomicOr(&ctl[CTL_PENDING], 1u << k);
     } else if (window > 0 && s[SC_ITS] - s[SC_CHK_ITS] >= (double)window) {
       bicg_fail(s, ctl, k, FAIL_STALL);
+    } else {  // the next iteration's beta from the fused <rhat, r>
+      bicg_beta(s, ctl, k, d1, d2, rn);
     }
   }
+}
+
+// <rhat, r> of right-hand side k's slot of two block fields, per-block partials (re,
+// im, 0) at partial[block * 3]; skipped unless bit k of *pred (the insert mask) is set.
+template <int P>
+__global__ void __launch_bounds__(kRedThreads) slot_dot_kernel(int vh, int nb, int k, Spinor a, Spinor b,
+                                                              const unsigned* pred, double* partial) {
+  using IO = SpinorIO<P>;
+  if (pred && !((*pred >> k) & 1u)) return;
+  const int n = vh * nb;
+  double re = 0.0, im = 0.0;
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < vh; s += gridDim.x * blockDim.x) {
+    cplx<typename IO::R> x[12], y[12];
+    IO::load(a.data, a.norm, n, s * nb + k, x);
+    IO::load(b.data, b.norm, n, s * nb + k, y);
+#pragma unroll
+    for (int q = 0; q < 12; ++q) {
+      re += (double)x[q].re * y[q].re + (double)x[q].im * y[q].im;
+      im += (double)x[q].re * y[q].im - (double)x[q].im * y[q].re;
+    }
+  }
+  __shared__ double red[2][kRedThreads];
+  red[0][threadIdx.x] = re;
+  red[1][threadIdx.x] = im;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) {
+      red[0][threadIdx.x] += red[0][threadIdx.x + o];
+      red[1][threadIdx.x] += red[1][threadIdx.x + o];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    partial[blockIdx.x * 3] = red[0][0];
+    partial[blockIdx.x * 3 + 1] = red[1][0];
+    partial[blockIdx.x * 3 + 2] = 0.0;
+  }
+}
+
+// After right-hand side k's residual was re-inserted (bit k of the insert mask, or
+// unconditionally when `always`): rho' = <rhat, r> from slot_dot_kernel's partials
+// (fixed-order sum), then beta and rho as at ST_BETA.  One block of 256 threads.
+static __global__ void reliable_rho_kernel(double* S, const int* slots, unsigned* ctl, int k,
+                                           const double* partial, int nblocks, int always) {
+  if (!always && !((ctl[CTL_INSERT] >> k) & 1u)) return;
+  __shared__ double red[2][256];
+  double a0 = 0.0, a1 = 0.0;
+  for (int b = threadIdx.x; b < nblocks; b += blockDim.x) {
+    a0 += partial[b * 3];
+    a1 += partial[b * 3 + 1];
+  }
+  red[0][threadIdx.x] = a0;
+  red[1][threadIdx.x] = a1;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) {
+      red[0][threadIdx.x] += red[0][threadIdx.x + o];
+      red[1][threadIdx.x] += red[1][threadIdx.x + o];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x != 0) return;
+  double* s = S + (size_t)slots[k] * kScal;
+  bicg_beta(s, ctl, k, red[0][0], red[1][0], sqrt(s[SC_R2]));
 }
 
 // End of right-hand side k's reliable update, after ||b - A x||^2 has landed in

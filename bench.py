@@ -33,6 +33,10 @@ notes' figures and the ncu captures under profiles/:
   --mode c4       the uneven batch: 48 Wilson solves over 8^3x16 .. 20^3x40
   --mode shift    multi-shift GMRES-DR against each shift alone
   --mode twvev    perturbative VEVs of the loop operators
+  --mode learned  the learned preconditioner: trained on a training configuration's own
+                  GMRES-DR solves (Z(2) sources, FP64 solutions) and deflation vectors,
+                  then flexible GMRES-DR with it against plain GMRES-DR on the held-out
+                  benchmark configuration, in wall time and operator applications
 """
 from __future__ import annotations
 
@@ -101,7 +105,10 @@ def parse(argv=None):
     p.add_argument("--e2e-steps", type=int, default=0, help="end-to-end steps (0: min(steps, 5))")
     p.add_argument("--cpu-threads", type=int, default=0, help="host threads of the CPU legs (0: all)")
     p.add_argument("--no-cpu", action="store_true")
-    p.add_argument("--mode", default="solve", choices=["solve", "dslash", "c3", "c4", "shift", "twvev"])
+    p.add_argument("--mode", default="solve", choices=["solve", "dslash", "c3", "c4", "shift", "twvev", "learned"])
+    p.add_argument("--train-solves", type=int, default=8, help="--mode learned: training solves")
+    p.add_argument("--train-steps", type=int, default=200, help="--mode learned: Adam steps")
+    p.add_argument("--channels", default="4,8,8,4", help="--mode learned: channels per layer")
     p.add_argument("--shape", type=int, default=0, help="--mode dslash: kernel shape (0: autotuned)")
     p.add_argument("--iters", type=int, default=20, help="--mode dslash: timed launches")
     p.add_argument("--nnoise", type=int, default=24, help="--mode c3: noises")
@@ -633,10 +640,64 @@ def run_twvev(a):
     return {"mode": "twvev", "lattice": list(dims), "nsub": a.nsub, "seconds": ts}
 
 
+def run_learned(a):
+    """The learned preconditioner on the benchmark operator.  Training configuration
+    (heatbath seed 14): --train-solves Z(2) sources solved by plain FP64 GMRES-DR(m,k) to
+    the tolerance (the deflation space of the first kept), the pairs (b, x) of those
+    solves and (Hdbletm v, v) of its deflation vectors; Adam on them.  Held-out
+    configuration (seed 13, the benchmark's): the point source of site (1,1,1,1) solved by
+    flexible GMRES-DR(m,k) with the network, without it, and by plain GMRES-DR."""
+    import baylorlqcd_b200 as qq
+
+    dims = tuple(int(x) for x in a.dims.split(","))
+    kappa = (a.kappa, a.mu)
+    G = (a.m, a.k)
+    chans = tuple(int(c) for c in a.channels.split(","))
+    train, _ = heatbath_lattice(qq, dims, a.sweeps, 14)
+    qq.initlagfib(0, 7)
+    B, X = [], []
+    d = train.deflation(a.m, a.k)
+    t0 = time.perf_counter()
+    for i in range(a.train_solves):
+        b, _ = train.z2source()
+        x, _ = train.gmresdr(b, train.new_half(), G, a.tol, kappa=kappa, defl=d if i == 0 else None)
+        B.append(b)
+        X.append(x)
+    for j in range(d.k):
+        v = d.vector(j)
+        X.append(v)
+        B.append(train.hdbletm(v, 0, kappa))
+    t_pairs = time.perf_counter() - t0
+    net = qq.Net(chans, seed=1, scale=a.kappa**2)
+    t0 = time.perf_counter()
+    losses = net.train_pairs(train, np.stack(B), np.stack(X), nsteps=a.train_steps, lr=2e-3)
+    t_train = time.perf_counter() - t0
+    d.close()
+    train.close()
+    test, _ = heatbath_lattice(qq, dims, a.sweeps, 13)
+    b = test.pointsource((1, 1, 1, 1), 1, 1)[0]
+    test.fgmres(b, kappa, m=G[0], k=G[1], resmax=1e-3, net=net)  # tuning
+    res = {}
+    for label, n in (("fgmresdr_net", net), ("fgmresdr_plain", None)):
+        _, info = test.fgmres(b, kappa, m=G[0], k=G[1], resmax=a.tol, max_cycles=500, net=n)
+        res[label] = {"seconds": info.seconds, "mvp": info.mvp, "status": info.status, "fallback": info.fallback,
+                      "true_rel": info.true_rel}
+    _, info = test.gmresdr(b, test.new_half(), G, a.tol, kappa=kappa)
+    res["gmresdr"] = {"seconds": info.seconds, "mvp": info.mvp, "status": info.status, "true_rel": info.true_rel}
+    test.close()
+    return {"mode": "learned", "lattice": list(dims), "kappa": kappa, "channels": list(chans), "GMRES": list(G),
+            "training": {"solves": a.train_solves, "low_modes": len(B) - a.train_solves, "pairs_seconds": t_pairs,
+                         "adam_steps": a.train_steps, "train_seconds": t_train, "loss_first": float(losses[0]),
+                         "loss_last": float(losses[-1])},
+            "held_out": res,
+            "gain_vs_gmresdr": res["gmresdr"]["seconds"] / res["fgmresdr_net"]["seconds"]}
+
+
 def main(argv=None):
     a = parse(argv)
     if a.mode != "solve":
-        fn = {"dslash": run_dslash, "c3": run_c3, "c4": run_c4, "shift": run_shift, "twvev": run_twvev}[a.mode]
+        fn = {"dslash": run_dslash, "c3": run_c3, "c4": run_c4, "shift": run_shift, "twvev": run_twvev,
+              "learned": run_learned}[a.mode]
         print(json.dumps(fn(a)), flush=True)
         return 0
     rank, world, local = dist_env()

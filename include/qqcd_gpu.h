@@ -136,6 +136,11 @@ int qq_defl_create(qq_ctx* ctx, int nmax, int kmax, qq_defl** out);
 int qq_defl_destroy(qq_defl* d);
 /* Number k of deflation vectors held (0 before a GMRES-DR solve). */
 int qq_defl_size(const qq_defl* d);
+/* Deflation vector j (0..k: the first k span the harmonic Ritz vectors of the last
+ * restart, the reference's vtemp(:,1:k+1), Q/shift.f90) as a reference-layout even half
+ * vector v (host or device).  No counterpart routine in the reference, which keeps them
+ * in the shift module; the learned preconditioner trains on these low modes. */
+int qq_defl_vector(const qq_defl* d, int j, double* v);
 
 /* gmresdr :2871-3572.  Solves Hdbletm x = phi.  GMRES[0] = n, GMRES[1] = k.
  * x: initial guess on entry, solution on exit.  defl (optional) receives the k+1
@@ -427,6 +432,12 @@ int qq_net_grad(qq_ctx* ctx, qq_net* net, int nsamples, const double* b, const d
  * x drawn from `seed`; losses[step] (may be NULL) receives the loss before each step. */
 int qq_net_train(qq_ctx* ctx, qq_net* net, const double kappa[2], int nsamples, int nsteps, double lr,
                  unsigned long long seed, double* losses);
+/* The same on the caller's pairs: nsamples sources b and targets x (reference-layout even
+ * half vectors back to back, host or device), the network learning N(b) = x -- e.g. the
+ * (source, FP64 solution) pairs and the low modes (Hdbletm v, v) of the deflated
+ * inverter's own solves. */
+int qq_net_train_pairs(qq_ctx* ctx, qq_net* net, int nsamples, const double* b, const double* x, int nsteps,
+                       double lr, double* losses);
 /* Flexible GMRES(m) on Hdbletm x = phi with the network as right preconditioner (net
  * NULL: none), FP64; converged when ||phi - A x|| / ||phi - A x0|| < resmax, checked
  * once per cycle.  If two consecutive cycles each gain less than a factor 2, plain

@@ -205,6 +205,13 @@ module qqcd_gpu
       type(c_ptr), value :: d
       integer(c_int) :: k
     end function qq_defl_size
+    function qq_defl_vector(d, j, v) bind(C, name="qq_defl_vector") result(st)
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: d
+      integer(c_int), value :: j
+      real(c_double), intent(out) :: v(*)
+      integer(c_int) :: st
+    end function qq_defl_vector
     function qq_gmresdr(ctx, phi, x, GMRES, resmax, itermin, kappa, iflag, defl, info) &
         bind(C, name="qq_gmresdr") result(st)
       import :: c_int, c_ptr, c_double, qq_solve_info
@@ -584,6 +591,17 @@ module qqcd_gpu
       real(c_double), intent(out) :: losses(*)
       integer(c_int) :: st
     end function qq_net_train
+    function qq_net_train_pairs(ctx, net, nsamples, b, x, nsteps, lr, losses) &
+        bind(C, name="qq_net_train_pairs") result(st)
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: ctx, net
+      integer(c_int), value :: nsamples
+      real(c_double), intent(in) :: b(*), x(*)
+      integer(c_int), value :: nsteps
+      real(c_double), value :: lr
+      real(c_double), intent(out) :: losses(*)
+      integer(c_int) :: st
+    end function qq_net_train_pairs
     function qq_fgmres(ctx, net, phi, x, m, resmax, max_cycles, kappa, info) bind(C, name="qq_fgmres") result(st)
       import :: c_int, c_ptr, c_double, qq_solve_info
       type(c_ptr), value :: ctx, net

@@ -166,3 +166,60 @@ def test_flexible_gmresdr_gains(config):
     assert np.linalg.norm((x_net - x_dr)[:, :, :, :nv]) / np.linalg.norm(x_dr[:, :, :, :nv]) < 1e-8
     assert inet.mvp < 0.8 * ipl.mvp, (inet.mvp, ipl.mvp)
     net.close()
+
+
+def test_deflation_vectors_are_the_gmresdr_space(config):
+    """qq_defl_vector returns the k + 1 orthonormal vectors the GMRES-DR restart keeps,
+    and A maps the first k into their span (A V_k = V_{k+1} H_k): the projection of each
+    A v_j onto the k + 1 vectors leaves a residual at rounding level."""
+    lat, _ = config
+    phi = random_half(lat.ntotal, lat.nvhalf, seed=12)
+    d = lat.deflation(24, 8)
+    lat.gmresdr(phi, np.zeros_like(phi), (24, 8), 1e-10, kappa=KAPPA, defl=d)
+    k = d.k
+    assert k == 8
+    nv = lat.nvhalf
+    V = [d.vector(j) for j in range(k + 1)]
+    cv = np.stack([(v[:, :, :, :nv, 0::2] + 1j * v[:, :, :, :nv, 1::2]).ravel() for v in V])
+    np.testing.assert_allclose(cv.conj() @ cv.T, np.eye(k + 1), atol=1e-10)
+    for j in range(k):
+        av = lat.hdbletm(V[j], 0, KAPPA)
+        ca = (av[:, :, :, :nv, 0::2] + 1j * av[:, :, :, :nv, 1::2]).ravel()
+        res = ca - cv.T @ (cv.conj() @ ca)
+        assert np.linalg.norm(res) < 1e-9 * np.linalg.norm(ca), j
+    with pytest.raises(Exception):
+        d.vector(k + 1)
+    d.close()
+
+
+def test_training_on_solver_pairs_gains(config):
+    """The network trained on the deflated inverter's own output -- (source, FP64
+    solution) pairs of GMRES-DR solves of Z(2) noises and (A v, v) of its deflation
+    vectors -- lowers its loss and cuts the operator applications of flexible GMRES-DR
+    on a held-out source, with the FP64 true residual judging the answer."""
+    import baylorlqcd_b200 as qq
+
+    lat, _ = config
+    qq.initlagfib(0, 3)
+    d = lat.deflation(32, 10)
+    B, X = [], []
+    for i in range(4):
+        b, _ = lat.z2source()
+        x, info = lat.gmresdr(b, lat.new_half(), (32, 10), 1e-10, kappa=KAPPA, defl=d if i == 0 else None)
+        assert info.status == 0
+        B.append(b)
+        X.append(x)
+    for j in range(d.k):
+        v = d.vector(j)
+        X.append(v)
+        B.append(lat.hdbletm(v, 0, KAPPA))
+    d.close()
+    net = qq.Net((4, 8, 8, 4), seed=4, scale=KAPPA[0] ** 2)
+    losses = net.train_pairs(lat, np.stack(B), np.stack(X), nsteps=150, lr=2e-3)
+    assert np.all(np.isfinite(losses)) and losses[-1] < 0.5 * losses[0]
+    phi = random_half(lat.ntotal, lat.nvhalf, seed=21)
+    _, inet = lat.fgmres(phi, KAPPA, m=32, k=10, resmax=1e-10, net=net)
+    _, ipl = lat.fgmres(phi, KAPPA, m=32, k=10, resmax=1e-10, net=None)
+    assert inet.status == 0 and inet.true_rel < 1e-10 and inet.fallback == 0
+    assert inet.mvp < 0.8 * ipl.mvp, (inet.mvp, ipl.mvp)
+    net.close()

@@ -27,7 +27,7 @@ constexpr int kMaxRhs = 8;     // right-hand sides per launch, separate fields
 constexpr int kMaxBatch = 32;  // right-hand sides per launch, one block field
 constexpr int kShapeMrhs = 200;  // kernel-shape code base of hop_mrhs_kernel (200 + RPT)
 constexpr int kShapeF2 = 300;    // kernel-shape code base of hop_f2_kernel (300 + RPT)
-constexpr int kShapeMax = kShapeF2 + 10;  // the largest kernel-shape code
+constexpr int kShapeMax = kShapeF2 + 11;  // the largest kernel-shape code
 
 struct HopArgs {
   Geom g;

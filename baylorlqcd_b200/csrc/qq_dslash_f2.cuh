@@ -445,9 +445,40 @@ __global__ void __launch_bounds__(128) hop_f2s_kernel(HopArgs a) {
 // ---------------------------------------------------------------------------
 constexpr int kF2aMatStride = 8 * 5 + 1;  // 16-byte entries per site
 
-inline size_t f2a_smem_bytes(int per_block, int threads, int depth, int rpt) {
-  return (size_t)per_block * 8 * 8 + (size_t)16 * per_block * (24 + kF2aMatStride) +
+// MB = 1 keeps every matrix entry pre-broadcast, (re, re, im, im) in one 16-byte entry,
+// 9 per hop: the SU(3) product reads a row's three entries just before it needs them
+// and uses their halves as packed operands, with no broadcast instructions.
+__host__ __device__ constexpr int f2a_mat_stride(int mb) { return mb ? 8 * 9 + 1 : kF2aMatStride; }
+
+inline size_t f2a_smem_bytes(int per_block, int threads, int depth, int rpt, int mb = 0) {
+  return (size_t)per_block * 8 * 8 + (size_t)16 * per_block * (24 + f2a_mat_stride(mb)) +
          (size_t)16 * depth * rpt * 6 * threads;
+}
+
+// w = M h with M's rows read from pre-broadcast shared entries e = (re, re, im, im).
+__device__ inline void matvec2_rows(const float4* mp, const float2* hre, const float2* him, float2* wre,
+                                    float2* wim) {
+  float2 nhim[3];
+#pragma unroll
+  for (int b = 0; b < 3; ++b) nhim[b] = f2mul(f2bc(-1.0f), him[b]);
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    float4 e = mp[3 * a];
+    float2 xr = f2mul(make_float2(e.x, e.y), hre[0]);
+    float2 xi = f2mul(make_float2(e.x, e.y), him[0]);
+    xr = f2fma(make_float2(e.z, e.w), nhim[0], xr);
+    xi = f2fma(make_float2(e.z, e.w), hre[0], xi);
+#pragma unroll
+    for (int b = 1; b < 3; ++b) {
+      e = mp[3 * a + b];
+      xr = f2fma(make_float2(e.x, e.y), hre[b], xr);
+      xr = f2fma(make_float2(e.z, e.w), nhim[b], xr);
+      xi = f2fma(make_float2(e.x, e.y), him[b], xi);
+      xi = f2fma(make_float2(e.z, e.w), hre[b], xi);
+    }
+    wre[a] = xr;
+    wim[a] = xi;
+  }
 }
 
 struct F2aShared {
@@ -486,7 +517,7 @@ __device__ inline void f2a_issue(const HopArgs& a, const F2aShared& sh, int s, i
   cp_async_commit();
 }
 
-template <int H, int D, int EPI, int RPT>
+template <int H, int D, int EPI, int RPT, int MB>
 __device__ inline void f2a_run(const HopArgs& a, const F2aShared& sh, int s, int sl, int j, int G, int T,
                                int tx, Pair12* acc) {
   if constexpr (H < 8) {
@@ -498,21 +529,23 @@ __device__ inline void f2a_run(const HopArgs& a, const F2aShared& sh, int s, int
       const float twice = MU == 3 ? 2.0f : 1.0f;
       const float cm = twice * sgn * (FWD ? a.c.fmf[MU] : a.c.bmf[MU]);
       const float cp = twice * sgn * (FWD ? a.c.fpf[MU] : a.c.bpf[MU]);
-      const float4* mp = sh.mat + sl * kF2aMatStride + H * 5;
-      float me[20];
-#pragma unroll
-      for (int e = 0; e < 5; ++e) {
-        const float4 t = mp[e];
-        me[4 * e] = t.x;
-        me[4 * e + 1] = t.y;
-        me[4 * e + 2] = t.z;
-        me[4 * e + 3] = t.w;
-      }
+      const float4* mp = sh.mat + sl * f2a_mat_stride(MB) + H * (MB ? 9 : 5);
       LinkPairs m;
+      if constexpr (MB == 0) {  // 18 floats in 5 entries, broadcast into pairs
+        float me[20];
 #pragma unroll
-      for (int e = 0; e < 9; ++e) {
-        m.r[e / 3][e % 3] = f2bc(me[2 * e]);
-        m.i[e / 3][e % 3] = f2bc(me[2 * e + 1]);
+        for (int e = 0; e < 5; ++e) {
+          const float4 t = mp[e];
+          me[4 * e] = t.x;
+          me[4 * e + 1] = t.y;
+          me[4 * e + 2] = t.z;
+          me[4 * e + 3] = t.w;
+        }
+#pragma unroll
+        for (int e = 0; e < 9; ++e) {
+          m.r[e / 3][e % 3] = f2bc(me[2 * e]);
+          m.i[e / 3][e % 3] = f2bc(me[2 * e + 1]);
+        }
       }
 #pragma unroll
       for (int k = 0; k < RPT; ++k) {
@@ -527,25 +560,32 @@ __device__ inline void f2a_run(const HopArgs& a, const F2aShared& sh, int s, int
         float2 hre[3], him[3], wre[3], wim[3];
         if (cm != 0.0f) {
           project2<MU, -1>(p, hre, him);
-          matvec2(m, hre, him, wre, wim);
+          if constexpr (MB == 1)
+            matvec2_rows(mp, hre, him, wre, wim);
+          else
+            matvec2(m, hre, him, wre, wim);
           recon2<MU, -1>(acc[k], cm, wre, wim);
         }
         if (cp != 0.0f) {
           project2<MU, +1>(p, hre, him);
-          matvec2(m, hre, him, wre, wim);
+          if constexpr (MB == 1)
+            matvec2_rows(mp, hre, him, wre, wim);
+          else
+            matvec2(m, hre, him, wre, wim);
           recon2<MU, +1>(acc[k], cp, wre, wim);
         }
       }
     }
     f2a_issue<H + D, D, EPI, RPT>(a, sh, s, sl, j, G, T, tx, true);
-    f2a_run<H + 1, D, EPI, RPT>(a, sh, s, sl, j, G, T, tx, acc);
+    f2a_run<H + 1, D, EPI, RPT, MB>(a, sh, s, sl, j, G, T, tx, acc);
   }
 }
 
 // Thread layout: threadIdx.x = (site-in-block) * G + j, G = nrhs / RPT threads per site.
 // MINB: resident blocks per SM the register allocation is capped for (4: none; 5 and 6
 // trade a few spilled registers for 25-50% more resident warps).
-template <int EPI, int D, int RPT, int MINB>
+// MB: hop-matrix layout (0: 5 packed entries per hop, 1: 9 pre-broadcast entries).
+template <int EPI, int D, int RPT, int MINB, int MB = 0>
 __global__ void __launch_bounds__(128, MINB) hop_f2a_kernel(HopArgs a) {
   extern __shared__ float4 f2a_smem[];
   const int T = blockDim.x, per = a.per_block, tx = threadIdx.x;
@@ -553,7 +593,7 @@ __global__ void __launch_bounds__(128, MINB) hop_f2a_kernel(HopArgs a) {
   F2aShared sh;
   sh.raw = f2a_smem;
   sh.mat = sh.raw + per * 24;
-  sh.ring = sh.mat + per * kF2aMatStride;
+  sh.ring = sh.mat + per * f2a_mat_stride(MB);
   sh.nbr = reinterpret_cast<int*>(sh.ring + D * RPT * 6 * T);
   sh.sgn = reinterpret_cast<float*>(sh.nbr + per * 8);
   const int s0 = blockIdx.x * per;
@@ -616,9 +656,15 @@ __global__ void __launch_bounds__(128, MINB) hop_f2a_kernel(HopArgs a) {
       v[2 * e + 1] = back ? -u.e[c][i].im : u.e[i][c].im;
     }
     v[18] = v[19] = 0.0f;
-    float4* dst = sh.mat + (k >> 3) * kF2aMatStride + (k & 7) * 5;
+    if constexpr (MB == 1) {
+      float4* dst = sh.mat + (k >> 3) * f2a_mat_stride(1) + (k & 7) * 9;
 #pragma unroll
-    for (int e = 0; e < 5; ++e) dst[e] = make_float4(v[4 * e], v[4 * e + 1], v[4 * e + 2], v[4 * e + 3]);
+      for (int e = 0; e < 9; ++e) dst[e] = make_float4(v[2 * e], v[2 * e], v[2 * e + 1], v[2 * e + 1]);
+    } else {
+      float4* dst = sh.mat + (k >> 3) * kF2aMatStride + (k & 7) * 5;
+#pragma unroll
+      for (int e = 0; e < 5; ++e) dst[e] = make_float4(v[4 * e], v[4 * e + 1], v[4 * e + 2], v[4 * e + 3]);
+    }
   }
   __syncthreads();
   double dsum[3] = {0.0, 0.0, 0.0};  // this thread's share of the fused dot products
@@ -628,7 +674,7 @@ __global__ void __launch_bounds__(128, MINB) hop_f2a_kernel(HopArgs a) {
     for (int k = 0; k < RPT; ++k)
 #pragma unroll
       for (int q = 0; q < 6; ++q) acc[k].re[q] = acc[k].im[q] = make_float2(0.0f, 0.0f);
-    f2a_run<0, D, EPI, RPT>(a, sh, s, sl, j, G, T, tx, acc);
+    f2a_run<0, D, EPI, RPT, MB>(a, sh, s, sl, j, G, T, tx, acc);
     if constexpr (EPI == EPI_DBLE) cp_async_wait<D - 2>();  // stages 8 and 9 (D >= 2)
 #pragma unroll
     for (int k = 0; k < RPT; ++k) {

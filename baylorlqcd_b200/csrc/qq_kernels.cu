@@ -171,7 +171,7 @@ static cudaError_t hop_f2s(const HopArgs& a, int epi, cudaStream_t st) {
 
 // Copy-ring kernel: D stages in flight per thread, RPT right-hand sides per thread,
 // registers capped for MINB resident blocks.
-template <int EPI, int D, int RPT, int MINB>
+template <int EPI, int D, int RPT, int MINB, int MB>
 static cudaError_t hop_f2a_epi(const HopArgs& b, size_t smem, cudaStream_t st) {
   // The limit is 227 KiB less the kernel's static shared memory (the same on every
   // device; a function-local static is initialised once even under concurrent launches).
@@ -181,32 +181,32 @@ static cudaError_t hop_f2a_epi(const HopArgs& b, size_t smem, cudaStream_t st) {
   };
   static const Attr attr = [] {
     cudaFuncAttributes fa;
-    cudaError_t e = cudaFuncGetAttributes(&fa, hop_f2a_kernel<EPI, D, RPT, MINB>);
+    cudaError_t e = cudaFuncGetAttributes(&fa, hop_f2a_kernel<EPI, D, RPT, MINB, MB>);
     if (e != cudaSuccess) return Attr{e, 0};
     return Attr{cudaSuccess, (size_t)227 * 1024 - fa.sharedSizeBytes};
   }();
   if (attr.err != cudaSuccess) return attr.err;
   if (smem > attr.max_dyn) return cudaErrorInvalidValue;
-  const cudaError_t e = smem_attr_once((const void*)hop_f2a_kernel<EPI, D, RPT, MINB>, (int)attr.max_dyn);
+  const cudaError_t e = smem_attr_once((const void*)hop_f2a_kernel<EPI, D, RPT, MINB, MB>, (int)attr.max_dyn);
   if (e != cudaSuccess) return e;
   const int G = b.nrhs / RPT;
   const dim3 blk(b.per_block * G), grd((b.g.vh + b.per_block - 1) / b.per_block);
-  hop_f2a_kernel<EPI, D, RPT, MINB><<<grd, blk, smem, st>>>(b);
+  hop_f2a_kernel<EPI, D, RPT, MINB, MB><<<grd, blk, smem, st>>>(b);
   return cudaGetLastError();
 }
 
-template <int D, int RPT, int MINB = 4>
+template <int D, int RPT, int MINB = 4, int MB = 0>
 static cudaError_t hop_f2a(const HopArgs& a, int epi, cudaStream_t st) {
   if (a.nrhs % RPT != 0 || (RPT > 1 && !a.blk)) return cudaErrorInvalidValue;
   const int G = a.nrhs / RPT;  // threads per site
   const int per_block = hop_sites_per_block(1, G);
   const HopArgs b = hop_prepare(a, per_block, G);
-  const size_t smem = f2a_smem_bytes(per_block, per_block * G, D, RPT);
+  const size_t smem = f2a_smem_bytes(per_block, per_block * G, D, RPT, MB);
   if (smem > 227 * 1024) return cudaErrorInvalidValue;
   switch (epi) {
-    case EPI_STORE: return hop_f2a_epi<EPI_STORE, D, RPT, MINB>(b, smem, st);
-    case EPI_TWIST: return hop_f2a_epi<EPI_TWIST, D, RPT, MINB>(b, smem, st);
-    case EPI_DBLE: return hop_f2a_epi<EPI_DBLE, D, RPT, MINB>(b, smem, st);
+    case EPI_STORE: return hop_f2a_epi<EPI_STORE, D, RPT, MINB, MB>(b, smem, st);
+    case EPI_TWIST: return hop_f2a_epi<EPI_TWIST, D, RPT, MINB, MB>(b, smem, st);
+    case EPI_DBLE: return hop_f2a_epi<EPI_DBLE, D, RPT, MINB, MB>(b, smem, st);
     default: return cudaErrorInvalidValue;
   }
 }
@@ -218,7 +218,8 @@ static cudaError_t hop_f2a(const HopArgs& a, int epi, cudaStream_t st) {
 // kShapeF2 + RPT (RPT = 1, 2, 3) = FP32 spinors with packed FP32x2 arithmetic (RPT > 1
 // on block fields only); kShapeF2 + 4 = the same, loads a hop ahead; + 5 = links staged
 // in shared memory (block fields); + 6, 7, 8 = copy ring with 2, 3, 4 stages in flight;
-// + 9, 10 = copy ring with 2 stages, registers capped for 5 / 6 resident blocks.
+// + 9, 10 = copy ring with 2 stages, registers capped for 5 / 6 resident blocks;
+// + 11 = copy ring with 3 stages and pre-broadcast hop matrices read row by row.
 cudaError_t launch_hop(const HopArgs& a, int sp, int recon, int epi, int tps, cudaStream_t st) {
   count_launch();
   const int maxr = a.blk ? kMaxBatch : kMaxRhs;
@@ -238,6 +239,7 @@ cudaError_t launch_hop(const HopArgs& a, int sp, int recon, int epi, int tps, cu
       case 8: return hop_f2a<4, 1>(a, epi, st);
       case 9: return hop_f2a<2, 1, 5>(a, epi, st);
       case 10: return hop_f2a<2, 1, 6>(a, epi, st);
+      case 11: return hop_f2a<3, 1, 4, 1>(a, epi, st);
 
       default: return cudaErrorInvalidValue;
     }

@@ -194,7 +194,7 @@ int launch_hop_tuned(qq_ctx* c, const HopArgs& a, int prec, int epi) {
   float best_ms = 1e30f;
   for (int tps : {1, 2, 32, 64, 96, 128, kShapeMrhs + 2, kShapeMrhs + 3, kShapeMrhs + 4, kShapeF2 + 1,
                   kShapeF2 + 2, kShapeF2 + 3, kShapeF2 + 4, kShapeF2 + 5, kShapeF2 + 6, kShapeF2 + 7,
-                  kShapeF2 + 8, kShapeF2 + 9, kShapeF2 + 10}) {
+                  kShapeF2 + 8, kShapeF2 + 9, kShapeF2 + 10, kShapeF2 + 11}) {
     const int per = tps <= 4 ? 128 / tps : tps;
     if (a.nrhs > per) continue;
     if (tps >= kShapeF2 + 6) {  // copy ring, every variant (its shared memory pays off from 4 RHS up)
@@ -359,7 +359,7 @@ int op_dbletm_block_impl(qq_ctx* c, Spinor out, Spinor in, Spinor tmp, int nb, i
     const int key = hop_tune_key(c, b, prec, EPI_DBLE);
     if (c->hop_tune.find(key) == c->hop_tune.end()) QQ_TRY(launch_hop_tuned(c, b, prec, EPI_DBLE));
     auto it = c->hop_tune.find(key);
-    if (it != c->hop_tune.end() && it->second >= kShapeF2 + 6 && it->second <= kShapeF2 + 10) {
+    if (it != c->hop_tune.end() && it->second >= kShapeF2 + 6 && it->second <= kShapeF2 + 11) {
       b.dot_op = dot_op.data;
       b.dot_part = dot_part;
       b.dot_mode = dot_mode;

@@ -173,7 +173,8 @@ def shape_name(shape: int) -> str:
         return "hop_mrhs_kernel"
     return {301: "hop_f2_kernel", 302: "hop_f2_kernel", 303: "hop_f2_kernel", 304: "hop_f2p_kernel",
             305: "hop_f2s_kernel", 306: "hop_f2a_kernel", 307: "hop_f2a_kernel",
-            308: "hop_f2a_kernel", 309: "hop_f2a_kernel", 310: "hop_f2a_kernel"}.get(shape, "hop kernel")
+            308: "hop_f2a_kernel", 309: "hop_f2a_kernel", 310: "hop_f2a_kernel",
+            311: "hop_f2a_kernel"}.get(shape, "hop kernel")
 
 
 # DRAM bytes (read + write) of one EPI_STORE launch from an ncu capture, keyed by

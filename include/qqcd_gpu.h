@@ -371,7 +371,7 @@ int qq_profile_hop_select(qq_ctx* ctx, int precision, int nrhs, long long* launc
  * 3, 4 hops in flight as asynchronous copies into a shared-memory ring, the links of
  * neighbour indices and hop matrices of the block's sites built once per block in
  * shared memory, >= 4 RHS recommended; 309, 310 = 306 with its registers capped for 5
- * and 6 resident blocks per SM).
+ * and 6 resident blocks per SM; 311 = 307 with the hop matrices kept pre-broadcast).
  * flush_l2 != 0 overwrites a 512 MiB buffer between launches so every launch reads
  * its operands from HBM.  ms_per_call: mean kernel time; bytes_per_call:
  * algorithmic bytes of one launch, V/2 * (8 * link bytes + nrhs * 2 * spinor bytes). */

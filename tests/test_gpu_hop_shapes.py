@@ -20,10 +20,10 @@ pytestmark = pytest.mark.gpu
 DIMS = (8, 4, 8, 12)
 BC = (1, 1, 1, -1)
 
-FP32_12 = [0, 1, 2, 4, 64, 128, 202, 203, 204, 301, 302, 303, 304, 305, 306, 307, 308, 309, 310]
-FP32_24 = [0, 306, 307, 308, 309, 310]
-FP32_1 = [1, 2, 4, 32, 128, 301, 304, 306, 307, 308, 309, 310]
-FP32_5 = [1, 301, 304, 306, 307, 308, 309, 310]
+FP32_12 = [0, 1, 2, 4, 64, 128, 202, 203, 204, 301, 302, 303, 304, 305, 306, 307, 308, 309, 310, 311]
+FP32_24 = [0, 306, 307, 308, 309, 310, 311]
+FP32_1 = [1, 2, 4, 32, 128, 301, 304, 306, 307, 308, 309, 310, 311]
+FP32_5 = [1, 301, 304, 306, 307, 308, 309, 310, 311]
 FP16_12 = [1, 2, 64, 202, 203, 204]
 
 
@@ -86,4 +86,4 @@ def test_unsupported_shape_is_an_error(pair):
     with pytest.raises(qq.QQError, match="BAD_ARG"):
         lat.hsingle_block(gin, 0, 1, precision=16, shape=301)  # packed FP32 kernel
     with pytest.raises(qq.QQError, match="BAD_ARG"):
-        lat.hsingle_block(gin, 0, 1, precision=32, shape=311)  # no such shape
+        lat.hsingle_block(gin, 0, 1, precision=32, shape=312)  # no such shape

@@ -114,10 +114,19 @@ int block_op(qq_ctx* c, int prec, const BlockBiArgs& A, int op, const int* dslot
   return QQ_OK;
 }
 
-// The scalar step alone, on partials already written (by a hop with a fused dot product).
+// The scalar step alone, on partials already written (by a hop with a fused dot product,
+// one per hop block: a long list, folded by a grid first).
 int scalar_step(qq_ctx* c, const BlockBiArgs& A, const int* dslots, int step, int nblocks, const ScalarCtl& sc) {
+  const double* part = A.partial;
+  if (nblocks > 2 * kFoldChunks) {
+    count_launch();
+    partial_fold_kernel<<<dim3(kFoldChunks, A.nb), 256, 0, c->st>>>(A.partial, nblocks, A.partial2, kFoldChunks);
+    QQ_CK(cudaGetLastError());
+    part = A.partial2;
+    nblocks = kFoldChunks;
+  }
   count_launch();
-  bicg_scalar_kernel<<<A.nb, 256, 0, c->st>>>(A.S, dslots, A.partial, nblocks, step, sc.ctl, sc.delta,
+  bicg_scalar_kernel<<<A.nb, 256, 0, c->st>>>(A.S, dslots, part, nblocks, step, sc.ctl, sc.delta,
                                               sc.half_tol, sc.window);
   QQ_CK(cudaGetLastError());
   return QQ_OK;
@@ -343,7 +352,8 @@ int bicgstab_block_sync(qq_ctx* c, std::vector<PerRhs*>& rhs, int prec, double t
   double *Sd = nullptr, *partd = nullptr;
   int* ds = nullptr;
   QQ_CK(ws_get(c, WS_SCAL, sizeof(double) * (kSyncDoubles), reinterpret_cast<void**>(&Sd)));
-  QQ_CK(ws_get(c, WS_PART, sizeof(double) * 3 * std::max(kRedBlocks, hop_block_count(c, nb)) * kMaxBatch,
+  const size_t npart = (size_t)3 * std::max(kRedBlocks, hop_block_count(c, nb)) * kMaxBatch;
+  QQ_CK(ws_get(c, WS_PART, sizeof(double) * (npart + (size_t)3 * kFoldChunks * kMaxBatch),
                reinterpret_cast<void**>(&partd)));
   QQ_CK(ws_get(c, WS_DSLOTS, sizeof(int) * kMaxBatch, reinterpret_cast<void**>(&ds)));
   unsigned* ctl = reinterpret_cast<unsigned*>(Sd + kScalDoubles);
@@ -403,6 +413,7 @@ int bicgstab_block_sync(qq_ctx* c, std::vector<PerRhs*>& rhs, int prec, double t
   for (int k = 0; k < nb; ++k) A.slot[k] = k;
   A.S = Sd;
   A.partial = partd;
+  A.partial2 = partd + npart;
   const ScalarCtl sc{ctl, delta, 0.5 * tol, window};
   // Iterations run in chunks without host synchronisation: a right-hand side whose
   // residual calls for a reliable update (or may have converged) takes itself out of
@@ -520,7 +531,8 @@ int bicgstab_block(qq_ctx* c, std::vector<PerRhs*>& rhs, int prec, double tol, d
   QQ_CK(ws_get(c, WS_SCAL, sbytes, reinterpret_cast<void**>(&Sd)));
   QQ_CK(ws_get(c, WS_HIST, sizeof(double) * kHist * nb, reinterpret_cast<void**>(&dhist)));
   QQ_CK(ws_get(c, WS_HITS, sizeof(int) * kHist * nb, reinterpret_cast<void**>(&dhits)));
-  QQ_CK(ws_get(c, WS_PART, sizeof(double) * 3 * std::max(kRedBlocks, hop_block_count(c, nb)) * kMaxBatch,
+  const size_t npart = (size_t)3 * std::max(kRedBlocks, hop_block_count(c, nb)) * kMaxBatch;
+  QQ_CK(ws_get(c, WS_PART, sizeof(double) * (npart + (size_t)3 * kFoldChunks * kMaxBatch),
                reinterpret_cast<void**>(&partd)));
   QQ_CK(ws_get(c, WS_DSLOTS, sizeof(int) * kMaxBatch, reinterpret_cast<void**>(&ds)));
   unsigned* ctl = reinterpret_cast<unsigned*>(Sd + kScalDoubles);
@@ -576,6 +588,7 @@ int bicgstab_block(qq_ctx* c, std::vector<PerRhs*>& rhs, int prec, double tol, d
   for (int k = 0; k < nb; ++k) A.slot[k] = k;
   A.S = Sd;
   A.partial = partd;
+  A.partial2 = partd + npart;
   const ScalarCtl sctl{ctl, delta, 0.5 * tol, window};
   constexpr int kChunk = 1;  // a pending RHS idles 1-2 iterations before its update runs
   auto run_chunk = [&]() -> int {

@@ -81,7 +81,13 @@ struct BlockBiArgs {
   int slot[kMaxBatch];         // scalar slot of each right-hand side
   double* S;                   // scalar array
   double* partial;             // [rhs][gridDim.x][3]
+  double* partial2;            // [rhs][kFoldChunks][3]: first-stage sums of long partial lists
 };
+
+// Per-block partial lists longer than this (the fused dot products of the hop kernel,
+// one entry per hop block) are first folded into kFoldChunks sums per right-hand side
+// by a grid of blocks, so the one-block-per-RHS scalar step sums few numbers.
+constexpr int kFoldChunks = 256;
 
 template <class R>
 __device__ inline cplx<R> cmuld(cplx<double> a, cplx<R> b) {
@@ -140,21 +146,25 @@ __global__ void __launch_bounds__(kRedThreads) bicg_block_kernel(BlockBiArgs A) 
         acc[2] += (double)a[q].re * a[q].re + (double)a[q].im * a[q].im;
       }
     } else {  // OP_XR_UPDATE
+      // every operand is loaded before the first store, so the loads overlap
+      cplx<R> d[12];
       IO::load(A.r.data, A.r.norm, n, s, c);
+      IO::load(A.rhat.data, A.rhat.norm, n, s, d);
       if (act) {
         IO::load(A.x.data, A.x.norm, n, s, a);
         IO::load(A.p.data, A.p.norm, n, s, b);
 #pragma unroll
         for (int q = 0; q < 12; ++q) a[q] = cadd(a[q], cadd(cmuld(alpha, b[q]), cmuld(omega, c[q])));
-        IO::store(A.x.data, A.x.norm, n, s, a);
         IO::load(A.t.data, A.t.norm, n, s, b);
+        IO::store(A.x.data, A.x.norm, n, s, a);
 #pragma unroll
         for (int q = 0; q < 12; ++q) c[q] = csub(c[q], cmuld(omega, b[q]));
         IO::store(A.r.data, A.r.norm, n, s, c);
         if (P == P16) IO::load(A.r.data, A.r.norm, n, s, c);  // reduce what was stored
       }
       // ||r||^2 and, fused, the next iteration's rho' = <rhat, r>
-      IO::load(A.rhat.data, A.rhat.norm, n, s, b);
+#pragma unroll
+      for (int q = 0; q < 12; ++q) b[q] = d[q];
 #pragma unroll
       for (int q = 0; q < 12; ++q) {
         acc[0] += (double)c[q].re * c[q].re + (double)c[q].im * c[q].im;
@@ -223,6 +233,29 @@ __device__ inline void bicg_beta(double* s, unsigned* ctl, int k, double d0, dou
   s[SC_RHO] = d0;
   s[SC_RHO + 1] = d1;
   if (!isfinite(s[SC_BETA]) || !isfinite(s[SC_BETA + 1])) bicg_fail(s, ctl, k, FAIL_NAN);
+}
+
+// First stage of a long per-block reduction: block (p, k) sums right-hand side k's
+// partials of hop blocks p*chunk .. (p+1)*chunk-1 in a fixed order into
+// partial2[(k * P + p) * 3 + q].
+static __global__ void __launch_bounds__(256) partial_fold_kernel(const double* partial, int nblocks,
+                                                                  double* partial2, int P) {
+  const int p = blockIdx.x, k = blockIdx.y;
+  const int chunk = (nblocks + P - 1) / P;
+  const int b0 = p * chunk, b1 = min(nblocks, b0 + chunk);
+  double a[3] = {0.0, 0.0, 0.0};
+  for (int b = b0 + threadIdx.x; b < b1; b += blockDim.x)
+    for (int q = 0; q < 3; ++q) a[q] += partial[((size_t)k * nblocks + b) * 3 + q];
+  __shared__ double red[3][256];
+  for (int q = 0; q < 3; ++q) red[q][threadIdx.x] = a[q];
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o)
+      for (int q = 0; q < 3; ++q) red[q][threadIdx.x] += red[q][threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    for (int q = 0; q < 3; ++q) partial2[((size_t)k * P + p) * 3 + q] = red[q][0];
 }
 
 // One block per right-hand side: sum the partials (fixed order), update the scalars.

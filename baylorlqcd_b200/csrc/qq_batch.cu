@@ -6,7 +6,7 @@
 //   2. optionally (deflate = 1) mixed-precision GMRES-DR(m, k) on the first source
 //      to tolerance defl_tol builds an FP32 deflation space (k harmonic-Ritz vectors);
 //   3. the right-hand sides are solved together, in blocks of rhs_block, by BiCGStab
-//      on RHS-interleaved block fields in FP64, FP32 or FP16 with FP64 reliable
+//      on RHS-interleaved block fields in FP64, FP32, FP16 or BF16 with FP64 reliable
 //      updates: whenever the iterated residual has dropped by `delta` since the last
 //      update, the FP64 solution is updated and the FP64 true residual replaces the
 //      low-precision one (projected onto the deflation space when there is one);
@@ -27,7 +27,7 @@ namespace {
 // Workspace ids of the batched solver in the context (qq_ctx::ws).  Solves of the
 // same size reuse the buffers, so a repeated qq_fermprop_batch allocates nothing.
 enum WsId : int {
-  WS_BLOCK = 0,  // + 2 f: data of block field f (7 fields), + 2 f + 1: its FP16 norms
+  WS_BLOCK = 0,  // + 2 f: data of block field f (7 fields), + 2 f + 1: its 16-bit norms
   WS_SCAL = 20,  // scalars and control words
   WS_PART,       // reduction partials
   WS_DSLOTS,     // scalar slot of each right-hand side
@@ -49,7 +49,7 @@ int ws_field(qq_ctx* c, WsField& f, int id, int prec, int nsites_mult = 1) {
   f.bytes = field_bytes(prec, c->g.vh) * nsites_mult;
   QQ_CK(ws_get(c, id, f.bytes, &d));
   f.norm_bytes = 0;
-  if (prec == P16) {
+  if (has_norm(prec)) {
     f.norm_bytes = sizeof(float) * c->g.vh * nsites_mult;
     QQ_CK(ws_get(c, id + 1, f.norm_bytes, &n));
   }
@@ -62,7 +62,7 @@ int block_fields(qq_ctx* c, int prec, int nb, WsField* const* fs) {
   for (int i = 0; i < 7; ++i) {
     QQ_TRY(ws_field(c, *fs[i], WS_BLOCK + 2 * i, prec, nb));
     QQ_CK(cudaMemsetAsync(fs[i]->s.data, 0, fs[i]->bytes, c->st));
-    if (prec == P16) QQ_CK(cudaMemsetAsync(fs[i]->s.norm, 0, fs[i]->norm_bytes, c->st));
+    if (has_norm(prec)) QQ_CK(cudaMemsetAsync(fs[i]->s.norm, 0, fs[i]->norm_bytes, c->st));
   }
   return QQ_OK;
 }
@@ -104,6 +104,8 @@ int block_op(qq_ctx* c, int prec, const BlockBiArgs& A, int op, const int* dslot
     QQ_TRY(launch_block_op<P32>(c, A, op));
   else if (prec == P16)
     QQ_TRY(launch_block_op<P16>(c, A, op));
+  else if (prec == PB16)
+    QQ_TRY(launch_block_op<PB16>(c, A, op));
   else
     QQ_TRY(launch_block_op<P64>(c, A, op));
   if (step >= 0) {
@@ -152,6 +154,8 @@ int block_slot(qq_ctx* c, int prec, int nb, int k, Spinor blockf, Spinor x, int 
     block_slot_kernel<P32><<<kRedBlocks, kRedThreads, 0, c->st>>>(c->g.vh, nb, k, blockf, x, mode, pred);
   else if (prec == P16)
     block_slot_kernel<P16><<<kRedBlocks, kRedThreads, 0, c->st>>>(c->g.vh, nb, k, blockf, x, mode, pred);
+  else if (prec == PB16)
+    block_slot_kernel<PB16><<<kRedBlocks, kRedThreads, 0, c->st>>>(c->g.vh, nb, k, blockf, x, mode, pred);
   else
     block_slot_kernel<P64><<<kRedBlocks, kRedThreads, 0, c->st>>>(c->g.vh, nb, k, blockf, x, mode, pred);
   QQ_CK(cudaGetLastError());
@@ -184,6 +188,8 @@ int reinsert_rho(qq_ctx* c, int prec, const BlockBiArgs& A, int k, const int* ds
     slot_dot_kernel<P32><<<kRedBlocks, kRedThreads, 0, c->st>>>(A.vh, A.nb, k, A.rhat, A.r, pred, A.partial);
   else if (prec == P16)
     slot_dot_kernel<P16><<<kRedBlocks, kRedThreads, 0, c->st>>>(A.vh, A.nb, k, A.rhat, A.r, pred, A.partial);
+  else if (prec == PB16)
+    slot_dot_kernel<PB16><<<kRedBlocks, kRedThreads, 0, c->st>>>(A.vh, A.nb, k, A.rhat, A.r, pred, A.partial);
   else
     slot_dot_kernel<P64><<<kRedBlocks, kRedThreads, 0, c->st>>>(A.vh, A.nb, k, A.rhat, A.r, pred, A.partial);
   QQ_CK(cudaGetLastError());
@@ -741,8 +747,8 @@ int bicgstab_block(qq_ctx* c, std::vector<PerRhs*>& rhs, int prec, double tol, d
 
 int batch_solve(qq_ctx* c, int nrhs, const double* be, const double* bo, const double kappa[2],
                 const qq_method* meth, double* xe, double* xo, qq_solve_info* infos) {
-  const int prec = meth->precision == 64 ? P64 : meth->precision == 32 ? P32 : meth->precision == 16 ? P16 : -1;
-  if (prec < 0) return set_error(QQ_BAD_ARG, "precision must be 64, 32 or 16");
+  const int prec = prec_of_code(meth->precision);
+  if (prec < 0) return set_error(QQ_BAD_ARG, "precision must be 64, 32, 16 or -16 (BF16)");
   if (meth->solver != 0 && meth->solver != 1) return set_error(QQ_BAD_ARG, "solver must be 0 or 1");
   if (meth->m < 2 || meth->k < 1 || meth->k >= meth->m || meth->m > 127)
     return set_error(QQ_BAD_ARG, "GMRES(m,k) out of range");
@@ -916,7 +922,7 @@ int batch_solve(qq_ctx* c, int nrhs, const double* be, const double* bo, const d
 // The uneven batch runs this for each context on the calling thread before its worker
 // threads start, so no candidate is timed while other contexts' solves share the GPU.
 int tune_batch_shapes(qq_ctx* c, int nrhs, const double kappa[2], const qq_method* meth) {
-  const int prec = meth->precision == 64 ? P64 : meth->precision == 32 ? P32 : meth->precision == 16 ? P16 : -1;
+  const int prec = prec_of_code(meth->precision);
   if (prec < 0 || nrhs < 1) return set_error(QQ_BAD_ARG, "bad method or nrhs");
   Tmp a64(c, P64), b64(c, P64), t64(c, P64);
   QQ_TRY(zero_field(c, a64.sp()));
@@ -932,7 +938,7 @@ int tune_batch_shapes(qq_ctx* c, int nrhs, const double kappa[2], const qq_metho
       for (int i = 0; i < 3; ++i) {
         QQ_TRY(ws_field(c, *fs[i], WS_BLOCK + 2 * i, prec, nb));
         QQ_CK(cudaMemsetAsync(fs[i]->s.data, 0, fs[i]->bytes, c->st));
-        if (prec == P16) QQ_CK(cudaMemsetAsync(fs[i]->s.norm, 0, fs[i]->norm_bytes, c->st));
+        if (has_norm(prec)) QQ_CK(cudaMemsetAsync(fs[i]->s.norm, 0, fs[i]->norm_bytes, c->st));
       }
       QQ_TRY(op_dbletm_block(c, out.sp(), in.sp(), tmp.sp(), nb, 0, kappa));
     }
@@ -952,7 +958,7 @@ int hsingle_block(qq_ctx* c, int prec, int nrhs, int shape, double* gout, const 
   in.prec = out.prec = prec;
   QQ_CK(in.data.alloc(field_bytes(prec, vh) * nrhs));
   QQ_CK(out.data.alloc(field_bytes(prec, vh) * nrhs));
-  if (prec == P16) {
+  if (has_norm(prec)) {
     QQ_CK(in.norm.alloc(sizeof(float) * vh * nrhs));
     QQ_CK(out.norm.alloc(sizeof(float) * vh * nrhs));
   }

@@ -109,7 +109,7 @@ __global__ void __launch_bounds__(kRedThreads) lincomb_kernel(LinArgs L) {
     if (L.red >= 1) {
       // reduce on the stored (rounded) values for FP16 consistency
       cplx<RO> q[12];
-      if (PO == P16)
+      if (has_norm(PO))
         SpinorIO<PO>::load(L.out.data, L.out.norm, L.vh, s, q);
       else
         for (int k = 0; k < 12; ++k) q[k] = o[k];

@@ -527,8 +527,8 @@ extern "C" int qq_hsingle_block(qq_ctx* c, int precision, int nrhs, int shape, d
   QQ_TRY(check_ctx(c));
   QQ_TRY(set_device(c));
   if (!c->have_gauge) return set_error(QQ_BAD_ARG, "no gauge field uploaded");
-  const int prec = precision == 32 ? P32 : precision == 16 ? P16 : -1;
-  if (prec < 0) return set_error(QQ_BAD_ARG, "precision must be 32 or 16");
+  const int prec = precision == 32 ? P32 : precision == 16 ? P16 : precision == -16 ? PB16 : -1;
+  if (prec < 0) return set_error(QQ_BAD_ARG, "precision must be 32, 16 or -16 (BF16)");
   if (nrhs < 1 || nrhs > kMaxBatch) return set_error(QQ_BAD_ARG, "nrhs must be 1..32");
   if (shape < 0 || shape > kShapeMax) return set_error(QQ_BAD_ARG, "bad kernel shape");
   if (gblclr != 1 && gblclr != 2) return set_error(QQ_BAD_ARG, "gblclr must be 1 or 2");
@@ -540,7 +540,7 @@ extern "C" int qq_hsingle_block(qq_ctx* c, int precision, int nrhs, int shape, d
 extern "C" int qq_hop_tuned_shape(qq_ctx* c, int precision, int nrhs, int* shape) {
   QQ_TRY(check_ctx(c));
   if (!shape) return set_error(QQ_BAD_ARG, "null argument");
-  const int prec = precision == 64 ? P64 : precision == 32 ? P32 : precision == 16 ? P16 : -1;
+  const int prec = prec_of_code(precision);
   if (prec < 0 || nrhs < 1 || nrhs > kMaxBatch) return set_error(QQ_BAD_ARG, "bad precision or nrhs");
   HopArgs a;
   std::memset(&a, 0, sizeof(a));
@@ -561,7 +561,7 @@ extern "C" int qq_bench_hsingle(qq_ctx* c, int precision, int nrhs, int tps, int
   QQ_TRY(check_ctx(c));
   QQ_TRY(set_device(c));
   if (!c->have_gauge) return set_error(QQ_BAD_ARG, "no gauge field uploaded");
-  const int prec = precision == 64 ? P64 : precision == 32 ? P32 : precision == 16 ? P16 : -1;
+  const int prec = prec_of_code(precision);
   if (prec < 0 || nrhs < 1 || nrhs > kMaxBatch || niter < 1 || tps < 0 || tps > kShapeMax)
     return set_error(QQ_BAD_ARG, "bad benchmark arguments");
   const int vh = c->g.vh;
@@ -571,7 +571,7 @@ extern "C" int qq_bench_hsingle(qq_ctx* c, int precision, int nrhs, int tps, int
   in.prec = out.prec = prec;
   QQ_CK(in.data.alloc(field_bytes(prec, vh) * nrhs));
   QQ_CK(out.data.alloc(field_bytes(prec, vh) * nrhs));
-  if (prec == P16) {
+  if (has_norm(prec)) {
     QQ_CK(in.norm.alloc(sizeof(float) * vh * nrhs));
     QQ_CK(out.norm.alloc(sizeof(float) * vh * nrhs));
   }
@@ -625,7 +625,7 @@ extern "C" int qq_bench_hsingle(qq_ctx* c, int precision, int nrhs, int tps, int
     total += ms;
   }
   const double link_bytes = prec == P64 ? (recon == 18 ? 144.0 : 96.0) : 48.0;
-  const double spinor_bytes = prec == P64 ? 192.0 : prec == P32 ? 96.0 : 52.0;
+  const double spinor_bytes = prec == P64 ? 192.0 : prec == P32 ? 96.0 : 52.0;  // 16-bit: + the norm
   if (ms_per_call) *ms_per_call = total / niter;
   if (bytes_per_call) *bytes_per_call = (double)vh * (8.0 * link_bytes + nrhs * 2.0 * spinor_bytes);
   return QQ_OK;
@@ -693,8 +693,8 @@ extern "C" int qq_profile_hop_select(qq_ctx* c, int precision, int nrhs, long lo
   long long n = 0;
   double ms = 0.0, by = 0.0, fl = 0.0;
   for (size_t i = 0; i < c->prof_used; ++i) {
-    const int p = c->prof_shape[i] / 1000, r = c->prof_shape[i] % 1000;
-    if ((precision && p != precision) || (nrhs && r != nrhs)) continue;
+    const int p = c->prof_shape[i] / 1000, r = c->prof_shape[i] % 1000;  // storage enum, RHS
+    if ((precision && p != prec_of_code(precision)) || (nrhs && r != nrhs)) continue;
     float t = 0.f;
     QQ_CK(cudaEventElapsedTime(&t, c->prof_events[i].first, c->prof_events[i].second));
     ++n;

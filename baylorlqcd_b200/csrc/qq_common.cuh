@@ -6,12 +6,14 @@
 //   * a Dirac half-vector is 12 complex components (spin-major, colour-minor) per site,
 //     stored component-major in 16-byte vectors ("planes"): plane q, site s at
 //     [q*Vh + s].  FP64: 12 planes of double2.  FP32: 6 planes of float4 (two
-//     complex per vector).  FP16: 3 planes of 8 halves + one float norm per site;
+//     complex per vector).  FP16 and BF16: 3 planes of 8 16-bit values + one float norm
+//     per site;
 //   * a gauge field stores, for each parity p and direction mu, the link U_mu(x) of
 //     every site x of parity p, component-major as well: recon-18 (9 complex) or
 //     recon-12 (first two rows, 6 complex; row 3 = conj(row1 x row2)).
 // A warp therefore reads 32 consecutive 16-byte vectors per plane: fully coalesced.
 #pragma once
+#include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -137,9 +139,18 @@ __host__ __device__ inline cplx<R> cconj(cplx<R> a) {
 }
 
 // ---------------- storage precisions ----------------
-enum Prec : int { P64 = 0, P32 = 1, P16 = 2 };
+enum Prec : int { P64 = 0, P32 = 1, P16 = 2, PB16 = 3 };
 
-// A Dirac half-vector in GPU layout.  For P16 `norm` holds one float per site.
+// The 16-bit storages (FP16, BF16) keep one FP32 scale per site beside the planes.
+__host__ __device__ constexpr bool has_norm(int p) { return p == P16 || p == PB16; }
+
+// Storage precision of a method's `precision` code: 64, 32, 16 (FP16) or -16 (BF16);
+// -1 for anything else.
+inline int prec_of_code(int code) {
+  return code == 64 ? P64 : code == 32 ? P32 : code == 16 ? P16 : code == -16 ? PB16 : -1;
+}
+
+// A Dirac half-vector in GPU layout.  For P16 and PB16 `norm` holds one float per site.
 struct Spinor {
   void* data;
   float* norm;

@@ -107,7 +107,7 @@ struct qq_ctx {
   bool prof_hop = false;                             // per-launch hop timing
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_events;
   std::vector<double> prof_bytes;
-  std::vector<int> prof_shape;                       // per profiled launch: precision * 1000 + nrhs
+  std::vector<int> prof_shape;                       // per profiled launch: Prec * 1000 + nrhs
   size_t prof_used = 0;
   std::vector<std::unique_ptr<qq::Field>> pool[3];  // temporaries per precision
   std::vector<bool> pool_busy[3];

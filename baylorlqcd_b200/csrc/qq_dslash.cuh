@@ -469,6 +469,23 @@ struct SlotSpinor<P16> {
   }
 };
 
+template <>
+struct SlotSpinor<PB16> {  // as SlotSpinor<P16>, bfloat16 values
+  __device__ static inline void load(const uint4* slot, int T, cplx<float>* v) {
+    const float nrm = *reinterpret_cast<const float*>(slot + 3 * T);
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      const uint4 t = slot[q * T];
+      const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&t);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const float2 f = __bfloat1622float2(h[k]);
+        v[4 * q + k] = {f.x * nrm, f.y * nrm};
+      }
+    }
+  }
+};
+
 template <int LP, int RECON>
 __device__ inline void slot_link(const uint4* slot, int T, Su3<typename LinkIO<LP, RECON>::R>& u) {
   if (LP == P64) {
@@ -514,7 +531,7 @@ __device__ inline int neighbour(const Geom& g, const int* x, int* sgn) {
 
 template <int SP, int LP, int RECON>
 struct StageShape {
-  static constexpr int SQ = SpinorIO<SP>::planes + (SP == P16 ? 1 : 0);  // + norm slot
+  static constexpr int SQ = SpinorIO<SP>::planes + (has_norm(SP) ? 1 : 0);  // + norm slot
   static constexpr int LQ = LinkIO<LP, RECON>::planes;
   static constexpr int NQ = SQ + LQ;
 };
@@ -532,7 +549,7 @@ __device__ inline void stage_hop(const HopArgs& a, uint4* slots, int T, int s, i
   const int vhe = a.vh_of(), iy = a.idx_of(sy, r);
 #pragma unroll
   for (int q = 0; q < SpinorIO<SP>::planes; ++q) cp_async16(dst + q * T, sp + (size_t)q * vhe + iy);
-  if (SP == P16) cp_async4(dst + SpinorIO<SP>::planes * T, a.in_nrm(r) + iy);
+  if (has_norm(SP)) cp_async4(dst + SpinorIO<SP>::planes * T, a.in_nrm(r) + iy);
   const int lp = FWD ? a.pout : 1 - a.pout;
   const int ls = FWD ? s : sy;
   const uint4* lk = static_cast<const uint4*>(a.gauge) + (size_t)(lp * 4 + MU) * Sh::LQ * a.g.vh;

@@ -107,6 +107,48 @@ struct SpinorIO<P16> {
   }
 };
 
+// BF16 storage with one FP32 scale per site, FP32 arithmetic: the layout of SpinorIO<P16>
+// with bfloat16 values (8 exponent bits, 8 significant bits).
+template <>
+struct SpinorIO<PB16> {
+  using R = float;
+  static constexpr int planes = 3;
+  static constexpr size_t bytes_per_site = 52;
+  __device__ static inline void load(const void* base, const float* norm, int vh, int s,
+                                     cplx<R>* v) {
+    const int4* f = static_cast<const int4*>(base);
+    const float nrm = __ldg(norm + s);
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      int4 t = __ldg(f + (size_t)q * vh + s);
+      const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&t);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        float2 ff = __bfloat1622float2(h[k]);
+        v[4 * q + k] = {ff.x * nrm, ff.y * nrm};
+      }
+    }
+  }
+  __device__ static inline void store(void* base, float* norm, int vh, int s,
+                                      const cplx<R>* v) {
+    float m = 0.f;
+#pragma unroll
+    for (int c = 0; c < 12; ++c) m = fmaxf(m, fmaxf(fabsf(v[c].re), fabsf(v[c].im)));
+    const float inv = m > 0.f ? 1.f / m : 0.f;
+    int4* f = static_cast<int4*>(base);
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      int4 t;
+      __nv_bfloat162* h = reinterpret_cast<__nv_bfloat162*>(&t);
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+        h[k] = __floats2bfloat162_rn(v[4 * q + k].re * inv, v[4 * q + k].im * inv);
+      f[(size_t)q * vh + s] = t;
+    }
+    norm[s] = m;
+  }
+};
+
 // ---------------------------------------------------------------------------
 // Links.  Storage: per parity p and direction mu, `planes` 16-byte vectors per site,
 // indexed [((p*4 + mu)*planes + q)*vh + s].

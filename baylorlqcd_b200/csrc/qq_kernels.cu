@@ -249,6 +249,7 @@ cudaError_t launch_hop(const HopArgs& a, int sp, int recon, int epi, int tps, cu
     if (!a.blk || rpt < 2 || a.nrhs % rpt != 0) return cudaErrorInvalidValue;
     if (sp == P32) return hop_mrhs<P32, P32, 12>(a, epi, rpt, st);
     if (sp == P16) return hop_mrhs<P16, P32, 12>(a, epi, rpt, st);
+    if (sp == PB16) return hop_mrhs<PB16, P32, 12>(a, epi, rpt, st);
     return cudaErrorInvalidValue;
   }
   const int per = tps <= 4 ? 128 / tps : tps;
@@ -260,6 +261,7 @@ cudaError_t launch_hop(const HopArgs& a, int sp, int recon, int epi, int tps, cu
   }
   if (sp == P32) return hop_tps<P32, P32, 12>(a, epi, tps, st);
   if (sp == P16) return hop_tps<P16, P32, 12>(a, epi, tps, st);
+  if (sp == PB16) return hop_tps<PB16, P32, 12>(a, epi, tps, st);
   return cudaErrorInvalidValue;
 }
 
@@ -284,17 +286,22 @@ cudaError_t launch_lincomb(const LinArgs& L, int px, int py, int pz, int po, cud
     if (po == P64) return lin4<P64, P64, P64, P64>(L, st);
     if (po == P32) return lin4<P32, P32, P32, P32>(L, st);
     if (po == P16) return lin4<P16, P16, P16, P16>(L, st);
+    if (po == PB16) return lin4<PB16, PB16, PB16, PB16>(L, st);
   }
   if (po == P64 && py == P64 && pz == P64) {
     if (px == P32) return lin4<P32, P64, P64, P64>(L, st);
     if (px == P16) return lin4<P16, P64, P64, P64>(L, st);
+    if (px == PB16) return lin4<PB16, P64, P64, P64>(L, st);
   }
   if (px == P64 && py == po && pz == po) {
     if (po == P32) return lin4<P64, P32, P32, P32>(L, st);
     if (po == P16) return lin4<P64, P16, P16, P16>(L, st);
+    if (po == PB16) return lin4<P64, PB16, PB16, PB16>(L, st);
   }
   if (po == P16 && px == P32 && py == P16 && pz == P16) return lin4<P32, P16, P16, P16>(L, st);
   if (po == P32 && px == P16 && py == P32 && pz == P32) return lin4<P16, P32, P32, P32>(L, st);
+  if (po == PB16 && px == P32 && py == PB16 && pz == PB16) return lin4<P32, PB16, PB16, PB16>(L, st);
+  if (po == P32 && px == PB16 && py == P32 && pz == P32) return lin4<PB16, P32, P32, P32>(L, st);
   return cudaErrorInvalidValue;
 }
 
@@ -306,6 +313,8 @@ cudaError_t launch_dot(int vh, Spinor x, Spinor y, double* partial, cudaStream_t
     dot_kernel<P32, P32><<<kRedBlocks, kRedThreads, 0, st>>>(vh, x, y, partial);
   else if (x.prec == P16 && y.prec == P16)
     dot_kernel<P16, P16><<<kRedBlocks, kRedThreads, 0, st>>>(vh, x, y, partial);
+  else if (x.prec == PB16 && y.prec == PB16)
+    dot_kernel<PB16, PB16><<<kRedBlocks, kRedThreads, 0, st>>>(vh, x, y, partial);
   else if (x.prec == P64 && y.prec == P32)
     dot_kernel<P64, P32><<<kRedBlocks, kRedThreads, 0, st>>>(vh, x, y, partial);
   else if (x.prec == P32 && y.prec == P64)
@@ -458,8 +467,10 @@ cudaError_t launch_spinor_from_ref(const Geom& g, const RefDims& d, int p, const
     spinor_from_ref_kernel<P64><<<grd, blk, 0, st>>>(g, d, p, ref, out);
   else if (out.prec == P32)
     spinor_from_ref_kernel<P32><<<grd, blk, 0, st>>>(g, d, p, ref, out);
-  else
+  else if (out.prec == P16)
     spinor_from_ref_kernel<P16><<<grd, blk, 0, st>>>(g, d, p, ref, out);
+  else
+    spinor_from_ref_kernel<PB16><<<grd, blk, 0, st>>>(g, d, p, ref, out);
   return cudaGetLastError();
 }
 
@@ -471,8 +482,10 @@ cudaError_t launch_spinor_to_ref(const Geom& g, const RefDims& d, int p, Spinor 
     spinor_to_ref_kernel<P64><<<grd, blk, 0, st>>>(g, d, p, in, ref);
   else if (in.prec == P32)
     spinor_to_ref_kernel<P32><<<grd, blk, 0, st>>>(g, d, p, in, ref);
-  else
+  else if (in.prec == P16)
     spinor_to_ref_kernel<P16><<<grd, blk, 0, st>>>(g, d, p, in, ref);
+  else
+    spinor_to_ref_kernel<PB16><<<grd, blk, 0, st>>>(g, d, p, in, ref);
   return cudaGetLastError();
 }
 
@@ -542,8 +555,10 @@ cudaError_t launch_spinmix(int vh, Spinor x, Spinor y, Spinor out, double a, dou
     spinmix_kernel<P64><<<kRedBlocks, kRedThreads, 0, st>>>(vh, x, y, out, a, ta, b, tb);
   else if (prec == P32)
     spinmix_kernel<P32><<<kRedBlocks, kRedThreads, 0, st>>>(vh, x, y, out, a, ta, b, tb);
-  else
+  else if (prec == P16)
     spinmix_kernel<P16><<<kRedBlocks, kRedThreads, 0, st>>>(vh, x, y, out, a, ta, b, tb);
+  else
+    spinmix_kernel<PB16><<<kRedBlocks, kRedThreads, 0, st>>>(vh, x, y, out, a, ta, b, tb);
   return cudaGetLastError();
 }
 

@@ -17,8 +17,8 @@ struct LinArgs;
 struct BasisArgs;
 struct Coef;
 
-// Dirac hopping term.  sp: spinor precision (P64/P32/P16); recon: 18 or 12 (P64
-// links) -- P32/P16 spinors always use the FP32 recon-12 links; epi: Epilogue;
+// Dirac hopping term.  sp: spinor precision (P64/P32/P16/PB16); recon: 18 or 12 (P64
+// links) -- P32 and 16-bit spinors always use the FP32 recon-12 links; epi: Epilogue;
 // tps: threads per site (direction groups: 1, 2 or 4).
 cudaError_t launch_hop(const HopArgs& a, int sp, int recon, int epi, int tps, cudaStream_t st);
 

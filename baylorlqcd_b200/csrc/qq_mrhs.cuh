@@ -160,7 +160,7 @@ __global__ void __launch_bounds__(kRedThreads) bicg_block_kernel(BlockBiArgs A) 
 #pragma unroll
         for (int q = 0; q < 12; ++q) c[q] = csub(c[q], cmuld(omega, b[q]));
         IO::store(A.r.data, A.r.norm, n, s, c);
-        if (P == P16) IO::load(A.r.data, A.r.norm, n, s, c);  // reduce what was stored
+        if (has_norm(P)) IO::load(A.r.data, A.r.norm, n, s, c);  // reduce what was stored
       }
       // ||r||^2 and, fused, the next iteration's rho' = <rhat, r>
 #pragma unroll

@@ -37,7 +37,7 @@ Tmp::Tmp(qq_ctx* c_, int prec_) : c(c_), prec(prec_), idx(-1), f(nullptr) {
       f = nullptr;
       return;
     }
-    if (prec == P16) nf->norm.alloc(sizeof(float) * c->g.vh);
+    if (has_norm(prec)) nf->norm.alloc(sizeof(float) * c->g.vh);
   }
   busy[idx] = true;
   f = pool[idx].get();
@@ -136,7 +136,7 @@ static int launch_hop_profiled(qq_ctx* c, const HopArgs& a, int prec, int recon,
   }
   auto& ev = c->prof_events[c->prof_used];
   c->prof_bytes[c->prof_used] = hop_bytes(c, prec, a.nrhs, epi);
-  c->prof_shape[c->prof_used] = (prec == P64 ? 64 : prec == P32 ? 32 : 16) * 1000 + a.nrhs;
+  c->prof_shape[c->prof_used] = prec * 1000 + a.nrhs;
   ++c->prof_used;
   QQ_CK(cudaEventRecord(ev.first, c->st));
   QQ_CK(launch_hop(a, prec, recon, epi, tps, c->st));
@@ -458,7 +458,7 @@ int copy_field(qq_ctx* c, Spinor out, Spinor in) { return lin(c, out, cimm(1.0),
 
 int zero_field(qq_ctx* c, Spinor f) {
   QQ_CK(cudaMemsetAsync(f.data, 0, field_bytes(f.prec, c->g.vh), c->st));
-  if (f.prec == P16 && f.norm) QQ_CK(cudaMemsetAsync(f.norm, 0, sizeof(float) * c->g.vh, c->st));
+  if (has_norm(f.prec) && f.norm) QQ_CK(cudaMemsetAsync(f.norm, 0, sizeof(float) * c->g.vh, c->st));
   return QQ_OK;
 }
 

@@ -92,7 +92,8 @@ def parse(argv=None):
     p.add_argument("--kappa", type=float, default=0.1566)
     p.add_argument("--mu", type=float, default=0.0025, help="twisted mass (0: Wilson)")
     p.add_argument("--nrhs", type=int, default=12)
-    p.add_argument("--precision", type=int, default=32, choices=[16, 32, 64])
+    p.add_argument("--precision", type=int, default=32, choices=[-16, 16, 32, 64],
+                   help="inner solver storage: 64, 32, 16 (FP16) or -16 (BF16)")
     p.add_argument("--rhs-block", type=int, default=12)
     p.add_argument("--deflate", action="store_true",
                    help="project onto GMRES-DR eigenvectors at every reliable update")
@@ -409,7 +410,7 @@ def run_ours(a, rank, world, local):
         "higher_is_better": False,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": {16: "fp16/fp64", 32: "fp32/fp64", 64: "fp64"}[a.precision],
+        "dtype": {-16: "bf16/fp64", 16: "fp16/fp64", 32: "fp32/fp64", 64: "fp64"}[a.precision],
         "data": "synthetic: GPU heatbath configuration (beta=6.0, cold start, %d sweeps), point sources" % a.sweeps,
         "config": {"workload": "%s %s kappa=%.4f, %d point sources, batched FP%d BiCGStab with FP64 "
                                "reliable updates%s, tol %.0e full-lattice FP64; plain = FP64 GMRES-DR(%d,%d)"

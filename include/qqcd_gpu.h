@@ -200,7 +200,9 @@ int qq_pointsource(qq_ctx* ctx, double* be, double* bo, const int src[4], int ic
  * reference-layout halves each, packed one after the other. */
 typedef struct qq_method {
   int m, k;          /* GMRES-DR(m, k) */
-  int precision;     /* BiCGStab arithmetic: 64, 32 or 16 (FP64 reliable updates) */
+  int precision;     /* BiCGStab storage: 64, 32, 16 (FP16) or -16 (BF16); the 16-bit
+                        storages keep one FP32 scale per site and compute in FP32; FP64
+                        reliable updates in every case */
   int rhs_block;     /* right-hand sides solved together (1..32) */
   double tol;        /* FP64 true full-lattice relative residual target */
   int max_outer;     /* iteration limit in thousands (0: none) */
@@ -359,7 +361,7 @@ int qq_profile_hop_select(qq_ctx* ctx, int precision, int nrhs, long long* launc
 
 /* Times `niter` launches of the hopping kernel alone (H_oe of random fields, output
  * parity gblclr = 2) with CUDA events on the library's stream.  precision: 64
- * (links at the uploaded recon), 32 or 16 (FP32 recon-12 links); nrhs right-hand
+ * (links at the uploaded recon), 32, 16 or -16 (BF16) (FP32 recon-12 links); nrhs right-hand
  * sides per launch (1..32; for nrhs > 1 one RHS-interleaved block field, the layout
  * of the batched solver); tps: kernel shape (0 = the autotuned choice the solvers
  * use; 1, 2, 4 direction groups per site; 32-128 threads per block of the staged
@@ -462,7 +464,7 @@ int qq_hop_tuned_shape(qq_ctx* ctx, int precision, int nrhs, int* shape);
 /* The hopping term of qq_hsingle (Hsingle, Q/diracops.f90:554-599) on nrhs half-lattice fields
  * at once, computed in reduced precision the way the batched solver applies it: gin
  * holds nrhs reference-layout input vectors back to back (parity opposite to gblclr),
- * converted to one RHS-interleaved block field of precision 32 or 16 (a plain field for
+ * converted to one RHS-interleaved block field of precision 32, 16 or -16 (BF16) (a plain field for
  * nrhs = 1), multiplied by kernel shape `shape` (the codes of qq_bench_hsingle; 0 = the
  * autotuned choice) with FP32 recon-12 links, and written to gout as nrhs FP64
  * reference-layout vectors.  QQ_BAD_ARG when the shape does not support this precision

@@ -134,7 +134,8 @@ def test_heatbath_plaquette(setup):
                                                       (301, 32, 0), (302, 32, 0), (303, 32, 0), (301, 32, 1),
                                                       (304, 32, 0), (304, 32, 1), (305, 32, 0),
                                                       (306, 32, 0), (307, 32, 0), (307, 32, 1), (308, 32, 0),
-                                                      (309, 32, 0), (310, 32, 1), (311, 32, 0)])
+                                                      (309, 32, 0), (310, 32, 1), (311, 32, 0),
+                                                      (1, -16, 0), (202, -16, 0), (204, -16, 0)])
 def test_block_kernel_shapes(setup, monkeypatch, shape, precision, deflate):
     """Each hopping-kernel shape, forced for the whole solve where the launch supports
     it: one RHS per thread; 2, 3 or 4 RHS per thread sharing links and neighbour

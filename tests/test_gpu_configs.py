@@ -8,7 +8,7 @@ count within one, the per-cycle gmresdr-norm history within 10%, the ten harmoni
 values of the last restart to 1e-6, and the solution to 1e-7 of the oracle's.
 
 C2 (error against the FP64 solve, per precision): on a heatbath configuration near
-critical kappa, the batched FP32 and FP16 solves are compared with the solution of the
+critical kappa, the batched FP32, FP16 and BF16 solves are compared with the solution of the
 reference's plain FP64 GMRES-DR: ||x_P - x_64|| / ||x_64|| must stay within 1e-7 at
 C1's kappa and 1e-6 at C2's near-critical kappa (every solve stops at an FP64 true
 residual of 1e-10; the operator's condition number sets how much solution error that
@@ -102,7 +102,7 @@ def test_kat6_c1_batched_methods(c1):
                                          tol=1e-11, solver=0)
     assert all(i.status == 0 for i in i64)
     nv = lat.nvhalf
-    for prec in (32, 16):
+    for prec in (32, 16, -16):
         xe, xo, infos = lat.fermprop_batch(be, bo, tuple(rec["kappa"]), m=30, k=10, precision=prec, rhs_block=4,
                                            tol=1e-10, solver=1, deflate=0)
         for i in range(4):
@@ -130,7 +130,7 @@ def test_c2_error_against_fp64_per_precision():
     assert all(i.status == 0 for i in i64)
     nv = lat.nvhalf
     errs = {}
-    for prec in (32, 16):
+    for prec in (32, 16, -16):
         xe, xo, infos = lat.fermprop_batch(be, bo, kappa, m=60, k=20, precision=prec, rhs_block=12, tol=1e-10,
                                            solver=1, deflate=0)
         assert all(i.status == 0 and i.true_rel <= 1e-10 for i in infos), prec

@@ -1,11 +1,13 @@
 """GPU parity of every hopping-kernel shape against the oracle's FP64 Hsingle
 (Q/diracops.f90:554-599), through qq_hsingle_block: nrhs half vectors converted to one
-RHS-interleaved block field in FP32 or FP16, multiplied by the forced kernel shape with
-FP32 recon-12 links, and returned in FP64.
+RHS-interleaved block field in FP32, FP16 or BF16, multiplied by the forced kernel shape
+with FP32 recon-12 links, and returned in FP64.
 
 Tolerances (max-abs error over max-abs value, interior sites): 5e-6 for FP32 (inputs,
-links and accumulation rounded to 24-bit mantissas, eight terms per site) and 2e-3 for
-FP16 (16-bit fixed point against a per-site FP32 norm).
+links and accumulation rounded to 24-bit mantissas, eight terms per site), 2e-3 for
+FP16 (11 significant bits against a per-site FP32 norm) and 1.5e-2 for BF16 (8
+significant bits against the same norm; its rounding 2^-9 of the largest component,
+summed over the eight hops, with FP32 arithmetic).
 
 The lattice 8x4x8x12 has V/2 = 1536 sites, so 5 right-hand sides (25 sites per block)
 leave the last block partly empty, and 12 or 24 fill blocks of 8 or 16 sites exactly."""
@@ -25,6 +27,7 @@ FP32_24 = [0, 306, 307, 308, 309, 310, 311]
 FP32_1 = [1, 2, 4, 32, 128, 301, 304, 306, 307, 308, 309, 310, 311]
 FP32_5 = [1, 301, 304, 306, 307, 308, 309, 310, 311]
 FP16_12 = [1, 2, 64, 202, 203, 204]
+BF16_12 = [1, 2, 64, 202, 203, 204]
 
 
 @pytest.fixture(scope="module")
@@ -74,6 +77,15 @@ def test_fp32_block5_ragged(pair, shape):
 @pytest.mark.parametrize("shape", FP16_12)
 def test_fp16_block12(pair, shape):
     check(*pair, 16, 12, shape, 0, 1, 2e-3)
+
+
+@pytest.mark.parametrize("shape", BF16_12)
+def test_bf16_block12(pair, shape):
+    check(*pair, -16, 12, shape, 1, 2, 1.5e-2)
+
+
+def test_bf16_single(pair):
+    check(*pair, -16, 1, 1, 0, 1, 1.5e-2)
 
 
 def test_unsupported_shape_is_an_error(pair):

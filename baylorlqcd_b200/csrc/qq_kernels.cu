@@ -199,7 +199,12 @@ template <int D, int RPT, int MINB = 4, int MB = 0>
 static cudaError_t hop_f2a(const HopArgs& a, int epi, cudaStream_t st) {
   if (a.nrhs % RPT != 0 || (RPT > 1 && !a.blk)) return cudaErrorInvalidValue;
   const int G = a.nrhs / RPT;  // threads per site
-  const int per_block = hop_sites_per_block(1, G);
+  int per_block = hop_sites_per_block(1, G);
+  // Pre-broadcast hop matrices (MB) take 1.2 KB of shared memory per site: with one
+  // thread per site, fewer sites per block (whole warps kept).
+  while (MB && f2a_smem_bytes(per_block, per_block * G, D, RPT, MB) > 200 * 1024 && per_block % 2 == 0 &&
+         (per_block / 2 * G) % 32 == 0)
+    per_block /= 2;
   const HopArgs b = hop_prepare(a, per_block, G);
   const size_t smem = f2a_smem_bytes(per_block, per_block * G, D, RPT, MB);
   if (smem > 227 * 1024) return cudaErrorInvalidValue;

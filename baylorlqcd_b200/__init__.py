@@ -40,6 +40,7 @@ EXPORTED = [
     "qq_hop_tuned_shape", "qq_net_create", "qq_net_destroy", "qq_net_nweights", "qq_net_get_weights",
     "qq_net_set_weights", "qq_net_apply", "qq_net_grad", "qq_net_train", "qq_fgmres", "qq_pionrho", "qq_twvev", "qq_twaverage", "qq_twistdiscon", "qq_average", "qq_momfacs",
     "qq_fgmresdr", "qq_fermprop_uneven",
+    "qq_eigmodes", "qq_eig_destroy", "qq_eig_info", "qq_eig_vector", "qq_xigenerator", "qq_eigaverage",
 ]
 
 
@@ -163,6 +164,12 @@ def load_library() -> C.CDLL:
         "qq_twvev": ([P, D, D, IP, I, I, I, I, I, P], I),
         "qq_average": ([P, P, P, P, P, D, I, I, I, P, P], I),
         "qq_momfacs": ([IP, IP, P], I),
+        "qq_eigmodes": ([P, I, IP, I, DP, P, P, C.POINTER(P), IP, DP], I),
+        "qq_eig_destroy": ([P], I),
+        "qq_eig_info": ([P, IP, IP, IP, IP, DP, DP], I),
+        "qq_eig_vector": ([P, I, I, P, P], I),
+        "qq_xigenerator": ([P, P, D, DP], I),
+        "qq_eigaverage": ([P, P, P, P, D, DP, I, I, P], I),
         "qq_twaverage": ([P, P, P, P, P, D, D, IP, I, I, I, I, I, P], I),
         "qq_twistdiscon": ([P, I, I, DP, P, D, IP, I, I, I, I, I, P, P, P], I),
         "qq_heatbath": ([P, D, I, C.c_ulonglong, P, DP], I),
@@ -234,6 +241,67 @@ class Deflation:
     def close(self):
         if self._h:
             self.lat.lib.qq_defl_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Eigenmodes:
+    """Kept eigenmodes of M (kind 1) or of M gamma5 (kind 2) on the device
+    (eigmodesofM / eigmodesofMprime, Q/disconloops.f90:1593-1937, 2573-2875)."""
+
+    def __init__(self, lat: "Lattice", kind: int, nGMRES, ncycles: int, kappa, se=None, so=None):
+        self.lat = lat
+        self.kind = int(kind)
+        self._h = C.c_void_p()
+        g = np.ascontiguousarray(nGMRES, dtype=np.int32)
+        k = np.ascontiguousarray(kappa, dtype=np.float64)
+        n = C.c_int(0)
+        ev = np.zeros(2 * int(nGMRES[1]))
+        _check(lat.lib.qq_eigmodes(lat._ctx, self.kind, g.ctypes.data_as(C.POINTER(C.c_int)), int(ncycles),
+                                   k.ctypes.data_as(C.POINTER(C.c_double)), _ptr(se) if se is not None else None,
+                                   _ptr(so) if so is not None else None, C.byref(self._h), C.byref(n),
+                                   ev.ctypes.data_as(C.POINTER(C.c_double))))
+        self.num = n.value
+        self.evals = ev[0:2 * self.num:2] + 1j * ev[1:2 * self.num:2]
+        cyc, mvp = C.c_int(0), C.c_int(0)
+        ritz = np.zeros(2 * int(nGMRES[1]))
+        _check(lat.lib.qq_eig_info(self._h, None, None, C.byref(cyc), C.byref(mvp), None,
+                                   ritz.ctypes.data_as(C.POINTER(C.c_double))))
+        self.cycles, self.mvp = cyc.value, mvp.value
+        self.ritz = ritz[0::2] + 1j * ritz[1::2]
+
+    def vector(self, j: int, left: bool = False):
+        """Mode j as (2,) + half_shape: the even and the odd reference-layout halves."""
+        out = np.zeros((2,) + self.lat.half_shape)
+        _check(self.lat.lib.qq_eig_vector(self._h, int(j), int(bool(left)), _ptr(out[0]), _ptr(out[1])))
+        return out
+
+    def xigenerator(self, kappa: float):
+        """xigenerator (Q/disconloops.f90:465-838): xiinv as complex (num, 6)."""
+        xi = np.zeros((max(self.num, 1), 6, 2))
+        _check(self.lat.lib.qq_xigenerator(self.lat._ctx, self._h, float(kappa),
+                                           xi.ctypes.data_as(C.POINTER(C.c_double))))
+        return (xi[..., 0] + 1j * xi[..., 1])[:self.num]
+
+    def eigaverage(self, ze, zo, kappa: float, scal, eigstart: int = 1, eigstep: int = 1):
+        """eigaverage (Q/disconloops.f90:3239-3342) at imom = 1: (9, num, nt, 2)."""
+        J = np.zeros((9, max(self.num, 1), self.lat.dims[3], 2))
+        s = np.zeros((max(self.num, 1), 2))
+        s[:self.num, 0] = np.real(scal)
+        s[:self.num, 1] = np.imag(scal)
+        _check(self.lat.lib.qq_eigaverage(self.lat._ctx, self._h, _ptr(ze), _ptr(zo), float(kappa),
+                                          s.ctypes.data_as(C.POINTER(C.c_double)), int(eigstart), int(eigstep),
+                                          _ptr(J)))
+        return J[:, :self.num]
+
+    def close(self):
+        if self._h:
+            self.lat.lib.qq_eig_destroy(self._h)
             self._h = C.c_void_p()
 
     def __del__(self):
@@ -406,6 +474,11 @@ class Lattice:
         _check(self.lib.qq_average(self._ctx, _ptr(be), _ptr(bo), _ptr(xe), _ptr(xo), float(kappa), int(nsub),
                                    int(nmom), int(nop), _ptr(mf) if mf is not None else None, _ptr(J)))
         return J
+
+    def eigenmodes(self, kind, nGMRES, ncycles, kappa, se=None, so=None) -> Eigenmodes:
+        """qq_eigmodes: kept eigenmodes of M (kind 1, from the unit source) or of M gamma5
+        (kind 2, from the start vector se, so)."""
+        return Eigenmodes(self, kind, nGMRES, ncycles, kappa, se, so)
 
     def twvev(self, kappa, delta=0.0, io=(1, 1, 1), dobndry=0, ir=1, nsub=6, nmom=5, nop=6):
         """twvev: the perturbative vacuum expectation values Jvev, as an array of shape

@@ -214,6 +214,27 @@ __global__ void diff_kernel(double* y, const double* x, const double* s, size_t 
 }
 
 }  // namespace
+
+// Loop operators of the reference-layout device halves y (solution side) and b (noise)
+// at zero momentum, summed per time slice, without the kappa factors: loopops with
+// ksub, then spacesum at imom = 1.  J_host[(iop * nt + t) * 2 + ri], iop < 9.
+// Scratch: val holds 18 V doubles, Jdev 18 nt doubles.
+int loop_slices(qq_ctx* c, const double* ye, const double* yo, const double* be, const double* bo, int ksub,
+                double* val, double* Jdev, double* J_host) {
+  const int nt = c->g.n[3], V = 2 * c->g.vh;
+  count_launch(2);
+  if (c->recon64 == 18)
+    loopops_kernel<18><<<(V + 127) / 128, 128, 0, c->st>>>(c->g, c->rd, ye, yo, be, bo, c->gauge64.p, ksub, val);
+  else
+    loopops_kernel<12><<<(V + 127) / 128, 128, 0, c->st>>>(c->g, c->rd, ye, yo, be, bo, c->gauge64.p, ksub, val);
+  QQ_CK(cudaGetLastError());
+  spacesum_kernel<<<dim3(nt, 1), 256, 0, c->st>>>(c->g, val, nt, nullptr, 1, Jdev);
+  QQ_CK(cudaGetLastError());
+  QQ_CK(cudaMemcpyAsync(J_host, Jdev, sizeof(double) * 18 * nt, cudaMemcpyDeviceToHost, c->st));
+  QQ_CK(cudaStreamSynchronize(c->st));
+  return QQ_OK;
+}
+
 }  // namespace qq
 
 using namespace qq;

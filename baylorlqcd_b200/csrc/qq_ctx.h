@@ -109,8 +109,8 @@ struct qq_ctx {
   std::vector<double> prof_bytes;
   std::vector<int> prof_shape;                       // per profiled launch: Prec * 1000 + nrhs
   size_t prof_used = 0;
-  std::vector<std::unique_ptr<qq::Field>> pool[3];  // temporaries per precision
-  std::vector<bool> pool_busy[3];
+  std::vector<std::unique_ptr<qq::Field>> pool[4];  // temporaries per precision (Prec)
+  std::vector<bool> pool_busy[4];
   // Persistent workspaces of the batched solver, by id (qq::ws_get): allocated on first
   // use, grown when a later call needs more, freed with the context.
   std::map<int, std::unique_ptr<qq::DevBuf>> ws;

@@ -276,6 +276,112 @@ inline void hess_lsq(const Mat& Hb, const std::vector<cd>& c, int m, std::vector
   }
 }
 
+// Eigenvalues w and right eigenvectors (columns of V) of a general complex n x n A:
+// Hessenberg reduction, complex Schur form T = Z^H A Z, then for each j the solution of
+// (T - T_jj) y = 0 with y_j = 1 by back substitution (Golub & Van Loan Sec. 7.6.4; a
+// denominator smaller than eps |T_jj| is replaced by that bound), and v_j = Z y.  Each
+// column has unit 2-norm and its largest-modulus entry (the first on ties) real and
+// positive, the normalisation of LAPACK's ZGEEV.  Returns false if QR did not converge.
+inline bool eig_vectors(const Mat& A, std::vector<cd>& w, Mat& V) {
+  const int n = A.n;
+  Mat T = A, Z;
+  hessenberg(T, Z);
+  if (!schur(T, Z)) return false;
+  const double eps = 2.220446049250313e-16, tiny = 1e-300;
+  w.resize(n);
+  for (int j = 0; j < n; ++j) w[j] = T(j, j);
+  V = Mat(n, n);
+  std::vector<cd> y(n);
+  for (int j = 0; j < n; ++j) {
+    const cd lam = T(j, j);
+    const double smin = std::max(eps * std::abs(lam), tiny);
+    std::fill(y.begin(), y.end(), cd(0, 0));
+    y[j] = 1.0;
+    for (int i = j - 1; i >= 0; --i) {
+      cd s = 0.0;
+      for (int l = i + 1; l <= j; ++l) s += T(i, l) * y[l];
+      cd d = T(i, i) - lam;
+      if (std::abs(d) < smin) d = smin;
+      y[i] = -s / d;
+    }
+    double nrm = 0.0;
+    for (int i = 0; i < n; ++i) {
+      cd s = 0.0;
+      for (int l = 0; l <= j; ++l) s += Z(i, l) * y[l];
+      V(i, j) = s;
+      nrm += std::norm(s);
+    }
+    nrm = std::sqrt(nrm);
+    int kmax = 0;
+    double best = -1.0;
+    for (int i = 0; i < n; ++i) {
+      V(i, j) /= nrm;
+      if (std::norm(V(i, j)) > best) {
+        best = std::norm(V(i, j));
+        kmax = i;
+      }
+    }
+    const cd ph = std::conj(V(kmax, j)) / std::abs(V(kmax, j));
+    for (int i = 0; i < n; ++i) V(i, j) *= ph;
+    V(kmax, j) = cd(V(kmax, j).real(), 0.0);
+  }
+  return true;
+}
+
+// Householder QR of a tall m x n matrix A (m >= n): Q (m x n) with orthonormal columns
+// and A = Q R, R upper triangular with a real positive diagonal (Householder
+// reflectors, Golub & Van Loan Alg. 5.2.1, Q accumulated backwards as ZUNGQR does).
+inline void house_q(const Mat& A, Mat& Q) {
+  const int m = A.m, n = A.n;
+  Mat R = A;
+  std::vector<std::vector<cd>> vs(n);
+  std::vector<double> taus(n, 0.0);
+  for (int k = 0; k < n; ++k) {
+    double xn = 0.0;
+    for (int i = k; i < m; ++i) xn += std::norm(R(i, k));
+    xn = std::sqrt(xn);
+    std::vector<cd> v(m, 0.0);
+    if (xn == 0.0) {
+      vs[k] = v;
+      continue;
+    }
+    const cd x0 = R(k, k);
+    const cd alpha = (std::abs(x0) == 0.0 ? cd(1, 0) : x0 / std::abs(x0)) * (-xn);
+    v[k] = x0 - alpha;
+    for (int i = k + 1; i < m; ++i) v[i] = R(i, k);
+    double vn = 0.0;
+    for (int i = k; i < m; ++i) vn += std::norm(v[i]);
+    const double tau = vn == 0.0 ? 0.0 : 2.0 / vn;
+    for (int j = k; j < n; ++j) {
+      cd s = 0.0;
+      for (int i = k; i < m; ++i) s += std::conj(v[i]) * R(i, j);
+      s *= tau;
+      for (int i = k; i < m; ++i) R(i, j) -= v[i] * s;
+    }
+    vs[k] = v;
+    taus[k] = tau;
+  }
+  // Q = H_0 H_1 ... H_{n-1} applied to the first n columns of the identity; each
+  // column is then rotated so that R's diagonal is real and positive.
+  Q = Mat(m, n);
+  for (int j = 0; j < n; ++j) Q(j, j) = 1.0;
+  for (int k = n - 1; k >= 0; --k) {
+    const std::vector<cd>& v = vs[k];
+    for (int j = 0; j < n; ++j) {
+      cd s = 0.0;
+      for (int i = k; i < m; ++i) s += std::conj(v[i]) * Q(i, j);
+      s *= taus[k];
+      for (int i = k; i < m; ++i) Q(i, j) -= v[i] * s;
+    }
+  }
+  for (int j = 0; j < n; ++j) {
+    const cd d = R(j, j);
+    if (std::abs(d) == 0.0) continue;
+    const cd ph = d / std::abs(d);
+    for (int i = 0; i < m; ++i) Q(i, j) *= ph;
+  }
+}
+
 // One GMRES-DR restart (Morgan 2002, steps 5-8): given Hb ((m+1) x m, the Arnoldi
 // relation A V_m = V_{m+1} Hb) and the least-squares residual srv (length m+1),
 // build P ((m+1) x (k+1), orthonormal columns), the new Hb_k = P^H Hb P_k

@@ -323,6 +323,53 @@ int qq_average(qq_ctx* ctx, const double* be, const double* bo, const double* xe
  * momfac(nvhalf, 2, 16, 4, 5), nvhalf = nx*ny*nz*nt/32. */
 int qq_momfacs(const int dims[4], const int io[3], double* momfac);
 
+/* ---- eigenmode subtraction of the Wilson loop driver (testFUNC,
+ * Q/disconloops.f90:1980-2569) ----
+ * A qq_eig handle holds kept eigenmodes on the device (right vectors R and, for kind 1,
+ * left vectors L; both halves of the lattice) and their eigenvalues. */
+typedef struct qq_eig qq_eig;
+/* kind 1: eigmodesofM Q/disconloops.f90:1593-1937, modes of M = 1 - kappa D.  The Ritz
+ * pairs of the even-odd operator Hdbletm (Hdouble when kappa[1] < 1e-8) after ncycles
+ * cycles of gmresdrEIGBS Q/working.f90:48-907 (GMRES-DR(nGMRES) whose restart keeps the
+ * k = nGMRES[1] harmonic Ritz vectors with the smallest |theta| plus their common
+ * residual direction; the reference runs 150 cycles of (200, 160)) from the unit source
+ * b(1,1,1,1,1) = 1; se, so are ignored.  Ritz values in conjugate pairs (to 1e-8) are
+ * lifted to M, lambda = 1 - sqrt(1 - kappa^2 theta), with odd halves
+ * kappa H_oe R_e / sqrt(1 - kappa^2 theta) and left vectors gamma5 times the partner's
+ * right vector, R scaled to <R, L> = 1; modes with ||M R - lambda R|| < 1e-8 are kept,
+ * sorted by |lambda|.  The reference's sort reads its permutation through the wrong
+ * index (ind2(ind(eig)), :1889-1899); the two agree whenever every pair is kept.
+ * kind 2: eigmodesofMprime :2573-2875, modes of the Hermitian M gamma5 on the full
+ * lattice after ncycles cycles of gmresdr5EIG Q/inverters.f90:1435-2070 (the restart
+ * keeps the least-squares residual; the reference allows 5500 cycles) from the start
+ * vector (se, so) (the reference draws a Z(4) noise, qq_z4source); unit-norm modes with
+ * ||M gamma5 R - Re(theta) R|| < 1e-5 are kept, sorted by |Re theta|, L = R.
+ * nGMRES: k < m <= 255.  numEV (may be NULL): modes kept; evals (may be NULL, room for
+ * 2 k doubles): their eigenvalues (re, im).  Release with qq_eig_destroy. */
+int qq_eigmodes(qq_ctx* ctx, int kind, const int nGMRES[2], int ncycles, const double kappa[2],
+                const double* se, const double* so, qq_eig** eig, int* numEV, double* evals);
+int qq_eig_destroy(qq_eig* eig);
+/* kind, modes kept, cycles run, operator applications, eigenvalues (2 numEV) and the
+ * k Ritz values of the last cycle (2 k); any output may be NULL. */
+int qq_eig_info(const qq_eig* eig, int* kind, int* numEV, int* cycles, int* mvp, double* evals,
+                double* ritz);
+/* Mode j (0-based) as reference-layout halves (host or device): R, or L if left != 0. */
+int qq_eig_vector(const qq_eig* eig, int j, int left, double* ve, double* vo);
+/* xigenerator Q/disconloops.f90:465-838: xiinv(2, 6, numEV) (Fortran order, host or
+ * device) = <L_j, S_isub R_j> with S_1 = 0 and S_isub = sum_{n=0}^{isub+1} kappa^n H^n
+ * (H = Hsingle on each half), times gamma5 for kind 2 (gammaid = 2). */
+int qq_xigenerator(qq_ctx* ctx, const qq_eig* eig, double kappa, double* xiinv);
+/* eigaverage Q/disconloops.f90:3239-3342: for each selected mode count j (j = eigstart,
+ * every eigstep-th after it, and numEV) the loop operators (loopops, ksub 0; kind 2:
+ * eigloopops_original :7919-8038, i.e. of gamma5 x') of the correction
+ * x'_j = sum_{i<=j} R_i s_i <L_i, z> against the noise z, summed per time slice;
+ * operators 1..4 times kappa; other counts zero.  scal(2, numEV): the multipliers s
+ * (1/lambda for the plain estimator, xiinv(:, isub, :) for the combined one).
+ * Jtime(2, nt, numEV, 9), Fortran order, host or device: the reference's
+ * Jtime(:, :, :, 1, :) (its momentum slots 2..5 stay zero, as its momfac is zero). */
+int qq_eigaverage(qq_ctx* ctx, const qq_eig* eig, const double* ze, const double* zo, double kappa,
+                  const double* scal, int eigstart, int eigstep, double* Jtime);
+
 /* ---- file formats (host memory; no device needed) ----
  * Fortran unformatted sequential files, as the reference writes them: every record is
  * framed by its 4-byte length, reals are 8 bytes, integers 4.  nvhalf and ntotal are

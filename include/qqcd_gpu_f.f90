@@ -426,6 +426,59 @@ module qqcd_gpu
       integer(c_int) :: st
     end function qq_momfacs
 
+    ! ---- eigenmode subtraction of the Wilson loop driver ----
+    function qq_eigmodes(ctx, kind, nGMRES, ncycles, kappa, se, so, eig, numEV, evals) &
+        bind(C, name="qq_eigmodes") result(st)
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: kind
+      integer(c_int), intent(in) :: nGMRES(2)
+      integer(c_int), value :: ncycles
+      real(c_double), intent(in) :: kappa(2)
+      real(c_double), intent(in) :: se(*), so(*)
+      type(c_ptr), intent(out) :: eig
+      integer(c_int), intent(out) :: numEV
+      real(c_double), intent(out) :: evals(*)
+      integer(c_int) :: st
+    end function qq_eigmodes
+    function qq_eig_destroy(eig) bind(C, name="qq_eig_destroy") result(st)
+      import :: c_int, c_ptr
+      type(c_ptr), value :: eig
+      integer(c_int) :: st
+    end function qq_eig_destroy
+    function qq_eig_info(eig, kind, numEV, cycles, mvp, evals, ritz) bind(C, name="qq_eig_info") result(st)
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: eig
+      integer(c_int), intent(out) :: kind, numEV, cycles, mvp
+      real(c_double), intent(out) :: evals(*), ritz(*)
+      integer(c_int) :: st
+    end function qq_eig_info
+    function qq_eig_vector(eig, j, left, ve, vo) bind(C, name="qq_eig_vector") result(st)
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: eig
+      integer(c_int), value :: j, left
+      real(c_double), intent(out) :: ve(*), vo(*)
+      integer(c_int) :: st
+    end function qq_eig_vector
+    function qq_xigenerator(ctx, eig, kappa, xiinv) bind(C, name="qq_xigenerator") result(st)
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: ctx, eig
+      real(c_double), value :: kappa
+      real(c_double), intent(out) :: xiinv(*)
+      integer(c_int) :: st
+    end function qq_xigenerator
+    function qq_eigaverage(ctx, eig, ze, zo, kappa, scal, eigstart, eigstep, Jtime) &
+        bind(C, name="qq_eigaverage") result(st)
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: ctx, eig
+      real(c_double), intent(in) :: ze(*), zo(*)
+      real(c_double), value :: kappa
+      real(c_double), intent(in) :: scal(*)
+      integer(c_int), value :: eigstart, eigstep
+      real(c_double), intent(out) :: Jtime(*)
+      integer(c_int) :: st
+    end function qq_eigaverage
+
     ! ---- file formats ----
     function qq_gfwrite(path, u, nvhalf, ntotal, gaction, beta, alat, tad, icfgsave, myid) &
         bind(C, name="qq_gfwrite") result(st)

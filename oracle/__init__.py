@@ -91,6 +91,9 @@ def lib() -> C.CDLL:
             "oq_twvev": ([P, DP, D, D, IP, I, I, I, I, I, DP], None),
             "oq_average": ([P, DP, DP, DP, DP, DP, D, I, I, I, DP, DP], None),
             "oq_momfacs": ([P, IP, DP], None),
+            "oq_eigmodes": ([P, DP, I, IP, I, DP, DP, DP, DP, DP, DP, IP], I),
+            "oq_xigenerator": ([P, DP, I, D, DP, DP, I, DP], None),
+            "oq_eigaverage": ([P, DP, I, I, I, DP, DP, D, DP, DP, DP, I, DP], None),
             "oq_twaverage_mom": ([P, DP, DP, DP, DP, DP, D, D, IP, I, I, I, DP], None),
             "oq_twvev_sites": ([P, DP, D, D, IP, I, I, I, IP, I, DP], None),
             "oq_set_kcyclim": ([I], None),
@@ -351,6 +354,44 @@ class OracleLattice:
         lib().oq_average(self._g, _dp(self.u), _dp(np.ascontiguousarray(be)), _dp(np.ascontiguousarray(bo)),
                          _dp(np.ascontiguousarray(xe)), _dp(np.ascontiguousarray(xo)), float(kappa), int(nsub),
                          int(nmom), int(nop), _dp(mf), _dp(J))
+        return J
+
+    def eigmodes(self, kind, nGMRES, ncycles, kappa, se=None, so=None):
+        """eigmodesofM (kind 1) / eigmodesofMprime (kind 2), Q/disconloops.f90:1593-1937,
+        2573-2875.  Returns (evals complex (numEV,), R, L) with R, L of numpy shape
+        (numEV, 2) + half_shape (even then odd half), and the cycles run."""
+        k = int(nGMRES[1])
+        R = np.zeros((k, 2) + self.half_shape)
+        L = np.zeros((k, 2) + self.half_shape)
+        ev = np.zeros(2 * k)
+        cyc = C.c_int(0)
+        _, gp = _ip(nGMRES)
+        kp = np.ascontiguousarray(kappa, dtype=np.float64)
+        z = np.zeros(self.half_shape)
+        se = z if se is None else np.ascontiguousarray(se)
+        so = z if so is None else np.ascontiguousarray(so)
+        n = lib().oq_eigmodes(self._g, _dp(self.u), int(kind), gp, int(ncycles), _dp(kp), _dp(se), _dp(so),
+                              _dp(R), _dp(L), _dp(ev), C.byref(cyc))
+        return ev[0:2 * n:2] + 1j * ev[1:2 * n:2], R[:n].copy(), L[:n].copy(), cyc.value
+
+    def xigenerator(self, R, L, kappa, gammaid):
+        """xigenerator (Q/disconloops.f90:465-838): xiinv as complex (numEV, 6)."""
+        n = R.shape[0]
+        xi = np.zeros((n, 6, 2))
+        lib().oq_xigenerator(self._g, _dp(self.u), n, float(kappa), _dp(np.ascontiguousarray(R)),
+                             _dp(np.ascontiguousarray(L)), int(gammaid), _dp(xi))
+        return xi[..., 0] + 1j * xi[..., 1]
+
+    def eigaverage(self, ze, zo, kappa, R, L, scal, eshfes, eigstart=1, eigstep=1):
+        """eigaverage (Q/disconloops.f90:3239-3342) at imom = 1: Jtime as (9, numEV, nt, 2)."""
+        n = R.shape[0]
+        J = np.zeros((9, n, self.dims[3], 2))
+        s = np.zeros((n, 2))
+        s[:, 0] = np.real(scal)
+        s[:, 1] = np.imag(scal)
+        lib().oq_eigaverage(self._g, _dp(self.u), n, int(eigstart), int(eigstep), _dp(np.ascontiguousarray(ze)),
+                            _dp(np.ascontiguousarray(zo)), float(kappa), _dp(np.ascontiguousarray(R)),
+                            _dp(np.ascontiguousarray(L)), _dp(s), int(eshfes), _dp(J))
         return J
 
     def twvev(self, kappa, delta=0.0, io=(1, 1, 1), dobndry=0, ir=1, nsub=6, nmom=5, nop=6):

@@ -1,0 +1,658 @@
+// CPU oracle (test infrastructure): the eigenmode subtraction of the reference's Wilson
+// loop driver (testFUNC, Q/disconloops.f90:1980-2569), restating
+//   * gmresdrEIGBS, Q/working.f90:48-907: GMRES-DR(m, k) on Hdbletm from b with the
+//     restart of the MATLAB form: least squares H d = c and the residual coordinates srv
+//     (:391-393), the harmonic Ritz matrix H_m + h^2 f e_m^T with H_m^H f = e_m
+//     (:465-482), its eigenpairs (eigencalc, :483) sorted by |theta|^2 (:490), the k
+//     smallest kept, their Ritz residuals rna (:499-513) sorted (:521), the vectors
+//     reordered by rna (:578), the extra column -h f with 1 in row m+1 (:589-598), QR of
+//     that (m+1) x (k+1) matrix (:604), hcnew = Q^H H Q (:614-615), the Ritz vectors
+//     V_m g and values (:625-648), the new basis V_{m+1} Q (:668-693), one Gram-Schmidt
+//     pass on v_{k+1} and its normalisation (:695-721); cycles while rn / rninit > 1e-160
+//     and icycle <= ncycles (:148; the reference: 150).  The blocks under if (.false.)
+//     and the per-cycle residual of every Ritz vector (written only to a log) are left
+//     out; so is the solution x, which the callers never read;
+//   * gmresdr5EIG, Q/inverters.f90:1435-2070: the same iteration on M gamma5 over the
+//     full lattice (gamma5, then (M y)_e = y_e - kappa H_eo y_o, (M y)_o = y_o -
+//     kappa H_oe y_e, :1561-1589) from (be, bo), with the least-squares residual srv as
+//     the extra column (:1877) and, while the i-th Ritz residual in |theta| order is
+//     below 1e-12, column i of hcnew zeroed below its diagonal (:1895-1899);
+//   * eigmodesofM, Q/disconloops.f90:1593-1937 (pairs of conjugate Ritz values to 1e-8,
+//     the odd halves kappa H_oe R_e / sqrt(1 - kappa^2 theta), eigenvalues
+//     1 - sqrt(1 - kappa^2 theta), left vectors gamma5 times the partner's right vector,
+//     <R, L> = 1, the 1e-8 residual test on M, the sort by |lambda|; the sort's final
+//     gather is done through ind(ind2(eig)) -- the reference writes ind2(ind(eig))
+//     (:1893-1899), which is the same permutation whenever every pair passes the
+//     residual test and reads outside ind2 otherwise);
+//   * eigmodesofMprime, :2573-2875 (unit norm, the 1e-5 residual test against Re theta,
+//     the sort by |Re theta|);
+//   * xigenerator, :465-838; eigaverage, :3239-3342, whose loopops + spacesum at
+//     imom = 1 with kappa on operators 1..4 are oq_average's level 1 of the correction
+//     (eigloopops_original, :7919-8038, equals loopops of gamma5 times it).
+// Small dense algebra: zgels (leastsquaresLAPACK, Q/inverters.f90:53-105) and
+// zgeqrf + zungqr (qrfactorizationLAPACK, :247-297) are restated as Householder QR;
+// eigencalc (Q/pseudolapack.f90:79-174) as the restated hessenberg, qgenerator and
+// evalues followed by back substitution on the Schur factor and eigencalc's
+// normalisation (unit norm, largest component real).  eigencalc's balancing and the
+// overflow guards of its triangular solve are left out: they change rounding, not the
+// eigenpairs.  Parity is of the converged eigenpairs and what is built from them.
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstring>
+#include <vector>
+
+#include "oracle_impl.h"
+
+namespace {
+
+using C = std::complex<double>;
+
+struct Mt {  // column-major complex matrix, 0-based
+  int m = 0, n = 0;
+  std::vector<C> a;
+  Mt() = default;
+  Mt(int m_, int n_) : m(m_), n(n_), a((size_t)m_ * n_, C(0, 0)) {}
+  C& operator()(int i, int j) { return a[(size_t)i + (size_t)m * j]; }
+  const C& operator()(int i, int j) const { return a[(size_t)i + (size_t)m * j]; }
+  double* raw() { return reinterpret_cast<double*>(a.data()); }
+};
+
+// Householder reflector for column k of A (rows k..m-1): v and tau with
+// (I - tau v v^H) A(k:, k) = beta e_k, beta real.
+void reflector(const Mt& A, int k, std::vector<C>& v, double& tau) {
+  const int m = A.m;
+  double xn = 0.0;
+  for (int i = k; i < m; ++i) xn += std::norm(A(i, k));
+  xn = std::sqrt(xn);
+  v.assign(m, 0.0);
+  tau = 0.0;
+  if (xn == 0.0) return;
+  const C x0 = A(k, k);
+  const C alpha = (std::abs(x0) == 0.0 ? C(1, 0) : x0 / std::abs(x0)) * (-xn);
+  v[k] = x0 - alpha;
+  for (int i = k + 1; i < m; ++i) v[i] = A(i, k);
+  double vn = 0.0;
+  for (int i = k; i < m; ++i) vn += std::norm(v[i]);
+  tau = vn == 0.0 ? 0.0 : 2.0 / vn;
+}
+
+void apply_reflector(Mt& A, int k, const std::vector<C>& v, double tau, int j0) {
+  for (int j = j0; j < A.n; ++j) {
+    C s = 0.0;
+    for (int i = k; i < A.m; ++i) s += std::conj(v[i]) * A(i, j);
+    s *= tau;
+    for (int i = k; i < A.m; ++i) A(i, j) -= v[i] * s;
+  }
+}
+
+// min || b - A x || for a full-rank m x n A (m >= n): x (n)
+std::vector<C> lsq(Mt A, std::vector<C> b) {
+  const int m = A.m, n = A.n;
+  Mt B(m, 1);
+  for (int i = 0; i < m; ++i) B(i, 0) = b[i];
+  std::vector<C> v;
+  double tau;
+  for (int k = 0; k < n; ++k) {
+    reflector(A, k, v, tau);
+    apply_reflector(A, k, v, tau, k);
+    apply_reflector(B, k, v, tau, 0);
+  }
+  std::vector<C> x(n);
+  for (int i = n - 1; i >= 0; --i) {
+    C s = B(i, 0);
+    for (int j = i + 1; j < n; ++j) s -= A(i, j) * x[j];
+    x[i] = s / A(i, i);
+  }
+  return x;
+}
+
+// Q (m x n, orthonormal columns) of A = Q R
+Mt qfactor(Mt A) {
+  const int m = A.m, n = A.n;
+  std::vector<std::vector<C>> vs(n);
+  std::vector<double> taus(n);
+  for (int k = 0; k < n; ++k) {
+    reflector(A, k, vs[k], taus[k]);
+    apply_reflector(A, k, vs[k], taus[k], k);
+  }
+  Mt Q(m, n);
+  for (int j = 0; j < n; ++j) Q(j, j) = 1.0;
+  for (int k = n - 1; k >= 0; --k) apply_reflector(Q, k, vs[k], taus[k], 0);
+  return Q;
+}
+
+// eigencalc with eigenvectors
+void eigencalc(const Mt& A, std::vector<C>& w, Mt& V) {
+  const int n = A.n;
+  Mt h = A, z(n, n);
+  std::vector<double> tau(2 * (size_t)n, 0.0), wr(2 * (size_t)n, 0.0);
+  oq_hessenberg(h.raw(), n, n, 1, n, tau.data());
+  for (int j = 0; j < n; ++j)
+    for (int i = j; i < n; ++i) z(i, j) = h(i, j);
+  oq_qgenerator(n, 1, n, z.raw(), n, tau.data());
+  oq_evalues(1, n, 1, n, h.raw(), n, wr.data(), z.raw(), n);
+  w.resize(n);
+  for (int i = 0; i < n; ++i) w[i] = C(wr[2 * i], wr[2 * i + 1]);
+  // h is now upper triangular (Schur form) with A = z h z^H
+  V = Mt(n, n);
+  const double eps = 2.220446049250313e-16;
+  std::vector<C> y(n);
+  for (int j = 0; j < n; ++j) {
+    const C lam = h(j, j);
+    const double smin = std::max(eps * std::abs(lam), 1e-300);
+    std::fill(y.begin(), y.end(), C(0, 0));
+    y[j] = 1.0;
+    for (int i = j - 1; i >= 0; --i) {
+      C s = 0.0;
+      for (int l = i + 1; l <= j; ++l) s += h(i, l) * y[l];
+      C d = h(i, i) - lam;
+      if (std::abs(d) < smin) d = smin;
+      y[i] = -s / d;
+    }
+    double nrm = 0.0;
+    for (int i = 0; i < n; ++i) {
+      C s = 0.0;
+      for (int l = 0; l <= j; ++l) s += z(i, l) * y[l];
+      V(i, j) = s;
+      nrm += std::norm(s);
+    }
+    nrm = std::sqrt(nrm);
+    int kx = 0;
+    double best = -1.0;
+    for (int i = 0; i < n; ++i) {
+      V(i, j) /= nrm;
+      if (std::norm(V(i, j)) > best) {
+        best = std::norm(V(i, j));
+        kx = i;
+      }
+    }
+    const C ph = std::conj(V(kx, j)) / std::abs(V(kx, j));
+    for (int i = 0; i < n; ++i) V(i, j) *= ph;
+    V(kx, j) = C(V(kx, j).real(), 0.0);
+  }
+}
+
+// sort basics.f90:81-115 (exchange sort, ascending, stable)
+std::vector<int> sort_index(const std::vector<double>& v) {
+  const int m = (int)v.size();
+  std::vector<double> t(v);
+  std::vector<int> ind(m);
+  for (int i = 0; i < m; ++i) ind[i] = i;
+  for (int j = 1; j <= m - 1; ++j)
+    for (int i = 0; i < m - j; ++i)
+      if (t[i] > t[i + 1]) {
+        std::swap(ind[i], ind[i + 1]);
+        std::swap(t[i], t[i + 1]);
+      }
+  return ind;
+}
+
+// cmpxsqrt basics.f90:286-343 (the Numerical Recipes branch)
+C cmpxsqrt(C z) {
+  const double c = z.real(), d = z.imag();
+  double w;
+  if (c == 0.0 && d == 0.0) {
+    w = 0.0;
+  } else if (std::fabs(c) >= std::fabs(d)) {
+    const double t1 = d / c;
+    w = std::sqrt(std::fabs(c)) * std::sqrt((1.0 + std::sqrt(1.0 + t1 * t1)) / 2.0);
+  } else {
+    const double t1 = c / d;
+    w = std::sqrt(std::fabs(d)) * std::sqrt((std::fabs(t1) + std::sqrt(1.0 + t1 * t1)) / 2.0);
+  }
+  if (w == 0.0) return C(0.0, 0.0);
+  if (c >= 0.0) return C(w, d / (2.0 * w));
+  if (d >= 0.0) return C(std::fabs(d) / (2.0 * w), w);
+  return C(std::fabs(d) / (2.0 * w), -w);
+}
+
+// oneover basics.f90:48-77
+C oneover(C z) {
+  const double c = z.real(), d = z.imag();
+  if (std::fabs(c) >= std::fabs(d)) {
+    const double t1 = d / c, t2 = t1 * d + c;
+    return C(1.0 / t2, -t1 / t2);
+  }
+  const double t1 = c / d, t2 = t1 * c + d;
+  return C(t1 / t2, -1.0 / t2);
+}
+
+struct Space {  // nhalf reference-layout half vectors per Krylov vector (1 or 2)
+  const oq_geom* g;
+  int nhalf;
+  size_t vs;
+  size_t size() const { return vs * nhalf; }
+  C dot(const double* a, const double* b) const {  // a^H b over the interior sites
+    C s = 0.0;
+    for (int h = 0; h < nhalf; ++h) {
+      double im = 0.0;
+      const double re = oq::vecdot_re(g, a + h * vs, b + h * vs, &im);
+      s += C(re, im);
+    }
+    return s;
+  }
+  void axpy(double* y, C a, const double* x) const {  // y += a x on the interior sites
+    for (int h = 0; h < nhalf; ++h) {
+      double* yy = y + h * vs;
+      const double* xx = x + h * vs;
+      for (int ibleo = 1; ibleo <= 8; ++ibleo)
+        for (int ieo = 1; ieo <= 2; ++ieo)
+          for (int id = 1; id <= 4; ++id)
+            for (int s = 1; s <= g->nvhalf; ++s)
+              for (int c = 1; c <= 5; c += 2) {
+                const size_t k = g->gi(c, s, id, ieo, ibleo);
+                const double xr = xx[k], xi = xx[k + 1];
+                yy[k] = yy[k] + a.real() * xr - a.imag() * xi;
+                yy[k + 1] = yy[k + 1] + a.imag() * xr + a.real() * xi;
+              }
+    }
+  }
+  void scale(double* y, double s) const {
+    for (int h = 0; h < nhalf; ++h)
+      g->for_interior([&](size_t k) { y[h * vs + k] *= s; });
+  }
+};
+
+// The Krylov operator of each variant: Hdbletm on the even half (1), M gamma5 on the
+// full lattice (2).
+void apply_op(const oq_geom* g, const double* u, int variant, const double kappa[2], double* out, double* in) {
+  const size_t vs = g->vsize();
+  if (variant == 1) {
+    oq::hdbletm(g, out, u, in, 0, kappa);
+    return;
+  }
+  std::vector<double> te(in, in + vs), to(in + vs, in + 2 * vs), he(vs, 0.0), ho(vs, 0.0);
+  oq_gam5x(g, te.data());
+  oq_gam5x(g, to.data());
+  oq::hsingle(g, ho.data(), u, te.data(), 0, 2);
+  oq::hsingle(g, he.data(), u, to.data(), 0, 1);
+  std::memset(out, 0, sizeof(double) * 2 * vs);
+  g->for_interior([&](size_t k) {
+    out[k] = te[k] - kappa[0] * he[k];
+    out[vs + k] = to[k] - kappa[0] * ho[k];
+  });
+}
+
+// gmresdrEIGBS (variant 1) / gmresdr5EIG (variant 2): evec (k vectors) and eval.
+void eig_gmresdr(const oq_geom* g, const double* u, int variant, const double kappa[2], const double* b, int m,
+                 int k, int ncycles, std::vector<double>& evec, std::vector<C>& eval, int* cycles) {
+  Space S{g, variant == 1 ? 1 : 2, g->vsize()};
+  const size_t n = S.size();
+  std::vector<double> v((size_t)(m + 1) * n, 0.0), work((size_t)(k + 1) * n, 0.0), wv(n);
+  auto V = [&](int i) { return v.data() + (size_t)i * n; };
+  Mt h(m + 1, m);
+  std::vector<C> c(m + 1, 0.0);
+  const double rninit = std::sqrt(S.dot(b, b).real());
+  std::memcpy(V(0), b, sizeof(double) * n);
+  S.scale(V(0), 1.0 / rninit);
+  c[0] = rninit;
+  double rn = rninit;
+  int j = 0, icycle = 1;
+  evec.assign((size_t)k * n, 0.0);
+  while (rn / rninit > 1e-160 && icycle <= ncycles) {
+    while (j < m) {
+      apply_op(g, u, variant, kappa, wv.data(), V(j));
+      const double vnf = std::sqrt(S.dot(wv.data(), wv.data()).real());
+      for (int i = 0; i <= j; ++i) {
+        h(i, j) = S.dot(V(i), wv.data());
+        S.axpy(wv.data(), -h(i, j), V(i));
+      }
+      double vn = std::sqrt(S.dot(wv.data(), wv.data()).real());
+      if (vn < 1.1 * vnf) {
+        for (int i = 0; i <= j; ++i) {
+          const C t = S.dot(V(i), wv.data());
+          S.axpy(wv.data(), -t, V(i));
+          h(i, j) += t;
+        }
+        vn = std::sqrt(S.dot(wv.data(), wv.data()).real());
+      }
+      h(j + 1, j) = vn;
+      std::memcpy(V(j + 1), wv.data(), sizeof(double) * n);
+      S.scale(V(j + 1), 1.0 / vn);
+      ++j;
+    }
+    const std::vector<C> d = lsq(h, c);
+    std::vector<C> srv(m + 1);
+    for (int i = 0; i <= m; ++i) {
+      C s = 0.0;
+      for (int l = 0; l < m; ++l) s += h(i, l) * d[l];
+      srv[i] = c[i] - s;
+    }
+    // r = V srv and its norm
+    {
+      std::vector<double> r(n, 0.0);
+      for (int i = 0; i <= m; ++i) S.axpy(r.data(), srv[i], V(i));
+      rn = std::sqrt(S.dot(r.data(), r.data()).real());
+    }
+    // harmonic Ritz
+    Mt hh(m, m), hcht(m, m);
+    for (int jj = 0; jj < m; ++jj)
+      for (int i = 0; i < m; ++i) {
+        hh(i, jj) = h(i, jj);
+        hcht(i, jj) = std::conj(h(jj, i));
+      }
+    std::vector<double> ff(2 * (size_t)m, 0.0);
+    std::vector<int> ipiv(m);
+    ff[2 * (m - 1)] = 1.0;
+    oq_linearsolver(m, 1, hcht.raw(), m, ipiv.data(), ff.data(), m);
+    std::vector<C> f(m);
+    for (int i = 0; i < m; ++i) f[i] = C(ff[2 * i], ff[2 * i + 1]);
+    const C hl = h(m, m - 1);
+    for (int i = 0; i < m; ++i) hh(i, m - 1) += hl * hl * f[i];
+    std::vector<C> dd;
+    Mt gg;
+    eigencalc(hh, dd, gg);
+    std::vector<double> dabbs(m);
+    for (int i = 0; i < m; ++i) dabbs[i] = std::norm(dd[i]);
+    const std::vector<int> ind = sort_index(dabbs);
+    std::vector<C> th(k);
+    Mt gk(m, k);
+    for (int i = 0; i < k; ++i) {
+      th[i] = dd[ind[i]];
+      for (int r = 0; r < m; ++r) gk(r, i) = gg(r, ind[i]);
+    }
+    std::vector<double> rna(k);
+    for (int i = 0; i < k; ++i) {
+      std::vector<C> tv(m);
+      C rho = 0.0;
+      for (int r = 0; r < m; ++r) {
+        C s = 0.0;
+        for (int l = 0; l < m; ++l) s += h(r, l) * gk(l, i);
+        tv[r] = s;
+        rho += std::conj(gk(r, i)) * s;
+      }
+      double t2 = 0.0;
+      for (int r = 0; r < m; ++r) t2 += std::norm(tv[r] - rho * gk(r, i));
+      rna[i] = std::sqrt(t2 + std::norm(hl) * std::norm(gk(m - 1, i)));
+    }
+    const std::vector<int> ind2 = sort_index(rna);
+    Mt G(m + 1, k + 1);
+    for (int i = 0; i < k; ++i)
+      for (int r = 0; r < m; ++r) G(r, i) = gk(r, ind2[i]);
+    if (variant == 1) {
+      for (int r = 0; r < m; ++r) G(r, k) = -hl * f[r];
+      G(m, k) = 1.0;
+    } else {
+      for (int r = 0; r <= m; ++r) G(r, k) = srv[r];
+    }
+    const Mt Q = qfactor(G);
+    Mt hcnew(k + 1, k);
+    {
+      Mt T(k + 1, m);
+      for (int jj = 0; jj < m; ++jj)
+        for (int i = 0; i <= k; ++i) {
+          C s = 0.0;
+          for (int l = 0; l <= m; ++l) s += std::conj(Q(l, i)) * h(l, jj);
+          T(i, jj) = s;
+        }
+      for (int jj = 0; jj < k; ++jj)
+        for (int i = 0; i <= k; ++i) {
+          C s = 0.0;
+          for (int l = 0; l < m; ++l) s += T(i, l) * Q(l, jj);
+          hcnew(i, jj) = s;
+        }
+    }
+    if (variant == 2)
+      for (int i = 0; i < k && rna[i] < 1e-12; ++i)
+        for (int r = i + 1; r <= k; ++r) hcnew(r, i) = 0.0;
+    // Ritz vectors and values of this cycle
+    for (int jj = 0; jj < k; ++jj) {
+      double* e = evec.data() + (size_t)jj * n;
+      std::memset(e, 0, sizeof(double) * n);
+      for (int kk = 0; kk < m; ++kk) S.axpy(e, G(kk, jj), V(kk));
+    }
+    eval.resize(k);
+    for (int jj = 0; jj < k; ++jj) eval[jj] = th[ind2[jj]];
+    for (int i = 0; i <= m; ++i)
+      for (int jj = 0; jj < m; ++jj) h(i, jj) = 0.0;
+    for (int i = 0; i < k; ++i)
+      for (int jj = 0; jj <= k; ++jj) h(jj, i) = hcnew(jj, i);
+    std::vector<C> cn(m + 1, 0.0);
+    for (int i = 0; i <= k; ++i) {
+      C s = 0.0;
+      for (int l = 0; l <= m; ++l) s += std::conj(Q(l, i)) * srv[l];
+      cn[i] = s;
+    }
+    c = cn;
+    for (int jj = 0; jj <= k; ++jj) {
+      double* w = work.data() + (size_t)jj * n;
+      std::memset(w, 0, sizeof(double) * n);
+      for (int kk = 0; kk <= m; ++kk) S.axpy(w, Q(kk, jj), V(kk));
+    }
+    std::memcpy(v.data(), work.data(), sizeof(double) * (size_t)(k + 1) * n);
+    for (int i = 0; i < k; ++i) {
+      const C t = S.dot(V(i), V(k));
+      S.axpy(V(k), -t, V(i));
+    }
+    S.scale(V(k), 1.0 / std::sqrt(S.dot(V(k), V(k)).real()));
+    *cycles = icycle;
+    j = k;
+    ++icycle;
+  }
+}
+
+}  // namespace
+
+// R, L: room for k vectors of two halves each (g->vsize() doubles per half, even then
+// odd); evals: 2 k.  Returns the number of modes kept.
+extern "C" int oq_eigmodes(const oq_geom* g, const double* u, int kind, const int nGMRES[2], int ncycles,
+                           const double kappa[2], const double* se, const double* so, double* R, double* L,
+                           double* evals, int* cycles) {
+  const size_t vs = g->vsize();
+  const int m = nGMRES[0], k = nGMRES[1];
+  std::vector<double> b((kind == 1 ? 1 : 2) * vs, 0.0);
+  if (kind == 1) {
+    b[0] = 1.0;  // b(1,1,1,1,1)
+  } else {
+    std::memcpy(b.data(), se, sizeof(double) * vs);
+    std::memcpy(b.data() + vs, so, sizeof(double) * vs);
+  }
+  std::vector<double> ev;
+  std::vector<C> th;
+  eig_gmresdr(g, u, kind, kappa, b.data(), m, k, ncycles, ev, th, cycles);
+  const Space S2{g, 2, vs};
+  if (kind == 2) {
+    std::vector<int> keep;
+    std::vector<double> x(2 * vs);
+    for (int ii = 0; ii < k; ++ii) {
+      double* e = ev.data() + (size_t)ii * 2 * vs;
+      S2.scale(e, 1.0 / std::sqrt(S2.dot(e, e).real()));
+      apply_op(g, u, 2, kappa, x.data(), e);
+      S2.axpy(x.data(), C(-th[ii].real(), 0.0), e);
+      if (std::sqrt(S2.dot(x.data(), x.data()).real()) < 1e-5) keep.push_back(ii);
+    }
+    std::vector<double> nrm(keep.size());
+    for (size_t i = 0; i < keep.size(); ++i) nrm[i] = std::fabs(th[keep[i]].real());
+    const std::vector<int> ind2 = sort_index(nrm);
+    for (size_t i = 0; i < keep.size(); ++i) {
+      const int e = keep[ind2[i]];
+      evals[2 * i] = th[e].real();
+      evals[2 * i + 1] = 0.0;
+      std::memcpy(R + i * 2 * vs, ev.data() + (size_t)e * 2 * vs, sizeof(double) * 2 * vs);
+      std::memcpy(L + i * 2 * vs, ev.data() + (size_t)e * 2 * vs, sizeof(double) * 2 * vs);
+    }
+    return (int)keep.size();
+  }
+  // eigmodesofM
+  std::vector<int> indpos, indneg, ind;
+  for (int e = 0; e < k; ++e) {
+    if (std::fabs(th[e].imag()) < 1e-8) continue;
+    (th[e].imag() > 0 ? indpos : indneg).push_back(e);
+  }
+  for (int p : indpos)
+    for (int q : indneg) {
+      const C t(th[p].real() - th[q].real(), th[p].imag() + th[q].imag());
+      if (std::abs(t) <= 1e-8) {
+        ind.push_back(p);
+        ind.push_back(q);
+        break;
+      }
+    }
+  const int eigpair = (int)ind.size();
+  std::vector<double> Rt((size_t)eigpair * 2 * vs, 0.0), Lt((size_t)eigpair * 2 * vs, 0.0);
+  std::vector<C> lam(eigpair);
+  for (int e = 0; e < eigpair; ++e) {
+    double* re = Rt.data() + (size_t)e * 2 * vs;
+    double* ro = re + vs;
+    std::memcpy(re, ev.data() + (size_t)ind[e] * vs, sizeof(double) * vs);
+    std::vector<double> bop(vs, 0.0);
+    oq::hsingle(g, bop.data(), u, re, 0, 2);
+    const C t1 = C(1.0, 0.0) + C(-kappa[0] * kappa[0], 0.0) * th[ind[e]];
+    const C t2 = cmpxsqrt(t1);
+    lam[e] = C(1.0, 0.0) - t2;
+    const C inv = oneover(t2);
+    g->for_spin_interior(
+        [&](size_t s1, size_t s2, size_t s3, size_t s4) {
+          for (size_t s : {s1, s2, s3, s4}) {
+            const double br = kappa[0] * bop[s], bi = kappa[0] * bop[s + 1];
+            ro[s] = inv.real() * br - inv.imag() * bi;
+            ro[s + 1] = inv.imag() * br + inv.real() * bi;
+          }
+        },
+        true);
+  }
+  for (int e = 0; e + 1 < eigpair; e += 2)
+    for (int p = 0; p < 2; ++p) {
+      double* le = Lt.data() + (size_t)e * 2 * vs + p * vs;
+      double* le1 = Lt.data() + (size_t)(e + 1) * 2 * vs + p * vs;
+      std::memcpy(le, Rt.data() + (size_t)(e + 1) * 2 * vs + p * vs, sizeof(double) * vs);
+      std::memcpy(le1, Rt.data() + (size_t)e * 2 * vs + p * vs, sizeof(double) * vs);
+      oq_gam5x(g, le);
+      oq_gam5x(g, le1);
+    }
+  for (int e = 0; e < eigpair; ++e) {
+    double* r = Rt.data() + (size_t)e * 2 * vs;
+    const C rl = S2.dot(r, Lt.data() + (size_t)e * 2 * vs);
+    const C t2 = oneover(rl);
+    std::vector<double> x(r, r + 2 * vs);
+    for (int p = 0; p < 2; ++p)
+      g->for_spin_interior(
+          [&](size_t s1, size_t s2, size_t s3, size_t s4) {
+            for (size_t s : {s1, s2, s3, s4}) {
+              const size_t q = p * vs + s;
+              r[q] = t2.real() * x[q] + t2.imag() * x[q + 1];
+              r[q + 1] = t2.real() * x[q + 1] - t2.imag() * x[q];
+            }
+          },
+          true);
+  }
+  std::vector<int> good;
+  for (int e = 0; e < eigpair; ++e) {
+    double* r = Rt.data() + (size_t)e * 2 * vs;
+    std::vector<double> xe(vs, 0.0), xo(vs, 0.0);
+    oq::hsingle(g, xo.data(), u, r, 0, 2);
+    oq::hsingle(g, xe.data(), u, r + vs, 0, 1);
+    std::vector<double> x(2 * vs, 0.0);
+    g->for_interior([&](size_t q) {
+      x[q] = r[q] - kappa[0] * xe[q];
+      x[vs + q] = r[vs + q] - kappa[0] * xo[q];
+    });
+    S2.axpy(x.data(), -lam[e], r);
+    if (std::sqrt(S2.dot(x.data(), x.data()).real()) < 1e-8) good.push_back(e);
+  }
+  const int numEV = (int)good.size();
+  std::vector<double> nrm(numEV);
+  for (int e = 0; e < numEV; ++e) nrm[e] = std::abs(lam[good[e]]);
+  const std::vector<int> ind2 = sort_index(nrm);
+  for (int e = 0; e < numEV; ++e) {
+    const int src = good[ind2[e]];
+    evals[2 * e] = lam[src].real();
+    evals[2 * e + 1] = lam[src].imag();
+    std::memcpy(R + (size_t)e * 2 * vs, Rt.data() + (size_t)src * 2 * vs, sizeof(double) * 2 * vs);
+    std::memcpy(L + (size_t)e * 2 * vs, Lt.data() + (size_t)src * 2 * vs, sizeof(double) * 2 * vs);
+  }
+  return numEV;
+}
+
+// xigenerator: xiinv(2, 6, numEV)
+extern "C" void oq_xigenerator(const oq_geom* g, const double* u, int numEV, double kappa, const double* R,
+                               const double* L, int gammaid, double* xiinv) {
+  const size_t vs = g->vsize();
+  const Space S1{g, 1, vs};
+  std::vector<double> be(vs), bo(vs), s1e(vs), s1o(vs), s2e(vs), s2o(vs), se(vs), so(vs), te(vs), to(vs);
+  auto H = [&](std::vector<double>& out, std::vector<double>& in, int gblclr) {
+    std::fill(out.begin(), out.end(), 0.0);
+    oq::hsingle(g, out.data(), u, in.data(), 0, gblclr);
+  };
+  auto addk = [&](std::vector<double>& y, double a, const std::vector<double>& x) {
+    g->for_interior([&](size_t k) { y[k] = y[k] + a * x[k]; });
+  };
+  for (int e = 0; e < numEV; ++e) {
+    std::memcpy(be.data(), R + (size_t)e * 2 * vs, sizeof(double) * vs);
+    std::memcpy(bo.data(), R + (size_t)e * 2 * vs + vs, sizeof(double) * vs);
+    for (int isub = 1; isub <= 6; ++isub) {
+      if (isub == 1) {
+        std::fill(se.begin(), se.end(), 0.0);
+        std::fill(so.begin(), so.end(), 0.0);
+      } else if (isub == 2) {
+        H(s1e, bo, 1);
+        H(s1o, be, 2);
+        se = be;
+        so = bo;
+        addk(se, kappa, s1e);
+        addk(so, kappa, s1o);
+        H(s2e, s1o, 1);
+        H(s2o, s1e, 2);
+        addk(se, kappa * kappa, s2e);
+        addk(so, kappa * kappa, s2o);
+        H(s1e, s2o, 1);
+        H(s1o, s2e, 2);
+        addk(se, kappa * kappa * kappa, s1e);
+        addk(so, kappa * kappa * kappa, s1o);
+      } else {
+        const double xk = std::pow(kappa, isub + 1);
+        if (isub % 2 == 1) {
+          H(s2e, s1o, 1);
+          H(s2o, s1e, 2);
+          addk(se, xk, s2e);
+          addk(so, xk, s2o);
+        } else {
+          H(s1e, s2o, 1);
+          H(s1o, s2e, 2);
+          addk(se, xk, s1e);
+          addk(so, xk, s1o);
+        }
+      }
+      te = se;
+      to = so;
+      if (gammaid != 1) {
+        oq_gam5x(g, te.data());
+        oq_gam5x(g, to.data());
+      }
+      const C x = S1.dot(L + (size_t)e * 2 * vs, te.data()) + S1.dot(L + (size_t)e * 2 * vs + vs, to.data());
+      xiinv[2 * ((size_t)(isub - 1) + 6 * (size_t)e)] = x.real();
+      xiinv[2 * ((size_t)(isub - 1) + 6 * (size_t)e) + 1] = x.imag();
+    }
+  }
+}
+
+// eigaverage: Jtime(2, nt, numEV, 9) at imom = 1; ESHFES 1 (loopops) or 2
+// (eigloopops_original = loopops of gamma5 x').
+extern "C" void oq_eigaverage(const oq_geom* g, const double* u, int numEV, int eigstart, int eigstep,
+                              const double* ze, const double* zo, double kappa, const double* R, const double* L,
+                              const double* scal, int eshfes, double* Jtime) {
+  const size_t vs = g->vsize();
+  const int nt = g->n[3];
+  const Space S2{g, 2, vs};
+  std::vector<double> z(2 * vs), cor(2 * vs, 0.0), y(2 * vs), J((size_t)2 * nt * 9);
+  std::memcpy(z.data(), ze, sizeof(double) * vs);
+  std::memcpy(z.data() + vs, zo, sizeof(double) * vs);
+  std::memset(Jtime, 0, sizeof(double) * 2 * nt * (size_t)numEV * 9);
+  for (int eig = 1; eig <= numEV; ++eig) {
+    const C t2 = S2.dot(L + (size_t)(eig - 1) * 2 * vs, z.data());
+    const C t1 = t2 * C(scal[2 * (eig - 1)], scal[2 * (eig - 1) + 1]);
+    S2.axpy(cor.data(), t1, R + (size_t)(eig - 1) * 2 * vs);
+    if (!(eig == eigstart || (eig > eigstart && (eig - eigstart) % eigstep == 0) || eig == numEV)) continue;
+    y = cor;
+    if (eshfes != 1) {
+      oq_gam5x(g, y.data());
+      oq_gam5x(g, y.data() + vs);
+    }
+    oq_average(g, u, ze, zo, y.data(), y.data() + vs, kappa, 1, 1, 9, nullptr, J.data());
+    for (int iop = 0; iop < 9; ++iop)
+      for (int t = 0; t < nt; ++t)
+        for (int ri = 0; ri < 2; ++ri)
+          Jtime[((((size_t)iop * numEV) + (eig - 1)) * nt + t) * 2 + ri] = J[((size_t)iop * nt + t) * 2 + ri];
+  }
+}

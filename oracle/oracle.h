@@ -171,6 +171,17 @@ void oq_twvev_sites(const oq_geom* g, const double* u, double kappa, double delt
                     int nsites, double* opertemp);
 
 // ---- gauge field helpers ----
+// Eigenmode subtraction of the Wilson loop driver (eigen.cpp).  R, L: room for
+// nGMRES[1] modes of two reference-layout halves each; evals: 2 nGMRES[1].
+int oq_eigmodes(const oq_geom* g, const double* u, int kind, const int nGMRES[2], int ncycles,
+                const double kappa[2], const double* se, const double* so, double* R, double* L,
+                double* evals, int* cycles);
+void oq_xigenerator(const oq_geom* g, const double* u, int numEV, double kappa, const double* R,
+                    const double* L, int gammaid, double* xiinv);
+void oq_eigaverage(const oq_geom* g, const double* u, int numEV, int eigstart, int eigstep,
+                   const double* ze, const double* zo, double kappa, const double* R,
+                   const double* L, const double* scal, int eshfes, double* Jtime);
+
 void oq_coldstart(const oq_geom* g, double* u);
 // The reference's pseudo-heatbath for the Wilson plaquette action at beta (sweep
 // C/cfgsprops.f90:1973-2001, staple G/gaugetools.f90:39-345, phbup / su2up / sprd1

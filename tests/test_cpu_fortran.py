@@ -3,7 +3,7 @@
 No Fortran compiler exists here, so the module is checked by parsing both files:
 every C prototype has a bind(C) interface of the same name, with the same number of
 arguments, each passed by value exactly where C passes by value (scalars and the opaque
-handles qq_ctx / qq_defl / qq_net), with the matching interoperable kind; every C struct
+handles qq_ctx / qq_defl / qq_net / qq_eig), with the matching interoperable kind; every C struct
 has a bind(C) derived type with the same members in the same order.  The shim module
 keeps the reference's procedure names and argument lists (Q/diracops.f90:264-599,
 Q/inverters.f90:302-487, 2871-3572, 4310-4465, Q/quark.f90:458-842), checked against the
@@ -14,7 +14,7 @@ from pathlib import Path
 import pytest
 
 INC = Path(__file__).resolve().parent.parent / "include"
-HANDLES = ("qq_ctx", "qq_defl", "qq_net")
+HANDLES = ("qq_ctx", "qq_defl", "qq_net", "qq_eig")
 
 
 def strip_c_comments(s):

@@ -1,0 +1,120 @@
+"""GPU parity of the eigenmode subtraction of the Wilson loop driver (qq_eigmodes,
+qq_xigenerator, qq_eigaverage: eigmodesofM, eigmodesofMprime, xigenerator, eigaverage,
+Q/disconloops.f90:1593-1937, 2573-2875, 465-838, 3239-3342) with the oracle's
+restatement (oracle/eigen.cpp, checked against numpy in test_cpu_eigen.py), through the C
+ABI, on heatbath configurations made by the oracle and uploaded.
+
+Both sides run the same deflated-restart iteration in a different summation order, so
+the kept modes agree up to the phase of each eigenvector.  What is compared is what does
+not depend on the phases: the eigenvalues (1e-9), the modes' residuals and left/right
+biorthogonality on the GPU's own vectors, xiinv (phase free: <L, S R> with <R, L> = 1,
+or <R, gamma5 S R> for unit R) and the eigaverage prefix sums (1e-8 of the largest
+entry).  Modes are compared over the leading run whose eigenvalues agree; a pair at the
+1e-8 acceptance border may be kept on one side only.  One case uses a 141-vector basis
+and 61 restart vectors, which takes the chunked multi-vector kernels (128 vectors per
+launch) and the tiled restart combination through more than one chunk."""
+import numpy as np
+import pytest
+
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+BC = (1, 1, 1, -1)
+KAPPA = (0.15, 0.0)
+
+
+def make(dims, seed, sweeps):
+    import baylorlqcd_b200 as qq
+
+    ol = oracle.OracleLattice(*dims, bc=BC)
+    u = ol.coldstart()
+    oracle.initlagfib(0, seed)
+    ol.heatbath(u, 5.8, sweeps)
+    ol.set_gauge(u)
+    lat = qq.Lattice(*dims, bc=BC)
+    lat.gauge_upload(u)
+    return ol, lat
+
+
+def leading_match(a, b, tol=1e-9):
+    n = 0
+    for x, y in zip(a, b):
+        if abs(x - y) > tol * max(1.0, abs(y)):
+            break
+        n += 1
+    return n
+
+
+def cvec(ol, full):
+    nv = ol.nvhalf
+    return (full[:, ..., :nv, 0::2] + 1j * full[:, ..., :nv, 1::2]).ravel()
+
+
+@pytest.fixture(scope="module")
+def small():
+    ol, lat = make((4, 4, 4, 4), 7, 20)
+    yield ol, lat
+    lat.close()
+
+
+@pytest.mark.parametrize("kind,nG,cyc", [(1, (30, 16), 40), (2, (30, 16), 40), (1, (140, 60), 4)])
+def test_eigenmodes_match_oracle(small, kind, nG, cyc):
+    ol, lat = small
+    se = so = None
+    if kind == 2:
+        oracle.initlagfib(0, 11)
+        se, so = ol.z4source()
+    ev_o, R_o, L_o, cyc_o = ol.eigmodes(kind, nG, cyc, KAPPA, se, so)
+    E = lat.eigenmodes(kind, nG, cyc, KAPPA, se, so)
+    assert E.cycles == cyc_o == cyc
+    n = leading_match(E.evals, ev_o)
+    assert len(ev_o) >= 4 and n >= min(E.num, len(ev_o)) - 2 and n >= 4, (E.evals, ev_o)
+    # the GPU's vectors: eigenpairs of the oracle's operator, biorthonormal
+    k = KAPPA[0]
+    R = np.stack([E.vector(j) for j in range(n)])
+    L = np.stack([E.vector(j, left=True) for j in range(n)])
+    for j in range(n):
+        r = R[j]
+        if kind == 1:
+            mr0 = r[0] - k * ol.hsingle(r[1], 0, 1)
+            mr1 = r[1] - k * ol.hsingle(r[0], 0, 2)
+            lam = E.evals[j]
+            bound = 1e-8
+        else:
+            g0, g1 = ol.gam5x(r[0]), ol.gam5x(r[1])
+            mr0 = g0 - k * ol.hsingle(g1, 0, 1)
+            mr1 = g1 - k * ol.hsingle(g0, 0, 2)
+            lam = E.evals[j].real
+            bound = 1e-5
+        res = np.concatenate([cvec(ol, mr0[None]) - lam * cvec(ol, r[0][None]),
+                              cvec(ol, mr1[None]) - lam * cvec(ol, r[1][None])])
+        assert np.linalg.norm(res) < bound, (j, np.linalg.norm(res))
+    G = np.array([[np.vdot(cvec(ol, R[i]), cvec(ol, L[j])) for j in range(n)] for i in range(n)])
+    np.testing.assert_allclose(G, np.eye(n), atol=1e-8)
+    # phase-free derived quantities against the oracle's
+    xi_g = E.xigenerator(k)[:n]
+    xi_o = ol.xigenerator(R_o[:n], L_o[:n], k, kind)
+    assert np.abs(xi_g - xi_o).max() <= 1e-8 * np.abs(xi_o).max()
+    oracle.initlagfib(0, 5)
+    ze, zo = ol.z4source()
+    scal = 1.0 / ev_o[:n]
+    for eigstart, eigstep in ((1, 1), (2, 3)):
+        J_o = ol.eigaverage(ze, zo, k, R_o[:n], L_o[:n], scal, kind, eigstart, eigstep)
+        J_g = E.eigaverage(ze, zo, k, np.concatenate([scal, np.zeros(E.num - n)]), eigstart, eigstep)
+        # counts up to the common leading run; the GPU's own last count may differ
+        m = n if E.num == n else n - 1
+        assert np.abs(J_g[:, :m] - J_o[:, :m]).max() <= 1e-8 * np.abs(J_o).max()
+    E.close()
+
+
+def test_unit_source_needs_no_start_vector_and_bad_arguments(small):
+    import baylorlqcd_b200 as qq
+
+    ol, lat = small
+    with pytest.raises(qq.QQError):
+        lat.eigenmodes(2, (20, 10), 2, KAPPA)  # kind 2 without a start vector
+    with pytest.raises(qq.QQError):
+        lat.eigenmodes(1, (20, 20), 2, KAPPA)  # k must be below m
+    with pytest.raises(qq.QQError):
+        lat.eigenmodes(3, (20, 10), 2, KAPPA)

@@ -41,6 +41,7 @@ EXPORTED = [
     "qq_net_set_weights", "qq_net_apply", "qq_net_grad", "qq_net_train", "qq_fgmres", "qq_pionrho", "qq_twvev", "qq_twaverage", "qq_twistdiscon", "qq_average", "qq_momfacs",
     "qq_fgmresdr", "qq_fermprop_uneven",
     "qq_eigmodes", "qq_eig_destroy", "qq_eig_info", "qq_eig_vector", "qq_xigenerator", "qq_eigaverage",
+    "qq_ppcoeffs", "qq_ppaverage", "qq_xipolygenerator", "qq_generalaverage",
 ]
 
 
@@ -170,6 +171,10 @@ def load_library() -> C.CDLL:
         "qq_eig_vector": ([P, I, I, P, P], I),
         "qq_xigenerator": ([P, P, D, DP], I),
         "qq_eigaverage": ([P, P, P, P, D, DP, I, I, P], I),
+        "qq_ppcoeffs": ([P, P, P, D, I, DP], I),
+        "qq_ppaverage": ([P, I, DP, P, P, P, P, D, I, P], I),
+        "qq_xipolygenerator": ([P, P, D, DP, DP], I),
+        "qq_generalaverage": ([P, P, P, P, P, P, P, D, I, I, DP, DP, DP, DP, P], I),
         "qq_twaverage": ([P, P, P, P, P, D, D, IP, I, I, I, I, I, P], I),
         "qq_twistdiscon": ([P, I, I, DP, P, D, IP, I, I, I, I, I, P, P, P], I),
         "qq_heatbath": ([P, D, I, C.c_ulonglong, P, DP], I),
@@ -250,6 +255,14 @@ class Deflation:
             pass
 
 
+def _c2(a) -> np.ndarray:
+    """Complex vector as contiguous (n, 2) doubles."""
+    a = np.asarray(a, complex).ravel()
+    out = np.zeros((len(a), 2))
+    out[:, 0], out[:, 1] = a.real, a.imag
+    return out
+
+
 class Eigenmodes:
     """Kept eigenmodes of M (kind 1) or of M gamma5 (kind 2) on the device
     (eigmodesofM / eigmodesofMprime, Q/disconloops.f90:1593-1937, 2573-2875)."""
@@ -298,6 +311,16 @@ class Eigenmodes:
                                           s.ctypes.data_as(C.POINTER(C.c_double)), int(eigstart), int(eigstep),
                                           _ptr(J)))
         return J[:, :self.num]
+
+    def xipolygenerator(self, kappa: float, co):
+        """xipolygenerator (Q/disconloops.f90:847-1584) with coefficients co (complex (8,)):
+        xiinv as complex (num, 6)."""
+        xi = np.zeros((max(self.num, 1), 6, 2))
+        c2 = _c2(co)
+        _check(self.lat.lib.qq_xipolygenerator(self.lat._ctx, self._h, float(kappa),
+                                               c2.ctypes.data_as(C.POINTER(C.c_double)),
+                                               xi.ctypes.data_as(C.POINTER(C.c_double))))
+        return (xi[..., 0] + 1j * xi[..., 1])[:self.num]
 
     def close(self):
         if self._h:
@@ -473,6 +496,33 @@ class Lattice:
         mf = None if momfac is None else np.ascontiguousarray(momfac, dtype=np.float64)
         _check(self.lib.qq_average(self._ctx, _ptr(be), _ptr(bo), _ptr(xe), _ptr(xo), float(kappa), int(nsub),
                                    int(nmom), int(nop), _ptr(mf) if mf is not None else None, _ptr(J)))
+        return J
+
+    def ppcoeffs(self, be, bo, kappa, p):
+        """qq_ppcoeffs: the least-squares polynomial of ppaverage* (complex (p,))."""
+        co = np.zeros((p, 2))
+        _check(self.lib.qq_ppcoeffs(self._ctx, _ptr(be), _ptr(bo), float(kappa), int(p),
+                                    co.ctypes.data_as(C.POINTER(C.c_double))))
+        return co[:, 0] + 1j * co[:, 1]
+
+    def ppaverage(self, p, co, be, bo, xe, xo, kappa, nsub=6):
+        """qq_ppaverage (ppaverage p = 5, ppaverage1 p = 8, ppaverage2 p = 11) at imom = 1:
+        Jtime as (9, nsub, nt, 2)."""
+        J = np.zeros((9, nsub, self.dims[3], 2))
+        c2 = _c2(co)
+        _check(self.lib.qq_ppaverage(self._ctx, int(p), c2.ctypes.data_as(C.POINTER(C.c_double)), _ptr(be), _ptr(bo),
+                                     _ptr(xe), _ptr(xo), float(kappa), int(nsub), _ptr(J)))
+        return J
+
+    def generalaverage(self, m: "Eigenmodes", mp: "Eigenmodes", ze, zo, xe, xo, kappa, co11, co8, co5, copoly,
+                       eigstart=1, eigstep=1):
+        """qq_generalaverage at imom = 1: Jave as (9, 10, numEV_MAX, 6, nt, 2)."""
+        ne = max(1, m.num, mp.num)
+        J = np.zeros((9, 10, ne, 6, self.dims[3], 2))
+        cs = [_c2(c) for c in (co11, co8, co5, copoly)]
+        _check(self.lib.qq_generalaverage(self._ctx, m._h, mp._h, _ptr(ze), _ptr(zo), _ptr(xe), _ptr(xo), float(kappa),
+                                          int(eigstart), int(eigstep),
+                                          *[c.ctypes.data_as(C.POINTER(C.c_double)) for c in cs], _ptr(J)))
         return J
 
     def eigenmodes(self, kind, nGMRES, ncycles, kappa, se=None, so=None) -> Eigenmodes:

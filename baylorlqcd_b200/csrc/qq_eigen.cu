@@ -617,6 +617,121 @@ void compose_eigaverage(const std::vector<double>& T, const std::vector<cd>& pro
   }
 }
 
+// (M y)_e = y_e - kappa H_eo y_o, (M y)_o = y_o - kappa H_oe y_e on full vectors.
+int apply_m(qq_ctx* c, void* out, const void* in, double kappa, size_t hn) {
+  const Spinor ie = half_of(const_cast<void*>(in), hn, 0), io = half_of(const_cast<void*>(in), hn, 1);
+  const Spinor oe = half_of(out, hn, 0), oo = half_of(out, hn, 1);
+  QQ_TRY(op_hsingle(c, oe, io, 0, 0));
+  QQ_TRY(lin(c, oe, cimm(1.0), ie, cimm(-kappa), oe));
+  QQ_TRY(op_hsingle(c, oo, ie, 0, 1));
+  QQ_TRY(lin(c, oo, cimm(1.0), io, cimm(-kappa), oo));
+  return QQ_OK;
+}
+
+// The least-squares polynomials of ppaverage (p = 5), ppaverage1 (p = 8) and ppaverage2
+// (p = 11), Q/disconloops.f90:6885-7434, 6290-6883, 5740-6288: the terms (coefficient
+// index, power index, both 1-based: co_c M^(v-1) b) added at levels isub = 2..6.  The
+// p = 5 form reuses its fifth coefficient on the powers 6, 7, 8 (:7217-7293).
+struct PolyTerm {
+  int co, v;
+};
+const std::vector<PolyTerm>& poly_terms(int p, int isub) {
+  static const std::vector<PolyTerm> none;
+  static const std::vector<PolyTerm> t11[7] = {{}, {}, {{1, 1}, {2, 2}, {3, 3}, {4, 4}}, {{5, 5}}, {{6, 6}}, {{7, 7}},
+                                               {{8, 8}, {9, 9}, {10, 10}, {11, 11}}};
+  static const std::vector<PolyTerm> t8[7] = {{}, {}, {{1, 1}, {2, 2}, {3, 3}, {4, 4}}, {{5, 5}}, {{6, 6}}, {{7, 7}},
+                                              {{8, 8}}};
+  static const std::vector<PolyTerm> t5[7] = {{}, {}, {{1, 1}, {2, 2}, {3, 3}, {4, 4}}, {{5, 5}}, {{5, 6}}, {{5, 7}},
+                                              {{5, 8}}};
+  if (isub < 1 || isub > 6) return none;
+  return p == 11 ? t11[isub] : p == 8 ? t8[isub] : t5[isub];
+}
+int poly_powers(int p) { return p == 11 ? 12 : p == 8 ? 9 : 8; }  // vectors M^0 b .. kept
+
+// P[i] = M^i b for i < n (full vectors)
+int krylov_powers(qq_ctx* c, const void* b, double kappa, size_t hn, int n, Basis& P) {
+  QQ_TRY(P.init(2 * hn, n));
+  QQ_CK(cudaMemcpyAsync(P.v(0), b, 2 * hn * 16, cudaMemcpyDeviceToDevice, c->st));
+  for (int i = 1; i < n; ++i) QQ_TRY(apply_m(c, P.v(i), P.v(i - 1), kappa, hn));
+  return QQ_OK;
+}
+
+// sub_isub accumulated in place: sub += sum over the level's terms co_c P[v-1]
+int poly_accumulate(qq_ctx* c, void* sub, const Basis& P, const double* co, int p, int isub, size_t hn) {
+  for (const PolyTerm& t : poly_terms(p, isub)) {
+    const cd a(co[2 * (t.co - 1)], co[2 * (t.co - 1) + 1]);
+    for (int h = 0; h < 2; ++h)
+      QQ_TRY(lin(c, half_of(sub, hn, h), cimm(1.0), half_of(sub, hn, h), cimm(a.real(), a.imag()),
+                 half_of(P.v(t.v - 1), hn, h)));
+  }
+  return QQ_OK;
+}
+
+int load_full(qq_ctx* c, const double* e, const double* o, void* full, size_t hn) {
+  const double* d = nullptr;
+  QQ_TRY(stage_in(c, 0, e, c->ref_doubles(), &d));
+  QQ_TRY(ref_to_field(c, d, 0, half_of(full, hn, 0)));
+  QQ_TRY(stage_in(c, 1, o, c->ref_doubles(), &d));
+  QQ_TRY(ref_to_field(c, d, 1, half_of(full, hn, 1)));
+  return QQ_OK;
+}
+
+// ppaverage*: Jtime(2, nt, nsub, 9) at imom = 1 (Fortran order), x and b full vectors in
+// GPU layout, b also in reference layout on the device (be_ref, bo_ref).
+int ppaverage_dev(qq_ctx* c, int p, const double* co, const void* b, const double* be_ref, const double* bo_ref,
+                  const void* x, double kappa, int nsub, double* J) {
+  const size_t hn = (size_t)12 * c->g.vh, nv = c->ref_doubles();
+  const int nt = c->g.n[3], V = 2 * c->g.vh;
+  Basis P, Y;
+  QQ_TRY(krylov_powers(c, b, kappa, hn, poly_powers(p), P));
+  QQ_TRY(Y.init(2 * hn, 2));  // sub and y
+  QQ_CK(cudaMemsetAsync(Y.v(0), 0, 2 * hn * 16, c->st));
+  void *val = nullptr, *Jd = nullptr, *ref = nullptr;
+  QQ_CK(ws_get(c, kWsVal, sizeof(double) * 18 * (size_t)V, &val));
+  QQ_CK(ws_get(c, kWsJ, sizeof(double) * 18 * (size_t)nt, &Jd));
+  QQ_CK(ws_get(c, kWsRef, sizeof(double) * 2 * nv, &ref));
+  double* ye = static_cast<double*>(ref);
+  std::vector<double> T((size_t)18 * nt);
+  std::memset(J, 0, sizeof(double) * 2 * (size_t)nt * nsub * 9);
+  for (int isub = 1; isub <= nsub; ++isub) {
+    QQ_TRY(poly_accumulate(c, Y.v(0), P, co, p, isub, hn));
+    for (int h = 0; h < 2; ++h)
+      QQ_TRY(lin(c, half_of(Y.v(1), hn, h), cimm(1.0), half_of(const_cast<void*>(x), hn, h), cimm(-1.0),
+                 half_of(Y.v(0), hn, h)));
+    QQ_TRY(field_to_ref(c, half_of(Y.v(1), hn, 0), 0, ye));
+    QQ_TRY(field_to_ref(c, half_of(Y.v(1), hn, 1), 1, ye + nv));
+    QQ_TRY(loop_slices(c, ye, ye + nv, be_ref, bo_ref, isub == 1 ? 0 : 1, static_cast<double*>(val),
+                       static_cast<double*>(Jd), T.data()));
+    for (int iop = 0; iop < 9; ++iop)
+      for (int it = 0; it < nt; ++it)
+        for (int ri = 0; ri < 2; ++ri)
+          J[((((size_t)iop * nsub) + (isub - 1)) * nt + it) * 2 + ri] =
+              (iop < 4 ? kappa : 1.0) * T[((size_t)iop * nt + it) * 2 + ri];
+  }
+  return QQ_OK;
+}
+
+// xipolygenerator: xiinv(2, 6, n) = <L_j, gamma5 sub_isub(R_j)> with the p = 8 terms.
+int xipoly_dev(qq_ctx* c, const qq_eig* e, double kappa, const double* co, double* xiinv) {
+  const size_t hn = e->half_nel;
+  Basis Y;
+  QQ_TRY(Y.init(2 * hn, 2));
+  for (int j = 0; j < e->num; ++j) {
+    Basis P;
+    QQ_TRY(krylov_powers(c, e->r(j), kappa, hn, poly_powers(8), P));
+    QQ_CK(cudaMemsetAsync(Y.v(0), 0, 2 * hn * 16, c->st));
+    for (int isub = 1; isub <= 6; ++isub) {
+      QQ_TRY(poly_accumulate(c, Y.v(0), P, co, 8, isub, hn));
+      QQ_TRY(g5(c, Y.v(0), Y.v(1), 2));
+      cd x;
+      QQ_TRY(dot_full(c, e->l(j), Y.v(1), hn, &x));
+      xiinv[2 * ((size_t)(isub - 1) + 6 * (size_t)j)] = x.real();
+      xiinv[2 * ((size_t)(isub - 1) + 6 * (size_t)j) + 1] = x.imag();
+    }
+  }
+  return QQ_OK;
+}
+
 }  // namespace
 }  // namespace qq
 
@@ -804,5 +919,218 @@ extern "C" int qq_eigaverage(qq_ctx* c, const qq_eig* e, const double* ze, const
   std::vector<double> out(2 * (size_t)c->g.n[3] * std::max(1, e->num) * 9);
   compose_eigaverage(T, proj, scal, e->num, c->g.n[3], eigstart, eigstep, kappa, out.data());
   QQ_CK(cudaMemcpy(Jtime, out.data(), sizeof(double) * 2 * (size_t)c->g.n[3] * e->num * 9, cudaMemcpyDefault));
+  return QQ_OK;
+}
+
+extern "C" int qq_ppcoeffs(qq_ctx* c, const double* be, const double* bo, double kappa, int p, double* co) {
+  if (!c || !be || !bo || !co) return set_error(QQ_BAD_ARG, "null argument");
+  if (p < 1 || p > 16) return set_error(QQ_BAD_ARG, "p must be 1..16");
+  if (!c->have_gauge) return set_error(QQ_BAD_ARG, "no gauge field uploaded");
+  QQ_CK(cudaSetDevice(c->device));
+  const size_t hn = (size_t)12 * c->g.vh;
+  DevBuf b, h;
+  QQ_CK(b.alloc(2 * hn * 16));
+  QQ_CK(h.alloc(sizeof(double) * 2 * (p + 1)));
+  QQ_TRY(load_full(c, be, bo, b.p, hn));
+  Basis P;
+  QQ_TRY(krylov_powers(c, b.p, kappa, hn, p + 1, P));
+  // normal equations G co = r, G(a, b) = <M^a b, M^b b>, r(a) = <M^a b, b> (a, b = 1..p)
+  dense::Mat G(p, p);
+  std::vector<dense::cd> r(p);
+  std::vector<double> hv(2 * (p + 1));
+  for (int bb = 0; bb <= p; ++bb) {
+    QQ_TRY(mdot(c, P, p + 1, P.v(bb), h.as<double>()));
+    QQ_TRY(read_scalars(c, h.as<double>(), 2 * (p + 1), hv.data()));
+    for (int a = 1; a <= p; ++a) {
+      const dense::cd v(hv[2 * a], hv[2 * a + 1]);
+      if (bb == 0)
+        r[a - 1] = v;
+      else
+        G(a - 1, bb - 1) = v;
+    }
+  }
+  if (!dense::lu_solve(G, r)) return set_error(QQ_SINGULAR, "singular normal equations");
+  for (int a = 0; a < p; ++a) {
+    co[2 * a] = r[a].real();
+    co[2 * a + 1] = r[a].imag();
+  }
+  return QQ_OK;
+}
+
+extern "C" int qq_ppaverage(qq_ctx* c, int p, const double* co, const double* be, const double* bo, const double* xe,
+                            const double* xo, double kappa, int nsub, double* Jtime) {
+  if (!c || !co || !be || !bo || !xe || !xo || !Jtime) return set_error(QQ_BAD_ARG, "null argument");
+  if (p != 5 && p != 8 && p != 11) return set_error(QQ_BAD_ARG, "p must be 5, 8 or 11");
+  if (nsub < 1 || nsub > 6) return set_error(QQ_BAD_ARG, "nsub must be 1..6");
+  if (!c->have_gauge) return set_error(QQ_BAD_ARG, "no gauge field uploaded");
+  QQ_CK(cudaSetDevice(c->device));
+  const size_t hn = (size_t)12 * c->g.vh, nv = c->ref_doubles();
+  DevBuf bx, bref;
+  QQ_CK(bx.alloc(2 * 2 * hn * 16));
+  QQ_CK(bref.alloc(sizeof(double) * 2 * nv));
+  void* b = bx.p;
+  void* x = static_cast<char*>(bx.p) + 2 * hn * 16;
+  QQ_TRY(load_full(c, be, bo, b, hn));
+  QQ_CK(cudaMemcpyAsync(bref.p, be, sizeof(double) * nv, cudaMemcpyDefault, c->st));
+  QQ_CK(cudaMemcpyAsync(bref.as<double>() + nv, bo, sizeof(double) * nv, cudaMemcpyDefault, c->st));
+  QQ_TRY(load_full(c, xe, xo, x, hn));
+  std::vector<double> J(2 * (size_t)c->g.n[3] * nsub * 9);
+  QQ_TRY(ppaverage_dev(c, p, co, b, bref.as<double>(), bref.as<double>() + nv, x, kappa, nsub, J.data()));
+  QQ_CK(cudaMemcpy(Jtime, J.data(), sizeof(double) * J.size(), cudaMemcpyDefault));
+  return QQ_OK;
+}
+
+extern "C" int qq_xipolygenerator(qq_ctx* c, const qq_eig* e, double kappa, const double* co, double* xiinv) {
+  if (!c || !e || !co || !xiinv) return set_error(QQ_BAD_ARG, "null argument");
+  if (e->ctx != c) return set_error(QQ_BAD_ARG, "handle belongs to another context");
+  QQ_CK(cudaSetDevice(c->device));
+  std::vector<double> xi(2 * 6 * (size_t)std::max(1, e->num));
+  QQ_TRY(xipoly_dev(c, e, kappa, co, xi.data()));
+  QQ_CK(cudaMemcpy(xiinv, xi.data(), sizeof(double) * 12 * (size_t)e->num, cudaMemcpyDefault));
+  return QQ_OK;
+}
+
+extern "C" int qq_generalaverage(qq_ctx* c, const qq_eig* m, const qq_eig* mp, const double* ze, const double* zo,
+                                 const double* xe, const double* xo, double kappa, int eigstart, int eigstep,
+                                 const double* co11, const double* co8, const double* co5, const double* copoly,
+                                 double* Jave) {
+  if (!c || !m || !mp || !ze || !zo || !xe || !xo || !co11 || !co8 || !co5 || !copoly || !Jave)
+    return set_error(QQ_BAD_ARG, "null argument");
+  if (m->ctx != c || mp->ctx != c) return set_error(QQ_BAD_ARG, "handle belongs to another context");
+  if (m->kind != 1 || mp->kind != 2) return set_error(QQ_BAD_ARG, "need the modes of M (kind 1) and of M gamma5 (kind 2)");
+  if (eigstart < 1 || eigstep < 1) return set_error(QQ_BAD_ARG, "eigstart and eigstep must be positive");
+  QQ_CK(cudaSetDevice(c->device));
+  const int nt = c->g.n[3], nsub = 6, nsty = 10;
+  const size_t hn = (size_t)12 * c->g.vh, nv = c->ref_doubles();
+  const int n1 = m->num, n2 = mp->num, nmax = std::max(n1, n2);
+  // device copies: z and x (reference layout), z and a zero solution (GPU layout)
+  DevBuf zr, zx, zero;
+  QQ_CK(zr.alloc(sizeof(double) * 4 * nv));
+  double* zref = zr.as<double>();
+  QQ_CK(cudaMemcpyAsync(zref, ze, sizeof(double) * nv, cudaMemcpyDefault, c->st));
+  QQ_CK(cudaMemcpyAsync(zref + nv, zo, sizeof(double) * nv, cudaMemcpyDefault, c->st));
+  QQ_CK(cudaMemcpyAsync(zref + 2 * nv, xe, sizeof(double) * nv, cudaMemcpyDefault, c->st));
+  QQ_CK(cudaMemcpyAsync(zref + 3 * nv, xo, sizeof(double) * nv, cudaMemcpyDefault, c->st));
+  QQ_CK(zx.alloc(2 * hn * 16));
+  QQ_CK(zero.alloc(2 * hn * 16));
+  QQ_CK(cudaMemsetAsync(zero.p, 0, zero.bytes, c->st));
+  QQ_TRY(ref_to_field(c, zref, 0, half_of(zx.p, hn, 0)));
+  QQ_TRY(ref_to_field(c, zref + nv, 1, half_of(zx.p, hn, 1)));
+  // NS: loop operators of the solution, operators 1..4 times kappa
+  std::vector<double> NS((size_t)18 * nt);
+  {
+    void *val = nullptr, *Jd = nullptr;
+    QQ_CK(ws_get(c, kWsVal, sizeof(double) * 18 * (size_t)2 * c->g.vh, &val));
+    QQ_CK(ws_get(c, kWsJ, sizeof(double) * 18 * (size_t)nt, &Jd));
+    QQ_TRY(loop_slices(c, zref + 2 * nv, zref + 3 * nv, zref, zref + nv, 0, static_cast<double*>(val),
+                       static_cast<double*>(Jd), NS.data()));
+    for (int iop = 0; iop < 4; ++iop)
+      for (int k = 0; k < 2 * nt; ++k) NS[(size_t)iop * 2 * nt + k] *= kappa;
+  }
+  // PS = -average(z, 0); PP = -ppaverage2(0), PP4 = -ppaverage(0), PP7 = -ppaverage1(0)
+  std::vector<double> PS((size_t)2 * nt * nsub * 9), PP(PS.size()), PP4(PS.size()), PP7(PS.size());
+  {
+    DevBuf zref0;
+    QQ_CK(zref0.alloc(sizeof(double) * nv));
+    QQ_CK(cudaMemsetAsync(zref0.p, 0, zref0.bytes, c->st));
+    QQ_TRY(qq_average(c, zref, zref + nv, zref0.as<double>(), zref0.as<double>(), kappa, nsub, 1, 9, nullptr,
+                      PS.data()));
+  }
+  QQ_TRY(ppaverage_dev(c, 11, co11, zx.p, zref, zref + nv, zero.p, kappa, nsub, PP.data()));
+  QQ_TRY(ppaverage_dev(c, 5, co5, zx.p, zref, zref + nv, zero.p, kappa, nsub, PP4.data()));
+  QQ_TRY(ppaverage_dev(c, 8, co8, zx.p, zref, zref + nv, zero.p, kappa, nsub, PP7.data()));
+  for (size_t i = 0; i < PS.size(); ++i) {
+    PS[i] = -PS[i];
+    PP[i] = -PP[i];
+    PP4[i] = -PP4[i];
+    PP7[i] = -PP7[i];
+  }
+  // the eigenmode corrections from each mode's traces
+  std::vector<double> T1, T2;
+  std::vector<cd> p1, p2;
+  QQ_TRY(mode_traces(c, m, zref, zref + nv, T1, p1));
+  QQ_TRY(mode_traces(c, mp, zref, zref + nv, T2, p2));
+  std::vector<double> s1(2 * (size_t)std::max(1, n1)), s2(2 * (size_t)std::max(1, n2));
+  for (int j = 0; j < n1; ++j) {
+    const cd v = nr_inv(m->lam[j]);
+    s1[2 * j] = v.real();
+    s1[2 * j + 1] = v.imag();
+  }
+  for (int j = 0; j < n2; ++j) {
+    s2[2 * j] = 1.0 / mp->lam[j].real();
+    s2[2 * j + 1] = 0.0;
+  }
+  std::vector<double> xi1(12 * (size_t)std::max(1, n1)), xi2(12 * (size_t)std::max(1, n2)),
+      xip(12 * (size_t)std::max(1, n2));
+  QQ_TRY(qq_xigenerator(c, m, kappa, xi1.data()));
+  QQ_TRY(qq_xigenerator(c, mp, kappa, xi2.data()));
+  QQ_TRY(xipoly_dev(c, mp, kappa, copoly, xip.data()));
+  const size_t blk1 = (size_t)2 * nt * std::max(1, n1) * 9, blk2 = (size_t)2 * nt * std::max(1, n2) * 9;
+  std::vector<double> ES(blk1), HFES(blk2), ESPS(blk1 * nsub), HFESPS(blk2 * nsub), HFESPOLY(blk2 * nsub);
+  compose_eigaverage(T1, p1, s1.data(), n1, nt, eigstart, eigstep, kappa, ES.data());
+  compose_eigaverage(T2, p2, s2.data(), n2, nt, eigstart, eigstep, kappa, HFES.data());
+  std::vector<double> sc(2 * (size_t)std::max(n1, n2) + 2);
+  for (int isub = 0; isub < nsub; ++isub) {
+    for (int j = 0; j < n1; ++j) {
+      sc[2 * j] = xi1[2 * ((size_t)isub + 6 * j)];
+      sc[2 * j + 1] = xi1[2 * ((size_t)isub + 6 * j) + 1];
+    }
+    compose_eigaverage(T1, p1, sc.data(), n1, nt, eigstart, eigstep, kappa, ESPS.data() + isub * blk1);
+    for (int j = 0; j < n2; ++j) {
+      sc[2 * j] = xi2[2 * ((size_t)isub + 6 * j)];
+      sc[2 * j + 1] = xi2[2 * ((size_t)isub + 6 * j) + 1];
+    }
+    compose_eigaverage(T2, p2, sc.data(), n2, nt, eigstart, eigstep, kappa, HFESPS.data() + isub * blk2);
+    for (int j = 0; j < n2; ++j) {
+      sc[2 * j] = xip[2 * ((size_t)isub + 6 * j)];
+      sc[2 * j + 1] = xip[2 * ((size_t)isub + 6 * j) + 1];
+    }
+    compose_eigaverage(T2, p2, sc.data(), n2, nt, eigstart, eigstep, kappa, HFESPOLY.data() + isub * blk2);
+  }
+  // generalaverage's styles at imom = 1 (Q/disconloops.f90:283-329); a mode count beyond
+  // one side's modes reads that side's (zero) entries, as the reference's arrays do
+  auto ns = [&](int iop, int t, int ri) { return NS[((size_t)iop * nt + t) * 2 + ri]; };
+  auto lvl = [&](const std::vector<double>& A, int iop, int isub, int t, int ri) {
+    return A[((((size_t)iop * nsub) + isub) * nt + t) * 2 + ri];
+  };
+  auto eg = [&](const std::vector<double>& A, int n, size_t off, int iop, int e, int t, int ri) {
+    return e < n ? A[off + ((((size_t)iop * n) + e) * nt + t) * 2 + ri] : 0.0;
+  };
+  const size_t total = (size_t)2 * nt * nsub * std::max(1, nmax) * nsty * 9;
+  std::vector<double> out(total, 0.0);
+  for (int iop = 0; iop < 9; ++iop)
+    for (int sty = 1; sty <= nsty; ++sty)
+      for (int e = 0; e < nmax; ++e)
+        for (int isub = 0; isub < nsub; ++isub)
+          for (int t = 0; t < nt; ++t)
+            for (int ri = 0; ri < 2; ++ri) {
+              const double N = ns(iop, t, ri);
+              double v = 0.0;
+              bool set = true;
+              switch (sty) {
+                case 1: set = e == 0 && isub == 0; v = N; break;
+                case 2: set = e == 0; v = N - lvl(PS, iop, isub, t, ri); break;
+                case 3: set = isub == 0; v = N - eg(ES, n1, 0, iop, e, t, ri); break;
+                case 4: set = isub == 0; v = N - eg(HFES, n2, 0, iop, e, t, ri); break;
+                case 5:
+                  v = N - eg(ES, n1, 0, iop, e, t, ri) -
+                      (lvl(PS, iop, isub, t, ri) - eg(ESPS, n1, isub * blk1, iop, e, t, ri));
+                  break;
+                case 6:
+                  v = N - eg(HFES, n2, 0, iop, e, t, ri) -
+                      (lvl(PS, iop, isub, t, ri) - eg(HFESPS, n2, isub * blk2, iop, e, t, ri));
+                  break;
+                case 7: set = e == 0; v = N - lvl(PP, iop, isub, t, ri); break;
+                case 8: set = e == 0; v = N - lvl(PP4, iop, isub, t, ri); break;
+                case 9: set = e == 0; v = N - lvl(PP7, iop, isub, t, ri); break;
+                default:
+                  v = N - eg(HFES, n2, 0, iop, e, t, ri) -
+                      (lvl(PP7, iop, isub, t, ri) - eg(HFESPOLY, n2, isub * blk2, iop, e, t, ri));
+                  break;
+              }
+              if (!set) continue;
+              out[((((((size_t)iop * nsty) + (sty - 1)) * std::max(1, nmax) + e) * nsub + isub) * nt + t) * 2 + ri] = v;
+            }
+  QQ_CK(cudaMemcpy(Jave, out.data(), sizeof(double) * out.size(), cudaMemcpyDefault));
   return QQ_OK;
 }

@@ -369,6 +369,41 @@ int qq_xigenerator(qq_ctx* ctx, const qq_eig* eig, double kappa, double* xiinv);
  * Jtime(:, :, :, 1, :) (its momentum slots 2..5 stay zero, as its momfac is zero). */
 int qq_eigaverage(qq_ctx* ctx, const qq_eig* eig, const double* ze, const double* zo, double kappa,
                   const double* scal, int eigstart, int eigstep, double* Jtime);
+/* The least-squares polynomial of ppaverage (p = 5), ppaverage1 (p = 8), ppaverage2
+ * (p = 11) and xipolygenerator (p = 8), Q/disconloops.f90:6885-7434, 6290-6883,
+ * 5740-6288, 847-1584: co(2, p) (host or device) solving the normal equations
+ * sum_b <M^a z, M^b z> co_b = <M^a z, z> (a, b = 1..p) of min || z - sum_b co_b M^b z ||,
+ * M = 1 - kappa D on the full lattice, z = (be, bo).  The reference fits these once, on
+ * the first noise (psignal, Q/shift.f90:45), and reuses them. */
+int qq_ppcoeffs(qq_ctx* ctx, const double* be, const double* bo, double kappa, int p, double* co);
+/* ppaverage / ppaverage1 / ppaverage2 (p = 5, 8, 11) at imom = 1: level isub = 1 the
+ * solution x, level isub >= 2 x - sub_isub with sub_isub = sum of co_c M^(v-1) b over the
+ * terms of levels 2..isub (level 2: c = v = 1..4; then one term per level, c = v = 5, 6,
+ * 7 and for p = 11 the four terms 8..11 at level 6; p = 5 reuses c = 5 with v = 6, 7, 8),
+ * through loopops (ksub 1 on levels >= 2) and spacesum; operators 1..4 times kappa.
+ * Jtime(2, nt, nsub, 9), Fortran order, host or device; nsub <= 6. */
+int qq_ppaverage(qq_ctx* ctx, int p, const double* co, const double* be, const double* bo,
+                 const double* xe, const double* xo, double kappa, int nsub, double* Jtime);
+/* xipolygenerator Q/disconloops.f90:847-1584: xiinv(2, 6, numEV) = <L_j, gamma5 sub_isub R_j>
+ * with the p = 8 terms above applied to each mode R_j and coefficients co(2, 8) (the
+ * reference fits them on a noise with qq_ppcoeffs for gamma5 modes, and sets them to 1
+ * otherwise). */
+int qq_xipolygenerator(qq_ctx* ctx, const qq_eig* eig, double kappa, const double* co, double* xiinv);
+/* generalaverage Q/disconloops.f90:119-333 for one noise z and its solution x (M x = z):
+ * Jave(2, nt, 6, numEV_MAX, 10, 9) (Fortran order, host or device; numEV_MAX the larger
+ * mode count) at imom = 1, zero where a style is not defined, with
+ *   NS = loopops of x (nsaverage :3079-3143),   PS = -average(z, 0) (qq_average),
+ *   ES / HFES = qq_eigaverage of m (1/lambda) / of mp (1/lambda'),
+ *   ESPS / HFESPS = qq_eigaverage with xiinv(:, isub, :) of m / mp,
+ *   HFESPOLY = qq_eigaverage of mp with qq_xipolygenerator(mp, copoly),
+ *   PP, PP4, PP7 = -qq_ppaverage(0) with p = 11 (co11), 5 (co5), 8 (co8):
+ * style 1 NS (mode 1, level 1); 2 NS - PS (mode 1); 3 NS - ES (level 1); 4 NS - HFES
+ * (level 1); 5 NS - ES - (PS - ESPS); 6 NS - HFES - (PS - HFESPS); 7 NS - PP, 8 NS - PP4,
+ * 9 NS - PP7 (mode 1); 10 NS - HFES - (PP7 - HFESPOLY).  m: kind 1, mp: kind 2. */
+int qq_generalaverage(qq_ctx* ctx, const qq_eig* m, const qq_eig* mp, const double* ze, const double* zo,
+                      const double* xe, const double* xo, double kappa, int eigstart, int eigstep,
+                      const double* co11, const double* co8, const double* co5, const double* copoly,
+                      double* Jave);
 
 /* ---- file formats (host memory; no device needed) ----
  * Fortran unformatted sequential files, as the reference writes them: every record is

@@ -478,6 +478,45 @@ module qqcd_gpu
       real(c_double), intent(out) :: Jtime(*)
       integer(c_int) :: st
     end function qq_eigaverage
+    function qq_ppcoeffs(ctx, be, bo, kappa, p, co) bind(C, name="qq_ppcoeffs") result(st)
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: ctx
+      real(c_double), intent(in) :: be(*), bo(*)
+      real(c_double), value :: kappa
+      integer(c_int), value :: p
+      real(c_double), intent(out) :: co(*)
+      integer(c_int) :: st
+    end function qq_ppcoeffs
+    function qq_ppaverage(ctx, p, co, be, bo, xe, xo, kappa, nsub, Jtime) bind(C, name="qq_ppaverage") result(st)
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: p
+      real(c_double), intent(in) :: co(*)
+      real(c_double), intent(in) :: be(*), bo(*), xe(*), xo(*)
+      real(c_double), value :: kappa
+      integer(c_int), value :: nsub
+      real(c_double), intent(out) :: Jtime(*)
+      integer(c_int) :: st
+    end function qq_ppaverage
+    function qq_xipolygenerator(ctx, eig, kappa, co, xiinv) bind(C, name="qq_xipolygenerator") result(st)
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: ctx, eig
+      real(c_double), value :: kappa
+      real(c_double), intent(in) :: co(*)
+      real(c_double), intent(out) :: xiinv(*)
+      integer(c_int) :: st
+    end function qq_xipolygenerator
+    function qq_generalaverage(ctx, m, mp, ze, zo, xe, xo, kappa, eigstart, eigstep, co11, co8, co5, copoly, &
+        Jave) bind(C, name="qq_generalaverage") result(st)
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: ctx, m, mp
+      real(c_double), intent(in) :: ze(*), zo(*), xe(*), xo(*)
+      real(c_double), value :: kappa
+      integer(c_int), value :: eigstart, eigstep
+      real(c_double), intent(in) :: co11(*), co8(*), co5(*), copoly(*)
+      real(c_double), intent(out) :: Jave(*)
+      integer(c_int) :: st
+    end function qq_generalaverage
 
     ! ---- file formats ----
     function qq_gfwrite(path, u, nvhalf, ntotal, gaction, beta, alat, tad, icfgsave, myid) &

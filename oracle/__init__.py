@@ -94,6 +94,12 @@ def lib() -> C.CDLL:
             "oq_eigmodes": ([P, DP, I, IP, I, DP, DP, DP, DP, DP, DP, IP], I),
             "oq_xigenerator": ([P, DP, I, D, DP, DP, I, DP], None),
             "oq_eigaverage": ([P, DP, I, I, I, DP, DP, D, DP, DP, DP, I, DP], None),
+            "oq_loop_slices": ([P, DP, DP, DP, DP, DP, I, D, DP], None),
+            "oq_ppcoeffs": ([P, DP, DP, DP, D, I, DP], None),
+            "oq_ppaverage": ([P, DP, I, DP, DP, DP, DP, DP, D, I, DP], None),
+            "oq_xipolygenerator": ([P, DP, I, D, DP, DP, DP, DP], None),
+            "oq_generalaverage": ([P, DP, I, DP, DP, DP, I, DP, DP, DP, DP, DP, DP, D, I, I, DP, DP, DP, DP,
+                                   DP], None),
             "oq_twaverage_mom": ([P, DP, DP, DP, DP, DP, D, D, IP, I, I, I, DP], None),
             "oq_twvev_sites": ([P, DP, D, D, IP, I, I, I, IP, I, DP], None),
             "oq_set_kcyclim": ([I], None),
@@ -392,6 +398,62 @@ class OracleLattice:
         lib().oq_eigaverage(self._g, _dp(self.u), n, int(eigstart), int(eigstep), _dp(np.ascontiguousarray(ze)),
                             _dp(np.ascontiguousarray(zo)), float(kappa), _dp(np.ascontiguousarray(R)),
                             _dp(np.ascontiguousarray(L)), _dp(s), int(eshfes), _dp(J))
+        return J
+
+    def ppcoeffs(self, be, bo, kappa, p):
+        """The least-squares polynomial of ppaverage* (complex (p,))."""
+        co = np.zeros((p, 2))
+        lib().oq_ppcoeffs(self._g, _dp(self.u), _dp(np.ascontiguousarray(be)), _dp(np.ascontiguousarray(bo)),
+                          float(kappa), int(p), _dp(co))
+        return co[:, 0] + 1j * co[:, 1]
+
+    @staticmethod
+    def _cplx2(a):
+        a = np.asarray(a, complex)
+        out = np.zeros((len(a), 2))
+        out[:, 0], out[:, 1] = a.real, a.imag
+        return out
+
+    def ppaverage(self, p, co, be, bo, xe, xo, kappa, nsub=6):
+        """ppaverage (p = 5) / ppaverage1 (8) / ppaverage2 (11) at imom = 1: (9, nsub, nt, 2)."""
+        J = np.zeros((9, nsub, self.dims[3], 2))
+        lib().oq_ppaverage(self._g, _dp(self.u), int(p), _dp(self._cplx2(co)), _dp(np.ascontiguousarray(be)),
+                           _dp(np.ascontiguousarray(bo)), _dp(np.ascontiguousarray(xe)),
+                           _dp(np.ascontiguousarray(xo)), float(kappa), int(nsub), _dp(J))
+        return J
+
+    def xipolygenerator(self, R, L, kappa, co):
+        n = R.shape[0]
+        xi = np.zeros((n, 6, 2))
+        lib().oq_xipolygenerator(self._g, _dp(self.u), n, float(kappa), _dp(np.ascontiguousarray(R)),
+                                 _dp(np.ascontiguousarray(L)), _dp(self._cplx2(co)), _dp(xi))
+        return xi[..., 0] + 1j * xi[..., 1]
+
+    def loop_slices(self, be, bo, ye, yo, ksub, kappa):
+        J = np.zeros((9, self.dims[3], 2))
+        lib().oq_loop_slices(self._g, _dp(self.u), _dp(np.ascontiguousarray(be)), _dp(np.ascontiguousarray(bo)),
+                             _dp(np.ascontiguousarray(ye)), _dp(np.ascontiguousarray(yo)), int(ksub), float(kappa),
+                             _dp(J))
+        return J
+
+    def generalaverage(self, m, mp, ze, zo, xe, xo, kappa, co11, co8, co5, copoly, eigstart=1, eigstep=1):
+        """generalaverage at imom = 1; m = (evals, R, L) of M, mp = (evals, R) of M gamma5.
+        Returns Jave as (9, 10, numEV_MAX, 6, nt, 2)."""
+        ev1, R1, L1 = m
+        ev2, R2 = mp[0], mp[1]
+        n1, n2 = len(ev1), len(ev2)
+        ne = max(1, n1, n2)
+        J = np.zeros((9, 10, ne, 6, self.dims[3], 2))
+        z = np.zeros((1, 2) + self.half_shape)
+        R1 = np.ascontiguousarray(R1 if n1 else z)
+        L1 = np.ascontiguousarray(L1 if n1 else z)
+        R2 = np.ascontiguousarray(R2 if n2 else z)
+        lib().oq_generalaverage(self._g, _dp(self.u), n1, _dp(R1), _dp(L1), _dp(self._cplx2(ev1) if n1 else np.zeros((1, 2))),
+                                n2, _dp(R2), _dp(self._cplx2(ev2) if n2 else np.zeros((1, 2))),
+                                _dp(np.ascontiguousarray(ze)), _dp(np.ascontiguousarray(zo)),
+                                _dp(np.ascontiguousarray(xe)), _dp(np.ascontiguousarray(xo)), float(kappa),
+                                int(eigstart), int(eigstep), _dp(self._cplx2(co11)), _dp(self._cplx2(co8)),
+                                _dp(self._cplx2(co5)), _dp(self._cplx2(copoly)), _dp(J))
         return J
 
     def twvev(self, kappa, delta=0.0, io=(1, 1, 1), dobndry=0, ir=1, nsub=6, nmom=5, nop=6):

@@ -93,6 +93,52 @@ C dot(const C a[4][3], const C b[4][3]) {  // a^+ b
   return s;
 }
 
+
+// loopops at lexicographic site s: the nine operators of y against the noise b.
+void site_ops(const AvLattice& L, const double* u, const double* ye, const double* yo, const double* be,
+              const double* bo, int s, int ksub, C op[10]) {
+  C y[4][3], b[4][3], yn[4][3], bn[4][3], w[4][3], gv[4][3];
+  L.spinor(ye, yo, s, y);
+  L.spinor(be, bo, s, b);
+  for (int mu = 0; mu < 4; ++mu) {
+    double f;
+    const int sn = L.nb(s, mu, 1, &f);
+    L.spinor(ye, yo, sn, yn);
+    L.spinor(be, bo, sn, bn);
+    // A = f y(x+mu)^+ (1 - gamma_mu) U^+ b(x)
+    C ub[4][3];
+    for (int d = 0; d < 4; ++d)
+      for (int a = 0; a < 3; ++a) {
+        C t = 0.0;
+        for (int c = 0; c < 3; ++c) t += std::conj(L.link(u, s, mu, c, a)) * b[d][c];
+        ub[d][a] = t;
+      }
+    gamma_mult(mu, ub, gv);
+    for (int d = 0; d < 4; ++d)
+      for (int a = 0; a < 3; ++a) w[d][a] = ub[d][a] - gv[d][a];
+    C A = dot(yn, w) * f;
+    // B = - y(x)^+ (1 + gamma_mu) U f b(x+mu)
+    for (int d = 0; d < 4; ++d)
+      for (int a = 0; a < 3; ++a) {
+        C t = 0.0;
+        for (int c = 0; c < 3; ++c) t += L.link(u, s, mu, a, c) * (f * bn[d][c]);
+        ub[d][a] = t;
+      }
+    gamma_mult(mu, ub, gv);
+    for (int d = 0; d < 4; ++d)
+      for (int a = 0; a < 3; ++a) w[d][a] = -(ub[d][a] + gv[d][a]);
+    const C B = dot(y, w);
+    op[mu] = std::conj(A + B);
+  }
+  C s5 = dot(y, b);
+  if (ksub == 1) s5 += 12.0;
+  op[4] = std::conj(s5);
+  for (int mu = 0; mu < 4; ++mu) {
+    gamma_mult(mu, b, gv);
+    op[5 + mu] = std::conj(dot(y, gv));
+  }
+}
+
 }  // namespace
 
 extern "C" void oq_average(const oq_geom* g, const double* u, const double* be, const double* bo, const double* xe,
@@ -164,47 +210,8 @@ extern "C" void oq_average(const oq_geom* g, const double* u, const double* be, 
     }
     // loopops per site, then spacesum
     for (int s = 0; s < L.V; ++s) {
-      C y[4][3], b[4][3], yn[4][3], bn[4][3], w[4][3], gv[4][3];
-      L.spinor(ye.data(), yo.data(), s, y);
-      L.spinor(b_e.data(), b_o.data(), s, b);
       C op[10];
-      for (int mu = 0; mu < 4; ++mu) {
-        double f;
-        const int sn = L.nb(s, mu, 1, &f);
-        L.spinor(ye.data(), yo.data(), sn, yn);
-        L.spinor(b_e.data(), b_o.data(), sn, bn);
-        // A = f y(x+mu)^+ (1 - gamma_mu) U^+ b(x)
-        C ub[4][3];
-        for (int d = 0; d < 4; ++d)
-          for (int a = 0; a < 3; ++a) {
-            C t = 0.0;
-            for (int c = 0; c < 3; ++c) t += std::conj(L.link(u, s, mu, c, a)) * b[d][c];
-            ub[d][a] = t;
-          }
-        gamma_mult(mu, ub, gv);
-        for (int d = 0; d < 4; ++d)
-          for (int a = 0; a < 3; ++a) w[d][a] = ub[d][a] - gv[d][a];
-        C A = dot(yn, w) * f;
-        // B = - y(x)^+ (1 + gamma_mu) U f b(x+mu)
-        for (int d = 0; d < 4; ++d)
-          for (int a = 0; a < 3; ++a) {
-            C t = 0.0;
-            for (int c = 0; c < 3; ++c) t += L.link(u, s, mu, a, c) * (f * bn[d][c]);
-            ub[d][a] = t;
-          }
-        gamma_mult(mu, ub, gv);
-        for (int d = 0; d < 4; ++d)
-          for (int a = 0; a < 3; ++a) w[d][a] = -(ub[d][a] + gv[d][a]);
-        const C B = dot(y, w);
-        op[mu] = std::conj(A + B);
-      }
-      C s5 = dot(y, b);
-      if (ksub == 1) s5 += 12.0;
-      op[4] = std::conj(s5);
-      for (int mu = 0; mu < 4; ++mu) {
-        gamma_mult(mu, b, gv);
-        op[5 + mu] = std::conj(dot(y, gv));
-      }
+      site_ops(L, u, ye.data(), yo.data(), b_e.data(), b_o.data(), s, ksub, op);
       const int t = s / (L.n[0] * L.n[1] * L.n[2]);
       for (int iop = 0; iop < 9 && iop < nop; ++iop) {
         J(0, t, isub - 1, 0, iop) += op[iop].real();
@@ -271,4 +278,24 @@ extern "C" void oq_momfacs(const oq_geom* g, const int io[3], double* momfac) {
         }
       }
     }
+}
+
+// The operators of y against b at zero momentum summed per time slice, operators 1..4
+// times kappa: J(2, nt, 9) (loopops with ksub, spacesum at imom = 1).
+extern "C" void oq_loop_slices(const oq_geom* g, const double* u, const double* be, const double* bo,
+                               const double* ye, const double* yo, int ksub, double kappa, double* J) {
+  const AvLattice L(g);
+  const int nt = g->n[3];
+  std::memset(J, 0, sizeof(double) * 2 * nt * 9);
+  for (int s = 0; s < L.V; ++s) {
+    C op[10];
+    site_ops(L, u, ye, yo, be, bo, s, ksub, op);
+    const int t = s / (L.n[0] * L.n[1] * L.n[2]);
+    for (int iop = 0; iop < 9; ++iop) {
+      J[((size_t)iop * nt + t) * 2] += op[iop].real();
+      J[((size_t)iop * nt + t) * 2 + 1] += op[iop].imag();
+    }
+  }
+  for (int iop = 0; iop < 4; ++iop)
+    for (int k = 0; k < 2 * nt; ++k) J[(size_t)iop * 2 * nt + k] *= kappa;
 }

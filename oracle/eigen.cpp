@@ -656,3 +656,254 @@ extern "C" void oq_eigaverage(const oq_geom* g, const double* u, int numEV, int 
           Jtime[((((size_t)iop * numEV) + (eig - 1)) * nt + t) * 2 + ri] = J[((size_t)iop * nt + t) * 2 + ri];
   }
 }
+
+// ---------------------------------------------------------------------------------------
+// The polynomial estimators: ppaverage2 (p = 11, Q/disconloops.f90:5740-6288), ppaverage1
+// (p = 8, :6290-6883), ppaverage (p = 5, :6885-7434), xipolygenerator (:847-1584) and
+// generalaverage (:119-333).  The powers vprime(i) = M^(i-1) b live in module shift
+// (Q/shift.f90:22-23); ppaverage's loop stops at vprime(6) but its levels 5 and 6 read
+// vprime(7) and vprime(8), which then hold M^6 b and M^7 b from the ppaverage2 and
+// ppaverage1 calls on the same noise that precede it in generalaverage (:234-242); they
+// are computed here directly.  The coefficients co / co2 / co4 are module variables fitted
+// only while psignal = 0 (the first noise, :5895-5923); here they are arguments.
+// ---------------------------------------------------------------------------------------
+namespace {
+
+struct PTerm {
+  int co, v;  // co_co * vprime_v, 1-based
+};
+
+// The terms each ppaverage variant adds at level isub (the select case blocks).
+std::vector<PTerm> level_terms(int p, int isub) {
+  if (isub == 2) return {{1, 1}, {2, 2}, {3, 3}, {4, 4}};
+  if (isub < 3 || isub > 6) return {};
+  if (p == 5) return {{5, isub + 2}};  // :7190-7293 reuse co4(:, 5)
+  if (p == 11 && isub == 6) return {{8, 8}, {9, 9}, {10, 10}, {11, 11}};
+  return {{isub + 2, isub + 2}};
+}
+
+// vprime(:, :, i+1) = vprime(:, :, i) - kappa H vprime(:, :, i) on each half (:5856-5873)
+void powers(const oq_geom* g, const double* u, const double* be, const double* bo, double kappa, int n,
+            std::vector<double>& ve, std::vector<double>& vo) {
+  const size_t vs = g->vsize();
+  ve.assign((size_t)n * vs, 0.0);
+  vo.assign((size_t)n * vs, 0.0);
+  g->for_interior([&](size_t k) {
+    ve[k] = be[k];
+    vo[k] = bo[k];
+  });
+  std::vector<double> tue(vs), tuo(vs), ti(vs);
+  for (int i = 1; i < n; ++i) {
+    std::fill(tue.begin(), tue.end(), 0.0);
+    std::fill(tuo.begin(), tuo.end(), 0.0);
+    std::memcpy(ti.data(), vo.data() + (i - 1) * vs, sizeof(double) * vs);
+    oq::hsingle(g, tue.data(), u, ti.data(), 0, 1);
+    std::memcpy(ti.data(), ve.data() + (i - 1) * vs, sizeof(double) * vs);
+    oq::hsingle(g, tuo.data(), u, ti.data(), 0, 2);
+    double* ne = ve.data() + i * vs;
+    double* no = vo.data() + i * vs;
+    const double* pe = ve.data() + (i - 1) * vs;
+    const double* po = vo.data() + (i - 1) * vs;
+    g->for_interior([&](size_t k) {
+      ne[k] = pe[k] - kappa * tue[k];
+      no[k] = po[k] - kappa * tuo[k];
+    });
+  }
+}
+
+void add_term(const oq_geom* g, double* sub, C co, const double* v) {
+  for (int ibleo = 1; ibleo <= 8; ++ibleo)
+    for (int ieo = 1; ieo <= 2; ++ieo)
+      for (int id = 1; id <= 4; ++id)
+        for (int s = 1; s <= g->nvhalf; ++s)
+          for (int c = 1; c <= 5; c += 2) {
+            const size_t k = g->gi(c, s, id, ieo, ibleo);
+            const double a = sub[k] + co.real() * v[k] - co.imag() * v[k + 1];
+            sub[k + 1] = sub[k + 1] + co.real() * v[k + 1] + co.imag() * v[k];
+            sub[k] = a;
+          }
+}
+
+}  // namespace
+
+// The normal equations of the polynomial fit (:5895-5923): co(2, p).
+extern "C" void oq_ppcoeffs(const oq_geom* g, const double* u, const double* be, const double* bo, double kappa,
+                            int p, double* co) {
+  const size_t vs = g->vsize();
+  std::vector<double> ve, vo;
+  powers(g, u, be, bo, kappa, p + 1, ve, vo);
+  std::vector<double> lsmat(2 * (size_t)p * p), cls(2 * (size_t)p);
+  std::vector<int> ipiv(p);
+  for (int i = 2; i <= p + 1; ++i)
+    for (int j = 2; j <= p + 1; ++j) {
+      double im1 = 0.0, im2 = 0.0;
+      const double r1 = oq::vecdot_re(g, ve.data() + (i - 1) * vs, ve.data() + (j - 1) * vs, &im1);
+      const double r2 = oq::vecdot_re(g, vo.data() + (i - 1) * vs, vo.data() + (j - 1) * vs, &im2);
+      lsmat[2 * ((size_t)(i - 2) + (size_t)p * (j - 2))] = r1 + r2;
+      lsmat[2 * ((size_t)(i - 2) + (size_t)p * (j - 2)) + 1] = im1 + im2;
+    }
+  for (int i = 2; i <= p + 1; ++i) {
+    double im1 = 0.0, im2 = 0.0;
+    const double r1 = oq::vecdot_re(g, ve.data() + (i - 1) * vs, ve.data(), &im1);
+    const double r2 = oq::vecdot_re(g, vo.data() + (i - 1) * vs, vo.data(), &im2);
+    cls[2 * (i - 2)] = r1 + r2;
+    cls[2 * (i - 2) + 1] = im1 + im2;
+  }
+  oq_linearsolver(p, 1, lsmat.data(), p, ipiv.data(), cls.data(), p);
+  std::memcpy(co, cls.data(), sizeof(double) * 2 * p);
+}
+
+// ppaverage (p = 5), ppaverage1 (p = 8), ppaverage2 (p = 11) at imom = 1: Jtime(2, nt, nsub, 9).
+extern "C" void oq_ppaverage(const oq_geom* g, const double* u, int p, const double* co, const double* be,
+                             const double* bo, const double* xe, const double* xo, double kappa, int nsub,
+                             double* Jtime) {
+  const size_t vs = g->vsize();
+  const int nt = g->n[3];
+  std::vector<double> ve, vo;
+  powers(g, u, be, bo, kappa, p == 11 ? 12 : (p == 8 ? 9 : 8), ve, vo);
+  std::vector<double> sube(vs, 0.0), subo(vs, 0.0), ye(vs, 0.0), yo(vs, 0.0), J((size_t)2 * nt * 9);
+  for (int isub = 1; isub <= nsub; ++isub) {
+    const int ksub = isub == 1 ? 0 : 1;
+    for (const PTerm& t : level_terms(p, isub)) {
+      const C c(co[2 * (t.co - 1)], co[2 * (t.co - 1) + 1]);
+      add_term(g, sube.data(), c, ve.data() + (t.v - 1) * vs);
+      add_term(g, subo.data(), c, vo.data() + (t.v - 1) * vs);
+    }
+    g->for_interior([&](size_t k) {
+      ye[k] = xe[k] - sube[k];
+      yo[k] = xo[k] - subo[k];
+    });
+    oq_loop_slices(g, u, be, bo, ye.data(), yo.data(), ksub, kappa, J.data());
+    for (int iop = 0; iop < 9; ++iop)
+      for (int t = 0; t < nt; ++t)
+        for (int ri = 0; ri < 2; ++ri)
+          Jtime[((((size_t)iop * nsub) + (isub - 1)) * nt + t) * 2 + ri] = J[((size_t)iop * nt + t) * 2 + ri];
+  }
+}
+
+// xipolygenerator: xiinv(2, 6, numEV) with the p = 8 terms and coefficients co(2, 8).
+extern "C" void oq_xipolygenerator(const oq_geom* g, const double* u, int numEV, double kappa, const double* R,
+                                   const double* L, const double* co, double* xiinv) {
+  const size_t vs = g->vsize();
+  std::vector<double> ve, vo, sube(vs), subo(vs), te(vs), to(vs);
+  for (int e = 0; e < numEV; ++e) {
+    std::fill(sube.begin(), sube.end(), 0.0);
+    std::fill(subo.begin(), subo.end(), 0.0);
+    for (int isub = 1; isub <= 6; ++isub) {
+      powers(g, u, R + (size_t)e * 2 * vs, R + (size_t)e * 2 * vs + vs, kappa, 9, ve, vo);
+      for (const PTerm& t : level_terms(8, isub)) {
+        const C c(co[2 * (t.co - 1)], co[2 * (t.co - 1) + 1]);
+        add_term(g, sube.data(), c, ve.data() + (t.v - 1) * vs);
+        add_term(g, subo.data(), c, vo.data() + (t.v - 1) * vs);
+      }
+      te = sube;
+      to = subo;
+      oq_gam5x(g, te.data());
+      oq_gam5x(g, to.data());
+      double im1 = 0.0, im2 = 0.0;
+      const double r1 = oq::vecdot_re(g, L + (size_t)e * 2 * vs, te.data(), &im1);
+      const double r2 = oq::vecdot_re(g, L + (size_t)e * 2 * vs + vs, to.data(), &im2);
+      xiinv[2 * ((size_t)(isub - 1) + 6 * (size_t)e)] = r1 + r2;
+      xiinv[2 * ((size_t)(isub - 1) + 6 * (size_t)e) + 1] = im1 + im2;
+    }
+  }
+}
+
+// generalaverage at imom = 1: Jave(2, nt, 6, max(n1, n2), 10, 9).  (R1, L1, ev1): the n1
+// modes of M; (R2, ev2): the n2 modes of M gamma5.
+extern "C" void oq_generalaverage(const oq_geom* g, const double* u, int n1, const double* R1, const double* L1,
+                                  const double* ev1, int n2, const double* R2, const double* ev2,
+                                  const double* ze, const double* zo, const double* xe, const double* xo,
+                                  double kappa, int eigstart, int eigstep, const double* co11, const double* co8,
+                                  const double* co5, const double* copoly, double* Jave) {
+  const size_t vs = g->vsize();
+  const int nt = g->n[3], nsub = 6, nsty = 10, nmax = std::max(n1, n2);
+  std::vector<double> NS((size_t)2 * nt * 9);
+  oq_loop_slices(g, u, ze, zo, xe, xo, 0, kappa, NS.data());
+  std::vector<double> zero(vs, 0.0), PS((size_t)2 * nt * nsub * 9), PP(PS.size()), PP4(PS.size()), PP7(PS.size());
+  oq_average(g, u, ze, zo, zero.data(), zero.data(), kappa, nsub, 1, 9, nullptr, PS.data());
+  oq_ppaverage(g, u, 11, co11, ze, zo, zero.data(), zero.data(), kappa, nsub, PP.data());
+  oq_ppaverage(g, u, 5, co5, ze, zo, zero.data(), zero.data(), kappa, nsub, PP4.data());
+  oq_ppaverage(g, u, 8, co8, ze, zo, zero.data(), zero.data(), kappa, nsub, PP7.data());
+  for (size_t i = 0; i < PS.size(); ++i) {
+    PS[i] = -PS[i];
+    PP[i] = -PP[i];
+    PP4[i] = -PP4[i];
+    PP7[i] = -PP7[i];
+  }
+  std::vector<double> s1(2 * (size_t)std::max(1, n1)), s2(2 * (size_t)std::max(1, n2));
+  for (int j = 0; j < n1; ++j) {
+    const C v = oneover(C(ev1[2 * j], ev1[2 * j + 1]));
+    s1[2 * j] = v.real();
+    s1[2 * j + 1] = v.imag();
+  }
+  for (int j = 0; j < n2; ++j) s2[2 * j] = 1.0 / ev2[2 * j];
+  std::vector<double> xi1(12 * (size_t)std::max(1, n1)), xi2(12 * (size_t)std::max(1, n2)),
+      xip(12 * (size_t)std::max(1, n2));
+  oq_xigenerator(g, u, n1, kappa, R1, L1, 1, xi1.data());
+  oq_xigenerator(g, u, n2, kappa, R2, R2, 2, xi2.data());
+  oq_xipolygenerator(g, u, n2, kappa, R2, R2, copoly, xip.data());
+  const size_t b1 = (size_t)2 * nt * std::max(1, n1) * 9, b2 = (size_t)2 * nt * std::max(1, n2) * 9;
+  std::vector<double> ES(b1), HFES(b2), ESPS(b1 * nsub), HFESPS(b2 * nsub), HFESPOLY(b2 * nsub), sc(2 * (size_t)nmax + 2);
+  oq_eigaverage(g, u, n1, eigstart, eigstep, ze, zo, kappa, R1, L1, s1.data(), 1, ES.data());
+  oq_eigaverage(g, u, n2, eigstart, eigstep, ze, zo, kappa, R2, R2, s2.data(), 2, HFES.data());
+  for (int isub = 0; isub < nsub; ++isub) {
+    for (int j = 0; j < n1; ++j) {
+      sc[2 * j] = xi1[2 * ((size_t)isub + 6 * j)];
+      sc[2 * j + 1] = xi1[2 * ((size_t)isub + 6 * j) + 1];
+    }
+    oq_eigaverage(g, u, n1, eigstart, eigstep, ze, zo, kappa, R1, L1, sc.data(), 1, ESPS.data() + isub * b1);
+    for (int j = 0; j < n2; ++j) {
+      sc[2 * j] = xi2[2 * ((size_t)isub + 6 * j)];
+      sc[2 * j + 1] = xi2[2 * ((size_t)isub + 6 * j) + 1];
+    }
+    oq_eigaverage(g, u, n2, eigstart, eigstep, ze, zo, kappa, R2, R2, sc.data(), 2, HFESPS.data() + isub * b2);
+    for (int j = 0; j < n2; ++j) {
+      sc[2 * j] = xip[2 * ((size_t)isub + 6 * j)];
+      sc[2 * j + 1] = xip[2 * ((size_t)isub + 6 * j) + 1];
+    }
+    oq_eigaverage(g, u, n2, eigstart, eigstep, ze, zo, kappa, R2, R2, sc.data(), 2, HFESPOLY.data() + isub * b2);
+  }
+  const int ne = std::max(1, nmax);
+  std::memset(Jave, 0, sizeof(double) * 2 * nt * nsub * (size_t)ne * nsty * 9);
+  auto E = [&](const std::vector<double>& A, int n, size_t off, int iop, int e, int t, int ri) {
+    return e < n ? A[off + ((((size_t)iop * n) + e) * nt + t) * 2 + ri] : 0.0;
+  };
+  auto P = [&](const std::vector<double>& A, int iop, int isub, int t, int ri) {
+    return A[((((size_t)iop * nsub) + isub) * nt + t) * 2 + ri];
+  };
+  for (int isub = 0; isub < nsub; ++isub)
+    for (int e = 0; e < nmax; ++e)
+      for (int sty = 1; sty <= nsty; ++sty)
+        for (int iop = 0; iop < 9; ++iop)
+          for (int t = 0; t < nt; ++t)
+            for (int ri = 0; ri < 2; ++ri) {
+              const double N = NS[((size_t)iop * nt + t) * 2 + ri];
+              double v;
+              if (sty == 1 && e == 0 && isub == 0)
+                v = N;
+              else if (sty == 2 && e == 0)
+                v = N - P(PS, iop, isub, t, ri);
+              else if (sty == 3 && isub == 0)
+                v = N - E(ES, n1, 0, iop, e, t, ri);
+              else if (sty == 4 && isub == 0)
+                v = N - E(HFES, n2, 0, iop, e, t, ri);
+              else if (sty == 5)
+                v = N - E(ES, n1, 0, iop, e, t, ri) - (P(PS, iop, isub, t, ri) - E(ESPS, n1, isub * b1, iop, e, t, ri));
+              else if (sty == 6)
+                v = N - E(HFES, n2, 0, iop, e, t, ri) -
+                    (P(PS, iop, isub, t, ri) - E(HFESPS, n2, isub * b2, iop, e, t, ri));
+              else if (sty == 7 && e == 0)
+                v = N - P(PP, iop, isub, t, ri);
+              else if (sty == 8 && e == 0)
+                v = N - P(PP4, iop, isub, t, ri);
+              else if (sty == 9 && e == 0)
+                v = N - P(PP7, iop, isub, t, ri);
+              else if (sty == 10)
+                v = N - E(HFES, n2, 0, iop, e, t, ri) -
+                    (P(PP7, iop, isub, t, ri) - E(HFESPOLY, n2, isub * b2, iop, e, t, ri));
+              else
+                continue;
+              Jave[((((((size_t)iop * nsty) + (sty - 1)) * ne + e) * nsub + isub) * nt + t) * 2 + ri] = v;
+            }
+}

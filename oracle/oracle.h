@@ -182,6 +182,21 @@ void oq_eigaverage(const oq_geom* g, const double* u, int numEV, int eigstart, i
                    const double* ze, const double* zo, double kappa, const double* R,
                    const double* L, const double* scal, int eshfes, double* Jtime);
 
+void oq_loop_slices(const oq_geom* g, const double* u, const double* be, const double* bo,
+                    const double* ye, const double* yo, int ksub, double kappa, double* J);
+void oq_ppcoeffs(const oq_geom* g, const double* u, const double* be, const double* bo, double kappa,
+                 int p, double* co);
+void oq_ppaverage(const oq_geom* g, const double* u, int p, const double* co, const double* be,
+                  const double* bo, const double* xe, const double* xo, double kappa, int nsub,
+                  double* Jtime);
+void oq_xipolygenerator(const oq_geom* g, const double* u, int numEV, double kappa, const double* R,
+                        const double* L, const double* co, double* xiinv);
+void oq_generalaverage(const oq_geom* g, const double* u, int n1, const double* R1, const double* L1,
+                       const double* ev1, int n2, const double* R2, const double* ev2,
+                       const double* ze, const double* zo, const double* xe, const double* xo,
+                       double kappa, int eigstart, int eigstep, const double* co11, const double* co8,
+                       const double* co5, const double* copoly, double* Jave);
+
 void oq_coldstart(const oq_geom* g, double* u);
 // The reference's pseudo-heatbath for the Wilson plaquette action at beta (sweep
 // C/cfgsprops.f90:1973-2001, staple G/gaugetools.f90:39-345, phbup / su2up / sprd1

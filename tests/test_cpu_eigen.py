@@ -149,3 +149,83 @@ def test_eigaverage_is_prefix_sum_of_mode_traces(lat, modes, modes_p, which, eig
             np.testing.assert_allclose(got, acc, rtol=0, atol=1e-12 * max(1.0, np.abs(acc).max()))
         else:
             assert np.all(got == 0.0)
+
+
+# ---- the polynomial estimators (ppaverage*, xipolygenerator, oracle/eigen.cpp) ----
+TERMS = {  # (coefficient, power) added at levels 2..6, 1-based (Q/disconloops.f90:5740-7434)
+    11: {2: [(1, 1), (2, 2), (3, 3), (4, 4)], 3: [(5, 5)], 4: [(6, 6)], 5: [(7, 7)],
+         6: [(8, 8), (9, 9), (10, 10), (11, 11)]},
+    8: {2: [(1, 1), (2, 2), (3, 3), (4, 4)], 3: [(5, 5)], 4: [(6, 6)], 5: [(7, 7)], 6: [(8, 8)]},
+    5: {2: [(1, 1), (2, 2), (3, 3), (4, 4)], 3: [(5, 5)], 4: [(5, 6)], 5: [(5, 7)], 6: [(5, 8)]},
+}
+
+
+def mpowers(links, b, n):
+    out = [b]
+    for _ in range(n - 1):
+        out.append(out[-1] - KAPPA[0] * hop_lex(links, out[-1], BC))
+    return out
+
+
+@pytest.fixture(scope="module")
+def noise(lat):
+    oracle.initlagfib(0, 23)
+    return lat.z4source()
+
+
+@pytest.mark.parametrize("p", [5, 8, 11])
+def test_ppcoeffs_minimise_the_polynomial_residual(lat, noise, p):
+    """The normal-equation fit reaches the least-squares residual of numpy's lstsq on the
+    Krylov matrix (the coefficients themselves are ill-conditioned)."""
+    ze, zo = noise
+    co = lat.ppcoeffs(ze, zo, KAPPA[0], p)
+    b = half_to_lex(ze, DIMS, 1) + half_to_lex(zo, DIMS, 2)
+    K = np.stack([v.ravel() for v in mpowers(links_of(lat), b, p + 1)[1:]], axis=1)
+    best = np.linalg.lstsq(K, b.ravel(), rcond=None)[0]
+    r_fit = np.linalg.norm(b.ravel() - K @ co)
+    r_best = np.linalg.norm(b.ravel() - K @ best)
+    assert r_fit <= r_best * (1 + 1e-5) + 1e-12 * np.linalg.norm(b)
+    assert r_fit < np.linalg.norm(b)
+
+
+@pytest.mark.parametrize("p", [5, 8, 11])
+def test_ppaverage_levels(lat, noise, p):
+    """Level isub: loop operators of x - sum of the level terms' co_c M^(v-1) b, against
+    numpy-built subtractions through the oracle's loop operators."""
+    from qqtest import lex_to_half
+
+    ze, zo = noise
+    rng = np.random.default_rng(p)
+    co = rng.standard_normal(p) + 1j * rng.standard_normal(p)
+    xe = lat.new_half()
+    xo = lat.new_half()
+    xe[:, :, :, :lat.nvhalf] = rng.standard_normal(xe[:, :, :, :lat.nvhalf].shape)
+    xo[:, :, :, :lat.nvhalf] = rng.standard_normal(xo[:, :, :, :lat.nvhalf].shape)
+    J = lat.ppaverage(p, co, ze, zo, xe, xo, KAPPA[0])
+    b = half_to_lex(ze, DIMS, 1) + half_to_lex(zo, DIMS, 2)
+    V = mpowers(links_of(lat), b, 12)
+    sub = np.zeros_like(b)
+    for isub in range(1, 7):
+        for c, v in TERMS[p].get(isub, []):
+            sub = sub + co[c - 1] * V[v - 1]
+        ye = xe - lex_to_half(sub, DIMS, lat.ntotal, 1)
+        yo = xo - lex_to_half(sub, DIMS, lat.ntotal, 2)
+        want = lat.loop_slices(ze, zo, ye, yo, 0 if isub == 1 else 1, KAPPA[0])
+        assert np.abs(J[:, isub - 1] - want).max() <= 1e-11 * np.abs(want).max(), isub
+
+
+def test_xipolygenerator(lat, modes_p, noise):
+    ev, R, _ = modes_p
+    ze, zo = noise
+    co = lat.ppcoeffs(ze, zo, KAPPA[0], 8)
+    xi = lat.xipolygenerator(R, R, KAPPA[0], co)
+    links = links_of(lat)
+    for j in range(len(ev)):
+        r = lex(R[j])
+        V = mpowers(links, r, 9)
+        sub = np.zeros_like(r)
+        for isub in range(1, 7):
+            for c, v in TERMS[8].get(isub, []):
+                sub = sub + co[c - 1] * V[v - 1]
+            want = np.vdot(r, spin(GAMMA5, sub))
+            assert abs(xi[j, isub - 1] - want) <= 1e-11 * max(1.0, abs(want)), (j, isub)

@@ -118,3 +118,83 @@ def test_unit_source_needs_no_start_vector_and_bad_arguments(small):
         lat.eigenmodes(1, (20, 20), 2, KAPPA)  # k must be below m
     with pytest.raises(qq.QQError):
         lat.eigenmodes(3, (20, 10), 2, KAPPA)
+
+
+@pytest.fixture(scope="module")
+def noise(small):
+    ol, _ = small
+    oracle.initlagfib(0, 23)
+    return ol.z4source()
+
+
+@pytest.mark.parametrize("p", [5, 8, 11])
+def test_ppcoeffs_and_ppaverage_match_oracle(small, noise, p):
+    """The GPU fit reaches the oracle's polynomial residual ||z - sum co_b M^b z|| (the
+    coefficients themselves are ill-conditioned); with the same coefficients the levels of
+    ppaverage / ppaverage1 / ppaverage2 agree to 1e-10."""
+    ol, lat = small
+    ze, zo = noise
+    co_g = lat.ppcoeffs(ze, zo, KAPPA[0], p)
+    co_o = ol.ppcoeffs(ze, zo, KAPPA[0], p)
+
+    def cmul(c, v):
+        w = np.zeros_like(v)
+        z = c * (v[..., 0::2] + 1j * v[..., 1::2])
+        w[..., 0::2], w[..., 1::2] = z.real, z.imag
+        return w
+
+    def resid(co):
+        ve, vo = ze.copy(), zo.copy()
+        re_, ro_ = ze.copy(), zo.copy()
+        for c in co:
+            ve, vo = ve - KAPPA[0] * ol.hsingle(vo, 0, 1), vo - KAPPA[0] * ol.hsingle(ve, 0, 2)
+            re_, ro_ = re_ - cmul(c, ve), ro_ - cmul(c, vo)
+        return np.sqrt(ol.vecdot(re_, re_).real + ol.vecdot(ro_, ro_).real)
+
+    r_g, r_o = resid(co_g), resid(co_o)
+    assert abs(r_g - r_o) <= 1e-6 * r_o, (r_g, r_o)
+    rng = np.random.default_rng(p)
+    xe, xo = ol.new_half(), ol.new_half()
+    xe[:, :, :, :ol.nvhalf] = rng.standard_normal(xe[:, :, :, :ol.nvhalf].shape)
+    xo[:, :, :, :ol.nvhalf] = rng.standard_normal(xo[:, :, :, :ol.nvhalf].shape)
+    J_g = lat.ppaverage(p, co_o, ze, zo, xe, xo, KAPPA[0])
+    J_o = ol.ppaverage(p, co_o, ze, zo, xe, xo, KAPPA[0])
+    assert np.abs(J_g - J_o).max() <= 1e-10 * np.abs(J_o).max()
+
+
+def test_generalaverage_matches_oracle(small, noise):
+    """All ten estimator styles of generalaverage for one noise: the GPU's modes and
+    components against the oracle's (same polynomial coefficients, a random solution
+    vector; every style is phase free)."""
+    ol, lat = small
+    ze, zo = noise
+    k = KAPPA[0]
+    oracle.initlagfib(0, 11)
+    se, so = ol.z4source()
+    m_o = ol.eigmodes(1, (30, 16), 40, KAPPA)
+    mp_o = ol.eigmodes(2, (30, 16), 40, KAPPA, se, so)
+    m_g = lat.eigenmodes(1, (30, 16), 40, KAPPA)
+    mp_g = lat.eigenmodes(2, (30, 16), 40, KAPPA, se, so)
+    assert m_g.num == len(m_o[0]) and mp_g.num == len(mp_o[0])
+    np.testing.assert_allclose(m_g.evals, m_o[0], rtol=1e-9)
+    np.testing.assert_allclose(mp_g.evals, mp_o[0], rtol=1e-9)
+    co = {p: ol.ppcoeffs(ze, zo, k, p) for p in (5, 8, 11)}
+    oracle.initlagfib(0, 31)
+    pe, po = ol.z4source()
+    copoly = ol.ppcoeffs(pe, po, k, 8)
+    xi_g = mp_g.xipolygenerator(k, copoly)
+    xi_o = ol.xipolygenerator(mp_o[1], mp_o[1], k, copoly)
+    assert np.abs(xi_g - xi_o).max() <= 1e-8 * np.abs(xi_o).max()
+    rng = np.random.default_rng(3)
+    xe, xo = ol.new_half(), ol.new_half()
+    xe[:, :, :, :ol.nvhalf] = rng.standard_normal(xe[:, :, :, :ol.nvhalf].shape)
+    xo[:, :, :, :ol.nvhalf] = rng.standard_normal(xo[:, :, :, :ol.nvhalf].shape)
+    J_g = lat.generalaverage(m_g, mp_g, ze, zo, xe, xo, k, co[11], co[8], co[5], copoly)
+    J_o = ol.generalaverage(m_o, mp_o, ze, zo, xe, xo, k, co[11], co[8], co[5], copoly)
+    assert J_g.shape == J_o.shape
+    scale = np.abs(J_o).max()
+    for sty in range(10):
+        assert np.abs(J_g[:, sty] - J_o[:, sty]).max() <= 1e-8 * scale, sty + 1
+    assert np.all(J_g[:, 0, 1:] == 0.0) and np.all(J_g[:, 0, 0, 1:] == 0.0)  # style 1: mode 1, level 1
+    m_g.close()
+    mp_g.close()

@@ -106,7 +106,8 @@ def parse(argv=None):
     p.add_argument("--e2e-steps", type=int, default=0, help="end-to-end steps (0: min(steps, 5))")
     p.add_argument("--cpu-threads", type=int, default=0, help="host threads of the CPU legs (0: all)")
     p.add_argument("--no-cpu", action="store_true")
-    p.add_argument("--mode", default="solve", choices=["solve", "dslash", "c3", "c4", "shift", "twvev", "learned"])
+    p.add_argument("--mode", default="solve",
+                   choices=["solve", "dslash", "c3", "c4", "shift", "twvev", "learned", "eigen"])
     p.add_argument("--train-solves", type=int, default=8, help="--mode learned: training solves")
     p.add_argument("--train-steps", type=int, default=200, help="--mode learned: Adam steps")
     p.add_argument("--channels", default="4,8,8,4", help="--mode learned: channels per layer")
@@ -115,6 +116,8 @@ def parse(argv=None):
     p.add_argument("--nnoise", type=int, default=24, help="--mode c3: noises")
     p.add_argument("--solver", type=int, default=1, help="--mode c3: 1 batched, 2 psc")
     p.add_argument("--nsub", type=int, default=6, help="--mode c3 / twvev: subtraction level")
+    p.add_argument("--eig", default="200,160,150", help="--mode eigen: m, k and cycles of the eigen-iteration")
+    p.add_argument("--cpu-cycles", type=int, default=1, help="--mode eigen: oracle cycles timed (0: none)")
     return p.parse_args(argv)
 
 
@@ -695,11 +698,70 @@ def run_learned(a):
             "gain_vs_gmresdr": res["gmresdr"]["seconds"] / res["fgmresdr_net"]["seconds"]}
 
 
+def run_eigen(a):
+    """The Wilson loop driver's eigenmode subtraction (testFUNC) on a heatbath
+    configuration: the modes of M (kind 1) and of M gamma5 (kind 2) with the
+    eigen-iteration's m, k and cycles (the reference's 200, 160, 150 by default), then one
+    Z(4) noise: its solve (GMRES-DR(80,40) to 1e-7, the driver's settings), the polynomial
+    fits and generalaverage (all ten styles).  Wall time of each call.  Beside it the
+    oracle's time for --cpu-cycles cycles of the kind-1 iteration on the same lattice."""
+    import baylorlqcd_b200 as qq
+
+    dims = tuple(int(x) for x in a.dims.split(","))
+    m, k, cyc = (int(x) for x in a.eig.split(","))
+    kappa = (a.kappa, 0.0)
+    lat, plaq = heatbath_lattice(qq, dims, a.sweeps, 3)
+    out = {"mode": "eigen", "lattice": list(dims), "kappa": a.kappa, "eig_GMRES": [m, k], "cycles": cyc,
+           "plaquette": plaq}
+    qq.initlagfib(0, 5)
+    se, so = lat.z4source()
+    t0 = time.perf_counter()
+    M = lat.eigenmodes(1, (m, k), cyc, kappa)
+    t1 = time.perf_counter()
+    Mp = lat.eigenmodes(2, (m, k), cyc, kappa, se, so)
+    t2 = time.perf_counter()
+    out["modes_of_M"] = {"seconds": t1 - t0, "kept": M.num, "mvp": M.mvp,
+                         "smallest": [abs(M.evals[0]) if M.num else None]}
+    out["modes_of_Mgamma5"] = {"seconds": t2 - t1, "kept": Mp.num, "mvp": Mp.mvp,
+                               "smallest": [abs(Mp.evals[0]) if Mp.num else None]}
+    ze, zo = lat.z4source()
+    t3 = time.perf_counter()
+    xe, xo, info = lat.fermprop(ze, zo, kappa, inverter=5, resmax=1e-7, nGMRES=(80, 40))
+    t4 = time.perf_counter()
+    co = {p: lat.ppcoeffs(ze, zo, a.kappa, p) for p in (5, 8, 11)}
+    copoly = lat.ppcoeffs(se, so, a.kappa, 8)
+    t5 = time.perf_counter()
+    J = lat.generalaverage(M, Mp, ze, zo, xe, xo, a.kappa, co[11], co[8], co[5], copoly)
+    t6 = time.perf_counter()
+    out["noise"] = {"solve_seconds": t4 - t3, "solve_status": info.status, "fits_seconds": t5 - t4,
+                    "generalaverage_seconds": t6 - t5, "finite": bool(np.isfinite(J).all())}
+    M.close()
+    Mp.close()
+    lat.close()
+    if a.cpu_cycles > 0 and not a.no_cpu:
+        import oracle
+
+        threads = oracle.use_timing_build(a.cpu_threads or None)
+        ol = oracle.OracleLattice(*dims, bc=(1, 1, 1, -1))
+        g = qq.Lattice(*dims, bc=(1, 1, 1, -1))
+        u, _ = g.heatbath(6.0, a.sweeps, seed=3)
+        g.close()
+        ol.set_gauge(u)
+        c0 = time.perf_counter()
+        ol.eigmodes(1, (m, k), a.cpu_cycles, kappa)
+        c1 = time.perf_counter()
+        out["cpu_baseline"] = {"kind": "port", "cores": threads, "cycles_timed": a.cpu_cycles,
+                               "seconds": c1 - c0,
+                               "modes_of_M_seconds_scaled": (c1 - c0) / a.cpu_cycles * cyc,
+                               "sample": f"{a.cpu_cycles} cycle(s) of the kind-1 eigen-iteration, scaled to {cyc}"}
+    return out
+
+
 def main(argv=None):
     a = parse(argv)
     if a.mode != "solve":
         fn = {"dslash": run_dslash, "c3": run_c3, "c4": run_c4, "shift": run_shift, "twvev": run_twvev,
-              "learned": run_learned}[a.mode]
+              "learned": run_learned, "eigen": run_eigen}[a.mode]
         print(json.dumps(fn(a)), flush=True)
         return 0
     rank, world, local = dist_env()

@@ -41,7 +41,7 @@ EXPORTED = [
     "qq_net_set_weights", "qq_net_apply", "qq_net_grad", "qq_net_train", "qq_fgmres", "qq_pionrho", "qq_twvev", "qq_twaverage", "qq_twistdiscon", "qq_average", "qq_momfacs",
     "qq_fgmresdr", "qq_fermprop_uneven",
     "qq_eigmodes", "qq_eig_destroy", "qq_eig_info", "qq_eig_vector", "qq_xigenerator", "qq_eigaverage",
-    "qq_ppcoeffs", "qq_ppaverage", "qq_xipolygenerator", "qq_generalaverage",
+    "qq_ppcoeffs", "qq_ppaverage", "qq_xipolygenerator", "qq_generalaverage", "qq_smear", "qq_mesoncorr",
 ]
 
 
@@ -172,6 +172,8 @@ def load_library() -> C.CDLL:
         "qq_xigenerator": ([P, P, D, DP], I),
         "qq_eigaverage": ([P, P, P, P, D, DP, I, I, P], I),
         "qq_ppcoeffs": ([P, P, P, D, I, DP], I),
+        "qq_smear": ([P, P, P, P, P, D, I], I),
+        "qq_mesoncorr": ([P, P, P, IP, I, P, P], I),
         "qq_ppaverage": ([P, I, DP, P, P, P, P, D, I, P], I),
         "qq_xipolygenerator": ([P, P, D, DP, DP], I),
         "qq_generalaverage": ([P, P, P, P, P, P, P, D, I, I, DP, DP, DP, DP, P], I),
@@ -497,6 +499,24 @@ class Lattice:
         _check(self.lib.qq_average(self._ctx, _ptr(be), _ptr(bo), _ptr(xe), _ptr(xo), float(kappa), int(nsub),
                                    int(nmom), int(nop), _ptr(mf) if mf is not None else None, _ptr(J)))
         return J
+
+    def smear(self, ge, go, asmear, nsmear):
+        """qq_smear: nsmear sweeps of gauge-covariant spatial smearing of a reference-layout
+        pair; returns (he, ho)."""
+        he, ho = self.new_half(), self.new_half()
+        _check(self.lib.qq_smear(self._ctx, _ptr(he), _ptr(ho), _ptr(ge), _ptr(go), float(asmear), int(nsmear)))
+        return he, ho
+
+    def mesoncorr(self, q, src, qbar=None, channels=0):
+        """qq_mesoncorr: q and qbar as (12, 2) + half_shape (column (jc-1)*4 + jd-1, even
+        then odd half).  Returns corrRe, corrIm as (28, 9, 9, 9, nt) arrays (the reverse of
+        the Fortran (nt, -4:4, -4:4, -4:4, 28))."""
+        re = np.zeros((28, 9, 9, 9, self.dims[3]))
+        im = np.zeros_like(re)
+        sv = np.ascontiguousarray(src, dtype=np.int32)
+        _check(self.lib.qq_mesoncorr(self._ctx, _ptr(q), _ptr(qbar) if qbar is not None else None,
+                                     sv.ctypes.data_as(C.POINTER(C.c_int)), int(channels), _ptr(re), _ptr(im)))
+        return re, im
 
     def ppcoeffs(self, be, bo, kappa, p):
         """qq_ppcoeffs: the least-squares polynomial of ppaverage* (complex (p,))."""

@@ -323,6 +323,25 @@ int qq_average(qq_ctx* ctx, const double* be, const double* bo, const double* xe
  * momfac(nvhalf, 2, 16, 4, 5), nvhalf = nx*ny*nz*nt/32. */
 int qq_momfacs(const int dims[4], const int io[3], double* momfac);
 
+/* smear Q/diracops.f90:712-858: nsmear sweeps of gauge-covariant spatial smearing
+ * h <- (1 - 6 asmear) h + asmear sum_{mu=1..3} [U_mu(x) h(x+mu) + U_mu(x-mu)^+ h(x-mu)]
+ * (spin diagonal, bc(mu) across the edge) of the reference-layout pair (ge, go) into
+ * (he, ho); host or device. */
+int qq_smear(qq_ctx* ctx, double* he, double* ho, const double* ge, const double* go, double asmear,
+             int nsmear);
+/* mesoncorr Q/quark.f90:1297-2137, the correlators of one (q, qbar) propagator pair:
+ * q: the 12 propagator columns of a point source src (1-based), column (jc - 1) * 4 +
+ * (jd - 1) for source colour jc and spin jd, each the even then the odd reference-layout
+ * half (2 * 6 * ntotal * 64 doubles per column; host or device); qbar the same for the
+ * antiquark (NULL: q).  corrRe, corrIm(nt, -4:4, -4:4, -4:4, 28) (Fortran order, host or
+ * device): per operator pair ii of the reference's table (corrsp set) the slice sums of
+ * the contraction times e^{2 pi i p.(x - src)/L}.  channels 0: the pairs the reference
+ * evaluates (P->P ii = 2, S->P ii = 11, P->S ii = 22; the rest zero, :1869-1870);
+ * 1: all 28.  Sink smearing is qq_smear on each column first; the file handling
+ * (FPread of the columns, the MESON.LOG lines) stays with the caller (qq_fpread). */
+int qq_mesoncorr(qq_ctx* ctx, const double* q, const double* qbar, const int src[4], int channels,
+                 double* corrRe, double* corrIm);
+
 /* ---- eigenmode subtraction of the Wilson loop driver (testFUNC,
  * Q/disconloops.f90:1980-2569) ----
  * A qq_eig handle holds kept eigenmodes on the device (right vectors R and, for kind 1,

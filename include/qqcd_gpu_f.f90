@@ -426,6 +426,25 @@ module qqcd_gpu
       integer(c_int) :: st
     end function qq_momfacs
 
+    function qq_smear(ctx, he, ho, ge, go, asmear, nsmear) bind(C, name="qq_smear") result(st)
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: ctx
+      real(c_double), intent(out) :: he(*), ho(*)
+      real(c_double), intent(in) :: ge(*), go(*)
+      real(c_double), value :: asmear
+      integer(c_int), value :: nsmear
+      integer(c_int) :: st
+    end function qq_smear
+    function qq_mesoncorr(ctx, q, qbar, src, channels, corrRe, corrIm) bind(C, name="qq_mesoncorr") result(st)
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: ctx
+      real(c_double), intent(in) :: q(*), qbar(*)
+      integer(c_int), intent(in) :: src(4)
+      integer(c_int), value :: channels
+      real(c_double), intent(out) :: corrRe(*), corrIm(*)
+      integer(c_int) :: st
+    end function qq_mesoncorr
+
     ! ---- eigenmode subtraction of the Wilson loop driver ----
     function qq_eigmodes(ctx, kind, nGMRES, ncycles, kappa, se, so, eig, numEV, evals) &
         bind(C, name="qq_eigmodes") result(st)

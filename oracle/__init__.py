@@ -95,6 +95,8 @@ def lib() -> C.CDLL:
             "oq_xigenerator": ([P, DP, I, D, DP, DP, I, DP], None),
             "oq_eigaverage": ([P, DP, I, I, I, DP, DP, D, DP, DP, DP, I, DP], None),
             "oq_loop_slices": ([P, DP, DP, DP, DP, DP, I, D, DP], None),
+            "oq_smear": ([P, DP, DP, DP, DP, DP, D, I], None),
+            "oq_mesoncorr": ([P, DP, DP, IP, I, DP, DP], None),
             "oq_ppcoeffs": ([P, DP, DP, DP, D, I, DP], None),
             "oq_ppaverage": ([P, DP, I, DP, DP, DP, DP, DP, D, I, DP], None),
             "oq_xipolygenerator": ([P, DP, I, D, DP, DP, DP, DP], None),
@@ -455,6 +457,22 @@ class OracleLattice:
                                 int(eigstart), int(eigstep), _dp(self._cplx2(co11)), _dp(self._cplx2(co8)),
                                 _dp(self._cplx2(co5)), _dp(self._cplx2(copoly)), _dp(J))
         return J
+
+    def smear(self, ge, go, asmear, nsmear):
+        he, ho = self.new_half(), self.new_half()
+        lib().oq_smear(self._g, _dp(self.u), _dp(he), _dp(ho), _dp(np.ascontiguousarray(ge)),
+                       _dp(np.ascontiguousarray(go)), float(asmear), int(nsmear))
+        return he, ho
+
+    def mesoncorr(self, q, src, qbar=None, channels=0):
+        """mesoncorr's correlators: q (12, 2) + half_shape; returns corrRe, corrIm as
+        (28, 9, 9, 9, nt) numpy arrays (the reverse of the Fortran order)."""
+        re = np.zeros((28, 9, 9, 9, self.dims[3]))
+        im = np.zeros_like(re)
+        _, sp = _ip(src)
+        qb = np.ascontiguousarray(q if qbar is None else qbar)
+        lib().oq_mesoncorr(self._g, _dp(np.ascontiguousarray(q)), _dp(qb), sp, int(channels), _dp(re), _dp(im))
+        return re, im
 
     def twvev(self, kappa, delta=0.0, io=(1, 1, 1), dobndry=0, ir=1, nsub=6, nmom=5, nop=6):
         """twvev (Q/vevbleft.f90:757-2536) on the stored gauge field: Jvev as a numpy

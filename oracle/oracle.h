@@ -197,6 +197,13 @@ void oq_generalaverage(const oq_geom* g, const double* u, int n1, const double* 
                        double kappa, int eigstart, int eigstep, const double* co11, const double* co8,
                        const double* co5, const double* copoly, double* Jave);
 
+// Sink smearing and the correlators of mesoncorr (meson.cpp).  q, qbar: 12 columns of two
+// reference-layout halves; corrRe, corrIm(nt, -4:4, -4:4, -4:4, 28).
+void oq_smear(const oq_geom* g, const double* u, double* he, double* ho, const double* ge,
+              const double* go, double asmear, int nsmear);
+void oq_mesoncorr(const oq_geom* g, const double* q, const double* qbar, const int src[4], int channels,
+                  double* corrRe, double* corrIm);
+
 void oq_coldstart(const oq_geom* g, double* u);
 // The reference's pseudo-heatbath for the Wilson plaquette action at beta (sweep
 // C/cfgsprops.f90:1973-2001, staple G/gaugetools.f90:39-345, phbup / su2up / sprd1

@@ -42,6 +42,7 @@ EXPORTED = [
     "qq_fgmresdr", "qq_fermprop_uneven",
     "qq_eigmodes", "qq_eig_destroy", "qq_eig_info", "qq_eig_vector", "qq_xigenerator", "qq_eigaverage",
     "qq_ppcoeffs", "qq_ppaverage", "qq_xipolygenerator", "qq_generalaverage", "qq_smear", "qq_mesoncorr",
+    "qq_vev", "qq_discon",
 ]
 
 
@@ -60,7 +61,7 @@ class qq_solve_info(C.Structure):
     _fields_ = [("status", C.c_int), ("itercount", C.c_int), ("mvp", C.c_int), ("ncycles", C.c_int),
                 ("true_rel", C.c_double), ("seconds", C.c_double), ("nhist", C.c_int),
                 ("hist", C.c_double * 1024), ("hist_mvp", C.c_int * 1024), ("nritz", C.c_int),
-                ("ritz", C.c_double * 1024), ("fallback", C.c_int)]
+                ("ritz", C.c_double * 1024), ("fallback", C.c_int), ("finished_by", C.c_int)]
 
 
 class qq_method(C.Structure):
@@ -87,6 +88,7 @@ class SolveInfo:
     hist_mvp: np.ndarray
     ritz: np.ndarray
     fallback: int = 0
+    finished_by: int = 0
 
     @classmethod
     def from_c(cls, s: qq_solve_info) -> "SolveInfo":
@@ -94,7 +96,8 @@ class SolveInfo:
         nr = s.nritz
         r = np.array(s.ritz[: 2 * nr]).reshape(nr, 2)
         return cls(s.status, s.itercount, s.mvp, s.ncycles, s.true_rel, s.seconds,
-                   np.array(s.hist[:n]), np.array(s.hist_mvp[:n]), r[:, 0] + 1j * r[:, 1], s.fallback)
+                   np.array(s.hist[:n]), np.array(s.hist_mvp[:n]), r[:, 0] + 1j * r[:, 1], s.fallback,
+                   s.finished_by)
 
 
 _lib = None
@@ -179,6 +182,8 @@ def load_library() -> C.CDLL:
         "qq_generalaverage": ([P, P, P, P, P, P, P, D, I, I, DP, DP, DP, DP, P], I),
         "qq_twaverage": ([P, P, P, P, P, D, D, IP, I, I, I, I, I, P], I),
         "qq_twistdiscon": ([P, I, I, DP, P, D, IP, I, I, I, I, I, P, P, P], I),
+        "qq_vev": ([P, D, IP, P, P, P], I),
+        "qq_discon": ([P, I, I, D, P, IP, I, I, I, P, P, P], I),
         "qq_heatbath": ([P, D, I, C.c_ulonglong, P, DP], I),
         "qq_ctx_stream": ([P, C.POINTER(P)], I),
         "qq_launch_count": ([], C.c_longlong),
@@ -701,6 +706,35 @@ class Lattice:
         if per_noise:
             return J, [SolveInfo.from_c(i) for i in infos], Jn
         return J, [SolveInfo.from_c(i) for i in infos]
+
+    def vev(self, kappa: float, io=(1, 1, 1)):
+        """vev (qq_vev): the Wilson loop driver's perturbative vacuum values on the uploaded
+        gauge field.  Returns (Jvev as an array (5 op, 5 momenta, nt, 2), the average
+        plaquette, <psibar psi>)."""
+        J = np.zeros((5, 5, self.dims[3], 2))
+        plaq = np.zeros(1)
+        psi = np.zeros(1)
+        iov = np.ascontiguousarray(io, dtype=np.int32)
+        _check(self.lib.qq_vev(self._ctx, float(kappa), iov.ctypes.data_as(C.POINTER(C.c_int)), _ptr(J),
+                               _ptr(plaq), _ptr(psi)))
+        return J, float(plaq[0]), float(psi[0])
+
+    def discon(self, noise_kind: int, nnoise: int, kappa: float, nsub: int = 6, nmom: int = 5, nop: int = 5,
+               io=(1, 1, 1), solver: int = 0, m: int = 30, k: int = 10, precision: int = 32, rhs_block: int = 12,
+               tol: float = 1e-10, max_outer: int = 0, deflate: int = 0, defl_tol: float = 1e-5):
+        """discon (qq_discon), one run of the Wilson loop driver: Jtotal as an array (nop, nmom,
+        nsub, nt, 2), the vev's Jvev (5, 5, nt, 2) and the per-noise solve reports.  Call
+        initlagfib first, as the reference does."""
+        J = np.zeros((nop, nmom, nsub, self.dims[3], 2))
+        Jv = np.zeros((5, 5, self.dims[3], 2))
+        infos = (qq_solve_info * nnoise)()
+        meth = qq_method(m, k, precision, rhs_block, tol, max_outer, solver, deflate, defl_tol)
+        iov = np.ascontiguousarray(io, dtype=np.int32)
+        st = self.lib.qq_discon(self._ctx, int(noise_kind), int(nnoise), float(kappa), C.byref(meth),
+                                iov.ctypes.data_as(C.POINTER(C.c_int)), int(nsub), int(nmom), int(nop), _ptr(J),
+                                _ptr(Jv), infos)
+        _check(st, allow_not_converged=True)
+        return J, Jv, [SolveInfo.from_c(i) for i in infos]
 
     def twaverage_level0(self, be, bo, xe, xo, kappa: float, delta: float = 0.0, dobndry: int = 0):
         """Level-0 loop traces of one noise (qq_twaverage_level0): J[iop, t, re/im]."""

@@ -332,6 +332,7 @@ void init_scalars(double* sc, const PerRhs& R) {
   sc[SC_CHK_R] = R.rn;
   sc[SC_CHK_ITS] = 0.0;
   sc[SC_FAIL] = 0.0;
+  sc[SC_NRST] = 0.0;
 }
 
 }  // namespace
@@ -465,6 +466,8 @@ int bicgstab_block_sync(qq_ctx* c, std::vector<PerRhs*>& rhs, int prec, double t
         sk[SC_CHK_R] = R.rn;
         sk[SC_CHK_ITS] = its;
       }
+      const bool restart = (hctl[CTL_RESTART] >> k) & 1u;
+      hctl[CTL_RESTART] &= ~(1u << k);
       if (!std::isfinite(R.rn)) {
         st.fallback = FAIL_NAN;
         active &= ~(1u << k);
@@ -476,6 +479,10 @@ int bicgstab_block_sync(qq_ctx* c, std::vector<PerRhs*>& rhs, int prec, double t
         continue;
       }
       QQ_TRY(block_slot(c, prec, nb, k, r.sp(), R.r64.sp(), 0));
+      if (restart) {  // the residual becomes the shadow residual (reinsert_rho sees the mark)
+        QQ_TRY(block_slot(c, prec, nb, k, rhat.sp(), R.r64.sp(), 0));
+        hctl[CTL_RESTART] |= 1u << k;
+      }
       R.rmax = R.rn;
       sk[SC_RMAX] = R.rmax;
       sk[SC_R2] = R.rn * R.rn;
@@ -619,6 +626,7 @@ int bicgstab_block(qq_ctx* c, std::vector<PerRhs*>& rhs, int prec, double tol, d
     reliable_decide_kernel<<<1, 1, 0, c->st>>>(Sd, ds, ctl, k, tol, dhist, dhits, kHist);
     QQ_CK(cudaGetLastError());
     QQ_TRY(block_slot(c, prec, nb, k, r.sp(), R.r64.sp(), 0, ctl + CTL_INSERT));
+    QQ_TRY(block_slot(c, prec, nb, k, rhat.sp(), R.r64.sp(), 0, ctl + CTL_RESTART));  // a restart
     QQ_TRY(reinsert_rho(c, prec, A, k, ds, ctl, ctl + CTL_INSERT));
     reliable_resume_kernel<<<1, 1, 0, c->st>>>(ctl, k);
     QQ_CK(cudaGetLastError());
@@ -824,8 +832,39 @@ int batch_solve(qq_ctx* c, int nrhs, const double* be, const double* bo, const d
       std::vector<SolveStats> bst(nb);
       for (int k = 0; k < nb; ++k) blk.push_back(R[i0 + k].get());
       tic();
-      int st = bicgstab_block(c, blk, prec, tol_even, 0.1, maxiter, window, kappa,
-                              defl.k > 0 ? &defl : nullptr, bst);
+      int st = bicgstab_block(c, blk, prec, tol_even, 0.1, maxiter, window, kappa, defl.k > 0 ? &defl : nullptr,
+                              bst);
+      // A 16-bit iteration that stopped short (near critical kappa it stalls at a true
+      // residual of ~1e-2: 11 or 8 significant bits cannot resolve the low modes) is
+      // continued by the batched FP32 BiCGStab from its FP64 solution, before any
+      // right-hand side goes to FP64 GMRES-DR; fallback keeps the 16-bit reason.
+      if ((prec == P16 || prec == PB16) && (st == QQ_OK || st == QQ_NOT_CONVERGED)) {
+        std::vector<PerRhs*> again;
+        std::vector<int> which;
+        for (int k = 0; k < nb; ++k)
+          if (!blk[k]->done) {
+            again.push_back(blk[k]);
+            which.push_back(k);
+          }
+        if (!again.empty()) {
+          std::vector<SolveStats> bst32(again.size());
+          st = bicgstab_block(c, again, P32, tol_even, 0.1, maxiter, window, kappa, defl.k > 0 ? &defl : nullptr,
+                              bst32);
+          for (size_t i = 0; i < again.size(); ++i) {
+            SolveStats& b0 = bst[which[i]];
+            const SolveStats& b1 = bst32[i];
+            const int mvp0 = b0.mvp;
+            b0.itercount += b1.itercount;
+            b0.mvp += b1.mvp;
+            b0.true_rel = b1.true_rel;
+            for (size_t h = 0; h < b1.hist.size(); ++h) {
+              b0.hist.push_back(b1.hist[h]);
+              b0.hist_mvp.push_back(mvp0 + b1.hist_mvp[h]);
+            }
+            if (again[i]->done) b0.finished_by = 32;
+          }
+        }
+      }
       const double sec = toc();
       // Every right-hand side the batched BiCGStab did not finish -- a breakdown (NaN,
       // vanishing rho or omega), a stall, or the iteration limit; bst[k].fallback holds
@@ -860,6 +899,7 @@ int batch_solve(qq_ctx* c, int nrhs, const double* be, const double* bo, const d
           fs.itercount += bst[k].itercount;
           fs.mvp += bst[k].mvp + 1;
           fs.fallback = bst[k].fallback != FAIL_NONE ? bst[k].fallback : FAIL_MAXITER;
+          fs.finished_by = 64;
           bst[k] = fs;
           fb_status[k] = sf == QQ_OK ? QQ_OK : QQ_NOT_CONVERGED;
         }

@@ -188,7 +188,8 @@ bool is_device_ptr(const void* p);
 // ---- Krylov solvers (qq_solvers.cu) ----
 struct SolveStats {
   int itercount = 0, mvp = 0, ncycles = 0;
-  int fallback = 0;  // 1: the reference method finished this solve (qq_solve_info.fallback)
+  int fallback = 0;     // 1: the reference method finished this solve (qq_solve_info.fallback)
+  int finished_by = 0;  // qq_solve_info.finished_by
   double true_rel = 0.0;
   std::vector<double> hist;
   std::vector<int> hist_mvp;

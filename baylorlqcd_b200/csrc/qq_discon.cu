@@ -31,10 +31,13 @@ namespace {
 // The noise loop: per noise (generator order), draw, solve, take the kappa-scaled traces
 // J(2, nt, nmom, 6) and hand them to add().  pre (may be empty) runs on the calling
 // thread while the first block of noises is drawn; it must not draw random numbers.
-int discon_loop(qq_ctx* c, int noise_kind, int nnoise, const double kappa[2], const qq_method* method,
-                double delta, const int io[3], int dobndry, int ir, int nmom,
-                const std::function<void(const double*)>& add, qq_solve_info* infos,
-                const std::function<int()>& pre = {}) {
+using PerNoise = std::function<int(const double* be, const double* bo, const double* xe, const double* xo)>;
+
+// The noise loop: per noise (generator order), draw, solve and hand the device pair
+// (noise, solution) to per_noise.  pre (may be empty) runs on the calling thread while the
+// first block of noises is drawn; it must not draw random numbers.
+int discon_loop_fn(qq_ctx* c, int noise_kind, int nnoise, const double kappa[2], const qq_method* method,
+                   const PerNoise& per_noise, qq_solve_info* infos, const std::function<int()>& pre = {}) {
   if (noise_kind != 2 && noise_kind != 4) return set_error(QQ_BAD_ARG, "noise_kind must be 2 or 4");
   if (nnoise < 1) return set_error(QQ_BAD_ARG, "nnoise must be >= 1");
   if (method->solver < 0 || method->solver > 2) return set_error(QQ_BAD_ARG, "solver must be 0, 1 or 2");
@@ -48,7 +51,6 @@ int discon_loop(qq_ctx* c, int noise_kind, int nnoise, const double kappa[2], co
   QQ_CK(dbo.alloc(sizeof(double) * nv * block));
   QQ_CK(dxe.alloc(sizeof(double) * nv * block));
   QQ_CK(dxo.alloc(sizeof(double) * nv * block));
-  std::vector<double> Jn((size_t)12 * nt * nmom);
   // Host noise, double-buffered: a second thread draws the next block while the device
   // solves this one.  The generator has one user at a time and draws noise by noise,
   // be then bo, exactly as many noises as requested: the stream is the reference's.
@@ -129,16 +131,31 @@ int discon_loop(qq_ctx* c, int noise_kind, int nnoise, const double kappa[2], co
       break;
     }
     if (st == QQ_NOT_CONVERGED) rc = QQ_NOT_CONVERGED;
-    for (int k = 0; k < nb; ++k) {
-      QQ_TRY(traces_mom(c, dbe.as<double>() + nv * k, dbo.as<double>() + nv * k, dxe.as<double>() + nv * k,
-                        dxo.as<double>() + nv * k, kappa[0], delta, io, dobndry, nmom, Jn.data(), ir));
-      add(Jn.data());
-    }
+    for (int k = 0; k < nb; ++k)
+      QQ_TRY(per_noise(dbe.as<double>() + nv * k, dbo.as<double>() + nv * k, dxe.as<double>() + nv * k,
+                       dxo.as<double>() + nv * k));
     if (gen.t.joinable()) gen.t.join();
     if (gen_rc != QQ_OK) return gen_rc;
     cur = 1 - cur;
   }
   return rc;
+}
+
+// The twisted-mass form: the kappa-scaled level-0 traces J(2, nt, nmom, 6) of every noise
+// handed to add().
+int discon_loop(qq_ctx* c, int noise_kind, int nnoise, const double kappa[2], const qq_method* method,
+                double delta, const int io[3], int dobndry, int ir, int nmom,
+                const std::function<void(const double*)>& add, qq_solve_info* infos,
+                const std::function<int()>& pre = {}) {
+  std::vector<double> Jn((size_t)12 * c->g.n[3] * nmom);
+  return discon_loop_fn(
+      c, noise_kind, nnoise, kappa, method,
+      [&](const double* be, const double* bo, const double* xe, const double* xo) -> int {
+        QQ_TRY(traces_mom(c, be, bo, xe, xo, kappa[0], delta, io, dobndry, nmom, Jn.data(), ir));
+        add(Jn.data());
+        return QQ_OK;
+      },
+      infos, pre);
 }
 
 // Levels twAverage fills (:4519-4580): 1 always, 4 for nsub = 4 or 6, 6 for nsub = 6
@@ -274,5 +291,64 @@ extern "C" int qq_twistdiscon(qq_ctx* c, int noise_kind, int nnoise, const doubl
       }
     QQ_CK(cudaMemcpy(Jnoise, jn.data(), sizeof(double) * jn.size(), cudaMemcpyDefault));
   }
+  return rc;
+}
+
+extern "C" int qq_vev(qq_ctx* c, double kappa, const int io[3], double* Jvev, double* plaq, double* psi);
+
+// discon, Q/disconloops.f90:3445-3608 (one run): Jtotal(isub >= 2) starts as the vev
+// Jvev; every noise's average (nsub levels, nmom momenta with the momfacs factors about
+// io) is added; the sum is divided by the number of noises (Jvev included, as the
+// reference does) and by nx*ny*nz.  The reference solves its noises with QMR (inverter
+// 2); here the method's solver runs.
+extern "C" int qq_discon(qq_ctx* c, int noise_kind, int nnoise, double kappa, const qq_method* method,
+                         const int io[3], int nsub, int nmom, int nop, double* Jtotal, double* Jvev_out,
+                         qq_solve_info* infos) {
+  if (!c) return set_error(QQ_BAD_ARG, "null context");
+  if (!method || !io || !Jtotal) return set_error(QQ_BAD_ARG, "null argument");
+  if (nsub < 1 || nsub > 6) return set_error(QQ_BAD_ARG, "nsub must be 1..6");
+  if (nmom < 1 || nmom > 5) return set_error(QQ_BAD_ARG, "nmom must be 1..5");
+  if (nop < 1 || nop > 9) return set_error(QQ_BAD_ARG, "nop must be 1..9");
+  QQ_CK(cudaSetDevice(c->device));
+  const int nt = c->g.n[3];
+  const size_t n = (size_t)2 * nt * nsub * nmom * nop, n9 = (size_t)2 * nt * nsub * nmom * 9;
+  std::vector<double> jv((size_t)2 * nt * 25), jt(n, 0.0), ja(n9);
+  QQ_TRY(qq_vev(c, kappa, io, jv.data(), nullptr, nullptr));
+  if (Jvev_out) QQ_CK(cudaMemcpy(Jvev_out, jv.data(), sizeof(double) * jv.size(), cudaMemcpyDefault));
+  auto at = [&](int ri, int t, int isub, int im, int iop) {  // Jtotal(2, nt, nsub, nmom, nop), 0-based
+    return ((((size_t)iop * nmom + im) * nsub + isub) * nt + t) * 2 + ri;
+  };
+  for (int iop = 0; iop < std::min(nop, 5); ++iop)  // :3545-3547
+    for (int im = 0; im < nmom; ++im)
+      for (int isub = 1; isub < nsub; ++isub)
+        for (int t = 0; t < nt; ++t)
+          for (int ri = 0; ri < 2; ++ri)
+            jt[at(ri, t, isub, im, iop)] = jv[((((size_t)iop * 5) + im) * nt + t) * 2 + ri];
+  DevBuf dmf;
+  if (nmom > 1) {
+    const size_t nmf = (size_t)5 * 4 * 16 * 2 * (c->g.vh / 16);
+    std::vector<double> mf(nmf);
+    QQ_TRY(qq_momfacs(c->g.n, io, mf.data()));
+    QQ_CK(dmf.alloc(sizeof(double) * nmf));
+    QQ_CK(cudaMemcpy(dmf.p, mf.data(), sizeof(double) * nmf, cudaMemcpyHostToDevice));
+  }
+  const double kap[2] = {kappa, 0.0};
+  const int rc = discon_loop_fn(
+      c, noise_kind, nnoise, kap, method,
+      [&](const double* be, const double* bo, const double* xe, const double* xo) -> int {
+        QQ_TRY(qq_average(c, be, bo, xe, xo, kappa, nsub, nmom, 9, nmom > 1 ? dmf.as<double>() : nullptr,
+                          ja.data()));
+        for (int iop = 0; iop < nop; ++iop)
+          for (int im = 0; im < nmom; ++im)
+            for (int isub = 0; isub < nsub; ++isub)
+              for (int t = 0; t < nt; ++t)
+                for (int ri = 0; ri < 2; ++ri) jt[at(ri, t, isub, im, iop)] += ja[((((size_t)iop * nmom + im) * nsub + isub) * nt + t) * 2 + ri];
+        return QQ_OK;
+      },
+      infos);
+  if (rc != QQ_OK && rc != QQ_NOT_CONVERGED) return rc;
+  const double nxyz = (double)c->g.n[0] * c->g.n[1] * c->g.n[2];
+  for (double& v : jt) v = v / (double)nnoise / nxyz;  // :3581-3584
+  QQ_CK(cudaMemcpy(Jtotal, jt.data(), sizeof(double) * n, cudaMemcpyDefault));
   return rc;
 }

@@ -26,18 +26,20 @@ enum ScalSlot : int {
   SC_T2 = 13,      // ||b - A x||^2 of the last reliable update (FP64)
   SC_TRUE = 14,    // ||b - A x|| / ||b|| of the last reliable update
   SC_NUPD = 15,    // reliable updates done
-  SC_RHATN = 16,   // ||rhat|| (the shadow residual is fixed for the whole solve)
+  SC_RHATN = 16,   // ||rhat|| (the shadow residual; replaced only at a restart)
   SC_CHK_R = 17,   // progress anchor: the FP64 true ||b - A x|| that last fell 10x
   SC_CHK_ITS = 18, // iterations done when the anchor was set
   SC_FAIL = 19,    // why the right-hand side was stopped (FailCode), 0 while it runs
-  kScal = 20,
+  SC_NRST = 20,    // restarts after a breakdown so far
+  kScal = 21,
 };
 
 // Control words after the scalar slots: bit k of ACTIVE / PENDING / DONE / INSERT /
-// NAN / FAIL = right-hand side k iterates / awaits its reliable update or convergence
-// test / is finished (converged or stopped) / is re-inserted / stopped on a non-finite
-// value / stopped without converging (reason in its SC_FAIL); ITER counts the
-// iterations of the graph-driven loop.
+// NAN / FAIL / RESTART = right-hand side k iterates / awaits its reliable update or
+// convergence test / is finished (converged or stopped) / is re-inserted / stopped on a
+// non-finite value / stopped without converging (reason in its SC_FAIL) / restarts with
+// its re-inserted residual as the shadow residual; ITER counts the iterations of the
+// graph-driven loop.
 enum CtlWord : int {
   CTL_ACTIVE = 0,
   CTL_PENDING = 1,
@@ -46,7 +48,8 @@ enum CtlWord : int {
   CTL_ITER = 4,
   CTL_NAN = 5,
   CTL_FAIL = 6,
-  kCtlWords = 7
+  CTL_RESTART = 7,
+  kCtlWords = 8
 };
 
 // Why the batched BiCGStab stopped a right-hand side short of its tolerance; the
@@ -55,6 +58,7 @@ enum FailCode : int {
   FAIL_NONE = 0,
   FAIL_NAN = 1,        // a non-finite scalar or residual
   FAIL_BREAKDOWN = 2,  // rho = <rhat, r>, <rhat, v>, ||t|| or omega = <t, s> / ||t||^2 vanished
+                       // again after kMaxRestarts restarts
   FAIL_STALL = 3,      // the FP64 true residual did not fall 10x within the stall window
   FAIL_MAXITER = 4,    // the iteration limit ran out (set by the host)
 };
@@ -63,6 +67,15 @@ enum FailCode : int {
 // |<rhat, r>| <= kBreakEps ||rhat|| ||r||, and the same for omega.  Only a degenerate
 // (numerically zero) product trips it; slow progress is the stall window's business.
 constexpr double kBreakEps = 1e-12;
+
+// Restarts a right-hand side may take after a breakdown before it stops for good.  A
+// restart is a reliable update after which the shadow residual becomes the re-inserted
+// FP64 residual (rho = ||r||^2, beta = 0, so the next search direction is r).  The
+// usual shadow residual rhat = r0 is one spin-colour component at one site for a point
+// source: every <rhat, .> is then a single component, which 16-bit storage against the
+// site's norm (or an exact FP32 cancellation) can make exactly zero while the Krylov
+// space is fine; the residual a few iterations on is spread over the lattice.
+constexpr int kMaxRestarts = 8;
 
 enum BiOp : int {
   OP_DOT_RHAT_R = 0,  // red: <rhat, r>
@@ -214,12 +227,27 @@ __device__ inline void bicg_fail(double* s, unsigned* ctl, int k, int code) {
   if (code == FAIL_NAN) atomicOr(&ctl[CTL_NAN], bit);
 }
 
+// A breakdown of right-hand side k: it restarts (goes pending with the restart mark;
+// its reliable update then replaces the shadow residual) while it has restarts left,
+// else it stops.
+__device__ inline void bicg_breakdown(double* s, unsigned* ctl, int k) {
+  if (s[SC_NRST] < (double)kMaxRestarts) {
+    const unsigned bit = 1u << k;
+    s[SC_NRST] += 1.0;
+    atomicOr(&ctl[CTL_RESTART], bit);
+    atomicAnd(&ctl[CTL_ACTIVE], ~bit);
+    atomicOr(&ctl[CTL_PENDING], bit);
+    return;
+  }
+  bicg_fail(s, ctl, k, FAIL_BREAKDOWN);
+}
+
 // rho' = <rhat, r> arrived: beta = (rho'/rho)(alpha/omega), rho = rho' -- or a stop on a
 // non-finite or vanishing rho' (rnorm = ||r||).
 __device__ inline void bicg_beta(double* s, unsigned* ctl, int k, double d0, double d1, double rnorm) {
   const double rho = sqrt(d0 * d0 + d1 * d1);
   if (!isfinite(rho)) return bicg_fail(s, ctl, k, FAIL_NAN);
-  if (rho <= kBreakEps * s[SC_RHATN] * rnorm) return bicg_fail(s, ctl, k, FAIL_BREAKDOWN);
+  if (rho <= kBreakEps * s[SC_RHATN] * rnorm) return bicg_breakdown(s, ctl, k);
   auto cdiv = [](double ar, double ai, double br, double bi, double* cr, double* ci) {
     const double den = br * br + bi * bi;
     *cr = (ar * br + ai * bi) / den;
@@ -296,13 +324,13 @@ static __global__ void bicg_scalar_kernel(double* S, const int* slots, const dou
   } else if (step == ST_ALPHA) {
     const double den = sqrt(d0 * d0 + d1 * d1);
     if (!isfinite(den)) return bicg_fail(s, ctl, k, FAIL_NAN);
-    if (!(den > 0.0)) return bicg_fail(s, ctl, k, FAIL_BREAKDOWN);
+    if (!(den > 0.0)) return bicg_breakdown(s, ctl, k);
     cdiv(s[SC_RHO], s[SC_RHO + 1], d0, d1, &s[SC_ALPHA], &s[SC_ALPHA + 1]);
     if (!isfinite(s[SC_ALPHA]) || !isfinite(s[SC_ALPHA + 1])) return bicg_fail(s, ctl, k, FAIL_NAN);
   } else if (step == ST_OMEGA) {
     if (!isfinite(d0) || !isfinite(d1) || !isfinite(d2)) return bicg_fail(s, ctl, k, FAIL_NAN);
     if (!(d2 > 0.0) || sqrt(d0 * d0 + d1 * d1) <= kBreakEps * sqrt(d2) * rnorm)
-      return bicg_fail(s, ctl, k, FAIL_BREAKDOWN);
+      return bicg_breakdown(s, ctl, k);
     s[SC_OMEGA] = d0 / d2;
     s[SC_OMEGA + 1] = d1 / d2;
     s[SC_TT] = d2;
@@ -361,7 +389,8 @@ __global__ void __launch_bounds__(kRedThreads) slot_dot_kernel(int vh, int nb, i
 
 // After right-hand side k's residual was re-inserted (bit k of the insert mask, or
 // unconditionally when `always`): rho' = <rhat, r> from slot_dot_kernel's partials
-// (fixed-order sum), then beta and rho as at ST_BETA.  One block of 256 threads.
+// (fixed-order sum), then beta and rho as at ST_BETA -- or, at a restart (rhat was set
+// to the same residual), rho = ||r||^2 and beta = 0.  One block of 256 threads.
 static __global__ void reliable_rho_kernel(double* S, const int* slots, unsigned* ctl, int k,
                                            const double* partial, int nblocks, int always) {
   if (!always && !((ctl[CTL_INSERT] >> k) & 1u)) return;
@@ -383,6 +412,18 @@ static __global__ void reliable_rho_kernel(double* S, const int* slots, unsigned
   }
   if (threadIdx.x != 0) return;
   double* s = S + (size_t)slots[k] * kScal;
+  const unsigned bit = 1u << k;
+  if (ctl[CTL_RESTART] & bit) {  // rhat was set to this residual: rho = ||r||^2, p = r next
+    atomicAnd(&ctl[CTL_RESTART], ~bit);
+    const double rho = red[0][0];
+    if (!isfinite(rho)) return bicg_fail(s, ctl, k, FAIL_NAN);
+    if (!(rho > 0.0)) return bicg_fail(s, ctl, k, FAIL_BREAKDOWN);
+    s[SC_RHO] = rho;
+    s[SC_RHO + 1] = 0.0;
+    s[SC_BETA] = s[SC_BETA + 1] = 0.0;
+    s[SC_RHATN] = sqrt(rho);
+    return;
+  }
   bicg_beta(s, ctl, k, red[0][0], red[1][0], sqrt(s[SC_R2]));
 }
 
@@ -411,12 +452,14 @@ static __global__ void reliable_decide_kernel(double* S, const int* slots, unsig
   }
   if (!isfinite(rel)) {
     atomicAnd(&ctl[CTL_INSERT], ~bit);
+    atomicAnd(&ctl[CTL_RESTART], ~bit);
     bicg_fail(s, ctl, k, FAIL_NAN);
     return;
   }
   if (!(rel > tol)) {  // converged
     atomicOr(&ctl[CTL_DONE], bit);
     atomicAnd(&ctl[CTL_INSERT], ~bit);
+    atomicAnd(&ctl[CTL_RESTART], ~bit);
   } else {
     s[SC_RMAX] = rn;
     s[SC_R2] = s[SC_T2];

@@ -65,6 +65,10 @@ typedef struct qq_solve_info {
                         <rhat, v>, ||t|| or omega vanished), 3 a stall (the true residual
                         did not fall 10x within qq_method.stall_window iterations),
                         4 the iteration limit */
+  int finished_by;    /* qq_fermprop_batch: what finished this right-hand side -- 0 the batched
+                        BiCGStab in the requested precision, 32 the batched FP32 BiCGStab
+                        after a 16-bit one stopped short (fallback holds why), 64 plain
+                        FP64 GMRES-DR(m, k) */
 } qq_solve_info;
 
 /* ---- context ---- */
@@ -341,6 +345,25 @@ int qq_smear(qq_ctx* ctx, double* he, double* ho, const double* ge, const double
  * (FPread of the columns, the MESON.LOG lines) stays with the caller (qq_fpread). */
 int qq_mesoncorr(qq_ctx* ctx, const double* q, const double* qbar, const int src[4], int channels,
                  double* corrRe, double* corrIm);
+
+/* vev Q/disconloops.f90:4653-5339: the perturbative vacuum values of the Wilson driver's
+ * loop operators from the plaquettes P = U_mu(x) U_nu(x+mu) U_mu(x+nu)^+ U_nu(x)^+ of
+ * every plane, summed per time slice with the reference's momentum weights about io
+ * (1-based), scaled by 8 kappa^4 and its multiplicities and negated: Jvev(2, nt, 5, 5)
+ * (Fortran order, host or device).  plaq (may be NULL): the average plaquette
+ * sum Re Tr P / (18 V); psi (may be NULL): the <psibar psi> value it logs. */
+int qq_vev(qq_ctx* ctx, double kappa, const int io[3], double* Jvev, double* plaq, double* psi);
+/* discon Q/disconloops.f90:3445-3608, one run: Jtotal(2, nt, nsub, nmom, nop) (nop <= 9; the
+ * reference uses 5) = (Jvev on levels 2..nsub + the sum over nnoise Z(2) / Z(4) noises of
+ * average(nsub, nmom, momfacs about io)) / nnoise / (nx ny nz) -- Jvev divided by the
+ * number of noises too, as the reference does.  The noises are solved by the method
+ * (the reference uses QMR, inverter 2, which is not on this path).  Jvev (may be NULL)
+ * receives qq_vev's output.  Call qq_initlagfib first.  The reference repeats this run
+ * numruns = 20 times on one generator stream (20 calls); its numnoises = 0 branch (one
+ * given source, no division) is qq_fermprop followed by qq_average. */
+int qq_discon(qq_ctx* ctx, int noise_kind, int nnoise, double kappa, const qq_method* method,
+              const int io[3], int nsub, int nmom, int nop, double* Jtotal, double* Jvev,
+              qq_solve_info* infos);
 
 /* ---- eigenmode subtraction of the Wilson loop driver (testFUNC,
  * Q/disconloops.f90:1980-2569) ----

@@ -49,6 +49,7 @@ module qqcd_gpu
     integer(c_int) :: nritz
     real(c_double) :: ritz(1024)
     integer(c_int) :: fallback
+    integer(c_int) :: finished_by
   end type qq_solve_info
 
   type, bind(C) :: qq_method
@@ -408,6 +409,27 @@ module qqcd_gpu
       type(qq_solve_info), intent(out) :: infos(*)
       integer(c_int) :: st
     end function qq_twistdiscon
+    function qq_vev(ctx, kappa, io, Jvev, plaq, psi) bind(C, name="qq_vev") result(st)
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: ctx
+      real(c_double), value :: kappa
+      integer(c_int), intent(in) :: io(3)
+      real(c_double), intent(out) :: Jvev(*), plaq, psi
+      integer(c_int) :: st
+    end function qq_vev
+    function qq_discon(ctx, noise_kind, nnoise, kappa, method, io, nsub, nmom, nop, Jtotal, Jvev, infos) &
+        bind(C, name="qq_discon") result(st)
+      import :: c_int, c_ptr, c_double, qq_method, qq_solve_info
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: noise_kind, nnoise
+      real(c_double), value :: kappa
+      type(qq_method), intent(in) :: method
+      integer(c_int), intent(in) :: io(3)
+      integer(c_int), value :: nsub, nmom, nop
+      real(c_double), intent(out) :: Jtotal(*), Jvev(*)
+      type(qq_solve_info), intent(out) :: infos(*)
+      integer(c_int) :: st
+    end function qq_discon
     function qq_average(ctx, be, bo, xe, xo, kappa, nsub, nmom, nop, momfac, Jtime) &
         bind(C, name="qq_average") result(st)
       import :: c_int, c_ptr, c_double

@@ -89,6 +89,7 @@ def lib() -> C.CDLL:
             "oq_orgschur": ([IP, I, DP, I, DP, I, DP, IP], None),
             "oq_twaverage_level0": ([P, DP, DP, DP, DP, DP, D, D, C.c_int, DP], None),
             "oq_twvev": ([P, DP, D, D, IP, I, I, I, I, I, DP], None),
+            "oq_vevw": ([P, DP, IP, D, DP, DP, DP], I),
             "oq_average": ([P, DP, DP, DP, DP, DP, D, I, I, I, DP, DP], None),
             "oq_momfacs": ([P, IP, DP], None),
             "oq_eigmodes": ([P, DP, I, IP, I, DP, DP, DP, DP, DP, DP, IP], I),
@@ -483,6 +484,19 @@ class OracleLattice:
         lib().oq_twvev(self._g, _dp(self.u), float(kappa), float(delta), iop, int(dobndry), int(ir), int(nsub),
                        int(nmom), int(nop), _dp(J))
         return J
+
+    def vev(self, kappa, io=(1, 1, 1)):
+        """vev (Q/disconloops.f90:4653-5339) on the stored gauge field: (Jvev, plaq, psi),
+        Jvev as a numpy array of shape (5 op, 5 momenta, nt, 2), the reverse of the
+        Fortran (2, nt, 5, 5)."""
+        J = np.zeros((5, 5, self.dims[3], 2))
+        plaq = np.zeros(1)
+        psi = np.zeros(1)
+        _, iop = _ip(io)
+        rc = lib().oq_vevw(self._g, _dp(self.u), iop, float(kappa), _dp(J), _dp(plaq), _dp(psi))
+        if rc != 0:
+            raise RuntimeError("oq_vevw: site enumeration disagrees with the site map")
+        return J, float(plaq[0]), float(psi[0])
 
     def twvev_sites(self, sites, kappa, delta=0.0, io=(1, 1, 1), dobndry=0, ir=1, nsub=6):
         """opertemp contributions of the listed 1-based lexicographic sites:

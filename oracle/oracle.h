@@ -158,6 +158,13 @@ void oq_average(const oq_geom* g, const double* u, const double* be, const doubl
 // momfacs: momfac(nvhalf, 2, 16, 4, 5) about the origin io (1-based).
 void oq_momfacs(const oq_geom* g, const int io[3], double* momfac);
 
+// ---- the Wilson loop driver's vacuum values (Q/disconloops.f90 vev; see vevw.cpp) ----
+// Jvev(2, nt, 5, 5), Fortran order (nmom = nop = 5), the average plaquette and
+// <psibar psi>.  io: momentum origin (1-based).  Returns 0, or -1 when the reference's
+// site enumeration disagrees with the pointsource site map.
+int oq_vevw(const oq_geom* g, const double* u, const int io[3], double kappa, double* Jvev, double* plaq,
+            double* psi);
+
 // ---- perturbative vacuum expectation values (Q/vevbleft.f90 twvev; see vev.cpp) ----
 // Jvev(2, nt, 6, nmom, nop), Fortran order; levels 4 (orders kappa^3 / kappa^4, and
 // kappa^1 / kappa^2 when delta /= 0) and 6 (orders kappa^5 / kappa^6, nsub = 6) are

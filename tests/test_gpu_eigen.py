@@ -216,7 +216,7 @@ def test_generalaverage_matches_oracle(small, noise):
     xe[:, :, :, :ol.nvhalf] = rng.standard_normal(xe[:, :, :, :ol.nvhalf].shape)
     xo[:, :, :, :ol.nvhalf] = rng.standard_normal(xo[:, :, :, :ol.nvhalf].shape)
     J_g = lat.generalaverage(m_g, mp_g, ze, zo, xe, xo, k, co[11], co[8], co[5], copoly)
-    J_o = ol.generalaverage(m_o, mp_o, ze, zo, xe, xo, k, co[11], co[8], co[5], copoly)
+    J_o = ol.generalaverage(m_o[:3], mp_o[:2], ze, zo, xe, xo, k, co[11], co[8], co[5], copoly)
     assert J_g.shape == J_o.shape
     scale = np.abs(J_o).max()
     # styles 3 and 5 carry the M modes: whole pairs only (mode counts 2, 4, ...)

@@ -89,11 +89,13 @@ def test_uneven_rejects_bad_group(lattices):
         qq.fermprop_uneven([(lat, be, be, (0.150, 0.0))])
 
 
-def test_stall_forces_gmresdr_fallback(lattices):
+@pytest.mark.parametrize("precision", [32, 16])
+def test_stall_forces_gmresdr_fallback(lattices, precision):
     """The fallback path, triggered on purpose: with a stall window of one iteration no
     right-hand side can show the required 10x fall of its FP64 true residual, so the
     batched BiCGStab stops every one of them after its first iteration (fallback = 3,
-    stagnation) and plain FP64 GMRES-DR(m, k) finishes it from the BiCGStab's solution.
+    stagnation) -- in FP16 first, then in the FP32 iteration that continues a stopped
+    16-bit one -- and plain FP64 GMRES-DR(m, k) finishes it from the BiCGStab's solution.
     Every answer must still reach the FP64 full-lattice residual and agree with the
     oracle's FP64 solve (Q/quark.f90:458-842 with GMRES-DR, Q/inverters.f90:2871-3572)."""
     import baylorlqcd_b200 as qq
@@ -102,11 +104,11 @@ def test_stall_forces_gmresdr_fallback(lattices):
     qq.initlagfib(0, 9)
     be, bo = mixed_sources(qq, lat, 2, 2)
     kappa = (0.1565, 0.005)
-    xe, xo, infos = lat.fermprop_batch(be, bo, kappa, m=16, k=6, precision=32, rhs_block=4, tol=1e-10,
+    xe, xo, infos = lat.fermprop_batch(be, bo, kappa, m=16, k=6, precision=precision, rhs_block=4, tol=1e-10,
                                        solver=1, deflate=0, stall_window=1)
     for i in range(be.shape[0]):
         assert infos[i].status == 0, (i, infos[i])
-        assert infos[i].fallback == 3, (i, infos[i].fallback)
+        assert infos[i].fallback == 3 and infos[i].finished_by == 64, (i, infos[i].fallback, infos[i].finished_by)
         assert infos[i].true_rel <= 1e-10
         xe_o, xo_o, st, _ = ol.fermprop(be[i], bo[i], kappa, inverter=5, resmax=1e-12, nGMRES=(16, 6))
         assert st == 0

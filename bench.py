@@ -428,6 +428,7 @@ def run_ours(a, rank, world, local):
         "error_vs_fp64": {"precision": a.precision, "max_rel": err64, "rhs": npl,
                           "what": "||x - x_FP64|| / ||x_FP64|| over both halves, x_FP64 from plain FP64 GMRES-DR"},
         "fallback": [i.fallback for i in infos],
+        "finished_by": [i.finished_by for i in infos],
         "iterations": [i.itercount for i in infos],
         "plain_gmresdr_sec_per_rhs": plain,
         "plain_gmresdr_iterations": plain_iters,

@@ -33,6 +33,7 @@ notes' figures and the ncu captures under profiles/:
   --mode c4       the uneven batch: 48 Wilson solves over 8^3x16 .. 20^3x40
   --mode shift    multi-shift GMRES-DR against each shift alone
   --mode twvev    perturbative VEVs of the loop operators
+  --mode vevw     the Wilson loop driver's vev against the oracle's restatement
   --mode learned  the learned preconditioner: trained on a training configuration's own
                   GMRES-DR solves (Z(2) sources, FP64 solutions) and deflation vectors,
                   then flexible GMRES-DR with it against plain GMRES-DR on the held-out
@@ -107,7 +108,7 @@ def parse(argv=None):
     p.add_argument("--cpu-threads", type=int, default=0, help="host threads of the CPU legs (0: all)")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--mode", default="solve",
-                   choices=["solve", "dslash", "c3", "c4", "shift", "twvev", "learned", "eigen"])
+                   choices=["solve", "dslash", "c3", "c4", "shift", "twvev", "vevw", "learned", "eigen"])
     p.add_argument("--train-solves", type=int, default=8, help="--mode learned: training solves")
     p.add_argument("--train-steps", type=int, default=200, help="--mode learned: Adam steps")
     p.add_argument("--channels", default="4,8,8,4", help="--mode learned: channels per layer")
@@ -646,6 +647,38 @@ def run_twvev(a):
     return {"mode": "twvev", "lattice": list(dims), "nsub": a.nsub, "seconds": ts}
 
 
+def run_vevw(a):
+    """The Wilson loop driver's vev (qq_vev) on a heatbath configuration: wall time of the
+    entry point (one untimed call, then five), against the oracle's serial restatement of
+    the reference's loops on the same links (the whole computation, timed once), and the
+    largest difference of the two Jvev."""
+    import baylorlqcd_b200 as qq
+
+    dims = tuple(int(x) for x in a.dims.split(","))
+    lat = qq.Lattice(*dims, bc=(1, 1, 1, -1))
+    u, plaq = lat.heatbath(6.0, 20, seed=13)
+    kappa = a.kappa
+    lat.vev(kappa)
+    ts = []
+    for _ in range(5):
+        t0 = time.perf_counter()
+        J, plaq_g, psi = lat.vev(kappa)
+        ts.append(time.perf_counter() - t0)
+    lat.close()
+    res = {"mode": "vevw", "lattice": list(dims), "kappa": kappa, "gpu_seconds": ts, "plaquette": plaq_g}
+    if not a.no_cpu:
+        import oracle
+
+        ol = oracle.OracleLattice(*dims, bc=(1, 1, 1, -1))
+        ol.set_gauge(u)
+        t0 = time.perf_counter()
+        Jo, plaq_o, _ = ol.vev(kappa)
+        res["cpu_baseline"] = {"seconds": time.perf_counter() - t0, "cores": 1, "kind": "port",
+                               "sample": "the whole vev on the same links, the oracle's serial restatement"}
+        res["max_rel_diff"] = float(np.abs(J - Jo).max() / np.abs(Jo).max())
+    return res
+
+
 def run_learned(a):
     """The learned preconditioner on the benchmark operator.  Training configuration
     (heatbath seed 14): --train-solves Z(2) sources solved by plain FP64 GMRES-DR(m,k) to
@@ -765,7 +798,7 @@ def run_eigen(a):
 def main(argv=None):
     a = parse(argv)
     if a.mode != "solve":
-        fn = {"dslash": run_dslash, "c3": run_c3, "c4": run_c4, "shift": run_shift, "twvev": run_twvev,
+        fn = {"dslash": run_dslash, "c3": run_c3, "c4": run_c4, "shift": run_shift, "twvev": run_twvev, "vevw": run_vevw,
               "learned": run_learned, "eigen": run_eigen}[a.mode]
         print(json.dumps(fn(a)), flush=True)
         return 0

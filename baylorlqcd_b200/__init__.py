@@ -61,7 +61,8 @@ class qq_solve_info(C.Structure):
     _fields_ = [("status", C.c_int), ("itercount", C.c_int), ("mvp", C.c_int), ("ncycles", C.c_int),
                 ("true_rel", C.c_double), ("seconds", C.c_double), ("nhist", C.c_int),
                 ("hist", C.c_double * 1024), ("hist_mvp", C.c_int * 1024), ("nritz", C.c_int),
-                ("ritz", C.c_double * 1024), ("fallback", C.c_int), ("finished_by", C.c_int)]
+                ("ritz", C.c_double * 1024), ("fallback", C.c_int), ("finished_by", C.c_int),
+                ("restarts", C.c_int)]
 
 
 class qq_method(C.Structure):
@@ -89,6 +90,7 @@ class SolveInfo:
     ritz: np.ndarray
     fallback: int = 0
     finished_by: int = 0
+    restarts: int = 0
 
     @classmethod
     def from_c(cls, s: qq_solve_info) -> "SolveInfo":
@@ -97,7 +99,7 @@ class SolveInfo:
         r = np.array(s.ritz[: 2 * nr]).reshape(nr, 2)
         return cls(s.status, s.itercount, s.mvp, s.ncycles, s.true_rel, s.seconds,
                    np.array(s.hist[:n]), np.array(s.hist_mvp[:n]), r[:, 0] + 1j * r[:, 1], s.fallback,
-                   s.finished_by)
+                   s.finished_by, s.restarts)
 
 
 _lib = None

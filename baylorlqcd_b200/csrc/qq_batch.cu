@@ -453,6 +453,7 @@ int bicgstab_block_sync(qq_ctx* c, std::vector<PerRhs*>& rhs, int prec, double t
       const int its = (int)hS[(size_t)k * kScal + SC_ITS];
       st.mvp += 2 * (its - st.itercount);
       st.itercount = its;
+      st.restarts = (int)hS[(size_t)k * kScal + SC_NRST];
       if (!((pending >> k) & 1u)) continue;
       double* sk = &hS[(size_t)k * kScal];
       // reliable update
@@ -662,6 +663,7 @@ int bicgstab_block(qq_ctx* c, std::vector<PerRhs*>& rhs, int prec, double tol, d
       if (nupd > 0) st.true_rel = sk[SC_TRUE];
       nupd_all += nupd;
       if ((failed >> k) & 1u) st.fallback = (int)sk[SC_FAIL];
+      st.restarts = (int)sk[SC_NRST];
     }
     gl.count(hc[CTL_ITER], nupd_all);
     done = hc[CTL_DONE] & ~failed;  // converged
@@ -749,6 +751,7 @@ int bicgstab_block(qq_ctx* c, std::vector<PerRhs*>& rhs, int prec, double tol, d
     rhs[k]->done = (done >> k) & 1u;
     if ((failed >> k) & 1u) stats[k].fallback = (int)hS[(size_t)k * kScal + SC_FAIL];
     else if (!rhs[k]->done) stats[k].fallback = FAIL_MAXITER;
+    stats[k].restarts = (int)hS[(size_t)k * kScal + SC_NRST];
   }
   return rc == QQ_OK && (done & all) == all ? QQ_OK : QQ_NOT_CONVERGED;
 }
@@ -856,6 +859,7 @@ int batch_solve(qq_ctx* c, int nrhs, const double* be, const double* bo, const d
             const int mvp0 = b0.mvp;
             b0.itercount += b1.itercount;
             b0.mvp += b1.mvp;
+            b0.restarts += b1.restarts;
             b0.true_rel = b1.true_rel;
             for (size_t h = 0; h < b1.hist.size(); ++h) {
               b0.hist.push_back(b1.hist[h]);
@@ -900,6 +904,7 @@ int batch_solve(qq_ctx* c, int nrhs, const double* be, const double* bo, const d
           fs.mvp += bst[k].mvp + 1;
           fs.fallback = bst[k].fallback != FAIL_NONE ? bst[k].fallback : FAIL_MAXITER;
           fs.finished_by = 64;
+          fs.restarts = bst[k].restarts;
           bst[k] = fs;
           fb_status[k] = sf == QQ_OK ? QQ_OK : QQ_NOT_CONVERGED;
         }

@@ -190,6 +190,7 @@ struct SolveStats {
   int itercount = 0, mvp = 0, ncycles = 0;
   int fallback = 0;     // 1: the reference method finished this solve (qq_solve_info.fallback)
   int finished_by = 0;  // qq_solve_info.finished_by
+  int restarts = 0;     // qq_solve_info.restarts
   double true_rel = 0.0;
   std::vector<double> hist;
   std::vector<int> hist_mvp;

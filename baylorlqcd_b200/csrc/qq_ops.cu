@@ -473,6 +473,7 @@ void fill_info(qq_solve_info* info, int status, const SolveStats& s, double seco
   info->seconds = seconds;
   info->fallback = s.fallback;
   info->finished_by = s.finished_by;
+  info->restarts = s.restarts;
   info->nhist = (int)std::min<size_t>(s.hist.size(), 1024);
   for (int i = 0; i < info->nhist; ++i) {
     info->hist[i] = s.hist[i];

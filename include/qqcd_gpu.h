@@ -69,6 +69,8 @@ typedef struct qq_solve_info {
                         BiCGStab in the requested precision, 32 the batched FP32 BiCGStab
                         after a 16-bit one stopped short (fallback holds why), 64 plain
                         FP64 GMRES-DR(m, k) */
+  int restarts;       /* qq_fermprop_batch: restarts of the batched BiCGStab after a breakdown
+                        (the re-inserted residual became the shadow residual) */
 } qq_solve_info;
 
 /* ---- context ---- */

@@ -50,6 +50,7 @@ module qqcd_gpu
     real(c_double) :: ritz(1024)
     integer(c_int) :: fallback
     integer(c_int) :: finished_by
+    integer(c_int) :: restarts
   end type qq_solve_info
 
   type, bind(C) :: qq_method

@@ -62,6 +62,27 @@ def test_batch_vs_oracle(setup, solver, precision, deflate, kappa):
         assert interior_rel(xo[i], xo_o, ol.nvhalf) < 1e-7
 
 
+@pytest.mark.parametrize("precision", [16, -16])
+def test_point_source_breakdowns_restart(setup, precision):
+    """A point source makes the textbook shadow residual r0 one spin-colour component at
+    one site, so every <rhat, .> is a single component, which 16-bit storage against the
+    site's norm rounds to exactly zero within a few iterations.  Each such breakdown
+    restarts the right-hand side with its re-inserted FP64 residual as the shadow
+    residual, and the batched iteration converges on its own: no fallback, nothing
+    finished by another method, and (FP16) at least one restart taken."""
+    lat, ol, u = setup
+    be, bo = sources(lat, 4)
+    xe, xo, infos = lat.fermprop_batch(be, bo, (0.150, 0.01), m=16, k=6, precision=precision, rhs_block=4,
+                                       tol=1e-10, solver=1, deflate=0)
+    for i in infos:
+        assert i.status == 0 and i.true_rel <= 1e-10
+        assert i.fallback == 0 and i.finished_by == 0, (i.fallback, i.finished_by, i.restarts)
+    if precision == 16:
+        assert max(i.restarts for i in infos) >= 1, [i.restarts for i in infos]
+    xe_o, xo_o, st, _ = ol.fermprop(be[0], bo[0], (0.150, 0.01), inverter=5, resmax=1e-12, nGMRES=(16, 6))
+    assert interior_rel(xe[0], xe_o, ol.nvhalf) < 1e-7
+
+
 @pytest.mark.parametrize("precision", [32, 16, -16])
 def test_graph_and_host_loops_agree(setup, monkeypatch, precision):
     """The graph-driven loop (one CUDA graph with conditional nodes) and the host-driven

@@ -8,7 +8,8 @@ recon-18 links and two momentum origins.
 discon: Jtotal = (Jvev on levels 2..nsub + the sum over the noises of average(nsub,
 nmom, nop) with the momfacs factors about io) / nnoise / (nx ny nz); the oracle solves
 each noise with its GMRES-DR to 1e-12 and applies its average restatement with the
-reference's own nop = 5; 1e-8 of the largest entry (both sides solve to <= 1e-11)."""
+reference's own nop = 5; 1e-8 of the largest entry when the GPU solves with FP64
+GMRES-DR to 1e-11, 1e-7 with the batched FP32 BiCGStab to 1e-10."""
 import numpy as np
 import pytest
 
@@ -65,8 +66,10 @@ def oracle_discon(ol, noise_kind, nnoise, kappa, nsub, nmom, nop, io):
     return J / nnoise / (DIMS[0] * DIMS[1] * DIMS[2])
 
 
-@pytest.mark.parametrize("noise_kind,nsub,nmom,nop,io", [(2, 6, 5, 5, (1, 1, 1)), (4, 4, 1, 9, (2, 3, 1))])
-def test_discon_matches_oracle(config, noise_kind, nsub, nmom, nop, io):
+@pytest.mark.parametrize("noise_kind,nsub,nmom,nop,io,solver,rtol", [(2, 6, 5, 5, (1, 1, 1), 0, 1e-8),
+                                                                     (4, 4, 1, 9, (2, 3, 1), 0, 1e-8),
+                                                                     (2, 6, 5, 5, (1, 1, 1), 1, 1e-7)])
+def test_discon_matches_oracle(config, noise_kind, nsub, nmom, nop, io, solver, rtol):
     import baylorlqcd_b200 as qq
 
     ol, u = config
@@ -77,11 +80,11 @@ def test_discon_matches_oracle(config, noise_kind, nsub, nmom, nop, io):
         oracle.initlagfib(0, 9)
         want = oracle_discon(ol, noise_kind, nnoise, kappa, nsub, nmom, nop, io)
         qq.initlagfib(0, 9)
-        got, jv, infos = lat.discon(noise_kind, nnoise, kappa, nsub=nsub, nmom=nmom, nop=nop, io=io, solver=0,
-                                    m=30, k=10, tol=1e-11)
+        got, jv, infos = lat.discon(noise_kind, nnoise, kappa, nsub=nsub, nmom=nmom, nop=nop, io=io, solver=solver,
+                                    m=30, k=10, tol=1e-11 if solver == 0 else 1e-10, rhs_block=3)
         assert all(i.status == 0 for i in infos)
         assert got.shape == want.shape
-        assert np.abs(got - want).max() <= 1e-8 * np.abs(want).max()
+        assert np.abs(got - want).max() <= rtol * np.abs(want).max()
         jv_o, _, _ = ol.vev(kappa, io)
         assert np.abs(jv - jv_o).max() <= 1e-12 * np.abs(jv_o).max()
     finally:

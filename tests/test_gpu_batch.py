@@ -107,7 +107,9 @@ def test_graph_and_host_loops_agree(setup, monkeypatch, precision):
     (xg, og, ig), (xh, oh, ih) = res["0"], res["1"]
     for i in range(6):
         assert ig[i].status == 0 and ih[i].status == 0
-        assert ig[i].fallback == 0 and ih[i].fallback == 0
+        assert ig[i].fallback == ih[i].fallback and ig[i].finished_by == ih[i].finished_by
+        if precision != -16:
+            assert ig[i].fallback == 0
         assert ig[i].itercount == ih[i].itercount and ig[i].mvp == ih[i].mvp
         assert len(ig[i].hist) == len(ih[i].hist) > 0
         assert np.array_equal(ig[i].hist, ih[i].hist)
@@ -189,7 +191,10 @@ def test_block_kernel_shapes(setup, monkeypatch, shape, precision, deflate):
                                            tol=1e-10, solver=1, deflate=deflate)
         for i in range(12):
             assert infos[i].status == 0 and infos[i].true_rel <= 1e-10, (i, infos[i])
-            assert infos[i].fallback == 0, (i, infos[i].fallback)
+            if precision == -16:  # 8 significant bits may stall; the FP32 iteration finishes
+                assert infos[i].finished_by in (0, 32), (i, infos[i].fallback, infos[i].finished_by)
+            else:
+                assert infos[i].fallback == 0, (i, infos[i].fallback)
         for i in (0, 7, 11):
             xe_o, xo_o, st, _ = ol.fermprop(be[i], bo[i], kappa, inverter=5, resmax=1e-12, nGMRES=(16, 6))
             assert interior_rel(xe[i], xe_o, ol.nvhalf) < 1e-7

@@ -219,8 +219,10 @@ typedef struct qq_method {
                         residual onto them at each reliable update */
   double defl_tol;   /* relative residual the deflation-building solve stops at */
   int stall_window;  /* solver 1: a right-hand side whose FP64 true residual has not fallen
-                        10x within this many BiCGStab iterations stops and is solved by
-                        plain FP64 GMRES-DR(m, k), as after a breakdown (0: 2000) */
+                        10x within this many BiCGStab iterations stops; a 16-bit one is
+                        continued by the batched FP32 BiCGStab, an FP32 one is solved by
+                        plain FP64 GMRES-DR(m, k), as after a breakdown (0: 2000, and 400
+                        for a 16-bit iteration) */
 } qq_method;
 int qq_fermprop_batch(qq_ctx* ctx, int nrhs, const double* be, const double* bo,
                       const double kappa[2], const qq_method* method, double* xe, double* xo,

@@ -59,7 +59,13 @@ __device__ inline int lex_index(const NetGeom& g, const int* x) {
   return x[0] + g.n[0] * (x[1] + g.n[1] * (x[2] + g.n[2] * x[3]));
 }
 
-__device__ inline float2 cmulf(float2 a, float2 b) { return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+// acc += a b (complex) as four FMAs, two per component.
+__device__ inline void cmacf(float2& acc, float2 a, float2 b) {
+  acc.x = fmaf(a.x, b.x, acc.x);
+  acc.x = fmaf(-a.y, b.y, acc.x);
+  acc.y = fmaf(a.x, b.y, acc.y);
+  acc.y = fmaf(a.y, b.x, acc.y);
+}
 
 // (T_p f)(x) for one channel: v = f at the path's source site, transported to x.
 // Returns false when the path's boundary factor is zero.
@@ -106,9 +112,7 @@ __device__ inline void transport3(const qq::Su3<float>& u, bool back, float fac,
 #pragma unroll
     for (int b = 0; b < 3; ++b) {
       const float2 e = back ? make_float2(u.e[b][a].re, -u.e[b][a].im) : make_float2(u.e[a][b].re, u.e[a][b].im);
-      const float2 m = cmulf(e, v[b]);
-      s.x += m.x;
-      s.y += m.y;
+      cmacf(s, e, v[b]);
     }
     t[a] = make_float2(fac * s.x, fac * s.y);
   }
@@ -149,11 +153,7 @@ __global__ void __launch_bounds__(kNetThreads) ptc_kernel(NetGeom g, const void*
       for (int co = 0; co < COUT; ++co) {
         const float2 wc = sw[(p * COUT + co) * CIN + ci];
 #pragma unroll
-        for (int a = 0; a < 3; ++a) {
-          const float2 m = cmulf(wc, t[a]);
-          acc[co][a].x += m.x;
-          acc[co][a].y += m.y;
-        }
+        for (int a = 0; a < 3; ++a) cmacf(acc[co][a], wc, t[a]);
       }
     }
   }

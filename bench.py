@@ -1,7 +1,7 @@
 #!/usr/bin/env python
 """Benchmark of the qqcd solver hot path on B200.
 
-Workload (the north-star configuration): 24^3x48 quenched SU(3) configuration at
+Workload (configuration C5, the largest single-GPU one): 24^3x48 quenched SU(3) configuration at
 beta = 6.0 (cold start + 500 heatbath sweeps on the GPU), twisted-mass operator at
 kappa = 0.1566, mu = 0.0025 (near critical), periodic space / antiperiodic time, 12
 spin-colour point sources at site (1,1,1,1), every solution to FP64 true full-lattice

@@ -75,6 +75,17 @@ def test_uneven_batch_rejects_bad_arguments_before_device():
     assert b"group 0" in lib.qq_last_error()
 
 
+def test_loop_driver_entry_points_reject_bad_arguments_before_device():
+    """qq_vev and qq_discon check their context and arguments first (no device needed)."""
+    lib = qq.load_library()
+    io = (C.c_int * 3)(1, 1, 1)
+    J = np.zeros(2 * 8 * 6 * 5 * 9)
+    assert lib.qq_vev(None, 0.15, io, J.ctypes.data, None, None) == qq.QQ_BAD_ARG
+    meth = qq.qq_method(16, 6, 32, 4, 1e-10, 0, 0, 0, 1e-5)
+    assert lib.qq_discon(None, 2, 1, 0.15, C.byref(meth), io, 6, 5, 5, J.ctypes.data, None, None) == qq.QQ_BAD_ARG
+    assert b"null" in lib.qq_last_error()
+
+
 def test_missing_gpu_fails_loudly():
     """No CPU fallback: without a device the context cannot be created."""
     if gpu_present():

@@ -13,9 +13,12 @@
 // single-precision value).  The host scales the sums by 8 kappa^4 and the reference's
 // multiplicities and assembles Jvev(2, nt, 5, 5) (:5204-5310), negated.
 //
-// One thread per site, a block per (time slice, split); 65 sums per thread reduced per
-// block in a fixed order (warp shuffles, then the warps in order); the host adds the
-// splits in order.
+// One thread per site, a block per (time slice, split, plane); each plane's code keeps
+// only the sums it adds to (18 to 21 of the 65) and reads the momentum phases
+// from a small table the host fills once per call; the sums are reduced per block in a
+// fixed order (warp shuffles, then the warps in order) and a second kernel adds the splits and
+// planes in order on the device.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -73,14 +76,33 @@ struct Trig {  // cos, sin, cos 2, sin 2 per spatial axis at one corner
   double c[3], s[3], c2[3], s2[3];
 };
 
-template <int RECON>
-__global__ void __launch_bounds__(kVevThreads) vev_kernel(Geom g, const void* gauge, int io0, int io1, int io2,
-                                                          double twoPi, double* partial) {
+constexpr bool in4(int k, int b) { return k >= b && k < b + 4; }
+
+// The sums plane (MU, NU) adds to (0-based directions, MU < NU); the others stay zero
+// for it, so its kernel keeps only these in registers.
+__host__ __device__ constexpr bool vev_touches(int MU, int NU, int k) {
+  return k == (NU == 3 ? V_TSUM : V_SSUM) || in4(k, NU == 3 ? V_MT : V_MS) || (NU == 3 && in4(k, V_J4)) ||
+         (NU == 3 && k == V_J1T + MU) || (NU == 3 && MU == 0 && (in4(k, V_J13T) || in4(k, V_J12T))) ||
+         (NU == 3 && MU == 1 && (in4(k, V_J21T) || in4(k, V_J23T))) ||
+         (NU == 3 && MU == 2 && (in4(k, V_J32T) || in4(k, V_J31T))) ||
+         (MU == 0 && NU != 3 && (in4(k, V_J13S) || in4(k, V_J12S))) ||
+         (((MU == 1 && NU == 2) || (MU == 0 && NU == 1)) && (in4(k, V_J21S) || in4(k, V_J23S))) ||
+         (NU == 2 && (in4(k, V_J32S) || in4(k, V_J31S)));
+}
+
+// One plane (MU, NU) of every site of time slice blockIdx.x, split blockIdx.y of kVevSplit.
+// tab holds the momentum phases: tab[((a * 2 + sh) * 4 + f) * nmax + x] for spatial axis a,
+// 0-based coordinate x shifted by sh, f = cos, sin of twoPi (x + 1 + sh - io_a) / n_a and
+// cos, sin of twice that argument -- the values the reference forms per site, computed
+// once on the host.  partial[((t * kVevSplit + split) * 6 + plane) * kVevVals + k].
+template <int RECON, int MU, int NU>
+__device__ __forceinline__ void vev_plane(const Geom& g, const void* gauge, const double* tab, int nmax,
+                                          double* partial, double (*red)[kVevVals]) {
+  constexpr int kPlane = MU == 0 ? NU - 1 : MU == 1 ? NU + 1 : 5;  // (0,1) .. (2,3) -> 0 .. 5
   const int t = blockIdx.x, split = blockIdx.y;
   const int vs = g.n[0] * g.n[1] * g.n[2];
   const int chunk = (vs + kVevSplit - 1) / kVevSplit;
   const int i0 = split * chunk, i1 = min(vs, i0 + chunk);
-  const int io[3] = {io0, io1, io2};
   double acc[kVevVals];
 #pragma unroll
   for (int k = 0; k < kVevVals; ++k) acc[k] = 0.0;
@@ -92,18 +114,15 @@ __global__ void __launch_bounds__(kVevThreads) vev_kernel(Geom g, const void* ga
     for (int a = 0; a < 3; ++a)
 #pragma unroll
       for (int sh = 0; sh < 2; ++sh) {
-        const double X = (double)(sh + x[a] + 1 - io[a]);
-        const double arg = twoPi * X / (double)g.n[a], arg2 = twoPi * (2.0 * X) / (double)g.n[a];
-        cb[a][sh] = cos(arg);
-        sb[a][sh] = sin(arg);
-        c2b[a][sh] = cos(arg2);
-        s2b[a][sh] = sin(arg2);
+        const double* e = tab + (size_t)(a * 2 + sh) * 4 * nmax + x[a];
+        cb[a][sh] = __ldg(e);
+        sb[a][sh] = __ldg(e + nmax);
+        c2b[a][sh] = __ldg(e + 2 * nmax);
+        s2b[a][sh] = __ldg(e + 3 * nmax);
       }
     Su3<double> umu, unu, ua, ub, s1, s2, P;
-#pragma unroll
-    for (int mu = 0; mu < 3; ++mu)
-#pragma unroll
-      for (int nu = mu + 1; nu < 4; ++nu) {
+      {
+        constexpr int mu = MU, nu = NU;
         int xm[4] = {x[0], x[1], x[2], x[3]}, xn[4] = {x[0], x[1], x[2], x[3]};
         xm[mu] = (xm[mu] + 1) % g.n[mu];
         xn[nu] = (xn[nu] + 1) % g.n[nu];
@@ -116,7 +135,7 @@ __global__ void __launch_bounds__(kVevThreads) vev_kernel(Geom g, const void* ga
         su3_mul_dag(s2, unu, P);               // ... U_nu(x)^+
         const double re = P.e[0][0].re + P.e[1][1].re + P.e[2][2].re;
         const double im = P.e[0][0].im + P.e[1][1].im + P.e[2][2].im;
-        const int M = mu + 1, N = nu + 1;  // the reference's 1-based directions
+        constexpr int M = mu + 1, N = nu + 1;  // the reference's 1-based directions
         // the four corners: 0 site, 1 site + mu, 2 site + nu, 3 site + mu + nu
         Trig cr[4];
 #pragma unroll
@@ -232,22 +251,54 @@ __global__ void __launch_bounds__(kVevThreads) vev_kernel(Geom g, const void* ga
       }
   }
   // block reduction in a fixed order: lanes by shuffles, then the warps in order
-  __shared__ double red[kVevThreads / 32][kVevVals];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 #pragma unroll
   for (int k = 0; k < kVevVals; ++k) {
+    if (!vev_touches(MU, NU, k)) continue;
     double v = acc[k];
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
     if (lane == 0) red[w][k] = v;
   }
   __syncthreads();
+  double* dst = partial + (((size_t)t * kVevSplit + split) * 6 + kPlane) * kVevVals;
   for (int k = threadIdx.x; k < kVevVals; k += blockDim.x) {
     double s = 0.0;
-    for (int ww = 0; ww < kVevThreads / 32; ++ww) s += red[ww][k];
-    partial[((size_t)t * kVevSplit + split) * kVevVals + k] = s;
+    if (vev_touches(MU, NU, k))
+      for (int ww = 0; ww < kVevThreads / 32; ++ww) s += red[ww][k];
+    dst[k] = s;
   }
 }
+
+// The six planes of a slice split: blockIdx.z = 0 .. 5 for (0,1), (0,2), (0,3), (1,2),
+// (1,3), (2,3), so one launch gives every SM several waves of blocks.
+template <int RECON>
+__global__ void __launch_bounds__(kVevThreads) vev_kernel(Geom g, const void* gauge, const double* tab, int nmax,
+                                                          double* partial) {
+  __shared__ double red[kVevThreads / 32][kVevVals];
+  switch (blockIdx.z) {
+    case 0: vev_plane<RECON, 0, 1>(g, gauge, tab, nmax, partial, red); break;
+    case 1: vev_plane<RECON, 0, 2>(g, gauge, tab, nmax, partial, red); break;
+    case 2: vev_plane<RECON, 0, 3>(g, gauge, tab, nmax, partial, red); break;
+    case 3: vev_plane<RECON, 1, 2>(g, gauge, tab, nmax, partial, red); break;
+    case 4: vev_plane<RECON, 1, 3>(g, gauge, tab, nmax, partial, red); break;
+    default: vev_plane<RECON, 2, 3>(g, gauge, tab, nmax, partial, red); break;
+  }
+}
+
+// Per time slice and sum: the splits and planes added in a fixed order (split-major, then
+// plane), so the host copies back nt x 65 values.  One thread per (slice, sum).
+__global__ void vev_fold_kernel(const double* partial, int nt, double* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nt * kVevVals) return;
+  const int t = i / kVevVals, k = i - t * kVevVals;
+  double s = 0.0;
+  for (int sp = 0; sp < kVevSplit; ++sp)
+    for (int pl = 0; pl < 6; ++pl) s += partial[(((size_t)t * kVevSplit + sp) * 6 + pl) * kVevVals + k];
+  out[i] = s;
+}
+
+constexpr int kWsVev = 8192;  // context workspace id of the partial sums and the phase table
 
 }  // namespace
 }  // namespace qq
@@ -260,24 +311,40 @@ extern "C" int qq_vev(qq_ctx* c, double kappa, const int io[3], double* Jvev, do
   QQ_CK(cudaSetDevice(c->device));
   const int nt = c->g.n[3];
   const double V = 2.0 * c->g.vh;
-  DevBuf part;
-  QQ_CK(part.alloc(sizeof(double) * (size_t)nt * kVevSplit * kVevVals));
+  // the momentum phases per axis, coordinate and shift (:4823-4945 forms them per site)
   const double twoPi = (double)6.283185307179586f;  // the reference's default-kind literal
-  count_launch();
+  const int nmax = std::max(c->g.n[0], std::max(c->g.n[1], c->g.n[2]));
+  std::vector<double> tab((size_t)3 * 2 * 4 * nmax, 0.0);
+  for (int a = 0; a < 3; ++a)
+    for (int sh = 0; sh < 2; ++sh)
+      for (int x = 0; x < c->g.n[a]; ++x) {
+        const double X = (double)(sh + x + 1 - io[a]);
+        const double arg = twoPi * X / (double)c->g.n[a], arg2 = twoPi * (2.0 * X) / (double)c->g.n[a];
+        double* e = tab.data() + (size_t)(a * 2 + sh) * 4 * nmax + x;
+        e[0] = std::cos(arg);
+        e[nmax] = std::sin(arg);
+        e[2 * nmax] = std::cos(arg2);
+        e[3 * nmax] = std::sin(arg2);
+      }
+  const size_t npart = (size_t)nt * kVevSplit * 6 * kVevVals;
+  const size_t nout = (size_t)nt * kVevVals;
+  double* dp = nullptr;
+  QQ_CK(ws_get(c, kWsVev, sizeof(double) * (npart + nout + tab.size()), reinterpret_cast<void**>(&dp)));
+  double* dout = dp + npart;
+  double* dtab = dout + nout;
+  QQ_CK(cudaMemcpyAsync(dtab, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice, c->st));
+  const dim3 grd(nt, kVevSplit, 6);
+  count_launch(2);
   if (c->recon64 == 18)
-    vev_kernel<18><<<dim3(nt, kVevSplit), kVevThreads, 0, c->st>>>(c->g, c->gauge64.p, io[0], io[1], io[2], twoPi,
-                                                                     part.as<double>());
+    vev_kernel<18><<<grd, kVevThreads, 0, c->st>>>(c->g, c->gauge64.p, dtab, nmax, dp);
   else
-    vev_kernel<12><<<dim3(nt, kVevSplit), kVevThreads, 0, c->st>>>(c->g, c->gauge64.p, io[0], io[1], io[2], twoPi,
-                                                                     part.as<double>());
+    vev_kernel<12><<<grd, kVevThreads, 0, c->st>>>(c->g, c->gauge64.p, dtab, nmax, dp);
   QQ_CK(cudaGetLastError());
-  std::vector<double> h((size_t)nt * kVevSplit * kVevVals);
-  QQ_CK(cudaMemcpyAsync(h.data(), part.p, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, c->st));
+  vev_fold_kernel<<<(unsigned)((nout + 255) / 256), 256, 0, c->st>>>(dp, nt, dout);
+  QQ_CK(cudaGetLastError());
+  std::vector<double> S(nout);  // per slice
+  QQ_CK(cudaMemcpyAsync(S.data(), dout, sizeof(double) * nout, cudaMemcpyDeviceToHost, c->st));
   QQ_CK(cudaStreamSynchronize(c->st));
-  std::vector<double> S((size_t)nt * kVevVals, 0.0);  // per slice
-  for (int t = 0; t < nt; ++t)
-    for (int sp = 0; sp < kVevSplit; ++sp)
-      for (int k = 0; k < kVevVals; ++k) S[(size_t)t * kVevVals + k] += h[((size_t)t * kVevSplit + sp) * kVevVals + k];
   auto at = [&](int t, int k) -> double& { return S[(size_t)t * kVevVals + k]; };
   // :5204-5232: the plaquette average, then the normalisations
   double pl = 0.0;

@@ -21,6 +21,13 @@ INCLUDE = HERE.parent / "include"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
               "--expt-relaxed-constexpr", "-I", str(INCLUDE)]
+# Host-code flags of single sources.  The eigen-iteration's dense Schur step on the host
+# takes nearly all of an eigenmode solve's time; with AVX2 (x86-64-v3, the level the
+# oracle's timing build also assumes) and the plain complex multiply and divide formulas
+# (its values are finite and of modest size: no NaN recovery or range reduction needed)
+# it runs about twice as fast.  Contraction stays off.
+HOST_FLAGS = {"qq_eigen.cu": ["-Xcompiler", "-march=x86-64-v3", "-Xcompiler", "-fcx-limited-range",
+                              "-Xcompiler", "-ffp-contract=off"]}
 
 
 def _nvcc() -> str:
@@ -37,7 +44,7 @@ def _compile(src: Path, hdr_time: float) -> Path:
     obj = BUILD / (src.stem + ".o")
     if obj.exists() and obj.stat().st_mtime >= max(src.stat().st_mtime, hdr_time):
         return obj
-    cmd = [_nvcc(), *ARCH, *NVCC_FLAGS, "-c", str(src), "-o", str(obj)]
+    cmd = [_nvcc(), *ARCH, *NVCC_FLAGS, *HOST_FLAGS.get(src.name, []), "-c", str(src), "-o", str(obj)]
     res = subprocess.run(cmd, capture_output=True, text=True)
     if res.returncode != 0:
         raise RuntimeError(f"nvcc failed for {src.name}:\n{res.stderr}")

@@ -22,8 +22,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
               "--expt-relaxed-constexpr", "-I", str(INCLUDE)]
 # Host-code flags of single sources.  The eigen-iteration's dense Schur step on the host
-# takes nearly all of an eigenmode solve's time; with AVX2 (x86-64-v3, the level the
-# oracle's timing build also assumes) and the plain complex multiply and divide formulas
+# takes nearly all of an eigenmode solve's time; with AVX2 (x86-64-v3, present on the
+# B200 hosts' CPUs) and the plain complex multiply and divide formulas
 # (its values are finite and of modest size: no NaN recovery or range reduction needed)
 # it runs about twice as fast.  Contraction stays off.
 HOST_FLAGS = {"qq_eigen.cu": ["-Xcompiler", "-march=x86-64-v3", "-Xcompiler", "-fcx-limited-range",

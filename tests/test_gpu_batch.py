@@ -108,8 +108,10 @@ def test_graph_and_host_loops_agree(setup, monkeypatch, precision):
     for i in range(6):
         assert ig[i].status == 0 and ih[i].status == 0
         assert ig[i].fallback == ih[i].fallback and ig[i].finished_by == ih[i].finished_by
-        if precision != -16:
+        if precision == 32:
             assert ig[i].fallback == 0
+        else:  # a 16-bit iteration may stall (400-iteration window); the FP32 one finishes it
+            assert ig[i].finished_by in (0, 32)
         assert ig[i].itercount == ih[i].itercount and ig[i].mvp == ih[i].mvp
         assert len(ig[i].hist) == len(ih[i].hist) > 0
         assert np.array_equal(ig[i].hist, ih[i].hist)
